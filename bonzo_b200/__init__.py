@@ -1,0 +1,6 @@
+"""bonzo_b200: B200-native VL2 + HLLD + CT MHD step with the bonzo interface.
+
+Host-side modules are importable without a GPU; the compute path lives in
+libbnzgpu.so (built by bonzo_b200/build.py) and has no CPU fallback.
+"""
+__version__ = "0.1.0"

@@ -1,0 +1,220 @@
+"""ctypes binding of libbnzgpu.so (the C ABI in include/bnz_gpu.h).
+
+The library is built in-tree by bonzo_b200/build.py.  There is no CPU
+fallback: if the shared library is missing, or no CUDA device is visible, the
+calls fail loudly with BnzError.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbnzgpu.so")
+
+BNZ_OK, BNZ_ERR_ARG, BNZ_ERR_CUDA, BNZ_ERR_STATE, BNZ_ERR_UNSUPPORTED, BNZ_ERR_TIMEOUT, BNZ_ERR_NOMEM = range(7)
+STATUS_NAMES = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "non-physical state",
+                4: "unsupported", 5: "timeout", 6: "out of memory"}
+RS = {"hll": 0, "hllc": 1, "hlld": 2, "hllt": 3}
+RCN = {"const": 0, "linear": 1}
+LIM = {"vl": 0, "mc": 1, "mm": 2}
+TC = {"iso": 0, "aniso": 1}
+PATH = {"fused": 0, "plain": 1}
+
+# every entry point include/bnz_gpu.h declares (checked by the CPU tests)
+EXPORTS = [
+    "bnz_create", "bnz_destroy", "bnz_last_error", "bnz_shape", "bnz_set_state", "bnz_init",
+    "bnz_get_state", "bnz_apply_bc", "bnz_new_dt", "bnz_vl2_step", "bnz_diffuse", "bnz_advance",
+    "bnz_get_time", "bnz_set_time", "bnz_check", "bnz_sync", "bnz_advance_graph",
+    "bnz_device_state", "bnz_stream",
+]
+
+
+class BnzError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (STATUS_NAMES.get(code, "error"), code, msg))
+        self.code = code
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("Nx", C.c_int), ("Ny", C.c_int), ("Nz", C.c_int), ("dims", C.c_int),
+                ("lmin", C.c_double * 3), ("lmax", C.c_double * 3), ("bc", (C.c_int * 2) * 3)]
+
+
+class MethodDesc(C.Structure):
+    _fields_ = [("gam", C.c_double), ("cour", C.c_double),
+                ("rsolver", C.c_int), ("reconstr", C.c_int), ("limiter", C.c_int),
+                ("charact_proj", C.c_int),
+                ("kappa0", C.c_double), ("thcond_type", C.c_int), ("sat_hfe", C.c_int),
+                ("cour_diff", C.c_double), ("fixdt", C.c_int), ("dt_fixed", C.c_double),
+                ("outflow_face_aware", C.c_int), ("exact_fp", C.c_int), ("path", C.c_int)]
+
+
+_dp = C.POINTER(C.c_double)
+_lib = None
+
+
+def load():
+    """Load libbnzgpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise BnzError(BNZ_ERR_UNSUPPORTED, "libbnzgpu.so not built: run bonzo_b200/build.py "
+                       "(no CPU fallback exists)")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.bnz_create.argtypes = [C.POINTER(GridDesc), C.POINTER(MethodDesc), C.POINTER(vp)]
+    L.bnz_destroy.argtypes = [vp]
+    L.bnz_last_error.argtypes = [vp]
+    L.bnz_last_error.restype = C.c_char_p
+    L.bnz_shape.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.bnz_set_state.argtypes = [vp, _dp, C.c_int, _dp]
+    L.bnz_init.argtypes = [vp]
+    L.bnz_get_state.argtypes = [vp, _dp, _dp, _dp]
+    L.bnz_apply_bc.argtypes = [vp, C.c_uint32]
+    L.bnz_new_dt.argtypes = [vp, _dp]
+    L.bnz_vl2_step.argtypes = [vp, C.c_double]
+    L.bnz_diffuse.argtypes = [vp, C.c_double, C.POINTER(C.c_int)]
+    L.bnz_advance.argtypes = [vp, C.c_double, C.c_int, _dp, C.POINTER(C.c_long)]
+    L.bnz_get_time.argtypes = [vp, _dp, C.POINTER(C.c_long), _dp]
+    L.bnz_set_time.argtypes = [vp, C.c_double, C.c_long]
+    L.bnz_check.argtypes = [vp, C.POINTER(C.c_uint32)]
+    L.bnz_sync.argtypes = [vp]
+    L.bnz_advance_graph.argtypes = [vp, C.c_double, C.c_int]
+    L.bnz_device_state.argtypes = [vp, C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp)]
+    L.bnz_stream.argtypes = [vp, C.POINTER(vp)]
+    _lib = L
+    return L
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"], "float64 C-contiguous array expected"
+    return a.ctypes.data_as(_dp)
+
+
+class Context:
+    """One grid on the device (owns a bnz_ctx)."""
+
+    def __init__(self, Nx, Ny=1, Nz=1, dims=2, lmin=(0., 0., 0.), lmax=(1., 1., 1.),
+                 bc=((0, 0), (0, 0), (0, 0)), gam=5. / 3, cour=0.4, rsolver="hlld",
+                 reconstr="linear", limiter="vl", charact_proj=0, kappa0=0.0,
+                 thcond_type="aniso", sat_hfe=0, cour_diff=0.5, fixdt=False, dt_fixed=0.0,
+                 outflow_face_aware=1, exact_fp=False, path="plain"):
+        self.L = load()
+        g = GridDesc()
+        g.Nx, g.Ny, g.Nz, g.dims = Nx, Ny, Nz, dims
+        for a in range(3):
+            g.lmin[a], g.lmax[a] = lmin[a], lmax[a]
+            g.bc[a][0], g.bc[a][1] = bc[a][0], bc[a][1]
+        m = MethodDesc()
+        m.gam, m.cour = gam, cour
+        m.rsolver = RS[rsolver] if isinstance(rsolver, str) else rsolver
+        m.reconstr = RCN[reconstr] if isinstance(reconstr, str) else reconstr
+        m.limiter = LIM[limiter] if isinstance(limiter, str) else limiter
+        m.charact_proj = charact_proj
+        m.kappa0, m.thcond_type, m.sat_hfe, m.cour_diff = kappa0, TC[thcond_type], sat_hfe, cour_diff
+        m.fixdt, m.dt_fixed = int(bool(fixdt)), dt_fixed
+        m.outflow_face_aware, m.exact_fp = outflow_face_aware, int(bool(exact_fp))
+        m.path = PATH[path] if isinstance(path, str) else path
+        self.grid_desc, self.method_desc = g, m
+        h = C.c_void_p()
+        rc = self.L.bnz_create(C.byref(g), C.byref(m), C.byref(h))
+        self.h = h
+        if rc != BNZ_OK:
+            msg = self.L.bnz_last_error(h).decode() if h.value else "bnz_create failed"
+            self.L.bnz_destroy(h)
+            self.h = C.c_void_p()
+            raise BnzError(rc, msg)
+        nt = (C.c_int * 3)()
+        ng = C.c_int()
+        self.L.bnz_shape(h, nt, C.byref(ng))
+        self.shape = (nt[2], nt[1], nt[0])
+        self.ng = ng.value
+
+    def _ck(self, rc):
+        if rc != BNZ_OK:
+            raise BnzError(rc, self.L.bnz_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.bnz_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, prim_or_cons, bfld=None, is_prim=True):
+        a = np.ascontiguousarray(prim_or_cons, dtype=np.float64)
+        if a.shape != (9,) + self.shape:
+            raise ValueError("state must have shape %s" % ((9,) + self.shape,))
+        b = None
+        if bfld is not None:
+            b = np.ascontiguousarray(bfld, dtype=np.float64)
+            if b.shape != (3,) + self.shape:
+                raise ValueError("bfld must have shape %s" % ((3,) + self.shape,))
+        self._ck(self.L.bnz_set_state(self.h, _p(a), int(bool(is_prim)), _p(b)))
+
+    def init(self):
+        self._ck(self.L.bnz_init(self.h))
+
+    def get_state(self, prim=True, cons=True, bfld=True):
+        P = np.empty((9,) + self.shape) if prim else None
+        U = np.empty((9,) + self.shape) if cons else None
+        B = np.empty((3,) + self.shape) if bfld else None
+        self._ck(self.L.bnz_get_state(self.h, _p(P), _p(U), _p(B)))
+        return P, U, B
+
+    def apply_bc(self, mask=0xFFF):
+        self._ck(self.L.bnz_apply_bc(self.h, mask))
+
+    def new_dt(self):
+        dt = C.c_double()
+        self._ck(self.L.bnz_new_dt(self.h, C.byref(dt)))
+        return dt.value
+
+    def step(self, dt):
+        self._ck(self.L.bnz_vl2_step(self.h, dt))
+
+    def diffuse(self, dt):
+        n = C.c_int()
+        self._ck(self.L.bnz_diffuse(self.h, dt, C.byref(n)))
+        return n.value
+
+    def advance(self, tmax, max_steps=0):
+        t = C.c_double()
+        s = C.c_long()
+        self._ck(self.L.bnz_advance(self.h, tmax, max_steps, C.byref(t), C.byref(s)))
+        return t.value, s.value
+
+    def time(self):
+        t, s, d = C.c_double(), C.c_long(), C.c_double()
+        self._ck(self.L.bnz_get_time(self.h, C.byref(t), C.byref(s), C.byref(d)))
+        return t.value, s.value, d.value
+
+    def check(self):
+        """Raises BnzError(BNZ_ERR_STATE) if the device flagged a non-physical state."""
+        bits = C.c_uint32()
+        self._ck(self.L.bnz_check(self.h, C.byref(bits)))
+        return bits.value
+
+    def sync(self):
+        self._ck(self.L.bnz_sync(self.h))
+
+    def advance_graph(self, tmax, nsteps):
+        self._ck(self.L.bnz_advance_graph(self.h, tmax, nsteps))
+
+    def device_state(self):
+        p, u, b = _dp(), _dp(), _dp()
+        self._ck(self.L.bnz_device_state(self.h, C.byref(p), C.byref(u), C.byref(b)))
+        return (C.cast(p, C.c_void_p).value, C.cast(u, C.c_void_p).value, C.cast(b, C.c_void_p).value)
+
+    def stream(self):
+        s = C.c_void_p()
+        self._ck(self.L.bnz_stream(self.h, C.byref(s)))
+        return s.value

@@ -1,0 +1,66 @@
+// bnz_common.h -- structures shared by the host context and the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+// Grid geometry as the kernels see it.  Index conventions follow the
+// reference's GridCoord (src/coordinates/coord_c.h:19-99): Ntot cells per axis
+// including ng ghosts on active axes, active range i1..i2 / j1..j2 / k1..k2,
+// per-axis spacing arrays indexed by the cell index along that axis.
+struct GridDev {
+  int nx, ny, nz;     // Ntot per axis
+  int dims, ng;
+  int i1, i2, j1, j2, k1, k2;
+  long long sv;       // stride between variables: nx*ny*nz
+  double gam;
+  const double* dlf[3];      // face spacing lf[i+1]-lf[i]
+  const double* dlf_inv[3];
+  const double* lf[3];       // face coordinates (Ntot+1 entries)
+  const double* lv[3];       // volume (centre) coordinates
+  const double* dlv_inv[3];  // inverse centre spacing
+};
+
+// Device buffers and options used by one step of one grid.
+struct StepArgs {
+  GridDev g;
+  double* prim;
+  double* cons;
+  double* bfld;
+  double* cons_s;  // predictor conserved state (plain path)
+  double* bfld_s;  // predictor face field (plain path)
+  double* flx[3];  // Godunov fluxes (plain path)
+  double* ec;      // cell-centred E (plain path)
+  double* ee;      // edge E (plain path)
+  double* wnext;   // fused path: output prim buffer
+  double* bnext;   // fused path: output face-B buffer
+  unsigned* err;   // sticky device error word
+  int rsolver, reconstr_order, limiter, charact_proj;
+  int bc[3][2];
+  int face_aware;
+  cudaStream_t stream;
+};
+
+// Device time-step record used by graph-captured stepping.
+struct DtState {
+  double dt;          // step used by the current step
+  double time;        // simulation time after the last completed step
+  double tmax;        // clip target
+  unsigned long long cdsmax_bits;  // max of (|v|+cf)/dx as a bit pattern
+  long long step;
+};
+
+// Conduction scratch (thcond_elec.pyx DiffScratch).
+struct DiffArgs {
+  double* temp;
+  double* fx;
+  double* fy;
+  double* fz;
+  double* pres0;
+  double* presm1;
+  double* dtemp;
+  double* dtemp0;
+  double kappa0;
+  int aniso, sat;
+  double cour_diff;
+};

@@ -1,0 +1,608 @@
+// bnz_ctx.cu -- host side of the C ABI declared in include/bnz_gpu.h.
+//
+// One context = one grid (BnzGrid + BnzIntegr of the reference): coordinates,
+// device state, scratch and the CUDA stream its calls are ordered on.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/bnz_gpu.h"
+#include "bnz_common.h"
+#include "bnz_launch.h"
+
+struct bnz_ctx {
+  bnz_grid_desc gd;
+  bnz_method_desc md;
+  int Ntot[3];
+  int ng;
+  int i1, i2, j1, j2, k1, k2;
+  size_t ncell;
+  std::vector<double> lf[3], lv[3], dlf[3], dlf_inv[3], dlv[3], dlv_inv[3];
+  double* d_coord = nullptr;
+  GridDev g;
+  // state and scratch
+  double* prim = nullptr;
+  double* cons = nullptr;
+  double* bfld = nullptr;
+  double* cons_s = nullptr;
+  double* bfld_s = nullptr;
+  double* flx[3] = {nullptr, nullptr, nullptr};
+  double* ec = nullptr;
+  double* ee = nullptr;
+  double* wnext = nullptr;
+  double* bnext = nullptr;
+  // conduction scratch
+  double* dscr = nullptr;
+  DiffArgs da;
+  int last_nsts = 0;
+  // device scalars
+  unsigned* d_err = nullptr;
+  DtState* d_ds = nullptr;
+  double* d_sts = nullptr;  // stage coefficients (4 per stage)
+  int sts_cap = 0;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  double graph_tmax = -1.;
+  const Launchers* L = nullptr;
+  std::string err;
+  double time = 0.;
+  long step = 0;
+  double last_dt = 0.;
+};
+
+namespace {
+
+int fail(bnz_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+#define CKC(call)                                                                                \
+  do {                                                                                           \
+    cudaError_t _e = (call);                                                                     \
+    if (_e != cudaSuccess)                                                                       \
+      return fail(c, BNZ_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e));         \
+  } while (0)
+
+// coord.pyx:122-258 (uniform axes) + cartesian.pyx:18-43: face coordinates,
+// periodic / reflected ghost spacings, centres and spacings.
+void set_coordinates(bnz_ctx* c) {
+  for (int n = 0; n < 3; ++n) {
+    int Ntot = c->Ntot[n];
+    std::vector<double>& lf = c->lf[n];
+    lf.assign(Ntot + 1, 0.);
+    if (Ntot == 1) {
+      lf[0] = c->gd.lmin[n];
+      lf[1] = c->gd.lmax[n];
+    } else {
+      int ind1 = n == 0 ? c->i1 : n == 1 ? c->j1 : c->k1;
+      int ind2 = n == 0 ? c->i2 : n == 1 ? c->j2 : c->k2;
+      int Nact = ind2 - ind1 + 1;
+      double dx = (c->gd.lmax[n] - c->gd.lmin[n]) / Nact;
+      double l1 = 0 * Nact * dx;
+      for (int i = 0; i < Ntot + 1; ++i) lf[i] = l1 + (i - ind1) * dx;
+      int b0 = c->gd.bc[n][0], b1 = c->gd.bc[n][1];
+      if (b0 == BNZ_BC_PERIODIC)
+        for (int i = ind1 - 1; i > -1; --i) {
+          int i_ = ind2 - i + (ind1 - 1);
+          double d = lf[i_ + 1] - lf[i_];
+          lf[i] = lf[i + 1] - d;
+        }
+      if (b1 == BNZ_BC_PERIODIC)
+        for (int i = ind2 + 1; i < Ntot; ++i) {
+          int i_ = ind1 + i - (ind2 + 1);
+          double d = lf[i_ + 1] - lf[i_];
+          lf[i + 1] = lf[i] + d;
+        }
+      if (b0 == BNZ_BC_REFLECT)
+        for (int i = ind1 - 1; i > -1; --i) {
+          int i_ = ind1 - i + (ind1 - 1);
+          double d = lf[i_ + 1] - lf[i_];
+          lf[i] = lf[i + 1] - d;
+        }
+      if (b1 == BNZ_BC_REFLECT)
+        for (int i = ind2 + 1; i < Ntot; ++i) {
+          int i_ = ind2 - i + (ind2 + 1);
+          double d = lf[i_ + 1] - lf[i_];
+          lf[i + 1] = lf[i] + d;
+        }
+    }
+    c->dlf[n].assign(Ntot, 0.);
+    c->dlf_inv[n].assign(Ntot, 0.);
+    c->lv[n].assign(Ntot, 0.);
+    c->dlv[n].assign(Ntot, 0.);
+    c->dlv_inv[n].assign(Ntot, 0.);
+    for (int i = 0; i < Ntot; ++i) {
+      c->dlf[n][i] = lf[i + 1] - lf[i];
+      c->dlf_inv[n][i] = 1. / c->dlf[n][i];
+      c->lv[n][i] = 0.5 * (lf[i] + lf[i + 1]);
+    }
+    for (int i = 1; i < Ntot; ++i) {
+      c->dlv[n][i] = c->lv[n][i] - c->lv[n][i - 1];
+      c->dlv_inv[n][i] = 1. / c->dlv[n][i];
+    }
+  }
+}
+
+StepArgs step_args(bnz_ctx* c) {
+  StepArgs a;
+  memset(&a, 0, sizeof a);
+  a.g = c->g;
+  a.prim = c->prim;
+  a.cons = c->cons;
+  a.bfld = c->bfld;
+  a.cons_s = c->cons_s;
+  a.bfld_s = c->bfld_s;
+  // unused axes alias the x fluxes (never read there)
+  for (int d = 0; d < 3; ++d) a.flx[d] = c->flx[d] ? c->flx[d] : c->flx[0];
+  a.ec = c->ec;
+  a.ee = c->ee;
+  a.wnext = c->wnext;
+  a.bnext = c->bnext;
+  a.err = c->d_err;
+  a.rsolver = c->md.rsolver;
+  a.reconstr_order = c->md.reconstr == BNZ_RCN_CONST ? 0 : 1;
+  a.limiter = c->md.limiter;
+  a.charact_proj = c->md.charact_proj;
+  for (int x = 0; x < 3; ++x) {
+    a.bc[x][0] = c->gd.bc[x][0];
+    a.bc[x][1] = c->gd.bc[x][1];
+  }
+  a.face_aware = c->md.outflow_face_aware;
+  a.stream = c->stream;
+  return a;
+}
+
+void free_all(bnz_ctx* c) {
+  double** bufs[] = {&c->d_coord, &c->prim, &c->cons, &c->bfld, &c->cons_s, &c->bfld_s, &c->flx[0],
+                     &c->flx[1], &c->flx[2], &c->ec, &c->ee, &c->wnext, &c->bnext, &c->dscr, &c->d_sts};
+  for (double** b : bufs)
+    if (*b) {
+      cudaFree(*b);
+      *b = nullptr;
+    }
+  if (c->d_err) cudaFree(c->d_err);
+  if (c->d_ds) cudaFree(c->d_ds);
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  c->d_err = nullptr;
+  c->d_ds = nullptr;
+  c->graph = nullptr;
+  c->stream = nullptr;
+}
+
+bool fused_available(const bnz_grid_desc*, const bnz_method_desc*) { return false; }
+
+int validate(const bnz_grid_desc* g, const bnz_method_desc* m, std::string& why) {
+  if (g->dims < 1 || g->dims > 3) return why = "dims must be 1, 2 or 3", 0;
+  if (g->Nx < 1 || (g->dims >= 2 && g->Ny < 1) || (g->dims >= 3 && g->Nz < 1)) return why = "grid size < 1", 0;
+  if (g->dims < 2 && g->Ny != 1) return why = "cannot set Ny>1 without second dimension", 0;
+  if (g->dims < 3 && g->Nz != 1) return why = "cannot set Nz>1 without third dimension", 0;
+  for (int a = 0; a < g->dims; ++a) {
+    if (!(g->lmax[a] > g->lmin[a])) return why = "lmax must exceed lmin", 0;
+    for (int s = 0; s < 2; ++s)
+      if (g->bc[a][s] < 0 || g->bc[a][s] > 2) return why = "bc flag must be 0 (periodic), 1 (outflow) or 2 (reflect)", 0;
+    if ((g->bc[a][0] == BNZ_BC_PERIODIC) != (g->bc[a][1] == BNZ_BC_PERIODIC))
+      return why = "periodic boundaries must be set on both sides of an axis", 0;
+  }
+  if (!(m->gam > 1.)) return why = "gam must exceed 1", 0;
+  if (!(m->cour > 0.)) return why = "cour must be positive", 0;
+  if (m->rsolver != BNZ_RS_HLL && m->rsolver != BNZ_RS_HLLD && m->rsolver != BNZ_RS_HLLT)
+    return why = "rsolver must be hll, hlld or hllt for MHD (hllc is hydro-only in the reference)", 0;
+  if (m->reconstr != BNZ_RCN_CONST && m->reconstr != BNZ_RCN_LINEAR) return why = "reconstr must be const or linear", 0;
+  if (m->limiter < 0 || m->limiter > 2) return why = "limiter must be vl, mc or mm", 0;
+  if (m->charact_proj) return why = "charact_proj=1 is not supported by the device kernels", 0;
+  if (m->kappa0 < 0.) return why = "kappa0 must be >= 0", 0;
+  if (m->kappa0 > 0. && !(m->cour_diff > 0.)) return why = "cour_diff must be positive", 0;
+  if (m->path != BNZ_PATH_FUSED && m->path != BNZ_PATH_PLAIN) return why = "path must be fused or plain", 0;
+  if (m->path == BNZ_PATH_FUSED && !fused_available(g, m)) return why = "fused path not available for this grid", 0;
+  int ng = m->reconstr == BNZ_RCN_CONST ? 2 : 3;
+  int N[3] = {g->Nx, g->Ny, g->Nz};
+  for (int a = 0; a < g->dims; ++a)
+    if (N[a] < ng) return why = "each active axis needs at least ng cells", 0;
+  return 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bnz_create(const bnz_grid_desc* gd, const bnz_method_desc* md, bnz_ctx** out) {
+  if (!gd || !md || !out) return BNZ_ERR_ARG;
+  *out = nullptr;
+  std::string why;
+  bnz_ctx* c = new bnz_ctx();
+  if (!validate(gd, md, why)) {
+    // a context is still returned so that bnz_last_error can report why
+    c->err = why;
+    *out = c;
+    return BNZ_ERR_ARG;
+  }
+  c->gd = *gd;
+  c->md = *md;
+  c->ng = md->reconstr == BNZ_RCN_CONST ? 2 : 3;
+  int dims = gd->dims, ng = c->ng;
+  int Na[3] = {gd->Nx, dims >= 2 ? gd->Ny : 1, dims >= 3 ? gd->Nz : 1};
+  for (int a = 0; a < 3; ++a) c->Ntot[a] = a < dims ? Na[a] + 2 * ng : 1;
+  c->i1 = ng;
+  c->i2 = Na[0] + ng - 1;
+  c->j1 = dims >= 2 ? ng : 0;
+  c->j2 = dims >= 2 ? Na[1] + ng - 1 : 0;
+  c->k1 = dims >= 3 ? ng : 0;
+  c->k2 = dims >= 3 ? Na[2] + ng - 1 : 0;
+  c->ncell = (size_t)c->Ntot[0] * c->Ntot[1] * c->Ntot[2];
+  set_coordinates(c);
+  c->L = md->exact_fp ? &exact::table : &fast::table;
+
+  cudaError_t e;
+#define ALLOC(ptr, bytes)                                                                      \
+  do {                                                                                         \
+    e = cudaMalloc((void**)&(ptr), (bytes));                                                   \
+    if (e != cudaSuccess) {                                                                    \
+      int code = e == cudaErrorMemoryAllocation ? BNZ_ERR_NOMEM : BNZ_ERR_CUDA;                \
+      c->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);                            \
+      free_all(c);                                                                             \
+      *out = c;                                                                                \
+      return code;                                                                             \
+    }                                                                                          \
+  } while (0)
+
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    c->err = std::string("cudaStreamCreate: ") + cudaGetErrorString(e);
+    *out = c;
+    return BNZ_ERR_CUDA;
+  }
+  // coordinates: 5 arrays per axis, each Ntot+1 long
+  size_t ncoord = 0;
+  for (int a = 0; a < 3; ++a) ncoord += 5 * (size_t)(c->Ntot[a] + 1);
+  ALLOC(c->d_coord, ncoord * sizeof(double));
+  {
+    std::vector<double> h(ncoord, 0.);
+    size_t off = 0;
+    const double* ptrs[3][5];
+    for (int a = 0; a < 3; ++a) {
+      const std::vector<double>* src[5] = {&c->dlf[a], &c->dlf_inv[a], &c->lf[a], &c->lv[a], &c->dlv_inv[a]};
+      for (int q = 0; q < 5; ++q) {
+        std::copy(src[q]->begin(), src[q]->end(), h.begin() + off);
+        ptrs[a][q] = c->d_coord + off;
+        off += c->Ntot[a] + 1;
+      }
+    }
+    e = cudaMemcpy(c->d_coord, h.data(), ncoord * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      c->err = std::string("cudaMemcpy: ") + cudaGetErrorString(e);
+      free_all(c);
+      *out = c;
+      return BNZ_ERR_CUDA;
+    }
+    GridDev& g = c->g;
+    g.nx = c->Ntot[0];
+    g.ny = c->Ntot[1];
+    g.nz = c->Ntot[2];
+    g.dims = dims;
+    g.ng = ng;
+    g.i1 = c->i1; g.i2 = c->i2; g.j1 = c->j1; g.j2 = c->j2; g.k1 = c->k1; g.k2 = c->k2;
+    g.sv = (long long)c->ncell;
+    g.gam = md->gam;
+    for (int a = 0; a < 3; ++a) {
+      g.dlf[a] = ptrs[a][0];
+      g.dlf_inv[a] = ptrs[a][1];
+      g.lf[a] = ptrs[a][2];
+      g.lv[a] = ptrs[a][3];
+      g.dlv_inv[a] = ptrs[a][4];
+    }
+  }
+  size_t n9 = 9 * c->ncell * sizeof(double), n3 = 3 * c->ncell * sizeof(double);
+  ALLOC(c->prim, n9);
+  ALLOC(c->cons, n9);
+  ALLOC(c->bfld, n3);
+  if (md->path == BNZ_PATH_PLAIN) {
+    ALLOC(c->cons_s, n9);
+    ALLOC(c->bfld_s, n3);
+    for (int d = 0; d < dims; ++d) ALLOC(c->flx[d], n9);
+    ALLOC(c->ec, n3);
+    ALLOC(c->ee, n3);
+  } else {
+    ALLOC(c->wnext, n9);
+    ALLOC(c->bnext, n3);
+  }
+  if (md->kappa0 > 0.) {
+    ALLOC(c->dscr, 8 * c->ncell * sizeof(double));
+    double* p = c->dscr;
+    c->da.temp = p;
+    c->da.fx = p + c->ncell;
+    c->da.fy = p + 2 * c->ncell;
+    c->da.fz = p + 3 * c->ncell;
+    c->da.pres0 = p + 4 * c->ncell;
+    c->da.presm1 = p + 5 * c->ncell;
+    c->da.dtemp = p + 6 * c->ncell;
+    c->da.dtemp0 = p + 7 * c->ncell;
+    c->da.kappa0 = md->kappa0;
+    c->da.aniso = md->thcond_type == BNZ_TC_ANISO;
+    c->da.sat = md->sat_hfe;
+    c->da.cour_diff = md->cour_diff;
+    e = cudaMemsetAsync(c->dscr, 0, 8 * c->ncell * sizeof(double), c->stream);
+  }
+  e = cudaMalloc((void**)&c->d_err, sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_ds, sizeof(DtState));
+  if (e != cudaSuccess) {
+    c->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    free_all(c);
+    *out = c;
+    return BNZ_ERR_NOMEM;
+  }
+  cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), c->stream);
+  cudaMemsetAsync(c->d_ds, 0, sizeof(DtState), c->stream);
+  cudaMemsetAsync(c->prim, 0, n9, c->stream);
+  cudaMemsetAsync(c->cons, 0, n9, c->stream);
+  cudaMemsetAsync(c->bfld, 0, n3, c->stream);
+  if (c->cons_s) cudaMemsetAsync(c->cons_s, 0, n9, c->stream);
+  if (c->bfld_s) cudaMemsetAsync(c->bfld_s, 0, n3, c->stream);
+  for (int d = 0; d < dims; ++d)
+    if (c->flx[d]) cudaMemsetAsync(c->flx[d], 0, n9, c->stream);
+  e = cudaStreamSynchronize(c->stream);
+  *out = c;
+  if (e != cudaSuccess) return fail(c, BNZ_ERR_CUDA, std::string("init: ") + cudaGetErrorString(e));
+  return BNZ_OK;
+#undef ALLOC
+}
+
+int bnz_destroy(bnz_ctx* c) {
+  if (!c) return BNZ_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_all(c);
+  delete c;
+  return BNZ_OK;
+}
+
+const char* bnz_last_error(const bnz_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int bnz_shape(const bnz_ctx* c, int* ntot, int* ng) {
+  if (!c) return BNZ_ERR_ARG;
+  if (ntot)
+    for (int a = 0; a < 3; ++a) ntot[a] = c->Ntot[a];
+  if (ng) *ng = c->ng;
+  return BNZ_OK;
+}
+
+int bnz_set_state(bnz_ctx* c, const double* pc, int is_prim, const double* bfld) {
+  if (!c || !pc) return fail(c, BNZ_ERR_ARG, "null state pointer");
+  if (!c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
+  size_t n9 = 9 * c->ncell * sizeof(double), n3 = 3 * c->ncell * sizeof(double);
+  CKC(cudaMemcpyAsync(is_prim ? c->prim : c->cons, pc, n9, cudaMemcpyHostToDevice, c->stream));
+  if (bfld) CKC(cudaMemcpyAsync(c->bfld, bfld, n3, cudaMemcpyHostToDevice, c->stream));
+  if (!is_prim) {
+    StepArgs a = step_args(c);
+    c->L->cons2prim_all(a);
+  }
+  CKC(cudaGetLastError());
+  CKC(cudaStreamSynchronize(c->stream));
+  return BNZ_OK;
+}
+
+int bnz_init(bnz_ctx* c) {
+  if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
+  StepArgs a = step_args(c);
+  c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
+  c->L->interp_bc_active(a);
+  c->L->apply_bc(a, c->prim, c->bfld, (1u << 6) | (1u << 7) | (1u << 8));
+  c->L->prim2cons_all(a);
+  DtState ds;
+  memset(&ds, 0, sizeof ds);
+  CKC(cudaMemcpyAsync(c->d_ds, &ds, sizeof ds, cudaMemcpyHostToDevice, c->stream));
+  CKC(cudaGetLastError());
+  CKC(cudaStreamSynchronize(c->stream));
+  c->time = 0.;
+  c->step = 0;
+  return BNZ_OK;
+}
+
+int bnz_get_state(bnz_ctx* c, double* prim, double* cons, double* bfld) {
+  if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
+  size_t n9 = 9 * c->ncell * sizeof(double), n3 = 3 * c->ncell * sizeof(double);
+  if (prim) CKC(cudaMemcpyAsync(prim, c->prim, n9, cudaMemcpyDeviceToHost, c->stream));
+  if (cons) CKC(cudaMemcpyAsync(cons, c->cons, n9, cudaMemcpyDeviceToHost, c->stream));
+  if (bfld) CKC(cudaMemcpyAsync(bfld, c->bfld, n3, cudaMemcpyDeviceToHost, c->stream));
+  CKC(cudaStreamSynchronize(c->stream));
+  return BNZ_OK;
+}
+
+int bnz_apply_bc(bnz_ctx* c, uint32_t mask) {
+  if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
+  if (mask & ~0xFFFu) return fail(c, BNZ_ERR_ARG, "var_mask has bits above 11");
+  StepArgs a = step_args(c);
+  c->L->apply_bc(a, c->prim, c->bfld, mask);
+  CKC(cudaGetLastError());
+  return BNZ_OK;
+}
+
+int bnz_new_dt(bnz_ctx* c, double* dt_out) {
+  if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
+  StepArgs a = step_args(c);
+  c->L->new_dt(a, c->prim, c->d_ds, c->md.cour, 0);
+  CKC(cudaGetLastError());
+  DtState ds;
+  CKC(cudaMemcpyAsync(&ds, c->d_ds, sizeof ds, cudaMemcpyDeviceToHost, c->stream));
+  CKC(cudaStreamSynchronize(c->stream));
+  if (dt_out) *dt_out = ds.dt;
+  return BNZ_OK;
+}
+
+namespace {
+
+// RKL2 stage loop (thcond_elec.pyx:17-113); dtp points at the hyperbolic dt.
+int diffuse_impl(bnz_ctx* c, const double* dtp, double dt_hyp, int* nsts_out) {
+  if (c->md.kappa0 == 0.) {
+    if (nsts_out) *nsts_out = 0;
+    return BNZ_OK;
+  }
+  StepArgs a = step_args(c);
+  c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
+  // diffusive dt: max over active cells, read back to size the stage loop
+  unsigned long long* slot = &c->d_ds->cdsmax_bits;
+  CKC(cudaMemsetAsync(slot, 0, sizeof(unsigned long long), c->stream));
+  c->L->diff_dt_max(a, c->da, slot);
+  unsigned long long bits = 0;
+  CKC(cudaMemcpyAsync(&bits, slot, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
+  CKC(cudaStreamSynchronize(c->stream));
+  double mx;
+  memcpy(&mx, &bits, sizeof mx);
+  double dt_diff = c->md.cour_diff / mx;
+  // diffusion.pyx:217-224
+  int s = dt_diff >= dt_hyp ? 1 : (int)(0.5 * (std::sqrt(9. + 16. * dt_hyp / dt_diff) - 1.)) + 1;
+  // diffusion.pyx:227-260, columns MU NU MUT GAMT
+  std::vector<double> cf((size_t)(s + 1) * 4, 0.);
+  if (s == 1) {
+    cf[4 + 2] = 1.;
+  } else {
+    std::vector<double> b(s + 1, 0.);
+    double one3rd = 1. / 3;
+    double w1 = 4. / (s * s + s - 2);
+    b[0] = one3rd;
+    b[1] = one3rd;
+    cf[4 + 2] = w1 * b[1];
+    for (int j = 2; j <= s; ++j) {
+      b[j] = (double)(j * j + j - 2) / (2 * j * (j + 1));
+      cf[j * 4 + 0] = (double)(2 * j - 1) / j * b[j] / b[j - 1];
+      cf[j * 4 + 1] = (1. - j) / j * b[j] / b[j - 2];
+      cf[j * 4 + 2] = w1 * cf[j * 4 + 0];
+      cf[j * 4 + 3] = (b[j - 1] - 1) * cf[j * 4 + 2];
+    }
+  }
+  c->last_nsts = s;
+  if (nsts_out) *nsts_out = s;
+  for (int n = 1; n <= s; ++n) {
+    c->L->diff_operator(a, c->da);
+    c->L->diff_stage_update(a, c->da, n == 1, &cf[(size_t)n * 4], dtp);
+    if (n % c->ng == 0 && n != s) c->L->apply_bc(a, c->prim, c->bfld, 1u << 4);
+  }
+  CKC(cudaGetLastError());
+  return BNZ_OK;
+}
+
+// vanleer.pyx:101-163 with dt already in d_ds->dt
+int step_impl(bnz_ctx* c, double dt_host) {
+  StepArgs a = step_args(c);
+  const double* dtp = &c->d_ds->dt;
+  if (c->md.path == BNZ_PATH_PLAIN) {
+    c->L->plain_predictor_corrector(a, dtp);
+  } else {
+    c->L->fused_step(a, dtp);
+    // the fused kernel writes the next state into the second buffers
+    std::swap(c->prim, c->wnext);
+    std::swap(c->bfld, c->bnext);
+    a = step_args(c);
+  }
+  CKC(cudaGetLastError());
+  int rc = diffuse_impl(c, dtp, dt_host, nullptr);
+  if (rc) return rc;
+  c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
+  c->L->prim2cons_all(a);
+  CKC(cudaGetLastError());
+  return BNZ_OK;
+}
+
+}  // namespace
+
+int bnz_diffuse(bnz_ctx* c, double dt, int* nsts_out) {
+  if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
+  if (!(dt >= 0.)) return fail(c, BNZ_ERR_ARG, "dt must be >= 0");
+  c->L->set_dt(c->stream, c->d_ds, dt);
+  return diffuse_impl(c, &c->d_ds->dt, dt, nsts_out);
+}
+
+int bnz_vl2_step(bnz_ctx* c, double dt) {
+  if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
+  if (!(dt >= 0.) || std::isinf(dt)) return fail(c, BNZ_ERR_ARG, "dt must be finite and >= 0");
+  c->L->set_dt(c->stream, c->d_ds, dt);
+  return step_impl(c, dt);
+}
+
+int bnz_advance(bnz_ctx* c, double tmax, int max_steps, double* time_out, long* step_out) {
+  if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
+  int n = 0;
+  while (c->time < tmax && (max_steps <= 0 || n < max_steps)) {
+    double dt;
+    if (!c->md.fixdt) {
+      StepArgs a = step_args(c);
+      c->L->new_dt(a, c->prim, c->d_ds, c->md.cour, 0);
+      DtState ds;
+      CKC(cudaMemcpyAsync(&ds, c->d_ds, sizeof ds, cudaMemcpyDeviceToHost, c->stream));
+      CKC(cudaStreamSynchronize(c->stream));
+      dt = ds.dt;
+      if (c->time + dt > tmax) dt = tmax - c->time;
+    } else {
+      dt = c->md.dt_fixed;
+    }
+    c->L->set_dt(c->stream, c->d_ds, dt);
+    int rc = step_impl(c, dt);
+    if (rc) return rc;
+    c->time += dt;
+    c->step += 1;
+    c->last_dt = dt;
+    ++n;
+  }
+  CKC(cudaStreamSynchronize(c->stream));
+  if (time_out) *time_out = c->time;
+  if (step_out) *step_out = c->step;
+  return BNZ_OK;
+}
+
+int bnz_get_time(const bnz_ctx* c, double* t, long* s, double* last_dt) {
+  if (!c) return BNZ_ERR_ARG;
+  if (t) *t = c->time;
+  if (s) *s = c->step;
+  if (last_dt) *last_dt = c->last_dt;
+  return BNZ_OK;
+}
+
+int bnz_set_time(bnz_ctx* c, double t, long s) {
+  if (!c) return BNZ_ERR_ARG;
+  c->time = t;
+  c->step = s;
+  return BNZ_OK;
+}
+
+int bnz_check(bnz_ctx* c, uint32_t* bits) {
+  if (!c || !c->d_err) return fail(c, BNZ_ERR_ARG, "context not created");
+  unsigned h = 0;
+  CKC(cudaMemcpyAsync(&h, c->d_err, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  CKC(cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), c->stream));
+  CKC(cudaStreamSynchronize(c->stream));
+  if (bits) *bits = h;
+  if (h & 16u) return fail(c, BNZ_ERR_TIMEOUT, "a bounded device wait ran out");
+  if (h) return fail(c, BNZ_ERR_STATE, "non-physical state on the device (error bits " + std::to_string(h) + ")");
+  return BNZ_OK;
+}
+
+int bnz_sync(bnz_ctx* c) {
+  if (!c || !c->stream) return fail(c, BNZ_ERR_ARG, "context not created");
+  CKC(cudaStreamSynchronize(c->stream));
+  return BNZ_OK;
+}
+
+int bnz_advance_graph(bnz_ctx* c, double tmax, int nsteps) {
+  if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
+  return fail(c, BNZ_ERR_UNSUPPORTED, "graph stepping not built yet");
+}
+
+int bnz_device_state(bnz_ctx* c, double** prim, double** cons, double** bfld) {
+  if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
+  if (prim) *prim = c->prim;
+  if (cons) *cons = c->cons;
+  if (bfld) *bfld = c->bfld;
+  return BNZ_OK;
+}
+
+int bnz_stream(bnz_ctx* c, void** s) {
+  if (!c) return BNZ_ERR_ARG;
+  if (s) *s = (void*)c->stream;
+  return BNZ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,343 @@
+// bnz_device.cuh -- per-point device math of the VL2 step (FP64).
+//
+// EOS, fast magnetosonic speed, Riemann solvers (HLL, HLLT, HLLD; HLLC for
+// the hydro system), slope limiters and PLM reconstruction of one interface.
+// Every expression keeps the evaluation order of the reference's C kernels
+// (src/mhd/eos_c.h, src/mhd/fluxes_c.c, src/coordinates/reconstr_c.{c,h}) so
+// that a build with --fmad=false reproduces them bit for bit; the default
+// build lets the compiler contract multiply-adds into DFMA.
+//
+// This header is included inside a namespace by bnz_kernels_impl.cuh, once per
+// floating-point mode.
+#pragma once
+
+#ifndef BNZ_NM
+#define BNZ_NM 9
+#endif
+
+namespace dev {
+
+constexpr int NM = 9;
+enum { RHO = 0, MX = 1, MY = 2, MZ = 3, EN = 4, PSC = 5, BX = 6, BY = 7, BZ = 8 };
+enum { VX = 1, VY = 2, VZ = 3, PR = 4 };
+enum { RS_HLL = 0, RS_HLLC = 1, RS_HLLD = 2, RS_HLLT = 3 };
+enum { LIM_VL = 0, LIM_MC = 1, LIM_MM = 2 };
+// bits of the device error word
+enum { ERR_RHO = 1, ERR_PRES = 2, ERR_NAN = 4, ERR_FAN = 8, ERR_TIMEOUT = 16 };
+
+__device__ __forceinline__ double sqr(double x) { return x * x; }
+__device__ __forceinline__ double sgnd(double a) { return (double)((0.0 < a) - (a < 0.0)); }
+
+// eos_c.h:20-55 (MHD, no CGL / two-temperature terms)
+__device__ __forceinline__ void cons2prim(double* w, const double* u, double gam) {
+  double rhoi = 1. / u[RHO];
+  w[RHO] = u[RHO];
+  w[VX] = u[MX] * rhoi;
+  w[VY] = u[MY] * rhoi;
+  w[VZ] = u[MZ] * rhoi;
+  double v2 = sqr(w[VX]) + sqr(w[VY]) + sqr(w[VZ]);
+  double b2 = sqr(u[BX]) + sqr(u[BY]) + sqr(u[BZ]);
+  w[PR] = (gam - 1.) * (u[EN] - 0.5 * (b2 + v2 * u[RHO]));
+  w[PSC] = u[PSC];
+  w[BX] = u[BX];
+  w[BY] = u[BY];
+  w[BZ] = u[BZ];
+}
+
+// eos_c.h:60-95
+__device__ __forceinline__ void prim2cons(double* u, const double* w, double gam) {
+  double gamm1i = 1. / (gam - 1.);
+  u[RHO] = w[RHO];
+  u[MX] = w[RHO] * w[VX];
+  u[MY] = w[RHO] * w[VY];
+  u[MZ] = w[RHO] * w[VZ];
+  double v2 = sqr(w[VX]) + sqr(w[VY]) + sqr(w[VZ]);
+  double b2 = sqr(w[BX]) + sqr(w[BY]) + sqr(w[BZ]);
+  u[EN] = 0.5 * (w[RHO] * v2 + b2) + w[PR] * gamm1i;
+  u[PSC] = w[PSC];
+  u[BX] = w[BX];
+  u[BY] = w[BY];
+  u[BZ] = w[BZ];
+}
+
+// eos_c.h:416-461 with a = 1 (no pressure anisotropy)
+__device__ __forceinline__ void primcons2flux(double* f, const double* w, const double* u) {
+  double bx2 = sqr(w[BX]);
+  double b2 = bx2 + sqr(w[BY]) + sqr(w[BZ]);
+  double bxby = w[BX] * w[BY];
+  double bxbz = w[BX] * w[BZ];
+  double ptot = 0.5 * b2 + w[PR];
+#pragma unroll
+  for (int n = 0; n < BX; ++n) f[n] = u[n] * w[VX];
+  f[MX] += ptot;
+  f[EN] += ptot * w[VX];
+  f[MX] -= bx2;
+  f[MY] -= bxby;
+  f[MZ] -= bxbz;
+  f[EN] -= (w[VX] * bx2 + w[VY] * bxby + w[VZ] * bxbz);
+  f[BX] = 0.;
+  f[BY] = w[VX] * w[BY] - w[VY] * w[BX];
+  f[BZ] = w[VX] * w[BZ] - w[VZ] * w[BX];
+}
+
+// eos_c.h:468-530 -- the normal field is read from w[BX] (the reference's
+// bx argument is unused, so the CFL estimate uses the x fast speed on every axis).
+__device__ __forceinline__ double fms(const double* w, double gam) {
+  double bx2 = sqr(w[BX]);
+  double b2 = bx2 + sqr(w[BY]) + sqr(w[BZ]);
+  double gamp = gam * w[PR];
+  double c1 = gamp + b2;
+  double c2 = sqrt(fabs(c1 * c1 - 4. * gamp * bx2));
+  return sqrt(0.5 / w[RHO] * (c1 + c2));
+}
+
+// fluxes_c.c:25-42
+__device__ __forceinline__ void wave_speeds(const double* wL, const double* wR, double gam,
+                                            double& sL, double& sR) {
+  double cfL = fms(wL, gam);
+  double cfR = fms(wR, gam);
+  double cf_max = fmax(cfL, cfR);
+  sL = fmin(wL[VX], wR[VX]) - cf_max;
+  sR = fmax(wL[VX], wR[VX]) + cf_max;
+}
+
+// fluxes_c.c:175-223
+__device__ __forceinline__ void flux_hll(double* flux, const double* wL, const double* wR, double gam) {
+  double uL[NM], uR[NM], fL[NM], fR[NM];
+  prim2cons(uL, wL, gam);
+  prim2cons(uR, wR, gam);
+  primcons2flux(fL, wL, uL);
+  primcons2flux(fR, wR, uR);
+  double sL, sR;
+  wave_speeds(wL, wR, gam, sL, sR);
+  double aL = fmin(sL, 0.);
+  double aR = fmax(sR, 0.);
+  double aLaR = aL * aR;
+  double aRmaLi = 1. / (aR - aL);
+#pragma unroll
+  for (int n = 0; n < NM; ++n) flux[n] = (aR * fL[n] - aL * fR[n] + aLaR * (uR[n] - uL[n])) * aRmaLi;
+  flux[BX] = 0.;
+}
+
+// fluxes_c.c:447-607 (Mignone 2012 isothermal-type three-wave solver).  The
+// reference leaves the energy entries of its star states uninitialised; they
+// are zero here.
+__device__ __forceinline__ void flux_hllt(double* flux, const double* wL, const double* wR, double gam,
+                                          unsigned& err) {
+  double uL[NM], uR[NM], fL[NM], fR[NM];
+  prim2cons(uL, wL, gam);
+  prim2cons(uR, wR, gam);
+  primcons2flux(fL, wL, uL);
+  primcons2flux(fR, wR, uR);
+  double sL, sR;
+  wave_speeds(wL, wR, gam, sL, sR);
+  double bx = wL[BX];
+  double sRsLi = 1. / (sR - sL);
+  double rhos = (sR * uR[RHO] - sL * uL[RHO] - (fR[RHO] - fL[RHO])) * sRsLi;
+  double mxs = (sR * uR[MX] - sL * uL[MX] - (fR[MX] - fL[MX])) * sRsLi;
+  double frhos = (sR * fL[RHO] - sL * fR[RHO] + sR * sL * (uR[RHO] - uL[RHO])) * sRsLi;
+  double us = frhos / rhos;
+  double pscs = (sR * uR[PSC] - sL * uL[PSC] - (fR[PSC] - fL[PSC])) * sRsLi;
+  double uLs[NM], uRs[NM], uCs[NM];
+#pragma unroll
+  for (int n = 0; n < NM; ++n) { uLs[n] = 0.; uRs[n] = 0.; uCs[n] = 0.; }
+  uLs[RHO] = rhos; uRs[RHO] = rhos;
+  uLs[MX] = mxs;   uRs[MX] = mxs;
+  uLs[PSC] = pscs; uRs[PSC] = pscs;
+  uLs[MY] = rhos * wL[VY];
+  uRs[MY] = rhos * wR[VY];
+  uLs[MZ] = rhos * wL[VZ];
+  uRs[MZ] = rhos * wR[VZ];
+  double sLs = us, sRs = us;
+  double rhosi = 1. / rhos;
+  double sqrt_rhosi = sqrt(rhosi);
+  sLs -= fabs(bx) * sqrt_rhosi;
+  sRs += fabs(bx) * sqrt_rhosi;
+  double xL = 1. / ((sL - sLs) * (sL - sRs));
+  double xR = 1. / ((sR - sLs) * (sR - sRs));
+  double yL = bx * xL * (us - wL[VX]);
+  double yR = bx * xR * (us - wR[VX]);
+  uLs[MY] -= yL * wL[BY];
+  uRs[MY] -= yR * wR[BY];
+  uLs[MZ] -= yL * wL[BZ];
+  uRs[MZ] -= yR * wR[BZ];
+  yL = (wL[RHO] * sqr(sL - wL[VX]) - sqr(bx)) * rhosi * xL;
+  yR = (wR[RHO] * sqr(sR - wR[VX]) - sqr(bx)) * rhosi * xR;
+  uLs[BY] = yL * wL[BY];
+  uRs[BY] = yR * wR[BY];
+  uLs[BZ] = yL * wL[BZ];
+  uRs[BZ] = yR * wR[BZ];
+  uCs[RHO] = rhos;
+  uCs[MX] = mxs;
+  uCs[PSC] = pscs;
+  double sgnb = sgnd(bx);
+  double x = 0.5 * sgnb / sqrt_rhosi;
+  uCs[MY] = 0.5 * (uLs[MY] + uRs[MY]) + x * (uRs[BY] - uLs[BY]);
+  uCs[MZ] = 0.5 * (uLs[MZ] + uRs[MZ]) + x * (uRs[BZ] - uLs[BZ]);
+  uCs[BY] = 0.5 * (uLs[BY] + uRs[BY]) + x * rhosi * (uRs[MY] - uLs[MY]);
+  uCs[BZ] = 0.5 * (uLs[BZ] + uRs[BZ]) + x * rhosi * (uRs[MZ] - uLs[MZ]);
+  // sequential region tests of the reference; the last match wins
+  int r = 0;
+  if (sL > 0.) r = 1;
+  if (sL <= 0. && 0. < sLs) r = 2;
+  if (sLs <= 0. && 0. < sRs) r = 3;
+  if (sRs <= 0. && 0. < sR) r = 4;
+  if (sR <= 0.) r = 5;
+  if (r == 0) err |= ERR_FAN;
+#pragma unroll
+  for (int n = 0; n < NM; ++n) {
+    double v;
+    if (r == 1) v = fL[n];
+    else if (r == 2) v = fL[n] + sL * (uLs[n] - uL[n]);
+    else if (r == 3) v = fL[n] + sL * (uLs[n] - uL[n]) + sLs * (uCs[n] - uLs[n]);
+    else if (r == 4) v = fR[n] + sR * (uRs[n] - uR[n]);
+    else if (r == 5) v = fR[n];
+    else v = 0.;
+    flux[n] = v;
+  }
+  flux[BX] = 0.;
+}
+
+// fluxes_c.c:616-834 (Miyoshi & Kusano 2005 HLLD)
+__device__ __forceinline__ void flux_hlld(double* flux, const double* wL, const double* wR, double gam,
+                                          unsigned& err) {
+  double uL[NM], uR[NM], fL[NM], fR[NM];
+  prim2cons(uL, wL, gam);
+  prim2cons(uR, wR, gam);
+  primcons2flux(fL, wL, uL);
+  primcons2flux(fR, wR, uR);
+  double sL, sR;
+  wave_speeds(wL, wR, gam, sL, sR);
+  const double bx = wL[BX];
+
+  double b2hL = 0.5 * (sqr(bx) + sqr(wL[BY]) + sqr(wL[BZ]));
+  double b2hR = 0.5 * (sqr(bx) + sqr(wR[BY]) + sqr(wR[BZ]));
+  double ptL = wL[PR] + b2hL;
+  double ptR = wR[PR] + b2hR;
+
+  double deni = 1. / (sR * uR[RHO] - sL * uL[RHO] - (fR[RHO] - fL[RHO]));
+  double sM = (sR * uR[MX] - sL * uL[MX] - (fR[MX] - fL[MX])) * deni;
+
+  double sLvxL = sL - wL[VX];
+  double sRvxR = sR - wR[VX];
+  double sLsMi = 1. / (sL - sM);
+  double sRsMi = 1. / (sR - sM);
+  double xL = sLvxL * sLsMi;
+  double xR = sRvxR * sRsMi;
+
+  // single-star states (index order RHO MX MY MZ EN PSC . BY BZ)
+  double rLs = uL[RHO] * xL, rRs = uR[RHO] * xR;
+  double psL = uL[PSC] * xL, psR = uR[PSC] * xR;
+  double pts = wL[RHO] * sLvxL * (sM - wL[VX]) + ptL;
+
+  double rhosLvxL = wL[RHO] * sLvxL;
+  double rhosRvxR = wR[RHO] * sRvxR;
+  double bx2 = sqr(bx);
+  double wvbL = 1. / (rhosLvxL * (sL - sM) - bx2);
+  double wvbR = 1. / (rhosRvxR * (sR - sM) - bx2);
+  double bxsMvxL = bx * (sM - wL[VX]);
+  double bxsMvxR = bx * (sM - wR[VX]);
+  double wvL = bxsMvxL * wvbL;
+  double wvR = bxsMvxR * wvbR;
+  double vyLs = wL[VY] - wL[BY] * wvL;
+  double vyRs = wR[VY] - wR[BY] * wvR;
+  double vzLs = wL[VZ] - wL[BZ] * wvL;
+  double vzRs = wR[VZ] - wR[BZ] * wvR;
+
+  double mxLs = rLs * sM, mxRs = rRs * sM;
+  double myLs = rLs * vyLs, myRs = rRs * vyRs;
+  double mzLs = rLs * vzLs, mzRs = rRs * vzRs;
+
+  double rhosLvxL2_bx2 = rhosLvxL * sLvxL - bx2;
+  double rhosRvxR2_bx2 = rhosRvxR * sRvxR - bx2;
+  double wbL = rhosLvxL2_bx2 * wvbL;
+  double wbR = rhosRvxR2_bx2 * wvbR;
+  double byLs = wL[BY] * wbL, byRs = wR[BY] * wbR;
+  double bzLs = wL[BZ] * wbL, bzRs = wR[BZ] * wbR;
+
+  double vsbsL = sM * bx + vyLs * byLs + vzLs * bzLs;
+  double vsbsR = sM * bx + vyRs * byRs + vzRs * bzRs;
+  double eLs = (sLvxL * uL[EN] - ptL * wL[VX] + pts * sM +
+                bx * (wL[VX] * bx + wL[VY] * wL[BY] + wL[VZ] * wL[BZ] - vsbsL)) * sLsMi;
+  double eRs = (sRvxR * uR[EN] - ptR * wR[VX] + pts * sM +
+                bx * (wR[VX] * bx + wR[VY] * wR[BY] + wR[VZ] * wR[BZ] - vsbsR)) * sRsMi;
+
+  // double-star states
+  double sqrt_rhoLs = sqrt(rLs);
+  double sqrt_rhoRs = sqrt(rRs);
+  double sLs = sM - fabs(bx) / sqrt_rhoLs;
+  double sRs = sM + fabs(bx) / sqrt_rhoRs;
+  double rhoLRi = 1. / (sqrt_rhoLs + sqrt_rhoRs);
+  double sgnb = sgnd(bx);
+
+  double vyss = (sqrt_rhoLs * vyLs + sqrt_rhoRs * vyRs + (byRs - byLs) * sgnb) * rhoLRi;
+  double vzss = (sqrt_rhoLs * vzLs + sqrt_rhoRs * vzRs + (bzRs - bzLs) * sgnb) * rhoLRi;
+  double myLss = rLs * vyss, myRss = rRs * vyss;
+  double mzLss = rLs * vzss, mzRss = rRs * vzss;
+  double byss = (sqrt_rhoLs * byRs + sqrt_rhoRs * byLs + sqrt_rhoLs * sqrt_rhoRs * (vyRs - vyLs) * sgnb) * rhoLRi;
+  double bzss = (sqrt_rhoLs * bzRs + sqrt_rhoRs * bzLs + sqrt_rhoLs * sqrt_rhoRs * (vzRs - vzLs) * sgnb) * rhoLRi;
+  double vssbss = sM * bx + vyss * byss + vzss * bzss;
+  double eLss = eLs - sqrt_rhoLs * (vsbsL - vssbss) * sgnb;
+  double eRss = eRs + sqrt_rhoRs * (vsbsR - vssbss) * sgnb;
+
+  int r = 0;
+  if (sL > 0.) r = 1;
+  if (sL <= 0. && 0. < sLs) r = 2;
+  if (sLs <= 0. && 0. < sM) r = 3;
+  if (sM <= 0. && 0. < sRs) r = 4;
+  if (sRs <= 0. && 0. < sR) r = 5;
+  if (sR <= 0.) r = 6;
+  if (r == 0) err |= ERR_FAN;
+
+  // left / right single- and double-star vectors in variable order
+  const double uLs[NM] = {rLs, mxLs, myLs, mzLs, eLs, psL, 0., byLs, bzLs};
+  const double uRs[NM] = {rRs, mxRs, myRs, mzRs, eRs, psR, 0., byRs, bzRs};
+  const double uLss[NM] = {rLs, mxLs, myLss, mzLss, eLss, psL, 0., byss, bzss};
+  const double uRss[NM] = {rRs, mxRs, myRss, mzRss, eRss, psR, 0., byss, bzss};
+#pragma unroll
+  for (int n = 0; n < NM; ++n) {
+    double v;
+    if (r == 1) v = fL[n];
+    else if (r == 2) v = fL[n] + sL * (uLs[n] - uL[n]);
+    else if (r == 3) v = fL[n] + sL * (uLs[n] - uL[n]) + sLs * (uLss[n] - uLs[n]);
+    else if (r == 4) v = fR[n] + sR * (uRs[n] - uR[n]) + sRs * (uRss[n] - uRs[n]);
+    else if (r == 5) v = fR[n] + sR * (uRs[n] - uR[n]);
+    else if (r == 6) v = fR[n];
+    else v = 0.;
+    flux[n] = v;
+  }
+  flux[BX] = 0.;
+}
+
+template <int RS>
+__device__ __forceinline__ void riemann(double* flux, const double* wL, const double* wR, double gam,
+                                        unsigned& err) {
+  if constexpr (RS == RS_HLLD) flux_hlld(flux, wL, wR, gam, err);
+  else if constexpr (RS == RS_HLLT) flux_hllt(flux, wL, wR, gam, err);
+  else flux_hll(flux, wL, wR, gam);
+}
+
+// reconstr_c.h:28-44
+__device__ __forceinline__ double mm_lim(double a, double b) {
+  return (a * b <= 0.) ? 0. : ((a > 0.) ? ((a < b) ? a : b) : ((a > b) ? a : b));
+}
+__device__ __forceinline__ double mc_lim(double a, double b) { return mm_lim(2. * mm_lim(a, b), 0.5 * (a + b)); }
+__device__ __forceinline__ double vl_lim(double a, double b) {
+  double ab = a * b;
+  return (ab > 0.) ? (2. * ab / (a + b)) : 0.;
+}
+template <int LIM>
+__device__ __forceinline__ double limit(double a, double b) {
+  if constexpr (LIM == LIM_MC) return mc_lim(a, b);
+  else if constexpr (LIM == LIM_MM) return mm_lim(a, b);
+  else return vl_lim(a, b);
+}
+
+// reconstr_c.c:54-91 for one cell: half slope d = 0.5 lim(dm, dp); the face
+// states are wc - d (left face of the cell) and wc + d (right face).
+template <int LIM>
+__device__ __forceinline__ double half_slope(double wm, double wc, double wp) {
+  return 0.5 * limit<LIM>(wc - wm, wp - wc);
+}
+
+}  // namespace dev

@@ -1,0 +1,215 @@
+// bnz_diffusion.cuh -- RKL2 super-time-stepped electron thermal conduction.
+//
+// Follows src/dissipation/thcond_elec.pyx:17-466 and util_diffusion.pyx:16-159:
+// temperature T = p/rho, harmonic-mean face conductivity, field-aligned face
+// flux q = -kappa b (b . grad T) with limited transverse gradients (or the
+// isotropic flux), optional saturation, dp/dt = -(gamma-1) div q, and the
+// Meyer et al. (2014) RKL2 stage recursion (diffusion.pyx:217-260).
+// Included inside the per-floating-point-mode namespace.
+#pragma once
+
+namespace diff {
+
+using namespace dev;
+constexpr double SMALL_NUM = 1.0e-20;
+
+__device__ __forceinline__ long long c3(const GridDev& g, int i, int j, int k) {
+  return ((long long)k * g.ny + j) * g.nx + i;
+}
+
+// util_diffusion.pyx:16-20 (returns a magnitude, as the reference does)
+__device__ __forceinline__ double dlim(double a, double b) {
+  double _a = fabs(a), _b = fabs(b);
+  return fmax(0., fmin(fmin(0.5 * (_a + _b), _a), _b));
+}
+
+// thcond_elec.pyx:146-152 -- T = p / rho on every cell
+__global__ void k_temp(GridDev g, const double* __restrict__ w, double* __restrict__ T) {
+  const long long n = g.sv;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+    T[c] = w[PR * g.sv + c] / w[RHO * g.sv + c];
+}
+
+__device__ __forceinline__ double saturate(double f, double h, double Tl, double Tr, double rl, double rr) {
+  double Tc = 0.5 * (Tl + Tr);
+  double rhoc = 0.5 * (rl + rr);
+  double mom = 0.5 * h * rhoc * sqrt(0.67 * Tc);
+  double qsat = f > 0. ? Tl * mom : Tr * mom;
+  return f * qsat / (fabs(f) + qsat + SMALL_NUM);
+}
+
+// thcond_elec.pyx:154-303: face flux along AX on faces [lo, hi] of that axis,
+// cells 1..Ntot-2 on the other active axes.
+template <int AX>
+__global__ void k_flux(GridDev g, const double* __restrict__ w, const double* __restrict__ bf,
+                       const double* __restrict__ T, double* __restrict__ F, DiffArgs da, int3 lo, int3 hi) {
+  const int nxr = hi.x - lo.x + 1, nyr = hi.y - lo.y + 1, nzr = hi.z - lo.z + 1;
+  const long long n = (long long)nxr * nyr * nzr;
+  const long long sy = g.nx, sz = (long long)g.nx * g.ny, sv = g.sv;
+  const double k0 = da.kappa0;
+  const double kappah = (2. * k0 * k0 / (k0 + k0 + SMALL_NUM));
+  const double* dvi0 = g.dlv_inv[0];
+  const double* dvi1 = g.dlv_inv[1];
+  const double* dvi2 = g.dlv_inv[2];
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    int i = lo.x + (int)(t % nxr);
+    long long r = t / nxr;
+    int j = lo.y + (int)(r % nyr), k = lo.z + (int)(r / nyr);
+    const long long c = c3(g, i, j, k);
+    const long long s = AX == 0 ? 1 : AX == 1 ? sy : sz;
+    double dTdx = 0., dTdy = 0., dTdz = 0., h = 0., f;
+    // neighbours: cell c (right of the face) and c - s (left)
+    if (AX == 0) dTdx = dvi0[i] * (T[c] - T[c - 1]);
+    if (AX == 1) dTdy = dvi1[j] * (T[c] - T[c - sy]);
+    if (AX == 2) dTdz = dvi2[k] * (T[c] - T[c - sz]);
+    if (da.aniso) {
+      double bxh, byh, bzh;
+      if (AX == 0) {
+        bxh = bf[c];
+        byh = 0.5 * (w[BY * sv + c - 1] + w[BY * sv + c]);
+        bzh = 0.5 * (w[BZ * sv + c - 1] + w[BZ * sv + c]);
+      } else if (AX == 1) {
+        byh = bf[sv + c];
+        bxh = 0.5 * (w[BX * sv + c - sy] + w[BX * sv + c]);
+        bzh = 0.5 * (w[BZ * sv + c - sy] + w[BZ * sv + c]);
+      } else {
+        bzh = bf[2 * sv + c];
+        bxh = 0.5 * (w[BX * sv + c - sz] + w[BX * sv + c]);
+        byh = 0.5 * (w[BY * sv + c - sz] + w[BY * sv + c]);
+      }
+      double bhi = 1. / sqrt(bxh * bxh + byh * byh + bzh * bzh + SMALL_NUM);
+      double bxh1 = bxh * bhi, byh1 = byh * bhi, bzh1 = bzh * bhi;
+      if (AX == 0) {
+        h = fabs(bxh1);
+        if (g.dims >= 2)  // tr_grad_lim_yx (syxv = 1 on Cartesian grids)
+          dTdy = dlim(dlim((T[c - 1] - T[c - 1 - sy]) * dvi1[j], (T[c - 1 + sy] - T[c - 1]) * dvi1[j + 1]) * 1.,
+                      dlim((T[c] - T[c - sy]) * dvi1[j], (T[c + sy] - T[c]) * dvi1[j + 1]) * 1.);
+        if (g.dims >= 3)  // tr_grad_lim_zx
+          dTdz = dlim(dlim((T[c - 1] - T[c - 1 - sz]) * dvi2[k], (T[c - 1 + sz] - T[c - 1]) * dvi2[k + 1]) * 1. * 1.,
+                      dlim((T[c] - T[c - sz]) * dvi2[k], (T[c + sz] - T[c]) * dvi2[k + 1]) * 1. * 1.);
+        f = -kappah * bxh1 * (bxh1 * dTdx + byh1 * dTdy + bzh1 * dTdz);
+      } else if (AX == 1) {
+        h = fabs(byh1);
+        // tr_grad_lim_xy
+        dTdx = dlim(dlim((T[c - sy] - T[c - sy - 1]) * dvi0[i], (T[c - sy + 1] - T[c - sy]) * dvi0[i + 1]),
+                    dlim((T[c] - T[c - 1]) * dvi0[i], (T[c + 1] - T[c]) * dvi0[i + 1]));
+        if (g.dims >= 3)  // tr_grad_lim_zy
+          dTdz = dlim(dlim((T[c - sy] - T[c - sy - sz]) * dvi2[k], (T[c - sy + sz] - T[c - sy]) * dvi2[k + 1]) * 1. * 1.,
+                      dlim((T[c] - T[c - sz]) * dvi2[k], (T[c + sz] - T[c]) * dvi2[k + 1]) * 1. * 1.);
+        f = -kappah * byh1 * (bxh1 * dTdx + byh1 * dTdy + bzh1 * dTdz);
+      } else {
+        h = fabs(bzh1);
+        // tr_grad_lim_xz, tr_grad_lim_yz
+        dTdx = dlim(dlim((T[c - sz] - T[c - sz - 1]) * dvi0[i], (T[c - sz + 1] - T[c - sz]) * dvi0[i + 1]),
+                    dlim((T[c] - T[c - 1]) * dvi0[i], (T[c + 1] - T[c]) * dvi0[i + 1]));
+        dTdy = dlim(dlim((T[c - sz] - T[c - sz - sy]) * dvi1[j], (T[c - sz + sy] - T[c - sz]) * dvi1[j + 1]) * 1.,
+                    dlim((T[c] - T[c - sy]) * dvi1[j], (T[c + sy] - T[c]) * dvi1[j + 1]) * 1.);
+        f = -kappah * bzh1 * (bxh1 * dTdx + byh1 * dTdy + bzh1 * dTdz);
+      }
+    } else {
+      if (AX == 0) {
+        if (g.dims >= 2)  // tr_grad_yx
+          dTdy = 0.25 * (((T[c - 1] - T[c - 1 - sy]) * dvi1[j] + (T[c - 1 + sy] - T[c - 1]) * dvi1[j + 1]) * 1. +
+                         ((T[c] - T[c - sy]) * dvi1[j] + (T[c + sy] - T[c]) * dvi1[j + 1]) * 1.);
+        if (g.dims >= 3)  // tr_grad_zx
+          dTdz = 0.25 * (((T[c - sy] - T[c - sy - sz]) * dvi2[k] + (T[c - sy + sz] - T[c - sy]) * dvi2[k + 1]) * 1. * 1. +
+                         ((T[c] - T[c - sz]) * dvi2[k] + (T[c + sz] - T[c]) * dvi2[k + 1]) * 1. * 1.);
+        double dTds = sqrt(dTdx * dTdx + dTdy * dTdy + dTdz * dTdz + SMALL_NUM);
+        h = fabs(dTdx / dTds);
+        f = -kappah * dTdx;
+      } else if (AX == 1) {
+        dTdx = 0.25 * (((T[c - sy] - T[c - sy - 1]) * dvi0[i] + (T[c - sy + 1] - T[c - sy]) * dvi0[i + 1]) +
+                       ((T[c] - T[c - 1]) * dvi0[i] + (T[c + 1] - T[c]) * dvi0[i + 1]));
+        if (g.dims >= 3)  // tr_grad_zy
+          dTdz = 0.25 * (((T[c - sy] - T[c - sy - sz]) * dvi2[k] + (T[c - sy + sz] - T[c - sy]) * dvi2[k + 1]) * 1. * 1. +
+                         ((T[c] - T[c - sz]) * dvi2[k] + (T[c + sz] - T[c]) * dvi2[k + 1]) * 1. * 1.);
+        double dTds = sqrt(dTdx * dTdx + dTdy * dTdy + dTdz * dTdz + SMALL_NUM);
+        h = fabs(dTdy / dTds);
+        f = -kappah * dTdy;
+      } else {
+        dTdx = 0.25 * (((T[c - sz] - T[c - sz - 1]) * dvi0[i] + (T[c - sz + 1] - T[c - sz]) * dvi0[i + 1]) +
+                       ((T[c] - T[c - 1]) * dvi0[i] + (T[c + 1] - T[c]) * dvi0[i + 1]));
+        dTdy = 0.25 * (((T[c - sz] - T[c - sz - sy]) * dvi1[j] + (T[c - sz + sy] - T[c - sz]) * dvi1[j + 1]) * 1. +
+                       ((T[c] - T[c - sy]) * dvi1[j] + (T[c + sy] - T[c]) * dvi1[j + 1]) * 1.);
+        double dTds = sqrt(dTdx * dTdx + dTdy * dTdy + dTdz * dTdz + SMALL_NUM);
+        h = fabs(dTdz / dTds);
+        f = -kappah * dTdz;
+      }
+    }
+    if (da.sat) f = saturate(f, h, T[c - s], T[c], w[RHO * sv + c - s], w[RHO * sv + c]);
+    F[c] = f;
+  }
+}
+
+// thcond_elec.pyx:332-338
+__global__ void k_dtemp(GridDev g, const double* __restrict__ fx, const double* __restrict__ fy,
+                        const double* __restrict__ fz, double* __restrict__ dT, int3 lo, int3 hi) {
+  const int nxr = hi.x - lo.x + 1, nyr = hi.y - lo.y + 1, nzr = hi.z - lo.z + 1;
+  const long long n = (long long)nxr * nyr * nzr;
+  const long long sy = g.nx, sz = (long long)g.nx * g.ny;
+  const double gamm1 = g.gam - 1.;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    int i = lo.x + (int)(t % nxr);
+    long long r = t / nxr;
+    int j = lo.y + (int)(r % nyr), k = lo.z + (int)(r / nyr);
+    const long long c = c3(g, i, j, k);
+    double v = -(fx[c + 1] - fx[c]) * gamm1 * g.dlf_inv[0][i];
+    if (g.dims >= 2) v -= (fy[c + sy] - fy[c]) * gamm1 * g.dlf_inv[1][j];
+    if (g.dims >= 3) v -= (fz[c + sz] - fz[c]) * gamm1 * g.dlf_inv[2][k];
+    dT[c] = v;
+  }
+}
+
+// thcond_elec.pyx:75-94: (stage 1) save p0 and M(p0); RKL2 update of p.
+__global__ void k_sts_update(GridDev g, double* __restrict__ w, DiffArgs da, int3 lo, int3 hi, int first,
+                             double mu, double nu, double mut, double gamt, const double* dtp) {
+  const double dt = *dtp;
+  const int nxr = hi.x - lo.x + 1, nyr = hi.y - lo.y + 1, nzr = hi.z - lo.z + 1;
+  const long long n = (long long)nxr * nyr * nzr;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    int i = lo.x + (int)(t % nxr);
+    long long r = t / nxr;
+    int j = lo.y + (int)(r % nyr), k = lo.z + (int)(r / nyr);
+    const long long c = c3(g, i, j, k);
+    double* pp = w + PR * g.sv + c;
+    if (first) {
+      da.pres0[c] = *pp;
+      da.dtemp0[c] = da.dtemp[c];
+    }
+    double a = *pp;
+    *pp = (mu * a + nu * da.presm1[c] + (1. - mu - nu) * da.pres0[c] + dt * (mut * da.dtemp[c] + gamt * da.dtemp0[c]));
+    da.presm1[c] = a;
+  }
+}
+
+// thcond_elec.pyx:355-466: max over active cells of kappa0 (gamma-1)/rho sum 1/dx^2
+__global__ void k_diff_dt_max(GridDev g, const double* __restrict__ w, double kappa0, unsigned long long* slot) {
+  double m = 0.;
+  const double gamm1 = g.gam - 1.;
+  const int nxa = g.i2 - g.i1 + 1, nya = g.j2 - g.j1 + 1, nza = g.k2 - g.k1 + 1;
+  const long long n = (long long)nxa * nya * nza;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    int i = g.i1 + (int)(t % nxa);
+    long long r = t / nxa;
+    int j = g.j1 + (int)(r % nya), k = g.k1 + (int)(r / nya);
+    long long c = c3(g, i, j, k);
+    double dsx = g.dlf[0][i], dsy = g.dlf[1][j], dsz = g.dlf[2][k];
+    double ad = kappa0 / w[RHO * g.sv + c] * gamm1;
+    double ad_dl2 = ad / sqr(dsx);
+    if (g.dims >= 2) ad_dl2 = ad_dl2 + ad / sqr(dsy);
+    if (g.dims >= 3) ad_dl2 = ad_dl2 + ad / sqr(dsz);
+    if (ad_dl2 > m) m = ad_dl2;
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double red[32];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) red[wid] = m;
+  __syncthreads();
+  if (wid == 0) {
+    m = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0 && m > 0.) atomicMax(slot, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+}  // namespace diff

@@ -1,0 +1,5 @@
+// Exact build: compiled with --fmad=false, so every multiply and add rounds
+// separately as in the CPU reference (bit-for-bit parity mode).
+#define BNZ_NS exact
+#include "bnz_kernels_impl.cuh"
+BNZ_DEFINE_TABLE(exact)

@@ -1,0 +1,255 @@
+// bnz_kernels_impl.cuh -- kernels and their host launchers, compiled once per
+// floating-point mode: bnz_kernels_exact.cu (no multiply-add contraction, the
+// bit-for-bit parity build) and bnz_kernels_fast.cu (DFMA contraction).
+// The including file defines BNZ_NS (the namespace name).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "bnz_common.h"
+#include "bnz_launch.h"
+
+namespace BNZ_NS {
+
+#include "bnz_device.cuh"
+#include "bnz_plain.cuh"
+#include "bnz_bc_dt.cuh"
+#include "bnz_diffusion.cuh"
+#include "bnz_fused.cuh"
+
+namespace {
+
+inline int nblocks(long long n, int threads, int cap = 148 * 32) {
+  long long b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return (int)b;
+}
+
+inline plain::Box mkbox(int x0, int x1, int y0, int y1, int z0, int z1) {
+  plain::Box b;
+  b.lo = make_int3(x0, y0, z0);
+  b.hi = make_int3(x1, y1, z1);
+  return b;
+}
+
+inline long long boxn(const plain::Box& b) {
+  return (long long)(b.hi.x - b.lo.x + 1) * (b.hi.y - b.lo.y + 1) * (b.hi.z - b.lo.z + 1);
+}
+
+// integrator.pyx:375-383
+inline void integr_lims(const GridDev& g, int order, int* l) {
+  const int N[3] = {g.nx, g.ny, g.nz};
+  for (int a = 0; a < 3; ++a) {
+    l[2 * a] = order + 1;
+    l[2 * a + 1] = N[a] - 2 - order;
+  }
+  if (g.dims < 2) l[2] = l[3] = 0;
+  if (g.dims < 3) l[4] = l[5] = 0;
+}
+
+template <int AX, int ORDER>
+void launch_flux_rs(const StepArgs& a, const double* w, const double* bf, const plain::Box& b) {
+  const int T = 128;
+  int nb = nblocks(boxn(b), T);
+  switch (a.rsolver) {
+    case dev::RS_HLLD:
+      plain::k_flux<AX, ORDER, dev::RS_HLLD><<<nb, T, 0, a.stream>>>(a.g, w, bf, a.flx[AX], b, a.limiter, a.err);
+      break;
+    case dev::RS_HLLT:
+      plain::k_flux<AX, ORDER, dev::RS_HLLT><<<nb, T, 0, a.stream>>>(a.g, w, bf, a.flx[AX], b, a.limiter, a.err);
+      break;
+    default:
+      plain::k_flux<AX, ORDER, dev::RS_HLL><<<nb, T, 0, a.stream>>>(a.g, w, bf, a.flx[AX], b, a.limiter, a.err);
+      break;
+  }
+}
+
+template <int AX>
+void launch_flux(const StepArgs& a, int order, const double* w, const double* bf, const plain::Box& b) {
+  if (order == 0) launch_flux_rs<AX, 0>(a, w, bf, b);
+  else launch_flux_rs<AX, 1>(a, w, bf, b);
+}
+
+// godunov.pyx:20-209 + 215-252 (integrate_hydro, integrator.pyx:51-79)
+void integrate_hydro(const StepArgs& a, double* u1, const double* u0, const double* w0, const double* b0, int order,
+                     const double* dtp, double fac) {
+  const GridDev& g = a.g;
+  int l[6];
+  integr_lims(g, order, l);
+  int il = l[0], iu = l[1], jl = l[2], ju = l[3], kl = l[4], ku = l[5];
+  {  // x faces il..iu+1 on rows jl-1..ju+1, kl-1..ku+1
+    int jb = jl - 1, je = ju + 1, kb = kl - 1, ke = ku + 1;
+    if (g.dims < 2) jb = je = 0;
+    if (g.dims < 3) kb = ke = 0;
+    launch_flux<0>(a, order, w0, b0, mkbox(il, iu + 1, jb, je, kb, ke));
+  }
+  if (g.dims >= 2) {
+    int kb = kl - 1, ke = ku + 1;
+    if (g.dims < 3) kb = ke = 0;
+    launch_flux<1>(a, order, w0, b0, mkbox(il - 1, iu + 1, jl, ju + 1, kb, ke));
+  }
+  if (g.dims >= 3) launch_flux<2>(a, order, w0, b0, mkbox(il - 1, iu + 1, jl - 1, ju + 1, kl, ku + 1));
+  plain::Box b = mkbox(il, iu, jl, ju, kl, ku);
+  plain::k_advance_hydro<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, u1, u0, a.flx[0], a.flx[1], a.flx[2], b,
+                                                                        dtp, fac);
+}
+
+// integrator.pyx:85-126
+void integrate_field(const StepArgs& a, double* u1, double* b1, const double* w0, const double* b0, int order,
+                     const double* dtp, double fac) {
+  const GridDev& g = a.g;
+  int l[6];
+  integr_lims(g, order, l);
+  {
+    int il = l[0] - 1, iu = l[1] + 1, jl = l[2] - 1, ju = l[3] + 1, kl = l[4] - 1, ku = l[5] + 1;
+    if (g.dims < 2) jl = ju = 0;
+    if (g.dims < 3) kl = ku = 0;
+    plain::Box b = mkbox(il, iu, jl, ju, kl, ku);
+    plain::k_ec<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, w0, a.ec, b);
+  }
+  {
+    int il = l[0], iu = l[1] + 1, jl = l[2], ju = l[3] + 1, kl = l[4], ku = l[5] + 1;
+    if (g.dims < 2) jl = ju = 0;
+    if (g.dims < 3) kl = ku = 0;
+    plain::Box b = mkbox(il, iu, jl, ju, kl, ku);
+    plain::k_ee<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, a.ec, a.flx[0], a.flx[1], a.flx[2], a.ee, b);
+  }
+  {
+    plain::Box bx = mkbox(l[0], l[1] + 1, l[2], l[3], l[4], l[5]);
+    // y faces to lims[3]+1 like x and z (the reference's ct.pyx:48 stops at
+    // lims[3] and leaves the top predictor face stale)
+    plain::Box by = mkbox(l[0], l[1], l[2], g.dims >= 2 ? l[3] + 1 : l[3], l[4], l[5]);
+    plain::Box bz = mkbox(l[0], l[1], l[2], l[3], l[4], g.dims >= 3 ? l[5] + 1 : l[5]);
+    plain::k_advance_b<0><<<nblocks(boxn(bx), 256), 256, 0, a.stream>>>(g, b1, b0, a.ee, bx, dtp, fac);
+    plain::k_advance_b<1><<<nblocks(boxn(by), 256), 256, 0, a.stream>>>(g, b1, b0, a.ee, by, dtp, fac);
+    plain::k_advance_b<2><<<nblocks(boxn(bz), 256), 256, 0, a.stream>>>(g, b1, b0, a.ee, bz, dtp, fac);
+  }
+  plain::Box b = mkbox(l[0], l[1], l[2], l[3], l[4], l[5]);
+  plain::k_interp_bc<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, u1, b1, b);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Launchers exported to the host context (declared in bnz_launch.h).
+// ---------------------------------------------------------------------------
+
+void plain_predictor_corrector(const StepArgs& a, const double* dtp) {
+  const GridDev& g = a.g;
+  int l[6];
+  // predictor (vanleer.pyx:104-120): order 0, dt/2, Us from U, W, B
+  integrate_hydro(a, a.cons_s, a.cons, a.prim, a.bfld, 0, dtp, 0.5);
+  integrate_field(a, a.cons_s, a.bfld_s, a.prim, a.bfld, 0, dtp, 0.5);
+  integr_lims(g, 0, l);
+  {
+    plain::Box b = mkbox(l[0], l[1], l[2], l[3], l[4], l[5]);
+    plain::k_cons2prim<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, a.prim, a.cons_s, b, a.err);
+  }
+  // corrector (vanleer.pyx:130-151): order reconstr_order, dt, U from Ws, Bs
+  int order = a.reconstr_order;
+  integrate_hydro(a, a.cons, a.cons, a.prim, a.bfld_s, order, dtp, 1.0);
+  integrate_field(a, a.cons, a.bfld, a.prim, a.bfld, order, dtp, 1.0);
+  integr_lims(g, order, l);
+  {
+    plain::Box b = mkbox(l[0], l[1], l[2], l[3], l[4], l[5]);
+    plain::k_cons2prim<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, a.prim, a.cons, b, a.err);
+  }
+}
+
+void apply_bc(const StepArgs& a, double* prim, double* bfld, unsigned mask) {
+  const GridDev& g = a.g;
+  bcdt::FieldList fl;
+  fl.n = 0;
+  for (int f = 0; f < 12; ++f)
+    if (mask & (1u << f)) fl.f[fl.n++] = f;
+  if (fl.n == 0) return;
+  for (int ax = 2; ax >= 0; --ax) {
+    if (ax >= g.dims) continue;
+    const int N[3] = {g.nx, g.ny, g.nz};
+    long long nother = (long long)N[ax == 0 ? 1 : 0] * N[ax == 2 ? 1 : 2];
+    long long n = 2LL * g.ng * nother;
+    dim3 grid(nblocks(n, 256, 4096), fl.n);
+    bcdt::k_bc_axis<<<grid, 256, 0, a.stream>>>(g, ax, prim, bfld, fl, a.bc[ax][0], a.bc[ax][1], a.face_aware);
+  }
+}
+
+void prim2cons_all(const StepArgs& a) {
+  const GridDev& g = a.g;
+  plain::Box b = mkbox(0, g.nx - 1, 0, g.ny - 1, 0, g.nz - 1);
+  plain::k_prim2cons<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, a.cons, a.prim, b);
+}
+
+void cons2prim_all(const StepArgs& a) {
+  const GridDev& g = a.g;
+  plain::Box b = mkbox(0, g.nx - 1, 0, g.ny - 1, 0, g.nz - 1);
+  plain::k_cons2prim<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, a.prim, a.cons, b, a.err);
+}
+
+void interp_bc_active(const StepArgs& a) {
+  const GridDev& g = a.g;
+  plain::Box b = mkbox(g.i1, g.i2, g.j1, g.j2, g.k1, g.k2);
+  plain::k_interp_bc<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, a.prim, a.bfld, b);
+}
+
+void new_dt(const StepArgs& a, const double* prim, DtState* ds, double cour, int clip) {
+  const GridDev& g = a.g;
+  long long n = (long long)(g.i2 - g.i1 + 1) * (g.j2 - g.j1 + 1) * (g.k2 - g.k1 + 1);
+  bcdt::k_dt_reset<<<1, 1, 0, a.stream>>>(ds);
+  bcdt::k_cds_max<<<nblocks(n, 256, 148 * 8), 256, 0, a.stream>>>(g, prim, &ds->cdsmax_bits);
+  bcdt::k_dt_finalize<<<1, 1, 0, a.stream>>>(ds, cour, clip);
+}
+
+void set_dt(cudaStream_t s, DtState* ds, double dt) { bcdt::k_dt_set<<<1, 1, 0, s>>>(ds, dt); }
+void time_advance(cudaStream_t s, DtState* ds) { bcdt::k_time_advance<<<1, 1, 0, s>>>(ds); }
+
+// --- conduction ---------------------------------------------------------
+
+void diff_dt_max(const StepArgs& a, const DiffArgs& d, unsigned long long* slot) {
+  const GridDev& g = a.g;
+  long long n = (long long)(g.i2 - g.i1 + 1) * (g.j2 - g.j1 + 1) * (g.k2 - g.k1 + 1);
+  diff::k_diff_dt_max<<<nblocks(n, 256, 148 * 8), 256, 0, a.stream>>>(g, a.prim, d.kappa0, slot);
+}
+
+// thcond_elec.pyx:118-338 (apply_diff_oper)
+void diff_operator(const StepArgs& a, const DiffArgs& d) {
+  const GridDev& g = a.g;
+  diff::k_temp<<<nblocks(g.sv, 256), 256, 0, a.stream>>>(g, a.prim, d.temp);
+  int il = 1, iu = g.nx - 2;
+  int jl = g.dims >= 2 ? 1 : 0, ju = g.dims >= 2 ? g.ny - 2 : 0;
+  int kl = g.dims >= 3 ? 1 : 0, ku = g.dims >= 3 ? g.nz - 2 : 0;
+  {
+    int3 lo = make_int3(il, jl, kl), hi = make_int3(iu + 1, ju, ku);
+    long long n = (long long)(hi.x - lo.x + 1) * (hi.y - lo.y + 1) * (hi.z - lo.z + 1);
+    diff::k_flux<0><<<nblocks(n, 256), 256, 0, a.stream>>>(g, a.prim, a.bfld, d.temp, d.fx, d, lo, hi);
+  }
+  if (g.dims >= 2) {
+    int3 lo = make_int3(il, jl, kl), hi = make_int3(iu, ju + 1, ku);
+    long long n = (long long)(hi.x - lo.x + 1) * (hi.y - lo.y + 1) * (hi.z - lo.z + 1);
+    diff::k_flux<1><<<nblocks(n, 256), 256, 0, a.stream>>>(g, a.prim, a.bfld, d.temp, d.fy, d, lo, hi);
+  }
+  if (g.dims >= 3) {
+    int3 lo = make_int3(il, jl, kl), hi = make_int3(iu, ju, ku + 1);
+    long long n = (long long)(hi.x - lo.x + 1) * (hi.y - lo.y + 1) * (hi.z - lo.z + 1);
+    diff::k_flux<2><<<nblocks(n, 256), 256, 0, a.stream>>>(g, a.prim, a.bfld, d.temp, d.fz, d, lo, hi);
+  }
+  int3 lo = make_int3(il, jl, kl), hi = make_int3(iu, ju, ku);
+  long long n = (long long)(hi.x - lo.x + 1) * (hi.y - lo.y + 1) * (hi.z - lo.z + 1);
+  diff::k_dtemp<<<nblocks(n, 256), 256, 0, a.stream>>>(g, d.fx, d.fy, d.fz, d.dtemp, lo, hi);
+}
+
+void diff_stage_update(const StepArgs& a, const DiffArgs& d, int first, const double* coef, const double* dtp) {
+  const GridDev& g = a.g;
+  int il = 1, iu = g.nx - 2;
+  int jl = g.dims >= 2 ? 1 : 0, ju = g.dims >= 2 ? g.ny - 2 : 0;
+  int kl = g.dims >= 3 ? 1 : 0, ku = g.dims >= 3 ? g.nz - 2 : 0;
+  int3 lo = make_int3(il, jl, kl), hi = make_int3(iu, ju, ku);
+  long long n = (long long)(hi.x - lo.x + 1) * (hi.y - lo.y + 1) * (hi.z - lo.z + 1);
+  diff::k_sts_update<<<nblocks(n, 256), 256, 0, a.stream>>>(g, a.prim, d, lo, hi, first, coef[0], coef[1], coef[2],
+                                                              coef[3], dtp);
+}
+
+// Fused path: not selectable yet (the context rejects BNZ_PATH_FUSED).
+void fused_step(const StepArgs&, const double*) {}
+
+}  // namespace BNZ_NS

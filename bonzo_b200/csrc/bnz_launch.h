@@ -1,0 +1,46 @@
+// bnz_launch.h -- host launchers of one floating-point mode, and the dispatch
+// table the context uses to pick the exact (no contraction) or fast build.
+#pragma once
+
+#include "bnz_common.h"
+
+struct Launchers {
+  void (*plain_predictor_corrector)(const StepArgs&, const double* dtp);
+  void (*fused_step)(const StepArgs&, const double* dtp);
+  void (*apply_bc)(const StepArgs&, double* prim, double* bfld, unsigned mask);
+  void (*prim2cons_all)(const StepArgs&);
+  void (*cons2prim_all)(const StepArgs&);
+  void (*interp_bc_active)(const StepArgs&);
+  void (*new_dt)(const StepArgs&, const double* prim, DtState* ds, double cour, int clip);
+  void (*set_dt)(cudaStream_t, DtState*, double);
+  void (*time_advance)(cudaStream_t, DtState*);
+  void (*diff_dt_max)(const StepArgs&, const DiffArgs&, unsigned long long* slot);
+  void (*diff_operator)(const StepArgs&, const DiffArgs&);
+  void (*diff_stage_update)(const StepArgs&, const DiffArgs&, int first, const double* coef, const double* dtp);
+};
+
+#define BNZ_DECLARE_LAUNCHERS(NS)                                                                     \
+  namespace NS {                                                                                      \
+  void plain_predictor_corrector(const StepArgs&, const double* dtp);                                \
+  void fused_step(const StepArgs&, const double* dtp);                                               \
+  void apply_bc(const StepArgs&, double* prim, double* bfld, unsigned mask);                         \
+  void prim2cons_all(const StepArgs&);                                                                \
+  void cons2prim_all(const StepArgs&);                                                                \
+  void interp_bc_active(const StepArgs&);                                                             \
+  void new_dt(const StepArgs&, const double* prim, DtState* ds, double cour, int clip);              \
+  void set_dt(cudaStream_t, DtState*, double);                                                        \
+  void time_advance(cudaStream_t, DtState*);                                                          \
+  void diff_dt_max(const StepArgs&, const DiffArgs&, unsigned long long* slot);                      \
+  void diff_operator(const StepArgs&, const DiffArgs&);                                               \
+  void diff_stage_update(const StepArgs&, const DiffArgs&, int first, const double* coef, const double* dtp); \
+  extern const Launchers table;                                                                       \
+  }
+
+BNZ_DECLARE_LAUNCHERS(exact)
+BNZ_DECLARE_LAUNCHERS(fast)
+
+#define BNZ_DEFINE_TABLE(NS)                                                                          \
+  const Launchers NS::table = {NS::plain_predictor_corrector, NS::fused_step, NS::apply_bc,          \
+                               NS::prim2cons_all, NS::cons2prim_all, NS::interp_bc_active,           \
+                               NS::new_dt, NS::set_dt, NS::time_advance, NS::diff_dt_max,            \
+                               NS::diff_operator, NS::diff_stage_update};

@@ -1,0 +1,140 @@
+/*
+ * bnz_gpu.h -- C ABI of the B200 VL2 + HLLD + CT step (libbnzgpu.so).
+ *
+ * Drop-in boundary for the reference's integrator / grid calls
+ * (sergekomarov/bonzo).  Plain C types only: integer status codes, opaque
+ * contexts, double arrays in the reference's layout.
+ *
+ * Layout of every state array (the reference's GridData, src/coordinates/
+ * grid.pyx:30-52): C-contiguous [var][k][j][i] over the FULL grid including
+ * ghost cells, FP64.  prim / cons have 9 variables in the order
+ * rho, vx|mx, vy|my, vz|mz, p|E, passive scalar, Bx, By, Bz (src/defs_c.h:68-85);
+ * bfld has 3 face-centred components, bfld[0][k][j][i] on the x face at the
+ * left edge of cell i (and likewise for y, z).
+ *
+ * Ownership: host pointers are borrowed for the duration of a call only.
+ * Device buffers belong to the context.  Calls on one context are ordered on
+ * its CUDA stream and are not re-entrant; one context per host thread.
+ *
+ * Every function returns BNZ_OK (0) or a positive bnz_status; the message of
+ * the last failure is bnz_last_error(ctx).
+ */
+#ifndef BNZ_GPU_H
+#define BNZ_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  BNZ_OK = 0,
+  BNZ_ERR_ARG = 1,         /* bad argument or configuration (rejected before any launch) */
+  BNZ_ERR_CUDA = 2,        /* CUDA runtime error */
+  BNZ_ERR_STATE = 3,       /* non-physical state met on the device (rho<=0, p<=0, NaN) */
+  BNZ_ERR_UNSUPPORTED = 4, /* option not available in this build */
+  BNZ_ERR_TIMEOUT = 5,     /* a bounded device wait ran out */
+  BNZ_ERR_NOMEM = 6
+} bnz_status;
+
+/* Method enums, values as the reference's integrator enums
+ * (src/integration/integrator.pxd:52-91) where it has them. */
+enum { BNZ_RS_HLL = 0, BNZ_RS_HLLC = 1, BNZ_RS_HLLD = 2, BNZ_RS_HLLT = 3 };
+enum { BNZ_RCN_CONST = 0, BNZ_RCN_LINEAR = 1 };
+enum { BNZ_LIM_VL = 0, BNZ_LIM_MC = 1, BNZ_LIM_MM = 2 };
+enum { BNZ_BC_PERIODIC = 0, BNZ_BC_OUTFLOW = 1, BNZ_BC_REFLECT = 2 };
+enum { BNZ_TC_ISO = 0, BNZ_TC_ANISO = 1 };
+/* kernel path: fused tile kernels (default) or one kernel per reference loop */
+enum { BNZ_PATH_FUSED = 0, BNZ_PATH_PLAIN = 1 };
+
+/* Grid: the [computation] Nx..Nz / xmin..zmax keys and the [physics]
+ * bc_x1..bc_z2 flags (src/coordinates/grid.pyx:107-232,
+ * src/bc/grid_bc.pyx:45-50).  dims replaces the reference's D2D/D3D build
+ * flags. */
+typedef struct {
+  int Nx, Ny, Nz;
+  int dims;
+  double lmin[3], lmax[3];
+  int bc[3][2];
+} bnz_grid_desc;
+
+/* Method: the [computation] / [physics] keys of the step
+ * (src/integration/integrator.pyx:205-291, src/dissipation/diffusion.pyx:30-49).
+ * limiter is the added `limiter: vl|mc|mm` key (the reference hard-wires vl).
+ * outflow_face_aware keeps the CT-updated outer face under outflow BCs.
+ * exact_fp selects kernels built without multiply-add contraction, which
+ * reproduce the CPU reference bit for bit; path selects fused or plain kernels. */
+typedef struct {
+  double gam, cour;
+  int rsolver, reconstr, limiter, charact_proj;
+  double kappa0;
+  int thcond_type, sat_hfe;
+  double cour_diff;
+  int fixdt;
+  double dt_fixed;
+  int outflow_face_aware;
+  int exact_fp;
+  int path;
+} bnz_method_desc;
+
+typedef struct bnz_ctx bnz_ctx;
+
+/* BnzGrid(usr_dir) + BnzIntegr(gc, usr_dir): src/coordinates/grid.pyx:59-81,
+ * src/integration/integrator.pyx:23-28.  Allocates the device state. */
+int bnz_create(const bnz_grid_desc* grid, const bnz_method_desc* method, bnz_ctx** out);
+int bnz_destroy(bnz_ctx* ctx);
+const char* bnz_last_error(const bnz_ctx* ctx);
+/* Ntot[3] (x, y, z, ghosts included) and the ghost width ng. */
+int bnz_shape(const bnz_ctx* ctx, int* ntot, int* ng);
+
+/* Upload a full state (the arrays set_problem writes; problem.pyx API,
+ * called at src/integration/vanleer.pyx:32).  is_prim=0 means cons is given
+ * and is converted to primitives on every cell.  bfld may be NULL to keep the
+ * current face field. */
+int bnz_set_state(bnz_ctx* ctx, const double* prim_or_cons, int is_prim, const double* bfld);
+/* init_sim after set_problem (src/integration/vanleer.pyx:41-48): ghost fill,
+ * face-to-cell B, ghost fill of cell B, prim2cons everywhere; time = 0. */
+int bnz_init(bnz_ctx* ctx);
+/* Download (any pointer may be NULL): GridData.prim / cons / bfld. */
+int bnz_get_state(bnz_ctx* ctx, double* prim, double* cons, double* bfld);
+
+/* GridBC.apply_grid_bc(bvars) (src/bc/grid_bc.pyx:323-339): bit n of var_mask
+ * selects prim variable n (0..8) or face component n-9 (9..11). */
+int bnz_apply_bc(bnz_ctx* ctx, uint32_t var_mask);
+/* BnzIntegr.new_dt (src/integration/new_dt.pyx:18-135): CFL time step. */
+int bnz_new_dt(bnz_ctx* ctx, double* dt_out);
+/* One VL2 step of size dt (src/integration/vanleer.pyx:101-163): predictor,
+ * corrector, conduction (if kappa0 != 0), ghost fill, prim2cons. */
+int bnz_vl2_step(bnz_ctx* ctx, double dt);
+/* BnzDiffusion.diffuse (src/dissipation/diffusion.pyx:158-198): RKL2
+ * super-time-stepped field-aligned conduction over dt.  *nsts_out (may be
+ * NULL) receives the stage count. */
+int bnz_diffuse(bnz_ctx* ctx, double dt, int* nsts_out);
+/* vanleer.advance (src/integration/vanleer.pyx:59-179): step until time >=
+ * tmax or max_steps (>0) steps.  The CFL step is computed and clipped to tmax
+ * on the device; the host reads back 8 bytes per step to stop the loop. */
+int bnz_advance(bnz_ctx* ctx, double tmax, int max_steps, double* time_out, long* step_out);
+int bnz_get_time(const bnz_ctx* ctx, double* time_out, long* step_out, double* last_dt);
+int bnz_set_time(bnz_ctx* ctx, double time, long step);
+/* Sticky device error word (bits: 1 rho<=0, 2 p<=0, 4 NaN, 8 unordered
+ * Riemann fan, 16 timeout); cleared by the call. */
+int bnz_check(bnz_ctx* ctx, uint32_t* err_bits);
+/* Wait for the context's stream. */
+int bnz_sync(bnz_ctx* ctx);
+
+/* Capture one full step (dt from the device CFL, clipped to tmax) into a CUDA
+ * graph and replay it n times: vanleer.advance with the host out of the loop. */
+int bnz_advance_graph(bnz_ctx* ctx, double tmax, int nsteps);
+
+/* Device pointers of the context's state (prim, cons, bfld), for zero-copy
+ * interop; valid until bnz_destroy. */
+int bnz_device_state(bnz_ctx* ctx, double** prim, double** cons, double** bfld);
+/* Raw CUDA stream handle of the context (cudaStream_t as void*). */
+int bnz_stream(bnz_ctx* ctx, void** stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,1988 @@
+/*
+ * bnz_oracle.c -- CPU ORACLE (test infrastructure only; see bnz_oracle.h).
+ *
+ * Plain-C restatement of the reference's VL2 + Riemann + CT step.  Every
+ * function names the reference file:line it follows.  Expressions keep the
+ * reference's evaluation order so that, built with -ffp-contract=off, the
+ * restated kernels reproduce the reference's compiled kernels bit for bit.
+ *
+ * Documented deviations from the reference as shipped (the reference does not
+ * build; these follow its evident intent):
+ *   D10  y/z sweeps roll the left state between rows (util.pyx:204-208 is a
+ *        no-op swap of local copies).
+ *   D12  the 2D Bz-face loop runs k=0 only (ct.pyx:75 writes past the array).
+ *   D13  outflow on the face field normal to the boundary keeps the
+ *        CT-updated outer face when outflow_face_aware=1 (the variant left
+ *        commented in grid_bc_funcs.pyx:137-138); =0 reproduces :135.
+ *   D15  RKL2 coefficient columns MU,NU,MUT,GAMT are 0..3.
+ *   D16  the previous-stage buffers are pressure buffers.
+ *   D18  `limiter` selects vl (reference default), mc or mm.
+ *   D20  z1 outflow copies from the first active layer k1 into k1-ng..k1-1
+ *        (grid_bc_funcs.pyx:177 passes k1 where x/y pass i1-1/j1-1, which
+ *        would overwrite the first active layer).
+ *   D22  reflect BC: the normal velocity / cell B take the sign flip only
+ *        (grid_bc_funcs.pyx:215-223 lets the trailing else overwrite it).
+ *   D26  the y-face CT loop runs to lims[3]+1 like the x and z loops
+ *        (ct.pyx:48 stops at lims[3]; the predictor's top y face is then never
+ *        written, its stale value reaches the top active row through the
+ *        corrector's PLM stencil and, with periodic BCs, breaks div B).
+ * Faithful quirks kept on purpose:
+ *   - fms(w, bx, gam) ignores bx and uses w[BX] (eos_c.h:476-477), so new_dt
+ *     uses the x fast speed in every direction (new_dt.pyx:76-85).
+ *   - the conduction transverse-gradient limiter returns a magnitude
+ *     (util_diffusion.pyx:16-20).
+ */
+#include "bnz_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define NM ORC_NMODE
+#define SQR(x) ((x) * (x))
+#define SIGN(a) ((0.0 < (a)) - ((a) < 0.0))
+#define SMALL_NUM 1.0e-20
+
+#if ORC_MFIELD
+#define BX O_BX
+#define BY O_BY
+#define BZ O_BZ
+#endif
+#define RHO O_RHO
+#define MX O_MX
+#define MY O_MY
+#define MZ O_MZ
+#define EN O_EN
+#define PSC O_PSC
+#define VX O_VX
+#define VY O_VY
+#define VZ O_VZ
+#define PR O_PR
+
+/* ======================================================================
+ * EOS  (src/mhd/eos_c.h)
+ * ====================================================================== */
+
+/* eos_c.h:20-55 */
+static inline void o_cons2prim(real *w, const real *u, real gam) {
+  real rhoi = 1. / u[RHO];
+  w[RHO] = u[RHO];
+  w[VX] = u[MX] * rhoi;
+  w[VY] = u[MY] * rhoi;
+  w[VZ] = u[MZ] * rhoi;
+  real v2 = SQR(w[VX]) + SQR(w[VY]) + SQR(w[VZ]);
+  real b2 = 0.;
+#if ORC_MFIELD
+  b2 = SQR(u[BX]) + SQR(u[BY]) + SQR(u[BZ]);
+#endif
+  w[PR] = (gam - 1.) * (u[EN] - 0.5 * (b2 + v2 * u[RHO]));
+  w[PSC] = u[PSC];
+#if ORC_MFIELD
+  w[BX] = u[BX];
+  w[BY] = u[BY];
+  w[BZ] = u[BZ];
+#endif
+}
+
+/* eos_c.h:60-95 */
+static inline void o_prim2cons(real *u, const real *w, real gam) {
+  real gamm1i = 1. / (gam - 1.);
+  u[RHO] = w[RHO];
+  u[MX] = w[RHO] * w[VX];
+  u[MY] = w[RHO] * w[VY];
+  u[MZ] = w[RHO] * w[VZ];
+  real v2 = SQR(w[VX]) + SQR(w[VY]) + SQR(w[VZ]);
+  real b2 = 0.;
+#if ORC_MFIELD
+  b2 = SQR(w[BX]) + SQR(w[BY]) + SQR(w[BZ]);
+#endif
+  u[EN] = 0.5 * (w[RHO] * v2 + b2) + w[PR] * gamm1i;
+  u[PSC] = w[PSC];
+#if ORC_MFIELD
+  u[BX] = w[BX];
+  u[BY] = w[BY];
+  u[BZ] = w[BZ];
+#endif
+}
+
+/* eos_c.h:416-461 (no CGL / TWOTEMP: a = 1) */
+static inline void o_primcons2flux(real *f, const real *w, const real *u, real gam) {
+  (void)gam;
+  real ptot = 0.;
+#if ORC_MFIELD
+  real bx2 = SQR(w[BX]);
+  real b2 = bx2 + SQR(w[BY]) + SQR(w[BZ]);
+  real bxby = w[BX] * w[BY];
+  real bxbz = w[BX] * w[BZ];
+  ptot += 0.5 * b2;
+#endif
+  real a = 1.;
+  ptot += w[PR];
+#if ORC_MFIELD
+  for (int n = 0; n < BX; ++n) f[n] = u[n] * w[VX];
+#else
+  for (int n = 0; n < NM; ++n) f[n] = u[n] * w[VX];
+#endif
+  f[MX] += ptot;
+  f[EN] += ptot * w[VX];
+#if ORC_MFIELD
+  f[MX] -= a * bx2;
+  f[MY] -= a * bxby;
+  f[MZ] -= a * bxbz;
+  f[EN] -= a * (w[VX] * bx2 + w[VY] * bxby + w[VZ] * bxbz);
+  f[BX] = 0.;
+  f[BY] = w[VX] * w[BY] - w[VY] * w[BX];
+  f[BZ] = w[VX] * w[BZ] - w[VZ] * w[BX];
+#else
+  (void)a;
+#endif
+}
+
+/* eos_c.h:468-530.  The bx argument is not read (the reference uses w[BX]). */
+real orc_fms(real *w, real bx, real gam) {
+  (void)bx;
+  real p = w[PR];
+  real gamp = gam * p;
+#if ORC_MFIELD
+  real bx2 = SQR(w[BX]);
+  real b2 = bx2 + SQR(w[BY]) + SQR(w[BZ]);
+  real c1 = gamp + b2;
+  real c2 = sqrt(fabs(c1 * c1 - 4. * gamp * bx2));
+  return sqrt(0.5 / w[RHO] * (c1 + c2));
+#else
+  return sqrt(gamp / w[RHO]);
+#endif
+}
+
+/* eos_c.h:100-216 prim2char (MHD branch; hydro branch :218-240) */
+static void o_prim2char(real *vc, const real *w, real gam) {
+#if ORC_MFIELD
+  real vc_rho = vc[RHO], vc_vx = vc[VX], vc_vy = vc[VY], vc_vz = vc[VZ];
+  real vc_p = vc[PR], vc_by = vc[BY], vc_bz = vc[BZ];
+  real w_rho = w[RHO], w_p = w[PR], w_bx = w[BX], w_by = w[BY], w_bz = w[BZ];
+  real rhoi = 1. / w_rho;
+  real s = SIGN(w_bx);
+  real a2rho = gam * w_p;
+  real a = sqrt(a2rho * rhoi);
+  real bx2 = SQR(w_bx);
+  real bperp2 = SQR(w_by) + SQR(w_bz);
+  real b2 = bx2 + bperp2;
+  real x = a2rho + b2;
+  real y = sqrt(fabs(x * x - 4. * a2rho * bx2));
+  real cf2rho = 0.5 * (x + y);
+  real cs2rho = 0.5 * (x - y);
+  real cf = sqrt(rhoi * cf2rho);
+  real cs = sqrt(rhoi * fabs(cs2rho));
+  real z = 1. / (cf2rho - cs2rho);
+  real alphaf, alphas;
+  if (cf <= cs) { alphaf = 1.; alphas = 0.; }
+  else if (a <= cs) { alphaf = 0.; alphas = 1.; }
+  else if (cf <= a) { alphaf = 1.; alphas = 0.; }
+  else {
+    alphaf = sqrt(z * fabs(a2rho - cs2rho));
+    alphas = sqrt(z * fabs(cf2rho - a2rho));
+  }
+  real nf = 0.5 / (a2rho * rhoi);
+  real qf_ = nf * cf * alphaf * s;
+  real qs_ = nf * cs * alphas * s;
+  real alphaf_ = nf * alphaf;
+  real alphas_ = nf * alphas;
+  real rhoisr = sqrt(rhoi);
+  real arhoisr = a * rhoisr;
+  real Af_ = alphaf_ * arhoisr;
+  real As_ = alphas_ * arhoisr;
+  x = s * rhoisr;
+  real betay = 0., betaz = 0.;
+  if (bperp2 != 0.) {
+    real bperpi = 1. / sqrt(bperp2);
+    betay = bperpi * w_by;
+    betaz = bperpi * w_bz;
+  }
+  vc[RHO] = (alphaf_ * (rhoi * vc_p - cf * vc_vx) + qs_ * (betay * vc_vy + betaz * vc_vz) +
+             As_ * (betay * vc_by + betaz * vc_bz));
+  vc[VX] = 0.5 * ((-betaz * vc_vy + betay * vc_vz) + x * (-betaz * vc_by + betay * vc_bz));
+  vc[VY] = (alphas_ * (rhoi * vc_p - cs * vc_vx) - qf_ * (betay * vc_vy + betaz * vc_vz) -
+            Af_ * (betay * vc_by + betaz * vc_bz));
+  vc[VZ] = vc_rho - 2. * nf * vc_p;
+  vc[PR] = (alphas_ * (rhoi * vc_p + cs * vc_vx) + qf_ * (betay * vc_vy + betaz * vc_vz) -
+            Af_ * (betay * vc_by + betaz * vc_bz));
+  vc[BY] = 0.5 * ((betaz * vc_vy - betay * vc_vz) + x * (-betaz * vc_by + betay * vc_bz));
+  vc[BZ] = (alphaf_ * (rhoi * vc_p + cf * vc_vx) - qs_ * (betay * vc_vy + betaz * vc_vz) +
+            As_ * (betay * vc_by + betaz * vc_bz));
+#else
+  real w_rho = w[RHO], w_p = w[PR];
+  real vc_rho = vc[RHO], vc_vx = vc[VX], vc_vy = vc[VY], vc_vz = vc[VZ], vc_p = vc[PR];
+  real a2i = w_rho / (gam * w_p);
+  real ai = sqrt(a2i);
+  vc[RHO] = 0.5 * (a2i * vc_p - ai * w_rho * vc_vx);
+  vc[VX] = vc_rho - a2i * vc_p;
+  vc[VY] = vc_vy;
+  vc[VZ] = vc_vz;
+  vc[PR] = 0.5 * (a2i * vc_p + ai * w_rho * vc_vx);
+#endif
+}
+
+/* eos_c.h:245-333 char2prim (MHD branch; hydro branch :315-331) */
+static void o_char2prim(real *vc, const real *w, real gam) {
+#if ORC_MFIELD
+  real vc_rho = vc[RHO], vc_vx = vc[VX], vc_vy = vc[VY], vc_vz = vc[VZ];
+  real vc_p = vc[PR], vc_by = vc[BY], vc_bz = vc[BZ];
+  real w_rho = w[RHO], w_p = w[PR], w_bx = w[BX], w_by = w[BY], w_bz = w[BZ];
+  real rhoi = 1. / w_rho;
+  real s = SIGN(w_bx);
+  real a2rho = gam * w_p;
+  real a = sqrt(a2rho * rhoi);
+  real bx2 = SQR(w_bx);
+  real bperp2 = SQR(w_by) + SQR(w_bz);
+  real b2 = bx2 + bperp2;
+  real x = a2rho + b2;
+  real y = sqrt(fabs(x * x - 4. * a2rho * bx2));
+  real cf2rho = 0.5 * (x + y);
+  real cs2rho = 0.5 * (x - y);
+  real cf = sqrt(rhoi * cf2rho);
+  real cs = sqrt(rhoi * fabs(cs2rho));
+  real z = 1. / (cf2rho - cs2rho);
+  real alphaf, alphas;
+  if (cf <= cs) { alphaf = 1.; alphas = 0.; }
+  else if (a <= cs) { alphaf = 0.; alphas = 1.; }
+  else if (cf <= a) { alphaf = 1.; alphas = 0.; }
+  else {
+    alphaf = sqrt(z * fabs(a2rho - cs2rho));
+    alphas = sqrt(z * fabs(cf2rho - a2rho));
+  }
+  real qf = cf * alphaf * s;
+  real qs = cs * alphas * s;
+  real rhosr = sqrt(w_rho);
+  real arhosr = a * rhosr;
+  real Af = alphaf * arhosr;
+  real As = alphas * arhosr;
+  real betay = 0., betaz = 0.;
+  if (bperp2 != 0.) {
+    real bperpi = 1. / sqrt(bperp2);
+    betay = bperpi * w_by;
+    betaz = bperpi * w_bz;
+  }
+  vc[RHO] = w_rho * (alphaf * (vc_rho + vc_bz) + alphas * (vc_vy + vc_p)) + vc_vz;
+  vc[VX] = cf * alphaf * (vc_bz - vc_rho) + cs * alphas * (vc_p - vc_vy);
+  vc[VY] = betay * (qs * (vc_rho - vc_bz) - qf * (vc_vy - vc_p)) - betaz * (vc_vx - vc_by);
+  vc[VZ] = betaz * (qs * (vc_rho - vc_bz) - qf * (vc_vy - vc_p)) + betay * (vc_vx - vc_by);
+  vc[PR] = a2rho * (alphaf * (vc_rho + vc_bz) + alphas * (vc_vy + vc_p));
+  vc[BY] = betay * (As * (vc_rho + vc_bz) - Af * (vc_vy + vc_p)) - betaz * s * rhosr * (vc_vx + vc_by);
+  vc[BZ] = betaz * (As * (vc_rho + vc_bz) - Af * (vc_vy + vc_p)) + betay * s * rhosr * (vc_vx + vc_by);
+#else
+  real vc_rho = vc[RHO], vc_vx = vc[VX], vc_vy = vc[VY], vc_vz = vc[VZ], vc_p = vc[PR];
+  real rhoi = 1. / w[RHO];
+  real a2 = gam * rhoi * w[PR];
+  real a = sqrt(a2);
+  vc[RHO] = vc_rho + vc_vx + vc_p;
+  vc[VX] = a * rhoi * (vc_p - vc_rho);
+  vc[VY] = vc_vy;
+  vc[VZ] = vc_vz;
+  vc[PR] = a2 * (vc_rho + vc_p);
+#endif
+}
+
+/* eos_c.c:9-26 */
+void orc_cons2prim_1(real **w1, real **u1, int i1, int i2, real gam) {
+  real w[NM], u[NM];
+  for (int i = i1; i <= i2; ++i) {
+    for (int n = 0; n < NM; ++n) u[n] = u1[n][i];
+    o_cons2prim(w, u, gam);
+    for (int n = 0; n < NM; ++n) w1[n][i] = w[n];
+  }
+}
+
+/* eos_c.c:31-48 */
+void orc_prim2cons_1(real **u1, real **w1, int i1, int i2, real gam) {
+  real w[NM], u[NM];
+  for (int i = i1; i <= i2; ++i) {
+    for (int n = 0; n < NM; ++n) w[n] = w1[n][i];
+    o_prim2cons(u, w, gam);
+    for (int n = 0; n < NM; ++n) u1[n][i] = u[n];
+  }
+}
+
+/* eos_c.c:53-94 with the loop bodies braced (D8). */
+static void o_prim2char_1(real **vc1, real **w1, int i1, int i2, real gam) {
+  real w[NM], vc[NM];
+  for (int i = i1; i <= i2; ++i) {
+    for (int n = 0; n < NM; ++n) { w[n] = w1[n][i]; vc[n] = vc1[n][i]; }
+    o_prim2char(vc, w, gam);
+    for (int n = 0; n < NM; ++n) vc1[n][i] = vc[n];
+  }
+}
+static void o_char2prim_1(real **vc1, real **w1, int i1, int i2, real gam) {
+  real w[NM], vc[NM];
+  for (int i = i1; i <= i2; ++i) {
+    for (int n = 0; n < NM; ++n) { w[n] = w1[n][i]; vc[n] = vc1[n][i]; }
+    o_char2prim(vc, w, gam);
+    for (int n = 0; n < NM; ++n) vc1[n][i] = vc[n];
+  }
+}
+
+/* ======================================================================
+ * Riemann solvers  (src/mhd/fluxes_c.c)
+ * ====================================================================== */
+
+/* fluxes_c.c:25-42 */
+static inline void o_sLsR_simple(real *sL, real *sR, real *wL, real *wR, real gam) {
+  real bx = 0.;
+#if ORC_MFIELD
+  bx = wL[BX];
+#endif
+  real cfL = orc_fms(wL, bx, gam);
+  real cfR = orc_fms(wR, bx, gam);
+  real cf_max = fmax(cfL, cfR);
+  *sL = fmin(wL[VX], wR[VX]) - cf_max;
+  *sR = fmax(wL[VX], wR[VX]) + cf_max;
+}
+
+#if !ORC_MFIELD
+/* fluxes_c.c:138-168 */
+static inline void o_sLsR_pressure(real *sL, real *sR, real *wL, real *wR, real gam) {
+  real g1gh = 0.5 * (gam + 1.) / gam;
+  real rhoL = wL[RHO], rhoR = wR[RHO];
+  real vxL = wL[VX], vxR = wR[VX];
+  real ptL = wL[PR], ptR = wR[PR];
+  real aL = orc_fms(wL, 0., gam);
+  real aR = orc_fms(wR, 0., gam);
+  real qL, qR;
+  real pvrs = fmax(0., 0.5 * (ptL + ptR) - 0.125 * (vxR - vxL) * (rhoL + rhoR) * (aL + aR));
+  if (pvrs < ptL) qL = 1.;
+  else qL = sqrt(1. + g1gh * (pvrs / ptL - 1.));
+  if (pvrs < ptR) qR = 1.;
+  else qR = sqrt(1. + g1gh * (pvrs / ptR - 1.));
+  *sL = vxL - aL * qL;
+  *sR = vxR + aR * qR;
+}
+#endif
+
+/* fluxes_c.c:175-223, one interface. */
+static void o_hll_pt(real *flux, real *wL, real *wR, real gam) {
+  real uL[NM], uR[NM], fL[NM], fR[NM];
+  o_prim2cons(uL, wL, gam);
+  o_prim2cons(uR, wR, gam);
+  o_primcons2flux(fL, wL, uL, gam);
+  o_primcons2flux(fR, wR, uR, gam);
+  real sL = 0., sR = 0.;
+  o_sLsR_simple(&sL, &sR, wL, wR, gam);
+  real aL = fmin(sL, 0.);
+  real aR = fmax(sR, 0.);
+  real aLaR = aL * aR;
+  real aRmaLi = 1. / (aR - aL);
+  for (int n = 0; n < NM; ++n)
+    flux[n] = (aR * fL[n] - aL * fR[n] + aLaR * (uR[n] - uL[n])) * aRmaLi;
+#if ORC_MFIELD
+  flux[BX] = 0.;
+#endif
+}
+
+void orc_hll_flux(real **_flux, real **_wL, real **_wR, real *_bx, int i1, int i2, real gam) {
+  real wL[NM], wR[NM], f[NM];
+  for (int i = i1; i <= i2; ++i) {
+    for (int n = 0; n < NM; ++n) { wL[n] = _wL[n][i]; wR[n] = _wR[n][i]; }
+#if ORC_MFIELD
+    wL[BX] = _bx[i];
+    wR[BX] = _bx[i];
+#else
+    (void)_bx;
+#endif
+    o_hll_pt(f, wL, wR, gam);
+    for (int n = 0; n < NM; ++n) _flux[n][i] = f[n];
+  }
+}
+
+#if !ORC_MFIELD
+/* fluxes_c.c:232-327 (hydro builds only). */
+void orc_hllc_flux(real **_flux, real **_wL, real **_wR, real *_bx, int i1, int i2, real gam) {
+  (void)_bx;
+  real wL[NM], wR[NM], uL[NM], uR[NM], fL[NM], fR[NM];
+  for (int i = i1; i <= i2; ++i) {
+    for (int n = 0; n < NM; ++n) { wL[n] = _wL[n][i]; wR[n] = _wR[n][i]; }
+    real sL = 0., sR = 0.;
+    o_prim2cons(uL, wL, gam);
+    o_prim2cons(uR, wR, gam);
+    o_sLsR_pressure(&sL, &sR, wL, wR, gam);
+    real ptL = wL[PR], ptR = wR[PR];
+    real vLsL = wL[VX] - sL;
+    real vRsR = wR[VX] - sR;
+    real xL = uL[RHO] * vLsL;
+    real xR = uR[RHO] * vRsR;
+    real xRxLi = 1. / (xR - xL);
+    real yL = ptL + uL[MX] * vLsL;
+    real yR = ptR + uR[MX] * vRsR;
+    real sM = xRxLi * (yR - yL);
+    real pts = xRxLi * (xR * yL - xL * yR);
+    sL = fmin(sL, 0.);
+    sR = fmax(sR, 0.);
+    vLsL = wL[VX] - sL;
+    vRsR = wR[VX] - sR;
+    for (int n = 0; n < NM; ++n) { fL[n] = uL[n] * vLsL; fR[n] = uR[n] * vRsR; }
+    fL[MX] += ptL;
+    fR[MX] += ptR;
+    fL[EN] += ptL * wL[VX];
+    fR[EN] += ptR * wR[VX];
+    real sLsMi = 1. / (sL - sM);
+    real sRsMi = 1. / (sR - sM);
+    real zL, zR, sLR;
+    if (sM > 0.) { zL = -sM * sLsMi; zR = 0.; sLR = sL * sLsMi; }
+    else { zL = 0.; zR = -sM * sRsMi; sLR = sR * sRsMi; }
+    for (int n = 0; n < NM; n++) _flux[n][i] = zL * fL[n] + zR * fR[n];
+    _flux[MX][i] += sLR * pts;
+    _flux[EN][i] += sLR * pts * sM;
+  }
+}
+#endif
+
+/* fluxes_c.c:447-607, one interface. */
+static void o_hllt_pt(real *flux, real *wL, real *wR, real gam) {
+  real uL[NM], uR[NM], uLs[NM], uRs[NM], uCs[NM], fL[NM], fR[NM];
+  memset(uLs, 0, sizeof uLs); memset(uRs, 0, sizeof uRs); memset(uCs, 0, sizeof uCs);
+  o_prim2cons(uL, wL, gam);
+  o_prim2cons(uR, wR, gam);
+  o_primcons2flux(fL, wL, uL, gam);
+  o_primcons2flux(fR, wR, uR, gam);
+  real sL = 0., sR = 0.;
+  o_sLsR_simple(&sL, &sR, wL, wR, gam);
+  real sRsLi = 1. / (sR - sL);
+  real rhos = (sR * uR[RHO] - sL * uL[RHO] - (fR[RHO] - fL[RHO])) * sRsLi;
+  real mxs = (sR * uR[MX] - sL * uL[MX] - (fR[MX] - fL[MX])) * sRsLi;
+  real frhos = (sR * fL[RHO] - sL * fR[RHO] + sR * sL * (uR[RHO] - uL[RHO])) * sRsLi;
+  real us = frhos / rhos;
+  real pscs = (sR * uR[PSC] - sL * uL[PSC] - (fR[PSC] - fL[PSC])) * sRsLi;
+  uLs[RHO] = rhos; uRs[RHO] = rhos;
+  uLs[MX] = mxs;   uRs[MX] = mxs;
+  uLs[PSC] = pscs; uRs[PSC] = pscs;
+  uLs[MY] = rhos * wL[VY];
+  uRs[MY] = rhos * wR[VY];
+  uLs[MZ] = rhos * wL[VZ];
+  uRs[MZ] = rhos * wR[VZ];
+  real sLs = us, sRs = us;
+#if ORC_MFIELD
+  real bx = wL[BX];
+  real rhosi = 1. / rhos;
+  real sqrt_rhosi = sqrt(rhosi);
+  sLs -= fabs(bx) * sqrt_rhosi;
+  sRs += fabs(bx) * sqrt_rhosi;
+  real xL = 1. / ((sL - sLs) * (sL - sRs));
+  real xR = 1. / ((sR - sLs) * (sR - sRs));
+  real yL = bx * xL * (us - wL[VX]);
+  real yR = bx * xR * (us - wR[VX]);
+  uLs[MY] -= yL * wL[BY];
+  uRs[MY] -= yR * wR[BY];
+  uLs[MZ] -= yL * wL[BZ];
+  uRs[MZ] -= yR * wR[BZ];
+  yL = (wL[RHO] * SQR(sL - wL[VX]) - SQR(bx)) * rhosi * xL;
+  yR = (wR[RHO] * SQR(sR - wR[VX]) - SQR(bx)) * rhosi * xR;
+  uLs[BY] = yL * wL[BY];
+  uRs[BY] = yR * wR[BY];
+  uLs[BZ] = yL * wL[BZ];
+  uRs[BZ] = yR * wR[BZ];
+  uCs[RHO] = rhos;
+  uCs[MX] = mxs;
+  uCs[PSC] = pscs;
+  real sgnb = SIGN(bx);
+  real x = 0.5 * sgnb / sqrt_rhosi;
+  uCs[MY] = 0.5 * (uLs[MY] + uRs[MY]) + x * (uRs[BY] - uLs[BY]);
+  uCs[MZ] = 0.5 * (uLs[MZ] + uRs[MZ]) + x * (uRs[BZ] - uLs[BZ]);
+  uCs[BY] = 0.5 * (uLs[BY] + uRs[BY]) + x * rhosi * (uRs[MY] - uLs[MY]);
+  uCs[BZ] = 0.5 * (uLs[BZ] + uRs[BZ]) + x * rhosi * (uRs[MZ] - uLs[MZ]);
+#endif
+  if (sL > 0.)
+    for (int n = 0; n < NM; ++n) flux[n] = fL[n];
+  if (sL <= 0. && 0. < sLs)
+    for (int n = 0; n < NM; ++n) flux[n] = fL[n] + sL * (uLs[n] - uL[n]);
+#if ORC_MFIELD
+  if (sLs <= 0. && 0. < sRs)
+    for (int n = 0; n < NM; ++n) flux[n] = fL[n] + sL * (uLs[n] - uL[n]) + sLs * (uCs[n] - uLs[n]);
+#endif
+  if (sRs <= 0. && 0. < sR)
+    for (int n = 0; n < NM; ++n) flux[n] = fR[n] + sR * (uRs[n] - uR[n]);
+  if (sR <= 0.)
+    for (int n = 0; n < NM; ++n) flux[n] = fR[n];
+#if ORC_MFIELD
+  flux[BX] = 0.;
+#endif
+}
+
+void orc_hllt_flux(real **_flux, real **_wL, real **_wR, real *_bx, int i1, int i2, real gam) {
+  real wL[NM], wR[NM], f[NM];
+  for (int i = i1; i <= i2; ++i) {
+    for (int n = 0; n < NM; ++n) { wL[n] = _wL[n][i]; wR[n] = _wR[n][i]; f[n] = _flux[n][i]; }
+#if ORC_MFIELD
+    wL[BX] = _bx[i];
+    wR[BX] = _bx[i];
+#else
+    (void)_bx;
+#endif
+    o_hllt_pt(f, wL, wR, gam);
+    for (int n = 0; n < NM; ++n) _flux[n][i] = f[n];
+  }
+}
+
+#if ORC_MFIELD
+/* fluxes_c.c:616-834 (Miyoshi & Kusano HLLD), one interface. */
+static void o_hlld_pt(real *flux, real *wL, real *wR, real gam) {
+  real uL[NM], uR[NM], uLs[NM], uRs[NM], uLss[NM], uRss[NM], fL[NM], fR[NM];
+  memset(uLs, 0, sizeof uLs); memset(uRs, 0, sizeof uRs);
+  memset(uLss, 0, sizeof uLss); memset(uRss, 0, sizeof uRss);
+  real bx = wL[BX];
+  o_prim2cons(uL, wL, gam);
+  o_prim2cons(uR, wR, gam);
+  o_primcons2flux(fL, wL, uL, gam);
+  o_primcons2flux(fR, wR, uR, gam);
+  real sL = 0., sR = 0.;
+  o_sLsR_simple(&sL, &sR, wL, wR, gam);
+
+  real b2hL = 0.5 * (SQR(bx) + SQR(wL[BY]) + SQR(wL[BZ]));
+  real b2hR = 0.5 * (SQR(bx) + SQR(wR[BY]) + SQR(wR[BZ]));
+  real ptL = wL[PR] + b2hL;
+  real ptR = wR[PR] + b2hR;
+
+  real deni = 1. / (sR * uR[RHO] - sL * uL[RHO] - (fR[RHO] - fL[RHO]));
+  real sM = (sR * uR[MX] - sL * uL[MX] - (fR[MX] - fL[MX])) * deni;
+
+  real sLvxL = sL - wL[VX];
+  real sRvxR = sR - wR[VX];
+  real sLsMi = 1. / (sL - sM);
+  real sRsMi = 1. / (sR - sM);
+  real xL = sLvxL * sLsMi;
+  real xR = sRvxR * sRsMi;
+
+  uLs[RHO] = uL[RHO] * xL;
+  uRs[RHO] = uR[RHO] * xR;
+  uLs[PSC] = uL[PSC] * xL;
+  uRs[PSC] = uR[PSC] * xR;
+
+  real pts = wL[RHO] * sLvxL * (sM - wL[VX]) + ptL;
+
+  real rhosLvxL = wL[RHO] * sLvxL;
+  real rhosRvxR = wR[RHO] * sRvxR;
+  real bx2 = SQR(bx);
+  real wvbL = 1. / (rhosLvxL * (sL - sM) - bx2);
+  real wvbR = 1. / (rhosRvxR * (sR - sM) - bx2);
+  real bxsMvxL = bx * (sM - wL[VX]);
+  real bxsMvxR = bx * (sM - wR[VX]);
+  real wvL = bxsMvxL * wvbL;
+  real wvR = bxsMvxR * wvbR;
+  real vyLs = wL[VY] - wL[BY] * wvL;
+  real vyRs = wR[VY] - wR[BY] * wvR;
+  real vzLs = wL[VZ] - wL[BZ] * wvL;
+  real vzRs = wR[VZ] - wR[BZ] * wvR;
+
+  uLs[MX] = uLs[RHO] * sM;
+  uRs[MX] = uRs[RHO] * sM;
+  uLs[MY] = uLs[RHO] * vyLs;
+  uRs[MY] = uRs[RHO] * vyRs;
+  uLs[MZ] = uLs[RHO] * vzLs;
+  uRs[MZ] = uRs[RHO] * vzRs;
+
+  real rhosLvxL2_bx2 = rhosLvxL * sLvxL - bx2;
+  real rhosRvxR2_bx2 = rhosRvxR * sRvxR - bx2;
+  real wbL = rhosLvxL2_bx2 * wvbL;
+  real wbR = rhosRvxR2_bx2 * wvbR;
+  uLs[BY] = wL[BY] * wbL;
+  uRs[BY] = wR[BY] * wbR;
+  uLs[BZ] = wL[BZ] * wbL;
+  uRs[BZ] = wR[BZ] * wbR;
+
+  real vsbsL = sM * bx + vyLs * uLs[BY] + vzLs * uLs[BZ];
+  real vsbsR = sM * bx + vyRs * uRs[BY] + vzRs * uRs[BZ];
+  uLs[EN] = (sLvxL * uL[EN] - ptL * wL[VX] + pts * sM +
+             bx * (wL[VX] * bx + wL[VY] * wL[BY] + wL[VZ] * wL[BZ] - vsbsL)) * sLsMi;
+  uRs[EN] = (sRvxR * uR[EN] - ptR * wR[VX] + pts * sM +
+             bx * (wR[VX] * bx + wR[VY] * wR[BY] + wR[VZ] * wR[BZ] - vsbsR)) * sRsMi;
+
+  uLss[RHO] = uLs[RHO];
+  uRss[RHO] = uRs[RHO];
+  uLss[MX] = uLs[MX];
+  uRss[MX] = uRs[MX];
+  uLss[PSC] = uLs[PSC];
+  uRss[PSC] = uRs[PSC];
+
+  real sqrt_rhoLs = sqrt(uLs[RHO]);
+  real sqrt_rhoRs = sqrt(uRs[RHO]);
+  real sLs = sM - fabs(bx) / sqrt_rhoLs;
+  real sRs = sM + fabs(bx) / sqrt_rhoRs;
+  real rhoLRi = 1. / (sqrt_rhoLs + sqrt_rhoRs);
+  real sgnb = SIGN(bx);
+
+  real vyss = (sqrt_rhoLs * vyLs + sqrt_rhoRs * vyRs + (uRs[BY] - uLs[BY]) * sgnb) * rhoLRi;
+  real vzss = (sqrt_rhoLs * vzLs + sqrt_rhoRs * vzRs + (uRs[BZ] - uLs[BZ]) * sgnb) * rhoLRi;
+  uLss[MY] = uLs[RHO] * vyss;
+  uRss[MY] = uRs[RHO] * vyss;
+  uLss[MZ] = uLs[RHO] * vzss;
+  uRss[MZ] = uRs[RHO] * vzss;
+
+  real byss = (sqrt_rhoLs * uRs[BY] + sqrt_rhoRs * uLs[BY] +
+               sqrt_rhoLs * sqrt_rhoRs * (vyRs - vyLs) * sgnb) * rhoLRi;
+  real bzss = (sqrt_rhoLs * uRs[BZ] + sqrt_rhoRs * uLs[BZ] +
+               sqrt_rhoLs * sqrt_rhoRs * (vzRs - vzLs) * sgnb) * rhoLRi;
+  uLss[BY] = byss;
+  uRss[BY] = byss;
+  uLss[BZ] = bzss;
+  uRss[BZ] = bzss;
+
+  real vssbss = sM * bx + vyss * byss + vzss * bzss;
+  uLss[EN] = uLs[EN] - sqrt_rhoLs * (vsbsL - vssbss) * sgnb;
+  uRss[EN] = uRs[EN] + sqrt_rhoRs * (vsbsR - vssbss) * sgnb;
+
+  if (sL > 0.)
+    for (int n = 0; n < NM; ++n) flux[n] = fL[n];
+  if (sL <= 0. && 0. < sLs)
+    for (int n = 0; n < NM; ++n) flux[n] = fL[n] + sL * (uLs[n] - uL[n]);
+  if (sLs <= 0. && 0. < sM)
+    for (int n = 0; n < NM; ++n)
+      flux[n] = fL[n] + sL * (uLs[n] - uL[n]) + sLs * (uLss[n] - uLs[n]);
+  if (sM <= 0. && 0. < sRs)
+    for (int n = 0; n < NM; ++n)
+      flux[n] = fR[n] + sR * (uRs[n] - uR[n]) + sRs * (uRss[n] - uRs[n]);
+  if (sRs <= 0. && 0. < sR)
+    for (int n = 0; n < NM; ++n) flux[n] = fR[n] + sR * (uRs[n] - uR[n]);
+  if (sR <= 0.)
+    for (int n = 0; n < NM; ++n) flux[n] = fR[n];
+  flux[BX] = 0.;
+}
+
+void orc_hlld_flux(real **_flux, real **_wL, real **_wR, real *_bx, int i1, int i2, real gam) {
+  real wL[NM], wR[NM], f[NM];
+  for (int i = i1; i <= i2; ++i) {
+    for (int n = 0; n < NM; ++n) { wL[n] = _wL[n][i]; wR[n] = _wR[n][i]; f[n] = _flux[n][i]; }
+    wL[BX] = _bx[i];
+    wR[BX] = _bx[i];
+    o_hlld_pt(f, wL, wR, gam);
+    for (int n = 0; n < NM; ++n) _flux[n][i] = f[n];
+  }
+}
+#endif
+
+/* ======================================================================
+ * Reconstruction  (src/coordinates/reconstr_c.{c,h})
+ * ====================================================================== */
+
+/* reconstr_c.h:28-44 */
+static inline real o_mm_lim(real a, real b) {
+  return (a * b <= 0.) ? 0. : ((a > 0.) ? ((a < b) ? a : b) : ((a > b) ? a : b));
+}
+static inline real o_mc_lim(real a, real b) { return o_mm_lim(2. * o_mm_lim(a, b), 0.5 * (a + b)); }
+static inline real o_vl_lim(real a, real b) {
+  real ab = a * b;
+  return (ab > 0.) ? (2. * ab / (a + b)) : 0.;
+}
+
+/* reconstr_c.c:8-22 */
+void orc_reconstr_const(real **wl, real **wr, real ***w, real ***scr, orc_coord *gc, int ax,
+                        int i1, int i2, int j, int k, int char_proj, real gam) {
+  (void)scr; (void)gc; (void)j; (void)k; (void)char_proj; (void)gam;
+  int ip = (ax == 0) ? 1 : 0;
+  for (int n = 0; n < NM; ++n)
+    for (int i = i1; i <= i2; ++i) {
+      wr[n][i] = w[0][n][i];
+      wl[n][i + ip] = w[0][n][i];
+    }
+}
+
+/* reconstr_c.c:29-91 (uniform Cartesian branch), limiter chosen by `lim`. */
+static void o_reconstr_linear_lim(int lim, real **wl, real **wr, real ***w, real ***scr,
+                                  int ax, int i1, int i2, int char_proj, real gam) {
+  real **dm = scr[0];
+  real **dp = scr[1];
+  real **d = scr[0];
+  real **wc = scr[2];
+  int ip = (ax == 0) ? 1 : 0;
+  for (int n = 0; n < NM; n++)
+    for (int i = i1; i <= i2; i++) {
+      wc[n][i] = w[1][n][i];
+      dm[n][i] = w[1][n][i] - w[0][n][i];
+      dp[n][i] = w[2][n][i] - w[1][n][i];
+    }
+  if (char_proj) {
+    o_prim2char_1(dm, wc, i1, i2, gam);
+    o_prim2char_1(dp, wc, i1, i2, gam);
+  }
+  for (int n = 0; n < NM; n++)
+    for (int i = i1; i <= i2; i++) {
+      real a = dm[n][i], b = dp[n][i];
+      real l = (lim == ORC_LIM_MC) ? o_mc_lim(a, b) : (lim == ORC_LIM_MM) ? o_mm_lim(a, b) : o_vl_lim(a, b);
+      d[n][i] = 0.5 * l;
+    }
+  if (char_proj) o_char2prim_1(d, wc, i1, i2, gam);
+  for (int n = 0; n < NM; n++)
+    for (int i = i1; i <= i2; i++) {
+      wr[n][i] = wc[n][i] - d[n][i];
+      wl[n][i + ip] = wc[n][i] + d[n][i];
+    }
+}
+
+void orc_reconstr_linear(real **wl, real **wr, real ***w, real ***scr, orc_coord *gc, int ax,
+                         int i1, int i2, int j, int k, int char_proj, real gam) {
+  (void)gc; (void)j; (void)k;
+  o_reconstr_linear_lim(ORC_LIM_VL, wl, wr, w, scr, ax, i1, i2, char_proj, gam);
+}
+void orc_reconstr_linear_mc(real **wl, real **wr, real ***w, real ***scr, orc_coord *gc, int ax,
+                            int i1, int i2, int j, int k, int char_proj, real gam) {
+  (void)gc; (void)j; (void)k;
+  o_reconstr_linear_lim(ORC_LIM_MC, wl, wr, w, scr, ax, i1, i2, char_proj, gam);
+}
+void orc_reconstr_linear_mm(real **wl, real **wr, real ***w, real ***scr, orc_coord *gc, int ax,
+                            int i1, int i2, int j, int k, int char_proj, real gam) {
+  (void)gc; (void)j; (void)k;
+  o_reconstr_linear_lim(ORC_LIM_MM, wl, wr, w, scr, ax, i1, i2, char_proj, gam);
+}
+
+/* ======================================================================
+ * Flat-array test entry points
+ * ====================================================================== */
+
+static orc_rsolver_fn pick_rsolver(int rs) {
+  switch (rs) {
+    case ORC_RS_HLL: return orc_hll_flux;
+    case ORC_RS_HLLT: return orc_hllt_flux;
+#if ORC_MFIELD
+    case ORC_RS_HLLD: return orc_hlld_flux;
+#else
+    case ORC_RS_HLLC: return orc_hllc_flux;
+#endif
+    default: return NULL;
+  }
+}
+
+void orc_flux_flat(int rsolver, real *flux, const real *wl, const real *wr, const real *bx,
+                   int n, real gam) {
+  real *f[NM], *l[NM], *r[NM];
+  for (int m = 0; m < NM; ++m) {
+    f[m] = flux + (size_t)m * n;
+    l[m] = (real *)wl + (size_t)m * n;
+    r[m] = (real *)wr + (size_t)m * n;
+  }
+  orc_rsolver_fn fn = pick_rsolver(rsolver);
+  if (fn) fn(f, l, r, (real *)bx, 0, n - 1, gam);
+}
+
+/* w: (NMODE, n) one row along x; wl/wr: (NMODE, n+1).  Cells 1..n-2. */
+void orc_reconstr_flat(int reconstr, int limiter, int char_proj, real *wl, real *wr,
+                       const real *w, int n, real gam) {
+  int order = reconstr == ORC_RCN_LINEAR ? 1 : 0;
+  real *wrow[3][NM];
+  real **wp[3];
+  real *wlr[NM], *wrr[NM];
+  real *scr_store = (real *)calloc((size_t)3 * NM * (n + 1), sizeof(real));
+  real *scr_rows[3][NM];
+  real **scr[3];
+  for (int d = 0; d < 3; ++d) {
+    for (int m = 0; m < NM; ++m) {
+      wrow[d][m] = (real *)w + (size_t)m * n + d - order;
+      scr_rows[d][m] = scr_store + ((size_t)d * NM + m) * (n + 1);
+    }
+    wp[d] = wrow[d];
+    scr[d] = scr_rows[d];
+  }
+  for (int m = 0; m < NM; ++m) { wlr[m] = wl + (size_t)m * (n + 1); wrr[m] = wr + (size_t)m * (n + 1); }
+  if (order == 0)
+    orc_reconstr_const(wlr, wrr, wp, scr, NULL, 0, 1, n - 2, 0, 0, char_proj, gam);
+  else
+    o_reconstr_linear_lim(limiter, wlr, wrr, wp, scr, 0, 1, n - 2, char_proj, gam);
+  free(scr_store);
+}
+
+/* ======================================================================
+ * Simulation driver
+ * ====================================================================== */
+
+struct orc_sim {
+  orc_params p;
+  orc_coord gc;
+  int nx, ny, nz;
+  size_t ncell;
+  real *prim, *cons, *bfld;
+  real *cons_s, *bfld_s;
+  real *flx[3];
+  real *ec, *ee;
+  /* diffusion scratch (thcond_elec.pyx / diffusion.pyx) */
+  real *temp, *kappa, *fxd, *fyd, *fzd, *pres0, *presm1, *dtemp, *dtemp0;
+  orc_rsolver_fn rsolver;
+  orc_reconstr_fn rc_const, rc_linear;
+  int reconstr_order;
+  real time, dt;
+  long step;
+  int last_nsts;
+  int nthr;
+  /* per-thread scratch rows (integrator.pyx:367-370) */
+  real *rowstore;
+  size_t rowlen;
+};
+
+#define IDX(s, n, k, j, i) ((((size_t)(n) * (s)->nz + (k)) * (s)->ny + (j)) * (s)->nx + (i))
+#define C3(s, k, j, i) ((((size_t)(k)) * (s)->ny + (j)) * (s)->nx + (i))
+
+static int nthreads_of(const orc_params *p) {
+#ifdef _OPENMP
+  return p->nthreads > 0 ? p->nthreads : omp_get_max_threads();
+#else
+  (void)p;
+  return 1;
+#endif
+}
+
+/* coord.pyx:122-258 (uniform axes) and cartesian.pyx:18-43. */
+static void set_coordinates(orc_sim *s) {
+  orc_coord *gc = &s->gc;
+  int ind1 = 0, ind2 = 0;
+  for (int n = 0; n < 3; ++n) {
+    int Ntot = gc->Ntot[n];
+    real *lf = gc->lf[n];
+    if (Ntot == 1) {
+      lf[0] = gc->lmin[n];
+      lf[1] = gc->lmax[n];
+    } else {
+      if (n == 0) { ind1 = gc->i1; ind2 = gc->i2; }
+      if (n == 1) { ind1 = gc->j1; ind2 = gc->j2; }
+      if (n == 2) { ind1 = gc->k1; ind2 = gc->k2; }
+      real dx = (gc->lmax[n] - gc->lmin[n]) / gc->Nact_glob[n];
+      real l1 = gc->pos[n] * gc->Nact[n] * dx;
+      for (int i = 0; i < Ntot + 1; ++i) lf[i] = l1 + (i - ind1) * dx;
+      if (s->p.bc[n][0] == ORC_BC_PERIODIC)
+        for (int i = ind1 - 1; i > -1; --i) {
+          int i_ = ind2 - i + (ind1 - 1);
+          real dlf_ = lf[i_ + 1] - lf[i_];
+          lf[i] = lf[i + 1] - dlf_;
+        }
+      if (s->p.bc[n][1] == ORC_BC_PERIODIC)
+        for (int i = ind2 + 1; i < Ntot; ++i) {
+          int i_ = ind1 + i - (ind2 + 1);
+          real dlf_ = lf[i_ + 1] - lf[i_];
+          lf[i + 1] = lf[i] + dlf_;
+        }
+      if (s->p.bc[n][0] == ORC_BC_REFLECT)
+        for (int i = ind1 - 1; i > -1; --i) {
+          int i_ = ind1 - i + (ind1 - 1);
+          real dlf_ = lf[i_ + 1] - lf[i_];
+          lf[i] = lf[i + 1] - dlf_;
+        }
+      if (s->p.bc[n][1] == ORC_BC_REFLECT)
+        for (int i = ind2 + 1; i < Ntot; ++i) {
+          int i_ = ind2 - i + (ind2 + 1);
+          real dlf_ = lf[i_ + 1] - lf[i_];
+          lf[i + 1] = lf[i] + dlf_;
+        }
+    }
+  }
+  for (int n = 0; n < 3; ++n)
+    for (int i = 0; i < gc->Ntot[n]; ++i) {
+      gc->dlf[n][i] = gc->lf[n][i + 1] - gc->lf[n][i];
+      gc->dlf_inv[n][i] = 1. / gc->dlf[n][i];
+    }
+  for (int n = 0; n < 3; ++n)
+    for (int i = 0; i < gc->Ntot[n]; ++i) gc->lv[n][i] = 0.5 * (gc->lf[n][i] + gc->lf[n][i + 1]);
+  for (int i = 0; i < gc->Ntot[0]; ++i) { gc->syxf[i] = 1.; gc->syxv[i] = 1.; gc->szxf[i] = 1.; gc->szxv[i] = 1.; }
+  for (int j = 0; j < gc->Ntot[1]; ++j) { gc->szyf[j] = 1.; gc->szyv[j] = 1.; }
+  for (int n = 0; n < 3; ++n)
+    for (int i = 1; i < gc->Ntot[n]; ++i) {
+      gc->dlv[n][i] = gc->lv[n][i] - gc->lv[n][i - 1];
+      gc->dlv_inv[n][i] = 1. / gc->dlv[n][i];
+    }
+}
+
+static real **alloc_rows(int nrow, int len) {
+  real **r = (real **)calloc(nrow, sizeof(real *));
+  for (int n = 0; n < nrow; ++n) r[n] = (real *)calloc(len, sizeof(real));
+  return r;
+}
+
+orc_sim *orc_create(const orc_params *pin) {
+  orc_sim *s = (orc_sim *)calloc(1, sizeof(orc_sim));
+  s->p = *pin;
+  orc_coord *gc = &s->gc;
+  int dims = s->p.dims;
+  int ng = (s->p.reconstr == ORC_RCN_CONST) ? 2 : 3;  /* grid.pyx:127-134 */
+  gc->ng = ng;
+  gc->interp_order = (s->p.reconstr == ORC_RCN_CONST) ? 1 : 2;
+  int Na[3] = {s->p.Nx, dims >= 2 ? s->p.Ny : 1, dims >= 3 ? s->p.Nz : 1};
+  for (int n = 0; n < 3; ++n) {
+    gc->Nact_glob[n] = Na[n];
+    gc->Nact[n] = Na[n];
+    gc->Ntot_glob[n] = (n < dims) ? Na[n] + 2 * ng : 1;
+    gc->Ntot[n] = gc->Ntot_glob[n];
+    gc->lmin[n] = s->p.lmin[n];
+    gc->lmax[n] = s->p.lmax[n];
+    gc->pos[n] = 0;
+    gc->size[n] = 1;
+  }
+  gc->size_tot = 1;
+  gc->i1 = ng; gc->i2 = Na[0] + ng - 1;
+  if (dims >= 2) { gc->j1 = ng; gc->j2 = Na[1] + ng - 1; } else { gc->j1 = gc->j2 = 0; }
+  if (dims >= 3) { gc->k1 = ng; gc->k2 = Na[2] + ng - 1; } else { gc->k1 = gc->k2 = 0; }
+  gc->geom = 0;
+  gc->scale[0] = gc->scale[1] = gc->scale[2] = 0;
+  int nmax = gc->Ntot[0];
+  if (gc->Ntot[1] > nmax) nmax = gc->Ntot[1];
+  if (gc->Ntot[2] > nmax) nmax = gc->Ntot[2];
+  gc->lf = alloc_rows(3, nmax + 1);
+  gc->lv = alloc_rows(3, nmax + 1);
+  gc->dlf = alloc_rows(3, nmax + 1);
+  gc->dlv = alloc_rows(3, nmax + 1);
+  gc->dlf_inv = alloc_rows(3, nmax + 1);
+  gc->dlv_inv = alloc_rows(3, nmax + 1);
+  gc->syxf = (real *)calloc(nmax + 1, sizeof(real));
+  gc->syxv = (real *)calloc(nmax + 1, sizeof(real));
+  gc->szxf = (real *)calloc(nmax + 1, sizeof(real));
+  gc->szxv = (real *)calloc(nmax + 1, sizeof(real));
+  gc->szyf = (real *)calloc(nmax + 1, sizeof(real));
+  gc->szyv = (real *)calloc(nmax + 1, sizeof(real));
+  set_coordinates(s);
+
+  s->nx = gc->Ntot[0];
+  s->ny = gc->Ntot[1];
+  s->nz = gc->Ntot[2];
+  s->ncell = (size_t)s->nx * s->ny * s->nz;
+  s->prim = (real *)calloc(NM * s->ncell, sizeof(real));
+  s->cons = (real *)calloc(NM * s->ncell, sizeof(real));
+  s->cons_s = (real *)calloc(NM * s->ncell, sizeof(real));
+  for (int d = 0; d < 3; ++d) s->flx[d] = (real *)calloc(NM * s->ncell, sizeof(real));
+#if ORC_MFIELD
+  s->bfld = (real *)calloc(3 * s->ncell, sizeof(real));
+  s->bfld_s = (real *)calloc(3 * s->ncell, sizeof(real));
+  s->ec = (real *)calloc(3 * s->ncell, sizeof(real));
+  s->ee = (real *)calloc(3 * s->ncell, sizeof(real));
+#endif
+  if (s->p.kappa0 != 0.) {
+    s->temp = (real *)calloc(s->ncell, sizeof(real));
+    s->kappa = (real *)calloc(s->ncell, sizeof(real));
+    s->fxd = (real *)calloc(s->ncell, sizeof(real));
+    s->fyd = (real *)calloc(s->ncell, sizeof(real));
+    s->fzd = (real *)calloc(s->ncell, sizeof(real));
+    s->pres0 = (real *)calloc(s->ncell, sizeof(real));
+    s->presm1 = (real *)calloc(s->ncell, sizeof(real));
+    s->dtemp = (real *)calloc(s->ncell, sizeof(real));
+    s->dtemp0 = (real *)calloc(s->ncell, sizeof(real));
+  }
+  s->rsolver = pick_rsolver(s->p.rsolver);
+  if (!s->rsolver) s->rsolver = orc_hll_flux; /* integrator.pyx:233 default */
+  s->rc_const = orc_reconstr_const;
+  s->rc_linear = (s->p.limiter == ORC_LIM_MC)   ? orc_reconstr_linear_mc
+                 : (s->p.limiter == ORC_LIM_MM) ? orc_reconstr_linear_mm
+                                                : orc_reconstr_linear;
+  s->reconstr_order = (s->p.reconstr == ORC_RCN_CONST) ? 0 : 1;
+  s->nthr = nthreads_of(&s->p);
+  /* per thread: wl, wl_, wr (NM rows each) + 8*NM reconstruction rows */
+  s->rowlen = (size_t)nmax + 4;
+  s->rowstore = (real *)calloc((size_t)s->nthr * 11 * NM * s->rowlen, sizeof(real));
+  return s;
+}
+
+void orc_destroy(orc_sim *s) {
+  if (!s) return;
+  orc_coord *gc = &s->gc;
+  real **rr[6] = {gc->lf, gc->lv, gc->dlf, gc->dlv, gc->dlf_inv, gc->dlv_inv};
+  for (int a = 0; a < 6; ++a) {
+    for (int n = 0; n < 3; ++n) free(rr[a][n]);
+    free(rr[a]);
+  }
+  free(gc->syxf); free(gc->syxv); free(gc->szxf); free(gc->szxv); free(gc->szyf); free(gc->szyv);
+  free(s->prim); free(s->cons); free(s->cons_s);
+  for (int d = 0; d < 3; ++d) free(s->flx[d]);
+  free(s->bfld); free(s->bfld_s); free(s->ec); free(s->ee);
+  free(s->temp); free(s->kappa); free(s->fxd); free(s->fyd); free(s->fzd);
+  free(s->pres0); free(s->presm1); free(s->dtemp); free(s->dtemp0);
+  free(s->rowstore);
+  free(s);
+}
+
+int orc_ntot(const orc_sim *s, int ax) { return s->gc.Ntot[ax]; }
+int orc_ng(const orc_sim *s) { return s->gc.ng; }
+void orc_get_coord(const orc_sim *s, int ax, real *lf, real *lv, real *dlf) {
+  int N = s->gc.Ntot[ax];
+  if (lf) memcpy(lf, s->gc.lf[ax], (N + 1) * sizeof(real));
+  if (lv) memcpy(lv, s->gc.lv[ax], N * sizeof(real));
+  if (dlf) memcpy(dlf, s->gc.dlf[ax], N * sizeof(real));
+}
+
+void orc_set_kernels(orc_sim *s, orc_rsolver_fn rs, orc_reconstr_fn rc_const, orc_reconstr_fn rc_linear) {
+  if (rs) s->rsolver = rs;
+  if (rc_const) s->rc_const = rc_const;
+  if (rc_linear) s->rc_linear = rc_linear;
+}
+
+void orc_set_state(orc_sim *s, const real *prim, const real *bfld) {
+  memcpy(s->prim, prim, NM * s->ncell * sizeof(real));
+#if ORC_MFIELD
+  if (bfld) memcpy(s->bfld, bfld, 3 * s->ncell * sizeof(real));
+#else
+  (void)bfld;
+#endif
+}
+
+void orc_get_state(const orc_sim *s, real *prim, real *cons, real *bfld) {
+  if (prim) memcpy(prim, s->prim, NM * s->ncell * sizeof(real));
+  if (cons) memcpy(cons, s->cons, NM * s->ncell * sizeof(real));
+#if ORC_MFIELD
+  if (bfld) memcpy(bfld, s->bfld, 3 * s->ncell * sizeof(real));
+#else
+  (void)bfld;
+#endif
+}
+
+real orc_time(const orc_sim *s) { return s->time; }
+long orc_step_count(const orc_sim *s) { return s->step; }
+real orc_last_dt(const orc_sim *s) { return s->dt; }
+int orc_last_nsts(const orc_sim *s) { return s->last_nsts; }
+
+/* ---------------------------------------------------------------------
+ * Boundary conditions: grid_bc.pyx:612-623, grid_bc_funcs.pyx:36-330,
+ * util_bc.pyx:9-251.  Field index f: 0..NM-1 prim, NM..NM+2 face B.
+ * ------------------------------------------------------------------- */
+
+static real *bc_field(orc_sim *s, int f) {
+  if (f < NM) return s->prim + (size_t)f * s->ncell;
+  return s->bfld + (size_t)(f - NM) * s->ncell;
+}
+
+/* A[dst + g] = A[src + g] along axis ax (util_bc.pyx:9-43). */
+static void copy_layer(orc_sim *s, real *A, int ax, int dst, int src, int width) {
+  int N[3] = {s->nx, s->ny, s->nz};
+  for (int k = 0; k < N[2]; ++k)
+    for (int j = 0; j < N[1]; ++j)
+      for (int i = 0; i < N[0]; ++i) {
+        int c[3] = {i, j, k};
+        int g = c[ax] - dst;
+        if (g < 0 || g >= width) continue;
+        int cs[3] = {i, j, k};
+        cs[ax] = src + g;
+        A[C3(s, k, j, i)] = A[C3(s, cs[2], cs[1], cs[0])];
+      }
+}
+
+/* prolong_*: LR=0 to the left, LR=1 to the right (util_bc.pyx:208-251). */
+static void prolong(orc_sim *s, real *A, int ax, int LR, int b0, int width) {
+  int b01 = b0 + 1 - 2 * LR;
+  int b1 = b01 - (1 - LR) * width + LR;
+  int N[3] = {s->nx, s->ny, s->nz};
+  for (int k = 0; k < N[2]; ++k)
+    for (int j = 0; j < N[1]; ++j)
+      for (int i = 0; i < N[0]; ++i) {
+        int c[3] = {i, j, k};
+        int g = c[ax] - b1;
+        if (g < 0 || g >= width) continue;
+        int cs[3] = {i, j, k};
+        cs[ax] = b01;
+        A[C3(s, k, j, i)] = A[C3(s, cs[2], cs[1], cs[0])];
+      }
+}
+
+/* copy_reflect_layer_*: A[b+width-1-g] = sgn*A[b0+g] (util_bc.pyx:48-85). */
+static void copy_reflect(orc_sim *s, real *A, int ax, real sgn, int b, int b0, int width) {
+  int b1 = b + width - 1;
+  int N[3] = {s->nx, s->ny, s->nz};
+  for (int k = 0; k < N[2]; ++k)
+    for (int j = 0; j < N[1]; ++j)
+      for (int i = 0; i < N[0]; ++i) {
+        int c[3] = {i, j, k};
+        int g = b1 - c[ax];
+        if (g < 0 || g >= width) continue;
+        int cs[3] = {i, j, k};
+        cs[ax] = b0 + g;
+        A[C3(s, k, j, i)] = sgn * A[C3(s, cs[2], cs[1], cs[0])];
+      }
+}
+
+static void set_layer(orc_sim *s, real *A, int ax, real v, int b, int width) {
+  int N[3] = {s->nx, s->ny, s->nz};
+  for (int k = 0; k < N[2]; ++k)
+    for (int j = 0; j < N[1]; ++j)
+      for (int i = 0; i < N[0]; ++i) {
+        int c[3] = {i, j, k};
+        int g = c[ax] - b;
+        if (g < 0 || g >= width) continue;
+        A[C3(s, k, j, i)] = v;
+      }
+}
+
+static void bc_side(orc_sim *s, int ax, int side, int f) {
+  orc_coord *gc = &s->gc;
+  int ng = gc->ng;
+  int a1 = ax == 0 ? gc->i1 : ax == 1 ? gc->j1 : gc->k1;
+  int a2 = ax == 0 ? gc->i2 : ax == 1 ? gc->j2 : gc->k2;
+  int flag = s->p.bc[ax][side];
+  real *A = bc_field(s, f);
+  int is_face_normal = (f >= NM) && (f - NM == ax);
+  if (flag == ORC_BC_PERIODIC) {
+    if (side == 0) copy_layer(s, A, ax, a1 - ng, a2 - ng + 1, ng);
+    else copy_layer(s, A, ax, a2 + 1, a1, ng);
+  } else if (flag == ORC_BC_OUTFLOW) {
+    if (side == 0) prolong(s, A, ax, 0, a1 - 1, ng);
+    else if (is_face_normal && s->p.outflow_face_aware) prolong(s, A, ax, 1, a2 + 2, ng - 1);
+    else prolong(s, A, ax, 1, a2 + 1, ng);
+  } else if (flag == ORC_BC_REFLECT) {
+#if ORC_MFIELD
+    int is_normal_cell = (f == VX + ax) || (f == BX + ax);
+#else
+    int is_normal_cell = (f == VX + ax);
+#endif
+    if (side == 0) {
+      if (is_normal_cell) copy_reflect(s, A, ax, -1., a1 - ng, a1, ng);
+      else if (is_face_normal) { set_layer(s, A, ax, 0., a1, 1); copy_reflect(s, A, ax, -1., a1 - ng, a1 + 1, ng); }
+      else copy_reflect(s, A, ax, 1., a1 - ng, a1, ng);
+    } else {
+      if (is_normal_cell) copy_reflect(s, A, ax, -1., a2 + 1, a2 - ng + 1, ng);
+      else if (is_face_normal) { set_layer(s, A, ax, 0., a2 + 1, 1); copy_reflect(s, A, ax, -1., a2 + 2, a2 - ng + 2, ng - 1); }
+      else copy_reflect(s, A, ax, 1., a2 + 1, a2 - ng + 1, ng);
+    }
+  }
+}
+
+/* apply_bc non-MPI branch: z, then y, then x (grid_bc.pyx:612-623). */
+void orc_apply_bc(orc_sim *s, uint32_t var_mask) {
+  int dims = s->p.dims;
+  for (int ax = 2; ax >= 0; --ax) {
+    if (ax >= dims) continue;
+    for (int side = 0; side < 2; ++side)
+      for (int f = 0; f < ORC_NVAR; ++f)
+        if (var_mask & (1u << f)) bc_side(s, ax, side, f);
+  }
+}
+
+/* ---------------------------------------------------------------------
+ * EOS over index ranges (eos.pyx:13-78)
+ * ------------------------------------------------------------------- */
+static void cons2prim_range(orc_sim *s, real *w, const real *u, const int *lims) {
+  real gam = s->p.gam;
+#pragma omp parallel for collapse(2) num_threads(s->nthr) schedule(static)
+  for (int k = lims[4]; k <= lims[5]; ++k)
+    for (int j = lims[2]; j <= lims[3]; ++j) {
+      real uu[NM], ww[NM];
+      for (int i = lims[0]; i <= lims[1]; ++i) {
+        for (int n = 0; n < NM; ++n) uu[n] = u[IDX(s, n, k, j, i)];
+        o_cons2prim(ww, uu, gam);
+        for (int n = 0; n < NM; ++n) w[IDX(s, n, k, j, i)] = ww[n];
+      }
+    }
+}
+
+static void prim2cons_range(orc_sim *s, real *u, const real *w, const int *lims) {
+  real gam = s->p.gam;
+#pragma omp parallel for collapse(2) num_threads(s->nthr) schedule(static)
+  for (int k = lims[4]; k <= lims[5]; ++k)
+    for (int j = lims[2]; j <= lims[3]; ++j) {
+      real uu[NM], ww[NM];
+      for (int i = lims[0]; i <= lims[1]; ++i) {
+        for (int n = 0; n < NM; ++n) ww[n] = w[IDX(s, n, k, j, i)];
+        o_prim2cons(uu, ww, gam);
+        for (int n = 0; n < NM; ++n) u[IDX(s, n, k, j, i)] = uu[n];
+      }
+    }
+}
+
+/* integrator.pyx:375-383 */
+static void integr_lims(const orc_sim *s, int order, int *lims) {
+  const int *Nt = s->gc.Ntot;
+  for (int a = 0; a < 3; ++a) {
+    lims[2 * a] = order + 1;
+    lims[2 * a + 1] = Nt[a] - 2 - order;
+  }
+  if (s->p.dims < 2) lims[2] = lims[3] = 0;
+  if (s->p.dims < 3) lims[4] = lims[5] = 0;
+}
+
+/* godunov.pyx:297-324 */
+static void swap_mhd_vec(int ax, int *vars) {
+  for (int n = 0; n < NM; ++n) vars[n] = n;
+  if (ax == 1) {
+    vars[VX] = VY; vars[VY] = VZ; vars[VZ] = VX;
+#if ORC_MFIELD
+    vars[BX] = BY; vars[BY] = BZ; vars[BZ] = BX;
+#endif
+  } else if (ax == 2) {
+    vars[VX] = VZ; vars[VY] = VX; vars[VZ] = VY;
+#if ORC_MFIELD
+    vars[BX] = BZ; vars[BY] = BX; vars[BZ] = BY;
+#endif
+  }
+}
+
+typedef struct {
+  real *wl[NM], *wl_[NM], *wr[NM];
+  real *rc[8][NM];
+  real **rcp[8];
+} row_scratch;
+
+static void thread_rows(orc_sim *s, int tid, row_scratch *r) {
+  real *base = s->rowstore + (size_t)tid * 11 * NM * s->rowlen;
+  for (int n = 0; n < NM; ++n) {
+    r->wl[n] = base + (size_t)(0 * NM + n) * s->rowlen;
+    r->wl_[n] = base + (size_t)(1 * NM + n) * s->rowlen;
+    r->wr[n] = base + (size_t)(2 * NM + n) * s->rowlen;
+    for (int d = 0; d < 8; ++d) r->rc[d][n] = base + (size_t)((3 + d) * NM + n) * s->rowlen;
+  }
+  for (int d = 0; d < 8; ++d) r->rcp[d] = r->rc[d];
+}
+
+static int thread_id(void) {
+#ifdef _OPENMP
+  return omp_get_thread_num();
+#else
+  return 0;
+#endif
+}
+
+/* One y or z column sweep over x-range [ib, ie] (godunov.pyx:132-160, :179-204). */
+static void sweep_transverse(orc_sim *s, int ax, const int *vars, real *prim, real *bfld, int order,
+                             orc_reconstr_fn rf, int fixed, int a_lo, int a_hi, int ib, int ie,
+                             row_scratch *r) {
+  real *prim1_rows[5][NM];
+  real **prim1[5];
+  real *flx1[NM];
+  real **wl = r->wl, **wl_ = r->wl_, **wr = r->wr;
+  for (int d = 0; d < 2 * order + 1; ++d) prim1[d] = prim1_rows[d];
+  /* first row (the left state of face a_lo) */
+  for (int d = 0; d < 2 * order + 1; ++d)
+    for (int n = 0; n < NM; ++n) {
+      int a = a_lo - 1 + d - order;
+      prim1_rows[d][n] = ax == 1 ? &prim[IDX(s, vars[n], fixed, a, 0)] : &prim[IDX(s, vars[n], a, fixed, 0)];
+    }
+  rf(wl, wr, prim1, r->rcp, &s->gc, ax, ib, ie, ax == 1 ? a_lo - 1 : fixed, ax == 1 ? fixed : a_lo - 1,
+     s->p.charact_proj, s->p.gam);
+  for (int a0 = a_lo; a0 <= a_hi; ++a0) {
+    for (int d = 0; d < 2 * order + 1; ++d)
+      for (int n = 0; n < NM; ++n) {
+        int a = a0 + d - order;
+        prim1_rows[d][n] = ax == 1 ? &prim[IDX(s, vars[n], fixed, a, 0)] : &prim[IDX(s, vars[n], a, fixed, 0)];
+      }
+    rf(wl_, wr, prim1, r->rcp, &s->gc, ax, ib, ie, ax == 1 ? a0 : fixed, ax == 1 ? fixed : a0,
+       s->p.charact_proj, s->p.gam);
+    real *F = s->flx[ax];
+    for (int n = 0; n < NM; ++n)
+      flx1[n] = ax == 1 ? &F[IDX(s, vars[n], fixed, a0, 0)] : &F[IDX(s, vars[n], a0, fixed, 0)];
+    real *b1 = NULL;
+#if ORC_MFIELD
+    b1 = ax == 1 ? &bfld[IDX(s, 1, fixed, a0, 0)] : &bfld[IDX(s, 2, a0, fixed, 0)];
+#else
+    (void)bfld;
+#endif
+    s->rsolver(flx1, wl, wr, b1, ib, ie, s->p.gam);
+    /* the intended roll of the left state (D10) */
+    real **t = wl; wl = wl_; wl_ = t;
+  }
+}
+
+/* godunov.pyx:20-209 */
+static void godunov_fluxes(orc_sim *s, real *prim, real *bfld, const int *lims, int order) {
+  orc_reconstr_fn rf = order == 0 ? s->rc_const : s->rc_linear;
+  int il = lims[0], iu = lims[1], jl = lims[2], ju = lims[3], kl = lims[4], ku = lims[5];
+  int dims = s->p.dims;
+  int varsx[NM], varsy[NM], varsz[NM];
+  swap_mhd_vec(0, varsx);
+  swap_mhd_vec(1, varsy);
+  swap_mhd_vec(2, varsz);
+  int nthr = s->nthr;
+
+  /* x sweep (godunov.pyx:84-112) */
+  {
+    int kb = kl - 1, ke = ku + 1, jb = jl - 1, je = ju + 1;
+    if (dims < 2) { jb = 0; je = 0; }
+    if (dims < 3) { kb = 0; ke = 0; }
+    int nj = je - jb + 1, nk = ke - kb + 1;
+    int nrows = nj * nk;
+    int par_rows = s->p.rows_parallel ? nrows : nk;
+#pragma omp parallel num_threads(nthr)
+    {
+      row_scratch r;
+      thread_rows(s, thread_id(), &r);
+      real *prim1_rows[5][NM];
+      real **prim1[5];
+      real *flx1[NM];
+      for (int d = 0; d < 5; ++d) prim1[d] = prim1_rows[d];
+#pragma omp for schedule(dynamic)
+      for (int q = 0; q < par_rows; ++q) {
+        int qlo = s->p.rows_parallel ? q : q * nj;
+        int qhi = s->p.rows_parallel ? q : q * nj + nj - 1;
+        for (int qq = qlo; qq <= qhi; ++qq) {
+          int k = kb + qq / nj, j = jb + qq % nj;
+          for (int d = 0; d < 2 * order + 1; ++d)
+            for (int n = 0; n < NM; ++n) prim1_rows[d][n] = &prim[IDX(s, varsx[n], k, j, 0)] + d - order;
+          rf(r.wl, r.wr, prim1, r.rcp, &s->gc, 0, il - 1, iu + 1, j, k, s->p.charact_proj, s->p.gam);
+          for (int n = 0; n < NM; ++n) flx1[n] = &s->flx[0][IDX(s, varsx[n], k, j, 0)];
+          real *b1 = NULL;
+#if ORC_MFIELD
+          b1 = &bfld[IDX(s, 0, k, j, 0)];
+#endif
+          s->rsolver(flx1, r.wl, r.wr, b1, il, iu + 1, s->p.gam);
+        }
+      }
+    }
+  }
+
+  /* y sweep (godunov.pyx:118-160) */
+  if (dims >= 2) {
+    int ib = il - 1, ie = iu + 1;
+    int kb = kl - 1, ke = ku + 1;
+    if (dims < 3) { kb = 0; ke = 0; }
+    int nk = ke - kb + 1;
+    int nchunk = (s->p.rows_parallel && nk < nthr) ? nthr : 1;
+    int nitem = nk * nchunk;
+#pragma omp parallel num_threads(nthr)
+    {
+      row_scratch r;
+      thread_rows(s, thread_id(), &r);
+#pragma omp for schedule(dynamic)
+      for (int q = 0; q < nitem; ++q) {
+        int k = kb + q / nchunk, c = q % nchunk;
+        int len = ie - ib + 1;
+        int lo = ib + (int)((long)len * c / nchunk), hi = ib + (int)((long)len * (c + 1) / nchunk) - 1;
+        if (hi < lo) continue;
+        sweep_transverse(s, 1, varsy, prim, bfld, order, rf, k, jl, ju + 1, lo, hi, &r);
+      }
+    }
+  }
+
+  /* z sweep (godunov.pyx:166-204) */
+  if (dims >= 3) {
+    int ib = il - 1, ie = iu + 1;
+    int jb = jl - 1, je = ju + 1;
+    int nj = je - jb + 1;
+#pragma omp parallel num_threads(nthr)
+    {
+      row_scratch r;
+      thread_rows(s, thread_id(), &r);
+#pragma omp for schedule(dynamic)
+      for (int q = 0; q < nj; ++q) {
+        int j = jb + q;
+        sweep_transverse(s, 2, varsz, prim, bfld, order, rf, j, kl, ku + 1, ib, ie, &r);
+      }
+    }
+  }
+}
+
+/* godunov.pyx:215-252 (Cartesian metric, cartesian.pyx:97-115). */
+static void advance_hydro(orc_sim *s, real *u1, const real *u0, const int *lims, real dt) {
+  orc_coord *gc = &s->gc;
+  int dims = s->p.dims;
+#if ORC_MFIELD
+  int nvh = NM - 3;
+#else
+  int nvh = NM;
+#endif
+  real *fx = s->flx[0], *fy = s->flx[1], *fz = s->flx[2];
+#pragma omp parallel for collapse(3) num_threads(s->nthr) schedule(static)
+  for (int n = 0; n < nvh; ++n)
+    for (int k = lims[4]; k <= lims[5]; ++k)
+      for (int j = lims[2]; j <= lims[3]; ++j)
+        for (int i = lims[0]; i <= lims[1]; ++i) {
+          real vol = gc->dlf[0][i] * gc->dlf[1][j] * gc->dlf[2][k];
+          real dtdv = dt / vol;
+          real dam = gc->dlf[1][j] * gc->dlf[2][k];
+          real dap = gc->dlf[1][j] * gc->dlf[2][k];
+          real v = u0[IDX(s, n, k, j, i)] - dtdv * (dap * fx[IDX(s, n, k, j, i + 1)] - dam * fx[IDX(s, n, k, j, i)]);
+          if (dims >= 2) {
+            dam = gc->dlf[0][i] * gc->dlf[2][k];
+            dap = gc->dlf[0][i] * gc->dlf[2][k];
+            v -= dtdv * (dap * fy[IDX(s, n, k, j + 1, i)] - dam * fy[IDX(s, n, k, j, i)]);
+          }
+          if (dims >= 3) {
+            dam = gc->dlf[0][i] * gc->dlf[1][j];
+            dap = gc->dlf[0][i] * gc->dlf[1][j];
+            v -= dtdv * (dap * fz[IDX(s, n, k + 1, j, i)] - dam * fz[IDX(s, n, k, j, i)]);
+          }
+          u1[IDX(s, n, k, j, i)] = v;
+        }
+}
+
+#if ORC_MFIELD
+/* ct.pyx:128-148 */
+static void ec_from_prim(orc_sim *s, const real *w, const int *lims) {
+  int il = lims[0] - 1, iu = lims[1] + 1, jl = lims[2] - 1, ju = lims[3] + 1, kl = lims[4] - 1, ku = lims[5] + 1;
+  if (s->p.dims < 2) { jl = 0; ju = 0; }
+  if (s->p.dims < 3) { kl = 0; ku = 0; }
+  real *ec = s->ec;
+#pragma omp parallel for collapse(2) num_threads(s->nthr) schedule(static)
+  for (int k = kl; k <= ku; ++k)
+    for (int j = jl; j <= ju; ++j)
+      for (int i = il; i <= iu; ++i) {
+        real vx = w[IDX(s, VX, k, j, i)], vy = w[IDX(s, VY, k, j, i)], vz = w[IDX(s, VZ, k, j, i)];
+        real bx = w[IDX(s, BX, k, j, i)], by = w[IDX(s, BY, k, j, i)], bz = w[IDX(s, BZ, k, j, i)];
+        ec[IDX(s, 0, k, j, i)] = -(vy * bz - vz * by);
+        ec[IDX(s, 1, k, j, i)] = (vx * bz - vz * bx);
+        ec[IDX(s, 2, k, j, i)] = -(vx * by - vy * bx);
+      }
+}
+
+/* ct.pyx:153-215 (interp_ee1: Gardiner & Stone 2005 simple average). */
+static void interp_ee1(orc_sim *s, const int *lims) {
+  int il = lims[0], iu = lims[1] + 1, jl = lims[2], ju = lims[3] + 1, kl = lims[4], ku = lims[5] + 1;
+  int dims = s->p.dims;
+  if (dims < 2) { jl = 0; ju = 0; }
+  if (dims < 3) { kl = 0; ku = 0; }
+  real *ee = s->ee, *ec = s->ec, *fx = s->flx[0], *fy = s->flx[1], *fz = s->flx[2];
+#define E(c, k, j, i) ec[IDX(s, c, k, j, i)]
+  if (dims == 3) {
+#pragma omp parallel for collapse(2) num_threads(s->nthr) schedule(static)
+    for (int k = kl; k <= ku; ++k)
+      for (int j = jl; j <= ju; ++j)
+        for (int i = il; i <= iu; ++i) {
+          ee[IDX(s, 0, k, j, i)] =
+              (0.5 * (-fy[IDX(s, BZ, k - 1, j, i)] - fy[IDX(s, BZ, k, j, i)] + fz[IDX(s, BY, k, j - 1, i)] +
+                      fz[IDX(s, BY, k, j, i)]) -
+               0.25 * (E(0, k, j - 1, i) + E(0, k, j, i) + E(0, k - 1, j - 1, i) + E(0, k - 1, j, i)));
+          ee[IDX(s, 1, k, j, i)] =
+              (0.5 * (-fz[IDX(s, BX, k, j, i - 1)] - fz[IDX(s, BX, k, j, i)] + fx[IDX(s, BZ, k - 1, j, i)] +
+                      fx[IDX(s, BZ, k, j, i)]) -
+               0.25 * (E(1, k, j, i - 1) + E(1, k, j, i) + E(1, k - 1, j, i - 1) + E(1, k - 1, j, i)));
+          ee[IDX(s, 2, k, j, i)] =
+              (0.5 * (-fx[IDX(s, BY, k, j - 1, i)] - fx[IDX(s, BY, k, j, i)] + fy[IDX(s, BX, k, j, i - 1)] +
+                      fy[IDX(s, BX, k, j, i)]) -
+               0.25 * (E(2, k, j, i - 1) + E(2, k, j, i) + E(2, k, j - 1, i - 1) + E(2, k, j - 1, i)));
+        }
+  } else if (dims == 2) {
+#pragma omp parallel for num_threads(s->nthr) schedule(static)
+    for (int j = jl; j <= ju; ++j)
+      for (int i = il; i <= iu; ++i) {
+        ee[IDX(s, 0, 0, j, i)] = -fy[IDX(s, BZ, 0, j, i)];
+        ee[IDX(s, 1, 0, j, i)] = fx[IDX(s, BZ, 0, j, i)];
+        ee[IDX(s, 2, 0, j, i)] =
+            (0.5 * (-fx[IDX(s, BY, 0, j - 1, i)] - fx[IDX(s, BY, 0, j, i)] + fy[IDX(s, BX, 0, j, i - 1)] +
+                    fy[IDX(s, BX, 0, j, i)]) -
+             0.25 * (E(2, 0, j, i - 1) + E(2, 0, j, i) + E(2, 0, j - 1, i - 1) + E(2, 0, j - 1, i)));
+      }
+  } else {
+    for (int i = il; i <= iu; ++i) {
+      ee[IDX(s, 0, 0, 0, i)] = -E(0, 0, 0, i);
+      ee[IDX(s, 1, 0, 0, i)] = fx[IDX(s, BZ, 0, 0, i)];
+      ee[IDX(s, 2, 0, 0, i)] = -fx[IDX(s, BY, 0, 0, i)];
+    }
+  }
+#undef E
+}
+
+/* ct.pyx:15-91 (Cartesian edge lengths / face areas, cartesian.pyx:57-109). */
+static void advance_b(orc_sim *s, real *b1, const real *b0, const int *lims, real dt) {
+  orc_coord *gc = &s->gc;
+  int dims = s->p.dims;
+  real *ee = s->ee;
+  real **dlf = gc->dlf;
+#pragma omp parallel for collapse(2) num_threads(s->nthr) schedule(static)
+  for (int k = lims[4]; k <= lims[5]; ++k)
+    for (int j = lims[2]; j <= lims[3]; ++j)
+      for (int i = lims[0]; i <= lims[1] + 1; ++i) {
+        real dtda = dt / (dlf[1][j] * dlf[2][k]);
+        real v = b0[IDX(s, 0, k, j, i)];
+        if (dims >= 2) {
+          real dsm = dlf[2][k], dsp = dlf[2][k];
+          v -= dtda * (dsp * ee[IDX(s, 2, k, j + 1, i)] - dsm * ee[IDX(s, 2, k, j, i)]);
+        }
+        if (dims >= 3) {
+          real dsm = dlf[1][j], dsp = dlf[1][j];
+          v += dtda * (dsp * ee[IDX(s, 1, k + 1, j, i)] - dsm * ee[IDX(s, 1, k, j, i)]);
+        }
+        b1[IDX(s, 0, k, j, i)] = v;
+      }
+  /* y faces: j up to lims[3]+1 like the x and z loops (D26; ct.pyx:48 stops
+     at lims[3], leaving the top predictor face stale) */
+  int jy_hi = dims >= 2 ? lims[3] + 1 : lims[3];
+#pragma omp parallel for collapse(2) num_threads(s->nthr) schedule(static)
+  for (int k = lims[4]; k <= lims[5]; ++k)
+    for (int j = lims[2]; j <= jy_hi; ++j)
+      for (int i = lims[0]; i <= lims[1]; ++i) {
+        real dtda = dt / (dlf[0][i] * dlf[2][k]);
+        real dsm = dlf[2][k], dsp = dlf[2][k];
+        real v = b0[IDX(s, 1, k, j, i)] + dtda * (dsp * ee[IDX(s, 2, k, j, i + 1)] - dsm * ee[IDX(s, 2, k, j, i)]);
+        if (dims >= 3) {
+          dsm = dlf[0][i]; dsp = dlf[0][i];
+          v -= dtda * (dsp * ee[IDX(s, 0, k + 1, j, i)] - dsm * ee[IDX(s, 0, k, j, i)]);
+        }
+        b1[IDX(s, 1, k, j, i)] = v;
+      }
+  int kz_hi = dims >= 3 ? lims[5] + 1 : lims[5]; /* D12 */
+#pragma omp parallel for collapse(2) num_threads(s->nthr) schedule(static)
+  for (int k = lims[4]; k <= kz_hi; ++k)
+    for (int j = lims[2]; j <= lims[3]; ++j)
+      for (int i = lims[0]; i <= lims[1]; ++i) {
+        real dtda = dt / (dlf[0][i] * dlf[1][j]);
+        real dsm = dlf[1][j], dsp = dlf[1][j];
+        real v = b0[IDX(s, 2, k, j, i)] - dtda * (dsp * ee[IDX(s, 1, k, j, i + 1)] - dsm * ee[IDX(s, 1, k, j, i)]);
+        if (dims >= 2) {
+          dsm = dlf[0][i]; dsp = dlf[0][i];
+          v += dtda * (dsp * ee[IDX(s, 0, k, j + 1, i)] - dsm * ee[IDX(s, 0, k, j, i)]);
+        }
+        b1[IDX(s, 2, k, j, i)] = v;
+      }
+}
+
+/* ct.pyx:96-123 */
+static void interp_bc(orc_sim *s, real *u, const real *b, const int *lims) {
+  orc_coord *gc = &s->gc;
+  int dims = s->p.dims;
+#pragma omp parallel for collapse(2) num_threads(s->nthr) schedule(static)
+  for (int k = lims[4]; k <= lims[5]; ++k)
+    for (int j = lims[2]; j <= lims[3]; ++j)
+      for (int i = lims[0]; i <= lims[1]; ++i) {
+        u[IDX(s, BX, k, j, i)] = ((gc->lv[0][i] - gc->lf[0][i]) * b[IDX(s, 0, k, j, i)] +
+                                  (gc->lf[0][i + 1] - gc->lv[0][i]) * b[IDX(s, 0, k, j, i + 1)]) *
+                                 gc->dlf_inv[0][i];
+        if (dims >= 2)
+          u[IDX(s, BY, k, j, i)] = ((gc->lv[1][j] - gc->lf[1][j]) * b[IDX(s, 1, k, j, i)] +
+                                    (gc->lf[1][j + 1] - gc->lv[1][j]) * b[IDX(s, 1, k, j + 1, i)]) *
+                                   gc->dlf_inv[1][j];
+        else
+          u[IDX(s, BY, k, j, i)] = b[IDX(s, 1, k, j, i)];
+        if (dims >= 3)
+          u[IDX(s, BZ, k, j, i)] = ((gc->lv[2][k] - gc->lf[2][k]) * b[IDX(s, 2, k, j, i)] +
+                                    (gc->lf[2][k + 1] - gc->lv[2][k]) * b[IDX(s, 2, k + 1, j, i)]) *
+                                   gc->dlf_inv[2][k];
+        else
+          u[IDX(s, BZ, k, j, i)] = b[IDX(s, 2, k, j, i)];
+      }
+}
+
+/* integrator.pyx:85-126 */
+static void integrate_field(orc_sim *s, real *cons1, real *bf1, const real *prim0, const real *bf0,
+                            int order, real dt) {
+  int lims[6];
+  integr_lims(s, order, lims);
+  ec_from_prim(s, prim0, lims);
+  interp_ee1(s, lims);
+  advance_b(s, bf1, bf0, lims, dt);
+  interp_bc(s, cons1, bf1, lims);
+}
+#endif
+
+/* integrator.pyx:51-79 */
+static void integrate_hydro(orc_sim *s, real *cons1, const real *cons0, real *prim0, real *bf0,
+                            int order, real dt) {
+  int lims[6];
+  integr_lims(s, order, lims);
+  godunov_fluxes(s, prim0, bf0, lims, order);
+  advance_hydro(s, cons1, cons0, lims, dt);
+}
+
+static void all_lims(const orc_sim *s, int *lims) {
+  lims[0] = 0; lims[1] = s->gc.Ntot[0] - 1;
+  lims[2] = 0; lims[3] = s->gc.Ntot[1] - 1;
+  lims[4] = 0; lims[5] = s->gc.Ntot[2] - 1;
+}
+
+void orc_init(orc_sim *s) {
+  /* vanleer.pyx:41-48 */
+  orc_apply_bc(s, (1u << ORC_NVAR) - 1u);
+#if ORC_MFIELD
+  int lims_act[6] = {s->gc.i1, s->gc.i2, s->gc.j1, s->gc.j2, s->gc.k1, s->gc.k2};
+  interp_bc(s, s->prim, s->bfld, lims_act);
+  orc_apply_bc(s, (1u << BX) | (1u << BY) | (1u << BZ));
+#endif
+  int lt[6];
+  all_lims(s, lt);
+  prim2cons_range(s, s->cons, s->prim, lt);
+  s->time = 0.;
+  s->step = 0;
+}
+
+/* new_dt.pyx:18-135 */
+real orc_new_dt(orc_sim *s) {
+  orc_coord *gc = &s->gc;
+  int dims = s->p.dims;
+  real gam = s->p.gam;
+  real cdsmax = 0.;
+  int nk = gc->k2 - gc->k1 + 1;
+  real *loc = (real *)calloc(s->nthr, sizeof(real));
+#pragma omp parallel num_threads(s->nthr)
+  {
+    int id = thread_id();
+    real w[NM];
+#pragma omp for schedule(dynamic)
+    for (int kk = 0; kk < nk * (gc->j2 - gc->j1 + 1); ++kk) {
+      int k = gc->k1 + kk / (gc->j2 - gc->j1 + 1), j = gc->j1 + kk % (gc->j2 - gc->j1 + 1);
+      real cx = 0., cy = 0., cz = 0.;
+      real bx = 0., by = 0., bz = 0.;
+      for (int i = gc->i1; i <= gc->i2; ++i) {
+        for (int n = 0; n < NM; ++n) w[n] = s->prim[IDX(s, n, k, j, i)];
+#if ORC_MFIELD
+        bx = w[BX]; by = w[BY]; bz = w[BZ];
+#endif
+        real vfx = orc_fms(w, bx, gam);
+        cx = fabs(w[VX]) + vfx;
+        if (dims >= 2) {
+          real vfy = orc_fms(w, by, gam);
+          cy = fabs(w[VY]) + vfy;
+        }
+        if (dims >= 3) {
+          real vfz = orc_fms(w, bz, gam);
+          cz = fabs(w[VZ]) + vfz;
+        }
+        real dsx = gc->dlf[0][i], dsy = gc->dlf[1][j], dsz = gc->dlf[2][k];
+        real cds = fmax(fmax(cx / dsx, cy / dsy), cz / dsz);
+        if (cds > loc[id]) loc[id] = cds;
+      }
+    }
+  }
+  for (int i = 0; i < s->nthr; ++i)
+    if (loc[i] > cdsmax) cdsmax = loc[i];
+  free(loc);
+  return s->p.cour / cdsmax;
+}
+
+/* ---------------------------------------------------------------------
+ * RKL2 field-aligned conduction (thcond_elec.pyx, util_diffusion.pyx,
+ * diffusion.pyx:217-260)
+ * ------------------------------------------------------------------- */
+
+/* util_diffusion.pyx:16-20 (magnitude only, faithful) */
+static inline real dlim(real a, real b) {
+  real _a = fabs(a), _b = fabs(b);
+  return fmax(0., fmin(fmin(0.5 * (_a + _b), _a), _b));
+}
+
+int orc_get_nsts(real dt_hyp, real dt_diff) {
+  if (dt_diff >= dt_hyp) return 1;
+  return (int)(0.5 * (sqrt(9. + 16. * dt_hyp / dt_diff) - 1.)) + 1;
+}
+
+void orc_get_sts_coeff(int s, real *coeff) {
+  /* columns MU, NU, MUT, GAMT = 0..3 (D15) */
+  memset(coeff, 0, (size_t)(s + 1) * 4 * sizeof(real));
+  if (s == 1) {
+    coeff[1 * 4 + 2] = 1.;
+    return;
+  }
+  real one3rd = 1. / 3;
+  real w1 = 4. / (s * s + s - 2);
+  real *b = (real *)calloc(s + 1, sizeof(real));
+  b[0] = one3rd;
+  b[1] = one3rd;
+  coeff[1 * 4 + 0] = 0.;
+  coeff[1 * 4 + 1] = 0.;
+  coeff[1 * 4 + 2] = w1 * b[1];
+  coeff[1 * 4 + 3] = 0.;
+  for (int j = 2; j <= s; ++j) {
+    b[j] = (real)(j * j + j - 2) / (2 * j * (j + 1));
+    coeff[j * 4 + 0] = (real)(2 * j - 1) / j * b[j] / b[j - 1];
+    coeff[j * 4 + 1] = (1. - j) / j * b[j] / b[j - 2];
+    coeff[j * 4 + 2] = w1 * coeff[j * 4 + 0];
+    coeff[j * 4 + 3] = (b[j - 1] - 1) * coeff[j * 4 + 2];
+  }
+  free(b);
+}
+
+#if ORC_MFIELD
+#define TC_BSEL 1
+#else
+#define TC_BSEL 0
+#endif
+
+/* thcond_elec.pyx:118-338 */
+static void apply_diff_oper(orc_sim *s) {
+  orc_coord *gc = &s->gc;
+  int dims = s->p.dims;
+  int il = 1, iu = gc->Ntot[0] - 2;
+  int jl = dims >= 2 ? 1 : 0, ju = dims >= 2 ? gc->Ntot[1] - 2 : 0;
+  int kl = dims >= 3 ? 1 : 0, ku = dims >= 3 ? gc->Ntot[2] - 2 : 0;
+  real gamm1 = s->p.gam - 1.;
+  real *T = s->temp, *kap = s->kappa, *fx = s->fxd, *fy = s->fyd, *fz = s->fzd;
+  const real *prim = s->prim;
+  int aniso = (s->p.thcond_type == ORC_TC_ANISO) && TC_BSEL;
+  real **dvi = gc->dlv_inv;
+#define TT(k, j, i) T[C3(s, k, j, i)]
+#define KK(k, j, i) kap[C3(s, k, j, i)]
+#define P(n, k, j, i) prim[IDX(s, n, k, j, i)]
+
+#pragma omp parallel for collapse(2) num_threads(s->nthr) schedule(static)
+  for (int k = 0; k < gc->Ntot[2]; ++k)
+    for (int j = 0; j < gc->Ntot[1]; ++j)
+      for (int i = 0; i < gc->Ntot[0]; ++i) {
+        TT(k, j, i) = P(PR, k, j, i) / P(RHO, k, j, i);
+        KK(k, j, i) = s->p.kappa0;
+      }
+
+  /* x faces */
+#pragma omp parallel for collapse(2) num_threads(s->nthr) schedule(static)
+  for (int k = kl; k <= ku; ++k)
+    for (int j = jl; j <= ju; ++j)
+      for (int i = il; i <= iu + 1; ++i) {
+        real dTdy = 0., dTdz = 0., h = 0.;
+        real kappah = (2. * KK(k, j, i - 1) * KK(k, j, i) / (KK(k, j, i - 1) + KK(k, j, i) + SMALL_NUM));
+        real dTdx = dvi[0][i] * (TT(k, j, i) - TT(k, j, i - 1));
+        real f;
+        if (aniso) {
+#if ORC_MFIELD
+          real bxh = s->bfld[IDX(s, 0, k, j, i)];
+          real byh = 0.5 * (P(BY, k, j, i - 1) + P(BY, k, j, i));
+          real bzh = 0.5 * (P(BZ, k, j, i - 1) + P(BZ, k, j, i));
+          real bhi = 1. / sqrt(bxh * bxh + byh * byh + bzh * bzh + SMALL_NUM);
+          real bxh1 = bxh * bhi, byh1 = byh * bhi, bzh1 = bzh * bhi;
+          h = fabs(bxh1);
+          if (dims >= 2)
+            dTdy = dlim(dlim((TT(k, j, i - 1) - TT(k, j - 1, i - 1)) * dvi[1][j],
+                             (TT(k, j + 1, i - 1) - TT(k, j, i - 1)) * dvi[1][j + 1]) * gc->syxv[i - 1],
+                        dlim((TT(k, j, i) - TT(k, j - 1, i)) * dvi[1][j],
+                             (TT(k, j + 1, i) - TT(k, j, i)) * dvi[1][j + 1]) * gc->syxv[i]);
+          if (dims >= 3)
+            dTdz = dlim(dlim((TT(k, j, i - 1) - TT(k - 1, j, i - 1)) * dvi[2][k],
+                             (TT(k + 1, j, i - 1) - TT(k, j, i - 1)) * dvi[2][k + 1]) * gc->szxv[i - 1] * gc->szyv[j],
+                        dlim((TT(k, j, i) - TT(k - 1, j, i)) * dvi[2][k],
+                             (TT(k + 1, j, i) - TT(k, j, i)) * dvi[2][k + 1]) * gc->szxv[i] * gc->szyv[j]);
+          f = -kappah * bxh1 * (bxh1 * dTdx + byh1 * dTdy + bzh1 * dTdz);
+#else
+          f = 0.;
+#endif
+        } else {
+          if (dims >= 2)
+            dTdy = 0.25 * (((TT(k, j, i - 1) - TT(k, j - 1, i - 1)) * dvi[1][j] +
+                            (TT(k, j + 1, i - 1) - TT(k, j, i - 1)) * dvi[1][j + 1]) * gc->syxv[i - 1] +
+                           ((TT(k, j, i) - TT(k, j - 1, i)) * dvi[1][j] +
+                            (TT(k, j + 1, i) - TT(k, j, i)) * dvi[1][j + 1]) * gc->syxv[i]);
+          if (dims >= 3)
+            dTdz = 0.25 * (((TT(k, j - 1, i) - TT(k - 1, j - 1, i)) * dvi[2][k] +
+                            (TT(k + 1, j - 1, i) - TT(k, j - 1, i)) * dvi[2][k + 1]) * gc->szxv[i] * gc->szyv[j - 1] +
+                           ((TT(k, j, i) - TT(k - 1, j, i)) * dvi[2][k] +
+                            (TT(k + 1, j, i) - TT(k, j, i)) * dvi[2][k + 1]) * gc->szxv[i] * gc->szyv[j]);
+          real dTds = sqrt(dTdx * dTdx + dTdy * dTdy + dTdz * dTdz + SMALL_NUM);
+          h = fabs(dTdx / dTds);
+          f = -kappah * dTdx;
+        }
+        if (s->p.sat_hfe) {
+          real Tl = TT(k, j, i - 1), Tr = TT(k, j, i);
+          real Tc = 0.5 * (Tl + Tr);
+          real rhoc = 0.5 * (P(RHO, k, j, i - 1) + P(RHO, k, j, i));
+          real mom = 0.5 * h * rhoc * sqrt(0.67 * Tc);
+          real qsat = f > 0. ? Tl * mom : Tr * mom;
+          f = f * qsat / (fabs(f) + qsat + SMALL_NUM);
+        }
+        fx[C3(s, k, j, i)] = f;
+      }
+
+  /* y faces */
+  if (dims >= 2) {
+#pragma omp parallel for collapse(2) num_threads(s->nthr) schedule(static)
+    for (int k = kl; k <= ku; ++k)
+      for (int j = jl; j <= ju + 1; ++j)
+        for (int i = il; i <= iu; ++i) {
+          real dTdx = 0., dTdz = 0., h = 0.;
+          real kappah = (2. * KK(k, j - 1, i) * KK(k, j, i) / (KK(k, j - 1, i) + KK(k, j, i) + SMALL_NUM));
+          real dTdy = dvi[1][j] * (TT(k, j, i) - TT(k, j - 1, i));
+          real f;
+          if (aniso) {
+#if ORC_MFIELD
+            real byh = s->bfld[IDX(s, 1, k, j, i)];
+            real bxh = 0.5 * (P(BX, k, j - 1, i) + P(BX, k, j, i));
+            real bzh = 0.5 * (P(BZ, k, j - 1, i) + P(BZ, k, j, i));
+            real bhi = 1. / sqrt(bxh * bxh + byh * byh + bzh * bzh + SMALL_NUM);
+            real bxh1 = bxh * bhi, byh1 = byh * bhi, bzh1 = bzh * bhi;
+            h = fabs(byh1);
+            dTdx = dlim(dlim((TT(k, j - 1, i) - TT(k, j - 1, i - 1)) * dvi[0][i],
+                             (TT(k, j - 1, i + 1) - TT(k, j - 1, i)) * dvi[0][i + 1]),
+                        dlim((TT(k, j, i) - TT(k, j, i - 1)) * dvi[0][i],
+                             (TT(k, j, i + 1) - TT(k, j, i)) * dvi[0][i + 1]));
+            if (dims >= 3)
+              dTdz = dlim(dlim((TT(k, j - 1, i) - TT(k - 1, j - 1, i)) * dvi[2][k],
+                               (TT(k + 1, j - 1, i) - TT(k, j - 1, i)) * dvi[2][k + 1]) * gc->szxv[i] * gc->szyv[j - 1],
+                          dlim((TT(k, j, i) - TT(k - 1, j, i)) * dvi[2][k],
+                               (TT(k + 1, j, i) - TT(k, j, i)) * dvi[2][k + 1]) * gc->szxv[i] * gc->szyv[j]);
+            f = -kappah * byh1 * (bxh1 * dTdx + byh1 * dTdy + bzh1 * dTdz);
+#else
+            f = 0.;
+#endif
+          } else {
+            dTdx = 0.25 * (((TT(k, j - 1, i) - TT(k, j - 1, i - 1)) * dvi[0][i] +
+                            (TT(k, j - 1, i + 1) - TT(k, j - 1, i)) * dvi[0][i + 1]) +
+                           ((TT(k, j, i) - TT(k, j, i - 1)) * dvi[0][i] +
+                            (TT(k, j, i + 1) - TT(k, j, i)) * dvi[0][i + 1]));
+            if (dims >= 3)
+              dTdz = 0.25 * (((TT(k, j - 1, i) - TT(k - 1, j - 1, i)) * dvi[2][k] +
+                              (TT(k + 1, j - 1, i) - TT(k, j - 1, i)) * dvi[2][k + 1]) * gc->szxv[i] * gc->szyv[j - 1] +
+                             ((TT(k, j, i) - TT(k - 1, j, i)) * dvi[2][k] +
+                              (TT(k + 1, j, i) - TT(k, j, i)) * dvi[2][k + 1]) * gc->szxv[i] * gc->szyv[j]);
+            real dTds = sqrt(dTdx * dTdx + dTdy * dTdy + dTdz * dTdz + SMALL_NUM);
+            h = fabs(dTdy / dTds);
+            f = -kappah * dTdy;
+          }
+          if (s->p.sat_hfe) {
+            real Tr = TT(k, j, i), Tl = TT(k, j - 1, i);
+            real Tc = 0.5 * (Tl + Tr);
+            real rhoc = 0.5 * (P(RHO, k, j - 1, i) + P(RHO, k, j, i));
+            real mom = 0.5 * h * rhoc * sqrt(0.67 * Tc);
+            real qsat = f > 0. ? Tl * mom : Tr * mom;
+            f = f * qsat / (fabs(f) + qsat + SMALL_NUM);
+          }
+          fy[C3(s, k, j, i)] = f;
+        }
+  }
+
+  /* z faces */
+  if (dims >= 3) {
+#pragma omp parallel for collapse(2) num_threads(s->nthr) schedule(static)
+    for (int k = kl; k <= ku + 1; ++k)
+      for (int j = jl; j <= ju; ++j)
+        for (int i = il; i <= iu; ++i) {
+          real dTdx = 0., dTdy = 0., h = 0.;
+          real kappah = (2. * KK(k - 1, j, i) * KK(k, j, i) / (KK(k - 1, j, i) + KK(k, j, i) + SMALL_NUM));
+          real dTdz = dvi[2][k] * (TT(k, j, i) - TT(k - 1, j, i));
+          real f;
+          if (aniso) {
+#if ORC_MFIELD
+            real bzh = s->bfld[IDX(s, 2, k, j, i)];
+            real bxh = 0.5 * (P(BX, k - 1, j, i) + P(BX, k, j, i));
+            real byh = 0.5 * (P(BY, k - 1, j, i) + P(BY, k, j, i));
+            real bhi = 1. / sqrt(bxh * bxh + byh * byh + bzh * bzh + SMALL_NUM);
+            real bxh1 = bxh * bhi, byh1 = byh * bhi, bzh1 = bzh * bhi;
+            h = fabs(bzh1);
+            dTdx = dlim(dlim((TT(k - 1, j, i) - TT(k - 1, j, i - 1)) * dvi[0][i],
+                             (TT(k - 1, j, i + 1) - TT(k - 1, j, i)) * dvi[0][i + 1]),
+                        dlim((TT(k, j, i) - TT(k, j, i - 1)) * dvi[0][i],
+                             (TT(k, j, i + 1) - TT(k, j, i)) * dvi[0][i + 1]));
+            dTdy = dlim(dlim((TT(k - 1, j, i) - TT(k - 1, j - 1, i)) * dvi[1][j],
+                             (TT(k - 1, j + 1, i) - TT(k - 1, j, i)) * dvi[1][j + 1]) * gc->syxv[i],
+                        dlim((TT(k, j, i) - TT(k, j - 1, i)) * dvi[1][j],
+                             (TT(k, j + 1, i) - TT(k, j, i)) * dvi[1][j + 1]) * gc->syxv[i]);
+            f = -kappah * bzh1 * (bxh1 * dTdx + byh1 * dTdy + bzh1 * dTdz);
+#else
+            f = 0.;
+#endif
+          } else {
+            dTdx = 0.25 * (((TT(k - 1, j, i) - TT(k - 1, j, i - 1)) * dvi[0][i] +
+                            (TT(k - 1, j, i + 1) - TT(k - 1, j, i)) * dvi[0][i + 1]) +
+                           ((TT(k, j, i) - TT(k, j, i - 1)) * dvi[0][i] +
+                            (TT(k, j, i + 1) - TT(k, j, i)) * dvi[0][i + 1]));
+            dTdy = 0.25 * (((TT(k - 1, j, i) - TT(k - 1, j - 1, i)) * dvi[1][j] +
+                            (TT(k - 1, j + 1, i) - TT(k - 1, j, i)) * dvi[1][j + 1]) * gc->syxv[i] +
+                           ((TT(k, j, i) - TT(k, j - 1, i)) * dvi[1][j] +
+                            (TT(k, j + 1, i) - TT(k, j, i)) * dvi[1][j + 1]) * gc->syxv[i]);
+            real dTds = sqrt(dTdx * dTdx + dTdy * dTdy + dTdz * dTdz + SMALL_NUM);
+            h = fabs(dTdz / dTds);
+            f = -kappah * dTdz;
+          }
+          if (s->p.sat_hfe) {
+            real Tl = TT(k - 1, j, i), Tr = TT(k, j, i);
+            real Tc = 0.5 * (Tl + Tr);
+            real rhoc = 0.5 * (P(RHO, k - 1, j, i) + P(RHO, k, j, i));
+            real mom = 0.5 * h * rhoc * sqrt(0.67 * Tc);
+            real qsat = f > 0. ? Tl * mom : Tr * mom;
+            f = f * qsat / (fabs(f) + qsat + SMALL_NUM);
+          }
+          fz[C3(s, k, j, i)] = f;
+        }
+  }
+
+#pragma omp parallel for collapse(2) num_threads(s->nthr) schedule(static)
+  for (int k = kl; k <= ku; ++k)
+    for (int j = jl; j <= ju; ++j)
+      for (int i = il; i <= iu; ++i) {
+        real v = -(fx[C3(s, k, j, i + 1)] - fx[C3(s, k, j, i)]) * gamm1 * gc->dlf_inv[0][i];
+        if (dims >= 2) v -= (fy[C3(s, k, j + 1, i)] - fy[C3(s, k, j, i)]) * gamm1 * gc->dlf_inv[1][j];
+        if (dims >= 3) v -= (fz[C3(s, k + 1, j, i)] - fz[C3(s, k, j, i)]) * gamm1 * gc->dlf_inv[2][k];
+        s->dtemp[C3(s, k, j, i)] = v;
+      }
+#undef TT
+#undef KK
+#undef P
+}
+
+/* thcond_elec.pyx:355-466 */
+static real diff_get_dt(orc_sim *s) {
+  orc_coord *gc = &s->gc;
+  int dims = s->p.dims;
+  real gamm1 = s->p.gam - 1.;
+  real mx = 0.;
+  for (int k = gc->k1; k <= gc->k2; ++k)
+    for (int j = gc->j1; j <= gc->j2; ++j)
+      for (int i = gc->i1; i <= gc->i2; ++i) {
+        real dsx = gc->dlf[0][i], dsy = gc->dlf[1][j], dsz = gc->dlf[2][k];
+        real ad = s->p.kappa0 / s->prim[IDX(s, RHO, k, j, i)] * gamm1;
+        real ad_dl2 = ad / SQR(dsx);
+        if (dims >= 2) ad_dl2 = ad_dl2 + ad / SQR(dsy);
+        if (dims >= 3) ad_dl2 = ad_dl2 + ad / SQR(dsz);
+        if (ad_dl2 > mx) mx = ad_dl2;
+      }
+  return s->p.cour_diff / mx;
+}
+
+/* thcond_elec.pyx:17-113 */
+void orc_diffuse(orc_sim *s, real dt) {
+  if (s->p.kappa0 == 0.) return;
+  orc_coord *gc = &s->gc;
+  int dims = s->p.dims;
+  int il = 1, iu = gc->Ntot[0] - 2;
+  int jl = dims >= 2 ? 1 : 0, ju = dims >= 2 ? gc->Ntot[1] - 2 : 0;
+  int kl = dims >= 3 ? 1 : 0, ku = dims >= 3 ? gc->Ntot[2] - 2 : 0;
+  real dt_hyp = dt;
+  orc_apply_bc(s, (1u << ORC_NVAR) - 1u);
+  real dt_diff = diff_get_dt(s);
+  int ns = orc_get_nsts(dt_hyp, dt_diff);
+  s->last_nsts = ns;
+  real *cf = (real *)calloc((size_t)(ns + 1) * 4, sizeof(real));
+  orc_get_sts_coeff(ns, cf);
+  for (int n = 1; n <= ns; ++n) {
+    apply_diff_oper(s);
+    if (n == 1) {
+#pragma omp parallel for collapse(2) num_threads(s->nthr) schedule(static)
+      for (int k = kl; k <= ku; ++k)
+        for (int j = jl; j <= ju; ++j)
+          for (int i = il; i <= iu; ++i) {
+            s->pres0[C3(s, k, j, i)] = s->prim[IDX(s, PR, k, j, i)];
+            s->dtemp0[C3(s, k, j, i)] = s->dtemp[C3(s, k, j, i)];
+          }
+    }
+    real mu = cf[n * 4 + 0], nu = cf[n * 4 + 1], mut = cf[n * 4 + 2], gamt = cf[n * 4 + 3];
+#pragma omp parallel for collapse(2) num_threads(s->nthr) schedule(static)
+    for (int k = kl; k <= ku; ++k)
+      for (int j = jl; j <= ju; ++j)
+        for (int i = il; i <= iu; ++i) {
+          size_t c = C3(s, k, j, i);
+          real *pp = &s->prim[IDX(s, PR, k, j, i)];
+          real a = *pp;
+          *pp = (mu * *pp + nu * s->presm1[c] + (1. - mu - nu) * s->pres0[c] +
+                 dt_hyp * (mut * s->dtemp[c] + gamt * s->dtemp0[c]));
+          s->presm1[c] = a;
+        }
+    if (n % gc->ng == 0 && n != ns) orc_apply_bc(s, 1u << PR);
+  }
+  free(cf);
+}
+
+/* vanleer.pyx:101-163 (one VL2 step without the dt selection). */
+void orc_vl2_step(orc_sim *s, real dtfull) {
+  real *w = s->prim, *u = s->cons, *ws = s->prim, *us = s->cons_s;
+  real *b = s->bfld, *bs = s->bfld_s;
+  int lims[6];
+  /* predictor */
+  int order = 0;
+  real dt = 0.5 * dtfull;
+  integr_lims(s, order, lims);
+  integrate_hydro(s, us, u, w, b, order, dt);
+#if ORC_MFIELD
+  integrate_field(s, us, bs, w, b, order, dt);
+#else
+  (void)bs;
+#endif
+  cons2prim_range(s, ws, us, lims);
+  /* corrector */
+  order = s->reconstr_order;
+  dt = dtfull;
+  integr_lims(s, order, lims);
+  integrate_hydro(s, u, u, ws, bs, order, dt);
+#if ORC_MFIELD
+  integrate_field(s, u, b, ws, b, order, dt);
+#endif
+  cons2prim_range(s, s->prim, s->cons, lims);
+  orc_diffuse(s, dt);
+  orc_apply_bc(s, (1u << ORC_NVAR) - 1u);
+  int lt[6];
+  all_lims(s, lt);
+  prim2cons_range(s, s->cons, s->prim, lt);
+}
+
+/* vanleer.pyx:87-167 */
+void orc_advance(orc_sim *s, real tmax, int max_steps) {
+  int n = 0;
+  while (s->time < tmax && (max_steps <= 0 || n < max_steps)) {
+    if (!s->p.fixdt) {
+      s->dt = orc_new_dt(s);
+      if (s->time + s->dt > tmax) s->dt = tmax - s->time;
+    } else {
+      s->dt = s->p.dt_fixed;
+    }
+    orc_vl2_step(s, s->dt);
+    s->time += s->dt;
+    s->step += 1;
+    ++n;
+  }
+}
