@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Headline benchmark: FP64 VL2 + PLM + HLLD + CT on the uneven 2D blast batch.
+
+Workload (the uneven parameter sweep the headline metric is quoted on): 64
+independent 2D MHD blast-wave runs, side lengths drawn from the seed in
+{64, 96, 128, 192, 256, 384, 512}, outflow boundaries, per-instance CFL dt,
+gamma = 5/3, VL2 + PLM (van Leer limiter, the reference default) + HLLD + CT.
+Synthetic seeded initial conditions (no dataset exists).  One "step" advances
+every instance by one VL2 step; a zone-update is one active cell advanced one
+step.  The batch state (~0.5 GB) is larger than L2, so no flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  Under torchrun each rank runs its own batch
+(weak scaling: the instances are independent, there is no data-path
+collective); the timed region is bracketed by barriers and the max over ranks
+is reported.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mzone-updates/s, 1 B200: batched FP64 VL2+HLLD+CT vs plain; adjoint/fwd ratio"
+UNIT = "Mzone-updates/s"
+BYTES_PER_ZONE = 192  # 9 conserved + 3 face-B doubles read once and written once
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--path", default="plain", choices=["plain", "fused"])
+    ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def build_batch(n, seed):
+    from bonzo_b200 import problems as P
+    out = []
+    for q in P.blast_batch_params(n, seed):
+        gc = P.make_grid(q["N"], q["N"], 1, dims=2, bc=1)
+        prim, bfld = P.blast(gc, b_mag=q["b_mag"], b_angle=q["b_angle"], center=q["center"],
+                             p_ratio=q["p_ratio"])
+        out.append((q, gc, prim, bfld))
+    return out
+
+
+METHOD = dict(dims=2, bc=((1, 1), (1, 1), (1, 1)), gam=5. / 3, cour=0.4, rsolver="hlld",
+              reconstr="linear", limiter="vl")
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    """Samples SM clock and clock-event reasons every 200 ms (NVML)."""
+
+    REASONS = {
+        "hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+        "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80,
+    }
+
+    def __init__(self, device_index):
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            import torch
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            try:
+                self.h = pynvml.nvmlDeviceGetHandleByUUID("GPU-" + uuid)
+            except Exception:
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.nv = pynvml
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for name, bit in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        if self.nv is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+
+    def record(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (the reference's compiled kernels through the oracle driver)
+# ---------------------------------------------------------------------------
+
+def cpu_sample(batch, min_zones=1_200_000):
+    """Instances (in seeded order) until the sample holds >= min_zones cells."""
+    sample, z = [], 0
+    for item in batch:
+        sample.append(item)
+        z += item[0]["N"] ** 2
+        if z >= min_zones:
+            break
+    return sample, z
+
+
+def run_cpu_reference(batch, steps, warmup):
+    from oracle import oracle as O
+    use_ref = O.ref_lib() is not None
+    sample, zones = cpu_sample(batch)
+    sims = []
+    for q, gc, prim, bfld in sample:
+        s = O.OracleSim(Nx=q["N"], Ny=q["N"], Nz=1, use_ref_kernels=use_ref, nthreads=0,
+                        rows_parallel=1, **METHOD)
+        s.set_state(prim, bfld)
+        s.init()
+        sims.append(s)
+    times = []
+    for it in range(warmup + steps):
+        t0 = time.perf_counter()
+        for s in sims:
+            s.advance(1e30, max_steps=1)
+        dt = time.perf_counter() - t0
+        if it >= warmup:
+            times.append(dt)
+    per_step = statistics.median(times)
+    value = zones / per_step / 1e6
+    desc = ("one VL2 step on the first %d instances of the batch (%d zones, N=%s); %s; "
+            "OpenMP rows-parallel over all host threads" %
+            (len(sample), zones, ",".join(str(x[0]["N"]) for x in sample),
+             "reference C kernels (src/mhd/fluxes_c.c, src/coordinates/reconstr_c.c, "
+             "src/mhd/eos_c.c) driven by the oracle's C restatement of the Cython sweeps"
+             if use_ref else "oracle C restatement"))
+    return dict(value=round(value, 3), unit=UNIT, cores=os.cpu_count(),
+                kind="reference" if use_ref else "port", sample=desc,
+                per_step_s=round(per_step, 4))
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args, rank, world, dist):
+    import torch
+    from bonzo_b200._lib import Context
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    batch = build_batch(args.instances, args.seed)
+    zones = sum(q["N"] ** 2 for q, _, _, _ in batch)
+    stream = torch.cuda.Stream()
+    ctxs = []
+    for q, gc, prim, bfld in batch:
+        c = Context(Nx=q["N"], Ny=q["N"], Nz=1, path=args.path, **METHOD)
+        c.set_stream(stream.cuda_stream)
+        c.set_state(prim, bfld)
+        c.init()
+        ctxs.append(c)
+
+    def one_step():
+        for c in ctxs:
+            c.advance_graph(1e30, 1)
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+    launches0 = sum(c.launch_count() for c in ctxs)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            for _ in range(args.steps):
+                one_step()
+            ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = sum(c.launch_count() for c in ctxs) - launches0
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    ms_step = ms_max / args.steps
+    value = world * zones * args.steps / (ms_max * 1e-3) / 1e6
+
+    # e2e: host state in pinned memory, copied in and out every step through the C ABI
+    host = []
+    for c in ctxs:
+        P = torch.empty((9,) + c.shape, dtype=torch.float64, pin_memory=True).numpy()
+        B = torch.empty((3,) + c.shape, dtype=torch.float64, pin_memory=True).numpy()
+        P[...], _, B[...] = c.get_state(prim=True, cons=False, bfld=True)
+        host.append((P, B))
+    h2d = sum(P.nbytes + B.nbytes for P, B in host)
+    ke = max(1, args.e2e_steps)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(ke):
+        for c, (P, B) in zip(ctxs, host):
+            c.set_state(P, B)
+            c.advance_graph(1e30, 1)
+            c.get_state_into(P, None, B)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ems], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+    e2e = world * zones * ke / (ems * 1e-3) / 1e6
+    for c in ctxs:
+        c.check()
+
+    from bonzo_b200.peaks import hbm_peak
+    peak, peak_src = hbm_peak()
+    achieved = BYTES_PER_ZONE * zones / (ms_step * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None,
+                "peak_source": peak_src,
+                "kernel": "whole step (%s path, %d launches per step over %d instances)" %
+                          (args.path, launches // max(1, args.steps), len(ctxs)),
+                "bytes_per_zone": BYTES_PER_ZONE}
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded blast-wave initial conditions)",
+        "config": {"workload": "uneven 2D MHD blast batch: %d instances, N^2 with N in "
+                               "{64,96,128,192,256,384,512} (seed %d), outflow BCs, VL2+PLM(vl)+HLLD+CT, "
+                               "per-instance CFL dt" % (len(ctxs), args.seed),
+                   "instances": len(ctxs), "zones_per_step_per_gpu": zones, "path": args.path,
+                   "l2": "inputs larger than L2 (%.0f MB of state)" % (
+                       sum(12 * 8 * np.prod(c.shape) for c in ctxs) / 1e6),
+                   "parallelism": "instances sharded per GPU (dp%d, no collective)" % world},
+        "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(h2d),
+                "how": "bnz_set_state + bnz_advance_graph + bnz_get_state per instance per step, "
+                       "pinned host buffers"},
+        "gpu_launches": int(launches),
+        "roofline": roofline,
+        "clocks": clk.record(),
+    }
+    return line
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        batch = build_batch(args.instances, args.seed)
+        cb = run_cpu_reference(batch, args.steps, args.warmup)
+        line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(cb["per_step_s"] * 1e3, 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded blast-wave initial conditions)", "impl": "reference",
+                "config": {"workload": "uneven 2D MHD blast batch (bounded CPU sample, see cpu_baseline)",
+                           "instances": args.instances},
+                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    line = run_ours(args, rank, world, dist)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        batch = build_batch(args.instances, args.seed)
+        cb = run_cpu_reference(batch, steps=2, warmup=1)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

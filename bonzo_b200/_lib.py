@@ -26,7 +26,7 @@ EXPORTS = [
     "bnz_create", "bnz_destroy", "bnz_last_error", "bnz_shape", "bnz_set_state", "bnz_init",
     "bnz_get_state", "bnz_apply_bc", "bnz_new_dt", "bnz_vl2_step", "bnz_diffuse", "bnz_advance",
     "bnz_get_time", "bnz_set_time", "bnz_check", "bnz_sync", "bnz_advance_graph",
-    "bnz_device_state", "bnz_stream",
+    "bnz_device_state", "bnz_stream", "bnz_set_stream", "bnz_launch_count",
 ]
 
 
@@ -84,6 +84,8 @@ def load():
     L.bnz_advance_graph.argtypes = [vp, C.c_double, C.c_int]
     L.bnz_device_state.argtypes = [vp, C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp)]
     L.bnz_stream.argtypes = [vp, C.POINTER(vp)]
+    L.bnz_set_stream.argtypes = [vp, vp]
+    L.bnz_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     _lib = L
     return L
 
@@ -170,6 +172,14 @@ class Context:
         self._ck(self.L.bnz_get_state(self.h, _p(P), _p(U), _p(B)))
         return P, U, B
 
+    def get_state_into(self, prim=None, cons=None, bfld=None):
+        """Download into caller-provided float64 arrays (e.g. pinned buffers)."""
+        for a, nv in ((prim, 9), (cons, 9), (bfld, 3)):
+            if a is not None and (a.shape != (nv,) + self.shape or a.dtype != np.float64
+                                  or not a.flags["C_CONTIGUOUS"]):
+                raise ValueError("output array has the wrong shape or layout")
+        self._ck(self.L.bnz_get_state(self.h, _p(prim), _p(cons), _p(bfld)))
+
     def apply_bc(self, mask=0xFFF):
         self._ck(self.L.bnz_apply_bc(self.h, mask))
 
@@ -213,6 +223,15 @@ class Context:
         p, u, b = _dp(), _dp(), _dp()
         self._ck(self.L.bnz_device_state(self.h, C.byref(p), C.byref(u), C.byref(b)))
         return (C.cast(p, C.c_void_p).value, C.cast(u, C.c_void_p).value, C.cast(b, C.c_void_p).value)
+
+    def set_stream(self, stream):
+        """Order this context's work on a caller-owned CUDA stream (handle as int)."""
+        self._ck(self.L.bnz_set_stream(self.h, C.c_void_p(stream)))
+
+    def launch_count(self):
+        n = C.c_longlong()
+        self._ck(self.L.bnz_launch_count(self.h, C.byref(n)))
+        return n.value
 
     def stream(self):
         s = C.c_void_p()

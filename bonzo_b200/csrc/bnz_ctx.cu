@@ -52,6 +52,10 @@ struct bnz_ctx {
   double time = 0.;
   long step = 0;
   double last_dt = 0.;
+  long long launches = 0;  // kernels launched through this context
+  long long graph_launches = 0;
+  bool time_on_device = false;  // the device DtState holds the current time
+  bool own_stream = true;
 };
 
 namespace {
@@ -168,7 +172,7 @@ void free_all(bnz_ctx* c) {
   if (c->d_err) cudaFree(c->d_err);
   if (c->d_ds) cudaFree(c->d_ds);
   if (c->graph) cudaGraphExecDestroy(c->graph);
-  if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
   c->d_err = nullptr;
   c->d_ds = nullptr;
   c->graph = nullptr;
@@ -205,6 +209,23 @@ int validate(const bnz_grid_desc* g, const bnz_method_desc* m, std::string& why)
   for (int a = 0; a < g->dims; ++a)
     if (N[a] < ng) return why = "each active axis needs at least ng cells", 0;
   return 1;
+}
+
+}  // namespace
+
+namespace {
+
+// Pull the device time record into the host copy after graph stepping.
+int sync_time(bnz_ctx* c) {
+  if (!c->time_on_device) return BNZ_OK;
+  DtState ds;
+  CKC(cudaMemcpyAsync(&ds, c->d_ds, sizeof ds, cudaMemcpyDeviceToHost, c->stream));
+  CKC(cudaStreamSynchronize(c->stream));
+  c->time = ds.time;
+  c->step = (long)ds.step;
+  c->last_dt = ds.dt;
+  c->time_on_device = false;
+  return BNZ_OK;
 }
 
 }  // namespace
@@ -376,10 +397,10 @@ int bnz_set_state(bnz_ctx* c, const double* pc, int is_prim, const double* bfld)
   size_t n9 = 9 * c->ncell * sizeof(double), n3 = 3 * c->ncell * sizeof(double);
   CKC(cudaMemcpyAsync(is_prim ? c->prim : c->cons, pc, n9, cudaMemcpyHostToDevice, c->stream));
   if (bfld) CKC(cudaMemcpyAsync(c->bfld, bfld, n3, cudaMemcpyHostToDevice, c->stream));
-  if (!is_prim) {
-    StepArgs a = step_args(c);
-    c->L->cons2prim_all(a);
-  }
+  // derive the other array on every cell, as init_sim does after set_problem
+  StepArgs a = step_args(c);
+  if (is_prim) c->launches += c->L->prim2cons_all(a);
+  else c->launches += c->L->cons2prim_all(a);
   CKC(cudaGetLastError());
   CKC(cudaStreamSynchronize(c->stream));
   return BNZ_OK;
@@ -388,10 +409,10 @@ int bnz_set_state(bnz_ctx* c, const double* pc, int is_prim, const double* bfld)
 int bnz_init(bnz_ctx* c) {
   if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
   StepArgs a = step_args(c);
-  c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
-  c->L->interp_bc_active(a);
-  c->L->apply_bc(a, c->prim, c->bfld, (1u << 6) | (1u << 7) | (1u << 8));
-  c->L->prim2cons_all(a);
+  c->launches += c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
+  c->launches += c->L->interp_bc_active(a);
+  c->launches += c->L->apply_bc(a, c->prim, c->bfld, (1u << 6) | (1u << 7) | (1u << 8));
+  c->launches += c->L->prim2cons_all(a);
   DtState ds;
   memset(&ds, 0, sizeof ds);
   CKC(cudaMemcpyAsync(c->d_ds, &ds, sizeof ds, cudaMemcpyHostToDevice, c->stream));
@@ -416,7 +437,7 @@ int bnz_apply_bc(bnz_ctx* c, uint32_t mask) {
   if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
   if (mask & ~0xFFFu) return fail(c, BNZ_ERR_ARG, "var_mask has bits above 11");
   StepArgs a = step_args(c);
-  c->L->apply_bc(a, c->prim, c->bfld, mask);
+  c->launches += c->L->apply_bc(a, c->prim, c->bfld, mask);
   CKC(cudaGetLastError());
   return BNZ_OK;
 }
@@ -424,7 +445,7 @@ int bnz_apply_bc(bnz_ctx* c, uint32_t mask) {
 int bnz_new_dt(bnz_ctx* c, double* dt_out) {
   if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
   StepArgs a = step_args(c);
-  c->L->new_dt(a, c->prim, c->d_ds, c->md.cour, 0);
+  c->launches += c->L->new_dt(a, c->prim, c->d_ds, c->md.cour, 0);
   CKC(cudaGetLastError());
   DtState ds;
   CKC(cudaMemcpyAsync(&ds, c->d_ds, sizeof ds, cudaMemcpyDeviceToHost, c->stream));
@@ -442,11 +463,11 @@ int diffuse_impl(bnz_ctx* c, const double* dtp, double dt_hyp, int* nsts_out) {
     return BNZ_OK;
   }
   StepArgs a = step_args(c);
-  c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
+  c->launches += c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
   // diffusive dt: max over active cells, read back to size the stage loop
   unsigned long long* slot = &c->d_ds->cdsmax_bits;
   CKC(cudaMemsetAsync(slot, 0, sizeof(unsigned long long), c->stream));
-  c->L->diff_dt_max(a, c->da, slot);
+  c->launches += c->L->diff_dt_max(a, c->da, slot);
   unsigned long long bits = 0;
   CKC(cudaMemcpyAsync(&bits, slot, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
   CKC(cudaStreamSynchronize(c->stream));
@@ -477,8 +498,8 @@ int diffuse_impl(bnz_ctx* c, const double* dtp, double dt_hyp, int* nsts_out) {
   c->last_nsts = s;
   if (nsts_out) *nsts_out = s;
   for (int n = 1; n <= s; ++n) {
-    c->L->diff_operator(a, c->da);
-    c->L->diff_stage_update(a, c->da, n == 1, &cf[(size_t)n * 4], dtp);
+    c->launches += c->L->diff_operator(a, c->da);
+    c->launches += c->L->diff_stage_update(a, c->da, n == 1, &cf[(size_t)n * 4], dtp);
     if (n % c->ng == 0 && n != s) c->L->apply_bc(a, c->prim, c->bfld, 1u << 4);
   }
   CKC(cudaGetLastError());
@@ -490,9 +511,9 @@ int step_impl(bnz_ctx* c, double dt_host) {
   StepArgs a = step_args(c);
   const double* dtp = &c->d_ds->dt;
   if (c->md.path == BNZ_PATH_PLAIN) {
-    c->L->plain_predictor_corrector(a, dtp);
+    c->launches += c->L->plain_predictor_corrector(a, dtp);
   } else {
-    c->L->fused_step(a, dtp);
+    c->launches += c->L->fused_step(a, dtp);
     // the fused kernel writes the next state into the second buffers
     std::swap(c->prim, c->wnext);
     std::swap(c->bfld, c->bnext);
@@ -501,8 +522,8 @@ int step_impl(bnz_ctx* c, double dt_host) {
   CKC(cudaGetLastError());
   int rc = diffuse_impl(c, dtp, dt_host, nullptr);
   if (rc) return rc;
-  c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
-  c->L->prim2cons_all(a);
+  c->launches += c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
+  c->launches += c->L->prim2cons_all(a);
   CKC(cudaGetLastError());
   return BNZ_OK;
 }
@@ -512,25 +533,27 @@ int step_impl(bnz_ctx* c, double dt_host) {
 int bnz_diffuse(bnz_ctx* c, double dt, int* nsts_out) {
   if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
   if (!(dt >= 0.)) return fail(c, BNZ_ERR_ARG, "dt must be >= 0");
-  c->L->set_dt(c->stream, c->d_ds, dt);
+  c->launches += c->L->set_dt(c->stream, c->d_ds, dt);
   return diffuse_impl(c, &c->d_ds->dt, dt, nsts_out);
 }
 
 int bnz_vl2_step(bnz_ctx* c, double dt) {
   if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
   if (!(dt >= 0.) || std::isinf(dt)) return fail(c, BNZ_ERR_ARG, "dt must be finite and >= 0");
-  c->L->set_dt(c->stream, c->d_ds, dt);
+  c->launches += c->L->set_dt(c->stream, c->d_ds, dt);
   return step_impl(c, dt);
 }
 
 int bnz_advance(bnz_ctx* c, double tmax, int max_steps, double* time_out, long* step_out) {
   if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
+  int rc0 = sync_time(c);
+  if (rc0) return rc0;
   int n = 0;
   while (c->time < tmax && (max_steps <= 0 || n < max_steps)) {
     double dt;
     if (!c->md.fixdt) {
       StepArgs a = step_args(c);
-      c->L->new_dt(a, c->prim, c->d_ds, c->md.cour, 0);
+      c->launches += c->L->new_dt(a, c->prim, c->d_ds, c->md.cour, 0);
       DtState ds;
       CKC(cudaMemcpyAsync(&ds, c->d_ds, sizeof ds, cudaMemcpyDeviceToHost, c->stream));
       CKC(cudaStreamSynchronize(c->stream));
@@ -539,7 +562,7 @@ int bnz_advance(bnz_ctx* c, double tmax, int max_steps, double* time_out, long* 
     } else {
       dt = c->md.dt_fixed;
     }
-    c->L->set_dt(c->stream, c->d_ds, dt);
+    c->launches += c->L->set_dt(c->stream, c->d_ds, dt);
     int rc = step_impl(c, dt);
     if (rc) return rc;
     c->time += dt;
@@ -553,8 +576,10 @@ int bnz_advance(bnz_ctx* c, double tmax, int max_steps, double* time_out, long* 
   return BNZ_OK;
 }
 
-int bnz_get_time(const bnz_ctx* c, double* t, long* s, double* last_dt) {
+int bnz_get_time(bnz_ctx* c, double* t, long* s, double* last_dt) {
   if (!c) return BNZ_ERR_ARG;
+  int rc = sync_time(c);
+  if (rc) return rc;
   if (t) *t = c->time;
   if (s) *s = c->step;
   if (last_dt) *last_dt = c->last_dt;
@@ -563,6 +588,8 @@ int bnz_get_time(const bnz_ctx* c, double* t, long* s, double* last_dt) {
 
 int bnz_set_time(bnz_ctx* c, double t, long s) {
   if (!c) return BNZ_ERR_ARG;
+  int rc = sync_time(c);
+  if (rc) return rc;
   c->time = t;
   c->step = s;
   return BNZ_OK;
@@ -586,9 +613,68 @@ int bnz_sync(bnz_ctx* c) {
   return BNZ_OK;
 }
 
+
 int bnz_advance_graph(bnz_ctx* c, double tmax, int nsteps) {
   if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
-  return fail(c, BNZ_ERR_UNSUPPORTED, "graph stepping not built yet");
+  if (nsteps < 0) return fail(c, BNZ_ERR_ARG, "nsteps must be >= 0");
+  if (c->md.kappa0 > 0.)
+    return fail(c, BNZ_ERR_UNSUPPORTED, "graph stepping with conduction needs the host stage count");
+  if (nsteps == 0) return BNZ_OK;
+  // the fused path ping-pongs its state buffers, so a captured graph holds two
+  // steps and returns the pointers to where they started
+  const int unroll = c->md.path == BNZ_PATH_FUSED ? 2 : 1;
+  if (!c->time_on_device) {
+    DtState ds;
+    memset(&ds, 0, sizeof ds);
+    ds.time = c->time;
+    ds.step = c->step;
+    ds.dt = c->last_dt;
+    ds.tmax = tmax;
+    CKC(cudaMemcpyAsync(c->d_ds, &ds, sizeof ds, cudaMemcpyHostToDevice, c->stream));
+  } else {
+    CKC(cudaMemcpyAsync(&c->d_ds->tmax, &tmax, sizeof tmax, cudaMemcpyHostToDevice, c->stream));
+  }
+  auto one_step = [&](void) -> int {
+    StepArgs a = step_args(c);
+    if (!c->md.fixdt) c->launches += c->L->new_dt(a, c->prim, c->d_ds, c->md.cour, 1);
+    else c->launches += c->L->set_dt(c->stream, c->d_ds, c->md.dt_fixed);
+    int rc = step_impl(c, 0.);
+    if (rc) return rc;
+    c->launches += c->L->time_advance(c->stream, c->d_ds);
+    return BNZ_OK;
+  };
+  int full = nsteps / unroll, rest = nsteps % unroll;
+  if (full > 0) {
+    if (!c->graph) {
+      CKC(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      long long before = c->launches;
+      int rc = BNZ_OK;
+      for (int u = 0; u < unroll && rc == BNZ_OK; ++u) rc = one_step();
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+      if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (e != cudaSuccess) return fail(c, BNZ_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&c->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return fail(c, BNZ_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+      c->graph_launches = c->launches - before;
+      c->launches = before;
+    }
+    for (int r = 0; r < full; ++r) {
+      CKC(cudaGraphLaunch(c->graph, c->stream));
+      c->launches += c->graph_launches;
+    }
+  }
+  for (int r = 0; r < rest; ++r) {
+    int rc = one_step();
+    if (rc) return rc;
+  }
+  CKC(cudaGetLastError());
+  c->time_on_device = true;
+  return BNZ_OK;
 }
 
 int bnz_device_state(bnz_ctx* c, double** prim, double** cons, double** bfld) {
@@ -596,6 +682,25 @@ int bnz_device_state(bnz_ctx* c, double** prim, double** cons, double** bfld) {
   if (prim) *prim = c->prim;
   if (cons) *cons = c->cons;
   if (bfld) *bfld = c->bfld;
+  return BNZ_OK;
+}
+
+int bnz_set_stream(bnz_ctx* c, void* stream) {
+  if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
+  CKC(cudaStreamSynchronize(c->stream));
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  c->stream = (cudaStream_t)stream;
+  c->own_stream = false;
+  return BNZ_OK;
+}
+
+int bnz_launch_count(const bnz_ctx* c, long long* n) {
+  if (!c) return BNZ_ERR_ARG;
+  if (n) *n = c->launches;
   return BNZ_OK;
 }
 

@@ -49,7 +49,7 @@ inline void integr_lims(const GridDev& g, int order, int* l) {
 }
 
 template <int AX, int ORDER>
-void launch_flux_rs(const StepArgs& a, const double* w, const double* bf, const plain::Box& b) {
+int launch_flux_rs(const StepArgs& a, const double* w, const double* bf, const plain::Box& b) {
   const int T = 128;
   int nb = nblocks(boxn(b), T);
   switch (a.rsolver) {
@@ -63,40 +63,43 @@ void launch_flux_rs(const StepArgs& a, const double* w, const double* bf, const 
       plain::k_flux<AX, ORDER, dev::RS_HLL><<<nb, T, 0, a.stream>>>(a.g, w, bf, a.flx[AX], b, a.limiter, a.err);
       break;
   }
+  return 1;
 }
 
 template <int AX>
-void launch_flux(const StepArgs& a, int order, const double* w, const double* bf, const plain::Box& b) {
-  if (order == 0) launch_flux_rs<AX, 0>(a, w, bf, b);
-  else launch_flux_rs<AX, 1>(a, w, bf, b);
+int launch_flux(const StepArgs& a, int order, const double* w, const double* bf, const plain::Box& b) {
+  if (order == 0) return launch_flux_rs<AX, 0>(a, w, bf, b);
+  return launch_flux_rs<AX, 1>(a, w, bf, b);
 }
 
 // godunov.pyx:20-209 + 215-252 (integrate_hydro, integrator.pyx:51-79)
-void integrate_hydro(const StepArgs& a, double* u1, const double* u0, const double* w0, const double* b0, int order,
+int integrate_hydro(const StepArgs& a, double* u1, const double* u0, const double* w0, const double* b0, int order,
                      const double* dtp, double fac) {
   const GridDev& g = a.g;
   int l[6];
   integr_lims(g, order, l);
   int il = l[0], iu = l[1], jl = l[2], ju = l[3], kl = l[4], ku = l[5];
+  int nl = 0;
   {  // x faces il..iu+1 on rows jl-1..ju+1, kl-1..ku+1
     int jb = jl - 1, je = ju + 1, kb = kl - 1, ke = ku + 1;
     if (g.dims < 2) jb = je = 0;
     if (g.dims < 3) kb = ke = 0;
-    launch_flux<0>(a, order, w0, b0, mkbox(il, iu + 1, jb, je, kb, ke));
+    nl += launch_flux<0>(a, order, w0, b0, mkbox(il, iu + 1, jb, je, kb, ke));
   }
   if (g.dims >= 2) {
     int kb = kl - 1, ke = ku + 1;
     if (g.dims < 3) kb = ke = 0;
-    launch_flux<1>(a, order, w0, b0, mkbox(il - 1, iu + 1, jl, ju + 1, kb, ke));
+    nl += launch_flux<1>(a, order, w0, b0, mkbox(il - 1, iu + 1, jl, ju + 1, kb, ke));
   }
-  if (g.dims >= 3) launch_flux<2>(a, order, w0, b0, mkbox(il - 1, iu + 1, jl - 1, ju + 1, kl, ku + 1));
+  if (g.dims >= 3) nl += launch_flux<2>(a, order, w0, b0, mkbox(il - 1, iu + 1, jl - 1, ju + 1, kl, ku + 1));
   plain::Box b = mkbox(il, iu, jl, ju, kl, ku);
   plain::k_advance_hydro<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, u1, u0, a.flx[0], a.flx[1], a.flx[2], b,
                                                                         dtp, fac);
+  return nl + 1;
 }
 
 // integrator.pyx:85-126
-void integrate_field(const StepArgs& a, double* u1, double* b1, const double* w0, const double* b0, int order,
+int integrate_field(const StepArgs& a, double* u1, double* b1, const double* w0, const double* b0, int order,
                      const double* dtp, double fac) {
   const GridDev& g = a.g;
   int l[6];
@@ -127,6 +130,7 @@ void integrate_field(const StepArgs& a, double* u1, double* b1, const double* w0
   }
   plain::Box b = mkbox(l[0], l[1], l[2], l[3], l[4], l[5]);
   plain::k_interp_bc<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, u1, b1, b);
+  return 6;
 }
 
 }  // namespace
@@ -135,12 +139,12 @@ void integrate_field(const StepArgs& a, double* u1, double* b1, const double* w0
 // Launchers exported to the host context (declared in bnz_launch.h).
 // ---------------------------------------------------------------------------
 
-void plain_predictor_corrector(const StepArgs& a, const double* dtp) {
+int plain_predictor_corrector(const StepArgs& a, const double* dtp) {
   const GridDev& g = a.g;
   int l[6];
   // predictor (vanleer.pyx:104-120): order 0, dt/2, Us from U, W, B
-  integrate_hydro(a, a.cons_s, a.cons, a.prim, a.bfld, 0, dtp, 0.5);
-  integrate_field(a, a.cons_s, a.bfld_s, a.prim, a.bfld, 0, dtp, 0.5);
+  int nl = integrate_hydro(a, a.cons_s, a.cons, a.prim, a.bfld, 0, dtp, 0.5);
+  nl += integrate_field(a, a.cons_s, a.bfld_s, a.prim, a.bfld, 0, dtp, 0.5);
   integr_lims(g, 0, l);
   {
     plain::Box b = mkbox(l[0], l[1], l[2], l[3], l[4], l[5]);
@@ -148,22 +152,24 @@ void plain_predictor_corrector(const StepArgs& a, const double* dtp) {
   }
   // corrector (vanleer.pyx:130-151): order reconstr_order, dt, U from Ws, Bs
   int order = a.reconstr_order;
-  integrate_hydro(a, a.cons, a.cons, a.prim, a.bfld_s, order, dtp, 1.0);
-  integrate_field(a, a.cons, a.bfld, a.prim, a.bfld, order, dtp, 1.0);
+  nl += integrate_hydro(a, a.cons, a.cons, a.prim, a.bfld_s, order, dtp, 1.0);
+  nl += integrate_field(a, a.cons, a.bfld, a.prim, a.bfld, order, dtp, 1.0);
   integr_lims(g, order, l);
   {
     plain::Box b = mkbox(l[0], l[1], l[2], l[3], l[4], l[5]);
     plain::k_cons2prim<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, a.prim, a.cons, b, a.err);
   }
+  return nl + 2;
 }
 
-void apply_bc(const StepArgs& a, double* prim, double* bfld, unsigned mask) {
+int apply_bc(const StepArgs& a, double* prim, double* bfld, unsigned mask) {
   const GridDev& g = a.g;
   bcdt::FieldList fl;
   fl.n = 0;
   for (int f = 0; f < 12; ++f)
     if (mask & (1u << f)) fl.f[fl.n++] = f;
-  if (fl.n == 0) return;
+  if (fl.n == 0) return 0;
+  int nl = 0;
   for (int ax = 2; ax >= 0; --ax) {
     if (ax >= g.dims) continue;
     const int N[3] = {g.nx, g.ny, g.nz};
@@ -171,48 +177,61 @@ void apply_bc(const StepArgs& a, double* prim, double* bfld, unsigned mask) {
     long long n = 2LL * g.ng * nother;
     dim3 grid(nblocks(n, 256, 4096), fl.n);
     bcdt::k_bc_axis<<<grid, 256, 0, a.stream>>>(g, ax, prim, bfld, fl, a.bc[ax][0], a.bc[ax][1], a.face_aware);
+    ++nl;
   }
+  return nl;
 }
 
-void prim2cons_all(const StepArgs& a) {
+int prim2cons_all(const StepArgs& a) {
   const GridDev& g = a.g;
   plain::Box b = mkbox(0, g.nx - 1, 0, g.ny - 1, 0, g.nz - 1);
   plain::k_prim2cons<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, a.cons, a.prim, b);
+  return 1;
 }
 
-void cons2prim_all(const StepArgs& a) {
+int cons2prim_all(const StepArgs& a) {
   const GridDev& g = a.g;
   plain::Box b = mkbox(0, g.nx - 1, 0, g.ny - 1, 0, g.nz - 1);
   plain::k_cons2prim<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, a.prim, a.cons, b, a.err);
+  return 1;
 }
 
-void interp_bc_active(const StepArgs& a) {
+int interp_bc_active(const StepArgs& a) {
   const GridDev& g = a.g;
   plain::Box b = mkbox(g.i1, g.i2, g.j1, g.j2, g.k1, g.k2);
   plain::k_interp_bc<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, a.prim, a.bfld, b);
+  return 1;
 }
 
-void new_dt(const StepArgs& a, const double* prim, DtState* ds, double cour, int clip) {
+int new_dt(const StepArgs& a, const double* prim, DtState* ds, double cour, int clip) {
   const GridDev& g = a.g;
   long long n = (long long)(g.i2 - g.i1 + 1) * (g.j2 - g.j1 + 1) * (g.k2 - g.k1 + 1);
   bcdt::k_dt_reset<<<1, 1, 0, a.stream>>>(ds);
   bcdt::k_cds_max<<<nblocks(n, 256, 148 * 8), 256, 0, a.stream>>>(g, prim, &ds->cdsmax_bits);
   bcdt::k_dt_finalize<<<1, 1, 0, a.stream>>>(ds, cour, clip);
+  return 3;
 }
 
-void set_dt(cudaStream_t s, DtState* ds, double dt) { bcdt::k_dt_set<<<1, 1, 0, s>>>(ds, dt); }
-void time_advance(cudaStream_t s, DtState* ds) { bcdt::k_time_advance<<<1, 1, 0, s>>>(ds); }
+int set_dt(cudaStream_t s, DtState* ds, double dt) {
+  bcdt::k_dt_set<<<1, 1, 0, s>>>(ds, dt);
+  return 1;
+}
+int time_advance(cudaStream_t s, DtState* ds) {
+  bcdt::k_time_advance<<<1, 1, 0, s>>>(ds);
+  return 1;
+}
 
 // --- conduction ---------------------------------------------------------
 
-void diff_dt_max(const StepArgs& a, const DiffArgs& d, unsigned long long* slot) {
+int diff_dt_max(const StepArgs& a, const DiffArgs& d, unsigned long long* slot) {
   const GridDev& g = a.g;
   long long n = (long long)(g.i2 - g.i1 + 1) * (g.j2 - g.j1 + 1) * (g.k2 - g.k1 + 1);
   diff::k_diff_dt_max<<<nblocks(n, 256, 148 * 8), 256, 0, a.stream>>>(g, a.prim, d.kappa0, slot);
+  return 1;
 }
 
 // thcond_elec.pyx:118-338 (apply_diff_oper)
-void diff_operator(const StepArgs& a, const DiffArgs& d) {
+int diff_operator(const StepArgs& a, const DiffArgs& d) {
   const GridDev& g = a.g;
   diff::k_temp<<<nblocks(g.sv, 256), 256, 0, a.stream>>>(g, a.prim, d.temp);
   int il = 1, iu = g.nx - 2;
@@ -236,9 +255,10 @@ void diff_operator(const StepArgs& a, const DiffArgs& d) {
   int3 lo = make_int3(il, jl, kl), hi = make_int3(iu, ju, ku);
   long long n = (long long)(hi.x - lo.x + 1) * (hi.y - lo.y + 1) * (hi.z - lo.z + 1);
   diff::k_dtemp<<<nblocks(n, 256), 256, 0, a.stream>>>(g, d.fx, d.fy, d.fz, d.dtemp, lo, hi);
+  return 2 + g.dims;
 }
 
-void diff_stage_update(const StepArgs& a, const DiffArgs& d, int first, const double* coef, const double* dtp) {
+int diff_stage_update(const StepArgs& a, const DiffArgs& d, int first, const double* coef, const double* dtp) {
   const GridDev& g = a.g;
   int il = 1, iu = g.nx - 2;
   int jl = g.dims >= 2 ? 1 : 0, ju = g.dims >= 2 ? g.ny - 2 : 0;
@@ -247,9 +267,10 @@ void diff_stage_update(const StepArgs& a, const DiffArgs& d, int first, const do
   long long n = (long long)(hi.x - lo.x + 1) * (hi.y - lo.y + 1) * (hi.z - lo.z + 1);
   diff::k_sts_update<<<nblocks(n, 256), 256, 0, a.stream>>>(g, a.prim, d, lo, hi, first, coef[0], coef[1], coef[2],
                                                               coef[3], dtp);
+  return 1;
 }
 
 // Fused path: not selectable yet (the context rejects BNZ_PATH_FUSED).
-void fused_step(const StepArgs&, const double*) {}
+int fused_step(const StepArgs&, const double*) { return 0; }
 
 }  // namespace BNZ_NS

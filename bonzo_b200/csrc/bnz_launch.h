@@ -5,34 +5,34 @@
 #include "bnz_common.h"
 
 struct Launchers {
-  void (*plain_predictor_corrector)(const StepArgs&, const double* dtp);
-  void (*fused_step)(const StepArgs&, const double* dtp);
-  void (*apply_bc)(const StepArgs&, double* prim, double* bfld, unsigned mask);
-  void (*prim2cons_all)(const StepArgs&);
-  void (*cons2prim_all)(const StepArgs&);
-  void (*interp_bc_active)(const StepArgs&);
-  void (*new_dt)(const StepArgs&, const double* prim, DtState* ds, double cour, int clip);
-  void (*set_dt)(cudaStream_t, DtState*, double);
-  void (*time_advance)(cudaStream_t, DtState*);
-  void (*diff_dt_max)(const StepArgs&, const DiffArgs&, unsigned long long* slot);
-  void (*diff_operator)(const StepArgs&, const DiffArgs&);
-  void (*diff_stage_update)(const StepArgs&, const DiffArgs&, int first, const double* coef, const double* dtp);
+  int (*plain_predictor_corrector)(const StepArgs&, const double* dtp);
+  int (*fused_step)(const StepArgs&, const double* dtp);
+  int (*apply_bc)(const StepArgs&, double* prim, double* bfld, unsigned mask);
+  int (*prim2cons_all)(const StepArgs&);
+  int (*cons2prim_all)(const StepArgs&);
+  int (*interp_bc_active)(const StepArgs&);
+  int (*new_dt)(const StepArgs&, const double* prim, DtState* ds, double cour, int clip);
+  int (*set_dt)(cudaStream_t, DtState*, double);
+  int (*time_advance)(cudaStream_t, DtState*);
+  int (*diff_dt_max)(const StepArgs&, const DiffArgs&, unsigned long long* slot);
+  int (*diff_operator)(const StepArgs&, const DiffArgs&);
+  int (*diff_stage_update)(const StepArgs&, const DiffArgs&, int first, const double* coef, const double* dtp);
 };
 
 #define BNZ_DECLARE_LAUNCHERS(NS)                                                                     \
   namespace NS {                                                                                      \
-  void plain_predictor_corrector(const StepArgs&, const double* dtp);                                \
-  void fused_step(const StepArgs&, const double* dtp);                                               \
-  void apply_bc(const StepArgs&, double* prim, double* bfld, unsigned mask);                         \
-  void prim2cons_all(const StepArgs&);                                                                \
-  void cons2prim_all(const StepArgs&);                                                                \
-  void interp_bc_active(const StepArgs&);                                                             \
-  void new_dt(const StepArgs&, const double* prim, DtState* ds, double cour, int clip);              \
-  void set_dt(cudaStream_t, DtState*, double);                                                        \
-  void time_advance(cudaStream_t, DtState*);                                                          \
-  void diff_dt_max(const StepArgs&, const DiffArgs&, unsigned long long* slot);                      \
-  void diff_operator(const StepArgs&, const DiffArgs&);                                               \
-  void diff_stage_update(const StepArgs&, const DiffArgs&, int first, const double* coef, const double* dtp); \
+  int plain_predictor_corrector(const StepArgs&, const double* dtp);                                \
+  int fused_step(const StepArgs&, const double* dtp);                                               \
+  int apply_bc(const StepArgs&, double* prim, double* bfld, unsigned mask);                         \
+  int prim2cons_all(const StepArgs&);                                                                \
+  int cons2prim_all(const StepArgs&);                                                                \
+  int interp_bc_active(const StepArgs&);                                                             \
+  int new_dt(const StepArgs&, const double* prim, DtState* ds, double cour, int clip);              \
+  int set_dt(cudaStream_t, DtState*, double);                                                        \
+  int time_advance(cudaStream_t, DtState*);                                                          \
+  int diff_dt_max(const StepArgs&, const DiffArgs&, unsigned long long* slot);                      \
+  int diff_operator(const StepArgs&, const DiffArgs&);                                               \
+  int diff_stage_update(const StepArgs&, const DiffArgs&, int first, const double* coef, const double* dtp); \
   extern const Launchers table;                                                                       \
   }
 

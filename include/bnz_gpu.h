@@ -89,9 +89,10 @@ const char* bnz_last_error(const bnz_ctx* ctx);
 int bnz_shape(const bnz_ctx* ctx, int* ntot, int* ng);
 
 /* Upload a full state (the arrays set_problem writes; problem.pyx API,
- * called at src/integration/vanleer.pyx:32).  is_prim=0 means cons is given
- * and is converted to primitives on every cell.  bfld may be NULL to keep the
- * current face field. */
+ * called at src/integration/vanleer.pyx:32).  With is_prim=1 the primitives
+ * are given and cons is derived on every cell (prim2cons); with is_prim=0
+ * cons is given and prim is derived (cons2prim).  bfld may be NULL to keep
+ * the current face field. */
 int bnz_set_state(bnz_ctx* ctx, const double* prim_or_cons, int is_prim, const double* bfld);
 /* init_sim after set_problem (src/integration/vanleer.pyx:41-48): ghost fill,
  * face-to-cell B, ghost fill of cell B, prim2cons everywhere; time = 0. */
@@ -115,7 +116,7 @@ int bnz_diffuse(bnz_ctx* ctx, double dt, int* nsts_out);
  * tmax or max_steps (>0) steps.  The CFL step is computed and clipped to tmax
  * on the device; the host reads back 8 bytes per step to stop the loop. */
 int bnz_advance(bnz_ctx* ctx, double tmax, int max_steps, double* time_out, long* step_out);
-int bnz_get_time(const bnz_ctx* ctx, double* time_out, long* step_out, double* last_dt);
+int bnz_get_time(bnz_ctx* ctx, double* time_out, long* step_out, double* last_dt);
 int bnz_set_time(bnz_ctx* ctx, double time, long step);
 /* Sticky device error word (bits: 1 rho<=0, 2 p<=0, 4 NaN, 8 unordered
  * Riemann fan, 16 timeout); cleared by the call. */
@@ -123,8 +124,11 @@ int bnz_check(bnz_ctx* ctx, uint32_t* err_bits);
 /* Wait for the context's stream. */
 int bnz_sync(bnz_ctx* ctx);
 
-/* Capture one full step (dt from the device CFL, clipped to tmax) into a CUDA
- * graph and replay it n times: vanleer.advance with the host out of the loop. */
+/* vanleer.advance with the host out of the loop: one full step (CFL dt on the
+ * device, clipped to tmax; FIXDT uses dt_fixed) is captured once into a CUDA
+ * graph and replayed nsteps times without host synchronisation.  Steps after
+ * time reaches tmax run with dt = 0.  Not available with conduction
+ * (kappa0 > 0), whose stage count is chosen on the host. */
 int bnz_advance_graph(bnz_ctx* ctx, double tmax, int nsteps);
 
 /* Device pointers of the context's state (prim, cons, bfld), for zero-copy
@@ -132,6 +136,11 @@ int bnz_advance_graph(bnz_ctx* ctx, double tmax, int nsteps);
 int bnz_device_state(bnz_ctx* ctx, double** prim, double** cons, double** bfld);
 /* Raw CUDA stream handle of the context (cudaStream_t as void*). */
 int bnz_stream(bnz_ctx* ctx, void** stream);
+/* Order the context's work on a caller-owned stream (cudaStream_t as void*;
+ * NULL is the legacy default stream).  The caller keeps ownership. */
+int bnz_set_stream(bnz_ctx* ctx, void* stream);
+/* Number of kernels this context has launched so far. */
+int bnz_launch_count(const bnz_ctx* ctx, long long* n);
 
 #ifdef __cplusplus
 }

@@ -788,6 +788,30 @@ void orc_reconstr_flat(int reconstr, int limiter, int char_proj, real *wl, real 
   free(scr_store);
 }
 
+/* Call any reconstruction function with the row ABI on a flat row (the
+ * reference's reconstr_linear reads coordinate arrays from a GridCoord, so a
+ * live simulation's coordinate block is passed). */
+void orc_reconstr_flat_with(orc_reconstr_fn fn, int order, int char_proj, real *wl, real *wr,
+                            const real *w, int n, real gam, void *gc) {
+  real *wrow[3][NM];
+  real **wp[3];
+  real *wlr[NM], *wrr[NM];
+  real *scr_store = (real *)calloc((size_t)8 * NM * (n + 1), sizeof(real));
+  real *scr_rows[8][NM];
+  real **scr[8];
+  for (int d = 0; d < 8; ++d) {
+    for (int m = 0; m < NM; ++m) {
+      if (d < 3) wrow[d][m] = (real *)w + (size_t)m * n + d - order;
+      scr_rows[d][m] = scr_store + ((size_t)d * NM + m) * (n + 1);
+    }
+    if (d < 3) wp[d] = wrow[d];
+    scr[d] = scr_rows[d];
+  }
+  for (int m = 0; m < NM; ++m) { wlr[m] = wl + (size_t)m * (n + 1); wrr[m] = wr + (size_t)m * (n + 1); }
+  fn(wlr, wrr, wp, scr, (orc_coord *)gc, 0, 1, n - 2, 0, 0, char_proj, gam);
+  free(scr_store);
+}
+
 /* ======================================================================
  * Simulation driver
  * ====================================================================== */
@@ -992,6 +1016,7 @@ void orc_destroy(orc_sim *s) {
 }
 
 int orc_ntot(const orc_sim *s, int ax) { return s->gc.Ntot[ax]; }
+void *orc_coord_block(orc_sim *s) { return &s->gc; }
 int orc_ng(const orc_sim *s) { return s->gc.ng; }
 void orc_get_coord(const orc_sim *s, int ax, real *lf, real *lv, real *dlf) {
   int N = s->gc.Ntot[ax];

@@ -131,6 +131,12 @@ orc_sim *orc_create(const orc_params *p);
 void orc_destroy(orc_sim *s);
 int orc_ntot(const orc_sim *s, int ax);
 int orc_ng(const orc_sim *s);
+/* Address of the simulation's GridCoord-compatible coordinate block. */
+void *orc_coord_block(orc_sim *s);
+/* Run a row-ABI reconstruction function (restated or the reference's) on one
+ * row w (NMODE, n): cells 1..n-2, wl/wr (NMODE, n+1), axis x. */
+void orc_reconstr_flat_with(orc_reconstr_fn fn, int order, int char_proj, real *wl, real *wr,
+                            const real *w, int n, real gam, void *gc);
 /* Coordinates (lf has Ntot+1 entries, the others Ntot). */
 void orc_get_coord(const orc_sim *s, int ax, real *lf, real *lv, real *dlf);
 

@@ -85,6 +85,10 @@ def _lib(hydro=False):
                                         C.c_double]
         L.orc_fms.argtypes = [_dp, C.c_double, C.c_double]
         L.orc_fms.restype = C.c_double
+        L.orc_coord_block.argtypes = [C.c_void_p]
+        L.orc_coord_block.restype = C.c_void_p
+        L.orc_reconstr_flat_with.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _dp, _dp, C.c_int,
+                                             C.c_double, C.c_void_p]
         L.orc_get_nsts.argtypes = [C.c_double, C.c_double]
         L.orc_get_nsts.restype = C.c_int
         L.orc_get_sts_coeff.argtypes = [C.c_int, _dp]
@@ -116,6 +120,39 @@ def _rows(a):
     for m in range(n):
         arr[m] = a[m].ctypes.data_as(_dp)
     return arr
+
+
+def ref_row_eos(name, a, gam, hydro=False):
+    """The reference's cons2prim_1 / prim2cons_1 over a flat (NMODE, n) array."""
+    L = ref_lib(hydro)
+    if L is None:
+        raise RuntimeError("oracle/_ref not built")
+    fn = getattr(L, name)
+    fn.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double]
+    a = np.ascontiguousarray(a)
+    out = np.zeros_like(a)
+    fn(_rows(out), _rows(a), 0, a.shape[1] - 1, gam)
+    return out
+
+
+def orc_row_eos(name, a, gam, hydro=False):
+    L = _lib(hydro)
+    fn = getattr(L, "orc_" + name)
+    fn.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double]
+    a = np.ascontiguousarray(a)
+    out = np.zeros_like(a)
+    fn(_rows(out), _rows(a), 0, a.shape[1] - 1, gam)
+    return out
+
+
+def ref_fms(w, gam, hydro=False):
+    L = ref_lib(hydro)
+    if L is None:
+        raise RuntimeError("oracle/_ref not built")
+    L.fms.argtypes = [_dp, C.c_double, C.c_double]
+    L.fms.restype = C.c_double
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    return L.fms(_ptr(w), 0.0, gam)
 
 
 def ref_flux_flat(rsolver, wl, wr, bx, gam, hydro=False):
@@ -151,6 +188,27 @@ def orc_reconstr_flat(reconstr, limiter, w, gam, char_proj=0, hydro=False):
     wr = np.zeros((nm, n + 1))
     L.orc_reconstr_flat(RCN[reconstr], LIM[limiter], char_proj, _ptr(wl), _ptr(wr),
                         _ptr(np.ascontiguousarray(w)), n, gam)
+    return wl, wr
+
+
+def reconstr_with(fn_name, order, w, gam, use_ref=False, hydro=False, char_proj=0):
+    """Run the reference's (use_ref) or the restated reconstruction function
+    `fn_name` ('reconstr_const' / 'reconstr_linear') on one row w (NMODE, n)."""
+    L = _lib(hydro)
+    nm, n = w.shape
+    wl = np.zeros((nm, n + 1))
+    wr = np.zeros((nm, n + 1))
+    if use_ref:
+        R = ref_lib(hydro)
+        if R is None:
+            raise RuntimeError("oracle/_ref not built")
+        fn = C.cast(getattr(R, fn_name), C.c_void_p)
+    else:
+        fn = C.cast(getattr(L, "orc_" + fn_name), C.c_void_p)
+    sim = OracleSim(Nx=max(n, 8), Ny=1, Nz=1, dims=1, hydro=hydro)
+    L.orc_reconstr_flat_with(fn, order, char_proj, _ptr(wl), _ptr(wr), _ptr(np.ascontiguousarray(w)),
+                             n, gam, L.orc_coord_block(sim.h))
+    del sim
     return wl, wr
 
 

@@ -1,0 +1,80 @@
+"""The C-ABI library loads, exports every symbol include/bnz_gpu.h declares and
+rejects bad configurations on the host before any device call (CPU-only)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from bonzo_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    names = []
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if h.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", h)).read()
+            names += re.findall(r"^\s*(?:int|const char\*|void)\s+(bnz_\w+)\s*\(", txt, re.M)
+    return sorted(set(names))
+
+
+def test_header_and_binding_agree():
+    assert sorted(_lib.EXPORTS) == [n for n in header_functions() if n in _lib.EXPORTS]
+    assert set(header_functions()) >= set(_lib.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol():
+    L = C.CDLL(_lib.LIB_PATH)
+    for name in header_functions():
+        assert hasattr(L, name), name
+
+
+def _try_create(**kw):
+    g = _lib.GridDesc()
+    m = _lib.MethodDesc()
+    base = dict(Nx=16, Ny=16, Nz=1, dims=2)
+    base.update({k: v for k, v in kw.items() if k in ("Nx", "Ny", "Nz", "dims")})
+    g.Nx, g.Ny, g.Nz, g.dims = base["Nx"], base["Ny"], base["Nz"], base["dims"]
+    for a in range(3):
+        g.lmax[a] = 1.0
+    for a, sides in enumerate(kw.get("bc", ((0, 0), (0, 0), (0, 0)))):
+        g.bc[a][0], g.bc[a][1] = sides
+    m.gam, m.cour = kw.get("gam", 5. / 3), kw.get("cour", 0.4)
+    m.rsolver, m.reconstr, m.limiter = kw.get("rsolver", 2), 1, kw.get("limiter", 0)
+    m.charact_proj = kw.get("charact_proj", 0)
+    m.kappa0, m.cour_diff = kw.get("kappa0", 0.), 0.5
+    m.path = kw.get("path", 1)
+    L = _lib.load()
+    h = C.c_void_p()
+    rc = L.bnz_create(C.byref(g), C.byref(m), C.byref(h))
+    msg = L.bnz_last_error(h).decode() if h.value else ""
+    if h.value:
+        L.bnz_destroy(h)
+    return rc, msg
+
+
+@pytest.mark.parametrize("kw,frag", [
+    (dict(dims=4), "dims"),
+    (dict(dims=2, Nz=4), "Nz>1"),
+    (dict(gam=1.0), "gam"),
+    (dict(cour=0.0), "cour"),
+    (dict(rsolver=1), "hllc"),
+    (dict(limiter=7), "limiter"),
+    (dict(bc=((0, 1), (0, 0), (0, 0))), "periodic"),
+    (dict(kappa0=-1.0), "kappa0"),
+    (dict(Nx=2), "ng"),
+    (dict(path=5), "path"),
+])
+def test_bad_config_rejected_on_host(kw, frag):
+    rc, msg = _try_create(**kw)
+    assert rc == _lib.BNZ_ERR_ARG
+    assert frag in msg
+
+
+def test_null_arguments():
+    L = _lib.load()
+    assert L.bnz_create(None, None, None) == _lib.BNZ_ERR_ARG
+    assert L.bnz_vl2_step(None, 0.1) == _lib.BNZ_ERR_ARG
+    assert L.bnz_destroy(None) == _lib.BNZ_OK
