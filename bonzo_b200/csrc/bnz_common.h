@@ -48,6 +48,57 @@ struct DtState {
   double tmax;        // clip target
   unsigned long long cdsmax_bits;  // max of (|v|+cf)/dx as a bit pattern
   long long step;
+  unsigned long long cds_bits[2];  // fused path: CFL max of the state of parity p
+};
+
+// Fused 2D path: one grid ("instance") of a batch, as the kernels see it.
+struct FusedInst {
+  int nx, ny;          // Ntot (x, y)
+  int N[2];            // active cells
+  int ng;
+  long long sv;        // variable stride nx*ny
+  double gam;
+  int bc[2][2];
+  int face_aware;
+  const double* dlf[2];
+  const double* dlf_inv[2];
+  const double* lf[2];
+  const double* lv[2];
+  double dlf2;         // z extent of the single z cell
+  double* w[2];        // prim, ping-pong by step parity
+  double* b[2];        // face field, ping-pong
+  double* ws;          // predictor prim
+  double* bs;          // predictor face field
+  DtState* ds;
+};
+
+// A tile of cells [x0, x0+wx) x [y0, y0+wy) (array coordinates) of one instance.
+struct FusedTile {
+  int inst;
+  int x0, y0;
+  int wx, wy;
+};
+
+// Tile shape of the fused kernels (cells per tile along x, y).
+constexpr int FUSED_TX = 32;
+constexpr int FUSED_TY = 8;
+
+// dt modes of the fused step
+enum { FDT_CFL = 0, FDT_EXPLICIT = 1, FDT_FIXED = 2 };
+
+struct FusedLaunch {
+  const FusedInst* insts;
+  int ninst;
+  const FusedTile* tilesA;  // predictor tiles (cells 1..Ntot-2 of each axis)
+  int ntA;
+  const FusedTile* tilesB;  // corrector tiles (active cells)
+  int ntB;
+  int rsolver, limiter;
+  double cour;
+  int dt_mode;
+  double dt_fixed;
+  unsigned* err;
+  cudaStream_t stream;
 };
 
 // Conduction scratch (thcond_elec.pyx DiffScratch).

@@ -35,6 +35,15 @@ struct bnz_ctx {
   double* ee = nullptr;
   double* wnext = nullptr;
   double* bnext = nullptr;
+  // fused path: ping-pong state buffers, tile lists, instance descriptor
+  double* wbuf[2] = {nullptr, nullptr};
+  double* bbuf[2] = {nullptr, nullptr};
+  int parity = 0;
+  bool ghosts_stale = false;  // fused path: ghosts / cons not refreshed since the last step
+  FusedInst* d_inst = nullptr;
+  FusedTile* d_tiles = nullptr;
+  int ntA = 0, ntB = 0;
+  int graph_parity = -1;
   // conduction scratch
   double* dscr = nullptr;
   DiffArgs da;
@@ -54,6 +63,8 @@ struct bnz_ctx {
   double last_dt = 0.;
   long long launches = 0;  // kernels launched through this context
   long long graph_launches = 0;
+  double h_stage[3] = {0., 0., 0.};  // host staging for async copies of the time record
+  long long h_step = 0;
   bool time_on_device = false;  // the device DtState holds the current time
   bool own_stream = true;
 };
@@ -162,15 +173,27 @@ StepArgs step_args(bnz_ctx* c) {
 }
 
 void free_all(bnz_ctx* c) {
-  double** bufs[] = {&c->d_coord, &c->prim, &c->cons, &c->bfld, &c->cons_s, &c->bfld_s, &c->flx[0],
-                     &c->flx[1], &c->flx[2], &c->ec, &c->ee, &c->wnext, &c->bnext, &c->dscr, &c->d_sts};
-  for (double** b : bufs)
-    if (*b) {
-      cudaFree(*b);
-      *b = nullptr;
-    }
+  // every device buffer exactly once (the fused path aliases prim/bfld with its ping-pong pair)
+  double* bufs[] = {c->d_coord, c->prim, c->cons, c->bfld, c->cons_s, c->bfld_s, c->flx[0], c->flx[1], c->flx[2],
+                    c->ec, c->ee, c->wnext, c->bnext, c->dscr, c->d_sts, c->wbuf[0], c->wbuf[1], c->bbuf[0],
+                    c->bbuf[1]};
+  const int nb = sizeof bufs / sizeof bufs[0];
+  for (int q = 0; q < nb; ++q) {
+    if (!bufs[q]) continue;
+    bool seen = false;
+    for (int r = 0; r < q; ++r) seen |= bufs[r] == bufs[q];
+    if (!seen) cudaFree(bufs[q]);
+  }
+  c->d_coord = c->prim = c->cons = c->bfld = c->cons_s = c->bfld_s = c->ec = c->ee = nullptr;
+  c->wnext = c->bnext = c->dscr = c->d_sts = nullptr;
+  for (int d = 0; d < 3; ++d) c->flx[d] = nullptr;
+  c->wbuf[0] = c->wbuf[1] = c->bbuf[0] = c->bbuf[1] = nullptr;
   if (c->d_err) cudaFree(c->d_err);
   if (c->d_ds) cudaFree(c->d_ds);
+  if (c->d_inst) cudaFree(c->d_inst);
+  if (c->d_tiles) cudaFree(c->d_tiles);
+  c->d_inst = nullptr;
+  c->d_tiles = nullptr;
   if (c->graph) cudaGraphExecDestroy(c->graph);
   if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
   c->d_err = nullptr;
@@ -179,7 +202,91 @@ void free_all(bnz_ctx* c) {
   c->stream = nullptr;
 }
 
-bool fused_available(const bnz_grid_desc*, const bnz_method_desc*) { return false; }
+// The fused kernels cover 2D grids with PLM (the corrector is order 1).
+bool fused_available(const bnz_grid_desc* g, const bnz_method_desc* m) {
+  return g->dims == 2 && m->reconstr == BNZ_RCN_LINEAR;
+}
+
+// Tiles of FUSED_TX x FUSED_TY cells over the active range; the predictor's
+// edge tiles also cover the two ghost rings it updates (cells 1..Ntot-2).
+void make_tiles(int inst, int N0, int N1, int ng, bool pred, std::vector<FusedTile>& out) {
+  const int T[2] = {FUSED_TX, FUSED_TY};
+  const int N[2] = {N0, N1};
+  int nt[2];
+  for (int a = 0; a < 2; ++a) nt[a] = (N[a] + T[a] - 1) / T[a];
+  for (int ty = 0; ty < nt[1]; ++ty)
+    for (int tx = 0; tx < nt[0]; ++tx) {
+      int lo[2], hi[2];  // inclusive, array coordinates
+      const int t[2] = {tx, ty};
+      for (int a = 0; a < 2; ++a) {
+        lo[a] = ng + t[a] * T[a];
+        hi[a] = std::min(ng + (t[a] + 1) * T[a], ng + N[a]) - 1;
+        if (pred) {
+          if (t[a] == 0) lo[a] = 1;
+          if (t[a] == nt[a] - 1) hi[a] = N[a] + 2 * ng - 2;
+        }
+      }
+      FusedTile ft;
+      ft.inst = inst;
+      ft.x0 = lo[0];
+      ft.y0 = lo[1];
+      ft.wx = hi[0] - lo[0] + 1;
+      ft.wy = hi[1] - lo[1] + 1;
+      out.push_back(ft);
+    }
+}
+
+FusedInst make_inst(const bnz_ctx* c) {
+  FusedInst I;
+  memset(&I, 0, sizeof I);
+  I.nx = c->Ntot[0];
+  I.ny = c->Ntot[1];
+  I.N[0] = c->i2 - c->i1 + 1;
+  I.N[1] = c->j2 - c->j1 + 1;
+  I.ng = c->ng;
+  I.sv = (long long)c->ncell;
+  I.gam = c->md.gam;
+  for (int a = 0; a < 2; ++a) {
+    I.bc[a][0] = c->gd.bc[a][0];
+    I.bc[a][1] = c->gd.bc[a][1];
+    I.dlf[a] = c->g.dlf[a];
+    I.dlf_inv[a] = c->g.dlf_inv[a];
+    I.lf[a] = c->g.lf[a];
+    I.lv[a] = c->g.lv[a];
+  }
+  I.face_aware = c->md.outflow_face_aware;
+  I.dlf2 = c->dlf[2][0];
+  I.w[0] = c->wbuf[0];
+  I.w[1] = c->wbuf[1];
+  I.b[0] = c->bbuf[0];
+  I.b[1] = c->bbuf[1];
+  I.ws = c->cons_s;
+  I.bs = c->bfld_s;
+  I.ds = c->d_ds;
+  return I;
+}
+
+int ensure_ghosts(bnz_ctx* c);
+int refresh_cds(bnz_ctx* c);
+
+FusedLaunch fused_launch(const bnz_ctx* c, int dt_mode) {
+  FusedLaunch f;
+  memset(&f, 0, sizeof f);
+  f.insts = c->d_inst;
+  f.ninst = 1;
+  f.tilesA = c->d_tiles;
+  f.ntA = c->ntA;
+  f.tilesB = c->d_tiles + c->ntA;
+  f.ntB = c->ntB;
+  f.rsolver = c->md.rsolver;
+  f.limiter = c->md.limiter;
+  f.cour = c->md.cour;
+  f.dt_mode = dt_mode;
+  f.dt_fixed = c->md.dt_fixed;
+  f.err = c->d_err;
+  f.stream = c->stream;
+  return f;
+}
 
 int validate(const bnz_grid_desc* g, const bnz_method_desc* m, std::string& why) {
   if (g->dims < 1 || g->dims > 3) return why = "dims must be 1, 2 or 3", 0;
@@ -331,6 +438,12 @@ int bnz_create(const bnz_grid_desc* gd, const bnz_method_desc* md, bnz_ctx** out
   } else {
     ALLOC(c->wnext, n9);
     ALLOC(c->bnext, n3);
+    ALLOC(c->cons_s, n9);   // predictor prim ws
+    ALLOC(c->bfld_s, n3);   // predictor faces bs
+    c->wbuf[0] = c->prim;
+    c->wbuf[1] = c->wnext;
+    c->bbuf[0] = c->bfld;
+    c->bbuf[1] = c->bnext;
   }
   if (md->kappa0 > 0.) {
     ALLOC(c->dscr, 8 * c->ncell * sizeof(double));
@@ -351,6 +464,21 @@ int bnz_create(const bnz_grid_desc* gd, const bnz_method_desc* md, bnz_ctx** out
   }
   e = cudaMalloc((void**)&c->d_err, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_ds, sizeof(DtState));
+  if (e == cudaSuccess && md->path == BNZ_PATH_FUSED) {
+    std::vector<FusedTile> tiles;
+    make_tiles(0, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, ng, true, tiles);
+    c->ntA = (int)tiles.size();
+    make_tiles(0, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, ng, false, tiles);
+    c->ntB = (int)tiles.size() - c->ntA;
+    e = cudaMalloc((void**)&c->d_tiles, tiles.size() * sizeof(FusedTile));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_inst, sizeof(FusedInst));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(c->d_tiles, tiles.data(), tiles.size() * sizeof(FusedTile), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      FusedInst I = make_inst(c);
+      e = cudaMemcpy(c->d_inst, &I, sizeof I, cudaMemcpyHostToDevice);
+    }
+  }
   if (e != cudaSuccess) {
     c->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
     free_all(c);
@@ -364,6 +492,8 @@ int bnz_create(const bnz_grid_desc* gd, const bnz_method_desc* md, bnz_ctx** out
   cudaMemsetAsync(c->bfld, 0, n3, c->stream);
   if (c->cons_s) cudaMemsetAsync(c->cons_s, 0, n9, c->stream);
   if (c->bfld_s) cudaMemsetAsync(c->bfld_s, 0, n3, c->stream);
+  if (c->wnext) cudaMemsetAsync(c->wnext, 0, n9, c->stream);
+  if (c->bnext) cudaMemsetAsync(c->bnext, 0, n3, c->stream);
   for (int d = 0; d < dims; ++d)
     if (c->flx[d]) cudaMemsetAsync(c->flx[d], 0, n9, c->stream);
   e = cudaStreamSynchronize(c->stream);
@@ -401,6 +531,9 @@ int bnz_set_state(bnz_ctx* c, const double* pc, int is_prim, const double* bfld)
   StepArgs a = step_args(c);
   if (is_prim) c->launches += c->L->prim2cons_all(a);
   else c->launches += c->L->cons2prim_all(a);
+  c->ghosts_stale = false;
+  int rc = refresh_cds(c);
+  if (rc) return rc;
   CKC(cudaGetLastError());
   CKC(cudaStreamSynchronize(c->stream));
   return BNZ_OK;
@@ -416,15 +549,21 @@ int bnz_init(bnz_ctx* c) {
   DtState ds;
   memset(&ds, 0, sizeof ds);
   CKC(cudaMemcpyAsync(c->d_ds, &ds, sizeof ds, cudaMemcpyHostToDevice, c->stream));
+  c->ghosts_stale = false;
+  int rc = refresh_cds(c);
+  if (rc) return rc;
   CKC(cudaGetLastError());
   CKC(cudaStreamSynchronize(c->stream));
   c->time = 0.;
   c->step = 0;
+  c->time_on_device = false;
   return BNZ_OK;
 }
 
 int bnz_get_state(bnz_ctx* c, double* prim, double* cons, double* bfld) {
   if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
+  int rc = ensure_ghosts(c);
+  if (rc) return rc;
   size_t n9 = 9 * c->ncell * sizeof(double), n3 = 3 * c->ncell * sizeof(double);
   if (prim) CKC(cudaMemcpyAsync(prim, c->prim, n9, cudaMemcpyDeviceToHost, c->stream));
   if (cons) CKC(cudaMemcpyAsync(cons, c->cons, n9, cudaMemcpyDeviceToHost, c->stream));
@@ -436,6 +575,8 @@ int bnz_get_state(bnz_ctx* c, double* prim, double* cons, double* bfld) {
 int bnz_apply_bc(bnz_ctx* c, uint32_t mask) {
   if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
   if (mask & ~0xFFFu) return fail(c, BNZ_ERR_ARG, "var_mask has bits above 11");
+  int rc = ensure_ghosts(c);
+  if (rc) return rc;
   StepArgs a = step_args(c);
   c->launches += c->L->apply_bc(a, c->prim, c->bfld, mask);
   CKC(cudaGetLastError());
@@ -453,6 +594,8 @@ int bnz_new_dt(bnz_ctx* c, double* dt_out) {
   if (dt_out) *dt_out = ds.dt;
   return BNZ_OK;
 }
+
+}  // extern "C"
 
 namespace {
 
@@ -506,35 +649,78 @@ int diffuse_impl(bnz_ctx* c, const double* dtp, double dt_hyp, int* nsts_out) {
   return BNZ_OK;
 }
 
-// vanleer.pyx:101-163 with dt already in d_ds->dt
-int step_impl(bnz_ctx* c, double dt_host) {
+// Fill ghosts and cons of the fused path's current state (what the
+// reference's end-of-step BC + prim2cons leave behind, vanleer.pyx:162-163).
+int ensure_ghosts(bnz_ctx* c) {
+  if (!c->ghosts_stale) return BNZ_OK;
+  StepArgs a = step_args(c);
+  c->launches += c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
+  c->launches += c->L->prim2cons_all(a);
+  CKC(cudaGetLastError());
+  c->ghosts_stale = false;
+  return BNZ_OK;
+}
+
+// CFL max of the current state into the fused slot of the current parity.
+int refresh_cds(bnz_ctx* c) {
+  if (c->md.path != BNZ_PATH_FUSED) return BNZ_OK;
+  CKC(cudaMemsetAsync(&c->d_ds->cds_bits[c->parity], 0, sizeof(unsigned long long), c->stream));
+  c->launches += c->L->fused_cds(fused_launch(c, FDT_EXPLICIT), c->parity);
+  CKC(cudaGetLastError());
+  return BNZ_OK;
+}
+
+void set_parity(bnz_ctx* c, int p) {
+  c->parity = p;
+  c->prim = c->wbuf[p];
+  c->bfld = c->bbuf[p];
+}
+
+// vanleer.pyx:101-163 with dt already in d_ds->dt.  dt_mode selects how the
+// fused path obtains dt (explicit host value, device CFL, or FIXDT).
+int step_impl(bnz_ctx* c, double dt_host, int dt_mode = FDT_EXPLICIT) {
   StepArgs a = step_args(c);
   const double* dtp = &c->d_ds->dt;
   if (c->md.path == BNZ_PATH_PLAIN) {
     c->launches += c->L->plain_predictor_corrector(a, dtp);
   } else {
-    c->launches += c->L->fused_step(a, dtp);
-    // the fused kernel writes the next state into the second buffers
-    std::swap(c->prim, c->wnext);
-    std::swap(c->bfld, c->bnext);
+    c->launches += c->L->fused_step(fused_launch(c, dt_mode), c->parity);
+    set_parity(c, c->parity ^ 1);
+    c->ghosts_stale = true;
     a = step_args(c);
   }
   CKC(cudaGetLastError());
-  int rc = diffuse_impl(c, dtp, dt_host, nullptr);
-  if (rc) return rc;
-  c->launches += c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
-  c->launches += c->L->prim2cons_all(a);
+  if (c->md.kappa0 > 0.) {
+    int rc = diffuse_impl(c, dtp, dt_host, nullptr);
+    if (rc) return rc;
+    if (c->md.path == BNZ_PATH_FUSED) {
+      rc = refresh_cds(c);
+      if (rc) return rc;
+    }
+  }
+  if (c->md.path == BNZ_PATH_PLAIN) {
+    c->launches += c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
+    c->launches += c->L->prim2cons_all(a);
+  }
   CKC(cudaGetLastError());
   return BNZ_OK;
 }
 
 }  // namespace
 
+extern "C" {
+
 int bnz_diffuse(bnz_ctx* c, double dt, int* nsts_out) {
   if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
   if (!(dt >= 0.)) return fail(c, BNZ_ERR_ARG, "dt must be >= 0");
   c->launches += c->L->set_dt(c->stream, c->d_ds, dt);
-  return diffuse_impl(c, &c->d_ds->dt, dt, nsts_out);
+  int rc = diffuse_impl(c, &c->d_ds->dt, dt, nsts_out);
+  if (rc) return rc;
+  if (c->md.path == BNZ_PATH_FUSED) {
+    c->ghosts_stale = true;  // cons no longer matches prim
+    rc = refresh_cds(c);
+  }
+  return rc;
 }
 
 int bnz_vl2_step(bnz_ctx* c, double dt) {
@@ -624,28 +810,41 @@ int bnz_advance_graph(bnz_ctx* c, double tmax, int nsteps) {
   // steps and returns the pointers to where they started
   const int unroll = c->md.path == BNZ_PATH_FUSED ? 2 : 1;
   if (!c->time_on_device) {
-    DtState ds;
-    memset(&ds, 0, sizeof ds);
-    ds.time = c->time;
-    ds.step = c->step;
-    ds.dt = c->last_dt;
-    ds.tmax = tmax;
-    CKC(cudaMemcpyAsync(c->d_ds, &ds, sizeof ds, cudaMemcpyHostToDevice, c->stream));
+    // dt, time, tmax are the first three doubles of DtState; step follows cdsmax_bits
+    double h[3] = {c->last_dt, c->time, tmax};
+    long long st = c->step;
+    c->h_stage[0] = h[0];
+    c->h_stage[1] = h[1];
+    c->h_stage[2] = h[2];
+    c->h_step = st;
+    CKC(cudaMemcpyAsync(c->d_ds, c->h_stage, 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CKC(cudaMemcpyAsync(&c->d_ds->step, &c->h_step, sizeof(long long), cudaMemcpyHostToDevice, c->stream));
   } else {
-    CKC(cudaMemcpyAsync(&c->d_ds->tmax, &tmax, sizeof tmax, cudaMemcpyHostToDevice, c->stream));
+    c->h_stage[2] = tmax;
+    CKC(cudaMemcpyAsync(&c->d_ds->tmax, &c->h_stage[2], sizeof(double), cudaMemcpyHostToDevice, c->stream));
   }
   auto one_step = [&](void) -> int {
-    StepArgs a = step_args(c);
-    if (!c->md.fixdt) c->launches += c->L->new_dt(a, c->prim, c->d_ds, c->md.cour, 1);
-    else c->launches += c->L->set_dt(c->stream, c->d_ds, c->md.dt_fixed);
-    int rc = step_impl(c, 0.);
+    int rc;
+    if (c->md.path == BNZ_PATH_FUSED) {
+      rc = step_impl(c, 0., c->md.fixdt ? FDT_FIXED : FDT_CFL);
+    } else {
+      StepArgs a = step_args(c);
+      if (!c->md.fixdt) c->launches += c->L->new_dt(a, c->prim, c->d_ds, c->md.cour, 1);
+      else c->launches += c->L->set_dt(c->stream, c->d_ds, c->md.dt_fixed);
+      rc = step_impl(c, 0.);
+    }
     if (rc) return rc;
     c->launches += c->L->time_advance(c->stream, c->d_ds);
     return BNZ_OK;
   };
   int full = nsteps / unroll, rest = nsteps % unroll;
   if (full > 0) {
+    if (c->graph && c->graph_parity != c->parity) {
+      cudaGraphExecDestroy(c->graph);
+      c->graph = nullptr;
+    }
     if (!c->graph) {
+      c->graph_parity = c->parity;
       CKC(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
       long long before = c->launches;
       int rc = BNZ_OK;
@@ -662,11 +861,15 @@ int bnz_advance_graph(bnz_ctx* c, double tmax, int nsteps) {
       if (e != cudaSuccess) return fail(c, BNZ_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
       c->graph_launches = c->launches - before;
       c->launches = before;
+      // capture recorded the pointer swaps of `unroll` steps; replaying starts
+      // from the parity it was captured at
+      set_parity(c, c->graph_parity);
     }
     for (int r = 0; r < full; ++r) {
       CKC(cudaGraphLaunch(c->graph, c->stream));
       c->launches += c->graph_launches;
     }
+    if (c->md.path == BNZ_PATH_FUSED) c->ghosts_stale = true;
   }
   for (int r = 0; r < rest; ++r) {
     int rc = one_step();

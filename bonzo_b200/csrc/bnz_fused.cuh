@@ -1,3 +1,559 @@
-// bnz_fused.cuh -- fused tile kernels (filled in below).
+// bnz_fused.cuh -- fused tile kernels of the 2D VL2 step (predictor, corrector)
+// and their batched launch over many independent grids.
+//
+// One step is three launches for the whole batch:
+//   k_dt_batch  per-instance CFL dt = cour / max(|v|+c_f)/dx (+ tmax clip),
+//               from the max the previous corrector accumulated;
+//   k_pred2d    predictor (vanleer.pyx:104-120): per tile, donor-cell HLLD
+//               fluxes -> shared memory, CT corner EMFs -> shared memory, then
+//               per cell the half-step conserved update, the half-step faces
+//               and cons2prim; writes ws (9) and bs (3) on the predictor range
+//               (cells 1..Ntot-2 of every active axis);
+//   k_corr2d    corrector (vanleer.pyx:130-151): per active tile, PLM + HLLD
+//               fluxes from ws/bs, EMFs, the full-step update of u^n and B^n,
+//               cons2prim; writes the new prim and face field, and reduces the
+//               next step's CFL max into the instance's slot.
+// u^n is rebuilt as prim2cons(w^n), which is bitwise what the reference keeps
+// in its cons array between steps (vanleer.pyx:163).  Ghost values are never
+// stored: loads outside the active range go through the boundary-condition
+// index map (the source index and sign grid_bc_funcs.pyx / util_bc.pyx would
+// copy), so no ghost-fill pass runs between steps.
+// Included inside the per-floating-point-mode namespace.
 #pragma once
-namespace fused {}
+
+namespace fused {
+
+using namespace dev;
+
+using Inst = FusedInst;
+using Tile = FusedTile;
+
+// ---------------------------------------------------------------------------
+// boundary-condition index maps (grid_bc_funcs.pyx:36-330, util_bc.pyx)
+// ---------------------------------------------------------------------------
+
+struct AxisMap {
+  int a1, a2, n, f0, f1, face_aware;
+};
+
+__device__ __forceinline__ AxisMap axis_map(const Inst& I, int ax) {
+  AxisMap m;
+  m.a1 = I.ng;
+  m.a2 = I.ng + I.N[ax] - 1;
+  m.n = I.N[ax];
+  m.f0 = I.bc[ax][0];
+  m.f1 = I.bc[ax][1];
+  m.face_aware = I.face_aware;
+  return m;
+}
+
+// cell-centred along this axis: source index, sign flips for the normal component
+__device__ __forceinline__ int map_cell(int a, const AxisMap& m, bool& flip) {
+  flip = false;
+  if (a < m.a1) {
+    if (m.f0 == 0) return a + m.n;
+    if (m.f0 == 1) return m.a1;
+    flip = true;
+    return 2 * m.a1 - 1 - a;
+  }
+  if (a > m.a2) {
+    if (m.f1 == 0) return a - m.n;
+    if (m.f1 == 1) return m.a2;
+    flip = true;
+    return 2 * m.a2 + 1 - a;
+  }
+  return a;
+}
+
+// face-centred along this axis (the face normal to it)
+__device__ __forceinline__ int map_face(int a, const AxisMap& m, bool& flip, bool& zero) {
+  flip = false;
+  zero = false;
+  if (a < m.a1) {
+    if (m.f0 == 0) return a + m.n;
+    if (m.f0 == 1) return m.a1;
+    flip = true;
+    return 2 * m.a1 - a;
+  }
+  if (a == m.a1 && m.f0 == 2) {
+    zero = true;
+    return a;
+  }
+  if (a > m.a2) {
+    if (m.f1 == 0) return a - m.n;
+    if (m.f1 == 1) {
+      if (!m.face_aware) return m.a2;
+      return a == m.a2 + 1 ? a : m.a2 + 1;
+    }
+    if (a == m.a2 + 1) {
+      zero = true;
+      return a;
+    }
+    flip = true;
+    return 2 * m.a2 + 2 - a;
+  }
+  return a;
+}
+
+// prim at cell (i, j) with ghost indices mapped; local sweep order along AX
+template <int AX>
+__device__ __forceinline__ void load_prim(const Inst& I, const double* __restrict__ w, int i, int j,
+                                          const AxisMap& mx, const AxisMap& my, bool interior, double* out) {
+  bool fx = false, fy = false;
+  int si = i, sj = j;
+  if (!interior) {
+    si = map_cell(i, mx, fx);
+    sj = map_cell(j, my, fy);
+  }
+  const long long c = (long long)sj * I.nx + si;
+#pragma unroll
+  for (int n = 0; n < NM; ++n) {
+    const int gv = plain::perm<AX>(n);
+    if (n == BX) continue;  // the normal component comes from the face array
+    double v = w[gv * I.sv + c];
+    if ((fx && (gv == VX || gv == BX)) || (fy && (gv == VY || gv == BY))) v = -v;
+    out[n] = v;
+  }
+}
+
+__device__ __forceinline__ void load_prim_all(const Inst& I, const double* __restrict__ w, int i, int j,
+                                              const AxisMap& mx, const AxisMap& my, bool interior, double* out) {
+  bool fx = false, fy = false;
+  int si = i, sj = j;
+  if (!interior) {
+    si = map_cell(i, mx, fx);
+    sj = map_cell(j, my, fy);
+  }
+  const long long c = (long long)sj * I.nx + si;
+#pragma unroll
+  for (int n = 0; n < NM; ++n) {
+    double v = w[n * I.sv + c];
+    if ((fx && (n == VX || n == BX)) || (fy && (n == VY || n == BY))) v = -v;
+    out[n] = v;
+  }
+}
+
+// face component COMP at (i, j) with ghost indices mapped
+template <int COMP>
+__device__ __forceinline__ double load_face(const Inst& I, const double* __restrict__ b, int i, int j,
+                                            const AxisMap& mx, const AxisMap& my, bool interior) {
+  if (interior) return b[COMP * I.sv + (long long)j * I.nx + i];
+  bool f1 = false, f2 = false, z1 = false, z2 = false;
+  int si, sj;
+  if (COMP == 0) {
+    si = map_face(i, mx, f1, z1);
+    sj = map_cell(j, my, f2);
+    f2 = false;  // tangential along y
+  } else if (COMP == 1) {
+    si = map_cell(i, mx, f1);
+    f1 = false;
+    sj = map_face(j, my, f2, z2);
+  } else {
+    si = map_cell(i, mx, f1);
+    sj = map_cell(j, my, f2);
+    f1 = f2 = false;
+  }
+  if (z1 || z2) return 0.;
+  double v = b[COMP * I.sv + (long long)sj * I.nx + si];
+  return (f1 != f2) ? -v : v;
+}
+
+// ---------------------------------------------------------------------------
+// shared-memory layout of one tile
+// ---------------------------------------------------------------------------
+
+constexpr int NF = 8;  // stored flux values: 6 hydro + 2 field (for the EMFs)
+
+struct Layout {
+  int wx, wy;
+  int nfx, nfy, nec, nee;
+  __device__ __forceinline__ void set(int wx_, int wy_) {
+    wx = wx_;
+    wy = wy_;
+    nfx = (wx + 1) * (wy + 2);
+    nfy = (wx + 2) * (wy + 1);
+    nec = (wx + 2) * (wy + 2);
+    nee = (wx + 1) * (wy + 1);
+  }
+  // x faces i = x0..x0+wx, rows j = y0-1..y0+wy
+  __device__ __forceinline__ int fx(int fi, int fj) const { return (fj + 1) * (wx + 1) + fi; }
+  // y faces j = y0..y0+wy, columns i = x0-1..x0+wx
+  __device__ __forceinline__ int fy(int fi, int fj) const { return fj * (wx + 2) + fi + 1; }
+  // cells i = x0-1..x0+wx, j = y0-1..y0+wy
+  __device__ __forceinline__ int ec(int ci, int cj) const { return (cj + 1) * (wx + 2) + ci + 1; }
+  // corners i = x0..x0+wx, j = y0..y0+wy
+  __device__ __forceinline__ int ee(int ci, int cj) const { return cj * (wx + 1) + ci; }
+};
+
+template <int TXM, int TYM>
+struct Smem {
+  static constexpr int NFX = (TXM + 1) * (TYM + 2);
+  static constexpr int NFY = (TXM + 2) * (TYM + 1);
+  static constexpr int NEC = (TXM + 2) * (TYM + 2);
+  static constexpr int NEE = (TXM + 1) * (TYM + 1);
+  static constexpr size_t bytes = sizeof(double) * ((size_t)NF * (NFX + NFY) + NEC + NEE);
+};
+
+// ---------------------------------------------------------------------------
+// Stage 1 of both kernels: interface fluxes and cell-centred EMF.
+// ORDER 0 (predictor): donor cell from w (ghosts mapped), normal B from b.
+// ORDER 1 (corrector): PLM from ws, normal B from bs (no ghost mapping: the
+// predictor wrote cells 1..Ntot-2).
+// ---------------------------------------------------------------------------
+
+template <int ORDER, int RS>
+__device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const Layout& L, const double* __restrict__ w,
+                                             const double* __restrict__ b, double* sFX, double* sFY, double* sEC,
+                                             int lim, bool interior, unsigned& err) {
+  const AxisMap mx = axis_map(I, 0), my = axis_map(I, 1);
+  const int total = L.nfx + L.nfy + L.nec;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    if (t < L.nfx) {
+      // x face at column i (between cells i-1 and i), row j
+      const int fi = t % (L.wx + 1), fj = t / (L.wx + 1) - 1;
+      const int i = T.x0 + fi, j = T.y0 + fj;
+      double wL[NM], wR[NM];
+      if (ORDER == 0) {
+        load_prim<0>(I, w, i - 1, j, mx, my, interior, wL);
+        load_prim<0>(I, w, i, j, mx, my, interior, wR);
+        wL[BX] = wR[BX] = load_face<0>(I, b, i, j, mx, my, interior);
+      } else {
+        const long long c = (long long)j * I.nx + i;
+#pragma unroll
+        for (int n = 0; n < NM; ++n) {
+          if (n == BX) continue;
+          const double* a = w + n * I.sv + c;
+          double wm2 = a[-2], wm1 = a[-1], w0 = a[0], wp1 = a[1];
+          wL[n] = wm1 + plain::half_slope_rt(lim, wm2, wm1, w0);
+          wR[n] = w0 - plain::half_slope_rt(lim, wm1, w0, wp1);
+        }
+        wL[BX] = wR[BX] = b[c];
+      }
+      double f[NM];
+      riemann<RS>(f, wL, wR, I.gam, err);
+      const int q = L.fx(fi, fj);
+#pragma unroll
+      for (int n = 0; n < 6; ++n) sFX[n * L.nfx + q] = f[n];
+      sFX[6 * L.nfx + q] = f[BY];  // fx[BY]
+      sFX[7 * L.nfx + q] = f[BZ];  // fx[BZ]
+    } else if (t < L.nfx + L.nfy) {
+      // y face at row j (between cells j-1 and j), column i; sweep frame AX = 1
+      const int u = t - L.nfx;
+      const int fi = u % (L.wx + 2) - 1, fj = u / (L.wx + 2);
+      const int i = T.x0 + fi, j = T.y0 + fj;
+      double wL[NM], wR[NM];
+      if (ORDER == 0) {
+        load_prim<1>(I, w, i, j - 1, mx, my, interior, wL);
+        load_prim<1>(I, w, i, j, mx, my, interior, wR);
+        wL[BX] = wR[BX] = load_face<1>(I, b, i, j, mx, my, interior);
+      } else {
+        const long long c = (long long)j * I.nx + i;
+        const long long s = I.nx;
+#pragma unroll
+        for (int n = 0; n < NM; ++n) {
+          if (n == BX) continue;
+          const double* a = w + plain::perm<1>(n) * I.sv + c;
+          double wm2 = a[-2 * s], wm1 = a[-s], w0 = a[0], wp1 = a[s];
+          wL[n] = wm1 + plain::half_slope_rt(lim, wm2, wm1, w0);
+          wR[n] = w0 - plain::half_slope_rt(lim, wm1, w0, wp1);
+        }
+        wL[BX] = wR[BX] = b[I.sv + c];
+      }
+      double f[NM];
+      riemann<RS>(f, wL, wR, I.gam, err);
+      // local -> global (godunov.pyx:297-324 for the y sweep)
+      const int q = L.fy(fi, fj);
+      sFY[0 * L.nfy + q] = f[RHO];
+      sFY[1 * L.nfy + q] = f[VZ];   // global MX
+      sFY[2 * L.nfy + q] = f[VX];   // global MY
+      sFY[3 * L.nfy + q] = f[VY];   // global MZ
+      sFY[4 * L.nfy + q] = f[EN];
+      sFY[5 * L.nfy + q] = f[PSC];
+      sFY[6 * L.nfy + q] = f[BZ];   // fy[BX]
+      sFY[7 * L.nfy + q] = f[BY];   // fy[BZ]
+    } else {
+      // cell-centred E_z = -(vx by - vy bx) (ct.pyx:148)
+      const int u = t - L.nfx - L.nfy;
+      const int ci = u % (L.wx + 2) - 1, cj = u / (L.wx + 2) - 1;
+      const int i = T.x0 + ci, j = T.y0 + cj;
+      double vx, vy, bxc, byc;
+      if (ORDER == 0 && !interior) {
+        double ww[NM];
+        load_prim_all(I, w, i, j, mx, my, false, ww);
+        vx = ww[VX]; vy = ww[VY]; bxc = ww[BX]; byc = ww[BY];
+      } else {
+        const long long c = (long long)j * I.nx + i;
+        vx = w[VX * I.sv + c]; vy = w[VY * I.sv + c]; bxc = w[BX * I.sv + c]; byc = w[BY * I.sv + c];
+      }
+      sEC[L.ec(ci, cj)] = -(vx * byc - vy * bxc);
+    }
+  }
+}
+
+// corner E_z (ct.pyx:204-207)
+__device__ __forceinline__ void stage_emf(const Layout& L, const double* sFX, const double* sFY, const double* sEC,
+                                          double* sEE) {
+  for (int t = threadIdx.x; t < L.nee; t += blockDim.x) {
+    const int ci = t % (L.wx + 1), cj = t / (L.wx + 1);
+    sEE[t] = (0.5 * (-sFX[6 * L.nfx + L.fx(ci, cj - 1)] - sFX[6 * L.nfx + L.fx(ci, cj)] +
+                     sFY[6 * L.nfy + L.fy(ci - 1, cj)] + sFY[6 * L.nfy + L.fy(ci, cj)]) -
+              0.25 * (sEC[L.ec(ci - 1, cj)] + sEC[L.ec(ci, cj)] + sEC[L.ec(ci - 1, cj - 1)] + sEC[L.ec(ci, cj - 1)]));
+  }
+}
+
+// Stage 3: per cell, the conserved update (godunov.pyx:215-252), the face
+// update (ct.pyx:15-91), face-to-cell B (ct.pyx:96-123) and cons2prim.
+// Returns the new primitive state and the cell's four (five) new faces.
+struct CellOut {
+  double w[NM];
+  double bxl, bxr, byb, byt, bz;
+};
+
+__device__ __forceinline__ void stage_cell(const Inst& I, const Layout& L, const Tile& T, int ci, int cj,
+                                           const double* un, double bxl0, double bxr0, double byb0, double byt0,
+                                           double bz0, const double* sFX, const double* sFY, const double* sEE,
+                                           double dt, CellOut& o) {
+  const int i = T.x0 + ci, j = T.y0 + cj;
+  const double dx = I.dlf[0][i], dy = I.dlf[1][j], dz = I.dlf2;
+  double vol = dx * dy * dz;
+  double dtdv = dt / vol;
+  double dax = dy * dz;
+  double day = dx * dz;
+  double u[NM];
+  const int ql = L.fx(ci, cj), qr = L.fx(ci + 1, cj);
+  const int qb = L.fy(ci, cj), qt = L.fy(ci, cj + 1);
+#pragma unroll
+  for (int n = 0; n < 6; ++n) {
+    double v = un[n] - dtdv * (dax * sFX[n * L.nfx + qr] - dax * sFX[n * L.nfx + ql]);
+    v -= dtdv * (day * sFY[n * L.nfy + qt] - day * sFY[n * L.nfy + qb]);
+    u[n] = v;
+  }
+  // faces (2D: E_z at corners, E_y = fx[BZ] on x faces, E_x = -fy[BZ] on y faces)
+  const double e00 = sEE[L.ee(ci, cj)], e10 = sEE[L.ee(ci + 1, cj)];
+  const double e01 = sEE[L.ee(ci, cj + 1)], e11 = sEE[L.ee(ci + 1, cj + 1)];
+  double dtda = dt / (dy * dz);
+  o.bxl = bxl0 - dtda * (dz * e01 - dz * e00);
+  o.bxr = bxr0 - dtda * (dz * e11 - dz * e10);
+  dtda = dt / (dx * dz);
+  o.byb = byb0 + dtda * (dz * e10 - dz * e00);
+  o.byt = byt0 + dtda * (dz * e11 - dz * e01);
+  dtda = dt / (dx * dy);
+  const double eyl = sFX[7 * L.nfx + ql], eyr = sFX[7 * L.nfx + qr];
+  const double exb = -sFY[7 * L.nfy + qb], ext = -sFY[7 * L.nfy + qt];
+  double bz = bz0 - dtda * (dy * eyr - dy * eyl);
+  bz += dtda * (dx * ext - dx * exb);
+  o.bz = bz;
+  u[BX] = ((I.lv[0][i] - I.lf[0][i]) * o.bxl + (I.lf[0][i + 1] - I.lv[0][i]) * o.bxr) * I.dlf_inv[0][i];
+  u[BY] = ((I.lv[1][j] - I.lf[1][j]) * o.byb + (I.lf[1][j + 1] - I.lv[1][j]) * o.byt) * I.dlf_inv[1][j];
+  u[BZ] = bz;
+  cons2prim(o.w, u, I.gam);
+}
+
+template <int TXM, int TYM, int RS>
+__global__ void __launch_bounds__(256) k_pred2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
+                                                int parity, int lim, unsigned* err) {
+  extern __shared__ double smem[];
+  const Tile T = tiles[blockIdx.x];
+  const Inst& I = insts[T.inst];
+  const double dtf = I.ds->dt;
+  if (!(dtf > 0.)) return;
+  const double dt = 0.5 * dtf;
+  Layout L;
+  L.set(T.wx, T.wy);
+  double* sFX = smem;
+  double* sFY = sFX + NF * Smem<TXM, TYM>::NFX;
+  double* sEC = sFY + NF * Smem<TXM, TYM>::NFY;
+  double* sEE = sEC + Smem<TXM, TYM>::NEC;
+  const double* __restrict__ w = I.w[parity];
+  const double* __restrict__ b = I.b[parity];
+  // a tile whose one-cell ring lies inside the active range needs no ghost mapping
+  const bool interior = T.x0 - 1 >= I.ng && T.x0 + T.wx <= I.ng + I.N[0] - 1 && T.y0 - 1 >= I.ng &&
+                        T.y0 + T.wy <= I.ng + I.N[1] - 1;
+  unsigned e = 0;
+  stage_fluxes<0, RS>(I, T, L, w, b, sFX, sFY, sEC, lim, interior, e);
+  __syncthreads();
+  stage_emf(L, sFX, sFY, sEC, sEE);
+  __syncthreads();
+  const AxisMap mx = axis_map(I, 0), my = axis_map(I, 1);
+  const int ilast = I.nx - 2, jlast = I.ny - 2;  // last predictor cell (vanleer lims)
+  for (int t = threadIdx.x; t < T.wx * T.wy; t += blockDim.x) {
+    const int ci = t % T.wx, cj = t / T.wx;
+    const int i = T.x0 + ci, j = T.y0 + cj;
+    double wn[NM], un[NM];
+    load_prim_all(I, w, i, j, mx, my, interior, wn);
+    prim2cons(un, wn, I.gam);
+    double bxl0 = load_face<0>(I, b, i, j, mx, my, interior);
+    double bxr0 = load_face<0>(I, b, i + 1, j, mx, my, interior);
+    double byb0 = load_face<1>(I, b, i, j, mx, my, interior);
+    double byt0 = load_face<1>(I, b, i, j + 1, mx, my, interior);
+    double bz0 = load_face<2>(I, b, i, j, mx, my, interior);
+    CellOut o;
+    stage_cell(I, L, T, ci, cj, un, bxl0, bxr0, byb0, byt0, bz0, sFX, sFY, sEE, dt, o);
+    const long long c = (long long)j * I.nx + i;
+#pragma unroll
+    for (int n = 0; n < NM; ++n) I.ws[n * I.sv + c] = o.w[n];
+    I.bs[c] = o.bxl;
+    I.bs[I.sv + c] = o.byb;
+    I.bs[2 * I.sv + c] = o.bz;
+    if (i == ilast) I.bs[c + 1] = o.bxr;
+    if (j == jlast) I.bs[I.sv + c + I.nx] = o.byt;
+  }
+  if (e) atomicOr(err, e);
+}
+
+__device__ __forceinline__ void copy_tile(const Inst& I, const Tile& T, int parity) {
+  const int i2 = I.ng + I.N[0] - 1, j2 = I.ng + I.N[1] - 1;
+  const double* w = I.w[parity];
+  const double* b = I.b[parity];
+  double* w1 = I.w[parity ^ 1];
+  double* b1 = I.b[parity ^ 1];
+  for (int t = threadIdx.x; t < T.wx * T.wy; t += blockDim.x) {
+    const int i = T.x0 + t % T.wx, j = T.y0 + t / T.wx;
+    const long long c = (long long)j * I.nx + i;
+#pragma unroll
+    for (int n = 0; n < NM; ++n) w1[n * I.sv + c] = w[n * I.sv + c];
+    for (int n = 0; n < 3; ++n) b1[n * I.sv + c] = b[n * I.sv + c];
+    if (i == i2) b1[c + 1] = b[c + 1];
+    if (j == j2) b1[I.sv + c + I.nx] = b[I.sv + c + I.nx];
+  }
+}
+
+template <int TXM, int TYM, int RS>
+__global__ void __launch_bounds__(256) k_corr2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
+                                                int parity, int lim, double cour, unsigned* err) {
+  extern __shared__ double smem[];
+  __shared__ double red[8];
+  const Tile T = tiles[blockIdx.x];
+  const Inst& I = insts[T.inst];
+  const double dt = I.ds->dt;
+  if (!(dt > 0.)) {
+    // time has reached tmax: carry the state over unchanged
+    copy_tile(I, T, parity);
+    return;
+  }
+  Layout L;
+  L.set(T.wx, T.wy);
+  double* sFX = smem;
+  double* sFY = sFX + NF * Smem<TXM, TYM>::NFX;
+  double* sEC = sFY + NF * Smem<TXM, TYM>::NFY;
+  double* sEE = sEC + Smem<TXM, TYM>::NEC;
+  unsigned e = 0;
+  stage_fluxes<1, RS>(I, T, L, I.ws, I.bs, sFX, sFY, sEC, lim, true, e);
+  __syncthreads();
+  stage_emf(L, sFX, sFY, sEC, sEE);
+  __syncthreads();
+  const double* __restrict__ w = I.w[parity];
+  const double* __restrict__ b = I.b[parity];
+  double* __restrict__ w1 = I.w[parity ^ 1];
+  double* __restrict__ b1 = I.b[parity ^ 1];
+  const AxisMap mx = axis_map(I, 0), my = axis_map(I, 1);
+  const int i2 = I.ng + I.N[0] - 1, j2 = I.ng + I.N[1] - 1;
+  double cmax = 0.;
+  for (int t = threadIdx.x; t < T.wx * T.wy; t += blockDim.x) {
+    const int ci = t % T.wx, cj = t / T.wx;
+    const int i = T.x0 + ci, j = T.y0 + cj;
+    const long long c = (long long)j * I.nx + i;
+    double wn[NM], un[NM];
+#pragma unroll
+    for (int n = 0; n < NM; ++n) wn[n] = w[n * I.sv + c];
+    prim2cons(un, wn, I.gam);
+    // B^n on the cell's faces; the upper boundary face goes through the BC map
+    const bool edge = (i == i2) || (j == j2) || (i == I.ng) || (j == I.ng);
+    double bxl0 = load_face<0>(I, b, i, j, mx, my, !edge);
+    double bxr0 = load_face<0>(I, b, i + 1, j, mx, my, !edge);
+    double byb0 = load_face<1>(I, b, i, j, mx, my, !edge);
+    double byt0 = load_face<1>(I, b, i, j + 1, mx, my, !edge);
+    double bz0 = b[2 * I.sv + c];
+    CellOut o;
+    stage_cell(I, L, T, ci, cj, un, bxl0, bxr0, byb0, byt0, bz0, sFX, sFY, sEE, dt, o);
+    e |= plain::check_prim(o.w);
+#pragma unroll
+    for (int n = 0; n < NM; ++n) w1[n * I.sv + c] = o.w[n];
+    b1[c] = o.bxl;
+    b1[I.sv + c] = o.byb;
+    b1[2 * I.sv + c] = o.bz;
+    if (i == i2) b1[c + 1] = o.bxr;
+    if (j == j2) b1[I.sv + c + I.nx] = o.byt;
+    // next step's CFL (new_dt.pyx:55-99) on the new state
+    double vf = fms(o.w, I.gam);
+    double cx = fabs(o.w[VX]) + vf, cy = fabs(o.w[VY]) + vf;
+    double cds = fmax(fmax(cx / I.dlf[0][i], cy / I.dlf[1][j]), 0. / I.dlf2);
+    if (cds > cmax) cmax = cds;
+  }
+  for (int o = 16; o > 0; o >>= 1) cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) red[wid] = cmax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) m = fmax(m, red[q]);
+    if (m > 0.) atomicMax(&I.ds->cds_bits[parity ^ 1], (unsigned long long)__double_as_longlong(m));
+  }
+  if (e) atomicOr(err, e);
+}
+
+// Per-instance dt for the step of parity p (new_dt.pyx:117, vanleer.pyx:95-96):
+// FDT_CFL  cour / max of slot p, clipped to tmax;
+// FDT_FIXED dt_fixed (the FIXDT build), clipped to tmax;
+// FDT_EXPLICIT keeps the dt the host wrote (bnz_vl2_step).
+// Clears the slot the corrector fills for the next step.
+__global__ void k_dt_batch(const Inst* __restrict__ insts, int n, int parity, double cour, int mode, double dt_fixed) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  DtState* ds = insts[q].ds;
+  if (mode != FDT_EXPLICIT) {
+    double dt;
+    if (mode == FDT_FIXED) {
+      dt = dt_fixed;
+    } else {
+      double m = __longlong_as_double((long long)ds->cds_bits[parity]);
+      dt = cour / m;
+      if (ds->time + dt > ds->tmax) dt = ds->tmax - ds->time;
+    }
+    if (ds->time >= ds->tmax) dt = 0.;
+    ds->dt = dt;
+  }
+  ds->cds_bits[parity ^ 1] = 0ULL;
+}
+
+__global__ void k_time_batch(const Inst* __restrict__ insts, int n) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  DtState* ds = insts[q].ds;
+  if (ds->dt > 0.) {
+    ds->time += ds->dt;
+    ds->step += 1;
+  }
+}
+
+// CFL max of the current state into slot `parity` (new_dt.pyx:18-135): the
+// first step of a run, or after the state was replaced.
+__global__ void k_cds_batch(const Inst* __restrict__ insts, const Tile* __restrict__ tiles, int parity) {
+  __shared__ double red[8];
+  const Tile T = tiles[blockIdx.x];
+  const Inst& I = insts[T.inst];
+  const double* w = I.w[parity];
+  double cmax = 0.;
+  for (int t = threadIdx.x; t < T.wx * T.wy; t += blockDim.x) {
+    const int i = T.x0 + t % T.wx, j = T.y0 + t / T.wx;
+    const long long c = (long long)j * I.nx + i;
+    double ww[NM];
+#pragma unroll
+    for (int n = 0; n < NM; ++n) ww[n] = w[n * I.sv + c];
+    double vf = fms(ww, I.gam);
+    double cx = fabs(ww[VX]) + vf, cy = fabs(ww[VY]) + vf;
+    double cds = fmax(fmax(cx / I.dlf[0][i], cy / I.dlf[1][j]), 0. / I.dlf2);
+    if (cds > cmax) cmax = cds;
+  }
+  for (int o = 16; o > 0; o >>= 1) cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) red[wid] = cmax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) m = fmax(m, red[q]);
+    if (m > 0.) atomicMax(&I.ds->cds_bits[parity], (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+}  // namespace fused

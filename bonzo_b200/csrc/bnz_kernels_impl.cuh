@@ -270,7 +270,53 @@ int diff_stage_update(const StepArgs& a, const DiffArgs& d, int first, const dou
   return 1;
 }
 
-// Fused path: not selectable yet (the context rejects BNZ_PATH_FUSED).
-int fused_step(const StepArgs&, const double*) { return 0; }
+// --- fused 2D path (one launch per stage for the whole batch) --------------
+
+namespace {
+constexpr int FA_TX = FUSED_TX + 4, FA_TY = FUSED_TY + 4;  // predictor tiles grow by the ghost rings
+constexpr size_t SMEM_A = fused::Smem<FA_TX, FA_TY>::bytes;
+constexpr size_t SMEM_B = fused::Smem<FUSED_TX, FUSED_TY>::bytes;
+
+template <int RS>
+void set_smem_attrs() {
+  static bool done = false;
+  if (done) return;
+  cudaFuncSetAttribute(fused::k_pred2d<FA_TX, FA_TY, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_A);
+  cudaFuncSetAttribute(fused::k_corr2d<FUSED_TX, FUSED_TY, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)SMEM_B);
+  done = true;
+}
+
+template <int RS>
+void launch_pred_corr(const FusedLaunch& f, int parity) {
+  set_smem_attrs<RS>();
+  fused::k_pred2d<FA_TX, FA_TY, RS><<<f.ntA, 256, SMEM_A, f.stream>>>(f.insts, f.tilesA, parity, f.limiter, f.err);
+  fused::k_corr2d<FUSED_TX, FUSED_TY, RS><<<f.ntB, 256, SMEM_B, f.stream>>>(f.insts, f.tilesB, parity, f.limiter,
+                                                                          f.cour, f.err);
+}
+}  // namespace
+
+int fused_step(const FusedLaunch& f, int parity) {
+  fused::k_dt_batch<<<(f.ninst + 127) / 128, 128, 0, f.stream>>>(f.insts, f.ninst, parity, f.cour, f.dt_mode,
+                                                                  f.dt_fixed);
+  switch (f.rsolver) {
+    case dev::RS_HLLD: launch_pred_corr<dev::RS_HLLD>(f, parity); break;
+    case dev::RS_HLLT: launch_pred_corr<dev::RS_HLLT>(f, parity); break;
+    default: launch_pred_corr<dev::RS_HLL>(f, parity); break;
+  }
+  return 3;
+}
+
+int fused_time(const FusedLaunch& f) {
+  fused::k_time_batch<<<(f.ninst + 127) / 128, 128, 0, f.stream>>>(f.insts, f.ninst);
+  return 1;
+}
+
+// CFL max of the current state into slot `parity` (needed before the first
+// fused step and after the state was replaced or diffused).
+int fused_cds(const FusedLaunch& f, int parity) {
+  fused::k_cds_batch<<<f.ntB, 256, 0, f.stream>>>(f.insts, f.tilesB, parity);
+  return 1;
+}
 
 }  // namespace BNZ_NS

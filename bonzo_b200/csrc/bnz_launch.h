@@ -6,7 +6,9 @@
 
 struct Launchers {
   int (*plain_predictor_corrector)(const StepArgs&, const double* dtp);
-  int (*fused_step)(const StepArgs&, const double* dtp);
+  int (*fused_step)(const FusedLaunch&, int parity);
+  int (*fused_time)(const FusedLaunch&);
+  int (*fused_cds)(const FusedLaunch&, int parity);
   int (*apply_bc)(const StepArgs&, double* prim, double* bfld, unsigned mask);
   int (*prim2cons_all)(const StepArgs&);
   int (*cons2prim_all)(const StepArgs&);
@@ -22,7 +24,9 @@ struct Launchers {
 #define BNZ_DECLARE_LAUNCHERS(NS)                                                                     \
   namespace NS {                                                                                      \
   int plain_predictor_corrector(const StepArgs&, const double* dtp);                                \
-  int fused_step(const StepArgs&, const double* dtp);                                               \
+  int fused_step(const FusedLaunch&, int parity);                                                    \
+  int fused_time(const FusedLaunch&);                                                                 \
+  int fused_cds(const FusedLaunch&, int parity);                                                      \
   int apply_bc(const StepArgs&, double* prim, double* bfld, unsigned mask);                         \
   int prim2cons_all(const StepArgs&);                                                                \
   int cons2prim_all(const StepArgs&);                                                                \
@@ -40,7 +44,8 @@ BNZ_DECLARE_LAUNCHERS(exact)
 BNZ_DECLARE_LAUNCHERS(fast)
 
 #define BNZ_DEFINE_TABLE(NS)                                                                          \
-  const Launchers NS::table = {NS::plain_predictor_corrector, NS::fused_step, NS::apply_bc,          \
+  const Launchers NS::table = {NS::plain_predictor_corrector, NS::fused_step, NS::fused_time,       \
+                               NS::fused_cds, NS::apply_bc,                                           \
                                NS::prim2cons_all, NS::cons2prim_all, NS::interp_bc_active,           \
                                NS::new_dt, NS::set_dt, NS::time_advance, NS::diff_dt_max,            \
                                NS::diff_operator, NS::diff_stage_update};

@@ -20,6 +20,16 @@ def setup_case(name, n=32, reconstr="linear", seed=0):
         gc = P.make_grid(n, n, 1, dims=2, bc=1, reconstr=reconstr)
         prim, bfld = P.blast(gc, b_angle=0.7, center=(0.45, 0.55, 0.5), p_ratio=30.)
         opts = dict(dims=2, bc=((1, 1), (1, 1), (1, 1)), gam=5. / 3, cour=0.4)
+    elif name == "blast_reflect":
+        gc = P.make_grid(n, n, 1, dims=2, bc=2, reconstr=reconstr)
+        prim, bfld = P.blast(gc, b_angle=0.3, center=(0.4, 0.6, 0.5), p_ratio=20.)
+        prim[1][gc.active] = 0.3
+        prim[2][gc.active] = -0.2
+        opts = dict(dims=2, bc=((2, 2), (2, 2), (2, 2)), gam=5. / 3, cour=0.4)
+    elif name == "mixed_bc":
+        gc = P.make_grid(n, n, 1, dims=2, bc=((0, 0), (1, 1), (0, 0)), reconstr=reconstr)
+        prim, bfld = P.otvortex(gc)
+        opts = dict(dims=2, bc=((0, 0), (1, 1), (0, 0)), gam=5. / 3, cour=0.4)
     elif name == "turb3d":
         gc = P.make_grid(n, n, n, dims=3, bc=0, reconstr=reconstr)
         prim, bfld = P.turbulence3d(gc, seed=seed, kmax=min(16, n // 3))
