@@ -38,10 +38,11 @@ BYTES_PER_ZONE = 192  # 9 conserved + 3 face-B doubles read once and written onc
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--path", default="plain", choices=["plain", "fused"])
+    ap.add_argument("--path", default="batch", choices=["batch", "plain", "fused"])
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain per-instance comparison")
     ap.add_argument("--instances", type=int, default=64)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -177,50 +178,88 @@ def run_cpu_reference(batch, steps, warmup):
 # our arm
 # ---------------------------------------------------------------------------
 
+def _timed(stream, step_fn, steps, dist):
+    import torch
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(steps):
+        step_fn()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
+def make_engine(kind, batch, stream):
+    """kind 'batch': one bnz_batch for all instances (one launch per stage);
+    'plain' / 'fused': one context per instance, one graph launch per instance."""
+    from bonzo_b200._lib import Batch, Context
+    if kind == "batch":
+        grids = [dict(Nx=q["N"], Ny=q["N"], Nz=1, dims=2, bc=METHOD["bc"]) for q, _, _, _ in batch]
+        meth = {k: v for k, v in METHOD.items() if k not in ("dims", "bc")}
+        eng = Batch(grids, **meth)
+        eng.set_stream(stream.cuda_stream)
+        ctxs = eng.instances
+        step = lambda: eng.advance(1e30, 1)
+        count = eng.launch_count
+    else:
+        ctxs = []
+        for q, gc, prim, bfld in batch:
+            c = Context(Nx=q["N"], Ny=q["N"], Nz=1, path=kind, **METHOD)
+            c.set_stream(stream.cuda_stream)
+            ctxs.append(c)
+        eng = ctxs
+
+        def step():
+            for c in ctxs:
+                c.advance_graph(1e30, 1)
+
+        count = lambda: sum(c.launch_count() for c in ctxs)
+    for c, (q, gc, prim, bfld) in zip(ctxs, batch):
+        c.set_state(prim, bfld)
+        c.init()
+    return eng, ctxs, step, count
+
+
 def run_ours(args, rank, world, dist):
     import torch
-    from bonzo_b200._lib import Context
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
     batch = build_batch(args.instances, args.seed)
     zones = sum(q["N"] ** 2 for q, _, _, _ in batch)
     stream = torch.cuda.Stream()
-    ctxs = []
-    for q, gc, prim, bfld in batch:
-        c = Context(Nx=q["N"], Ny=q["N"], Nz=1, path=args.path, **METHOD)
-        c.set_stream(stream.cuda_stream)
-        c.set_state(prim, bfld)
-        c.init()
-        ctxs.append(c)
 
-    def one_step():
+    # the plain one-instance-per-launch path (the comparison the headline quotes)
+    plain_ms = None
+    if args.path == "batch" and not args.no_plain:
+        eng, ctxs, step, count = make_engine("plain", batch, stream)
+        for _ in range(args.warmup):
+            step()
+        plain_steps = max(3, args.steps // 4)
+        plain_ms = _timed(stream, step, plain_steps, dist) / plain_steps
         for c in ctxs:
-            c.advance_graph(1e30, 1)
-
-    for _ in range(args.warmup):
-        one_step()
-    torch.cuda.synchronize()
-    launches0 = sum(c.launch_count() for c in ctxs)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(dev) as clk:
-        with torch.cuda.stream(stream):
-            ev0.record(stream)
-            for _ in range(args.steps):
-                one_step()
-            ev1.record(stream)
+            c.check()
+        del eng, ctxs, step, count
         torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    ms = ev0.elapsed_time(ev1)
-    launches = sum(c.launch_count() for c in ctxs) - launches0
-    ms_max = ms
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+        torch.cuda.empty_cache()
+
+    eng, ctxs, step, count = make_engine(args.path, batch, stream)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = count()
+    with ClockSampler(dev) as clk:
+        ms_max = _timed(stream, step, args.steps, dist)
+    launches = count() - launches0
     ms_step = ms_max / args.steps
     value = world * zones * args.steps / (ms_max * 1e-3) / 1e6
 
@@ -229,27 +268,19 @@ def run_ours(args, rank, world, dist):
     for c in ctxs:
         P = torch.empty((9,) + c.shape, dtype=torch.float64, pin_memory=True).numpy()
         B = torch.empty((3,) + c.shape, dtype=torch.float64, pin_memory=True).numpy()
-        P[...], _, B[...] = c.get_state(prim=True, cons=False, bfld=True)
+        c.get_state_into(P, None, B)
         host.append((P, B))
     h2d = sum(P.nbytes + B.nbytes for P, B in host)
     ke = max(1, args.e2e_steps)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(ke):
+
+    def e2e_step():
         for c, (P, B) in zip(ctxs, host):
             c.set_state(P, B)
-            c.advance_graph(1e30, 1)
+        step()
+        for c, (P, B) in zip(ctxs, host):
             c.get_state_into(P, None, B)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ems = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ems], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ems = float(t.item())
+
+    ems = _timed(stream, e2e_step, ke, dist)
     e2e = world * zones * ke / (ems * 1e-3) / 1e6
     for c in ctxs:
         c.check()
@@ -277,12 +308,17 @@ def run_ours(args, rank, world, dist):
                    "parallelism": "instances sharded per GPU (dp%d, no collective)" % world},
         "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(h2d),
-                "how": "bnz_set_state + bnz_advance_graph + bnz_get_state per instance per step, "
-                       "pinned host buffers"},
+                "how": "bnz_set_state of every instance, one batch step, bnz_get_state of every "
+                       "instance, pinned host buffers"},
         "gpu_launches": int(launches),
         "roofline": roofline,
         "clocks": clk.record(),
     }
+    if plain_ms is not None:
+        pv = world * zones / (plain_ms * 1e-3) / 1e6
+        line["plain_one_instance_per_launch"] = {"value": round(pv, 3), "unit": UNIT,
+                                                 "ms_per_step": round(plain_ms, 4)}
+        line["batched_vs_plain"] = round(value / pv, 3)
     return line
 
 

@@ -27,6 +27,9 @@ EXPORTS = [
     "bnz_get_state", "bnz_apply_bc", "bnz_new_dt", "bnz_vl2_step", "bnz_diffuse", "bnz_advance",
     "bnz_get_time", "bnz_set_time", "bnz_check", "bnz_sync", "bnz_advance_graph",
     "bnz_device_state", "bnz_stream", "bnz_set_stream", "bnz_launch_count",
+    "bnz_batch_create", "bnz_batch_destroy", "bnz_batch_last_error", "bnz_batch_size",
+    "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_set_stream", "bnz_batch_launch_count",
+    "bnz_batch_sync",
 ]
 
 
@@ -86,6 +89,16 @@ def load():
     L.bnz_stream.argtypes = [vp, C.POINTER(vp)]
     L.bnz_set_stream.argtypes = [vp, vp]
     L.bnz_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    L.bnz_batch_create.argtypes = [C.POINTER(GridDesc), C.c_int, C.POINTER(MethodDesc), C.POINTER(vp)]
+    L.bnz_batch_destroy.argtypes = [vp]
+    L.bnz_batch_last_error.argtypes = [vp]
+    L.bnz_batch_last_error.restype = C.c_char_p
+    L.bnz_batch_size.argtypes = [vp, C.POINTER(C.c_int)]
+    L.bnz_batch_instance.argtypes = [vp, C.c_int, C.POINTER(vp)]
+    L.bnz_batch_advance.argtypes = [vp, C.c_double, C.c_int]
+    L.bnz_batch_set_stream.argtypes = [vp, vp]
+    L.bnz_batch_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    L.bnz_batch_sync.argtypes = [vp]
     _lib = L
     return L
 
@@ -97,42 +110,58 @@ def _p(a):
     return a.ctypes.data_as(_dp)
 
 
-class Context:
-    """One grid on the device (owns a bnz_ctx)."""
+def grid_desc(Nx, Ny=1, Nz=1, dims=2, lmin=(0., 0., 0.), lmax=(1., 1., 1.),
+              bc=((0, 0), (0, 0), (0, 0))):
+    g = GridDesc()
+    g.Nx, g.Ny, g.Nz, g.dims = Nx, Ny, Nz, dims
+    for a in range(3):
+        g.lmin[a], g.lmax[a] = lmin[a], lmax[a]
+        g.bc[a][0], g.bc[a][1] = bc[a][0], bc[a][1]
+    return g
 
-    def __init__(self, Nx, Ny=1, Nz=1, dims=2, lmin=(0., 0., 0.), lmax=(1., 1., 1.),
-                 bc=((0, 0), (0, 0), (0, 0)), gam=5. / 3, cour=0.4, rsolver="hlld",
-                 reconstr="linear", limiter="vl", charact_proj=0, kappa0=0.0,
-                 thcond_type="aniso", sat_hfe=0, cour_diff=0.5, fixdt=False, dt_fixed=0.0,
-                 outflow_face_aware=1, exact_fp=False, path="plain"):
+
+def method_desc(gam=5. / 3, cour=0.4, rsolver="hlld", reconstr="linear", limiter="vl",
+                charact_proj=0, kappa0=0.0, thcond_type="aniso", sat_hfe=0, cour_diff=0.5,
+                fixdt=False, dt_fixed=0.0, outflow_face_aware=1, exact_fp=False, path="plain"):
+    m = MethodDesc()
+    m.gam, m.cour = gam, cour
+    m.rsolver = RS[rsolver] if isinstance(rsolver, str) else rsolver
+    m.reconstr = RCN[reconstr] if isinstance(reconstr, str) else reconstr
+    m.limiter = LIM[limiter] if isinstance(limiter, str) else limiter
+    m.charact_proj = charact_proj
+    m.kappa0, m.thcond_type, m.sat_hfe, m.cour_diff = kappa0, TC[thcond_type], sat_hfe, cour_diff
+    m.fixdt, m.dt_fixed = int(bool(fixdt)), dt_fixed
+    m.outflow_face_aware, m.exact_fp = outflow_face_aware, int(bool(exact_fp))
+    m.path = PATH[path] if isinstance(path, str) else path
+    return m
+
+
+_GRID_KEYS = ("Nx", "Ny", "Nz", "dims", "lmin", "lmax", "bc")
+
+
+class Context:
+    """One grid on the device (owns a bnz_ctx, or views an instance of a Batch)."""
+
+    def __init__(self, Nx=None, Ny=1, Nz=1, dims=2, lmin=(0., 0., 0.), lmax=(1., 1., 1.),
+                 bc=((0, 0), (0, 0), (0, 0)), _handle=None, _owner=None, **method):
         self.L = load()
-        g = GridDesc()
-        g.Nx, g.Ny, g.Nz, g.dims = Nx, Ny, Nz, dims
-        for a in range(3):
-            g.lmin[a], g.lmax[a] = lmin[a], lmax[a]
-            g.bc[a][0], g.bc[a][1] = bc[a][0], bc[a][1]
-        m = MethodDesc()
-        m.gam, m.cour = gam, cour
-        m.rsolver = RS[rsolver] if isinstance(rsolver, str) else rsolver
-        m.reconstr = RCN[reconstr] if isinstance(reconstr, str) else reconstr
-        m.limiter = LIM[limiter] if isinstance(limiter, str) else limiter
-        m.charact_proj = charact_proj
-        m.kappa0, m.thcond_type, m.sat_hfe, m.cour_diff = kappa0, TC[thcond_type], sat_hfe, cour_diff
-        m.fixdt, m.dt_fixed = int(bool(fixdt)), dt_fixed
-        m.outflow_face_aware, m.exact_fp = outflow_face_aware, int(bool(exact_fp))
-        m.path = PATH[path] if isinstance(path, str) else path
-        self.grid_desc, self.method_desc = g, m
-        h = C.c_void_p()
-        rc = self.L.bnz_create(C.byref(g), C.byref(m), C.byref(h))
-        self.h = h
-        if rc != BNZ_OK:
-            msg = self.L.bnz_last_error(h).decode() if h.value else "bnz_create failed"
-            self.L.bnz_destroy(h)
-            self.h = C.c_void_p()
-            raise BnzError(rc, msg)
+        if _handle is not None:
+            self.h, self._owner, self._owns = _handle, _owner, False
+        else:
+            g = grid_desc(Nx, Ny, Nz, dims, lmin, lmax, bc)
+            m = method_desc(**method)
+            self.grid_desc, self.method_desc = g, m
+            h = C.c_void_p()
+            rc = self.L.bnz_create(C.byref(g), C.byref(m), C.byref(h))
+            self.h, self._owner, self._owns = h, None, True
+            if rc != BNZ_OK:
+                msg = self.L.bnz_last_error(h).decode() if h.value else "bnz_create failed"
+                self.L.bnz_destroy(h)
+                self.h = C.c_void_p()
+                raise BnzError(rc, msg)
         nt = (C.c_int * 3)()
         ng = C.c_int()
-        self.L.bnz_shape(h, nt, C.byref(ng))
+        self.L.bnz_shape(self.h, nt, C.byref(ng))
         self.shape = (nt[2], nt[1], nt[0])
         self.ng = ng.value
 
@@ -141,7 +170,7 @@ class Context:
             raise BnzError(rc, self.L.bnz_last_error(self.h).decode())
 
     def close(self):
-        if getattr(self, "h", None) is not None and self.h.value:
+        if getattr(self, "_owns", False) and self.h.value:
             self.L.bnz_destroy(self.h)
             self.h = C.c_void_p()
 
@@ -237,3 +266,66 @@ class Context:
         s = C.c_void_p()
         self._ck(self.L.bnz_stream(self.h, C.byref(s)))
         return s.value
+
+
+class Batch:
+    """Many independent 2D grids of uneven size with one method, advanced by
+    one launch per stage (bnz_batch_* in include/bnz_gpu.h)."""
+
+    def __init__(self, grids, **method):
+        self.L = load()
+        n = len(grids)
+        arr = (GridDesc * n)()
+        for q, gkw in enumerate(grids):
+            arr[q] = grid_desc(**gkw)
+        m = method_desc(**method)
+        h = C.c_void_p()
+        rc = self.L.bnz_batch_create(arr, n, C.byref(m), C.byref(h))
+        self.h = h
+        if rc != BNZ_OK:
+            msg = self.L.bnz_batch_last_error(h).decode() if h.value else "bnz_batch_create failed"
+            self.L.bnz_batch_destroy(h)
+            self.h = C.c_void_p()
+            raise BnzError(rc, msg)
+        self.instances = []
+        for q in range(n):
+            ch = C.c_void_p()
+            self._ck(self.L.bnz_batch_instance(h, q, C.byref(ch)))
+            self.instances.append(Context(_handle=ch, _owner=self))
+
+    def _ck(self, rc):
+        if rc != BNZ_OK:
+            raise BnzError(rc, self.L.bnz_batch_last_error(self.h).decode())
+
+    def __len__(self):
+        return len(self.instances)
+
+    def __getitem__(self, i):
+        return self.instances[i]
+
+    def advance(self, tmax, nsteps):
+        self._ck(self.L.bnz_batch_advance(self.h, tmax, nsteps))
+
+    def set_stream(self, stream):
+        self._ck(self.L.bnz_batch_set_stream(self.h, C.c_void_p(stream)))
+
+    def launch_count(self):
+        n = C.c_longlong()
+        self._ck(self.L.bnz_batch_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    def sync(self):
+        self._ck(self.L.bnz_batch_sync(self.h))
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            for c in self.instances:
+                c.h = C.c_void_p()
+            self.L.bnz_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -863,7 +863,7 @@ int bnz_advance_graph(bnz_ctx* c, double tmax, int nsteps) {
       c->launches = before;
       // capture recorded the pointer swaps of `unroll` steps; replaying starts
       // from the parity it was captured at
-      set_parity(c, c->graph_parity);
+      if (c->md.path == BNZ_PATH_FUSED) set_parity(c, c->graph_parity);
     }
     for (int r = 0; r < full; ++r) {
       CKC(cudaGraphLaunch(c->graph, c->stream));
@@ -910,6 +910,234 @@ int bnz_launch_count(const bnz_ctx* c, long long* n) {
 int bnz_stream(bnz_ctx* c, void** s) {
   if (!c) return BNZ_ERR_ARG;
   if (s) *s = (void*)c->stream;
+  return BNZ_OK;
+}
+
+}  // extern "C"
+
+
+// ===========================================================================
+// Batches of independent grids (uneven parameter sweeps).  Every instance is a
+// fused-path context on the batch's stream; one step of the whole batch is
+// four launches (per-instance dt, predictor tiles, corrector tiles, time).
+// ===========================================================================
+
+struct bnz_batch {
+  std::vector<bnz_ctx*> ctx;
+  bnz_method_desc md;
+  FusedInst* d_inst = nullptr;
+  FusedTile* d_tiles = nullptr;
+  int ntA = 0, ntB = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = true;
+  cudaGraphExec_t graph = nullptr;
+  int graph_parity = -1;
+  int parity = 0;
+  long long launches = 0;
+  long long graph_launches = 0;
+  double h_tmax = 0.;
+  const Launchers* L = nullptr;
+  std::string err;
+};
+
+namespace {
+
+int bfail(bnz_batch* b, int code, const std::string& msg) {
+  if (b) b->err = msg;
+  return code;
+}
+
+#define CKB(call)                                                                                \
+  do {                                                                                           \
+    cudaError_t _e = (call);                                                                     \
+    if (_e != cudaSuccess)                                                                       \
+      return bfail(b, BNZ_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e));        \
+  } while (0)
+
+FusedLaunch batch_launch(const bnz_batch* b, int dt_mode) {
+  FusedLaunch f;
+  memset(&f, 0, sizeof f);
+  f.insts = b->d_inst;
+  f.ninst = (int)b->ctx.size();
+  f.tilesA = b->d_tiles;
+  f.ntA = b->ntA;
+  f.tilesB = b->d_tiles + b->ntA;
+  f.ntB = b->ntB;
+  f.rsolver = b->md.rsolver;
+  f.limiter = b->md.limiter;
+  f.cour = b->md.cour;
+  f.dt_mode = dt_mode;
+  f.dt_fixed = b->md.dt_fixed;
+  f.err = b->ctx.empty() ? nullptr : b->ctx[0]->d_err;
+  f.stream = b->stream;
+  return f;
+}
+
+__global__ void k_set_tmax(FusedInst* insts, int n, double tmax) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) insts[q].ds->tmax = tmax;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bnz_batch_create(const bnz_grid_desc* grids, int n, const bnz_method_desc* md, bnz_batch** out) {
+  if (!grids || !md || !out || n < 1) return BNZ_ERR_ARG;
+  bnz_batch* b = new bnz_batch();
+  *out = b;
+  b->md = *md;
+  b->md.path = BNZ_PATH_FUSED;
+  if (md->kappa0 > 0.) return bfail(b, BNZ_ERR_UNSUPPORTED, "batches advance the hyperbolic step only (kappa0 = 0)");
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bfail(b, BNZ_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+  std::vector<FusedInst> insts;
+  std::vector<FusedTile> tA, tB;
+  for (int q = 0; q < n; ++q) {
+    bnz_ctx* c = nullptr;
+    int rc = bnz_create(&grids[q], &b->md, &c);
+    if (rc) {
+      std::string m = "instance " + std::to_string(q) + ": " + (c ? c->err : std::string("create failed"));
+      if (c) bnz_destroy(c);
+      return bfail(b, rc, m);
+    }
+    b->ctx.push_back(c);
+    rc = bnz_set_stream(c, (void*)b->stream);
+    if (rc) return bfail(b, rc, c->err);
+    insts.push_back(make_inst(c));
+    make_tiles(q, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->ng, true, tA);
+    make_tiles(q, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->ng, false, tB);
+  }
+  b->L = b->ctx[0]->L;
+  b->ntA = (int)tA.size();
+  b->ntB = (int)tB.size();
+  std::vector<FusedTile> all(tA);
+  all.insert(all.end(), tB.begin(), tB.end());
+  CKB(cudaMalloc((void**)&b->d_inst, insts.size() * sizeof(FusedInst)));
+  CKB(cudaMalloc((void**)&b->d_tiles, all.size() * sizeof(FusedTile)));
+  CKB(cudaMemcpy(b->d_inst, insts.data(), insts.size() * sizeof(FusedInst), cudaMemcpyHostToDevice));
+  CKB(cudaMemcpy(b->d_tiles, all.data(), all.size() * sizeof(FusedTile), cudaMemcpyHostToDevice));
+  return BNZ_OK;
+}
+
+int bnz_batch_destroy(bnz_batch* b) {
+  if (!b) return BNZ_OK;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (bnz_ctx* c : b->ctx) bnz_destroy(c);
+  if (b->d_inst) cudaFree(b->d_inst);
+  if (b->d_tiles) cudaFree(b->d_tiles);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return BNZ_OK;
+}
+
+const char* bnz_batch_last_error(const bnz_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int bnz_batch_size(const bnz_batch* b, int* n) {
+  if (!b) return BNZ_ERR_ARG;
+  if (n) *n = (int)b->ctx.size();
+  return BNZ_OK;
+}
+
+int bnz_batch_instance(bnz_batch* b, int i, bnz_ctx** ctx) {
+  if (!b || i < 0 || i >= (int)b->ctx.size() || !ctx) return bfail(b, BNZ_ERR_ARG, "instance index out of range");
+  *ctx = b->ctx[i];
+  return BNZ_OK;
+}
+
+int bnz_batch_set_stream(bnz_batch* b, void* stream) {
+  if (!b) return BNZ_ERR_ARG;
+  CKB(cudaStreamSynchronize(b->stream));
+  if (b->own_stream) cudaStreamDestroy(b->stream);
+  b->stream = (cudaStream_t)stream;
+  b->own_stream = false;
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  for (bnz_ctx* c : b->ctx) {
+    int rc = bnz_set_stream(c, stream);
+    if (rc) return bfail(b, rc, c->err);
+  }
+  return BNZ_OK;
+}
+
+int bnz_batch_advance(bnz_batch* b, double tmax, int nsteps) {
+  if (!b || b->ctx.empty()) return BNZ_ERR_ARG;
+  if (nsteps < 0) return bfail(b, BNZ_ERR_ARG, "nsteps must be >= 0");
+  if (nsteps == 0) return BNZ_OK;
+  // every instance must be at the batch parity with its time record on the device
+  for (bnz_ctx* c : b->ctx) {
+    if (c->parity != b->parity) return bfail(b, BNZ_ERR_STATE, "instance stepped outside the batch");
+    if (!c->time_on_device) {
+      c->h_stage[0] = c->last_dt;
+      c->h_stage[1] = c->time;
+      c->h_stage[2] = tmax;
+      c->h_step = c->step;
+      CKB(cudaMemcpyAsync(c->d_ds, c->h_stage, 3 * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+      CKB(cudaMemcpyAsync(&c->d_ds->step, &c->h_step, sizeof(long long), cudaMemcpyHostToDevice, b->stream));
+      c->time_on_device = true;
+    }
+  }
+  const int n = (int)b->ctx.size();
+  k_set_tmax<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_inst, n, tmax);
+  b->launches += 1;
+  const int mode = b->md.fixdt ? FDT_FIXED : FDT_CFL;
+  auto one_step = [&](int p) {
+    FusedLaunch f = batch_launch(b, mode);
+    b->launches += b->L->fused_step(f, p);
+    b->launches += b->L->fused_time(f);
+  };
+  int full = nsteps / 2, rest = nsteps % 2;
+  if (full > 0) {
+    if (b->graph && b->graph_parity != b->parity) {
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+    if (!b->graph) {
+      b->graph_parity = b->parity;
+      CKB(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      long long before = b->launches;
+      one_step(b->parity);
+      one_step(b->parity ^ 1);
+      cudaGraph_t g = nullptr;
+      CKB(cudaStreamEndCapture(b->stream, &g));
+      cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return bfail(b, BNZ_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+      b->graph_launches = b->launches - before;
+      b->launches = before;
+    }
+    for (int r = 0; r < full; ++r) {
+      CKB(cudaGraphLaunch(b->graph, b->stream));
+      b->launches += b->graph_launches;
+    }
+  }
+  if (rest) {
+    one_step(b->parity);
+    b->parity ^= 1;
+  }
+  CKB(cudaGetLastError());
+  for (bnz_ctx* c : b->ctx) {
+    set_parity(c, b->parity);
+    c->ghosts_stale = true;
+    c->time_on_device = true;
+  }
+  return BNZ_OK;
+}
+
+int bnz_batch_launch_count(const bnz_batch* b, long long* n) {
+  if (!b) return BNZ_ERR_ARG;
+  long long t = b->launches;
+  for (const bnz_ctx* c : b->ctx) t += c->launches;
+  if (n) *n = t;
+  return BNZ_OK;
+}
+
+int bnz_batch_sync(bnz_batch* b) {
+  if (!b) return BNZ_ERR_ARG;
+  CKB(cudaStreamSynchronize(b->stream));
   return BNZ_OK;
 }
 

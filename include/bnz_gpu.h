@@ -142,6 +142,28 @@ int bnz_set_stream(bnz_ctx* ctx, void* stream);
 /* Number of kernels this context has launched so far. */
 int bnz_launch_count(const bnz_ctx* ctx, long long* n);
 
+/* ------------------------------------------------------------------------
+ * Batches: many independent grids of uneven sizes (parameter sweeps) with
+ * one shared method, advanced together -- each stage of a step is a single
+ * launch over a tile list that spans every instance, each instance keeps its
+ * own CFL time step, and steps are replayed from a CUDA graph.  No reference
+ * counterpart: the reference runs one grid per process (vanleer.advance).
+ * 2D grids, PLM, kappa0 = 0.
+ * ------------------------------------------------------------------------ */
+typedef struct bnz_batch bnz_batch;
+int bnz_batch_create(const bnz_grid_desc* grids, int n, const bnz_method_desc* method, bnz_batch** out);
+int bnz_batch_destroy(bnz_batch* batch);
+const char* bnz_batch_last_error(const bnz_batch* batch);
+int bnz_batch_size(const bnz_batch* batch, int* n);
+/* The i-th instance as a context: bnz_set_state / bnz_init / bnz_get_state /
+ * bnz_get_time / bnz_check work on it (do not step it on its own). */
+int bnz_batch_instance(bnz_batch* batch, int i, bnz_ctx** ctx);
+/* nsteps VL2 steps of every instance, each with its own CFL dt clipped to tmax. */
+int bnz_batch_advance(bnz_batch* batch, double tmax, int nsteps);
+int bnz_batch_set_stream(bnz_batch* batch, void* stream);
+int bnz_batch_launch_count(const bnz_batch* batch, long long* n);
+int bnz_batch_sync(bnz_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,75 @@
+"""Batched uneven instances: each instance of a batch advanced together must be
+bitwise the instance advanced alone by the oracle (own CFL dt per instance)."""
+import numpy as np
+import pytest
+
+from bonzo_b200 import problems as P
+from helpers import oracle_sim
+
+pytestmark = pytest.mark.gpu
+
+
+def _instances(sizes, seed=3):
+    rng = np.random.default_rng(seed)
+    out = []
+    for n in sizes:
+        gc = P.make_grid(n, n, 1, dims=2, bc=1)
+        prim, bfld = P.blast(gc, b_mag=rng.uniform(0.2, 0.6), b_angle=rng.uniform(0, 6.28),
+                             center=(rng.uniform(0.3, 0.7), rng.uniform(0.3, 0.7), 0.5),
+                             p_ratio=rng.uniform(10, 100))
+        out.append((n, gc, prim, bfld))
+    return out
+
+
+METHOD = dict(gam=5. / 3, cour=0.4, rsolver="hlld", limiter="vl")
+
+
+@pytest.mark.parametrize("steps", [1, 4, 5])
+def test_batch_bitwise_vs_oracle(steps):
+    from bonzo_b200._lib import Batch
+    inst = _instances([16, 40, 24, 33, 64, 20, 8])
+    grids = [dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((1, 1), (1, 1), (0, 0))) for n, *_ in inst]
+    b = Batch(grids, exact_fp=True, **METHOD)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        b[q].set_state(prim, bfld)
+        b[q].init()
+    b.advance(1e30, steps)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        o = oracle_sim(dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((1, 1), (1, 1), (0, 0))), **METHOD)
+        o.set_state(prim, bfld)
+        o.init()
+        o.advance(1e30, max_steps=steps)
+        t, s, _ = b[q].time()
+        assert s == steps and t == o.time, (q, t, o.time)
+        for x, y in zip(o.get_state(), b[q].get_state()):
+            assert np.array_equal(x, y), q
+        assert b[q].check() == 0
+
+
+def test_batch_per_instance_tmax():
+    from bonzo_b200._lib import Batch
+    inst = _instances([24, 48])
+    grids = [dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((1, 1), (1, 1), (0, 0))) for n, *_ in inst]
+    b = Batch(grids, exact_fp=True, **METHOD)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        b[q].set_state(prim, bfld)
+        b[q].init()
+    tmax = 0.01
+    b.advance(tmax, 40)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        o = oracle_sim(dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((1, 1), (1, 1), (0, 0))), **METHOD)
+        o.set_state(prim, bfld)
+        o.init()
+        o.advance(tmax)
+        t, s, _ = b[q].time()
+        assert t == tmax and s == o.nstep
+        for x, y in zip(o.get_state(), b[q].get_state()):
+            assert np.array_equal(x, y)
+
+
+def test_batch_rejects_3d_and_conduction():
+    from bonzo_b200._lib import Batch, BnzError
+    with pytest.raises(BnzError):
+        Batch([dict(Nx=8, Ny=8, Nz=8, dims=3)], **METHOD)
+    with pytest.raises(BnzError):
+        Batch([dict(Nx=8, Ny=8, Nz=1, dims=2)], kappa0=0.1, **METHOD)
