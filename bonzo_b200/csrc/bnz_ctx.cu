@@ -1049,16 +1049,17 @@ int bnz_batch_instance(bnz_batch* b, int i, bnz_ctx** ctx) {
 int bnz_batch_set_stream(bnz_batch* b, void* stream) {
   if (!b) return BNZ_ERR_ARG;
   CKB(cudaStreamSynchronize(b->stream));
+  // move the instances first: they still reference the old stream
+  for (bnz_ctx* c : b->ctx) {
+    int rc = bnz_set_stream(c, stream);
+    if (rc) return bfail(b, rc, c->err);
+  }
   if (b->own_stream) cudaStreamDestroy(b->stream);
   b->stream = (cudaStream_t)stream;
   b->own_stream = false;
   if (b->graph) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
-  }
-  for (bnz_ctx* c : b->ctx) {
-    int rc = bnz_set_stream(c, stream);
-    if (rc) return bfail(b, rc, c->err);
   }
   return BNZ_OK;
 }

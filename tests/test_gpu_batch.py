@@ -46,6 +46,23 @@ def test_batch_bitwise_vs_oracle(steps):
         assert b[q].check() == 0
 
 
+def test_batch_on_caller_stream():
+    """Moving a batch onto a caller-owned stream keeps it working."""
+    import torch
+    from bonzo_b200._lib import Batch
+    inst = _instances([16, 24])
+    grids = [dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((1, 1), (1, 1), (0, 0))) for n, *_ in inst]
+    b = Batch(grids, exact_fp=True, **METHOD)
+    st = torch.cuda.Stream()
+    b.set_stream(st.cuda_stream)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        b[q].set_state(prim, bfld)
+        b[q].init()
+    b.advance(1e30, 3)
+    b.sync()
+    assert all(b[q].time()[1] == 3 for q in range(len(inst)))
+
+
 def test_batch_per_instance_tmax():
     from bonzo_b200._lib import Batch
     inst = _instances([24, 48])
