@@ -198,25 +198,31 @@ __device__ __forceinline__ void flux_hllt(double* flux, const double* wL, const 
   flux[BX] = 0.;
 }
 
-// fluxes_c.c:616-834 (Miyoshi & Kusano 2005 HLLD)
+// fluxes_c.c:616-834 (Miyoshi & Kusano 2005 HLLD).
+// Every value is computed by the reference's expression, but the state and
+// flux vectors are built for ONE side only: regions 1-3 of the wave fan use
+// the left states (fL, uL*, uL**), regions 4-6 the right ones with the same
+// formulas.  The scalar star quantities (sM, p*, tangential star velocities
+// and fields) are formed for both sides, the side is chosen per lane, and the
+// 9-vectors are evaluated once -- about half the live registers of forming
+// both sides, with no warp divergence.
 __device__ __forceinline__ void flux_hlld(double* flux, const double* wL, const double* wR, double gam,
                                           unsigned& err) {
-  double uL[NM], uR[NM], fL[NM], fR[NM];
-  prim2cons(uL, wL, gam);
-  prim2cons(uR, wR, gam);
-  primcons2flux(fL, wL, uL);
-  primcons2flux(fR, wR, uR);
+  const double bx = wL[BX];
+  const double bx2 = sqr(bx);
+  // pieces of prim2cons / primcons2flux that the HLL average needs
+  const double b2L = bx2 + sqr(wL[BY]) + sqr(wL[BZ]);
+  const double b2R = bx2 + sqr(wR[BY]) + sqr(wR[BZ]);
+  const double ptL = wL[PR] + 0.5 * b2L;  // = primcons2flux's ptot (same operands)
+  const double ptR = wR[PR] + 0.5 * b2R;
+  const double mxL = wL[RHO] * wL[VX], mxR = wR[RHO] * wR[VX];  // u[MX] = f[RHO]
+  const double fmxL = mxL * wL[VX] + ptL - bx2;                   // f[MX]
+  const double fmxR = mxR * wR[VX] + ptR - bx2;
   double sL, sR;
   wave_speeds(wL, wR, gam, sL, sR);
-  const double bx = wL[BX];
 
-  double b2hL = 0.5 * (sqr(bx) + sqr(wL[BY]) + sqr(wL[BZ]));
-  double b2hR = 0.5 * (sqr(bx) + sqr(wR[BY]) + sqr(wR[BZ]));
-  double ptL = wL[PR] + b2hL;
-  double ptR = wR[PR] + b2hR;
-
-  double deni = 1. / (sR * uR[RHO] - sL * uL[RHO] - (fR[RHO] - fL[RHO]));
-  double sM = (sR * uR[MX] - sL * uL[MX] - (fR[MX] - fL[MX])) * deni;
+  double deni = 1. / (sR * wR[RHO] - sL * wL[RHO] - (mxR - mxL));
+  double sM = (sR * mxR - sL * mxL - (fmxR - fmxL)) * deni;
 
   double sLvxL = sL - wL[VX];
   double sRvxR = sR - wR[VX];
@@ -224,61 +230,30 @@ __device__ __forceinline__ void flux_hlld(double* flux, const double* wL, const 
   double sRsMi = 1. / (sR - sM);
   double xL = sLvxL * sLsMi;
   double xR = sRvxR * sRsMi;
-
-  // single-star states (index order RHO MX MY MZ EN PSC . BY BZ)
-  double rLs = uL[RHO] * xL, rRs = uR[RHO] * xR;
-  double psL = uL[PSC] * xL, psR = uR[PSC] * xR;
+  double rLs = wL[RHO] * xL, rRs = wR[RHO] * xR;
   double pts = wL[RHO] * sLvxL * (sM - wL[VX]) + ptL;
 
   double rhosLvxL = wL[RHO] * sLvxL;
   double rhosRvxR = wR[RHO] * sRvxR;
-  double bx2 = sqr(bx);
   double wvbL = 1. / (rhosLvxL * (sL - sM) - bx2);
   double wvbR = 1. / (rhosRvxR * (sR - sM) - bx2);
-  double bxsMvxL = bx * (sM - wL[VX]);
-  double bxsMvxR = bx * (sM - wR[VX]);
-  double wvL = bxsMvxL * wvbL;
-  double wvR = bxsMvxR * wvbR;
+  double wvL = bx * (sM - wL[VX]) * wvbL;
+  double wvR = bx * (sM - wR[VX]) * wvbR;
   double vyLs = wL[VY] - wL[BY] * wvL;
   double vyRs = wR[VY] - wR[BY] * wvR;
   double vzLs = wL[VZ] - wL[BZ] * wvL;
   double vzRs = wR[VZ] - wR[BZ] * wvR;
-
-  double mxLs = rLs * sM, mxRs = rRs * sM;
-  double myLs = rLs * vyLs, myRs = rRs * vyRs;
-  double mzLs = rLs * vzLs, mzRs = rRs * vzRs;
-
-  double rhosLvxL2_bx2 = rhosLvxL * sLvxL - bx2;
-  double rhosRvxR2_bx2 = rhosRvxR * sRvxR - bx2;
-  double wbL = rhosLvxL2_bx2 * wvbL;
-  double wbR = rhosRvxR2_bx2 * wvbR;
+  double wbL = (rhosLvxL * sLvxL - bx2) * wvbL;
+  double wbR = (rhosRvxR * sRvxR - bx2) * wvbR;
   double byLs = wL[BY] * wbL, byRs = wR[BY] * wbR;
   double bzLs = wL[BZ] * wbL, bzRs = wR[BZ] * wbR;
-
   double vsbsL = sM * bx + vyLs * byLs + vzLs * bzLs;
   double vsbsR = sM * bx + vyRs * byRs + vzRs * bzRs;
-  double eLs = (sLvxL * uL[EN] - ptL * wL[VX] + pts * sM +
-                bx * (wL[VX] * bx + wL[VY] * wL[BY] + wL[VZ] * wL[BZ] - vsbsL)) * sLsMi;
-  double eRs = (sRvxR * uR[EN] - ptR * wR[VX] + pts * sM +
-                bx * (wR[VX] * bx + wR[VY] * wR[BY] + wR[VZ] * wR[BZ] - vsbsR)) * sRsMi;
 
-  // double-star states
   double sqrt_rhoLs = sqrt(rLs);
   double sqrt_rhoRs = sqrt(rRs);
   double sLs = sM - fabs(bx) / sqrt_rhoLs;
   double sRs = sM + fabs(bx) / sqrt_rhoRs;
-  double rhoLRi = 1. / (sqrt_rhoLs + sqrt_rhoRs);
-  double sgnb = sgnd(bx);
-
-  double vyss = (sqrt_rhoLs * vyLs + sqrt_rhoRs * vyRs + (byRs - byLs) * sgnb) * rhoLRi;
-  double vzss = (sqrt_rhoLs * vzLs + sqrt_rhoRs * vzRs + (bzRs - bzLs) * sgnb) * rhoLRi;
-  double myLss = rLs * vyss, myRss = rRs * vyss;
-  double mzLss = rLs * vzss, mzRss = rRs * vzss;
-  double byss = (sqrt_rhoLs * byRs + sqrt_rhoRs * byLs + sqrt_rhoLs * sqrt_rhoRs * (vyRs - vyLs) * sgnb) * rhoLRi;
-  double bzss = (sqrt_rhoLs * bzRs + sqrt_rhoRs * bzLs + sqrt_rhoLs * sqrt_rhoRs * (vzRs - vzLs) * sgnb) * rhoLRi;
-  double vssbss = sM * bx + vyss * byss + vzss * bzss;
-  double eLss = eLs - sqrt_rhoLs * (vsbsL - vssbss) * sgnb;
-  double eRss = eRs + sqrt_rhoRs * (vsbsR - vssbss) * sgnb;
 
   int r = 0;
   if (sL > 0.) r = 1;
@@ -289,20 +264,48 @@ __device__ __forceinline__ void flux_hlld(double* flux, const double* wL, const 
   if (sR <= 0.) r = 6;
   if (r == 0) err |= ERR_FAN;
 
-  // left / right single- and double-star vectors in variable order
-  const double uLs[NM] = {rLs, mxLs, myLs, mzLs, eLs, psL, 0., byLs, bzLs};
-  const double uRs[NM] = {rRs, mxRs, myRs, mzRs, eRs, psR, 0., byRs, bzRs};
-  const double uLss[NM] = {rLs, mxLs, myLss, mzLss, eLss, psL, 0., byss, bzss};
-  const double uRss[NM] = {rRs, mxRs, myRss, mzRss, eRss, psR, 0., byss, bzss};
+  // double-star tangential state (needs both sides)
+  double rhoLRi = 1. / (sqrt_rhoLs + sqrt_rhoRs);
+  double sgnb = sgnd(bx);
+  double vyss = (sqrt_rhoLs * vyLs + sqrt_rhoRs * vyRs + (byRs - byLs) * sgnb) * rhoLRi;
+  double vzss = (sqrt_rhoLs * vzLs + sqrt_rhoRs * vzRs + (bzRs - bzLs) * sgnb) * rhoLRi;
+  double byss = (sqrt_rhoLs * byRs + sqrt_rhoRs * byLs + sqrt_rhoLs * sqrt_rhoRs * (vyRs - vyLs) * sgnb) * rhoLRi;
+  double bzss = (sqrt_rhoLs * bzRs + sqrt_rhoRs * bzLs + sqrt_rhoLs * sqrt_rhoRs * (vzRs - vzLs) * sgnb) * rhoLRi;
+  double vssbss = sM * bx + vyss * byss + vzss * bzss;
+
+  // one side: L for regions 1-3, R for 4-6
+  const bool left = r <= 3;
+  double w[NM];
+#pragma unroll
+  for (int n = 0; n < NM; ++n) w[n] = left ? wL[n] : wR[n];
+  const double s_o = left ? sL : sR;          // outer wave
+  const double s_i = left ? sLs : sRs;        // Alfven wave
+  const double x = left ? xL : xR;
+  const double svx = left ? sLvxL : sRvxR;
+  const double sMi = left ? sLsMi : sRsMi;
+  const double pt = left ? ptL : ptR;
+  const double rs = left ? rLs : rRs;
+  const double vys = left ? vyLs : vyRs, vzs = left ? vzLs : vzRs;
+  const double bys = left ? byLs : byRs, bzs = left ? bzLs : bzRs;
+  const double vsbs = left ? vsbsL : vsbsR;
+  const double srs = left ? sqrt_rhoLs : sqrt_rhoRs;
+
+  double u[NM], f[NM];
+  prim2cons(u, w, gam);
+  primcons2flux(f, w, u);
+  // single-star state (fluxes_c.c:690-760)
+  double es = (svx * u[EN] - pt * w[VX] + pts * sM + bx * (w[VX] * bx + w[VY] * w[BY] + w[VZ] * w[BZ] - vsbs)) * sMi;
+  const double us[NM] = {rs, rs * sM, rs * vys, rs * vzs, es, u[PSC] * x, 0., bys, bzs};
+  // double-star state (fluxes_c.c:764-812)
+  double t = srs * (vsbs - vssbss) * sgnb;
+  double ess = left ? es - t : es + t;
+  const double uss[NM] = {rs, rs * sM, rs * vyss, rs * vzss, ess, u[PSC] * x, 0., byss, bzss};
 #pragma unroll
   for (int n = 0; n < NM; ++n) {
     double v;
-    if (r == 1) v = fL[n];
-    else if (r == 2) v = fL[n] + sL * (uLs[n] - uL[n]);
-    else if (r == 3) v = fL[n] + sL * (uLs[n] - uL[n]) + sLs * (uLss[n] - uLs[n]);
-    else if (r == 4) v = fR[n] + sR * (uRs[n] - uR[n]) + sRs * (uRss[n] - uRs[n]);
-    else if (r == 5) v = fR[n] + sR * (uRs[n] - uR[n]);
-    else if (r == 6) v = fR[n];
+    if (r == 1 || r == 6) v = f[n];
+    else if (r == 2 || r == 5) v = f[n] + s_o * (us[n] - u[n]);
+    else if (r == 3 || r == 4) v = f[n] + s_o * (us[n] - u[n]) + s_i * (uss[n] - us[n]);
     else v = 0.;
     flux[n] = v;
   }

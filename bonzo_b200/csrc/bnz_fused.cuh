@@ -349,12 +349,25 @@ __device__ __forceinline__ void stage_cell(const Inst& I, const Layout& L, const
   cons2prim(o.w, u, I.gam);
 }
 
+// The instance descriptor, copied to shared memory by the first warp so the
+// kernels read its fields without global loads.
+__device__ __forceinline__ void stage_inst(Inst& sI, const Inst* __restrict__ insts, int q) {
+  constexpr int NW = sizeof(Inst) / sizeof(int);
+  static_assert(sizeof(Inst) % sizeof(int) == 0, "Inst must be int-aligned");
+  const int* src = reinterpret_cast<const int*>(insts + q);
+  int* dst = reinterpret_cast<int*>(&sI);
+  for (int t = threadIdx.x; t < NW; t += blockDim.x) dst[t] = src[t];
+  __syncthreads();
+}
+
 template <int TXM, int TYM, int RS>
-__global__ void __launch_bounds__(256) k_pred2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
+__global__ void __launch_bounds__(256, 2) k_pred2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
                                                 int parity, int lim, unsigned* err) {
   extern __shared__ double smem[];
+  __shared__ Inst sI;
   const Tile T = tiles[blockIdx.x];
-  const Inst& I = insts[T.inst];
+  stage_inst(sI, insts, T.inst);
+  const Inst& I = sI;
   const double dtf = I.ds->dt;
   if (!(dtf > 0.)) return;
   const double dt = 0.5 * dtf;
@@ -419,12 +432,14 @@ __device__ __forceinline__ void copy_tile(const Inst& I, const Tile& T, int pari
 }
 
 template <int TXM, int TYM, int RS>
-__global__ void __launch_bounds__(256) k_corr2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
+__global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
                                                 int parity, int lim, double cour, unsigned* err) {
   extern __shared__ double smem[];
   __shared__ double red[8];
+  __shared__ Inst sI;
   const Tile T = tiles[blockIdx.x];
-  const Inst& I = insts[T.inst];
+  stage_inst(sI, insts, T.inst);
+  const Inst& I = sI;
   const double dt = I.ds->dt;
   if (!(dt > 0.)) {
     // time has reached tmax: carry the state over unchanged
