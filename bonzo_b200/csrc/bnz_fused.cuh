@@ -185,106 +185,150 @@ struct Layout {
   __device__ __forceinline__ int ee(int ci, int cj) const { return cj * (wx + 1) + ci; }
 };
 
-template <int TXM, int TYM>
+template <int TXM, int TYM, int RING>
 struct Smem {
   static constexpr int NFX = (TXM + 1) * (TYM + 2);
   static constexpr int NFY = (TXM + 2) * (TYM + 1);
   static constexpr int NEC = (TXM + 2) * (TYM + 2);
   static constexpr int NEE = (TXM + 1) * (TYM + 1);
-  static constexpr size_t bytes = sizeof(double) * ((size_t)NF * (NFX + NFY) + NEC + NEE);
+  static constexpr int NSW = NM * (TXM + 2 * RING) * (TYM + 2 * RING);  // staged cells
+  static constexpr size_t bytes = sizeof(double) * ((size_t)NF * (NFX + NFY) + NEC + NEE + NSW);
 };
 
 // ---------------------------------------------------------------------------
-// Stage 1 of both kernels: interface fluxes and cell-centred EMF.
-// ORDER 0 (predictor): donor cell from w (ghosts mapped), normal B from b.
-// ORDER 1 (corrector): PLM from ws, normal B from bs (no ghost mapping: the
-// predictor wrote cells 1..Ntot-2).
+// Stage 0: the tile's input cells into shared memory in one coalesced pass.
+// Predictor: w^n on the tile plus one ring, ghost indices through the BC map.
+// Corrector: ws on the tile plus two rings (the predictor wrote those cells).
+// ---------------------------------------------------------------------------
+
+// t / d for small t (t * d < 2^32) by a multiply-high
+struct FastDiv {
+  unsigned d, m;
+  __device__ __forceinline__ void set(unsigned dd) {
+    d = dd;
+    m = 0xFFFFFFFFu / dd + 1u;
+  }
+  __device__ __forceinline__ unsigned div(unsigned t) const { return __umulhi(t, m); }
+};
+
+struct Stage {
+  int x0, y0, w, h;  // region origin (array coordinates) and size
+  __device__ __forceinline__ int at(int n, int i, int j) const { return (n * h + (j - y0)) * w + (i - x0); }
+  __device__ __forceinline__ int cells() const { return w * h; }
+};
+
+template <bool MAP>
+__device__ __forceinline__ void stage_cells(const Inst& I, const double* __restrict__ src, const Stage& S, double* sW) {
+  const AxisMap mx = axis_map(I, 0), my = axis_map(I, 1);
+  FastDiv dw;
+  dw.set(S.w);
+  for (int t = threadIdx.x; t < S.cells(); t += blockDim.x) {
+    const int cj = dw.div(t), ci = t - cj * S.w;
+    int i = S.x0 + ci, j = S.y0 + cj;
+    bool fx = false, fy = false;
+    if (MAP) {
+      i = map_cell(i, mx, fx);
+      j = map_cell(j, my, fy);
+    }
+    const long long c = (long long)j * I.nx + i;
+#pragma unroll
+    for (int n = 0; n < NM; ++n) {
+      double v = src[n * I.sv + c];
+      if (MAP && ((fx && (n == VX || n == BX)) || (fy && (n == VY || n == BY)))) v = -v;
+      sW[n * S.cells() + t] = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stage 1 of both kernels: interface fluxes and cell-centred EMF from the
+// staged cells.  ORDER 0 (predictor): donor cell, normal B from b with the BC
+// map.  ORDER 1 (corrector): PLM, normal B from bs.
 // ---------------------------------------------------------------------------
 
 template <int ORDER, int RS>
-__device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const Layout& L, const double* __restrict__ w,
-                                             const double* __restrict__ b, double* sFX, double* sFY, double* sEC,
-                                             int lim, bool interior, unsigned& err) {
+__device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const Layout& L, const Stage& S,
+                                             const double* sW, const double* __restrict__ b, double* sFX,
+                                             double* sFY, double* sEC, int lim, bool interior, unsigned& err) {
   const AxisMap mx = axis_map(I, 0), my = axis_map(I, 1);
   const int total = L.nfx + L.nfy + L.nec;
+  const int nc = S.cells();
+  FastDiv dx1, dx2;
+  dx1.set(L.wx + 1);
+  dx2.set(L.wx + 2);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
     if (t < L.nfx) {
       // x face at column i (between cells i-1 and i), row j
-      const int fi = t % (L.wx + 1), fj = t / (L.wx + 1) - 1;
+      const int q = dx1.div(t);
+      const int fi = t - q * (L.wx + 1), fj = q - 1;
       const int i = T.x0 + fi, j = T.y0 + fj;
       double wL[NM], wR[NM];
-      if (ORDER == 0) {
-        load_prim<0>(I, w, i - 1, j, mx, my, interior, wL);
-        load_prim<0>(I, w, i, j, mx, my, interior, wR);
-        wL[BX] = wR[BX] = load_face<0>(I, b, i, j, mx, my, interior);
-      } else {
-        const long long c = (long long)j * I.nx + i;
+      const int c = S.at(0, i, j);
 #pragma unroll
-        for (int n = 0; n < NM; ++n) {
-          if (n == BX) continue;
-          const double* a = w + n * I.sv + c;
+      for (int n = 0; n < NM; ++n) {
+        if (n == BX) continue;
+        const double* a = sW + n * nc + c;
+        if (ORDER == 0) {
+          wL[n] = a[-1];
+          wR[n] = a[0];
+        } else {
           double wm2 = a[-2], wm1 = a[-1], w0 = a[0], wp1 = a[1];
           wL[n] = wm1 + plain::half_slope_rt(lim, wm2, wm1, w0);
           wR[n] = w0 - plain::half_slope_rt(lim, wm1, w0, wp1);
         }
-        wL[BX] = wR[BX] = b[c];
       }
+      if (ORDER == 0) wL[BX] = wR[BX] = load_face<0>(I, b, i, j, mx, my, interior);
+      else wL[BX] = wR[BX] = b[(long long)j * I.nx + i];
       double f[NM];
       riemann<RS>(f, wL, wR, I.gam, err);
-      const int q = L.fx(fi, fj);
+      const int qq = L.fx(fi, fj);
 #pragma unroll
-      for (int n = 0; n < 6; ++n) sFX[n * L.nfx + q] = f[n];
-      sFX[6 * L.nfx + q] = f[BY];  // fx[BY]
-      sFX[7 * L.nfx + q] = f[BZ];  // fx[BZ]
+      for (int n = 0; n < 6; ++n) sFX[n * L.nfx + qq] = f[n];
+      sFX[6 * L.nfx + qq] = f[BY];  // fx[BY]
+      sFX[7 * L.nfx + qq] = f[BZ];  // fx[BZ]
     } else if (t < L.nfx + L.nfy) {
       // y face at row j (between cells j-1 and j), column i; sweep frame AX = 1
       const int u = t - L.nfx;
-      const int fi = u % (L.wx + 2) - 1, fj = u / (L.wx + 2);
+      const int q = dx2.div(u);
+      const int fi = u - q * (L.wx + 2) - 1, fj = q;
       const int i = T.x0 + fi, j = T.y0 + fj;
       double wL[NM], wR[NM];
-      if (ORDER == 0) {
-        load_prim<1>(I, w, i, j - 1, mx, my, interior, wL);
-        load_prim<1>(I, w, i, j, mx, my, interior, wR);
-        wL[BX] = wR[BX] = load_face<1>(I, b, i, j, mx, my, interior);
-      } else {
-        const long long c = (long long)j * I.nx + i;
-        const long long s = I.nx;
+      const int c = S.at(0, i, j);
+      const int sy = S.w;
 #pragma unroll
-        for (int n = 0; n < NM; ++n) {
-          if (n == BX) continue;
-          const double* a = w + plain::perm<1>(n) * I.sv + c;
-          double wm2 = a[-2 * s], wm1 = a[-s], w0 = a[0], wp1 = a[s];
+      for (int n = 0; n < NM; ++n) {
+        if (n == BX) continue;
+        const double* a = sW + plain::perm<1>(n) * nc + c;
+        if (ORDER == 0) {
+          wL[n] = a[-sy];
+          wR[n] = a[0];
+        } else {
+          double wm2 = a[-2 * sy], wm1 = a[-sy], w0 = a[0], wp1 = a[sy];
           wL[n] = wm1 + plain::half_slope_rt(lim, wm2, wm1, w0);
           wR[n] = w0 - plain::half_slope_rt(lim, wm1, w0, wp1);
         }
-        wL[BX] = wR[BX] = b[I.sv + c];
       }
+      if (ORDER == 0) wL[BX] = wR[BX] = load_face<1>(I, b, i, j, mx, my, interior);
+      else wL[BX] = wR[BX] = b[I.sv + (long long)j * I.nx + i];
       double f[NM];
       riemann<RS>(f, wL, wR, I.gam, err);
       // local -> global (godunov.pyx:297-324 for the y sweep)
-      const int q = L.fy(fi, fj);
-      sFY[0 * L.nfy + q] = f[RHO];
-      sFY[1 * L.nfy + q] = f[VZ];   // global MX
-      sFY[2 * L.nfy + q] = f[VX];   // global MY
-      sFY[3 * L.nfy + q] = f[VY];   // global MZ
-      sFY[4 * L.nfy + q] = f[EN];
-      sFY[5 * L.nfy + q] = f[PSC];
-      sFY[6 * L.nfy + q] = f[BZ];   // fy[BX]
-      sFY[7 * L.nfy + q] = f[BY];   // fy[BZ]
+      const int qq = L.fy(fi, fj);
+      sFY[0 * L.nfy + qq] = f[RHO];
+      sFY[1 * L.nfy + qq] = f[VZ];   // global MX
+      sFY[2 * L.nfy + qq] = f[VX];   // global MY
+      sFY[3 * L.nfy + qq] = f[VY];   // global MZ
+      sFY[4 * L.nfy + qq] = f[EN];
+      sFY[5 * L.nfy + qq] = f[PSC];
+      sFY[6 * L.nfy + qq] = f[BZ];   // fy[BX]
+      sFY[7 * L.nfy + qq] = f[BY];   // fy[BZ]
     } else {
       // cell-centred E_z = -(vx by - vy bx) (ct.pyx:148)
       const int u = t - L.nfx - L.nfy;
-      const int ci = u % (L.wx + 2) - 1, cj = u / (L.wx + 2) - 1;
-      const int i = T.x0 + ci, j = T.y0 + cj;
-      double vx, vy, bxc, byc;
-      if (ORDER == 0 && !interior) {
-        double ww[NM];
-        load_prim_all(I, w, i, j, mx, my, false, ww);
-        vx = ww[VX]; vy = ww[VY]; bxc = ww[BX]; byc = ww[BY];
-      } else {
-        const long long c = (long long)j * I.nx + i;
-        vx = w[VX * I.sv + c]; vy = w[VY * I.sv + c]; bxc = w[BX * I.sv + c]; byc = w[BY * I.sv + c];
-      }
+      const int q = dx2.div(u);
+      const int ci = u - q * (L.wx + 2) - 1, cj = q - 1;
+      const int c = S.at(0, T.x0 + ci, T.y0 + cj);
+      const double vx = sW[VX * nc + c], vy = sW[VY * nc + c], bxc = sW[BX * nc + c], byc = sW[BY * nc + c];
       sEC[L.ec(ci, cj)] = -(vx * byc - vy * bxc);
     }
   }
@@ -360,9 +404,9 @@ __device__ __forceinline__ void stage_inst(Inst& sI, const Inst* __restrict__ in
   __syncthreads();
 }
 
-template <int TXM, int TYM, int RS>
+template <int TXM, int TYM, int RS, int RING = 1>
 __global__ void __launch_bounds__(256, 2) k_pred2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
-                                                int parity, int lim, unsigned* err) {
+                                                   int parity, int lim, unsigned* err) {
   extern __shared__ double smem[];
   __shared__ Inst sI;
   const Tile T = tiles[blockIdx.x];
@@ -374,26 +418,40 @@ __global__ void __launch_bounds__(256, 2) k_pred2d(const Inst* __restrict__ inst
   Layout L;
   L.set(T.wx, T.wy);
   double* sFX = smem;
-  double* sFY = sFX + NF * Smem<TXM, TYM>::NFX;
-  double* sEC = sFY + NF * Smem<TXM, TYM>::NFY;
-  double* sEE = sEC + Smem<TXM, TYM>::NEC;
+  double* sFY = sFX + NF * Smem<TXM, TYM, RING>::NFX;
+  double* sEC = sFY + NF * Smem<TXM, TYM, RING>::NFY;
+  double* sEE = sEC + Smem<TXM, TYM, RING>::NEC;
+  double* sW = sEE + Smem<TXM, TYM, RING>::NEE;
   const double* __restrict__ w = I.w[parity];
   const double* __restrict__ b = I.b[parity];
   // a tile whose one-cell ring lies inside the active range needs no ghost mapping
   const bool interior = T.x0 - 1 >= I.ng && T.x0 + T.wx <= I.ng + I.N[0] - 1 && T.y0 - 1 >= I.ng &&
                         T.y0 + T.wy <= I.ng + I.N[1] - 1;
+  Stage S;
+  S.x0 = T.x0 - 1;
+  S.y0 = T.y0 - 1;
+  S.w = T.wx + 2;
+  S.h = T.wy + 2;
+  if (interior) stage_cells<false>(I, w, S, sW);
+  else stage_cells<true>(I, w, S, sW);
+  __syncthreads();
   unsigned e = 0;
-  stage_fluxes<0, RS>(I, T, L, w, b, sFX, sFY, sEC, lim, interior, e);
+  stage_fluxes<0, RS>(I, T, L, S, sW, b, sFX, sFY, sEC, lim, interior, e);
   __syncthreads();
   stage_emf(L, sFX, sFY, sEC, sEE);
   __syncthreads();
   const AxisMap mx = axis_map(I, 0), my = axis_map(I, 1);
   const int ilast = I.nx - 2, jlast = I.ny - 2;  // last predictor cell (vanleer lims)
+  const int nc = S.cells();
+  FastDiv dwx;
+  dwx.set(T.wx);
   for (int t = threadIdx.x; t < T.wx * T.wy; t += blockDim.x) {
-    const int ci = t % T.wx, cj = t / T.wx;
+    const int cj = dwx.div(t), ci = t - cj * T.wx;
     const int i = T.x0 + ci, j = T.y0 + cj;
     double wn[NM], un[NM];
-    load_prim_all(I, w, i, j, mx, my, interior, wn);
+    const int cs = S.at(0, i, j);
+#pragma unroll
+    for (int n = 0; n < NM; ++n) wn[n] = sW[n * nc + cs];
     prim2cons(un, wn, I.gam);
     double bxl0 = load_face<0>(I, b, i, j, mx, my, interior);
     double bxr0 = load_face<0>(I, b, i + 1, j, mx, my, interior);
@@ -431,7 +489,7 @@ __device__ __forceinline__ void copy_tile(const Inst& I, const Tile& T, int pari
   }
 }
 
-template <int TXM, int TYM, int RS>
+template <int TXM, int TYM, int RS, int RING = 2>
 __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
                                                 int parity, int lim, double cour, unsigned* err) {
   extern __shared__ double smem[];
@@ -449,11 +507,19 @@ __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ inst
   Layout L;
   L.set(T.wx, T.wy);
   double* sFX = smem;
-  double* sFY = sFX + NF * Smem<TXM, TYM>::NFX;
-  double* sEC = sFY + NF * Smem<TXM, TYM>::NFY;
-  double* sEE = sEC + Smem<TXM, TYM>::NEC;
+  double* sFY = sFX + NF * Smem<TXM, TYM, RING>::NFX;
+  double* sEC = sFY + NF * Smem<TXM, TYM, RING>::NFY;
+  double* sEE = sEC + Smem<TXM, TYM, RING>::NEC;
+  double* sW = sEE + Smem<TXM, TYM, RING>::NEE;
+  Stage S;
+  S.x0 = T.x0 - 2;
+  S.y0 = T.y0 - 2;
+  S.w = T.wx + 4;
+  S.h = T.wy + 4;
+  stage_cells<false>(I, I.ws, S, sW);
+  __syncthreads();
   unsigned e = 0;
-  stage_fluxes<1, RS>(I, T, L, I.ws, I.bs, sFX, sFY, sEC, lim, true, e);
+  stage_fluxes<1, RS>(I, T, L, S, sW, I.bs, sFX, sFY, sEC, lim, true, e);
   __syncthreads();
   stage_emf(L, sFX, sFY, sEC, sEE);
   __syncthreads();
@@ -464,8 +530,10 @@ __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ inst
   const AxisMap mx = axis_map(I, 0), my = axis_map(I, 1);
   const int i2 = I.ng + I.N[0] - 1, j2 = I.ng + I.N[1] - 1;
   double cmax = 0.;
+  FastDiv dwx;
+  dwx.set(T.wx);
   for (int t = threadIdx.x; t < T.wx * T.wy; t += blockDim.x) {
-    const int ci = t % T.wx, cj = t / T.wx;
+    const int cj = dwx.div(t), ci = t - cj * T.wx;
     const int i = T.x0 + ci, j = T.y0 + cj;
     const long long c = (long long)j * I.nx + i;
     double wn[NM], un[NM];

@@ -274,8 +274,8 @@ int diff_stage_update(const StepArgs& a, const DiffArgs& d, int first, const dou
 
 namespace {
 constexpr int FA_TX = FUSED_TX + 4, FA_TY = FUSED_TY + 4;  // predictor tiles grow by the ghost rings
-constexpr size_t SMEM_A = fused::Smem<FA_TX, FA_TY>::bytes;
-constexpr size_t SMEM_B = fused::Smem<FUSED_TX, FUSED_TY>::bytes;
+constexpr size_t SMEM_A = fused::Smem<FA_TX, FA_TY, 1>::bytes;
+constexpr size_t SMEM_B = fused::Smem<FUSED_TX, FUSED_TY, 2>::bytes;
 
 template <int RS>
 void set_smem_attrs() {
