@@ -70,6 +70,7 @@ struct FusedInst {
   double* ws;          // predictor prim
   double* bs;          // predictor face field
   DtState* ds;
+  unsigned* err;       // the instance's sticky error word
 };
 
 // A tile of cells [x0, x0+wx) x [y0, y0+wy) (array coordinates) of one instance.

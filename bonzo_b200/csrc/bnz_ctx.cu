@@ -263,6 +263,7 @@ FusedInst make_inst(const bnz_ctx* c) {
   I.ws = c->cons_s;
   I.bs = c->bfld_s;
   I.ds = c->d_ds;
+  I.err = c->d_err;
   return I;
 }
 

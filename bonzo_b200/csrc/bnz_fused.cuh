@@ -201,14 +201,15 @@ struct Smem {
 // Corrector: ws on the tile plus two rings (the predictor wrote those cells).
 // ---------------------------------------------------------------------------
 
-// t / d for small t (t * d < 2^32) by a multiply-high
+// t / d for small t (t * d < 2^32) by a multiply-high with m = ceil(2^32 / d);
+// d = 1 (m would need 33 bits) is handled separately.
 struct FastDiv {
   unsigned d, m;
   __device__ __forceinline__ void set(unsigned dd) {
     d = dd;
-    m = 0xFFFFFFFFu / dd + 1u;
+    m = dd > 1u ? 0xFFFFFFFFu / dd + 1u : 0u;
   }
-  __device__ __forceinline__ unsigned div(unsigned t) const { return __umulhi(t, m); }
+  __device__ __forceinline__ unsigned div(unsigned t) const { return d > 1u ? __umulhi(t, m) : t; }
 };
 
 struct Stage {
@@ -469,7 +470,7 @@ __global__ void __launch_bounds__(256, 2) k_pred2d(const Inst* __restrict__ inst
     if (i == ilast) I.bs[c + 1] = o.bxr;
     if (j == jlast) I.bs[I.sv + c + I.nx] = o.byt;
   }
-  if (e) atomicOr(err, e);
+  if (e) atomicOr(I.err, e);
 }
 
 __device__ __forceinline__ void copy_tile(const Inst& I, const Tile& T, int parity) {
@@ -572,7 +573,7 @@ __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ inst
     for (int q = 0; q < (int)(blockDim.x >> 5); ++q) m = fmax(m, red[q]);
     if (m > 0.) atomicMax(&I.ds->cds_bits[parity ^ 1], (unsigned long long)__double_as_longlong(m));
   }
-  if (e) atomicOr(err, e);
+  if (e) atomicOr(I.err, e);
 }
 
 // Per-instance dt for the step of parity p (new_dt.pyx:117, vanleer.pyx:95-96):

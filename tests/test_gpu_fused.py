@@ -17,7 +17,8 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden")
 CASES = [("vortex", 32, {}), ("vortex", 40, dict(rsolver="hll")), ("vortex", 32, dict(rsolver="hllt")),
          ("vortex_pert", 48, dict(limiter="mc")), ("vortex_pert", 36, dict(limiter="mm")),
          ("blast", 40, {}), ("blast", 33, dict(outflow_face_aware=0)), ("blast_reflect", 34, {}),
-         ("mixed_bc", 37, {}), ("cond2d", 32, {}), ("vortex", 8, {}), ("vortex", 70, {})]
+         ("mixed_bc", 37, {}), ("cond2d", 32, {}), ("vortex", 8, {}), ("vortex", 70, {}),
+         ("vortex", 65, {}), ("blast", 97, {})]
 
 
 @pytest.mark.parametrize("case,n,kw", CASES)
