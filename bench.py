@@ -253,6 +253,17 @@ def run_ours(args, rank, world, dist):
         torch.cuda.empty_cache()
 
     eng, ctxs, step, count = make_engine(args.path, batch, stream)
+    tune = None
+    if args.path == "batch":
+        # autotuner: tile shape / staging on this workload (state restored after each trial)
+        from bonzo_b200 import autotune
+        best, ms = autotune.tune_batch(eng, [q["N"] for q, _, _, _ in batch], METHOD["rsolver"],
+                                       METHOD["limiter"], steps=2, use_cache=False)
+        from bonzo_b200._lib import variants
+        vs = variants()
+        tune = {"chosen": {"tile": "%dx%d" % vs[best][:2], "staged_predictor": bool(vs[best][2])},
+                "ms_per_step": {"%dx%d%s" % (vs[v][0], vs[v][1], "s" if vs[v][2] else ""): round(t, 4)
+                                for v, t in ms.items()}}
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -305,7 +316,8 @@ def run_ours(args, rank, world, dist):
                    "instances": len(ctxs), "zones_per_step_per_gpu": zones, "path": args.path,
                    "l2": "inputs larger than L2 (%.0f MB of state)" % (
                        sum(12 * 8 * np.prod(c.shape) for c in ctxs) / 1e6),
-                   "parallelism": "instances sharded per GPU (dp%d, no collective)" % world},
+                   "parallelism": "instances sharded per GPU (dp%d, no collective)" % world,
+                   "autotune": tune},
         "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(h2d),
                 "how": "bnz_set_state of every instance, one batch step, bnz_get_state of every "

@@ -29,7 +29,8 @@ EXPORTS = [
     "bnz_device_state", "bnz_stream", "bnz_set_stream", "bnz_launch_count",
     "bnz_batch_create", "bnz_batch_destroy", "bnz_batch_last_error", "bnz_batch_size",
     "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_set_stream", "bnz_batch_launch_count",
-    "bnz_batch_sync",
+    "bnz_batch_sync", "bnz_variant_count", "bnz_batch_set_variant", "bnz_batch_get_variant",
+    "bnz_batch_time_variant", "bnz_batch_autotune",
 ]
 
 
@@ -99,6 +100,12 @@ def load():
     L.bnz_batch_set_stream.argtypes = [vp, vp]
     L.bnz_batch_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.bnz_batch_sync.argtypes = [vp]
+    ip = C.POINTER(C.c_int)
+    L.bnz_variant_count.argtypes = [ip, ip, ip, ip]
+    L.bnz_batch_set_variant.argtypes = [vp, C.c_int]
+    L.bnz_batch_get_variant.argtypes = [vp, ip]
+    L.bnz_batch_time_variant.argtypes = [vp, C.c_int, C.c_int, _dp]
+    L.bnz_batch_autotune.argtypes = [vp, C.c_int, ip, _dp]
     _lib = L
     return L
 
@@ -317,6 +324,21 @@ class Batch:
     def sync(self):
         self._ck(self.L.bnz_batch_sync(self.h))
 
+    @property
+    def variant(self):
+        v = C.c_int()
+        self._ck(self.L.bnz_batch_get_variant(self.h, C.byref(v)))
+        return v.value
+
+    def set_variant(self, v):
+        self._ck(self.L.bnz_batch_set_variant(self.h, int(v)))
+
+    def time_variant(self, v, steps=2):
+        """ms per batch step of variant v (state restored afterwards)."""
+        ms = C.c_double()
+        self._ck(self.L.bnz_batch_time_variant(self.h, int(v), int(steps), C.byref(ms)))
+        return ms.value
+
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:
             for c in self.instances:
@@ -329,3 +351,13 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def variants():
+    """[(tx, ty, staged)] of the fused kernel variants."""
+    L = load()
+    n = C.c_int()
+    L.bnz_variant_count(C.byref(n), None, None, None)
+    tx, ty, st = (C.c_int * n.value)(), (C.c_int * n.value)(), (C.c_int * n.value)()
+    L.bnz_variant_count(C.byref(n), tx, ty, st)
+    return [(tx[v], ty[v], st[v]) for v in range(n.value)]

@@ -80,9 +80,16 @@ struct FusedTile {
   int wx, wy;
 };
 
-// Tile shape of the fused kernels (cells per tile along x, y).
-constexpr int FUSED_TX = 32;
-constexpr int FUSED_TY = 8;
+// Variants of the fused kernels the autotuner chooses from: tile shape
+// (cells along x, y) and whether the predictor stages its input cells in
+// shared memory.  Variant 0 is the default and exists for every Riemann
+// solver; the others are built for HLLD.
+struct FusedVariant {
+  int tx, ty, staged;
+};
+constexpr int FUSED_NVARIANT = 5;
+constexpr FusedVariant FUSED_VARIANTS[FUSED_NVARIANT] = {
+    {32, 8, 0}, {32, 8, 1}, {16, 16, 0}, {16, 16, 1}, {64, 4, 0}};
 
 // dt modes of the fused step
 enum { FDT_CFL = 0, FDT_EXPLICIT = 1, FDT_FIXED = 2 };
@@ -95,6 +102,7 @@ struct FusedLaunch {
   const FusedTile* tilesB;  // corrector tiles (active cells)
   int ntB;
   int rsolver, limiter;
+  int variant;
   double cour;
   int dt_mode;
   double dt_fixed;

@@ -44,6 +44,7 @@ struct bnz_ctx {
   FusedTile* d_tiles = nullptr;
   int ntA = 0, ntB = 0;
   int graph_parity = -1;
+  int variant = 0;
   // conduction scratch
   double* dscr = nullptr;
   DiffArgs da;
@@ -207,10 +208,10 @@ bool fused_available(const bnz_grid_desc* g, const bnz_method_desc* m) {
   return g->dims == 2 && m->reconstr == BNZ_RCN_LINEAR;
 }
 
-// Tiles of FUSED_TX x FUSED_TY cells over the active range; the predictor's
-// edge tiles also cover the two ghost rings it updates (cells 1..Ntot-2).
-void make_tiles(int inst, int N0, int N1, int ng, bool pred, std::vector<FusedTile>& out) {
-  const int T[2] = {FUSED_TX, FUSED_TY};
+// Tiles of tx x ty cells over the active range; the predictor's edge tiles
+// also cover the two ghost rings it updates (cells 1..Ntot-2).
+void make_tiles(int inst, int N0, int N1, int ng, bool pred, int tx, int ty, std::vector<FusedTile>& out) {
+  const int T[2] = {tx, ty};
   const int N[2] = {N0, N1};
   int nt[2];
   for (int a = 0; a < 2; ++a) nt[a] = (N[a] + T[a] - 1) / T[a];
@@ -281,12 +282,29 @@ FusedLaunch fused_launch(const bnz_ctx* c, int dt_mode) {
   f.ntB = c->ntB;
   f.rsolver = c->md.rsolver;
   f.limiter = c->md.limiter;
+  f.variant = c->variant;
   f.cour = c->md.cour;
   f.dt_mode = dt_mode;
   f.dt_fixed = c->md.dt_fixed;
   f.err = c->d_err;
   f.stream = c->stream;
   return f;
+}
+
+// (Re)build the single-grid tile lists for the context's variant.
+cudaError_t build_ctx_tiles(bnz_ctx* c) {
+  const FusedVariant& v = FUSED_VARIANTS[c->variant];
+  std::vector<FusedTile> tiles;
+  make_tiles(0, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->ng, true, v.tx, v.ty, tiles);
+  c->ntA = (int)tiles.size();
+  make_tiles(0, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->ng, false, v.tx, v.ty, tiles);
+  c->ntB = (int)tiles.size() - c->ntA;
+  if (c->d_tiles) cudaFree(c->d_tiles);
+  c->d_tiles = nullptr;
+  cudaError_t e = cudaMalloc((void**)&c->d_tiles, tiles.size() * sizeof(FusedTile));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(c->d_tiles, tiles.data(), tiles.size() * sizeof(FusedTile), cudaMemcpyHostToDevice);
+  return e;
 }
 
 int validate(const bnz_grid_desc* g, const bnz_method_desc* m, std::string& why) {
@@ -466,15 +484,8 @@ int bnz_create(const bnz_grid_desc* gd, const bnz_method_desc* md, bnz_ctx** out
   e = cudaMalloc((void**)&c->d_err, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_ds, sizeof(DtState));
   if (e == cudaSuccess && md->path == BNZ_PATH_FUSED) {
-    std::vector<FusedTile> tiles;
-    make_tiles(0, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, ng, true, tiles);
-    c->ntA = (int)tiles.size();
-    make_tiles(0, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, ng, false, tiles);
-    c->ntB = (int)tiles.size() - c->ntA;
-    e = cudaMalloc((void**)&c->d_tiles, tiles.size() * sizeof(FusedTile));
+    e = build_ctx_tiles(c);
     if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_inst, sizeof(FusedInst));
-    if (e == cudaSuccess)
-      e = cudaMemcpy(c->d_tiles, tiles.data(), tiles.size() * sizeof(FusedTile), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
       FusedInst I = make_inst(c);
       e = cudaMemcpy(c->d_inst, &I, sizeof I, cudaMemcpyHostToDevice);
@@ -937,6 +948,7 @@ struct bnz_batch {
   long long launches = 0;
   long long graph_launches = 0;
   double h_tmax = 0.;
+  int variant = 0;
   const Launchers* L = nullptr;
   std::string err;
 };
@@ -966,12 +978,36 @@ FusedLaunch batch_launch(const bnz_batch* b, int dt_mode) {
   f.ntB = b->ntB;
   f.rsolver = b->md.rsolver;
   f.limiter = b->md.limiter;
+  f.variant = b->variant;
   f.cour = b->md.cour;
   f.dt_mode = dt_mode;
   f.dt_fixed = b->md.dt_fixed;
   f.err = b->ctx.empty() ? nullptr : b->ctx[0]->d_err;
   f.stream = b->stream;
   return f;
+}
+
+// Tile lists of every instance for the batch's variant (predictor list first).
+int batch_build_tiles(bnz_batch* b) {
+  const FusedVariant& v = FUSED_VARIANTS[b->variant];
+  std::vector<FusedTile> tA, tB;
+  for (int q = 0; q < (int)b->ctx.size(); ++q) {
+    const bnz_ctx* c = b->ctx[q];
+    make_tiles(q, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->ng, true, v.tx, v.ty, tA);
+    make_tiles(q, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->ng, false, v.tx, v.ty, tB);
+  }
+  b->ntA = (int)tA.size();
+  b->ntB = (int)tB.size();
+  tA.insert(tA.end(), tB.begin(), tB.end());
+  if (b->d_tiles) cudaFree(b->d_tiles);
+  b->d_tiles = nullptr;
+  CKB(cudaMalloc((void**)&b->d_tiles, tA.size() * sizeof(FusedTile)));
+  CKB(cudaMemcpy(b->d_tiles, tA.data(), tA.size() * sizeof(FusedTile), cudaMemcpyHostToDevice));
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  return BNZ_OK;
 }
 
 __global__ void k_set_tmax(FusedInst* insts, int n, double tmax) {
@@ -993,7 +1029,6 @@ int bnz_batch_create(const bnz_grid_desc* grids, int n, const bnz_method_desc* m
   cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bfail(b, BNZ_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
   std::vector<FusedInst> insts;
-  std::vector<FusedTile> tA, tB;
   for (int q = 0; q < n; ++q) {
     bnz_ctx* c = nullptr;
     int rc = bnz_create(&grids[q], &b->md, &c);
@@ -1006,19 +1041,11 @@ int bnz_batch_create(const bnz_grid_desc* grids, int n, const bnz_method_desc* m
     rc = bnz_set_stream(c, (void*)b->stream);
     if (rc) return bfail(b, rc, c->err);
     insts.push_back(make_inst(c));
-    make_tiles(q, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->ng, true, tA);
-    make_tiles(q, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->ng, false, tB);
   }
   b->L = b->ctx[0]->L;
-  b->ntA = (int)tA.size();
-  b->ntB = (int)tB.size();
-  std::vector<FusedTile> all(tA);
-  all.insert(all.end(), tB.begin(), tB.end());
   CKB(cudaMalloc((void**)&b->d_inst, insts.size() * sizeof(FusedInst)));
-  CKB(cudaMalloc((void**)&b->d_tiles, all.size() * sizeof(FusedTile)));
   CKB(cudaMemcpy(b->d_inst, insts.data(), insts.size() * sizeof(FusedInst), cudaMemcpyHostToDevice));
-  CKB(cudaMemcpy(b->d_tiles, all.data(), all.size() * sizeof(FusedTile), cudaMemcpyHostToDevice));
-  return BNZ_OK;
+  return batch_build_tiles(b);
 }
 
 int bnz_batch_destroy(bnz_batch* b) {
@@ -1141,6 +1168,103 @@ int bnz_batch_sync(bnz_batch* b) {
   if (!b) return BNZ_ERR_ARG;
   CKB(cudaStreamSynchronize(b->stream));
   return BNZ_OK;
+}
+
+int bnz_variant_count(int* n, int* tx, int* ty, int* staged) {
+  if (n) *n = FUSED_NVARIANT;
+  for (int v = 0; v < FUSED_NVARIANT; ++v) {
+    if (tx) tx[v] = FUSED_VARIANTS[v].tx;
+    if (ty) ty[v] = FUSED_VARIANTS[v].ty;
+    if (staged) staged[v] = FUSED_VARIANTS[v].staged;
+  }
+  return BNZ_OK;
+}
+
+int bnz_batch_set_variant(bnz_batch* b, int v) {
+  if (!b) return BNZ_ERR_ARG;
+  if (v < 0 || v >= FUSED_NVARIANT) return bfail(b, BNZ_ERR_ARG, "variant out of range");
+  if (v != 0 && b->md.rsolver != BNZ_RS_HLLD) return bfail(b, BNZ_ERR_UNSUPPORTED, "variants 1.. are built for hlld");
+  if (v == b->variant) return BNZ_OK;
+  CKB(cudaStreamSynchronize(b->stream));
+  b->variant = v;
+  return batch_build_tiles(b);
+}
+
+int bnz_batch_get_variant(const bnz_batch* b, int* v) {
+  if (!b || !v) return BNZ_ERR_ARG;
+  *v = b->variant;
+  return BNZ_OK;
+}
+
+// Time `steps` batch steps of variant v (after one untimed step) on the live
+// state, then put the state, the time records and the variant back.
+int bnz_batch_time_variant(bnz_batch* b, int v, int steps, double* ms) {
+  if (!b || steps < 1) return BNZ_ERR_ARG;
+  const int v0 = b->variant, p0 = b->parity;
+  int rc = bnz_batch_set_variant(b, v);
+  if (rc) return rc;
+  // save every instance's state of the current parity and its time record
+  std::vector<double*> saved(b->ctx.size(), nullptr);
+  std::vector<DtState> dts(b->ctx.size());
+  for (size_t q = 0; q < b->ctx.size(); ++q) {
+    bnz_ctx* c = b->ctx[q];
+    size_t n9 = 9 * c->ncell, n3 = 3 * c->ncell;
+    CKB(cudaMalloc((void**)&saved[q], (n9 + n3) * sizeof(double)));
+    CKB(cudaMemcpyAsync(saved[q], c->wbuf[p0], n9 * sizeof(double), cudaMemcpyDeviceToDevice, b->stream));
+    CKB(cudaMemcpyAsync(saved[q] + n9, c->bbuf[p0], n3 * sizeof(double), cudaMemcpyDeviceToDevice, b->stream));
+    CKB(cudaMemcpyAsync(&dts[q], c->d_ds, sizeof(DtState), cudaMemcpyDeviceToHost, b->stream));
+  }
+  CKB(cudaStreamSynchronize(b->stream));
+  const int mode = b->md.fixdt ? FDT_FIXED : FDT_CFL;
+  cudaEvent_t e0, e1;
+  CKB(cudaEventCreate(&e0));
+  CKB(cudaEventCreate(&e1));
+  int p = p0;
+  for (int s = 0; s <= steps; ++s) {
+    if (s == 1) CKB(cudaEventRecord(e0, b->stream));
+    b->L->fused_step(batch_launch(b, mode), p);
+    p ^= 1;
+  }
+  CKB(cudaEventRecord(e1, b->stream));
+  CKB(cudaEventSynchronize(e1));
+  float t = 0.f;
+  CKB(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (ms) *ms = t / steps;
+  for (size_t q = 0; q < b->ctx.size(); ++q) {
+    bnz_ctx* c = b->ctx[q];
+    size_t n9 = 9 * c->ncell, n3 = 3 * c->ncell;
+    CKB(cudaMemcpyAsync(c->wbuf[p0], saved[q], n9 * sizeof(double), cudaMemcpyDeviceToDevice, b->stream));
+    CKB(cudaMemcpyAsync(c->bbuf[p0], saved[q] + n9, n3 * sizeof(double), cudaMemcpyDeviceToDevice, b->stream));
+    CKB(cudaMemcpyAsync(c->d_ds, &dts[q], sizeof(DtState), cudaMemcpyHostToDevice, b->stream));
+  }
+  CKB(cudaStreamSynchronize(b->stream));
+  for (double* ptr : saved) cudaFree(ptr);
+  b->parity = p0;
+  for (bnz_ctx* c : b->ctx) set_parity(c, p0);
+  return bnz_batch_set_variant(b, v0);
+}
+
+int bnz_batch_autotune(bnz_batch* b, int steps, int* best, double* ms_per_variant) {
+  if (!b) return BNZ_ERR_ARG;
+  int nv = b->md.rsolver == BNZ_RS_HLLD ? FUSED_NVARIANT : 1;
+  double best_ms = 1e300;
+  int bv = 0;
+  for (int v = 0; v < FUSED_NVARIANT; ++v) {
+    double ms = -1.;
+    if (v < nv) {
+      int rc = bnz_batch_time_variant(b, v, steps, &ms);
+      if (rc) return rc;
+      if (ms < best_ms) {
+        best_ms = ms;
+        bv = v;
+      }
+    }
+    if (ms_per_variant) ms_per_variant[v] = ms;
+  }
+  if (best) *best = bv;
+  return bnz_batch_set_variant(b, bv);
 }
 
 }  // extern "C"

@@ -191,7 +191,7 @@ struct Smem {
   static constexpr int NFY = (TXM + 2) * (TYM + 1);
   static constexpr int NEC = (TXM + 2) * (TYM + 2);
   static constexpr int NEE = (TXM + 1) * (TYM + 1);
-  static constexpr int NSW = NM * (TXM + 2 * RING) * (TYM + 2 * RING);  // staged cells
+  static constexpr int NSW = RING ? NM * (TXM + 2 * RING) * (TYM + 2 * RING) : 0;  // staged cells
   static constexpr size_t bytes = sizeof(double) * ((size_t)NF * (NFX + NFY) + NEC + NEE + NSW);
 };
 
@@ -241,19 +241,44 @@ __device__ __forceinline__ void stage_cells(const Inst& I, const double* __restr
   }
 }
 
+// Cell readers for the flux stage: staged shared memory, or global memory
+// with the BC map applied on the fly.
+struct SmemCells {
+  const double* sW;
+  Stage S;
+  int nc;
+  __device__ __forceinline__ double get(int n, int i, int j) const { return sW[n * nc + S.at(0, i, j)]; }
+  // value at (i, j) shifted by `o` cells along the axis with stride `st` (1: x, S.w: y)
+  __device__ __forceinline__ const double* ptr(int n, int i, int j) const { return sW + n * nc + S.at(0, i, j); }
+  __device__ __forceinline__ int stride(int ax) const { return ax == 0 ? 1 : S.w; }
+};
+
+struct GlobalCells {
+  const Inst* I;
+  const double* w;
+  AxisMap mx, my;
+  bool interior;
+  __device__ __forceinline__ double get(int n, int i, int j) const {
+    if (interior) return w[n * I->sv + (long long)j * I->nx + i];
+    bool fx, fy;
+    const int si = map_cell(i, mx, fx), sj = map_cell(j, my, fy);
+    double v = w[n * I->sv + (long long)sj * I->nx + si];
+    return ((fx && (n == VX || n == BX)) || (fy && (n == VY || n == BY))) ? -v : v;
+  }
+};
+
 // ---------------------------------------------------------------------------
-// Stage 1 of both kernels: interface fluxes and cell-centred EMF from the
-// staged cells.  ORDER 0 (predictor): donor cell, normal B from b with the BC
-// map.  ORDER 1 (corrector): PLM, normal B from bs.
+// Stage 1 of both kernels: interface fluxes and cell-centred EMF.
+// ORDER 0 (predictor): donor cell, normal B from b with the BC map.
+// ORDER 1 (corrector): PLM from staged ws, normal B from bs.
 // ---------------------------------------------------------------------------
 
-template <int ORDER, int RS>
-__device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const Layout& L, const Stage& S,
-                                             const double* sW, const double* __restrict__ b, double* sFX,
-                                             double* sFY, double* sEC, int lim, bool interior, unsigned& err) {
+template <int ORDER, int RS, class Cells>
+__device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const Layout& L, const Cells& W,
+                                             const double* __restrict__ b, double* sFX, double* sFY, double* sEC,
+                                             int lim, bool interior, unsigned& err) {
   const AxisMap mx = axis_map(I, 0), my = axis_map(I, 1);
   const int total = L.nfx + L.nfy + L.nec;
-  const int nc = S.cells();
   FastDiv dx1, dx2;
   dx1.set(L.wx + 1);
   dx2.set(L.wx + 2);
@@ -264,15 +289,14 @@ __device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const
       const int fi = t - q * (L.wx + 1), fj = q - 1;
       const int i = T.x0 + fi, j = T.y0 + fj;
       double wL[NM], wR[NM];
-      const int c = S.at(0, i, j);
 #pragma unroll
       for (int n = 0; n < NM; ++n) {
         if (n == BX) continue;
-        const double* a = sW + n * nc + c;
-        if (ORDER == 0) {
-          wL[n] = a[-1];
-          wR[n] = a[0];
+        if constexpr (ORDER == 0) {
+          wL[n] = W.get(n, i - 1, j);
+          wR[n] = W.get(n, i, j);
         } else {
+          const double* a = W.ptr(n, i, j);
           double wm2 = a[-2], wm1 = a[-1], w0 = a[0], wp1 = a[1];
           wL[n] = wm1 + plain::half_slope_rt(lim, wm2, wm1, w0);
           wR[n] = w0 - plain::half_slope_rt(lim, wm1, w0, wp1);
@@ -294,16 +318,16 @@ __device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const
       const int fi = u - q * (L.wx + 2) - 1, fj = q;
       const int i = T.x0 + fi, j = T.y0 + fj;
       double wL[NM], wR[NM];
-      const int c = S.at(0, i, j);
-      const int sy = S.w;
 #pragma unroll
       for (int n = 0; n < NM; ++n) {
         if (n == BX) continue;
-        const double* a = sW + plain::perm<1>(n) * nc + c;
-        if (ORDER == 0) {
-          wL[n] = a[-sy];
-          wR[n] = a[0];
+        const int gv = plain::perm<1>(n);
+        if constexpr (ORDER == 0) {
+          wL[n] = W.get(gv, i, j - 1);
+          wR[n] = W.get(gv, i, j);
         } else {
+          const double* a = W.ptr(gv, i, j);
+          const int sy = W.stride(1);
           double wm2 = a[-2 * sy], wm1 = a[-sy], w0 = a[0], wp1 = a[sy];
           wL[n] = wm1 + plain::half_slope_rt(lim, wm2, wm1, w0);
           wR[n] = w0 - plain::half_slope_rt(lim, wm1, w0, wp1);
@@ -328,8 +352,8 @@ __device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const
       const int u = t - L.nfx - L.nfy;
       const int q = dx2.div(u);
       const int ci = u - q * (L.wx + 2) - 1, cj = q - 1;
-      const int c = S.at(0, T.x0 + ci, T.y0 + cj);
-      const double vx = sW[VX * nc + c], vy = sW[VY * nc + c], bxc = sW[BX * nc + c], byc = sW[BY * nc + c];
+      const int i = T.x0 + ci, j = T.y0 + cj;
+      const double vx = W.get(VX, i, j), vy = W.get(VY, i, j), bxc = W.get(BX, i, j), byc = W.get(BY, i, j);
       sEC[L.ec(ci, cj)] = -(vx * byc - vy * bxc);
     }
   }
@@ -405,9 +429,12 @@ __device__ __forceinline__ void stage_inst(Inst& sI, const Inst* __restrict__ in
   __syncthreads();
 }
 
-template <int TXM, int TYM, int RS, int RING = 1>
+// Predictor.  STAGED = 1 copies w^n (tile + one ring, BC-mapped) into shared
+// memory first; STAGED = 0 reads it from global memory in the flux stage.
+template <int TXM, int TYM, int RS, int STAGED>
 __global__ void __launch_bounds__(256, 2) k_pred2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
-                                                   int parity, int lim, unsigned* err) {
+                                                   int parity, int lim) {
+  constexpr int RING = STAGED ? 1 : 0;
   extern __shared__ double smem[];
   __shared__ Inst sI;
   const Tile T = tiles[blockIdx.x];
@@ -428,31 +455,40 @@ __global__ void __launch_bounds__(256, 2) k_pred2d(const Inst* __restrict__ inst
   // a tile whose one-cell ring lies inside the active range needs no ghost mapping
   const bool interior = T.x0 - 1 >= I.ng && T.x0 + T.wx <= I.ng + I.N[0] - 1 && T.y0 - 1 >= I.ng &&
                         T.y0 + T.wy <= I.ng + I.N[1] - 1;
+  const AxisMap mx = axis_map(I, 0), my = axis_map(I, 1);
   Stage S;
   S.x0 = T.x0 - 1;
   S.y0 = T.y0 - 1;
   S.w = T.wx + 2;
   S.h = T.wy + 2;
-  if (interior) stage_cells<false>(I, w, S, sW);
-  else stage_cells<true>(I, w, S, sW);
-  __syncthreads();
   unsigned e = 0;
-  stage_fluxes<0, RS>(I, T, L, S, sW, b, sFX, sFY, sEC, lim, interior, e);
+  if constexpr (STAGED) {
+    if (interior) stage_cells<false>(I, w, S, sW);
+    else stage_cells<true>(I, w, S, sW);
+    __syncthreads();
+    SmemCells W{sW, S, S.cells()};
+    stage_fluxes<0, RS>(I, T, L, W, b, sFX, sFY, sEC, lim, interior, e);
+  } else {
+    GlobalCells W{&I, w, mx, my, interior};
+    stage_fluxes<0, RS>(I, T, L, W, b, sFX, sFY, sEC, lim, interior, e);
+  }
   __syncthreads();
   stage_emf(L, sFX, sFY, sEC, sEE);
   __syncthreads();
-  const AxisMap mx = axis_map(I, 0), my = axis_map(I, 1);
   const int ilast = I.nx - 2, jlast = I.ny - 2;  // last predictor cell (vanleer lims)
-  const int nc = S.cells();
   FastDiv dwx;
   dwx.set(T.wx);
   for (int t = threadIdx.x; t < T.wx * T.wy; t += blockDim.x) {
     const int cj = dwx.div(t), ci = t - cj * T.wx;
     const int i = T.x0 + ci, j = T.y0 + cj;
     double wn[NM], un[NM];
-    const int cs = S.at(0, i, j);
+    if constexpr (STAGED) {
+      const int cs = S.at(0, i, j);
 #pragma unroll
-    for (int n = 0; n < NM; ++n) wn[n] = sW[n * nc + cs];
+      for (int n = 0; n < NM; ++n) wn[n] = sW[n * S.cells() + cs];
+    } else {
+      load_prim_all(I, w, i, j, mx, my, interior, wn);
+    }
     prim2cons(un, wn, I.gam);
     double bxl0 = load_face<0>(I, b, i, j, mx, my, interior);
     double bxr0 = load_face<0>(I, b, i + 1, j, mx, my, interior);
@@ -490,9 +526,10 @@ __device__ __forceinline__ void copy_tile(const Inst& I, const Tile& T, int pari
   }
 }
 
-template <int TXM, int TYM, int RS, int RING = 2>
+template <int TXM, int TYM, int RS>
 __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
-                                                int parity, int lim, double cour, unsigned* err) {
+                                                   int parity, int lim) {
+  constexpr int RING = 2;
   extern __shared__ double smem[];
   __shared__ double red[8];
   __shared__ Inst sI;
@@ -520,7 +557,8 @@ __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ inst
   stage_cells<false>(I, I.ws, S, sW);
   __syncthreads();
   unsigned e = 0;
-  stage_fluxes<1, RS>(I, T, L, S, sW, I.bs, sFX, sFY, sEC, lim, true, e);
+  SmemCells W{sW, S, S.cells()};
+  stage_fluxes<1, RS>(I, T, L, W, I.bs, sFX, sFY, sEC, lim, true, e);
   __syncthreads();
   stage_emf(L, sFX, sFY, sEC, sEE);
   __syncthreads();

@@ -273,26 +273,36 @@ int diff_stage_update(const StepArgs& a, const DiffArgs& d, int first, const dou
 // --- fused 2D path (one launch per stage for the whole batch) --------------
 
 namespace {
-constexpr int FA_TX = FUSED_TX + 4, FA_TY = FUSED_TY + 4;  // predictor tiles grow by the ghost rings
-constexpr size_t SMEM_A = fused::Smem<FA_TX, FA_TY, 1>::bytes;
-constexpr size_t SMEM_B = fused::Smem<FUSED_TX, FUSED_TY, 2>::bytes;
 
-template <int RS>
-void set_smem_attrs() {
-  static bool done = false;
-  if (done) return;
-  cudaFuncSetAttribute(fused::k_pred2d<FA_TX, FA_TY, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_A);
-  cudaFuncSetAttribute(fused::k_corr2d<FUSED_TX, FUSED_TY, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)SMEM_B);
-  done = true;
+template <int TX, int TY, int RS, int STAGED>
+void launch_variant(const FusedLaunch& f, int parity) {
+  constexpr int TXA = TX + 4, TYA = TY + 4;  // predictor tiles grow by the ghost rings
+  constexpr size_t smA = fused::Smem<TXA, TYA, STAGED ? 1 : 0>::bytes;
+  constexpr size_t smB = fused::Smem<TX, TY, 2>::bytes;
+  static bool attrs = false;
+  if (!attrs) {
+    cudaFuncSetAttribute(fused::k_pred2d<TXA, TYA, RS, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smA);
+    cudaFuncSetAttribute(fused::k_corr2d<TX, TY, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB);
+    attrs = true;
+  }
+  fused::k_pred2d<TXA, TYA, RS, STAGED><<<f.ntA, 256, smA, f.stream>>>(f.insts, f.tilesA, parity, f.limiter);
+  fused::k_corr2d<TX, TY, RS><<<f.ntB, 256, smB, f.stream>>>(f.insts, f.tilesB, parity, f.limiter);
 }
 
 template <int RS>
 void launch_pred_corr(const FusedLaunch& f, int parity) {
-  set_smem_attrs<RS>();
-  fused::k_pred2d<FA_TX, FA_TY, RS><<<f.ntA, 256, SMEM_A, f.stream>>>(f.insts, f.tilesA, parity, f.limiter, f.err);
-  fused::k_corr2d<FUSED_TX, FUSED_TY, RS><<<f.ntB, 256, SMEM_B, f.stream>>>(f.insts, f.tilesB, parity, f.limiter,
-                                                                          f.cour, f.err);
+  // FUSED_VARIANTS in bnz_common.h; non-default variants are built for HLLD
+  if constexpr (RS == dev::RS_HLLD) {
+    switch (f.variant) {
+      case 1: launch_variant<32, 8, RS, 1>(f, parity); return;
+      case 2: launch_variant<16, 16, RS, 0>(f, parity); return;
+      case 3: launch_variant<16, 16, RS, 1>(f, parity); return;
+      case 4: launch_variant<64, 4, RS, 0>(f, parity); return;
+      default: break;
+    }
+  }
+  launch_variant<32, 8, RS, 0>(f, parity);
 }
 }  // namespace
 

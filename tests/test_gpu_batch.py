@@ -90,3 +90,54 @@ def test_batch_rejects_3d_and_conduction():
         Batch([dict(Nx=8, Ny=8, Nz=8, dims=3)], **METHOD)
     with pytest.raises(BnzError):
         Batch([dict(Nx=8, Ny=8, Nz=1, dims=2)], kappa0=0.1, **METHOD)
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+def test_every_variant_bitwise_vs_oracle(variant):
+    """Every autotuner candidate (tile shape, predictor staging) gives the same bits."""
+    from bonzo_b200._lib import Batch
+    inst = _instances([16, 33, 64, 20, 97], seed=11)
+    grids = [dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((1, 1), (1, 1), (0, 0))) for n, *_ in inst]
+    b = Batch(grids, exact_fp=True, **METHOD)
+    b.set_variant(variant)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        b[q].set_state(prim, bfld)
+        b[q].init()
+    b.advance(1e30, 3)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        o = oracle_sim(dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((1, 1), (1, 1), (0, 0))), **METHOD)
+        o.set_state(prim, bfld)
+        o.init()
+        o.advance(1e30, max_steps=3)
+        for x, y in zip(o.get_state(), b[q].get_state()):
+            assert np.array_equal(x, y), (variant, q)
+        assert b[q].check() == 0
+
+
+def test_autotune_restores_state(tmp_path, monkeypatch):
+    """Timing the variants leaves the batch exactly where it was."""
+    from bonzo_b200 import autotune
+    from bonzo_b200._lib import Batch
+    monkeypatch.setenv("BNZ_TUNE_CACHE", str(tmp_path / "tune.json"))
+    inst = _instances([24, 48, 40])
+    grids = [dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((1, 1), (1, 1), (0, 0))) for n, *_ in inst]
+    a = Batch(grids, exact_fp=True, **METHOD)
+    b = Batch(grids, exact_fp=True, **METHOD)
+    for bb in (a, b):
+        for q, (n, gc, prim, bfld) in enumerate(inst):
+            bb[q].set_state(prim, bfld)
+            bb[q].init()
+    a.advance(1e30, 2)
+    b.advance(1e30, 2)
+    best, ms = autotune.tune_batch(a, [n for n, *_ in inst], steps=2)
+    assert best in ms and all(v > 0 for v in ms.values())
+    assert (tmp_path / "tune.json").exists()
+    a.advance(1e30, 3)
+    b.advance(1e30, 3)
+    for q in range(len(inst)):
+        assert a[q].time() == b[q].time()
+        for x, y in zip(a[q].get_state(), b[q].get_state()):
+            assert np.array_equal(x, y)
+    # a second tuner call is served from the cache
+    best2, _ = autotune.tune_batch(a, [n for n, *_ in inst], steps=2)
+    assert best2 == best and a.variant == best
