@@ -1215,6 +1215,12 @@ int bnz_batch_time_variant(bnz_batch* b, int v, int steps, double* ms) {
     CKB(cudaMemcpyAsync(&dts[q], c->d_ds, sizeof(DtState), cudaMemcpyDeviceToHost, b->stream));
   }
   CKB(cudaStreamSynchronize(b->stream));
+  // the trial must really step: no tmax clip (the time records are restored below)
+  {
+    const int n = (int)b->ctx.size();
+    k_set_tmax<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_inst, n, 1e300);
+    CKB(cudaGetLastError());
+  }
   const int mode = b->md.fixdt ? FDT_FIXED : FDT_CFL;
   cudaEvent_t e0, e1;
   CKB(cudaEventCreate(&e0));
