@@ -30,7 +30,8 @@ EXPORTS = [
     "bnz_batch_create", "bnz_batch_destroy", "bnz_batch_last_error", "bnz_batch_size",
     "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_set_stream", "bnz_batch_launch_count",
     "bnz_batch_sync", "bnz_variant_count", "bnz_batch_set_variant", "bnz_batch_get_variant",
-    "bnz_batch_time_variant", "bnz_batch_autotune",
+    "bnz_batch_time_variant", "bnz_batch_autotune", "bnz_vl2_step_noalloc", "bnz_noalloc_last_error",
+    "bnz_noalloc_scratch_bytes",
 ]
 
 

@@ -1,9 +1,10 @@
 """Build libbnzgpu.so in-tree for sm_100a (B200).
 
-Three translation units:
+Translation units:
   bnz_kernels_exact.cu  --fmad=false  (bit-for-bit parity kernels)
   bnz_kernels_fast.cu   --fmad=true   (DFMA-contracted production kernels)
   bnz_ctx.cu                          (C ABI host code)
+  bnz_noalloc.cu                      (the step that allocates no device memory)
 linked with -shared into bonzo_b200/libbnzgpu.so.  nvcc cross-compiles, so
 this runs on machines without a GPU.
 """
@@ -24,6 +25,7 @@ UNITS = [
     ("bnz_kernels_exact.cu", ["--fmad=false"]),
     ("bnz_kernels_fast.cu", ["--fmad=true"]),
     ("bnz_ctx.cu", []),
+    ("bnz_noalloc.cu", []),
 ]
 
 

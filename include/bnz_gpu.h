@@ -22,6 +22,7 @@
 #ifndef BNZ_GPU_H
 #define BNZ_GPU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -174,6 +175,29 @@ int bnz_batch_set_variant(bnz_batch* batch, int variant);
 int bnz_batch_get_variant(const bnz_batch* batch, int* variant);
 int bnz_batch_time_variant(bnz_batch* batch, int variant, int steps, double* ms);
 int bnz_batch_autotune(bnz_batch* batch, int steps, int* best, double* ms_per_variant);
+
+/* ------------------------------------------------------------------------
+ * One VL2 step that allocates no device memory.  No counterpart in the
+ * reference: it exists for callers that must not let a library allocate --
+ * programs whose device memory belongs to a framework allocator that reserved
+ * it up front, or time loops that cannot take the device-wide synchronisation
+ * of a cudaMalloc / cudaFree.  The caller passes device pointers to full
+ * (ghosts included) prim / bfld arrays: the input state and the output state
+ * (different buffers).  The step (predictor + corrector + ghost fill of the
+ * outputs, no conduction) keeps its scratch in one fixed 4 MiB device array
+ * that every GPU loading the library holds until exit, which bounds the grid
+ * to 2D with (Nx+6)*(Ny+6) up to about 40000 cells (e.g. 192 x 192, PLM);
+ * larger grids are rejected with BNZ_ERR_ARG.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress); make that first
+ * call before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race and corrupt each other.  Work is queued on `stream`
+ * (cudaStream_t as void*, NULL for the legacy stream).  The message of the
+ * last failure on this host thread is bnz_noalloc_last_error(). */
+int bnz_vl2_step_noalloc(const bnz_grid_desc* grid, const bnz_method_desc* method, const double* prim_in,
+                         const double* bfld_in, double* prim_out, double* bfld_out, double dt, void* stream);
+const char* bnz_noalloc_last_error(void);
+/* Size in bytes of the fixed scratch array. */
+size_t bnz_noalloc_scratch_bytes(void);
 
 #ifdef __cplusplus
 }

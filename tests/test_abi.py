@@ -16,7 +16,7 @@ def header_functions():
     for h in os.listdir(os.path.join(ROOT, "include")):
         if h.endswith(".h"):
             txt = open(os.path.join(ROOT, "include", h)).read()
-            names += re.findall(r"^\s*(?:int|const char\*|void)\s+(bnz_\w+)\s*\(", txt, re.M)
+            names += re.findall(r"^\s*(?:int|const char\*|void|size_t)\s+(bnz_\w+)\s*\(", txt, re.M)
     return sorted(set(names))
 
 
