@@ -33,12 +33,21 @@ sys.path.insert(0, ROOT)
 METRIC = "Mzone-updates/s, 1 B200: batched FP64 VL2+HLLD+CT vs plain; adjoint/fwd ratio"
 UNIT = "Mzone-updates/s"
 BYTES_PER_ZONE = 192  # 9 conserved + 3 face-B doubles read once and written once
+# Corrector launch (the dominant kernel): reads w^n (9 doubles, u^n is rebuilt
+# from it), b^n (3), w^(n+1/2) (9) and b^(n+1/2) (3); writes w^(n+1) (9) and
+# b^(n+1) (3): 36 doubles per active zone.  The predictor reads 12 and writes
+# 12 per zone it covers (active zones plus two ghost rings).
+CORR_BYTES_PER_ZONE = 288
+# DRAM bytes per active zone of one corrector launch (dram__bytes_read.sum +
+# dram__bytes_write.sum), from the ncu capture summarised in
+# profiles/k_corr2d_blast_batch.md (16-instance capture, scaled per zone).
+CORR_TRAFFIC_PER_ZONE = 267.7
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--path", default="batch", choices=["batch", "plain", "fused"])
@@ -70,7 +79,7 @@ METHOD = dict(dims=2, bc=((1, 1), (1, 1), (1, 1)), gam=5. / 3, cour=0.4, rsolver
 # ---------------------------------------------------------------------------
 
 class ClockSampler:
-    """Samples SM clock and clock-event reasons every 200 ms (NVML)."""
+    """Samples SM clock and clock-event reasons every 50 ms (NVML)."""
 
     REASONS = {
         "hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
@@ -108,7 +117,7 @@ class ClockSampler:
                         self.reasons.add(name)
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(0.05)
 
     def __enter__(self):
         if self.nv is not None:
@@ -298,13 +307,32 @@ def run_ours(args, rank, world, dist):
 
     from bonzo_b200.peaks import hbm_peak
     peak, peak_src = hbm_peak()
-    achieved = BYTES_PER_ZONE * zones / (ms_step * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None,
-                "peak_source": peak_src,
-                "kernel": "whole step (%s path, %d launches per step over %d instances)" %
-                          (args.path, launches // max(1, args.steps), len(ctxs)),
-                "bytes_per_zone": BYTES_PER_ZONE}
+    step_achieved = BYTES_PER_ZONE * zones / (ms_step * 1e-3) / 1e9
+    step_roof = {"achieved": round(step_achieved, 1), "frac": round(step_achieved / peak, 4),
+                 "bytes_per_zone": BYTES_PER_ZONE,
+                 "what": "whole step (%s path, %d launches per step over %d instances)" %
+                         (args.path, launches // max(1, args.steps), len(ctxs))}
+    if args.path == "batch":
+        # the dominant kernel, timed live: the same batch steps launched one by
+        # one with CUDA events on the batch stream around every launch
+        if dist:
+            dist.barrier()
+        kms = eng.advance_timed(1e30, args.steps)
+        for c in ctxs:
+            c.check()
+        achieved = CORR_BYTES_PER_ZONE * zones / (kms["corrector"] * 1e-3) / 1e9
+        traffic = None if CORR_TRAFFIC_PER_ZONE is None else int(CORR_TRAFFIC_PER_ZONE * zones)
+        roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                    "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_src,
+                    "kernel": "k_corr2d (corrector, one launch covers every instance)",
+                    "algorithmic_bytes_per_launch": CORR_BYTES_PER_ZONE * zones,
+                    "ms_per_launch": round(kms["corrector"], 4),
+                    "kernel_ms_per_launch": {k: round(v, 4) for k, v in kms.items()},
+                    "step": step_roof}
+    else:
+        roofline = {"bound": "hbm", "achieved": step_roof["achieved"], "peak": peak, "unit": "GB/s",
+                    "frac": step_roof["frac"], "traffic": None, "peak_source": peak_src,
+                    "kernel": step_roof["what"], "bytes_per_zone": BYTES_PER_ZONE}
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),

@@ -28,7 +28,7 @@ EXPORTS = [
     "bnz_get_time", "bnz_set_time", "bnz_check", "bnz_sync", "bnz_advance_graph",
     "bnz_device_state", "bnz_stream", "bnz_set_stream", "bnz_launch_count",
     "bnz_batch_create", "bnz_batch_destroy", "bnz_batch_last_error", "bnz_batch_size",
-    "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_set_stream", "bnz_batch_launch_count",
+    "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_advance_timed", "bnz_batch_set_stream", "bnz_batch_launch_count",
     "bnz_batch_sync", "bnz_variant_count", "bnz_batch_set_variant", "bnz_batch_get_variant",
     "bnz_batch_time_variant", "bnz_batch_autotune", "bnz_vl2_step_noalloc", "bnz_noalloc_last_error",
     "bnz_noalloc_scratch_bytes",
@@ -98,6 +98,7 @@ def load():
     L.bnz_batch_size.argtypes = [vp, C.POINTER(C.c_int)]
     L.bnz_batch_instance.argtypes = [vp, C.c_int, C.POINTER(vp)]
     L.bnz_batch_advance.argtypes = [vp, C.c_double, C.c_int]
+    L.bnz_batch_advance_timed.argtypes = [vp, C.c_double, C.c_int, _dp]
     L.bnz_batch_set_stream.argtypes = [vp, vp]
     L.bnz_batch_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.bnz_batch_sync.argtypes = [vp]
@@ -313,6 +314,13 @@ class Batch:
 
     def advance(self, tmax, nsteps):
         self._ck(self.L.bnz_batch_advance(self.h, tmax, nsteps))
+
+    def advance_timed(self, tmax, nsteps):
+        """advance() launched one by one with events around every launch:
+        returns the mean ms per launch of the dt, predictor and corrector kernels."""
+        ms = (C.c_double * 3)()
+        self._ck(self.L.bnz_batch_advance_timed(self.h, tmax, int(nsteps), ms))
+        return {"dt": ms[0], "predictor": ms[1], "corrector": ms[2]}
 
     def set_stream(self, stream):
         self._ck(self.L.bnz_batch_set_stream(self.h, C.c_void_p(stream)))

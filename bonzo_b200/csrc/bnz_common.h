@@ -108,6 +108,9 @@ struct FusedLaunch {
   double dt_fixed;
   unsigned* err;
   cudaStream_t stream;
+  // optional: events recorded before k_dt_batch, before the predictor, before
+  // the corrector and after it (kernel timing; null in normal stepping)
+  cudaEvent_t* events;
 };
 
 // Conduction scratch (thcond_elec.pyx DiffScratch).

@@ -1092,11 +1092,13 @@ int bnz_batch_set_stream(bnz_batch* b, void* stream) {
   return BNZ_OK;
 }
 
-int bnz_batch_advance(bnz_batch* b, double tmax, int nsteps) {
-  if (!b || b->ctx.empty()) return BNZ_ERR_ARG;
-  if (nsteps < 0) return bfail(b, BNZ_ERR_ARG, "nsteps must be >= 0");
-  if (nsteps == 0) return BNZ_OK;
-  // every instance must be at the batch parity with its time record on the device
+}  // extern "C"
+
+namespace {
+
+// Common start of a batch advance: every instance must be at the batch parity
+// with its time record on the device; then the stop time is set.
+int batch_prologue(bnz_batch* b, double tmax) {
   for (bnz_ctx* c : b->ctx) {
     if (c->parity != b->parity) return bfail(b, BNZ_ERR_STATE, "instance stepped outside the batch");
     if (!c->time_on_device) {
@@ -1112,6 +1114,27 @@ int bnz_batch_advance(bnz_batch* b, double tmax, int nsteps) {
   const int n = (int)b->ctx.size();
   k_set_tmax<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_inst, n, tmax);
   b->launches += 1;
+  return BNZ_OK;
+}
+
+void batch_epilogue(bnz_batch* b) {
+  for (bnz_ctx* c : b->ctx) {
+    set_parity(c, b->parity);
+    c->ghosts_stale = true;
+    c->time_on_device = true;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int bnz_batch_advance(bnz_batch* b, double tmax, int nsteps) {
+  if (!b || b->ctx.empty()) return BNZ_ERR_ARG;
+  if (nsteps < 0) return bfail(b, BNZ_ERR_ARG, "nsteps must be >= 0");
+  if (nsteps == 0) return BNZ_OK;
+  int rc = batch_prologue(b, tmax);
+  if (rc) return rc;
   const int mode = b->md.fixdt ? FDT_FIXED : FDT_CFL;
   auto one_step = [&](int p) {
     FusedLaunch f = batch_launch(b, mode);
@@ -1148,11 +1171,39 @@ int bnz_batch_advance(bnz_batch* b, double tmax, int nsteps) {
     b->parity ^= 1;
   }
   CKB(cudaGetLastError());
-  for (bnz_ctx* c : b->ctx) {
-    set_parity(c, b->parity);
-    c->ghosts_stale = true;
-    c->time_on_device = true;
+  batch_epilogue(b);
+  return BNZ_OK;
+}
+
+int bnz_batch_advance_timed(bnz_batch* b, double tmax, int nsteps, double* ms_kernels) {
+  if (!b || b->ctx.empty() || !ms_kernels) return BNZ_ERR_ARG;
+  if (nsteps < 1) return bfail(b, BNZ_ERR_ARG, "nsteps must be >= 1");
+  int rc = batch_prologue(b, tmax);
+  if (rc) return rc;
+  const int mode = b->md.fixdt ? FDT_FIXED : FDT_CFL;
+  // one event set per step, so every launch of the run is timed
+  std::vector<cudaEvent_t> ev(4 * (size_t)nsteps, nullptr);
+  for (auto& e : ev) CKB(cudaEventCreate(&e));
+  for (int s = 0; s < nsteps; ++s) {
+    FusedLaunch f = batch_launch(b, mode);
+    f.events = &ev[4 * (size_t)s];
+    b->launches += b->L->fused_step(f, b->parity);
+    b->launches += b->L->fused_time(f);
+    b->parity ^= 1;
   }
+  CKB(cudaGetLastError());
+  cudaError_t e = cudaEventSynchronize(ev.back());
+  double sum[3] = {0., 0., 0.};
+  for (int s = 0; s < nsteps && e == cudaSuccess; ++s)
+    for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
+      float t = 0.f;
+      e = cudaEventElapsedTime(&t, ev[4 * (size_t)s + k], ev[4 * (size_t)s + k + 1]);
+      sum[k] += t;
+    }
+  for (auto& x : ev) cudaEventDestroy(x);
+  if (e != cudaSuccess) return bfail(b, BNZ_ERR_CUDA, std::string("kernel timing: ") + cudaGetErrorString(e));
+  for (int k = 0; k < 3; ++k) ms_kernels[k] = sum[k] / nsteps;
+  batch_epilogue(b);
   return BNZ_OK;
 }
 

@@ -286,8 +286,11 @@ void launch_variant(const FusedLaunch& f, int parity) {
     cudaFuncSetAttribute(fused::k_corr2d<TX, TY, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB);
     attrs = true;
   }
+  if (f.events) cudaEventRecord(f.events[1], f.stream);
   fused::k_pred2d<TXA, TYA, RS, STAGED><<<f.ntA, 256, smA, f.stream>>>(f.insts, f.tilesA, parity, f.limiter);
+  if (f.events) cudaEventRecord(f.events[2], f.stream);
   fused::k_corr2d<TX, TY, RS><<<f.ntB, 256, smB, f.stream>>>(f.insts, f.tilesB, parity, f.limiter);
+  if (f.events) cudaEventRecord(f.events[3], f.stream);
 }
 
 template <int RS>
@@ -307,6 +310,7 @@ void launch_pred_corr(const FusedLaunch& f, int parity) {
 }  // namespace
 
 int fused_step(const FusedLaunch& f, int parity) {
+  if (f.events) cudaEventRecord(f.events[0], f.stream);
   fused::k_dt_batch<<<(f.ninst + 127) / 128, 128, 0, f.stream>>>(f.insts, f.ninst, parity, f.cour, f.dt_mode,
                                                                   f.dt_fixed);
   switch (f.rsolver) {

@@ -161,6 +161,10 @@ int bnz_batch_size(const bnz_batch* batch, int* n);
 int bnz_batch_instance(bnz_batch* batch, int i, bnz_ctx** ctx);
 /* nsteps VL2 steps of every instance, each with its own CFL dt clipped to tmax. */
 int bnz_batch_advance(bnz_batch* batch, double tmax, int nsteps);
+/* The same steps launched one by one (no graph) with events around every
+ * launch; ms_kernels[3] receives the mean duration in ms of the per-instance
+ * dt launch, the predictor launch and the corrector launch.  For measurement. */
+int bnz_batch_advance_timed(bnz_batch* batch, double tmax, int nsteps, double* ms_kernels);
 int bnz_batch_set_stream(bnz_batch* batch, void* stream);
 int bnz_batch_launch_count(const bnz_batch* batch, long long* n);
 int bnz_batch_sync(bnz_batch* batch);
