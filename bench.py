@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
     return ap.parse_args()
 
 
@@ -362,6 +363,55 @@ def run_ours(args, rank, world, dist):
     return line
 
 
+def run_adjoint(warmup=1, reps=3):
+    """adjoint/forward cost of a differentiable rollout: 256^2 periodic vortex
+    with a seeded smooth perturbation (Fourier modes |k| <= 4, amplitude 1e-2 on
+    v and Az), VL2 + PLM(mc) + HLLD + CT, 100 steps of fixed dt = 1e-4, loss =
+    squared misfit of the final density, checkpoint every 10 steps.  Forward =
+    the autograd Function's forward (state in, 100 recorded steps, state out);
+    adjoint = its backward (segment recompute + reverse steps)."""
+    import torch
+    from bonzo_b200 import problems as P
+    from bonzo_b200._lib import Context
+    from bonzo_b200.adjoint import rollout
+    n, nsteps, dt, every = 256, 100, 1e-4, 10
+    gc = P.make_grid(n, n, 1, dims=2, bc=0)
+    prim, bfld = P.otvortex(gc, pert_amp=1e-2, seed=0)
+    eng = Context(Nx=n, Ny=n, Nz=1, dims=2, bc=((0, 0), (0, 0), (0, 0)), gam=5. / 3, cour=0.4,
+                  rsolver="hlld", limiter="mc", path="fused")
+    eng.set_state(prim, bfld)
+    eng.init()
+    P0, _, B0 = eng.get_state()
+    p0 = torch.from_numpy(P0).cuda()
+    b0 = torch.from_numpy(B0).cuda()
+    target = p0[0].clone() * 1.01
+    stream = torch.cuda.current_stream()
+    fwd, adj = [], []
+    for it in range(warmup + reps):
+        p = p0.clone().requires_grad_(True)
+        b = b0.clone().requires_grad_(True)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        e0.record(stream)
+        xp, xb = rollout(p, b, eng, nsteps, dt, checkpoint_every=every)
+        e1.record(stream)
+        loss = ((xp[0] - target) ** 2).sum()
+        g = torch.autograd.grad(loss, (p, b), retain_graph=False)
+        e2.record(stream)
+        torch.cuda.synchronize()
+        if it >= warmup:
+            fwd.append(e0.elapsed_time(e1))
+            adj.append(e1.elapsed_time(e2))
+        del g
+    f, a = statistics.median(fwd), statistics.median(adj)
+    return {"workload": "256^2 periodic vortex + smooth perturbation, VL2+PLM(mc)+HLLD+CT, 100 steps of "
+                        "dt=1e-4, checkpoint every 10 steps, loss = density misfit",
+            "fwd_ms": round(f, 3), "adj_ms": round(a, 3), "ratio": round(a / f, 3),
+            "fwd_mzone_updates_per_s": round(n * n * nsteps / (f * 1e-3) / 1e6, 1),
+            "how": "CUDA events on the current stream around the autograd Function's forward and around "
+                   "backward (incl. the loss); median of %d after %d warm-up" % (reps, warmup)}
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -393,6 +443,8 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = tdist
     line = run_ours(args, rank, world, dist)
+    if rank == 0 and not args.no_adjoint:
+        line["adjoint"] = run_adjoint()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         batch = build_batch(args.instances, args.seed)
         cb = run_cpu_reference(batch, steps=2, warmup=1)

@@ -31,7 +31,8 @@ EXPORTS = [
     "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_advance_timed", "bnz_batch_set_stream", "bnz_batch_launch_count",
     "bnz_batch_sync", "bnz_variant_count", "bnz_batch_set_variant", "bnz_batch_get_variant",
     "bnz_batch_time_variant", "bnz_batch_autotune", "bnz_vl2_step_noalloc", "bnz_noalloc_last_error",
-    "bnz_noalloc_scratch_bytes",
+    "bnz_noalloc_scratch_bytes", "bnz_set_state_device", "bnz_get_state_device", "bnz_rollout_forward",
+    "bnz_rollout_adjoint", "bnz_step_adjoint",
 ]
 
 
@@ -99,6 +100,11 @@ def load():
     L.bnz_batch_instance.argtypes = [vp, C.c_int, C.POINTER(vp)]
     L.bnz_batch_advance.argtypes = [vp, C.c_double, C.c_int]
     L.bnz_batch_advance_timed.argtypes = [vp, C.c_double, C.c_int, _dp]
+    L.bnz_set_state_device.argtypes = [vp, vp, vp]
+    L.bnz_get_state_device.argtypes = [vp, vp, vp]
+    L.bnz_rollout_forward.argtypes = [vp, C.c_int, C.c_double, C.c_int]
+    L.bnz_rollout_adjoint.argtypes = [vp, vp, vp, vp, vp]
+    L.bnz_step_adjoint.argtypes = [vp, C.c_double, vp, vp, vp, vp, vp, vp]
     L.bnz_batch_set_stream.argtypes = [vp, vp]
     L.bnz_batch_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.bnz_batch_sync.argtypes = [vp]
@@ -261,6 +267,25 @@ class Context:
         p, u, b = _dp(), _dp(), _dp()
         self._ck(self.L.bnz_device_state(self.h, C.byref(p), C.byref(u), C.byref(b)))
         return (C.cast(p, C.c_void_p).value, C.cast(u, C.c_void_p).value, C.cast(b, C.c_void_p).value)
+
+    # --- device-pointer state and the adjoint (pointers are ints) ---------
+    def set_state_device(self, prim_ptr, bfld_ptr):
+        self._ck(self.L.bnz_set_state_device(self.h, C.c_void_p(prim_ptr), C.c_void_p(bfld_ptr)))
+
+    def get_state_device(self, prim_ptr, bfld_ptr):
+        self._ck(self.L.bnz_get_state_device(self.h, C.c_void_p(prim_ptr), C.c_void_p(bfld_ptr)))
+
+    def rollout_forward(self, nsteps, dt, checkpoint_every=10):
+        self._ck(self.L.bnz_rollout_forward(self.h, int(nsteps), float(dt), int(checkpoint_every)))
+
+    def rollout_adjoint(self, gprim_ptr, gbfld_ptr, gprim0_ptr, gbfld0_ptr):
+        self._ck(self.L.bnz_rollout_adjoint(self.h, C.c_void_p(gprim_ptr), C.c_void_p(gbfld_ptr),
+                                            C.c_void_p(gprim0_ptr), C.c_void_p(gbfld0_ptr)))
+
+    def step_adjoint(self, dt, prim_ptr, bfld_ptr, gprim1_ptr, gbfld1_ptr, gprim0_ptr, gbfld0_ptr):
+        self._ck(self.L.bnz_step_adjoint(self.h, float(dt), C.c_void_p(prim_ptr), C.c_void_p(bfld_ptr),
+                                         C.c_void_p(gprim1_ptr), C.c_void_p(gbfld1_ptr),
+                                         C.c_void_p(gprim0_ptr), C.c_void_p(gbfld0_ptr)))
 
     def set_stream(self, stream):
         """Order this context's work on a caller-owned CUDA stream (handle as int)."""

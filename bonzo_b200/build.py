@@ -5,6 +5,7 @@ Translation units:
   bnz_kernels_fast.cu   --fmad=true   (DFMA-contracted production kernels)
   bnz_ctx.cu                          (C ABI host code)
   bnz_noalloc.cu                      (the step that allocates no device memory)
+  bnz_adjoint.cu                      (adjoint rollouts: tape and reverse pass)
 linked with -shared into bonzo_b200/libbnzgpu.so.  nvcc cross-compiles, so
 this runs on machines without a GPU.
 """
@@ -26,6 +27,7 @@ UNITS = [
     ("bnz_kernels_fast.cu", ["--fmad=true"]),
     ("bnz_ctx.cu", []),
     ("bnz_noalloc.cu", []),
+    ("bnz_adjoint.cu", []),
 ]
 
 

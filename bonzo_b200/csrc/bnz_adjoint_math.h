@@ -1,0 +1,729 @@
+// bnz_adjoint_math.h -- pointwise vector-Jacobian products (reverse mode) of
+// the per-point math of the VL2 step: EOS conversions, the ideal-MHD flux,
+// the fast magnetosonic speed, the HLL and HLLD Riemann solvers and the PLM
+// slope limiters.  Hand-derived from the forward expressions in
+// bnz_device.cuh (which restate src/mhd/eos_c.h, src/mhd/fluxes_c.c and
+// src/coordinates/reconstr_c.h); the reference has no adjoint.
+//
+// Every function takes the forward inputs, recomputes what it needs and adds
+// (+=) the input cotangents; the branch taken at a kink (limiter cases, the
+// Riemann fan region, min/max of wave speeds, |x|) is the one the forward
+// takes for the same inputs.  Variables are in the sweep's local frame with
+// the layout of dev::NM (RHO, VX, VY, VZ, PR, PSC, BX, BY, BZ); the normal
+// field is w[BX] on both sides and its cotangent is returned separately.
+//
+// The header compiles as CUDA device code (included inside the kernels'
+// namespace) and as plain C++ for host-side tests.
+#pragma once
+
+#ifdef __CUDACC__
+#define BNZ_HD __host__ __device__ __forceinline__
+#else
+#include <cmath>
+#define BNZ_HD inline
+#endif
+
+namespace adj {
+
+enum { RHO = 0, VX = 1, VY = 2, VZ = 3, PR = 4, PSC = 5, BX = 6, BY = 7, BZ = 8 };
+enum { MX = 1, MY = 2, MZ = 3, EN = 4 };
+constexpr int NM = 9;
+
+BNZ_HD double sq(double x) { return x * x; }
+BNZ_HD double sgn(double a) { return (double)((0.0 < a) - (a < 0.0)); }
+
+// w = cons2prim(u): given wbar, add ubar.  Expressed through w (the forward's
+// output), which holds rho, v and B.
+BNZ_HD void vjp_cons2prim(const double* w, const double* wb, double gam, double* ub) {
+  const double g1 = gam - 1.;
+  const double rhoi = 1. / w[RHO];
+  const double pb = wb[PR];
+  const double v2 = sq(w[VX]) + sq(w[VY]) + sq(w[VZ]);
+  ub[EN] += g1 * pb;
+  ub[RHO] += wb[RHO] - (wb[VX] * w[VX] + wb[VY] * w[VY] + wb[VZ] * w[VZ]) * rhoi + 0.5 * g1 * v2 * pb;
+  ub[MX] += wb[VX] * rhoi - g1 * w[VX] * pb;
+  ub[MY] += wb[VY] * rhoi - g1 * w[VY] * pb;
+  ub[MZ] += wb[VZ] * rhoi - g1 * w[VZ] * pb;
+  ub[PSC] += wb[PSC];
+  ub[BX] += wb[BX] - g1 * w[BX] * pb;
+  ub[BY] += wb[BY] - g1 * w[BY] * pb;
+  ub[BZ] += wb[BZ] - g1 * w[BZ] * pb;
+}
+
+// u = prim2cons(w): given ubar, add wbar.
+BNZ_HD void vjp_prim2cons(const double* w, const double* ub, double gam, double* wb) {
+  const double gamm1i = 1. / (gam - 1.);
+  const double eb = ub[EN];
+  const double v2 = sq(w[VX]) + sq(w[VY]) + sq(w[VZ]);
+  wb[RHO] += ub[RHO] + ub[MX] * w[VX] + ub[MY] * w[VY] + ub[MZ] * w[VZ] + 0.5 * v2 * eb;
+  wb[VX] += ub[MX] * w[RHO] + eb * w[RHO] * w[VX];
+  wb[VY] += ub[MY] * w[RHO] + eb * w[RHO] * w[VY];
+  wb[VZ] += ub[MZ] * w[RHO] + eb * w[RHO] * w[VZ];
+  wb[PR] += eb * gamm1i;
+  wb[PSC] += ub[PSC];
+  wb[BX] += ub[BX] + eb * w[BX];
+  wb[BY] += ub[BY] + eb * w[BY];
+  wb[BZ] += ub[BZ] + eb * w[BZ];
+}
+
+// f = flux(w) of ideal MHD along x (primcons2flux of prim2cons(w); f[BX] = 0):
+// given fbar (entry BX ignored), add wbar; the w[BX] part goes to wb[BX].
+BNZ_HD void vjp_flux(const double* w, const double* fb, double gam, double* wb) {
+  const double r = w[RHO], vx = w[VX], vy = w[VY], vz = w[VZ], p = w[PR];
+  const double bx = w[BX], by = w[BY], bz = w[BZ];
+  const double b2 = sq(bx) + sq(by) + sq(bz);
+  const double v2 = sq(vx) + sq(vy) + sq(vz);
+  const double pt = p + 0.5 * b2;
+  const double en = 0.5 * (r * v2 + b2) + p / (gam - 1.);
+  const double dot = vx * bx + vy * by + vz * bz;
+  double rb = 0., vxb = 0., vyb = 0., vzb = 0., pb = 0., bxb = 0., byb = 0., bzb = 0.;
+  double ptb = 0., enb = 0.;
+  // f[RHO] = r vx
+  rb += fb[RHO] * vx;
+  vxb += fb[RHO] * r;
+  // f[MX] = r vx vx + pt - bx^2
+  rb += fb[MX] * vx * vx;
+  vxb += 2. * fb[MX] * r * vx;
+  ptb += fb[MX];
+  bxb -= 2. * fb[MX] * bx;
+  // f[MY] = r vx vy - bx by
+  rb += fb[MY] * vx * vy;
+  vxb += fb[MY] * r * vy;
+  vyb += fb[MY] * r * vx;
+  bxb -= fb[MY] * by;
+  byb -= fb[MY] * bx;
+  // f[MZ] = r vx vz - bx bz
+  rb += fb[MZ] * vx * vz;
+  vxb += fb[MZ] * r * vz;
+  vzb += fb[MZ] * r * vx;
+  bxb -= fb[MZ] * bz;
+  bzb -= fb[MZ] * bx;
+  // f[EN] = (en + pt) vx - bx dot
+  enb += fb[EN] * vx;
+  ptb += fb[EN] * vx;
+  vxb += fb[EN] * (en + pt);
+  bxb -= fb[EN] * dot;
+  {
+    const double dotb = -fb[EN] * bx;
+    vxb += dotb * bx;
+    bxb += dotb * vx;
+    vyb += dotb * by;
+    byb += dotb * vy;
+    vzb += dotb * bz;
+    bzb += dotb * vz;
+  }
+  // f[PSC] = psc vx
+  wb[PSC] += fb[PSC] * vx;
+  vxb += fb[PSC] * w[PSC];
+  // f[BY] = vx by - vy bx ; f[BZ] = vx bz - vz bx
+  vxb += fb[BY] * by + fb[BZ] * bz;
+  byb += fb[BY] * vx;
+  vyb -= fb[BY] * bx;
+  bxb -= fb[BY] * vy + fb[BZ] * vz;
+  bzb += fb[BZ] * vx;
+  vzb -= fb[BZ] * bx;
+  // en = 0.5 (r v2 + b2) + p / (gam - 1)
+  rb += enb * 0.5 * v2;
+  vxb += enb * r * vx;
+  vyb += enb * r * vy;
+  vzb += enb * r * vz;
+  bxb += enb * bx;
+  byb += enb * by;
+  bzb += enb * bz;
+  pb += enb / (gam - 1.);
+  // pt = p + 0.5 b2
+  pb += ptb;
+  bxb += ptb * bx;
+  byb += ptb * by;
+  bzb += ptb * bz;
+  wb[RHO] += rb;
+  wb[VX] += vxb;
+  wb[VY] += vyb;
+  wb[VZ] += vzb;
+  wb[PR] += pb;
+  wb[BX] += bxb;
+  wb[BY] += byb;
+  wb[BZ] += bzb;
+}
+
+// conserved vector u = prim2cons(w): value (for the Riemann VJPs)
+BNZ_HD void cons_of(const double* w, double gam, double* u) {
+  u[RHO] = w[RHO];
+  u[MX] = w[RHO] * w[VX];
+  u[MY] = w[RHO] * w[VY];
+  u[MZ] = w[RHO] * w[VZ];
+  u[EN] = 0.5 * (w[RHO] * (sq(w[VX]) + sq(w[VY]) + sq(w[VZ])) + sq(w[BX]) + sq(w[BY]) + sq(w[BZ])) +
+          w[PR] / (gam - 1.);
+  u[PSC] = w[PSC];
+  u[BX] = w[BX];
+  u[BY] = w[BY];
+  u[BZ] = w[BZ];
+}
+
+BNZ_HD void flux_of(const double* w, double gam, double* f) {
+  const double b2 = sq(w[BX]) + sq(w[BY]) + sq(w[BZ]);
+  const double pt = w[PR] + 0.5 * b2;
+  const double en = 0.5 * (w[RHO] * (sq(w[VX]) + sq(w[VY]) + sq(w[VZ])) + b2) + w[PR] / (gam - 1.);
+  const double dot = w[VX] * w[BX] + w[VY] * w[BY] + w[VZ] * w[BZ];
+  f[RHO] = w[RHO] * w[VX];
+  f[MX] = w[RHO] * w[VX] * w[VX] + pt - sq(w[BX]);
+  f[MY] = w[RHO] * w[VX] * w[VY] - w[BX] * w[BY];
+  f[MZ] = w[RHO] * w[VX] * w[VZ] - w[BX] * w[BZ];
+  f[EN] = (en + pt) * w[VX] - w[BX] * dot;
+  f[PSC] = w[PSC] * w[VX];
+  f[BX] = 0.;
+  f[BY] = w[VX] * w[BY] - w[VY] * w[BX];
+  f[BZ] = w[VX] * w[BZ] - w[VZ] * w[BX];
+}
+
+// cf = fms(w) (eos_c.h:468-530; the normal field is w[BX]): value and VJP.
+BNZ_HD double fms_val(const double* w, double gam) {
+  const double bx2 = sq(w[BX]);
+  const double b2 = bx2 + sq(w[BY]) + sq(w[BZ]);
+  const double gamp = gam * w[PR];
+  const double c1 = gamp + b2;
+  const double c2 = sqrt(fabs(c1 * c1 - 4. * gamp * bx2));
+  return sqrt(0.5 / w[RHO] * (c1 + c2));
+}
+
+BNZ_HD void vjp_fms(const double* w, double cfb, double gam, double* wb) {
+  const double bx2 = sq(w[BX]);
+  const double b2 = bx2 + sq(w[BY]) + sq(w[BZ]);
+  const double gamp = gam * w[PR];
+  const double c1 = gamp + b2;
+  const double disc = c1 * c1 - 4. * gamp * bx2;
+  const double c2 = sqrt(fabs(disc));
+  const double cf = sqrt(0.5 / w[RHO] * (c1 + c2));
+  if (!(cf > 0.)) return;
+  const double qb = cfb * 0.5 / cf;  // q = 0.5 / rho (c1 + c2)
+  wb[RHO] += -qb * 0.5 / (w[RHO] * w[RHO]) * (c1 + c2);
+  double c1b = qb * 0.5 / w[RHO];
+  const double c2b = qb * 0.5 / w[RHO];
+  double gampb = 0., bx2b = 0., b2b = 0.;
+  if (c2 > 0.) {
+    const double discb = c2b * 0.5 / c2 * sgn(disc);
+    c1b += 2. * c1 * discb;
+    gampb -= 4. * bx2 * discb;
+    bx2b -= 4. * gamp * discb;
+  }
+  gampb += c1b;
+  b2b += c1b;
+  wb[PR] += gam * gampb;
+  bx2b += b2b;
+  wb[BY] += 2. * w[BY] * b2b;
+  wb[BZ] += 2. * w[BZ] * b2b;
+  wb[BX] += 2. * w[BX] * bx2b;
+}
+
+// sL = min(vxL, vxR) - max(cfL, cfR), sR = max(vxL, vxR) + max(cfL, cfR)
+// (fluxes_c.c:25-42): VJP given sLb, sRb.
+BNZ_HD void vjp_wave_speeds(const double* wL, const double* wR, double gam, double sLb, double sRb, double* wLb,
+                            double* wRb) {
+  const double cfL = fms_val(wL, gam), cfR = fms_val(wR, gam);
+  const double cfmb = -sLb + sRb;
+  // fmax / fmin pick the first argument on ties
+  if (cfL >= cfR) vjp_fms(wL, cfmb, gam, wLb);
+  else vjp_fms(wR, cfmb, gam, wRb);
+  if (wL[VX] <= wR[VX]) wLb[VX] += sLb;
+  else wRb[VX] += sLb;
+  if (wL[VX] >= wR[VX]) wLb[VX] += sRb;
+  else wRb[VX] += sRb;
+}
+
+// HLL flux (fluxes_c.c:175-223): given fb, add wLb, wRb (normal field into
+// the BX entries of both; the caller sums them).
+BNZ_HD void vjp_hll(const double* wL, const double* wR, double gam, const double* fb, double* wLb, double* wRb) {
+  double uL[NM], uR[NM], fL[NM], fR[NM];
+  cons_of(wL, gam, uL);
+  cons_of(wR, gam, uR);
+  flux_of(wL, gam, fL);
+  flux_of(wR, gam, fR);
+  const double cfL = fms_val(wL, gam), cfR = fms_val(wR, gam);
+  const double cfm = cfL > cfR ? cfL : cfR;
+  const double sL = (wL[VX] < wR[VX] ? wL[VX] : wR[VX]) - cfm;
+  const double sR = (wL[VX] > wR[VX] ? wL[VX] : wR[VX]) + cfm;
+  const double aL = sL < 0. ? sL : 0.;
+  const double aR = sR > 0. ? sR : 0.;
+  const double inv = 1. / (aR - aL);
+  double fLb[NM], fRb[NM], uLb[NM], uRb[NM];
+  double aLb = 0., aRb = 0., invb = 0.;
+  for (int n = 0; n < NM; ++n) {
+    const double fbn = n == BX ? 0. : fb[n];
+    const double g = aR * fL[n] - aL * fR[n] + aL * aR * (uR[n] - uL[n]);
+    const double gb = fbn * inv;
+    invb += fbn * g;
+    fLb[n] = gb * aR;
+    fRb[n] = -gb * aL;
+    uRb[n] = gb * aL * aR;
+    uLb[n] = -gb * aL * aR;
+    aRb += gb * fL[n] + gb * aL * (uR[n] - uL[n]);
+    aLb += -gb * fR[n] + gb * aR * (uR[n] - uL[n]);
+  }
+  const double db = -invb * inv * inv;
+  aRb += db;
+  aLb -= db;
+  const double sLb = sL < 0. ? aLb : 0.;
+  const double sRb = sR > 0. ? aRb : 0.;
+  vjp_flux(wL, fLb, gam, wLb);
+  vjp_flux(wR, fRb, gam, wRb);
+  vjp_prim2cons(wL, uLb, gam, wLb);
+  vjp_prim2cons(wR, uRb, gam, wRb);
+  vjp_wave_speeds(wL, wR, gam, sLb, sRb, wLb, wRb);
+}
+
+// HLLD flux (fluxes_c.c:616-834, as restated in bnz_device.cuh flux_hlld):
+// given fb, add wLb, wRb (the normal field's cotangent is split over the BX
+// entries of both sides; the caller sums them).  The fan region is the one
+// the forward selects for these states.
+BNZ_HD void vjp_hlld(const double* wL, const double* wR, double gam, const double* fb, double* wLb, double* wRb) {
+  // ---- forward (values kept for the reverse sweep) ----
+  const double bx = wL[BX];
+  const double bx2 = sq(bx);
+  const double rL = wL[RHO], rR = wR[RHO];
+  const double vxL = wL[VX], vxR = wR[VX];
+  const double b2L = bx2 + sq(wL[BY]) + sq(wL[BZ]);
+  const double b2R = bx2 + sq(wR[BY]) + sq(wR[BZ]);
+  const double ptL = wL[PR] + 0.5 * b2L, ptR = wR[PR] + 0.5 * b2R;
+  const double mxL = rL * vxL, mxR = rR * vxR;
+  const double fmxL = mxL * vxL + ptL - bx2, fmxR = mxR * vxR + ptR - bx2;
+  const double cfL = fms_val(wL, gam), cfR = fms_val(wR, gam);
+  const double cfm = cfL > cfR ? cfL : cfR;
+  const double sL = (vxL < vxR ? vxL : vxR) - cfm;
+  const double sR = (vxL > vxR ? vxL : vxR) + cfm;
+  const double den = sR * rR - sL * rL - (mxR - mxL);
+  const double deni = 1. / den;
+  const double num = sR * mxR - sL * mxL - (fmxR - fmxL);
+  const double sM = num * deni;
+  const double sLvxL = sL - vxL, sRvxR = sR - vxR;
+  const double sLsMi = 1. / (sL - sM), sRsMi = 1. / (sR - sM);
+  const double xL = sLvxL * sLsMi, xR = sRvxR * sRsMi;
+  const double rLs = rL * xL, rRs = rR * xR;
+  const double pts = rL * sLvxL * (sM - vxL) + ptL;
+  const double rvL = rL * sLvxL, rvR = rR * sRvxR;
+  const double wvbL = 1. / (rvL * (sL - sM) - bx2), wvbR = 1. / (rvR * (sR - sM) - bx2);
+  const double wvL = bx * (sM - vxL) * wvbL, wvR = bx * (sM - vxR) * wvbR;
+  const double vyLs = wL[VY] - wL[BY] * wvL, vyRs = wR[VY] - wR[BY] * wvR;
+  const double vzLs = wL[VZ] - wL[BZ] * wvL, vzRs = wR[VZ] - wR[BZ] * wvR;
+  const double QL = rvL * sLvxL - bx2, QR = rvR * sRvxR - bx2;
+  const double wbL = QL * wvbL, wbR = QR * wvbR;
+  const double byLs = wL[BY] * wbL, byRs = wR[BY] * wbR;
+  const double bzLs = wL[BZ] * wbL, bzRs = wR[BZ] * wbR;
+  const double vsbsL = sM * bx + vyLs * byLs + vzLs * bzLs;
+  const double vsbsR = sM * bx + vyRs * byRs + vzRs * bzRs;
+  const double srL = sqrt(rLs), srR = sqrt(rRs);
+  const double abx = fabs(bx);
+  const double sLs = sM - abx / srL, sRs = sM + abx / srR;
+  int r = 0;
+  if (sL > 0.) r = 1;
+  if (sL <= 0. && 0. < sLs) r = 2;
+  if (sLs <= 0. && 0. < sM) r = 3;
+  if (sM <= 0. && 0. < sRs) r = 4;
+  if (sRs <= 0. && 0. < sR) r = 5;
+  if (sR <= 0.) r = 6;
+  if (r == 0) return;
+  const double dsum = srL + srR;
+  const double rhoLRi = 1. / dsum;
+  const double sgnb = sgn(bx);
+  const double Nvy = srL * vyLs + srR * vyRs + (byRs - byLs) * sgnb;
+  const double Nvz = srL * vzLs + srR * vzRs + (bzRs - bzLs) * sgnb;
+  const double Nby = srL * byRs + srR * byLs + srL * srR * (vyRs - vyLs) * sgnb;
+  const double Nbz = srL * bzRs + srR * bzLs + srL * srR * (vzRs - vzLs) * sgnb;
+  const double vyss = Nvy * rhoLRi, vzss = Nvz * rhoLRi;
+  const double byss = Nby * rhoLRi, bzss = Nbz * rhoLRi;
+  const double vssbss = sM * bx + vyss * byss + vzss * bzss;
+
+  const bool left = r <= 3;
+  const double* w = left ? wL : wR;
+  double* wb = left ? wLb : wRb;
+  const double s_o = left ? sL : sR;
+  const double s_i = left ? sLs : sRs;
+  const double x = left ? xL : xR;
+  const double svx = left ? sLvxL : sRvxR;
+  const double sMi = left ? sLsMi : sRsMi;
+  const double pt = left ? ptL : ptR;
+  const double rs = left ? rLs : rRs;
+  const double vys = left ? vyLs : vyRs, vzs = left ? vzLs : vzRs;
+  const double bys = left ? byLs : byRs, bzs = left ? bzLs : bzRs;
+  const double vsbs = left ? vsbsL : vsbsR;
+  const double srs = left ? srL : srR;
+  double u[NM], f[NM];
+  cons_of(w, gam, u);
+  flux_of(w, gam, f);
+  const double dotvb = w[VX] * bx + w[VY] * w[BY] + w[VZ] * w[BZ];
+  const double nume = svx * u[EN] - pt * w[VX] + pts * sM + bx * (dotvb - vsbs);
+  const double es = nume * sMi;
+  const double us[NM] = {rs, rs * sM, rs * vys, rs * vzs, es, u[PSC] * x, 0., bys, bzs};
+  const double t = srs * (vsbs - vssbss) * sgnb;
+  const double ess = left ? es - t : es + t;
+  const double uss[NM] = {rs, rs * sM, rs * vyss, rs * vzss, ess, u[PSC] * x, 0., byss, bzss};
+
+  // ---- reverse ----
+  double F[NM];
+  for (int n = 0; n < NM; ++n) F[n] = n == BX ? 0. : fb[n];
+  double fbb[NM], ub[NM], usb[NM], ussb[NM];
+  double s_ob = 0., s_ib = 0.;
+  for (int n = 0; n < NM; ++n) {
+    fbb[n] = F[n];
+    ub[n] = 0.;
+    usb[n] = 0.;
+    ussb[n] = 0.;
+  }
+  if (r == 2 || r == 5 || r == 3 || r == 4) {
+    for (int n = 0; n < NM; ++n) {
+      s_ob += F[n] * (us[n] - u[n]);
+      usb[n] += s_o * F[n];
+      ub[n] -= s_o * F[n];
+    }
+  }
+  if (r == 3 || r == 4) {
+    for (int n = 0; n < NM; ++n) {
+      s_ib += F[n] * (uss[n] - us[n]);
+      ussb[n] += s_i * F[n];
+      usb[n] -= s_i * F[n];
+    }
+  }
+  // scalar cotangents
+  double rsb = 0., sMb = 0., vyssb = 0., vzssb = 0., essb = 0., xb = 0., byssb = 0., bzssb = 0.;
+  double vysb = 0., vzsb = 0., esb = 0., bysb = 0., bzsb = 0.;
+  double uPSCb = 0.;
+  // uss
+  rsb += ussb[0] + ussb[1] * sM + ussb[2] * vyss + ussb[3] * vzss;
+  sMb += ussb[1] * rs;
+  vyssb += ussb[2] * rs;
+  vzssb += ussb[3] * rs;
+  essb += ussb[4];
+  uPSCb += ussb[5] * x;
+  xb += ussb[5] * u[PSC];
+  byssb += ussb[7];
+  bzssb += ussb[8];
+  // ess = es -+ t ; t = srs (vsbs - vssbss) sgnb
+  esb += essb;
+  const double tb = left ? -essb : essb;
+  double srsb = tb * (vsbs - vssbss) * sgnb;
+  double vsbsb = tb * srs * sgnb;
+  double vssbssb = -tb * srs * sgnb;
+  // us
+  rsb += usb[0] + usb[1] * sM + usb[2] * vys + usb[3] * vzs;
+  sMb += usb[1] * rs;
+  vysb += usb[2] * rs;
+  vzsb += usb[3] * rs;
+  esb += usb[4];
+  uPSCb += usb[5] * x;
+  xb += usb[5] * u[PSC];
+  bysb += usb[7];
+  bzsb += usb[8];
+  // es = nume * sMi
+  const double numeb = esb * sMi;
+  double sMib = esb * nume;
+  double svxb = numeb * u[EN];
+  ub[EN] += numeb * svx;
+  double ptb = -numeb * w[VX];
+  wb[VX] -= numeb * pt;
+  double ptsb = numeb * sM;
+  sMb += numeb * pts;
+  double bxb = numeb * (dotvb - vsbs);
+  vsbsb -= numeb * bx;
+  {
+    const double db = numeb * bx;
+    wb[VX] += db * bx;
+    bxb += db * w[VX];
+    wb[VY] += db * w[BY];
+    wb[BY] += db * w[VY];
+    wb[VZ] += db * w[BZ];
+    wb[BZ] += db * w[VZ];
+  }
+  ub[PSC] += uPSCb;
+  // u and f of the side (u = prim2cons(w), f = flux(w))
+  vjp_flux(w, fbb, gam, wb);
+  vjp_prim2cons(w, ub, gam, wb);
+  // vssbss = sM bx + vyss byss + vzss bzss
+  sMb += vssbssb * bx;
+  bxb += vssbssb * sM;
+  vyssb += vssbssb * byss;
+  byssb += vssbssb * vyss;
+  vzssb += vssbssb * bzss;
+  bzssb += vssbssb * vzss;
+  // double-star tangential state
+  double srLb = 0., srRb = 0., rhoLRib = 0.;
+  double vyLsb = 0., vyRsb = 0., vzLsb = 0., vzRsb = 0., byLsb = 0., byRsb = 0., bzLsb = 0., bzRsb = 0.;
+  {
+    const double Nb = byssb * rhoLRi;
+    rhoLRib += byssb * Nby;
+    srLb += Nb * (byRs + srR * (vyRs - vyLs) * sgnb);
+    srRb += Nb * (byLs + srL * (vyRs - vyLs) * sgnb);
+    byRsb += Nb * srL;
+    byLsb += Nb * srR;
+    vyRsb += Nb * srL * srR * sgnb;
+    vyLsb -= Nb * srL * srR * sgnb;
+  }
+  {
+    const double Nb = bzssb * rhoLRi;
+    rhoLRib += bzssb * Nbz;
+    srLb += Nb * (bzRs + srR * (vzRs - vzLs) * sgnb);
+    srRb += Nb * (bzLs + srL * (vzRs - vzLs) * sgnb);
+    bzRsb += Nb * srL;
+    bzLsb += Nb * srR;
+    vzRsb += Nb * srL * srR * sgnb;
+    vzLsb -= Nb * srL * srR * sgnb;
+  }
+  {
+    const double Nb = vyssb * rhoLRi;
+    rhoLRib += vyssb * Nvy;
+    srLb += Nb * vyLs;
+    vyLsb += Nb * srL;
+    srRb += Nb * vyRs;
+    vyRsb += Nb * srR;
+    byRsb += Nb * sgnb;
+    byLsb -= Nb * sgnb;
+  }
+  {
+    const double Nb = vzssb * rhoLRi;
+    rhoLRib += vzssb * Nvz;
+    srLb += Nb * vzLs;
+    vzLsb += Nb * srL;
+    srRb += Nb * vzRs;
+    vzRsb += Nb * srR;
+    bzRsb += Nb * sgnb;
+    bzLsb -= Nb * sgnb;
+  }
+  {
+    const double db = -rhoLRib * rhoLRi * rhoLRi;
+    srLb += db;
+    srRb += db;
+  }
+  // side selections (one side's copies of the scalar star quantities)
+  double sLb = 0., sRb = 0., sLsb = 0., sRsb = 0., xLb = 0., xRb = 0., sLvxLb = 0., sRvxRb = 0.;
+  double sLsMib = 0., sRsMib = 0., ptLb = 0., ptRb = 0., rLsb = 0., rRsb = 0.;
+  if (left) {
+    sLb += s_ob;
+    sLsb += s_ib;
+    xLb += xb;
+    sLvxLb += svxb;
+    sLsMib += sMib;
+    ptLb += ptb;
+    rLsb += rsb;
+    vyLsb += vysb;
+    vzLsb += vzsb;
+    byLsb += bysb;
+    bzLsb += bzsb;
+    srLb += srsb;
+  } else {
+    sRb += s_ob;
+    sRsb += s_ib;
+    xRb += xb;
+    sRvxRb += svxb;
+    sRsMib += sMib;
+    ptRb += ptb;
+    rRsb += rsb;
+    vyRsb += vysb;
+    vzRsb += vzsb;
+    byRsb += bysb;
+    bzRsb += bzsb;
+    srRb += srsb;
+  }
+  // vsbs (the chosen side's copy) and pts
+  double vsbsLb = left ? vsbsb : 0., vsbsRb = left ? 0. : vsbsb;
+  // sLs = sM - |bx| / srL ; sRs = sM + |bx| / srR
+  sMb += sLsb + sRsb;
+  bxb += -sLsb * sgn(bx) / srL + sRsb * sgn(bx) / srR;
+  srLb += sLsb * abx / (srL * srL);
+  srRb -= sRsb * abx / (srR * srR);
+  // srL = sqrt(rLs)
+  rLsb += srLb * 0.5 / srL;
+  rRsb += srRb * 0.5 / srR;
+  // vsbs = sM bx + vys bys + vzs bzs (both sides)
+  sMb += (vsbsLb + vsbsRb) * bx;
+  bxb += (vsbsLb + vsbsRb) * sM;
+  vyLsb += vsbsLb * byLs;
+  byLsb += vsbsLb * vyLs;
+  vzLsb += vsbsLb * bzLs;
+  bzLsb += vsbsLb * vzLs;
+  vyRsb += vsbsRb * byRs;
+  byRsb += vsbsRb * vyRs;
+  vzRsb += vsbsRb * bzRs;
+  bzRsb += vsbsRb * vzRs;
+  // bys = by wb
+  double wbLb = byLsb * wL[BY] + bzLsb * wL[BZ];
+  double wbRb = byRsb * wR[BY] + bzRsb * wR[BZ];
+  wLb[BY] += byLsb * wbL;
+  wLb[BZ] += bzLsb * wbL;
+  wRb[BY] += byRsb * wbR;
+  wRb[BZ] += bzRsb * wbR;
+  // wb = Q wvb
+  double wvbLb = wbLb * QL, wvbRb = wbRb * QR;
+  const double QLb = wbLb * wvbL, QRb = wbRb * wvbR;
+  double rvLb = QLb * sLvxL, rvRb = QRb * sRvxR;
+  sLvxLb += QLb * rvL;
+  sRvxRb += QRb * rvR;
+  double bx2b = -QLb - QRb;
+  // vys = vy - by wv ; vzs = vz - bz wv
+  wLb[VY] += vyLsb;
+  wLb[VZ] += vzLsb;
+  wRb[VY] += vyRsb;
+  wRb[VZ] += vzRsb;
+  wLb[BY] -= vyLsb * wvL;
+  wLb[BZ] -= vzLsb * wvL;
+  wRb[BY] -= vyRsb * wvR;
+  wRb[BZ] -= vzRsb * wvR;
+  const double wvLb = -vyLsb * wL[BY] - vzLsb * wL[BZ];
+  const double wvRb = -vyRsb * wR[BY] - vzRsb * wR[BZ];
+  // wv = bx (sM - vx) wvb
+  bxb += wvLb * (sM - vxL) * wvbL + wvRb * (sM - vxR) * wvbR;
+  sMb += wvLb * bx * wvbL + wvRb * bx * wvbR;
+  wLb[VX] -= wvLb * bx * wvbL;
+  wRb[VX] -= wvRb * bx * wvbR;
+  wvbLb += wvLb * bx * (sM - vxL);
+  wvbRb += wvRb * bx * (sM - vxR);
+  // wvb = 1 / (rv (s - sM) - bx2)
+  {
+    const double DLb = -wvbLb * wvbL * wvbL, DRb = -wvbRb * wvbR * wvbR;
+    rvLb += DLb * (sL - sM);
+    sLb += DLb * rvL;
+    sMb -= DLb * rvL;
+    bx2b -= DLb;
+    rvRb += DRb * (sR - sM);
+    sRb += DRb * rvR;
+    sMb -= DRb * rvR;
+    bx2b -= DRb;
+  }
+  // rv = rho (s - vx)
+  double rLb = rvLb * sLvxL, rRb = rvRb * sRvxR;
+  sLvxLb += rvLb * rL;
+  sRvxRb += rvRb * rR;
+  // pts = rL sLvxL (sM - vxL) + ptL
+  rLb += ptsb * sLvxL * (sM - vxL);
+  sLvxLb += ptsb * rL * (sM - vxL);
+  sMb += ptsb * rL * sLvxL;
+  wLb[VX] -= ptsb * rL * sLvxL;
+  ptLb += ptsb;
+  // rs = rho x
+  rLb += rLsb * xL;
+  xLb += rLsb * rL;
+  rRb += rRsb * xR;
+  xRb += rRsb * rR;
+  // x = svx sMi
+  sLvxLb += xLb * sLsMi;
+  sLsMib += xLb * sLvxL;
+  sRvxRb += xRb * sRsMi;
+  sRsMib += xRb * sRvxR;
+  // sMi = 1 / (s - sM)
+  {
+    const double eL = -sLsMib * sLsMi * sLsMi, eR = -sRsMib * sRsMi * sRsMi;
+    sLb += eL;
+    sMb -= eL;
+    sRb += eR;
+    sMb -= eR;
+  }
+  // svx = s - vx
+  sLb += sLvxLb;
+  wLb[VX] -= sLvxLb;
+  sRb += sRvxRb;
+  wRb[VX] -= sRvxRb;
+  // sM = num deni ; deni = 1 / den
+  const double numb = sMb * deni;
+  const double denb = -sMb * num * deni * deni;
+  // num = sR mxR - sL mxL - (fmxR - fmxL)
+  sRb += numb * mxR;
+  double mxRb = numb * sR;
+  sLb -= numb * mxL;
+  double mxLb = -numb * sL;
+  const double fmxRb = -numb, fmxLb = numb;
+  // den = sR rR - sL rL - (mxR - mxL)
+  sRb += denb * rR;
+  rRb += denb * sR;
+  sLb -= denb * rL;
+  rLb -= denb * sL;
+  mxRb -= denb;
+  mxLb += denb;
+  // fmx = mx vx + pt - bx2
+  mxLb += fmxLb * vxL;
+  wLb[VX] += fmxLb * mxL;
+  ptLb += fmxLb;
+  mxRb += fmxRb * vxR;
+  wRb[VX] += fmxRb * mxR;
+  ptRb += fmxRb;
+  bx2b -= fmxLb + fmxRb;
+  // mx = rho vx
+  rLb += mxLb * vxL;
+  wLb[VX] += mxLb * rL;
+  rRb += mxRb * vxR;
+  wRb[VX] += mxRb * rR;
+  // pt = p + 0.5 b2 ; b2 = bx2 + by^2 + bz^2
+  wLb[PR] += ptLb;
+  wRb[PR] += ptRb;
+  bx2b += 0.5 * (ptLb + ptRb);
+  wLb[BY] += ptLb * wL[BY];
+  wLb[BZ] += ptLb * wL[BZ];
+  wRb[BY] += ptRb * wR[BY];
+  wRb[BZ] += ptRb * wR[BZ];
+  wLb[RHO] += rLb;
+  wRb[RHO] += rRb;
+  // wave speeds
+  vjp_wave_speeds(wL, wR, gam, sLb, sRb, wLb, wRb);
+  // the normal field
+  bxb += 2. * bx * bx2b;
+  wLb[BX] += bxb;
+}
+
+// Slope limiters (reconstr_c.h:28-44): partial derivatives of lim(a, b).
+template <int LIM>
+BNZ_HD void lim_grad(double a, double b, double& da, double& db) {
+  if (LIM == 2) {  // minmod
+    da = db = 0.;
+    if (a * b <= 0.) return;
+    if (a > 0.) {
+      if (a < b) da = 1.;
+      else db = 1.;
+    } else {
+      if (a > b) da = 1.;
+      else db = 1.;
+    }
+  } else if (LIM == 1) {  // mc: mm(2 mm(a, b), 0.5 (a + b))
+    da = db = 0.;
+    double m1a, m1b;
+    lim_grad<2>(a, b, m1a, m1b);
+    double m1;
+    m1 = (a * b <= 0.) ? 0. : ((a > 0.) ? ((a < b) ? a : b) : ((a > b) ? a : b));
+    const double p = 2. * m1, q = 0.5 * (a + b);
+    double dp, dq;
+    lim_grad<2>(p, q, dp, dq);
+    da = dp * 2. * m1a + dq * 0.5;
+    db = dp * 2. * m1b + dq * 0.5;
+  } else {  // van Leer: 2ab / (a + b) for ab > 0
+    const double ab = a * b;
+    if (ab > 0.) {
+      const double s = a + b;
+      da = 2. * b * b / (s * s);
+      db = 2. * a * a / (s * s);
+    } else {
+      da = db = 0.;
+    }
+  }
+}
+
+BNZ_HD void lim_grad_rt(int lim, double a, double b, double& da, double& db) {
+  if (lim == 1) lim_grad<1>(a, b, da, db);
+  else if (lim == 2) lim_grad<2>(a, b, da, db);
+  else lim_grad<0>(a, b, da, db);
+}
+
+// PLM face states of one variable at a face (reconstr_c.c:54-91):
+//   wL = wm1 + 0.5 lim(wm1 - wm2, w0 - wm1),  wR = w0 - 0.5 lim(w0 - wm1, wp1 - w0).
+// Given wLb, wRb, return the cotangents of (wm2, wm1, w0, wp1) in c[0..3].
+BNZ_HD void vjp_plm(int lim, double wm2, double wm1, double w0, double wp1, double wLb, double wRb, double* c) {
+  double la, lb;
+  lim_grad_rt(lim, wm1 - wm2, w0 - wm1, la, lb);
+  // wL
+  c[0] = -0.5 * la * wLb;
+  c[1] = wLb * (1. + 0.5 * la - 0.5 * lb);
+  c[2] = 0.5 * lb * wLb;
+  double ra, rb;
+  lim_grad_rt(lim, w0 - wm1, wp1 - w0, ra, rb);
+  // wR
+  c[1] += 0.5 * ra * wRb;
+  c[2] += wRb * (1. - 0.5 * ra + 0.5 * rb);
+  c[3] = -0.5 * rb * wRb;
+  c[0] += 0.;
+}
+
+}  // namespace adj

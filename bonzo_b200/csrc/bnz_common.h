@@ -113,6 +113,28 @@ struct FusedLaunch {
   cudaEvent_t* events;
 };
 
+// One reverse (adjoint) step of the fused 2D path: the recorded forward
+// values, the incoming and outgoing cotangents and the scratch.
+struct AdjStep {
+  const double* Wn;   // w^n, b^n (the step's input state)
+  const double* Bn;
+  const double* Ws;   // ws, bs (the predictor's output for that state)
+  const double* Bs;
+  const double* W1;   // w^(n+1) (the step's output prim)
+  double* G1w;        // cotangent of the output (folded in place first)
+  double* G1b;
+  double* Vw;         // out: cotangent of the input state (9 + 3 fields)
+  double* Vb;
+  double* Wsb;        // scratch: 9, 3, 9, 1 and 72 fields of Ntot cells
+  double* Bsb;
+  double* Ub;
+  double* Eb;
+  double* Q;
+  double dt;
+  int rsolver, limiter;
+  cudaStream_t stream;
+};
+
 // Conduction scratch (thcond_elec.pyx DiffScratch).
 struct DiffArgs {
   double* temp;

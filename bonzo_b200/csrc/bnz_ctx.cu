@@ -10,79 +10,16 @@
 #include <string>
 #include <vector>
 
-#include "../../include/bnz_gpu.h"
-#include "bnz_common.h"
-#include "bnz_launch.h"
+#include "bnz_ctx_internal.h"
 
-struct bnz_ctx {
-  bnz_grid_desc gd;
-  bnz_method_desc md;
-  int Ntot[3];
-  int ng;
-  int i1, i2, j1, j2, k1, k2;
-  size_t ncell;
-  std::vector<double> lf[3], lv[3], dlf[3], dlf_inv[3], dlv[3], dlv_inv[3];
-  double* d_coord = nullptr;
-  GridDev g;
-  // state and scratch
-  double* prim = nullptr;
-  double* cons = nullptr;
-  double* bfld = nullptr;
-  double* cons_s = nullptr;
-  double* bfld_s = nullptr;
-  double* flx[3] = {nullptr, nullptr, nullptr};
-  double* ec = nullptr;
-  double* ee = nullptr;
-  double* wnext = nullptr;
-  double* bnext = nullptr;
-  // fused path: ping-pong state buffers, tile lists, instance descriptor
-  double* wbuf[2] = {nullptr, nullptr};
-  double* bbuf[2] = {nullptr, nullptr};
-  int parity = 0;
-  bool ghosts_stale = false;  // fused path: ghosts / cons not refreshed since the last step
-  FusedInst* d_inst = nullptr;
-  FusedTile* d_tiles = nullptr;
-  int ntA = 0, ntB = 0;
-  int graph_parity = -1;
-  int variant = 0;
-  // conduction scratch
-  double* dscr = nullptr;
-  DiffArgs da;
-  int last_nsts = 0;
-  // device scalars
-  unsigned* d_err = nullptr;
-  DtState* d_ds = nullptr;
-  double* d_sts = nullptr;  // stage coefficients (4 per stage)
-  int sts_cap = 0;
-  cudaStream_t stream = nullptr;
-  cudaGraphExec_t graph = nullptr;
-  double graph_tmax = -1.;
-  const Launchers* L = nullptr;
-  std::string err;
-  double time = 0.;
-  long step = 0;
-  double last_dt = 0.;
-  long long launches = 0;  // kernels launched through this context
-  long long graph_launches = 0;
-  double h_stage[3] = {0., 0., 0.};  // host staging for async copies of the time record
-  long long h_step = 0;
-  bool time_on_device = false;  // the device DtState holds the current time
-  bool own_stream = true;
-};
+using namespace bnzi;
 
-namespace {
+namespace bnzi {
 
 int fail(bnz_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;
   return code;
 }
-
-#define CKC(call)                                                                                \
-  do {                                                                                           \
-    cudaError_t _e = (call);                                                                     \
-    if (_e != cudaSuccess)                                                                       \
-      return fail(c, BNZ_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e));         \
-  } while (0)
 
 // coord.pyx:122-258 (uniform axes) + cartesian.pyx:18-43: face coordinates,
 // periodic / reflected ghost spacings, centres and spacings.
@@ -337,7 +274,7 @@ int validate(const bnz_grid_desc* g, const bnz_method_desc* m, std::string& why)
   return 1;
 }
 
-}  // namespace
+}  // namespace bnzi
 
 namespace {
 
@@ -518,6 +455,7 @@ int bnz_create(const bnz_grid_desc* gd, const bnz_method_desc* md, bnz_ctx** out
 int bnz_destroy(bnz_ctx* c) {
   if (!c) return BNZ_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  adj_free(c);
   free_all(c);
   delete c;
   return BNZ_OK;
@@ -609,7 +547,7 @@ int bnz_new_dt(bnz_ctx* c, double* dt_out) {
 
 }  // extern "C"
 
-namespace {
+namespace bnzi {
 
 // RKL2 stage loop (thcond_elec.pyx:17-113); dtp points at the hyperbolic dt.
 int diffuse_impl(bnz_ctx* c, const double* dtp, double dt_hyp, int* nsts_out) {
@@ -690,7 +628,7 @@ void set_parity(bnz_ctx* c, int p) {
 
 // vanleer.pyx:101-163 with dt already in d_ds->dt.  dt_mode selects how the
 // fused path obtains dt (explicit host value, device CFL, or FIXDT).
-int step_impl(bnz_ctx* c, double dt_host, int dt_mode = FDT_EXPLICIT) {
+int step_impl(bnz_ctx* c, double dt_host, int dt_mode) {
   StepArgs a = step_args(c);
   const double* dtp = &c->d_ds->dt;
   if (c->md.path == BNZ_PATH_PLAIN) {
@@ -718,7 +656,7 @@ int step_impl(bnz_ctx* c, double dt_host, int dt_mode = FDT_EXPLICIT) {
   return BNZ_OK;
 }
 
-}  // namespace
+}  // namespace bnzi
 
 extern "C" {
 

@@ -16,6 +16,8 @@ namespace BNZ_NS {
 #include "bnz_bc_dt.cuh"
 #include "bnz_diffusion.cuh"
 #include "bnz_fused.cuh"
+#include "bnz_adjoint_math.h"
+#include "bnz_adjoint.cuh"
 
 namespace {
 
@@ -331,6 +333,77 @@ int fused_time(const FusedLaunch& f) {
 int fused_cds(const FusedLaunch& f, int parity) {
   fused::k_cds_batch<<<f.ntB, 256, 0, f.stream>>>(f.insts, f.tilesB, parity);
   return 1;
+}
+
+// --- discrete adjoint of one fused 2D step ------------------------------
+
+namespace {
+template <int RS>
+void adj_stage(const FusedInst& I, const adjk::StageArgs& a, int lim, cudaStream_t st) {
+  const int T = 128;
+  const adjk::Box& R = a.R;
+  const long long ncell = (long long)(R.ib - R.ia + 1) * (R.jb - R.ja + 1);
+  const long long ncorner = (long long)(R.ib - R.ia + 2) * (R.jb - R.ja + 2);
+  const long long nfx = (long long)(R.ib - R.ia + 2) * (R.jb - R.ja + 3);
+  const long long nfy = (long long)(R.ib - R.ia + 3) * (R.jb - R.ja + 2);
+  const int h = a.order == 0 ? 1 : 2;
+  const long long ngat = (long long)(R.ib - R.ia + 1 + 2 * h) * (R.jb - R.ja + 1 + 2 * h);
+  adjk::k_cells<<<nblocks(ncell, T), T, 0, st>>>(I, a);
+  adjk::k_corners<<<nblocks(ncorner, T), T, 0, st>>>(I, a);
+  adjk::k_faces<0, RS><<<nblocks(nfx, T), T, 0, st>>>(I, a, lim);
+  adjk::k_faces<1, RS><<<nblocks(nfy, T), T, 0, st>>>(I, a, lim);
+  adjk::k_gather<<<nblocks(ngat, T), T, 0, st>>>(I, a);
+}
+
+void adj_fold(const FusedInst& I, double* Vw, double* Vb, cudaStream_t st) {
+  adjk::k_fold<0><<<nblocks(12LL * I.ny, 128), 128, 0, st>>>(I, Vw, Vb);
+  adjk::k_fold<1><<<nblocks(12LL * I.nx, 128), 128, 0, st>>>(I, Vw, Vb);
+}
+}  // namespace
+
+int adj_step(const FusedInst& I, const AdjStep& s) {
+  const size_t nc = (size_t)I.sv;
+  int launches = 0;
+  adj_fold(I, s.G1w, s.G1b, s.stream);
+  cudaMemsetAsync(s.Vw, 0, 9 * nc * sizeof(double), s.stream);
+  cudaMemsetAsync(s.Vb, 0, 3 * nc * sizeof(double), s.stream);
+  cudaMemsetAsync(s.Bsb, 0, 3 * nc * sizeof(double), s.stream);
+  launches += 2;
+  adjk::StageArgs a;
+  // corrector: order 1 on the active cells
+  a.order = 1;
+  a.dt = s.dt;
+  a.R = {I.ng, I.ng + I.N[0] - 1, I.ng, I.ng + I.N[1] - 1};
+  a.Wout = s.W1;
+  a.Gw = s.G1w;
+  a.Gb = s.G1b;
+  a.Wsrc = s.Ws;
+  a.Bsrc = s.Bs;
+  a.Wn = s.Wn;
+  a.Vw = s.Vw;
+  a.Vb = s.Vb;
+  a.Wsrc_b = s.Wsb;
+  a.Bsrc_b = s.Bsb;
+  a.Ub = s.Ub;
+  a.Eb = s.Eb;
+  a.Q = s.Q;
+  if (s.rsolver == dev::RS_HLLD) adj_stage<dev::RS_HLLD>(I, a, s.limiter, s.stream);
+  else adj_stage<dev::RS_HLL>(I, a, s.limiter, s.stream);
+  // predictor: order 0 on cells 1..Ntot-2, half step
+  a.order = 0;
+  a.dt = 0.5 * s.dt;
+  a.R = {1, I.nx - 2, 1, I.ny - 2};
+  a.Wout = s.Ws;
+  a.Gw = s.Wsb;
+  a.Gb = s.Bsb;
+  a.Wsrc = s.Wn;
+  a.Bsrc = s.Bn;
+  a.Wsrc_b = s.Vw;
+  a.Bsrc_b = s.Vb;
+  if (s.rsolver == dev::RS_HLLD) adj_stage<dev::RS_HLLD>(I, a, s.limiter, s.stream);
+  else adj_stage<dev::RS_HLL>(I, a, s.limiter, s.stream);
+  adj_fold(I, s.Vw, s.Vb, s.stream);
+  return launches + 4 + 2 * 5;
 }
 
 }  // namespace BNZ_NS

@@ -19,6 +19,7 @@ struct Launchers {
   int (*diff_dt_max)(const StepArgs&, const DiffArgs&, unsigned long long* slot);
   int (*diff_operator)(const StepArgs&, const DiffArgs&);
   int (*diff_stage_update)(const StepArgs&, const DiffArgs&, int first, const double* coef, const double* dtp);
+  int (*adj_step)(const FusedInst& I, const AdjStep& s);
 };
 
 #define BNZ_DECLARE_LAUNCHERS(NS)                                                                     \
@@ -37,6 +38,7 @@ struct Launchers {
   int diff_dt_max(const StepArgs&, const DiffArgs&, unsigned long long* slot);                      \
   int diff_operator(const StepArgs&, const DiffArgs&);                                               \
   int diff_stage_update(const StepArgs&, const DiffArgs&, int first, const double* coef, const double* dtp); \
+  int adj_step(const FusedInst& I, const AdjStep& s);                                                \
   extern const Launchers table;                                                                       \
   }
 
@@ -48,4 +50,4 @@ BNZ_DECLARE_LAUNCHERS(fast)
                                NS::fused_cds, NS::apply_bc,                                           \
                                NS::prim2cons_all, NS::cons2prim_all, NS::interp_bc_active,           \
                                NS::new_dt, NS::set_dt, NS::time_advance, NS::diff_dt_max,            \
-                               NS::diff_operator, NS::diff_stage_update};
+                               NS::diff_operator, NS::diff_stage_update, NS::adj_step};

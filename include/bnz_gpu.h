@@ -181,6 +181,33 @@ int bnz_batch_time_variant(bnz_batch* batch, int variant, int steps, double* ms)
 int bnz_batch_autotune(bnz_batch* batch, int steps, int* best, double* ms_per_variant);
 
 /* ------------------------------------------------------------------------
+ * Discrete adjoint of the VL2 step (fused 2D path, PLM, rsolver hll or hlld,
+ * no conduction, fixed dt).  No counterpart in the reference, which has no
+ * adjoint; these serve the torch.autograd wrapper (bonzo_b200/adjoint.py).
+ * All state and cotangent pointers are DEVICE pointers to full arrays with
+ * ghosts, (9, Ntot) prim and (3, Ntot) face field, ordered on the context's
+ * stream.  A cotangent of an output refers to the arrays as
+ * bnz_get_state_device returns them (ghosts filled); the cotangent of an input
+ * is zero on ghost entries, which the step never reads. */
+
+/* Device-to-device state copies (bnz_set_state / bnz_get_state with device
+ * buffers; set takes prim and derives cons). */
+int bnz_set_state_device(bnz_ctx* ctx, const double* prim, const double* bfld);
+int bnz_get_state_device(bnz_ctx* ctx, double* prim, double* bfld);
+/* nsteps steps of fixed dt from the current state, keeping the input state of
+ * every checkpoint_every-th step on the device (the tape for the reverse pass). */
+int bnz_rollout_forward(bnz_ctx* ctx, int nsteps, double dt, int checkpoint_every);
+/* Reverse pass of the recorded rollout: cotangent of the final state ->
+ * cotangent of the initial state.  Segments between checkpoints are recomputed;
+ * the context's state is left at the rollout's final state. */
+int bnz_rollout_adjoint(bnz_ctx* ctx, const double* gprim, const double* gbfld, double* gprim0, double* gbfld0);
+/* VJP of one step of dt at the state (prim, bfld): cotangent of the step's
+ * output (gprim1, gbfld1) -> cotangent of its input (gprim0, gbfld0).  The
+ * context's state becomes the step's output. */
+int bnz_step_adjoint(bnz_ctx* ctx, double dt, const double* prim, const double* bfld, const double* gprim1,
+                     const double* gbfld1, double* gprim0, double* gbfld0);
+
+/* ------------------------------------------------------------------------
  * One VL2 step that allocates no device memory.  No counterpart in the
  * reference: it exists for callers that must not let a library allocate --
  * programs whose device memory belongs to a framework allocator that reserved
