@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
+    ap.add_argument("--adjoint-only", action="store_true", help="print only the adjoint/forward measurement")
     return ap.parse_args()
 
 
@@ -433,6 +434,12 @@ def main():
                 "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
+        return 0
+    if args.adjoint_only:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "adjoint": run_adjoint()}), flush=True)
         return 0
     if world > 1:
         import datetime

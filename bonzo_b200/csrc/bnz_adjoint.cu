@@ -4,11 +4,18 @@
 //
 // Tape of a rollout of nsteps steps with a checkpoint every K steps:
 //   ckpt   the input state (w 9 + b 3 fields) of steps 0, K, 2K, ...
-//   slot   K+1 records of one segment rebuilt during the reverse pass: the
-//          state w, b of each step and its predictor output ws, bs
-//   work   two cotangent buffers (ping-pong, 12 fields each) and the reverse
-//          step's scratch (Wsb 9, Bsb 3, Ub 9, Eb 1, Q 72 fields)
-// Memory: (12 ceil(nsteps/K) + 24 (K+1) + 118) fields of Ntot cells.
+//   slot   two sets of K+1 records of one segment: the state w, b of each step
+//          and its predictor output ws, bs.  The forward pass fills the last
+//          segment's set directly; the reverse pass rebuilds every other
+//          segment from its checkpoint.
+//   work   two cotangent buffers (ping-pong, 12 fields each), the reverse
+//          step's scratch (Wsb 9, Bsb 3, Ub 9, Eb 1, Q 72 fields) and a copy
+//          of the final state (12)
+// Memory: (12 ceil(nsteps/K) + 48 (K+1) + 142) fields of Ntot cells.
+//
+// The reverse pass runs on its own stream: while segment s is reversed there,
+// segment s-1 is recomputed on the context's stream into the other slot set
+// (events order the two).
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -19,20 +26,24 @@
 using namespace bnzi;
 
 struct bnz_adj {
-  int nsteps = 0, K = 0, nck = 0, nslot = 0;
+  int nsteps = 0, K = 0, nck = 0;
   double dt = 0.;
   bool recorded = false;
   double* ckpt = nullptr;
   double* slot = nullptr;
   double* work = nullptr;
   size_t ckpt_cap = 0, slot_cap = 0, work_cap = 0;
+  cudaStream_t rev = nullptr;         // reverse-pass stream
+  cudaEvent_t ev_rec[2] = {nullptr, nullptr};  // slot set p rebuilt
+  cudaEvent_t ev_rev[2] = {nullptr, nullptr};  // slot set p consumed
+  cudaEvent_t ev_in = nullptr;
 };
 
 namespace {
 
 constexpr int NW = 12;     // fields of a state record (9 prim + 3 face)
 constexpr int NSLOT = 24;  // fields of a segment slot (w, b, ws, bs)
-constexpr int NWORK = 2 * NW + 9 + 3 + 9 + 1 + 72;
+constexpr int NWORK = 2 * NW + 9 + 3 + 9 + 1 + 72 + NW;
 
 int ensure_buf(bnz_ctx* c, double** p, size_t* cap, size_t fields) {
   const size_t bytes = fields * c->ncell * sizeof(double);
@@ -54,42 +65,71 @@ int check_adjoint_ctx(bnz_ctx* c) {
   if (c->md.rsolver != BNZ_RS_HLL && c->md.rsolver != BNZ_RS_HLLD)
     return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built for rsolver hll and hlld");
   if (!c->adj) c->adj = new bnz_adj();
+  bnz_adj* A = c->adj;
+  if (!A->rev) {
+    CKC(cudaStreamCreateWithFlags(&A->rev, cudaStreamNonBlocking));
+    for (int p = 0; p < 2; ++p) {
+      CKC(cudaEventCreateWithFlags(&A->ev_rec[p], cudaEventDisableTiming));
+      CKC(cudaEventCreateWithFlags(&A->ev_rev[p], cudaEventDisableTiming));
+    }
+    CKC(cudaEventCreateWithFlags(&A->ev_in, cudaEventDisableTiming));
+  }
   return BNZ_OK;
 }
 
 double* field(double* base, bnz_ctx* c, size_t k) { return base + k * c->ncell; }
 
-// copy a 12-field state record (w then b) in or out of the context's state
-int copy_state(bnz_ctx* c, double* dw, double* db, const double* sw, const double* sb) {
-  CKC(cudaMemcpyAsync(dw, sw, 9 * c->ncell * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-  CKC(cudaMemcpyAsync(db, sb, 3 * c->ncell * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+// slot q of slot set p
+double* slot_at(bnz_ctx* c, int p, int q) { return field(c->adj->slot, c, ((size_t)p * (c->adj->K + 1) + q) * NSLOT); }
+
+// copy a 12-field state record (w then b) on stream st
+int copy_state(bnz_ctx* c, double* dw, double* db, const double* sw, const double* sb, cudaStream_t st) {
+  CKC(cudaMemcpyAsync(dw, sw, 9 * c->ncell * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CKC(cudaMemcpyAsync(db, sb, 3 * c->ncell * sizeof(double), cudaMemcpyDeviceToDevice, st));
   return BNZ_OK;
 }
 
-// one forward step of fixed dt from the context's state, recording its input
-// state and predictor output into slot q (and the output state into q + 1)
-int record_step(bnz_ctx* c, double dt, int q, bool last) {
-  bnz_adj* A = c->adj;
-  double* s = field(A->slot, c, (size_t)q * NSLOT);
-  int rc = copy_state(c, s, s + 9 * c->ncell, c->prim, c->bfld);
+// one forward step of fixed dt from the context's state (on its stream),
+// recording its input state and predictor output into slot q of set p (and,
+// when last, the output state into slot q + 1)
+int record_step(bnz_ctx* c, double dt, int p, int q, bool last) {
+  double* s = slot_at(c, p, q);
+  int rc = copy_state(c, s, s + 9 * c->ncell, c->prim, c->bfld, c->stream);
   if (rc) return rc;
   c->launches += c->L->set_dt(c->stream, c->d_ds, dt);
   rc = step_impl(c, dt);
   if (rc) return rc;
-  rc = copy_state(c, s + 12 * c->ncell, s + 21 * c->ncell, c->cons_s, c->bfld_s);
+  rc = copy_state(c, s + 12 * c->ncell, s + 21 * c->ncell, c->cons_s, c->bfld_s, c->stream);
   if (rc) return rc;
   if (last) {
-    double* s1 = field(A->slot, c, (size_t)(q + 1) * NSLOT);
-    rc = copy_state(c, s1, s1 + 9 * c->ncell, c->prim, c->bfld);
+    double* s1 = slot_at(c, p, q + 1);
+    rc = copy_state(c, s1, s1 + 9 * c->ncell, c->prim, c->bfld, c->stream);
   }
   return rc;
 }
 
-// reverse step of slot q: cotangent (gw, gb) of slot q+1's state -> (vw, vb)
-int reverse_step(bnz_ctx* c, double dt, int q, double* gw, double* gb, double* vw, double* vb) {
+// rebuild segment seg of the recorded rollout into slot set p (context stream)
+int recompute_segment(bnz_ctx* c, int seg, int p) {
   bnz_adj* A = c->adj;
-  double* s = field(A->slot, c, (size_t)q * NSLOT);
-  double* s1 = field(A->slot, c, (size_t)(q + 1) * NSLOT);
+  const int n0 = seg * A->K;
+  const int m = (A->nsteps - n0) < A->K ? (A->nsteps - n0) : A->K;
+  double* ck = field(A->ckpt, c, (size_t)seg * NW);
+  int rc = copy_state(c, c->prim, c->bfld, ck, ck + 9 * c->ncell, c->stream);
+  if (rc) return rc;
+  for (int q = 0; q < m; ++q) {
+    rc = record_step(c, A->dt, p, q, q == m - 1);
+    if (rc) return rc;
+  }
+  return BNZ_OK;
+}
+
+// reverse step of slot q of set p on stream st: cotangent (gw, gb) of the step's
+// output -> (vw, vb); fold_in: gw, gb may carry ghost entries
+int reverse_step(bnz_ctx* c, double dt, int p, int q, double* gw, double* gb, double* vw, double* vb, bool fold_in,
+                 cudaStream_t st) {
+  bnz_adj* A = c->adj;
+  double* s = slot_at(c, p, q);
+  double* s1 = slot_at(c, p, q + 1);
   double* wk = field(A->work, c, 2 * NW);
   AdjStep a;
   a.Wn = s;
@@ -109,21 +149,32 @@ int reverse_step(bnz_ctx* c, double dt, int q, double* gw, double* gb, double* v
   a.dt = dt;
   a.rsolver = c->md.rsolver;
   a.limiter = c->md.limiter;
-  a.stream = c->stream;
+  a.fold_in = fold_in ? 1 : 0;
+  a.stream = st;
   c->launches += c->L->adj_step(make_inst(c), a);
   CKC(cudaGetLastError());
   return BNZ_OK;
 }
+
+double* keep_at(bnz_ctx* c) { return field(c->adj->work, c, NWORK - NW); }
 
 }  // namespace
 
 namespace bnzi {
 void adj_free(bnz_ctx* c) {
   if (!c || !c->adj) return;
-  if (c->adj->ckpt) cudaFree(c->adj->ckpt);
-  if (c->adj->slot) cudaFree(c->adj->slot);
-  if (c->adj->work) cudaFree(c->adj->work);
-  delete c->adj;
+  bnz_adj* A = c->adj;
+  if (A->rev) cudaStreamSynchronize(A->rev);
+  if (A->ckpt) cudaFree(A->ckpt);
+  if (A->slot) cudaFree(A->slot);
+  if (A->work) cudaFree(A->work);
+  for (int p = 0; p < 2; ++p) {
+    if (A->ev_rec[p]) cudaEventDestroy(A->ev_rec[p]);
+    if (A->ev_rev[p]) cudaEventDestroy(A->ev_rev[p]);
+  }
+  if (A->ev_in) cudaEventDestroy(A->ev_in);
+  if (A->rev) cudaStreamDestroy(A->rev);
+  delete A;
   c->adj = nullptr;
 }
 }  // namespace bnzi
@@ -133,7 +184,7 @@ extern "C" {
 int bnz_set_state_device(bnz_ctx* c, const double* prim, const double* bfld) {
   if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
   if (!prim || !bfld) return fail(c, BNZ_ERR_ARG, "null state pointer");
-  int rc = copy_state(c, c->prim, c->bfld, prim, bfld);
+  int rc = copy_state(c, c->prim, c->bfld, prim, bfld, c->stream);
   if (rc) return rc;
   StepArgs a = step_args(c);
   c->launches += c->L->prim2cons_all(a);
@@ -162,20 +213,30 @@ int bnz_rollout_forward(bnz_ctx* c, int nsteps, double dt, int checkpoint_every)
   A->recorded = false;
   const int K = checkpoint_every < nsteps ? checkpoint_every : nsteps;
   const int nck = (nsteps + K - 1) / K;
+  A->K = K;
   rc = ensure_buf(c, &A->ckpt, &A->ckpt_cap, (size_t)NW * nck);
   if (rc) return rc;
+  rc = ensure_buf(c, &A->slot, &A->slot_cap, (size_t)NSLOT * 2 * (K + 1));
+  if (rc) return rc;
+  // the previous reverse pass may still read the slots
+  CKC(cudaStreamSynchronize(A->rev));
+  const int last = nck - 1, n_last = last * K;
   for (int n = 0; n < nsteps; ++n) {
     if (n % K == 0) {
       double* ck = field(A->ckpt, c, (size_t)(n / K) * NW);
-      rc = copy_state(c, ck, ck + 9 * c->ncell, c->prim, c->bfld);
+      rc = copy_state(c, ck, ck + 9 * c->ncell, c->prim, c->bfld, c->stream);
       if (rc) return rc;
     }
-    c->launches += c->L->set_dt(c->stream, c->d_ds, dt);
-    rc = step_impl(c, dt);
+    if (n >= n_last) {
+      // the last segment is recorded as it runs: the reverse pass starts there
+      rc = record_step(c, dt, last & 1, n - n_last, n == nsteps - 1);
+    } else {
+      c->launches += c->L->set_dt(c->stream, c->d_ds, dt);
+      rc = step_impl(c, dt);
+    }
     if (rc) return rc;
   }
   A->nsteps = nsteps;
-  A->K = K;
   A->nck = nck;
   A->dt = dt;
   A->recorded = true;
@@ -189,43 +250,52 @@ int bnz_rollout_adjoint(bnz_ctx* c, const double* gprim, const double* gbfld, do
   bnz_adj* A = c->adj;
   if (!A->recorded) return fail(c, BNZ_ERR_STATE, "no rollout recorded (bnz_rollout_forward first)");
   if (!gprim || !gbfld || !gprim0 || !gbfld0) return fail(c, BNZ_ERR_ARG, "null cotangent pointer");
-  rc = ensure_buf(c, &A->slot, &A->slot_cap, (size_t)NSLOT * (A->K + 1));
-  if (rc) return rc;
   rc = ensure_buf(c, &A->work, &A->work_cap, NWORK);
   if (rc) return rc;
-  // keep the final state: the reverse pass rebuilds segments in the context
-  double* keep = field(A->slot, c, (size_t)A->K * NSLOT + 12);
-  rc = copy_state(c, keep, keep + 9 * c->ncell, c->prim, c->bfld);
+  cudaStream_t S1 = c->stream, S2 = A->rev;
+  // keep the final state: recomputing segments moves the context's state
+  double* keep = keep_at(c);
+  rc = copy_state(c, keep, keep + 9 * c->ncell, c->prim, c->bfld, S1);
   if (rc) return rc;
   double* G = field(A->work, c, 0);
   double* V = field(A->work, c, NW);
-  rc = copy_state(c, G, G + 9 * c->ncell, gprim, gbfld);
+  rc = copy_state(c, G, G + 9 * c->ncell, gprim, gbfld, S1);
   if (rc) return rc;
+  CKC(cudaEventRecord(A->ev_in, S1));
+  CKC(cudaStreamWaitEvent(S2, A->ev_in, 0));
+  // the last segment's slots were filled by the forward pass
   for (int seg = A->nck - 1; seg >= 0; --seg) {
-    const int n0 = seg * A->K;
-    const int m = (A->nsteps - n0) < A->K ? (A->nsteps - n0) : A->K;
-    double* ck = field(A->ckpt, c, (size_t)seg * NW);
-    rc = copy_state(c, c->prim, c->bfld, ck, ck + 9 * c->ncell);
-    if (rc) return rc;
-    for (int q = 0; q < m; ++q) {
-      rc = record_step(c, A->dt, q, q == m - 1);
+    const int p = seg & 1;
+    const int m = (A->nsteps - seg * A->K) < A->K ? (A->nsteps - seg * A->K) : A->K;
+    if (seg >= 1) {
+      // rebuild the previous segment into the other set once segment seg+1
+      // (the last user of that set) has been reversed
+      if (seg + 1 <= A->nck - 1) CKC(cudaStreamWaitEvent(S1, A->ev_rev[p ^ 1], 0));
+      rc = recompute_segment(c, seg - 1, p ^ 1);
       if (rc) return rc;
+      CKC(cudaEventRecord(A->ev_rec[p ^ 1], S1));
     }
     for (int q = m - 1; q >= 0; --q) {
-      rc = reverse_step(c, A->dt, q, G, G + 9 * c->ncell, V, V + 9 * c->ncell);
+      const bool first = seg == A->nck - 1 && q == m - 1;
+      rc = reverse_step(c, A->dt, p, q, G, G + 9 * c->ncell, V, V + 9 * c->ncell, first, S2);
       if (rc) return rc;
       double* t = G;
       G = V;
       V = t;
     }
+    CKC(cudaEventRecord(A->ev_rev[p], S2));
+    if (seg >= 1) CKC(cudaStreamWaitEvent(S2, A->ev_rec[p ^ 1], 0));
   }
-  rc = copy_state(c, gprim0, gbfld0, G, G + 9 * c->ncell);
+  CKC(cudaStreamWaitEvent(S1, A->ev_rev[0], 0));
+  rc = copy_state(c, gprim0, gbfld0, G, G + 9 * c->ncell, S1);
   if (rc) return rc;
-  rc = copy_state(c, c->prim, c->bfld, keep, keep + 9 * c->ncell);
+  rc = copy_state(c, c->prim, c->bfld, keep, keep + 9 * c->ncell, S1);
   if (rc) return rc;
   c->ghosts_stale = true;
   rc = refresh_cds(c);
   if (rc) return rc;
+  // the slots now hold segment 0: a second reverse pass needs a new forward
+  A->recorded = false;
   CKC(cudaGetLastError());
   return BNZ_OK;
 }
@@ -238,21 +308,23 @@ int bnz_step_adjoint(bnz_ctx* c, double dt, const double* prim, const double* bf
   if (!prim || !bfld || !gprim1 || !gbfld1 || !gprim0 || !gbfld0) return fail(c, BNZ_ERR_ARG, "null pointer");
   bnz_adj* A = c->adj;
   A->recorded = false;
-  rc = ensure_buf(c, &A->slot, &A->slot_cap, (size_t)NSLOT * 2);
+  CKC(cudaStreamSynchronize(A->rev));
+  A->K = 1;
+  rc = ensure_buf(c, &A->slot, &A->slot_cap, (size_t)NSLOT * 2 * 2);
   if (rc) return rc;
   rc = ensure_buf(c, &A->work, &A->work_cap, NWORK);
   if (rc) return rc;
-  rc = copy_state(c, c->prim, c->bfld, prim, bfld);
+  rc = copy_state(c, c->prim, c->bfld, prim, bfld, c->stream);
   if (rc) return rc;
-  rc = record_step(c, dt, 0, true);
+  rc = record_step(c, dt, 0, 0, true);
   if (rc) return rc;
   double* G = field(A->work, c, 0);
   double* V = field(A->work, c, NW);
-  rc = copy_state(c, G, G + 9 * c->ncell, gprim1, gbfld1);
+  rc = copy_state(c, G, G + 9 * c->ncell, gprim1, gbfld1, c->stream);
   if (rc) return rc;
-  rc = reverse_step(c, dt, 0, G, G + 9 * c->ncell, V, V + 9 * c->ncell);
+  rc = reverse_step(c, dt, 0, 0, G, G + 9 * c->ncell, V, V + 9 * c->ncell, true, c->stream);
   if (rc) return rc;
-  rc = copy_state(c, gprim0, gbfld0, V, V + 9 * c->ncell);
+  rc = copy_state(c, gprim0, gbfld0, V, V + 9 * c->ncell, c->stream);
   if (rc) return rc;
   c->ghosts_stale = true;
   rc = refresh_cds(c);

@@ -19,6 +19,10 @@
 // Included inside the per-floating-point-mode namespace.
 #pragma once
 
+#ifndef BNZ_ADJ_FACE_MINB
+#define BNZ_ADJ_FACE_MINB 1  // blocks of 128 per SM the face kernel is compiled for (register budget)
+#endif
+
 namespace adjk {
 
 using namespace fused;  // Inst, AxisMap, map_cell, map_face
@@ -161,27 +165,39 @@ __device__ __forceinline__ double corner_b(const Inst& I, const StageArgs& a, in
 }
 
 // --- S3: per face, the flux cotangent, the Riemann VJP and the PLM VJP ----
-template <int AX, int RS>
-__global__ void k_faces(const Inst I, const StageArgs a, int lim) {
+// The PLM stencil is not kept live across the Riemann VJP: the face states are
+// built, the stencil dropped, and the four cells reloaded (L1) for the PLM VJP.
+template <int AX, int ORDER>
+__device__ __forceinline__ double plm_cell(const Inst& I, const double* W, int i, int j, int q, int gv) {
+  const int ci = AX == 0 ? i - 2 + q : i, cj = AX == 0 ? j : j - 2 + q;
+  return W[gv * I.sv + cidx(I, ci, cj)];
+}
+
+// x faces: i in [ia, ib+1], rows [ja-1, jb+1]; y faces: rows [ja, jb+1], columns [ia-1, ib+1]
+template <int AX>
+__device__ __forceinline__ void face_range(const Box& R, int& fi0, int& fj0, int& w, long long& n) {
+  fi0 = AX == 0 ? R.ia : R.ia - 1;
+  fj0 = AX == 0 ? R.ja - 1 : R.ja;
+  w = R.ib + 1 - fi0 + 1;
+  n = (long long)w * (R.jb + 1 - fj0 + 1);
+}
+
+template <int AX, int ORDER, int RS>
+__device__ __forceinline__ void face_vjp(const Inst& I, const StageArgs& a, int lim, long long t) {
   const Box R = a.R;
-  // x faces: i in [ia, ib+1], rows [ja-1, jb+1]; y faces: rows [ja, jb+1], columns [ia-1, ib+1]
-  const int fi0 = AX == 0 ? R.ia : R.ia - 1, fi1 = R.ib + 1;
-  const int fj0 = AX == 0 ? R.ja - 1 : R.ja, fj1 = R.jb + 1;
-  const int w = fi1 - fi0 + 1;
-  const long long n = (long long)w * (fj1 - fj0 + 1);
+  int fi0, fj0, w;
+  long long n;
+  face_range<AX>(R, fi0, fj0, w, n);
   const double dz = I.dlf2;
-  const bool map = a.order == 0;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+  {
     const int i = fi0 + (int)(t % w), j = fj0 + (int)(t / w);
     const long long f = cidx(I, i, j);
     // the two cells this face separates: (il, jl) and (i, j)
     const int il = AX == 0 ? i - 1 : i, jl = AX == 0 ? j : j - 1;
     const bool inL = in(R, il, jl), inR = in(R, i, j);
-    // flux cotangent in global variable order: 0..5 hydro, 6 = the component
-    // the corner EMF uses (Fx[BY] / Fy[BX]), 7 = Fx[BZ] / Fy[BZ]
-    double F[8];
-#pragma unroll
-    for (int v = 0; v < 8; ++v) F[v] = 0.;
+    // flux cotangent, local frame of the sweep (godunov.pyx:297-324 permutation);
+    // global 6 = the component the corner EMF uses (Fx[BY] / Fy[BX]), global 7 = Fx[BZ] / Fy[BZ]
+    double fb[NM];
     {
       const double cL = inL ? (a.dt / (I.dlf[0][il] * I.dlf[1][jl] * dz)) * (AX == 0 ? I.dlf[1][jl] * dz : I.dlf[0][il] * dz) : 0.;
       const double cR = inR ? (a.dt / (I.dlf[0][i] * I.dlf[1][j] * dz)) * (AX == 0 ? I.dlf[1][j] * dz : I.dlf[0][i] * dz) : 0.;
@@ -190,42 +206,23 @@ __global__ void k_faces(const Inst I, const StageArgs a, int lim) {
         double g = 0.;
         if (inR) g += cR * a.Ub[v * I.sv + f];
         if (inL) g -= cL * a.Ub[v * I.sv + cidx(I, il, jl)];
-        F[v] = g;
+        // global v -> local position
+        fb[AX == 0 ? v : (v == 1 ? VZ : v == 2 ? VX : v == 3 ? VY : v)] = g;
       }
-      // bz: -dt/(dx dy) dy (Fx7(i+1) - Fx7(i))  and  +dt/(dx dy) dx (Fy7(j+1) ... ) with exb = -Fy7
-      const double zR = inR ? (a.dt / (I.dlf[0][i] * I.dlf[1][j])) * (AX == 0 ? I.dlf[1][j] : I.dlf[0][i]) : 0.;
-      const double zL = inL ? (a.dt / (I.dlf[0][il] * I.dlf[1][jl])) * (AX == 0 ? I.dlf[1][jl] : I.dlf[0][il]) : 0.;
+      // bz: -dt/(dx dy) dy (Fx7(i+1) - Fx7(i)) and +dt/(dx dy) dx (ext - exb) with exb = -Fy7
       double g7 = 0.;
-      if (inR) g7 += zR * bz_total(I, a, i, j);
-      if (inL) g7 -= zL * bz_total(I, a, il, jl);
-      F[7] = g7;
+      if (inR) g7 += (a.dt / (I.dlf[0][i] * I.dlf[1][j])) * (AX == 0 ? I.dlf[1][j] : I.dlf[0][i]) * bz_total(I, a, i, j);
+      if (inL) g7 -= (a.dt / (I.dlf[0][il] * I.dlf[1][jl])) * (AX == 0 ? I.dlf[1][jl] : I.dlf[0][il]) * bz_total(I, a, il, jl);
       // corner EMF: E(ci,cj) = 0.5 (-Fx6(ci,cj-1) - Fx6(ci,cj) + Fy6(ci-1,cj) + Fy6(ci,cj)) - ...
-      if (AX == 0) F[6] = -0.5 * (corner_b(I, a, i, j) + corner_b(I, a, i, j + 1));
-      else F[6] = 0.5 * (corner_b(I, a, i, j) + corner_b(I, a, i + 1, j));
-    }
-    // local-frame flux cotangent (godunov.pyx:297-324 permutation)
-    double fb[NM];
-    if (AX == 0) {
-#pragma unroll
-      for (int v = 0; v < 6; ++v) fb[v] = F[v];
+      const double g6 = AX == 0 ? -0.5 * (corner_b(I, a, i, j) + corner_b(I, a, i, j + 1))
+                                : 0.5 * (corner_b(I, a, i, j) + corner_b(I, a, i + 1, j));
       fb[BX] = 0.;
-      fb[BY] = F[6];
-      fb[BZ] = F[7];
-    } else {
-      fb[RHO] = F[0];
-      fb[VX] = F[2];
-      fb[VY] = F[3];
-      fb[VZ] = F[1];
-      fb[EN] = F[4];
-      fb[PSC] = F[5];
-      fb[BX] = 0.;
-      fb[BY] = F[7];
-      fb[BZ] = F[6];
+      fb[BY] = AX == 0 ? g6 : g7;
+      fb[BZ] = AX == 0 ? g7 : g6;
     }
     // face states exactly as the forward builds them
-    double wL[NM], wR[NM], wLb[NM], wRb[NM];
-    double s4[4][NM];  // order 1: the four cells along the axis (local frame)
-    if (a.order == 0) {
+    double wL[NM], wR[NM];
+    if (ORDER == 0) {
       double cl_[NM], cr_[NM];
       read_cell(I, a.Wsrc, il, jl, true, cl_);
       read_cell(I, a.Wsrc, i, j, true, cr_);
@@ -237,20 +234,18 @@ __global__ void k_faces(const Inst I, const StageArgs a, int lim) {
       }
     } else {
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int ci = AX == 0 ? i - 2 + q : i, cj = AX == 0 ? j : j - 2 + q;
-        const long long cc = cidx(I, ci, cj);
-#pragma unroll
-        for (int v = 0; v < NM; ++v) s4[q][v] = a.Wsrc[plain::perm<AX>(v) * I.sv + cc];
-      }
-#pragma unroll
       for (int v = 0; v < NM; ++v) {
-        wL[v] = s4[1][v] + plain::half_slope_rt(lim, s4[0][v], s4[1][v], s4[2][v]);
-        wR[v] = s4[2][v] - plain::half_slope_rt(lim, s4[1][v], s4[2][v], s4[3][v]);
+        if (v == BX) continue;
+        const int gv = plain::perm<AX>(v);
+        const double c0 = plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 0, gv), c1 = plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 1, gv);
+        const double c2 = plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 2, gv), c3 = plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 3, gv);
+        wL[v] = c1 + plain::half_slope_rt(lim, c0, c1, c2);
+        wR[v] = c2 - plain::half_slope_rt(lim, c1, c2, c3);
       }
     }
-    const double bn = read_face<AX>(I, a.Bsrc, i, j, map);
+    const double bn = read_face<AX>(I, a.Bsrc, i, j, ORDER == 0);
     wL[BX] = wR[BX] = bn;
+    double wLb[NM], wRb[NM];
 #pragma unroll
     for (int v = 0; v < NM; ++v) wLb[v] = wRb[v] = 0.;
     if (RS == dev::RS_HLLD) adj::vjp_hlld(wL, wR, I.gam, fb, wLb, wRb);
@@ -261,12 +256,14 @@ __global__ void k_faces(const Inst I, const StageArgs a, int lim) {
     for (int v = 0; v < NM; ++v) {
       if (v == BX) continue;
       const int gv = plain::perm<AX>(v);
-      if (a.order == 0) {
+      if (ORDER == 0) {
         Qa[(1 * NM + gv) * I.sv + f] = wLb[v];
         Qa[(2 * NM + gv) * I.sv + f] = wRb[v];
       } else {
         double c4[4];
-        adj::vjp_plm(lim, s4[0][v], s4[1][v], s4[2][v], s4[3][v], wLb[v], wRb[v], c4);
+        adj::vjp_plm(lim, plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 0, gv), plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 1, gv),
+                     plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 2, gv), plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 3, gv), wLb[v],
+                     wRb[v], c4);
 #pragma unroll
         for (int q = 0; q < 4; ++q) Qa[(q * NM + gv) * I.sv + f] = c4[q];
       }
@@ -275,9 +272,24 @@ __global__ void k_faces(const Inst I, const StageArgs a, int lim) {
     const double bnb = wLb[BX] + wRb[BX];
     const bool out = AX == 0 ? (j >= R.ja && j <= R.jb) : (i >= R.ia && i <= R.ib);
     double vb = out ? face_total<AX>(I, a, i, j) : 0.;
-    if (a.order == 0) vb += bnb;
+    if (ORDER == 0) vb += bnb;
     else a.Bsrc_b[AX * I.sv + f] = bnb;
     if (vb != 0.) a.Vb[AX * I.sv + f] += vb;
+  }
+}
+
+// Both face directions in one launch (the x faces first), so the two halves
+// share the waves of one grid.
+template <int ORDER, int RS>
+__global__ void __launch_bounds__(128, BNZ_ADJ_FACE_MINB) k_faces(const Inst I, const StageArgs a, int lim) {
+  int fi0, fj0, w;
+  long long nx, ny;
+  face_range<0>(a.R, fi0, fj0, w, nx);
+  face_range<1>(a.R, fi0, fj0, w, ny);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nx + ny;
+       t += (long long)gridDim.x * blockDim.x) {
+    if (t < nx) face_vjp<0, ORDER, RS>(I, a, lim, t);
+    else face_vjp<1, ORDER, RS>(I, a, lim, t - nx);
   }
 }
 
@@ -370,25 +382,31 @@ __device__ __forceinline__ int fold_src(const Inst& I, int f, int a, double& sig
   return s;
 }
 
+// One thread per (field, line, remappable position): the ghosts on both sides
+// and the first active position (a zeroed reflecting face).  Sources are never
+// ghosts, so moving a ghost's value into its source with an atomic add is
+// exact whatever the order (several ghosts share a source under outflow).
 template <int AX>
 __global__ void k_fold(const Inst I, double* Vw, double* Vb) {
   const int nline = AX == 0 ? I.ny : I.nx;
   const int len = AX == 0 ? I.nx : I.ny;
-  const int total = 12 * nline;
+  const int a1 = I.ng, a2 = I.ng + I.N[AX] - 1;
+  const int nrem = a1 + 1 + (len - a2 - 1);  // positions 0..a1 and a2+1..len-1
+  const int total = 12 * nline * nrem;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-    const int f = t / nline, line = t % nline;
+    const int r = t % nrem, fl = t / nrem;
+    const int f = fl / nline, line = fl % nline;
+    const int p = r <= a1 ? r : a2 + 1 + (r - a1 - 1);
     double* V = f < NM ? Vw + (long long)f * I.sv : Vb + (long long)(f - NM) * I.sv;
     const long long st = AX == 0 ? 1 : I.nx;
     const long long base = AX == 0 ? (long long)line * I.nx : line;
-    for (int p = 0; p < len; ++p) {
-      double sign;
-      bool zero;
-      const int s = fold_src<AX>(I, f, p, sign, zero);
-      if (s == p && !zero) continue;
-      const double v = V[base + p * st];
-      V[base + p * st] = 0.;
-      if (!zero) V[base + s * st] += sign * v;
-    }
+    double sign;
+    bool zero;
+    const int s = fold_src<AX>(I, f, p, sign, zero);
+    if (s == p && !zero) continue;
+    const double v = V[base + p * st];
+    V[base + p * st] = 0.;
+    if (!zero && v != 0.) atomicAdd(&V[base + s * st], sign * v);
   }
 }
 

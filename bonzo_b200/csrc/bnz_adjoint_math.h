@@ -74,7 +74,8 @@ BNZ_HD void vjp_flux(const double* w, const double* fb, double gam, double* wb) 
   const double b2 = sq(bx) + sq(by) + sq(bz);
   const double v2 = sq(vx) + sq(vy) + sq(vz);
   const double pt = p + 0.5 * b2;
-  const double en = 0.5 * (r * v2 + b2) + p / (gam - 1.);
+  const double gamm1i = 1. / (gam - 1.);
+  const double en = 0.5 * (r * v2 + b2) + p * gamm1i;
   const double dot = vx * bx + vy * by + vz * bz;
   double rb = 0., vxb = 0., vyb = 0., vzb = 0., pb = 0., bxb = 0., byb = 0., bzb = 0.;
   double ptb = 0., enb = 0.;
@@ -130,7 +131,7 @@ BNZ_HD void vjp_flux(const double* w, const double* fb, double gam, double* wb) 
   bxb += enb * bx;
   byb += enb * by;
   bzb += enb * bz;
-  pb += enb / (gam - 1.);
+  pb += enb * gamm1i;
   // pt = p + 0.5 b2
   pb += ptb;
   bxb += ptb * bx;
@@ -186,19 +187,20 @@ BNZ_HD double fms_val(const double* w, double gam) {
   return sqrt(0.5 / w[RHO] * (c1 + c2));
 }
 
-BNZ_HD void vjp_fms(const double* w, double cfb, double gam, double* wb) {
+// VJP of cf = fms(w) given its value cf (> 0)
+BNZ_HD void vjp_fms(const double* w, double cf, double cfb, double gam, double* wb) {
+  if (!(cf > 0.)) return;
   const double bx2 = sq(w[BX]);
   const double b2 = bx2 + sq(w[BY]) + sq(w[BZ]);
   const double gamp = gam * w[PR];
   const double c1 = gamp + b2;
   const double disc = c1 * c1 - 4. * gamp * bx2;
   const double c2 = sqrt(fabs(disc));
-  const double cf = sqrt(0.5 / w[RHO] * (c1 + c2));
-  if (!(cf > 0.)) return;
+  const double rhoi = 1. / w[RHO];
   const double qb = cfb * 0.5 / cf;  // q = 0.5 / rho (c1 + c2)
-  wb[RHO] += -qb * 0.5 / (w[RHO] * w[RHO]) * (c1 + c2);
-  double c1b = qb * 0.5 / w[RHO];
-  const double c2b = qb * 0.5 / w[RHO];
+  wb[RHO] += -qb * 0.5 * rhoi * rhoi * (c1 + c2);
+  double c1b = qb * 0.5 * rhoi;
+  const double c2b = c1b;
   double gampb = 0., bx2b = 0., b2b = 0.;
   if (c2 > 0.) {
     const double discb = c2b * 0.5 / c2 * sgn(disc);
@@ -217,13 +219,12 @@ BNZ_HD void vjp_fms(const double* w, double cfb, double gam, double* wb) {
 
 // sL = min(vxL, vxR) - max(cfL, cfR), sR = max(vxL, vxR) + max(cfL, cfR)
 // (fluxes_c.c:25-42): VJP given sLb, sRb.
-BNZ_HD void vjp_wave_speeds(const double* wL, const double* wR, double gam, double sLb, double sRb, double* wLb,
-                            double* wRb) {
-  const double cfL = fms_val(wL, gam), cfR = fms_val(wR, gam);
+BNZ_HD void vjp_wave_speeds(const double* wL, const double* wR, double cfL, double cfR, double gam, double sLb,
+                            double sRb, double* wLb, double* wRb) {
   const double cfmb = -sLb + sRb;
   // fmax / fmin pick the first argument on ties
-  if (cfL >= cfR) vjp_fms(wL, cfmb, gam, wLb);
-  else vjp_fms(wR, cfmb, gam, wRb);
+  if (cfL >= cfR) vjp_fms(wL, cfL, cfmb, gam, wLb);
+  else vjp_fms(wR, cfR, cfmb, gam, wRb);
   if (wL[VX] <= wR[VX]) wLb[VX] += sLb;
   else wRb[VX] += sLb;
   if (wL[VX] >= wR[VX]) wLb[VX] += sRb;
@@ -268,7 +269,7 @@ BNZ_HD void vjp_hll(const double* wL, const double* wR, double gam, const double
   vjp_flux(wR, fRb, gam, wRb);
   vjp_prim2cons(wL, uLb, gam, wLb);
   vjp_prim2cons(wR, uRb, gam, wRb);
-  vjp_wave_speeds(wL, wR, gam, sLb, sRb, wLb, wRb);
+  vjp_wave_speeds(wL, wR, cfL, cfR, gam, sLb, sRb, wLb, wRb);
 }
 
 // HLLD flux (fluxes_c.c:616-834, as restated in bnz_device.cuh flux_hlld):
@@ -311,8 +312,9 @@ BNZ_HD void vjp_hlld(const double* wL, const double* wR, double gam, const doubl
   const double vsbsL = sM * bx + vyLs * byLs + vzLs * bzLs;
   const double vsbsR = sM * bx + vyRs * byRs + vzRs * bzRs;
   const double srL = sqrt(rLs), srR = sqrt(rRs);
+  const double isrL = 1. / srL, isrR = 1. / srR;
   const double abx = fabs(bx);
-  const double sLs = sM - abx / srL, sRs = sM + abx / srR;
+  const double sLs = sM - abx * isrL, sRs = sM + abx * isrR;
   int r = 0;
   if (sL > 0.) r = 1;
   if (sL <= 0. && 0. < sLs) r = 2;
@@ -525,12 +527,12 @@ BNZ_HD void vjp_hlld(const double* wL, const double* wR, double gam, const doubl
   double vsbsLb = left ? vsbsb : 0., vsbsRb = left ? 0. : vsbsb;
   // sLs = sM - |bx| / srL ; sRs = sM + |bx| / srR
   sMb += sLsb + sRsb;
-  bxb += -sLsb * sgn(bx) / srL + sRsb * sgn(bx) / srR;
-  srLb += sLsb * abx / (srL * srL);
-  srRb -= sRsb * abx / (srR * srR);
+  bxb += (-sLsb * isrL + sRsb * isrR) * sgn(bx);
+  srLb += sLsb * abx * isrL * isrL;
+  srRb -= sRsb * abx * isrR * isrR;
   // srL = sqrt(rLs)
-  rLsb += srLb * 0.5 / srL;
-  rRsb += srRb * 0.5 / srR;
+  rLsb += srLb * 0.5 * isrL;
+  rRsb += srRb * 0.5 * isrR;
   // vsbs = sM bx + vys bys + vzs bzs (both sides)
   sMb += (vsbsLb + vsbsRb) * bx;
   bxb += (vsbsLb + vsbsRb) * sM;
@@ -659,7 +661,7 @@ BNZ_HD void vjp_hlld(const double* wL, const double* wR, double gam, const doubl
   wLb[RHO] += rLb;
   wRb[RHO] += rRb;
   // wave speeds
-  vjp_wave_speeds(wL, wR, gam, sLb, sRb, wLb, wRb);
+  vjp_wave_speeds(wL, wR, cfL, cfR, gam, sLb, sRb, wLb, wRb);
   // the normal field
   bxb += 2. * bx * bx2b;
   wLb[BX] += bxb;

@@ -132,6 +132,7 @@ struct AdjStep {
   double* Q;
   double dt;
   int rsolver, limiter;
+  int fold_in;        // fold G1 first (it may carry ghost entries)
   cudaStream_t stream;
 };
 

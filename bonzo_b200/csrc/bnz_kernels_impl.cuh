@@ -350,25 +350,27 @@ void adj_stage(const FusedInst& I, const adjk::StageArgs& a, int lim, cudaStream
   const long long ngat = (long long)(R.ib - R.ia + 1 + 2 * h) * (R.jb - R.ja + 1 + 2 * h);
   adjk::k_cells<<<nblocks(ncell, T), T, 0, st>>>(I, a);
   adjk::k_corners<<<nblocks(ncorner, T), T, 0, st>>>(I, a);
-  adjk::k_faces<0, RS><<<nblocks(nfx, T), T, 0, st>>>(I, a, lim);
-  adjk::k_faces<1, RS><<<nblocks(nfy, T), T, 0, st>>>(I, a, lim);
+  if (a.order == 0) adjk::k_faces<0, RS><<<nblocks(nfx + nfy, T), T, 0, st>>>(I, a, lim);
+  else adjk::k_faces<1, RS><<<nblocks(nfx + nfy, T), T, 0, st>>>(I, a, lim);
   adjk::k_gather<<<nblocks(ngat, T), T, 0, st>>>(I, a);
 }
 
 void adj_fold(const FusedInst& I, double* Vw, double* Vb, cudaStream_t st) {
-  adjk::k_fold<0><<<nblocks(12LL * I.ny, 128), 128, 0, st>>>(I, Vw, Vb);
-  adjk::k_fold<1><<<nblocks(12LL * I.nx, 128), 128, 0, st>>>(I, Vw, Vb);
+  const long long rx = I.nx - I.N[0] + 1, ry = I.ny - I.N[1] + 1;  // remappable positions per line
+  adjk::k_fold<0><<<nblocks(12LL * I.ny * rx, 128), 128, 0, st>>>(I, Vw, Vb);
+  adjk::k_fold<1><<<nblocks(12LL * I.nx * ry, 128), 128, 0, st>>>(I, Vw, Vb);
 }
 }  // namespace
 
 int adj_step(const FusedInst& I, const AdjStep& s) {
-  const size_t nc = (size_t)I.sv;
   int launches = 0;
-  adj_fold(I, s.G1w, s.G1b, s.stream);
-  cudaMemsetAsync(s.Vw, 0, 9 * nc * sizeof(double), s.stream);
-  cudaMemsetAsync(s.Vb, 0, 3 * nc * sizeof(double), s.stream);
-  cudaMemsetAsync(s.Bsb, 0, 3 * nc * sizeof(double), s.stream);
-  launches += 2;
+  cudaMemsetAsync(s.Vw, 0, 9 * (size_t)I.sv * sizeof(double), s.stream);
+  cudaMemsetAsync(s.Vb, 0, 3 * (size_t)I.sv * sizeof(double), s.stream);
+  cudaMemsetAsync(s.Bsb, 0, 3 * (size_t)I.sv * sizeof(double), s.stream);
+  if (s.fold_in) {
+    adj_fold(I, s.G1w, s.G1b, s.stream);
+    launches += 2;
+  }
   adjk::StageArgs a;
   // corrector: order 1 on the active cells
   a.order = 1;
@@ -403,7 +405,7 @@ int adj_step(const FusedInst& I, const AdjStep& s) {
   if (s.rsolver == dev::RS_HLLD) adj_stage<dev::RS_HLLD>(I, a, s.limiter, s.stream);
   else adj_stage<dev::RS_HLL>(I, a, s.limiter, s.stream);
   adj_fold(I, s.Vw, s.Vb, s.stream);
-  return launches + 4 + 2 * 5;
+  return launches + 2 * 4 + 2;  // two stages of four kernels, the output fold
 }
 
 }  // namespace BNZ_NS
