@@ -32,7 +32,7 @@ EXPORTS = [
     "bnz_batch_sync", "bnz_variant_count", "bnz_batch_set_variant", "bnz_batch_get_variant",
     "bnz_batch_time_variant", "bnz_batch_autotune", "bnz_vl2_step_noalloc", "bnz_noalloc_last_error",
     "bnz_noalloc_scratch_bytes", "bnz_set_state_device", "bnz_get_state_device", "bnz_rollout_forward",
-    "bnz_rollout_adjoint", "bnz_step_adjoint",
+    "bnz_rollout_adjoint", "bnz_step_adjoint", "bnz_history", "bnz_snapshot", "bnz_snapshot_wait",
 ]
 
 
@@ -105,6 +105,9 @@ def load():
     L.bnz_rollout_forward.argtypes = [vp, C.c_int, C.c_double, C.c_int]
     L.bnz_rollout_adjoint.argtypes = [vp, vp, vp, vp, vp]
     L.bnz_step_adjoint.argtypes = [vp, C.c_double, vp, vp, vp, vp, vp, vp]
+    L.bnz_history.argtypes = [vp, _dp]
+    L.bnz_snapshot.argtypes = [vp, _dp, _dp, _dp]
+    L.bnz_snapshot_wait.argtypes = [vp]
     L.bnz_batch_set_stream.argtypes = [vp, vp]
     L.bnz_batch_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.bnz_batch_sync.argtypes = [vp]
@@ -246,6 +249,9 @@ class Context:
         self._ck(self.L.bnz_advance(self.h, tmax, max_steps, C.byref(t), C.byref(s)))
         return t.value, s.value
 
+    def set_time(self, time, step):
+        self._ck(self.L.bnz_set_time(self.h, float(time), int(step)))
+
     def time(self):
         t, s, d = C.c_double(), C.c_long(), C.c_double()
         self._ck(self.L.bnz_get_time(self.h, C.byref(t), C.byref(s), C.byref(d)))
@@ -267,6 +273,25 @@ class Context:
         p, u, b = _dp(), _dp(), _dp()
         self._ck(self.L.bnz_device_state(self.h, C.byref(p), C.byref(u), C.byref(b)))
         return (C.cast(p, C.c_void_p).value, C.cast(u, C.c_void_p).value, C.cast(b, C.c_void_p).value)
+
+    # --- output support ---------------------------------------------------
+    def history(self):
+        """The reference's 16-column history row (output.pyx get_hst_vars_grid)."""
+        out = np.zeros(16)
+        self._ck(self.L.bnz_history(self.h, _p(out)))
+        return out
+
+    def snapshot(self, prim=None, cons=None, bfld=None):
+        """Queue a device->host copy of the state into the given float64 arrays
+        (keep them alive, ideally page-locked, until snapshot_wait())."""
+        for a, nv in ((prim, 9), (cons, 9), (bfld, 3)):
+            if a is not None and (a.shape != (nv,) + self.shape or a.dtype != np.float64
+                                  or not a.flags["C_CONTIGUOUS"]):
+                raise ValueError("snapshot array has the wrong shape or layout")
+        self._ck(self.L.bnz_snapshot(self.h, _p(prim), _p(cons), _p(bfld)))
+
+    def snapshot_wait(self):
+        self._ck(self.L.bnz_snapshot_wait(self.h))
 
     # --- device-pointer state and the adjoint (pointers are ints) ---------
     def set_state_device(self, prim_ptr, bfld_ptr):

@@ -6,6 +6,7 @@ Translation units:
   bnz_ctx.cu                          (C ABI host code)
   bnz_noalloc.cu                      (the step that allocates no device memory)
   bnz_adjoint.cu                      (adjoint rollouts: tape and reverse pass)
+  bnz_io.cu                           (history reduction, asynchronous snapshots)
 linked with -shared into bonzo_b200/libbnzgpu.so.  nvcc cross-compiles, so
 this runs on machines without a GPU.
 """
@@ -28,6 +29,7 @@ UNITS = [
     ("bnz_ctx.cu", []),
     ("bnz_noalloc.cu", []),
     ("bnz_adjoint.cu", []),
+    ("bnz_io.cu", []),
 ]
 
 

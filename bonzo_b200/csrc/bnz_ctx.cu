@@ -456,6 +456,7 @@ int bnz_destroy(bnz_ctx* c) {
   if (!c) return BNZ_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
   adj_free(c);
+  io_free(c);
   free_all(c);
   delete c;
   return BNZ_OK;

@@ -67,6 +67,7 @@ struct bnz_ctx {
   bool time_on_device = false;  // the device DtState holds the current time
   bool own_stream = true;
   struct bnz_adj* adj = nullptr;  // adjoint tape (bnz_adjoint.cu), created on first use
+  struct bnz_io* io = nullptr;    // history / snapshot resources (bnz_io.cu), created on first use
 };
 
 namespace bnzi {
@@ -82,8 +83,9 @@ int ensure_ghosts(bnz_ctx* c);
 int refresh_cds(bnz_ctx* c);
 // vanleer.pyx:101-163 with dt taken as dt_mode says (FDT_EXPLICIT: d_ds->dt)
 int step_impl(bnz_ctx* c, double dt_host, int dt_mode = FDT_EXPLICIT);
-// release the adjoint tape (bnz_adjoint.cu)
+// release the adjoint tape (bnz_adjoint.cu) and the output resources (bnz_io.cu)
 void adj_free(bnz_ctx* c);
+void io_free(bnz_ctx* c);
 
 }  // namespace bnzi
 

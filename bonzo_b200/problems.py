@@ -353,3 +353,88 @@ def make_grid(Nx, Ny=1, Nz=1, dims=2, bc=0, reconstr="linear", lmin=(0., 0., 0.)
         bc = ((bc, bc), (bc, bc), (bc, bc))
     ng = 2 if reconstr == "const" else 3
     return GridCoord(Nx, Ny, Nz, dims, lmin, lmax, bc, ng)
+
+
+# ---------------------------------------------------------------------------
+# set_problem(grid, integr, usr_dir) entry points for bonzo_b200.Simulation:
+# parameters from the [problem] section (read_user_param), as the reference's
+# src/problem/*.pyx read them; each fills grid.prim and grid.bfld.
+# ---------------------------------------------------------------------------
+
+def _fill(grid, prim, bfld):
+    grid.prim[...] = prim
+    grid.bfld[...] = bfld
+
+
+def _user(usr_dir, key, dtype, default):
+    from .config import read_user_param
+    return read_user_param(key, dtype, usr_dir, default)
+
+
+def set_problem_otvortex(grid, integr, usr_dir):
+    """src/problem/otvortex.pyx: beta from [problem] beta (default 4 pi);
+    optional seeded perturbation: pert_amp, pert_kmax, seed."""
+    prim, bfld = otvortex(grid.coord, beta=_user(usr_dir, "beta", "f", 4 * math.pi), gam=integr.gam,
+                          pert_amp=_user(usr_dir, "pert_amp", "f", 0.0),
+                          pert_kmax=_user(usr_dir, "pert_kmax", "i", 4), seed=_user(usr_dir, "seed", "i", 0))
+    _fill(grid, prim, bfld)
+
+
+def set_problem_blast(grid, integr, usr_dir):
+    """src/problem/blast_MHD.pyx: rho = 1, p = 10 inside r < 0.1 of the box
+    centre and 0.1 outside, B = (1, 1, 1) / sqrt(1.5 beta) ([problem] beta);
+    the uneven-batch parameters (b_mag, b_angle, p_ratio, center) override."""
+    gc = grid.coord
+    beta = _user(usr_dir, "beta", "f", 1.0)
+    bt = 1.0 / math.sqrt(1.5 * beta)
+    prim, bfld = blast(gc, rho0=1.0, p0=0.1, b_mag=_user(usr_dir, "b_mag", "f", bt * math.sqrt(2.0)),
+                       b_angle=_user(usr_dir, "b_angle", "f", math.pi / 4),
+                       center=(_user(usr_dir, "xc", "f", 0.5), _user(usr_dir, "yc", "f", 0.5),
+                               _user(usr_dir, "zc", "f", 0.5)),
+                       radius=_user(usr_dir, "radius", "f", 0.1), p_ratio=_user(usr_dir, "p_ratio", "f", 100.0))
+    # the reference's blast also carries Bz = bt (cell-centred face in 2D)
+    a = gc.active
+    ks, js, is_ = a
+    if gc.dims >= 3:
+        bfld[2][gc.k1:gc.k2 + 2, js, is_] = _user(usr_dir, "bz", "f", bt)
+    else:
+        bfld[2][a] = _user(usr_dir, "bz", "f", bt)
+    _fill(grid, prim, bfld)
+
+
+def set_problem_turbulence3d(grid, integr, usr_dir):
+    """Decaying driven-free MHD turbulence (seed, mach, beta, kmax from [problem])."""
+    prim, bfld = turbulence3d(grid.coord, seed=_user(usr_dir, "seed", "i", 0), gam=integr.gam,
+                              mach=_user(usr_dir, "mach", "f", 1.0), beta=_user(usr_dir, "beta", "f", 1.0),
+                              kmax=_user(usr_dir, "kmax", "i", 16))
+    _fill(grid, prim, bfld)
+
+
+def set_problem_conduction3d(grid, integr, usr_dir):
+    """Field-aligned conduction test box (seed, kmax, beta from [problem])."""
+    prim, bfld = conduction3d(grid.coord, seed=_user(usr_dir, "seed", "i", 0), kmax=_user(usr_dir, "kmax", "i", 8),
+                              beta=_user(usr_dir, "beta", "f", 100.0))
+    _fill(grid, prim, bfld)
+
+
+def set_problem_thcond_gauss(grid, integr, usr_dir):
+    """src/problem/thcond_gauss.pyx: Gaussian temperature profile along B."""
+    prim, bfld = thcond_gauss(grid.coord, sig=_user(usr_dir, "sig", "f", 0.15), bx=_user(usr_dir, "bx", "f", 0.1))
+    _fill(grid, prim, bfld)
+
+
+def set_problem_linear_wave(grid, integr, usr_dir):
+    """Linear MHD eigenmode (src/problem/linwaves2d.pyx): wave fast/alfven/slow/entropy, amp."""
+    prim, bfld, _ = linear_wave(grid.coord, _user(usr_dir, "wave", "s", "fast"), amp=_user(usr_dir, "amp", "f", 1e-6),
+                                gam=integr.gam)
+    _fill(grid, prim, bfld)
+
+
+SET_PROBLEM = {
+    "otvortex": set_problem_otvortex,
+    "blast": set_problem_blast,
+    "turbulence3d": set_problem_turbulence3d,
+    "conduction3d": set_problem_conduction3d,
+    "thcond_gauss": set_problem_thcond_gauss,
+    "linear_wave": set_problem_linear_wave,
+}

@@ -181,6 +181,21 @@ int bnz_batch_time_variant(bnz_batch* batch, int variant, int steps, double* ms)
 int bnz_batch_autotune(bnz_batch* batch, int steps, int* best, double* ms_per_variant);
 
 /* ------------------------------------------------------------------------
+ * Output support (src/io/output.pyx, src/io/io.pyx).
+ * bnz_history fills out[16] with the reference's history row
+ * (get_hst_vars_grid, output.pyx:20-140): step, time, <rho>, <E_kin>, <E_th>,
+ * <E_mag>, <E>, <mx>, <my>, <mz>, <Bx>, <By>, <Bz>, rms(Bx), rms(By), rms(Bz)
+ * (means over active cells), reduced on the device; it synchronises.
+ * bnz_snapshot queues a copy of the current state (ghosts filled, cons derived)
+ * into caller-owned host buffers of (9|9|3, Ntot) doubles (NULL skips one) and
+ * returns at once: the copy drains on a separate stream while the next steps
+ * run.  The host buffers must stay valid (page-locked for a true overlap)
+ * until bnz_snapshot_wait returns. */
+int bnz_history(bnz_ctx* ctx, double* out);
+int bnz_snapshot(bnz_ctx* ctx, double* prim, double* cons, double* bfld);
+int bnz_snapshot_wait(bnz_ctx* ctx);
+
+/* ------------------------------------------------------------------------
  * Discrete adjoint of the VL2 step (fused 2D path, PLM, rsolver hll or hlld,
  * no conduction, fixed dt).  No counterpart in the reference, which has no
  * adjoint; these serve the torch.autograd wrapper (bonzo_b200/adjoint.py).
