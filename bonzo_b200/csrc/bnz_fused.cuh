@@ -192,7 +192,8 @@ struct Smem {
   static constexpr int NEC = (TXM + 2) * (TYM + 2);
   static constexpr int NEE = (TXM + 1) * (TYM + 1);
   static constexpr int NSW = RING ? NM * (TXM + 2 * RING) * (TYM + 2 * RING) : 0;  // staged cells
-  static constexpr size_t bytes = sizeof(double) * ((size_t)NF * (NFX + NFY) + NEC + NEE + NSW);
+  static constexpr int NSD = RING == 2 ? 8 * (TXM + 2) * (TYM + 2) : 0;              // corrector slopes
+  static constexpr size_t bytes = sizeof(double) * ((size_t)NF * (NFX + NFY) + NEC + NEE + NSW + NSD);
 };
 
 // ---------------------------------------------------------------------------
@@ -359,11 +360,129 @@ __device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const
   }
 }
 
+// Corrector flux stage with the PLM slopes formed once per cell: for each
+// direction, half slopes d = 0.5 lim(w - w_-, w_+ - w) of the 8 swept variables
+// go to shared memory (cells x0-1..x0+wx, y0-1..y0+wy), then each face takes
+// wL = w(i-1) + d(i-1), wR = w(i) - d(i) -- the same values reconstr_linear
+// forms per face (reconstr_c.c:54-91), with half the limiter evaluations.
+struct SlopeBuf {
+  double* d;  // 8 x (wx+2) x (wy+2)
+  int w, n;   // row width (wx+2), cells
+  int x0, y0; // array coordinates of the first cell (x0-1, y0-1)
+  __device__ __forceinline__ int at(int i, int j) const { return (j - y0) * w + (i - x0); }
+};
+
+__device__ __forceinline__ int slot8(int n) { return n < BX ? n : n - 1; }
+
+template <int AX, int LIM>
+__device__ __forceinline__ void stage_slopes(const Layout& L, const SmemCells& W, const SlopeBuf& D) {
+  FastDiv dw;
+  dw.set(D.w);
+  const int st = W.stride(AX);
+  for (int t = threadIdx.x; t < D.n; t += blockDim.x) {
+    const int cj = dw.div(t), ci = t - cj * D.w;
+    const int i = D.x0 + ci, j = D.y0 + cj;
+#pragma unroll
+    for (int n = 0; n < NM; ++n) {
+      if (n == BX) continue;
+      const double* a = W.ptr(plain::perm<AX>(n), i, j);
+      D.d[slot8(n) * D.n + t] = half_slope<LIM>(a[-st], a[0], a[st]);
+    }
+  }
+}
+
+template <int LIM, int RS>
+__device__ __forceinline__ void stage_fluxes_plm(const Inst& I, const Tile& T, const Layout& L, const SmemCells& W,
+                                                 const double* __restrict__ b, double* sFX, double* sFY, double* sEC,
+                                                 double* sD, unsigned& err) {
+  SlopeBuf D;
+  D.d = sD;
+  D.w = L.wx + 2;
+  D.n = (L.wx + 2) * (L.wy + 2);
+  D.x0 = T.x0 - 1;
+  D.y0 = T.y0 - 1;
+  // x direction: slopes, then x faces i = x0..x0+wx on rows y0-1..y0+wy
+  stage_slopes<0, LIM>(L, W, D);
+  __syncthreads();
+  {
+    FastDiv dx1;
+    dx1.set(L.wx + 1);
+    for (int t = threadIdx.x; t < L.nfx; t += blockDim.x) {
+      const int q = dx1.div(t);
+      const int fi = t - q * (L.wx + 1), fj = q - 1;
+      const int i = T.x0 + fi, j = T.y0 + fj;
+      const int cl = D.at(i - 1, j), cr = D.at(i, j);
+      double wL[NM], wR[NM];
+#pragma unroll
+      for (int n = 0; n < NM; ++n) {
+        if (n == BX) continue;
+        wL[n] = W.get(n, i - 1, j) + D.d[slot8(n) * D.n + cl];
+        wR[n] = W.get(n, i, j) - D.d[slot8(n) * D.n + cr];
+      }
+      wL[BX] = wR[BX] = b[(long long)j * I.nx + i];
+      double f[NM];
+      riemann<RS>(f, wL, wR, I.gam, err);
+      const int qq = L.fx(fi, fj);
+#pragma unroll
+      for (int n = 0; n < 6; ++n) sFX[n * L.nfx + qq] = f[n];
+      sFX[6 * L.nfx + qq] = f[BY];  // fx[BY]
+      sFX[7 * L.nfx + qq] = f[BZ];  // fx[BZ]
+    }
+  }
+  __syncthreads();
+  // y direction: slopes, y faces j = y0..y0+wy on columns x0-1..x0+wx, and E_c
+  stage_slopes<1, LIM>(L, W, D);
+  __syncthreads();
+  {
+    FastDiv dx2;
+    dx2.set(L.wx + 2);
+    const int total = L.nfy + L.nec;
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      if (t < L.nfy) {
+        const int q = dx2.div(t);
+        const int fi = t - q * (L.wx + 2) - 1, fj = q;
+        const int i = T.x0 + fi, j = T.y0 + fj;
+        const int cl = D.at(i, j - 1), cr = D.at(i, j);
+        double wL[NM], wR[NM];
+#pragma unroll
+        for (int n = 0; n < NM; ++n) {
+          if (n == BX) continue;
+          const int gv = plain::perm<1>(n);
+          wL[n] = W.get(gv, i, j - 1) + D.d[slot8(n) * D.n + cl];
+          wR[n] = W.get(gv, i, j) - D.d[slot8(n) * D.n + cr];
+        }
+        wL[BX] = wR[BX] = b[I.sv + (long long)j * I.nx + i];
+        double f[NM];
+        riemann<RS>(f, wL, wR, I.gam, err);
+        const int qq = L.fy(fi, fj);
+        sFY[0 * L.nfy + qq] = f[RHO];
+        sFY[1 * L.nfy + qq] = f[VZ];   // global MX
+        sFY[2 * L.nfy + qq] = f[VX];   // global MY
+        sFY[3 * L.nfy + qq] = f[VY];   // global MZ
+        sFY[4 * L.nfy + qq] = f[EN];
+        sFY[5 * L.nfy + qq] = f[PSC];
+        sFY[6 * L.nfy + qq] = f[BZ];   // fy[BX]
+        sFY[7 * L.nfy + qq] = f[BY];   // fy[BZ]
+      } else {
+        // cell-centred E_z = -(vx by - vy bx) (ct.pyx:148)
+        const int u = t - L.nfy;
+        const int q = dx2.div(u);
+        const int ci = u - q * (L.wx + 2) - 1, cj = q - 1;
+        const int i = T.x0 + ci, j = T.y0 + cj;
+        const double vx = W.get(VX, i, j), vy = W.get(VY, i, j), bxc = W.get(BX, i, j), byc = W.get(BY, i, j);
+        sEC[L.ec(ci, cj)] = -(vx * byc - vy * bxc);
+      }
+    }
+  }
+}
+
 // corner E_z (ct.pyx:204-207)
 __device__ __forceinline__ void stage_emf(const Layout& L, const double* sFX, const double* sFY, const double* sEC,
                                           double* sEE) {
+  FastDiv dw;
+  dw.set(L.wx + 1);
   for (int t = threadIdx.x; t < L.nee; t += blockDim.x) {
-    const int ci = t % (L.wx + 1), cj = t / (L.wx + 1);
+    const int cj = dw.div(t), ci = t - cj * (L.wx + 1);
     sEE[t] = (0.5 * (-sFX[6 * L.nfx + L.fx(ci, cj - 1)] - sFX[6 * L.nfx + L.fx(ci, cj)] +
                      sFY[6 * L.nfy + L.fy(ci - 1, cj)] + sFY[6 * L.nfy + L.fy(ci, cj)]) -
               0.25 * (sEC[L.ec(ci - 1, cj)] + sEC[L.ec(ci, cj)] + sEC[L.ec(ci - 1, cj - 1)] + sEC[L.ec(ci, cj - 1)]));
@@ -526,9 +645,9 @@ __device__ __forceinline__ void copy_tile(const Inst& I, const Tile& T, int pari
   }
 }
 
-template <int TXM, int TYM, int RS>
+template <int TXM, int TYM, int RS, int LIM>
 __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
-                                                   int parity, int lim) {
+                                                   int parity) {
   constexpr int RING = 2;
   extern __shared__ double smem[];
   __shared__ double red[8];
@@ -549,6 +668,7 @@ __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ inst
   double* sEC = sFY + NF * Smem<TXM, TYM, RING>::NFY;
   double* sEE = sEC + Smem<TXM, TYM, RING>::NEC;
   double* sW = sEE + Smem<TXM, TYM, RING>::NEE;
+  double* sD = sW + Smem<TXM, TYM, RING>::NSW;
   Stage S;
   S.x0 = T.x0 - 2;
   S.y0 = T.y0 - 2;
@@ -558,7 +678,7 @@ __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ inst
   __syncthreads();
   unsigned e = 0;
   SmemCells W{sW, S, S.cells()};
-  stage_fluxes<1, RS>(I, T, L, W, I.bs, sFX, sFY, sEC, lim, true, e);
+  stage_fluxes_plm<LIM, RS>(I, T, L, W, I.bs, sFX, sFY, sEC, sD, e);
   __syncthreads();
   stage_emf(L, sFX, sFY, sEC, sEE);
   __syncthreads();

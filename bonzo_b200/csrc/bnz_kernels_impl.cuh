@@ -276,22 +276,34 @@ int diff_stage_update(const StepArgs& a, const DiffArgs& d, int first, const dou
 
 namespace {
 
+template <int TX, int TY, int RS, int LIM>
+void launch_corr(const FusedLaunch& f, int parity) {
+  constexpr size_t smB = fused::Smem<TX, TY, 2>::bytes;
+  static bool attrs = false;
+  if (!attrs) {
+    cudaFuncSetAttribute(fused::k_corr2d<TX, TY, RS, LIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB);
+    attrs = true;
+  }
+  fused::k_corr2d<TX, TY, RS, LIM><<<f.ntB, 256, smB, f.stream>>>(f.insts, f.tilesB, parity);
+}
+
 template <int TX, int TY, int RS, int STAGED>
 void launch_variant(const FusedLaunch& f, int parity) {
   constexpr int TXA = TX + 4, TYA = TY + 4;  // predictor tiles grow by the ghost rings
   constexpr size_t smA = fused::Smem<TXA, TYA, STAGED ? 1 : 0>::bytes;
-  constexpr size_t smB = fused::Smem<TX, TY, 2>::bytes;
   static bool attrs = false;
   if (!attrs) {
     cudaFuncSetAttribute(fused::k_pred2d<TXA, TYA, RS, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smA);
-    cudaFuncSetAttribute(fused::k_corr2d<TX, TY, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB);
     attrs = true;
   }
   if (f.events) cudaEventRecord(f.events[1], f.stream);
   fused::k_pred2d<TXA, TYA, RS, STAGED><<<f.ntA, 256, smA, f.stream>>>(f.insts, f.tilesA, parity, f.limiter);
   if (f.events) cudaEventRecord(f.events[2], f.stream);
-  fused::k_corr2d<TX, TY, RS><<<f.ntB, 256, smB, f.stream>>>(f.insts, f.tilesB, parity, f.limiter);
+  // the limiter is a compile-time choice of the corrector (reconstr_c.h:28-44)
+  if (f.limiter == dev::LIM_MC) launch_corr<TX, TY, RS, dev::LIM_MC>(f, parity);
+  else if (f.limiter == dev::LIM_MM) launch_corr<TX, TY, RS, dev::LIM_MM>(f, parity);
+  else launch_corr<TX, TY, RS, dev::LIM_VL>(f, parity);
   if (f.events) cudaEventRecord(f.events[3], f.stream);
 }
 
