@@ -226,8 +226,16 @@ __device__ __forceinline__ void flux_hlld(double* flux, const double* wL, const 
 
   double sLvxL = sL - wL[VX];
   double sRvxR = sR - wR[VX];
+#if BNZ_FAST_MATH
+  // one division for both reciprocals (sL < sM < sR)
+  const double dLM = sL - sM, dRM = sR - sM;
+  const double inv2 = 1. / (dLM * dRM);
+  double sLsMi = dRM * inv2;
+  double sRsMi = dLM * inv2;
+#else
   double sLsMi = 1. / (sL - sM);
   double sRsMi = 1. / (sR - sM);
+#endif
   double xL = sLvxL * sLsMi;
   double xR = sRvxR * sRsMi;
   double rLs = wL[RHO] * xL, rRs = wR[RHO] * xR;
@@ -250,10 +258,18 @@ __device__ __forceinline__ void flux_hlld(double* flux, const double* wL, const 
   double vsbsL = sM * bx + vyLs * byLs + vzLs * bzLs;
   double vsbsR = sM * bx + vyRs * byRs + vzRs * bzRs;
 
+#if BNZ_FAST_MATH
+  const double isrL = rsqrt(rLs), isrR = rsqrt(rRs);
+  double sqrt_rhoLs = rLs * isrL;
+  double sqrt_rhoRs = rRs * isrR;
+  double sLs = sM - fabs(bx) * isrL;
+  double sRs = sM + fabs(bx) * isrR;
+#else
   double sqrt_rhoLs = sqrt(rLs);
   double sqrt_rhoRs = sqrt(rRs);
   double sLs = sM - fabs(bx) / sqrt_rhoLs;
   double sRs = sM + fabs(bx) / sqrt_rhoRs;
+#endif
 
   int r = 0;
   if (sL > 0.) r = 1;

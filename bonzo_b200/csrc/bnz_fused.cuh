@@ -503,8 +503,13 @@ __device__ __forceinline__ void stage_cell(const Inst& I, const Layout& L, const
                                            double dt, CellOut& o) {
   const int i = T.x0 + ci, j = T.y0 + cj;
   const double dx = I.dlf[0][i], dy = I.dlf[1][j], dz = I.dlf2;
+#if BNZ_FAST_MATH
+  const double idx = I.dlf_inv[0][i], idy = I.dlf_inv[1][j], idz = 1. / dz;
+  double dtdv = dt * idx * idy * idz;
+#else
   double vol = dx * dy * dz;
   double dtdv = dt / vol;
+#endif
   double dax = dy * dz;
   double day = dx * dz;
   double u[NM];
@@ -519,13 +524,25 @@ __device__ __forceinline__ void stage_cell(const Inst& I, const Layout& L, const
   // faces (2D: E_z at corners, E_y = fx[BZ] on x faces, E_x = -fy[BZ] on y faces)
   const double e00 = sEE[L.ee(ci, cj)], e10 = sEE[L.ee(ci + 1, cj)];
   const double e01 = sEE[L.ee(ci, cj + 1)], e11 = sEE[L.ee(ci + 1, cj + 1)];
+#if BNZ_FAST_MATH
+  double dtda = dt * idy * idz;
+#else
   double dtda = dt / (dy * dz);
+#endif
   o.bxl = bxl0 - dtda * (dz * e01 - dz * e00);
   o.bxr = bxr0 - dtda * (dz * e11 - dz * e10);
+#if BNZ_FAST_MATH
+  dtda = dt * idx * idz;
+#else
   dtda = dt / (dx * dz);
+#endif
   o.byb = byb0 + dtda * (dz * e10 - dz * e00);
   o.byt = byt0 + dtda * (dz * e11 - dz * e01);
+#if BNZ_FAST_MATH
+  dtda = dt * idx * idy;
+#else
   dtda = dt / (dx * dy);
+#endif
   const double eyl = sFX[7 * L.nfx + ql], eyr = sFX[7 * L.nfx + qr];
   const double exb = -sFY[7 * L.nfy + qb], ext = -sFY[7 * L.nfy + qt];
   double bz = bz0 - dtda * (dy * eyr - dy * eyl);
@@ -719,7 +736,11 @@ __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ inst
     // next step's CFL (new_dt.pyx:55-99) on the new state
     double vf = fms(o.w, I.gam);
     double cx = fabs(o.w[VX]) + vf, cy = fabs(o.w[VY]) + vf;
+#if BNZ_FAST_MATH
+    double cds = fmax(cx * I.dlf_inv[0][i], cy * I.dlf_inv[1][j]);
+#else
     double cds = fmax(fmax(cx / I.dlf[0][i], cy / I.dlf[1][j]), 0. / I.dlf2);
+#endif
     if (cds > cmax) cmax = cds;
   }
   for (int o = 16; o > 0; o >>= 1) cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
