@@ -91,11 +91,36 @@ __device__ __forceinline__ double fms(const double* w, double gam) {
   return sqrt(0.5 / w[RHO] * (c1 + c2));
 }
 
+#if BNZ_FAST_MATH
+// fms of both face states with one division for the two 0.5 / rho
+__device__ __forceinline__ void fms2(const double* wL, const double* wR, double gam, double& cfL, double& cfR) {
+  const double h = 0.5 / (wL[RHO] * wR[RHO]);
+  double q[2];
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const double* w = s ? wR : wL;
+    double bx2 = sqr(w[BX]);
+    double b2 = bx2 + sqr(w[BY]) + sqr(w[BZ]);
+    double gamp = gam * w[PR];
+    double c1 = gamp + b2;
+    double c2 = sqrt(fabs(c1 * c1 - 4. * gamp * bx2));
+    q[s] = (s ? wL[RHO] : wR[RHO]) * h * (c1 + c2);
+  }
+  cfL = sqrt(q[0]);
+  cfR = sqrt(q[1]);
+}
+#endif
+
 // fluxes_c.c:25-42
 __device__ __forceinline__ void wave_speeds(const double* wL, const double* wR, double gam,
                                             double& sL, double& sR) {
+#if BNZ_FAST_MATH
+  double cfL, cfR;
+  fms2(wL, wR, gam, cfL, cfR);
+#else
   double cfL = fms(wL, gam);
   double cfR = fms(wR, gam);
+#endif
   double cf_max = fmax(cfL, cfR);
   sL = fmin(wL[VX], wR[VX]) - cf_max;
   sR = fmax(wL[VX], wR[VX]) + cf_max;
@@ -243,8 +268,15 @@ __device__ __forceinline__ void flux_hlld(double* flux, const double* wL, const 
 
   double rhosLvxL = wL[RHO] * sLvxL;
   double rhosRvxR = wR[RHO] * sRvxR;
+#if BNZ_FAST_MATH
+  const double DL = rhosLvxL * (sL - sM) - bx2, DR = rhosRvxR * (sR - sM) - bx2;
+  const double iD = 1. / (DL * DR);
+  double wvbL = DR * iD;
+  double wvbR = DL * iD;
+#else
   double wvbL = 1. / (rhosLvxL * (sL - sM) - bx2);
   double wvbR = 1. / (rhosRvxR * (sR - sM) - bx2);
+#endif
   double wvL = bx * (sM - wL[VX]) * wvbL;
   double wvR = bx * (sM - wR[VX]) * wvbR;
   double vyLs = wL[VY] - wL[BY] * wvL;
