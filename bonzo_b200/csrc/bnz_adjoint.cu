@@ -64,6 +64,7 @@ int check_adjoint_ctx(bnz_ctx* c) {
   if (c->md.kappa0 > 0.) return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint covers the hyperbolic step only (kappa0 = 0)");
   if (c->md.rsolver != BNZ_RS_HLL && c->md.rsolver != BNZ_RS_HLLD)
     return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built for rsolver hll and hlld");
+  if (c->md.charact_proj) return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built without charact_proj");
   if (!c->adj) c->adj = new bnz_adj();
   bnz_adj* A = c->adj;
   if (!A->rev) {

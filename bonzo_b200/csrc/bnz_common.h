@@ -101,7 +101,7 @@ struct FusedLaunch {
   int ntA;
   const FusedTile* tilesB;  // corrector tiles (active cells)
   int ntB;
-  int rsolver, limiter;
+  int rsolver, limiter, charact_proj;
   int variant;
   double cour;
   int dt_mode;

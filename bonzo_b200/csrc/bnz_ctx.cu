@@ -219,6 +219,7 @@ FusedLaunch fused_launch(const bnz_ctx* c, int dt_mode) {
   f.ntB = c->ntB;
   f.rsolver = c->md.rsolver;
   f.limiter = c->md.limiter;
+  f.charact_proj = c->md.charact_proj;
   f.variant = c->variant;
   f.cour = c->md.cour;
   f.dt_mode = dt_mode;
@@ -262,7 +263,7 @@ int validate(const bnz_grid_desc* g, const bnz_method_desc* m, std::string& why)
     return why = "rsolver must be hll, hlld or hllt for MHD (hllc is hydro-only in the reference)", 0;
   if (m->reconstr != BNZ_RCN_CONST && m->reconstr != BNZ_RCN_LINEAR) return why = "reconstr must be const or linear", 0;
   if (m->limiter < 0 || m->limiter > 2) return why = "limiter must be vl, mc or mm", 0;
-  if (m->charact_proj) return why = "charact_proj=1 is not supported by the device kernels", 0;
+  if (m->charact_proj != 0 && m->charact_proj != 1) return why = "charact_proj must be 0 or 1", 0;
   if (m->kappa0 < 0.) return why = "kappa0 must be >= 0", 0;
   if (m->kappa0 > 0. && !(m->cour_diff > 0.)) return why = "cour_diff must be positive", 0;
   if (m->path != BNZ_PATH_FUSED && m->path != BNZ_PATH_PLAIN) return why = "path must be fused or plain", 0;
@@ -917,6 +918,7 @@ FusedLaunch batch_launch(const bnz_batch* b, int dt_mode) {
   f.ntB = b->ntB;
   f.rsolver = b->md.rsolver;
   f.limiter = b->md.limiter;
+  f.charact_proj = b->md.charact_proj;
   f.variant = b->variant;
   f.cour = b->md.cour;
   f.dt_mode = dt_mode;

@@ -360,6 +360,123 @@ __device__ __forceinline__ void flux_hlld(double* flux, const double* wL, const 
   flux[BX] = 0.;
 }
 
+// eos_c.h:100-216 prim2char (MHD): the differences vc (local sweep frame) in
+// the characteristic basis of the state w; PSC and BX pass through.
+__device__ __forceinline__ void prim2char(double* vc, const double* w, double gam) {
+  const double vc_rho = vc[RHO], vc_vx = vc[VX], vc_vy = vc[VY], vc_vz = vc[VZ];
+  const double vc_p = vc[PR], vc_by = vc[BY], vc_bz = vc[BZ];
+  const double w_rho = w[RHO], w_p = w[PR], w_bx = w[BX], w_by = w[BY], w_bz = w[BZ];
+  double rhoi = 1. / w_rho;
+  double s = sgnd(w_bx);
+  double a2rho = gam * w_p;
+  double a = sqrt(a2rho * rhoi);
+  double bx2 = sqr(w_bx);
+  double bperp2 = sqr(w_by) + sqr(w_bz);
+  double b2 = bx2 + bperp2;
+  double x = a2rho + b2;
+  double y = sqrt(fabs(x * x - 4. * a2rho * bx2));
+  double cf2rho = 0.5 * (x + y);
+  double cs2rho = 0.5 * (x - y);
+  double cf = sqrt(rhoi * cf2rho);
+  double cs = sqrt(rhoi * fabs(cs2rho));
+  double z = 1. / (cf2rho - cs2rho);
+  double alphaf, alphas;
+  if (cf <= cs) {
+    alphaf = 1.;
+    alphas = 0.;
+  } else if (a <= cs) {
+    alphaf = 0.;
+    alphas = 1.;
+  } else if (cf <= a) {
+    alphaf = 1.;
+    alphas = 0.;
+  } else {
+    alphaf = sqrt(z * fabs(a2rho - cs2rho));
+    alphas = sqrt(z * fabs(cf2rho - a2rho));
+  }
+  double nf = 0.5 / (a2rho * rhoi);
+  double qf_ = nf * cf * alphaf * s;
+  double qs_ = nf * cs * alphas * s;
+  double alphaf_ = nf * alphaf;
+  double alphas_ = nf * alphas;
+  double rhoisr = sqrt(rhoi);
+  double arhoisr = a * rhoisr;
+  double Af_ = alphaf_ * arhoisr;
+  double As_ = alphas_ * arhoisr;
+  x = s * rhoisr;
+  double betay = 0., betaz = 0.;
+  if (bperp2 != 0.) {
+    double bperpi = 1. / sqrt(bperp2);
+    betay = bperpi * w_by;
+    betaz = bperpi * w_bz;
+  }
+  vc[RHO] = (alphaf_ * (rhoi * vc_p - cf * vc_vx) + qs_ * (betay * vc_vy + betaz * vc_vz) +
+             As_ * (betay * vc_by + betaz * vc_bz));
+  vc[VX] = 0.5 * ((-betaz * vc_vy + betay * vc_vz) + x * (-betaz * vc_by + betay * vc_bz));
+  vc[VY] = (alphas_ * (rhoi * vc_p - cs * vc_vx) - qf_ * (betay * vc_vy + betaz * vc_vz) -
+            Af_ * (betay * vc_by + betaz * vc_bz));
+  vc[VZ] = vc_rho - 2. * nf * vc_p;
+  vc[PR] = (alphas_ * (rhoi * vc_p + cs * vc_vx) + qf_ * (betay * vc_vy + betaz * vc_vz) -
+            Af_ * (betay * vc_by + betaz * vc_bz));
+  vc[BY] = 0.5 * ((betaz * vc_vy - betay * vc_vz) + x * (-betaz * vc_by + betay * vc_bz));
+  vc[BZ] = (alphaf_ * (rhoi * vc_p + cf * vc_vx) - qs_ * (betay * vc_vy + betaz * vc_vz) +
+            As_ * (betay * vc_by + betaz * vc_bz));
+}
+
+// eos_c.h:245-333 char2prim (MHD): back to primitive differences.
+__device__ __forceinline__ void char2prim(double* vc, const double* w, double gam) {
+  const double vc_rho = vc[RHO], vc_vx = vc[VX], vc_vy = vc[VY], vc_vz = vc[VZ];
+  const double vc_p = vc[PR], vc_by = vc[BY], vc_bz = vc[BZ];
+  const double w_rho = w[RHO], w_p = w[PR], w_bx = w[BX], w_by = w[BY], w_bz = w[BZ];
+  double rhoi = 1. / w_rho;
+  double s = sgnd(w_bx);
+  double a2rho = gam * w_p;
+  double a = sqrt(a2rho * rhoi);
+  double bx2 = sqr(w_bx);
+  double bperp2 = sqr(w_by) + sqr(w_bz);
+  double b2 = bx2 + bperp2;
+  double x = a2rho + b2;
+  double y = sqrt(fabs(x * x - 4. * a2rho * bx2));
+  double cf2rho = 0.5 * (x + y);
+  double cs2rho = 0.5 * (x - y);
+  double cf = sqrt(rhoi * cf2rho);
+  double cs = sqrt(rhoi * fabs(cs2rho));
+  double z = 1. / (cf2rho - cs2rho);
+  double alphaf, alphas;
+  if (cf <= cs) {
+    alphaf = 1.;
+    alphas = 0.;
+  } else if (a <= cs) {
+    alphaf = 0.;
+    alphas = 1.;
+  } else if (cf <= a) {
+    alphaf = 1.;
+    alphas = 0.;
+  } else {
+    alphaf = sqrt(z * fabs(a2rho - cs2rho));
+    alphas = sqrt(z * fabs(cf2rho - a2rho));
+  }
+  double qf = cf * alphaf * s;
+  double qs = cs * alphas * s;
+  double rhosr = sqrt(w_rho);
+  double arhosr = a * rhosr;
+  double Af = alphaf * arhosr;
+  double As = alphas * arhosr;
+  double betay = 0., betaz = 0.;
+  if (bperp2 != 0.) {
+    double bperpi = 1. / sqrt(bperp2);
+    betay = bperpi * w_by;
+    betaz = bperpi * w_bz;
+  }
+  vc[RHO] = w_rho * (alphaf * (vc_rho + vc_bz) + alphas * (vc_vy + vc_p)) + vc_vz;
+  vc[VX] = cf * alphaf * (vc_bz - vc_rho) + cs * alphas * (vc_p - vc_vy);
+  vc[VY] = betay * (qs * (vc_rho - vc_bz) - qf * (vc_vy - vc_p)) - betaz * (vc_vx - vc_by);
+  vc[VZ] = betaz * (qs * (vc_rho - vc_bz) - qf * (vc_vy - vc_p)) + betay * (vc_vx - vc_by);
+  vc[PR] = a2rho * (alphaf * (vc_rho + vc_bz) + alphas * (vc_vy + vc_p));
+  vc[BY] = betay * (As * (vc_rho + vc_bz) - Af * (vc_vy + vc_p)) - betaz * s * rhosr * (vc_vx + vc_by);
+  vc[BZ] = betaz * (As * (vc_rho + vc_bz) - Af * (vc_vy + vc_p)) + betay * s * rhosr * (vc_vx + vc_by);
+}
+
 template <int RS>
 __device__ __forceinline__ void riemann(double* flux, const double* wL, const double* wR, double gam,
                                         unsigned& err) {
@@ -389,6 +506,25 @@ __device__ __forceinline__ double limit(double a, double b) {
 template <int LIM>
 __device__ __forceinline__ double half_slope(double wm, double wc, double wp) {
   return 0.5 * limit<LIM>(wc - wm, wp - wc);
+}
+
+// reconstr_c.c:54-91 with charact_proj: the one-sided differences of all nine
+// local variables are projected on the characteristic basis of the cell
+// (prim2char), limited, scaled by 1/2 and projected back (char2prim).
+template <int LIM>
+__device__ __forceinline__ void half_slopes_char(const double* wm, const double* wc, const double* wp, double gam,
+                                                 double* d) {
+  double dm[NM], dp[NM];
+#pragma unroll
+  for (int n = 0; n < NM; ++n) {
+    dm[n] = wc[n] - wm[n];
+    dp[n] = wp[n] - wc[n];
+  }
+  prim2char(dm, wc, gam);
+  prim2char(dp, wc, gam);
+#pragma unroll
+  for (int n = 0; n < NM; ++n) d[n] = 0.5 * limit<LIM>(dm[n], dp[n]);
+  char2prim(d, wc, gam);
 }
 
 }  // namespace dev

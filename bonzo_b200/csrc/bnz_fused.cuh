@@ -374,19 +374,37 @@ struct SlopeBuf {
 
 __device__ __forceinline__ int slot8(int n) { return n < BX ? n : n - 1; }
 
+// cp (charact_proj): the nine local variables are limited in characteristic
+// variables of the cell (reconstr_c.c:54-91 with prim2char / char2prim).
 template <int AX, int LIM>
-__device__ __forceinline__ void stage_slopes(const Layout& L, const SmemCells& W, const SlopeBuf& D) {
+__device__ __forceinline__ void stage_slopes(const Layout& L, const SmemCells& W, const SlopeBuf& D, int cp,
+                                             double gam) {
   FastDiv dw;
   dw.set(D.w);
   const int st = W.stride(AX);
   for (int t = threadIdx.x; t < D.n; t += blockDim.x) {
     const int cj = dw.div(t), ci = t - cj * D.w;
     const int i = D.x0 + ci, j = D.y0 + cj;
+    if (cp) {
+      double wm[NM], wc[NM], wp[NM], d[NM];
 #pragma unroll
-    for (int n = 0; n < NM; ++n) {
-      if (n == BX) continue;
-      const double* a = W.ptr(plain::perm<AX>(n), i, j);
-      D.d[slot8(n) * D.n + t] = half_slope<LIM>(a[-st], a[0], a[st]);
+      for (int n = 0; n < NM; ++n) {
+        const double* a = W.ptr(plain::perm<AX>(n), i, j);
+        wm[n] = a[-st];
+        wc[n] = a[0];
+        wp[n] = a[st];
+      }
+      half_slopes_char<LIM>(wm, wc, wp, gam, d);
+#pragma unroll
+      for (int n = 0; n < NM; ++n)
+        if (n != BX) D.d[slot8(n) * D.n + t] = d[n];
+    } else {
+#pragma unroll
+      for (int n = 0; n < NM; ++n) {
+        if (n == BX) continue;
+        const double* a = W.ptr(plain::perm<AX>(n), i, j);
+        D.d[slot8(n) * D.n + t] = half_slope<LIM>(a[-st], a[0], a[st]);
+      }
     }
   }
 }
@@ -394,7 +412,7 @@ __device__ __forceinline__ void stage_slopes(const Layout& L, const SmemCells& W
 template <int LIM, int RS>
 __device__ __forceinline__ void stage_fluxes_plm(const Inst& I, const Tile& T, const Layout& L, const SmemCells& W,
                                                  const double* __restrict__ b, double* sFX, double* sFY, double* sEC,
-                                                 double* sD, unsigned& err) {
+                                                 double* sD, int cp, unsigned& err) {
   SlopeBuf D;
   D.d = sD;
   D.w = L.wx + 2;
@@ -402,7 +420,7 @@ __device__ __forceinline__ void stage_fluxes_plm(const Inst& I, const Tile& T, c
   D.x0 = T.x0 - 1;
   D.y0 = T.y0 - 1;
   // x direction: slopes, then x faces i = x0..x0+wx on rows y0-1..y0+wy
-  stage_slopes<0, LIM>(L, W, D);
+  stage_slopes<0, LIM>(L, W, D, cp, I.gam);
   __syncthreads();
   {
     FastDiv dx1;
@@ -431,7 +449,7 @@ __device__ __forceinline__ void stage_fluxes_plm(const Inst& I, const Tile& T, c
   }
   __syncthreads();
   // y direction: slopes, y faces j = y0..y0+wy on columns x0-1..x0+wx, and E_c
-  stage_slopes<1, LIM>(L, W, D);
+  stage_slopes<1, LIM>(L, W, D, cp, I.gam);
   __syncthreads();
   {
     FastDiv dx2;
@@ -664,7 +682,7 @@ __device__ __forceinline__ void copy_tile(const Inst& I, const Tile& T, int pari
 
 template <int TXM, int TYM, int RS, int LIM>
 __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
-                                                   int parity) {
+                                                   int parity, int cp) {
   constexpr int RING = 2;
   extern __shared__ double smem[];
   __shared__ double red[8];
@@ -695,7 +713,7 @@ __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ inst
   __syncthreads();
   unsigned e = 0;
   SmemCells W{sW, S, S.cells()};
-  stage_fluxes_plm<LIM, RS>(I, T, L, W, I.bs, sFX, sFY, sEC, sD, e);
+  stage_fluxes_plm<LIM, RS>(I, T, L, W, I.bs, sFX, sFY, sEC, sD, cp, e);
   __syncthreads();
   stage_emf(L, sFX, sFY, sEC, sEE);
   __syncthreads();

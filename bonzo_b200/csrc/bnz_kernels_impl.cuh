@@ -56,13 +56,16 @@ int launch_flux_rs(const StepArgs& a, const double* w, const double* bf, const p
   int nb = nblocks(boxn(b), T);
   switch (a.rsolver) {
     case dev::RS_HLLD:
-      plain::k_flux<AX, ORDER, dev::RS_HLLD><<<nb, T, 0, a.stream>>>(a.g, w, bf, a.flx[AX], b, a.limiter, a.err);
+      plain::k_flux<AX, ORDER, dev::RS_HLLD><<<nb, T, 0, a.stream>>>(a.g, w, bf, a.flx[AX], b, a.limiter, a.charact_proj,
+                                                                  a.err);
       break;
     case dev::RS_HLLT:
-      plain::k_flux<AX, ORDER, dev::RS_HLLT><<<nb, T, 0, a.stream>>>(a.g, w, bf, a.flx[AX], b, a.limiter, a.err);
+      plain::k_flux<AX, ORDER, dev::RS_HLLT><<<nb, T, 0, a.stream>>>(a.g, w, bf, a.flx[AX], b, a.limiter, a.charact_proj,
+                                                                  a.err);
       break;
     default:
-      plain::k_flux<AX, ORDER, dev::RS_HLL><<<nb, T, 0, a.stream>>>(a.g, w, bf, a.flx[AX], b, a.limiter, a.err);
+      plain::k_flux<AX, ORDER, dev::RS_HLL><<<nb, T, 0, a.stream>>>(a.g, w, bf, a.flx[AX], b, a.limiter, a.charact_proj,
+                                                                  a.err);
       break;
   }
   return 1;
@@ -284,7 +287,7 @@ void launch_corr(const FusedLaunch& f, int parity) {
     cudaFuncSetAttribute(fused::k_corr2d<TX, TY, RS, LIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB);
     attrs = true;
   }
-  fused::k_corr2d<TX, TY, RS, LIM><<<f.ntB, 256, smB, f.stream>>>(f.insts, f.tilesB, parity);
+  fused::k_corr2d<TX, TY, RS, LIM><<<f.ntB, 256, smB, f.stream>>>(f.insts, f.tilesB, parity, f.charact_proj);
 }
 
 template <int TX, int TY, int RS, int STAGED>

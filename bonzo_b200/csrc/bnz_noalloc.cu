@@ -152,7 +152,6 @@ int bnz_vl2_step_noalloc(const bnz_grid_desc* g, const bnz_method_desc* m, const
   if (g->dims != 2 || g->Nz != 1) return fail(BNZ_ERR_UNSUPPORTED, "the no-alloc step covers 2D grids");
   if (m->reconstr != BNZ_RCN_LINEAR) return fail(BNZ_ERR_UNSUPPORTED, "the no-alloc step uses PLM (reconstr linear)");
   if (m->kappa0 != 0.) return fail(BNZ_ERR_UNSUPPORTED, "the no-alloc step has no conduction (kappa0 = 0)");
-  if (m->charact_proj) return fail(BNZ_ERR_UNSUPPORTED, "charact_proj=1 is not supported by the device kernels");
   if (m->rsolver != BNZ_RS_HLL && m->rsolver != BNZ_RS_HLLD && m->rsolver != BNZ_RS_HLLT)
     return fail(BNZ_ERR_ARG, "rsolver must be hll, hlld or hllt");
   if (m->limiter < 0 || m->limiter > 2) return fail(BNZ_ERR_ARG, "limiter must be vl, mc or mm");
@@ -271,6 +270,7 @@ int bnz_vl2_step_noalloc(const bnz_grid_desc* g, const bnz_method_desc* m, const
   f.ntB = ntB;
   f.rsolver = m->rsolver;
   f.limiter = m->limiter;
+  f.charact_proj = m->charact_proj;
   f.variant = 0;
   f.cour = m->cour;
   f.dt_mode = FDT_EXPLICIT;

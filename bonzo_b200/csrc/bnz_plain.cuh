@@ -29,6 +29,13 @@ __device__ __forceinline__ double half_slope_rt(int lim, double wm, double wc, d
   return half_slope<LIM_VL>(wm, wc, wp);
 }
 
+__device__ __forceinline__ void half_slopes_char_rt(int lim, const double* wm, const double* wc, const double* wp,
+                                                    double gam, double* d) {
+  if (lim == LIM_MC) half_slopes_char<LIM_MC>(wm, wc, wp, gam, d);
+  else if (lim == LIM_MM) half_slopes_char<LIM_MM>(wm, wc, wp, gam, d);
+  else half_slopes_char<LIM_VL>(wm, wc, wp, gam, d);
+}
+
 struct Box {
   int3 lo, hi;
   __device__ __forceinline__ long long size() const {
@@ -51,26 +58,42 @@ struct Box {
 // godunov.pyx:84-207: Godunov flux on the AX faces of `box` (face index along
 // AX = the cell on its right).  ORDER 0: donor cell (reconstr_c.c:8-22);
 // ORDER 1: PLM (reconstr_c.c:29-91).  Normal field from the face array.
+// cp = 1 (charact_proj): the slopes are limited in characteristic variables.
 template <int AX, int ORDER, int RS>
 __global__ void __launch_bounds__(128) k_flux(GridDev g, const double* __restrict__ w,
                                               const double* __restrict__ bf, double* __restrict__ F,
-                                              Box box, int lim, unsigned* err) {
+                                              Box box, int lim, int cp, unsigned* err) {
   const long long s = AX == 0 ? 1LL : AX == 1 ? (long long)g.nx : (long long)g.nx * g.ny;
   unsigned e = 0;
   BOX_LOOP(box, i, j, k) {
     const long long c = cidx(g, i, j, k);
     double wL[NM], wR[NM];
+    if (ORDER == 1 && cp) {
+      double c4[4][NM], dl[NM], dr[NM];
 #pragma unroll
-    for (int n = 0; n < NM; ++n) {
-      if (n == BX) continue;
-      const double* a = w + perm<AX>(n) * g.sv + c;
-      if (ORDER == 0) {
-        wL[n] = a[-s];
-        wR[n] = a[0];
-      } else {
-        double wm2 = a[-2 * s], wm1 = a[-s], w0 = a[0], wp1 = a[s];
-        wL[n] = wm1 + half_slope_rt(lim, wm2, wm1, w0);
-        wR[n] = w0 - half_slope_rt(lim, wm1, w0, wp1);
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int n = 0; n < NM; ++n) c4[q][n] = w[perm<AX>(n) * g.sv + c + (q - 2) * s];
+      half_slopes_char_rt(lim, c4[0], c4[1], c4[2], g.gam, dl);
+      half_slopes_char_rt(lim, c4[1], c4[2], c4[3], g.gam, dr);
+#pragma unroll
+      for (int n = 0; n < NM; ++n) {
+        wL[n] = c4[1][n] + dl[n];
+        wR[n] = c4[2][n] - dr[n];
+      }
+    } else {
+#pragma unroll
+      for (int n = 0; n < NM; ++n) {
+        if (n == BX) continue;
+        const double* a = w + perm<AX>(n) * g.sv + c;
+        if (ORDER == 0) {
+          wL[n] = a[-s];
+          wR[n] = a[0];
+        } else {
+          double wm2 = a[-2 * s], wm1 = a[-s], w0 = a[0], wp1 = a[s];
+          wL[n] = wm1 + half_slope_rt(lim, wm2, wm1, w0);
+          wR[n] = w0 - half_slope_rt(lim, wm1, w0, wp1);
+        }
       }
     }
     const double bx = bf[AX * g.sv + c];

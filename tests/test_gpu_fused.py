@@ -18,7 +18,8 @@ CASES = [("vortex", 32, {}), ("vortex", 40, dict(rsolver="hll")), ("vortex", 32,
          ("vortex_pert", 48, dict(limiter="mc")), ("vortex_pert", 36, dict(limiter="mm")),
          ("blast", 40, {}), ("blast", 33, dict(outflow_face_aware=0)), ("blast_reflect", 34, {}),
          ("mixed_bc", 37, {}), ("cond2d", 32, {}), ("vortex", 8, {}), ("vortex", 70, {}),
-         ("vortex", 65, {}), ("blast", 97, {})]
+         ("vortex", 65, {}), ("blast", 97, {}), ("vortex_pert", 40, dict(limiter="mc", charact_proj=1)),
+         ("blast", 36, dict(charact_proj=1)), ("blast_reflect", 30, dict(limiter="mm", charact_proj=1))]
 
 
 @pytest.mark.parametrize("case,n,kw", CASES)

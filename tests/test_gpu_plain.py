@@ -38,7 +38,9 @@ CASES = [("vortex", 32, {}), ("vortex", 32, dict(rsolver="hll")), ("vortex", 32,
          ("vortex_pert", 32, dict(limiter="mc")), ("vortex_pert", 32, dict(limiter="mm")),
          ("vortex", 32, dict(reconstr="const")), ("blast", 32, {}), ("blast", 32, dict(outflow_face_aware=0)),
          ("turb3d", 12, {}), ("cond2d", 32, {}), ("cond2d", 32, dict(thcond_type="iso")),
-         ("cond3d", 12, {}), ("cond3d", 12, dict(sat_hfe=1)), ("wave1d", 64, {})]
+         ("cond3d", 12, {}), ("cond3d", 12, dict(sat_hfe=1)), ("wave1d", 64, {}),
+         ("vortex_pert", 32, dict(limiter="mc", charact_proj=1)), ("blast", 32, dict(charact_proj=1)),
+         ("turb3d", 12, dict(charact_proj=1))]
 
 
 @pytest.mark.parametrize("case,n,kw", CASES)
