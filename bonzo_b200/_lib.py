@@ -53,7 +53,9 @@ class MethodDesc(C.Structure):
                 ("charact_proj", C.c_int),
                 ("kappa0", C.c_double), ("thcond_type", C.c_int), ("sat_hfe", C.c_int),
                 ("cour_diff", C.c_double), ("fixdt", C.c_int), ("dt_fixed", C.c_double),
-                ("outflow_face_aware", C.c_int), ("exact_fp", C.c_int), ("path", C.c_int)]
+                ("outflow_face_aware", C.c_int), ("exact_fp", C.c_int), ("path", C.c_int),
+                ("grav", C.c_double * 3), ("drive_f0", C.c_double), ("drive_tau", C.c_double),
+                ("drive_nmod", C.c_int), ("drive_seed", C.c_uint64)]
 
 
 _dp = C.POINTER(C.c_double)
@@ -140,7 +142,8 @@ def grid_desc(Nx, Ny=1, Nz=1, dims=2, lmin=(0., 0., 0.), lmax=(1., 1., 1.),
 
 def method_desc(gam=5. / 3, cour=0.4, rsolver="hlld", reconstr="linear", limiter="vl",
                 charact_proj=0, kappa0=0.0, thcond_type="aniso", sat_hfe=0, cour_diff=0.5,
-                fixdt=False, dt_fixed=0.0, outflow_face_aware=1, exact_fp=False, path="plain"):
+                fixdt=False, dt_fixed=0.0, outflow_face_aware=1, exact_fp=False, path="plain",
+                grav=(0.0, 0.0, 0.0), drive_f0=0.0, drive_tau=1.0, drive_nmod=1, drive_seed=0):
     m = MethodDesc()
     m.gam, m.cour = gam, cour
     m.rsolver = RS[rsolver] if isinstance(rsolver, str) else rsolver
@@ -151,6 +154,9 @@ def method_desc(gam=5. / 3, cour=0.4, rsolver="hlld", reconstr="linear", limiter
     m.fixdt, m.dt_fixed = int(bool(fixdt)), dt_fixed
     m.outflow_face_aware, m.exact_fp = outflow_face_aware, int(bool(exact_fp))
     m.path = PATH[path] if isinstance(path, str) else path
+    for a in range(3):
+        m.grav[a] = grav[a]
+    m.drive_f0, m.drive_tau, m.drive_nmod, m.drive_seed = drive_f0, drive_tau, drive_nmod, drive_seed
     return m
 
 

@@ -39,6 +39,10 @@ struct StepArgs {
   int bc[3][2];
   int face_aware;
   cudaStream_t stream;
+  // source terms: constant gravity and the driving force field (3 x Ntot)
+  double grav[3];
+  const double* fdriv;
+  int src;  // any source term on
 };
 
 // Device time-step record used by graph-captured stepping.
@@ -71,6 +75,9 @@ struct FusedInst {
   double* bs;          // predictor face field
   DtState* ds;
   unsigned* err;       // the instance's sticky error word
+  double grav[3];      // source terms (gravity, driving force field or null)
+  const double* fdriv;
+  int src;
 };
 
 // A tile of cells [x0, x0+wx) x [y0, y0+wy) (array coordinates) of one instance.
@@ -134,6 +141,16 @@ struct AdjStep {
   int rsolver, limiter;
   int fold_in;        // fold G1 first (it may carry ghost entries)
   cudaStream_t stream;
+};
+
+// Turbulence driving (turb_driv.pyx): force field, this step's mode
+// amplitudes (device), base wavenumbers 2 pi / L and the OU parameters.
+struct DriveArgs {
+  double* fdriv;
+  const double* modes;
+  int nmod;
+  double k0[3];
+  double tau, f0;
 };
 
 // Conduction scratch (thcond_elec.pyx DiffScratch).

@@ -107,7 +107,66 @@ StepArgs step_args(bnz_ctx* c) {
   }
   a.face_aware = c->md.outflow_face_aware;
   a.stream = c->stream;
+  for (int d = 0; d < 3; ++d) a.grav[d] = c->md.grav[d];
+  a.fdriv = c->fdriv;
+  a.src = src_on(c->md) ? 1 : 0;
   return a;
+}
+
+bool drive_on(const bnz_method_desc& m) { return m.drive_f0 != 0.; }
+bool src_on(const bnz_method_desc& m) {
+  return m.grav[0] != 0. || m.grav[1] != 0. || m.grav[2] != 0. || drive_on(m);
+}
+
+// splitmix64 (Steele, Lea & Flood 2014): the uniform stream behind the driving
+// amplitudes (the reference's rand() / RAND_MAX has no reproducible seed)
+unsigned long long splitmix64(unsigned long long& st) {
+  unsigned long long z = (st += 0x9E3779B97F4A7C15ULL);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+// turb_driv.pyx:50-79: Gaussian amplitudes c1, c2 of every mode (zero when a
+// wavenumber component is zero), Box-Muller from two uniforms
+void drive_modes(int nmod, unsigned long long& rng, double* c1, double* c2) {
+  const int nmod2 = 2 * nmod + 1;
+  for (int p = 0; p < nmod2; ++p)
+    for (int q = 0; q < nmod2; ++q)
+      for (int r = 0; r < nmod2; ++r)
+        for (int n = 0; n < 3; ++n) {
+          double norm;
+          if (p == nmod || q == nmod || r == nmod) norm = 0.;
+          else norm = 1. / ((double)((p - nmod) * (p - nmod)) + (double)((q - nmod) * (q - nmod)) +
+                            (double)((r - nmod) * (r - nmod)));
+          double w1 = (double)(splitmix64(rng) >> 11) * (1.0 / 9007199254740992.0);
+          double w2 = (double)(splitmix64(rng) >> 11) * (1.0 / 9007199254740992.0);
+          if (w1 == 0.) w1 = 1e-20;
+          const int m = n + 3 * (r + nmod2 * q + nmod2 * nmod2 * p);
+          c1[m] = norm * std::sqrt(-2 * std::log(w1)) * std::cos(2 * M_PI * w2);
+          c2[m] = norm * std::sqrt(-2 * std::log(w1)) * std::sin(2 * M_PI * w2);
+        }
+}
+
+// update_physics (integrator.pyx:176-194): new amplitudes, then the force
+// field advanced with the dt the device record holds for this step
+int drive_advance(bnz_ctx* c) {
+  const int nmod = c->md.drive_nmod, nmod2 = 2 * nmod + 1;
+  const size_t nc = 3 * (size_t)nmod2 * nmod2 * nmod2;
+  CKC(cudaEventSynchronize(c->ev_modes));  // the staging buffer's previous copy is done
+  drive_modes(nmod, c->rng, c->h_modes, c->h_modes + nc);
+  CKC(cudaMemcpyAsync(c->d_modes, c->h_modes, 2 * nc * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CKC(cudaEventRecord(c->ev_modes, c->stream));
+  DriveArgs d;
+  d.fdriv = c->fdriv;
+  d.modes = c->d_modes;
+  d.nmod = nmod;
+  for (int a = 0; a < 3; ++a) d.k0[a] = 2. * M_PI / (c->gd.lmax[a] - c->gd.lmin[a]);
+  d.tau = c->md.drive_tau;
+  d.f0 = c->md.drive_f0;
+  c->launches += c->L->drive(step_args(c), d, &c->d_ds->dt);
+  CKC(cudaGetLastError());
+  return BNZ_OK;
 }
 
 void free_all(bnz_ctx* c) {
@@ -126,6 +185,12 @@ void free_all(bnz_ctx* c) {
   c->wnext = c->bnext = c->dscr = c->d_sts = nullptr;
   for (int d = 0; d < 3; ++d) c->flx[d] = nullptr;
   c->wbuf[0] = c->wbuf[1] = c->bbuf[0] = c->bbuf[1] = nullptr;
+  if (c->fdriv) cudaFree(c->fdriv);
+  if (c->d_modes) cudaFree(c->d_modes);
+  if (c->h_modes) cudaFreeHost(c->h_modes);
+  if (c->ev_modes) cudaEventDestroy(c->ev_modes);
+  c->fdriv = c->d_modes = c->h_modes = nullptr;
+  c->ev_modes = nullptr;
   if (c->d_err) cudaFree(c->d_err);
   if (c->d_ds) cudaFree(c->d_ds);
   if (c->d_inst) cudaFree(c->d_inst);
@@ -202,6 +267,9 @@ FusedInst make_inst(const bnz_ctx* c) {
   I.bs = c->bfld_s;
   I.ds = c->d_ds;
   I.err = c->d_err;
+  for (int d = 0; d < 3; ++d) I.grav[d] = c->md.grav[d];
+  I.fdriv = c->fdriv;
+  I.src = src_on(c->md) ? 1 : 0;
   return I;
 }
 
@@ -264,6 +332,10 @@ int validate(const bnz_grid_desc* g, const bnz_method_desc* m, std::string& why)
   if (m->reconstr != BNZ_RCN_CONST && m->reconstr != BNZ_RCN_LINEAR) return why = "reconstr must be const or linear", 0;
   if (m->limiter < 0 || m->limiter > 2) return why = "limiter must be vl, mc or mm", 0;
   if (m->charact_proj != 0 && m->charact_proj != 1) return why = "charact_proj must be 0 or 1", 0;
+  if (m->drive_f0 != 0.) {
+    if (!(m->drive_tau > 0.)) return why = "tau must be positive when the driving is on", 0;
+    if (m->drive_nmod < 1 || m->drive_nmod > 8) return why = "nmod must be 1..8", 0;
+  }
   if (m->kappa0 < 0.) return why = "kappa0 must be >= 0", 0;
   if (m->kappa0 > 0. && !(m->cour_diff > 0.)) return why = "cour_diff must be positive", 0;
   if (m->path != BNZ_PATH_FUSED && m->path != BNZ_PATH_PLAIN) return why = "path must be fused or plain", 0;
@@ -418,6 +490,16 @@ int bnz_create(const bnz_grid_desc* gd, const bnz_method_desc* md, bnz_ctx** out
     c->da.sat = md->sat_hfe;
     c->da.cour_diff = md->cour_diff;
     e = cudaMemsetAsync(c->dscr, 0, 8 * c->ncell * sizeof(double), c->stream);
+  }
+  if (drive_on(*md)) {
+    const int nmod2 = 2 * md->drive_nmod + 1;
+    const size_t nm = 2 * 3 * (size_t)nmod2 * nmod2 * nmod2;
+    ALLOC(c->fdriv, 3 * c->ncell * sizeof(double));
+    ALLOC(c->d_modes, nm * sizeof(double));
+    e = cudaMallocHost((void**)&c->h_modes, nm * sizeof(double));
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_modes, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->fdriv, 0, 3 * c->ncell * sizeof(double), c->stream);
+    c->rng = md->drive_seed;
   }
   e = cudaMalloc((void**)&c->d_err, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_ds, sizeof(DtState));
@@ -631,6 +713,12 @@ void set_parity(bnz_ctx* c, int p) {
 // vanleer.pyx:101-163 with dt already in d_ds->dt.  dt_mode selects how the
 // fused path obtains dt (explicit host value, device CFL, or FIXDT).
 int step_impl(bnz_ctx* c, double dt_host, int dt_mode) {
+  if (drive_on(c->md)) {
+    // the force needs this step's dt in the device record before the stages
+    if (dt_mode != FDT_EXPLICIT) return fail(c, BNZ_ERR_UNSUPPORTED, "driving needs the host dt of each step");
+    int rc = drive_advance(c);
+    if (rc) return rc;
+  }
   StepArgs a = step_args(c);
   const double* dtp = &c->d_ds->dt;
   if (c->md.path == BNZ_PATH_PLAIN) {
@@ -753,6 +841,12 @@ int bnz_sync(bnz_ctx* c) {
 
 
 int bnz_advance_graph(bnz_ctx* c, double tmax, int nsteps) {
+  if (c && c->prim && drive_on(c->md)) {
+    // new driving amplitudes every step come from the host: step without a graph
+    double t;
+    long st;
+    return bnz_advance(c, tmax, nsteps, &t, &st);
+  }
   if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
   if (nsteps < 0) return fail(c, BNZ_ERR_ARG, "nsteps must be >= 0");
   if (c->md.kappa0 > 0.)
@@ -967,6 +1061,7 @@ int bnz_batch_create(const bnz_grid_desc* grids, int n, const bnz_method_desc* m
   b->md = *md;
   b->md.path = BNZ_PATH_FUSED;
   if (md->kappa0 > 0.) return bfail(b, BNZ_ERR_UNSUPPORTED, "batches advance the hyperbolic step only (kappa0 = 0)");
+  if (drive_on(*md)) return bfail(b, BNZ_ERR_UNSUPPORTED, "batches do not drive turbulence (drive_f0 = 0)");
   cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bfail(b, BNZ_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
   std::vector<FusedInst> insts;

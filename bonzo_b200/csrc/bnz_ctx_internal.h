@@ -68,6 +68,13 @@ struct bnz_ctx {
   bool own_stream = true;
   struct bnz_adj* adj = nullptr;  // adjoint tape (bnz_adjoint.cu), created on first use
   struct bnz_io* io = nullptr;    // history / snapshot resources (bnz_io.cu), created on first use
+  // turbulence driving: force field, this step's mode amplitudes (device and
+  // pinned staging, guarded by an event), the amplitude stream's state
+  double* fdriv = nullptr;
+  double* d_modes = nullptr;
+  double* h_modes = nullptr;
+  cudaEvent_t ev_modes = nullptr;
+  unsigned long long rng = 0;
 };
 
 namespace bnzi {
@@ -83,6 +90,9 @@ int ensure_ghosts(bnz_ctx* c);
 int refresh_cds(bnz_ctx* c);
 // vanleer.pyx:101-163 with dt taken as dt_mode says (FDT_EXPLICIT: d_ds->dt)
 int step_impl(bnz_ctx* c, double dt_host, int dt_mode = FDT_EXPLICIT);
+// sources on: gravity or driving
+bool src_on(const bnz_method_desc& m);
+bool drive_on(const bnz_method_desc& m);
 // release the adjoint tape (bnz_adjoint.cu) and the output resources (bnz_io.cu)
 void adj_free(bnz_ctx* c);
 void io_free(bnz_ctx* c);

@@ -515,10 +515,11 @@ struct CellOut {
   double bxl, bxr, byb, byt, bz;
 };
 
+// w0: the stage input's prim at the cell (rho, vx, vy, vz used by the source terms)
 __device__ __forceinline__ void stage_cell(const Inst& I, const Layout& L, const Tile& T, int ci, int cj,
-                                           const double* un, double bxl0, double bxr0, double byb0, double byt0,
-                                           double bz0, const double* sFX, const double* sFY, const double* sEE,
-                                           double dt, CellOut& o) {
+                                           const double* un, const double* w0, double bxl0, double bxr0,
+                                           double byb0, double byt0, double bz0, const double* sFX,
+                                           const double* sFY, const double* sEE, double dt, CellOut& o) {
   const int i = T.x0 + ci, j = T.y0 + cj;
   const double dx = I.dlf[0][i], dy = I.dlf[1][j], dz = I.dlf2;
 #if BNZ_FAST_MATH
@@ -569,6 +570,18 @@ __device__ __forceinline__ void stage_cell(const Inst& I, const Layout& L, const
   u[BX] = ((I.lv[0][i] - I.lf[0][i]) * o.bxl + (I.lf[0][i + 1] - I.lv[0][i]) * o.bxr) * I.dlf_inv[0][i];
   u[BY] = ((I.lv[1][j] - I.lf[1][j]) * o.byb + (I.lf[1][j + 1] - I.lv[1][j]) * o.byt) * I.dlf_inv[1][j];
   u[BZ] = bz;
+  if (I.src) {
+    // integrator.pyx:132-170 add_source_terms (bnz_source.cuh)
+    double f[3];
+    if (I.fdriv) {
+      const long long c = (long long)j * I.nx + i;
+      f[0] = I.fdriv[c];
+      f[1] = I.fdriv[I.sv + c];
+      f[2] = I.fdriv[2 * I.sv + c];
+    }
+    const bool grav = I.grav[0] != 0. || I.grav[1] != 0. || I.grav[2] != 0.;
+    srcterm::apply(u, w0[RHO], w0[VX], w0[VY], w0[VZ], I.grav, grav, I.fdriv ? f : nullptr, dt);
+  }
   cons2prim(o.w, u, I.gam);
 }
 
@@ -650,7 +663,7 @@ __global__ void __launch_bounds__(256, 2) k_pred2d(const Inst* __restrict__ inst
     double byt0 = load_face<1>(I, b, i, j + 1, mx, my, interior);
     double bz0 = load_face<2>(I, b, i, j, mx, my, interior);
     CellOut o;
-    stage_cell(I, L, T, ci, cj, un, bxl0, bxr0, byb0, byt0, bz0, sFX, sFY, sEE, dt, o);
+    stage_cell(I, L, T, ci, cj, un, wn, bxl0, bxr0, byb0, byt0, bz0, sFX, sFY, sEE, dt, o);
     const long long c = (long long)j * I.nx + i;
 #pragma unroll
     for (int n = 0; n < NM; ++n) I.ws[n * I.sv + c] = o.w[n];
@@ -741,8 +754,10 @@ __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ inst
     double byb0 = load_face<1>(I, b, i, j, mx, my, !edge);
     double byt0 = load_face<1>(I, b, i, j + 1, mx, my, !edge);
     double bz0 = b[2 * I.sv + c];
+    // the corrector's sources use the half-step state ws (vanleer.pyx:143)
+    const double w0[4] = {W.get(RHO, i, j), W.get(VX, i, j), W.get(VY, i, j), W.get(VZ, i, j)};
     CellOut o;
-    stage_cell(I, L, T, ci, cj, un, bxl0, bxr0, byb0, byt0, bz0, sFX, sFY, sEE, dt, o);
+    stage_cell(I, L, T, ci, cj, un, w0, bxl0, bxr0, byb0, byt0, bz0, sFX, sFY, sEE, dt, o);
     e |= plain::check_prim(o.w);
 #pragma unroll
     for (int n = 0; n < NM; ++n) w1[n * I.sv + c] = o.w[n];

@@ -15,6 +15,7 @@ namespace BNZ_NS {
 #include "bnz_plain.cuh"
 #include "bnz_bc_dt.cuh"
 #include "bnz_diffusion.cuh"
+#include "bnz_source.cuh"
 #include "bnz_fused.cuh"
 #include "bnz_adjoint_math.h"
 #include "bnz_adjoint.cuh"
@@ -144,12 +145,33 @@ int integrate_field(const StepArgs& a, double* u1, double* b1, const double* w0,
 // Launchers exported to the host context (declared in bnz_launch.h).
 // ---------------------------------------------------------------------------
 
+// integrator.pyx:132-170 add_source_terms on the stage's update range
+int source(const StepArgs& a, double* u1, const double* w0, int order, const double* dtp, double fac) {
+  int l[6];
+  integr_lims(a.g, order, l);
+  plain::Box b = mkbox(l[0], l[1], l[2], l[3], l[4], l[5]);
+  srcterm::k_source<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(a.g, u1, w0, a.fdriv, a.grav[0], a.grav[1],
+                                                                  a.grav[2], b, dtp, fac);
+  return 1;
+}
+
+// integrator.pyx:176-194 update_physics: the driving force on the predictor range
+int drive(const StepArgs& a, const DriveArgs& d, const double* dtp) {
+  int l[6];
+  integr_lims(a.g, 0, l);
+  plain::Box b = mkbox(l[0], l[1], l[2], l[3], l[4], l[5]);
+  srcterm::k_drive<<<nblocks(boxn(b), 128), 128, 0, a.stream>>>(a.g, d.fdriv, d.modes, d.nmod, d.k0[0], d.k0[1],
+                                                                 d.k0[2], d.tau, d.f0, b, dtp);
+  return 1;
+}
+
 int plain_predictor_corrector(const StepArgs& a, const double* dtp) {
   const GridDev& g = a.g;
   int l[6];
   // predictor (vanleer.pyx:104-120): order 0, dt/2, Us from U, W, B
   int nl = integrate_hydro(a, a.cons_s, a.cons, a.prim, a.bfld, 0, dtp, 0.5);
   nl += integrate_field(a, a.cons_s, a.bfld_s, a.prim, a.bfld, 0, dtp, 0.5);
+  if (a.src) nl += source(a, a.cons_s, a.prim, 0, dtp, 0.5);
   integr_lims(g, 0, l);
   {
     plain::Box b = mkbox(l[0], l[1], l[2], l[3], l[4], l[5]);
@@ -159,6 +181,7 @@ int plain_predictor_corrector(const StepArgs& a, const double* dtp) {
   int order = a.reconstr_order;
   nl += integrate_hydro(a, a.cons, a.cons, a.prim, a.bfld_s, order, dtp, 1.0);
   nl += integrate_field(a, a.cons, a.bfld, a.prim, a.bfld, order, dtp, 1.0);
+  if (a.src) nl += source(a, a.cons, a.prim, order, dtp, 1.0);
   integr_lims(g, order, l);
   {
     plain::Box b = mkbox(l[0], l[1], l[2], l[3], l[4], l[5]);

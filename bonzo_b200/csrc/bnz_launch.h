@@ -20,6 +20,8 @@ struct Launchers {
   int (*diff_operator)(const StepArgs&, const DiffArgs&);
   int (*diff_stage_update)(const StepArgs&, const DiffArgs&, int first, const double* coef, const double* dtp);
   int (*adj_step)(const FusedInst& I, const AdjStep& s);
+  int (*source)(const StepArgs&, double* u1, const double* w0, int order, const double* dtp, double fac);
+  int (*drive)(const StepArgs&, const DriveArgs&, const double* dtp);
 };
 
 #define BNZ_DECLARE_LAUNCHERS(NS)                                                                     \
@@ -39,6 +41,8 @@ struct Launchers {
   int diff_operator(const StepArgs&, const DiffArgs&);                                               \
   int diff_stage_update(const StepArgs&, const DiffArgs&, int first, const double* coef, const double* dtp); \
   int adj_step(const FusedInst& I, const AdjStep& s);                                                \
+  int source(const StepArgs&, double* u1, const double* w0, int order, const double* dtp, double fac);  \
+  int drive(const StepArgs&, const DriveArgs&, const double* dtp);                                    \
   extern const Launchers table;                                                                       \
   }
 
@@ -50,4 +54,5 @@ BNZ_DECLARE_LAUNCHERS(fast)
                                NS::fused_cds, NS::apply_bc,                                           \
                                NS::prim2cons_all, NS::cons2prim_all, NS::interp_bc_active,           \
                                NS::new_dt, NS::set_dt, NS::time_advance, NS::diff_dt_max,            \
-                               NS::diff_operator, NS::diff_stage_update, NS::adj_step};
+                               NS::diff_operator, NS::diff_stage_update, NS::adj_step, NS::source,    \
+                               NS::drive};

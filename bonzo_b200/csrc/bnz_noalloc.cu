@@ -152,6 +152,7 @@ int bnz_vl2_step_noalloc(const bnz_grid_desc* g, const bnz_method_desc* m, const
   if (g->dims != 2 || g->Nz != 1) return fail(BNZ_ERR_UNSUPPORTED, "the no-alloc step covers 2D grids");
   if (m->reconstr != BNZ_RCN_LINEAR) return fail(BNZ_ERR_UNSUPPORTED, "the no-alloc step uses PLM (reconstr linear)");
   if (m->kappa0 != 0.) return fail(BNZ_ERR_UNSUPPORTED, "the no-alloc step has no conduction (kappa0 = 0)");
+  if (m->drive_f0 != 0.) return fail(BNZ_ERR_UNSUPPORTED, "the no-alloc step has no turbulence driving (drive_f0 = 0)");
   if (m->rsolver != BNZ_RS_HLL && m->rsolver != BNZ_RS_HLLD && m->rsolver != BNZ_RS_HLLT)
     return fail(BNZ_ERR_ARG, "rsolver must be hll, hlld or hllt");
   if (m->limiter < 0 || m->limiter > 2) return fail(BNZ_ERR_ARG, "limiter must be vl, mc or mm");
@@ -240,6 +241,8 @@ int bnz_vl2_step_noalloc(const bnz_grid_desc* g, const bnz_method_desc* m, const
   I.bs = reinterpret_cast<double*>(base + o_bs);
   I.ds = reinterpret_cast<DtState*>(base + o_ds);
   I.err = reinterpret_cast<unsigned*>(base + o_err);
+  for (int d = 0; d < 3; ++d) I.grav[d] = m->grav[d];
+  I.src = (m->grav[0] != 0. || m->grav[1] != 0. || m->grav[2] != 0.) ? 1 : 0;
   // the time record and the error word start from zero on every call: the
   // array keeps whatever the previous call left in it
   DtState ds;

@@ -98,6 +98,15 @@ class BnzIntegr:
         self.thcond_type = rp("physics", "elec_thcond_type", "s")
         self.sat_hfe = rp("physics", "sat_hfe", "i")
         self.tmax = rp("computation", "tmax", "f")
+        # source terms (gravity.pyx:17-19 gx/gy/gz; the shipped config's g0 is
+        # "constant negative g along Y"; turb_driv.pyx:27-29 f0/tau/nmod)
+        rd = lambda s_, k, t, d: cfg.read_param(s_, k, t, usr_dir, d)
+        g0 = rd("physics", "g0", "f", 0.0)
+        self.grav = (rd("physics", "gx", "f", 0.0), rd("physics", "gy", "f", -g0), rd("physics", "gz", "f", 0.0))
+        self.drive_f0 = rd("physics", "f0", "f", 0.0)
+        self.drive_tau = rd("physics", "tau", "f", 1.0) or 1.0
+        self.drive_nmod = rd("physics", "nmod", "i", 1)
+        self.drive_seed = rd("physics", "driving_seed", "i", 0)
         self.time = 0.0
         self.step = 0
         self.dt = 0.0
@@ -105,7 +114,9 @@ class BnzIntegr:
     def method(self):
         return dict(gam=self.gam, cour=self.cour, rsolver=self.rsolver, reconstr=self.reconstr,
                     limiter=self.limiter, charact_proj=self.char_proj, kappa0=self.kappa0,
-                    thcond_type=self.thcond_type, sat_hfe=self.sat_hfe, cour_diff=self.cour_diff)
+                    thcond_type=self.thcond_type, sat_hfe=self.sat_hfe, cour_diff=self.cour_diff,
+                    grav=self.grav, drive_f0=self.drive_f0, drive_tau=self.drive_tau,
+                    drive_nmod=self.drive_nmod, drive_seed=self.drive_seed)
 
 
 class BnzIO:

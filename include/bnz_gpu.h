@@ -65,7 +65,13 @@ typedef struct {
  * limiter is the added `limiter: vl|mc|mm` key (the reference hard-wires vl).
  * outflow_face_aware keeps the CT-updated outer face under outflow BCs.
  * exact_fp selects kernels built without multiply-add contraction, which
- * reproduce the CPU reference bit for bit; path selects fused or plain kernels. */
+ * reproduce the CPU reference bit for bit; path selects fused or plain kernels.
+ * Source terms (src/srcterms, applied in both stages by
+ * integrator.pyx:132-170 add_source_terms): grav = the [physics] gx, gy, gz
+ * constant acceleration (gravity.pyx:17-19); drive_f0 / drive_tau / drive_nmod
+ * = the [physics] f0, tau, nmod of the solenoidal driving force
+ * (turb_driv.pyx:27-29), whose random mode amplitudes come from a splitmix64
+ * stream seeded with drive_seed.  Zero f0 and grav switch them off. */
 typedef struct {
   double gam, cour;
   int rsolver, reconstr, limiter, charact_proj;
@@ -77,6 +83,10 @@ typedef struct {
   int outflow_face_aware;
   int exact_fp;
   int path;
+  double grav[3];
+  double drive_f0, drive_tau;
+  int drive_nmod;
+  unsigned long long drive_seed;
 } bnz_method_desc;
 
 typedef struct bnz_ctx bnz_ctx;

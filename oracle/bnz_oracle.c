@@ -837,6 +837,9 @@ struct orc_sim {
   /* per-thread scratch rows (integrator.pyx:367-370) */
   real *rowstore;
   size_t rowlen;
+  /* turbulence driving (turb_driv.pyx): force field and mode-amplitude stream */
+  real *fdriv;
+  uint64_t rng;
 };
 
 #define IDX(s, n, k, j, i) ((((size_t)(n) * (s)->nz + (k)) * (s)->ny + (j)) * (s)->nx + (i))
@@ -994,6 +997,8 @@ orc_sim *orc_create(const orc_params *pin) {
   /* per thread: wl, wl_, wr (NM rows each) + 8*NM reconstruction rows */
   s->rowlen = (size_t)nmax + 4;
   s->rowstore = (real *)calloc((size_t)s->nthr * 11 * NM * s->rowlen, sizeof(real));
+  s->fdriv = (real *)calloc(3 * s->ncell, sizeof(real));
+  s->rng = s->p.drive_seed;
   return s;
 }
 
@@ -1012,6 +1017,7 @@ void orc_destroy(orc_sim *s) {
   free(s->temp); free(s->kappa); free(s->fxd); free(s->fyd); free(s->fzd);
   free(s->pres0); free(s->presm1); free(s->dtemp); free(s->dtemp0);
   free(s->rowstore);
+  free(s->fdriv);
   free(s);
 }
 
@@ -1964,10 +1970,158 @@ void orc_diffuse(orc_sim *s, real dt) {
 }
 
 /* vanleer.pyx:101-163 (one VL2 step without the dt selection). */
+/* ======================================================================
+ * Source terms (src/srcterms) and the driving force
+ * ====================================================================== */
+
+/* Uniform doubles in [0, 1) from splitmix64 (Steele, Lea & Flood 2014); the
+ * reference draws rand()/RAND_MAX (util.pyx:45-47) with an unset seed, which
+ * cannot be reproduced, so the stream is seeded from drive_seed instead. */
+static uint64_t o_splitmix64(uint64_t *st) {
+  uint64_t z = (*st += 0x9E3779B97F4A7C15ULL);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+static real o_rand01(uint64_t *st) { return (real)(o_splitmix64(st) >> 11) * (1.0 / 9007199254740992.0); }
+
+/* turb_driv.pyx:34-86: Gaussian mode amplitudes c1, c2 (3 per mode), zero for
+ * modes with a zero wavenumber component, Box-Muller from two uniforms. */
+static void o_drive_modes(orc_sim *s, real *c1, real *c2) {
+  const int nmod = s->p.drive_nmod, nmod2 = 2 * nmod + 1;
+  for (int p = 0; p < nmod2; ++p)
+    for (int q = 0; q < nmod2; ++q)
+      for (int r = 0; r < nmod2; ++r)
+        for (int n = 0; n < 3; ++n) {
+          real norm;
+          if (p == nmod || q == nmod || r == nmod) norm = 0.;
+          else norm = 1. / (SQR(p - nmod) + SQR(q - nmod) + SQR(r - nmod));
+          real w1 = o_rand01(&s->rng);
+          real w2 = o_rand01(&s->rng);
+          if (w1 == 0.) w1 = 1e-20;
+          int m = n + 3 * (r + nmod2 * q + nmod2 * nmod2 * p);
+          c1[m] = norm * sqrt(-2 * log(w1)) * cos(2 * M_PI * w2);
+          c2[m] = norm * sqrt(-2 * log(w1)) * sin(2 * M_PI * w2);
+        }
+}
+
+/* turb_driv_c.c:5-95: the force at one cell, the curl of the mode sum with
+ * the phases advanced by trigonometric recurrences, then the OU update. */
+static void o_drive_cell(real *f, const real *c1, const real *c2, real x, real y, real z, real kx0, real ky0,
+                         real kz0, real dt_tau, real f1, int nmod) {
+  int nmod2 = 2 * nmod + 1;
+  real nmodf = (real)nmod;
+  real th = -nmodf * (kx0 * x + ky0 * y + kz0 * z);
+  real cn = cos(th), sn = sin(th);
+  real cnx = cos(kx0 * x), cny = cos(ky0 * y), cnz = cos(kz0 * z);
+  real snx = sin(kx0 * x), sny = sin(ky0 * y), snz = sin(kz0 * z);
+  real gx = 0., gy = 0., gz = 0.;
+  real tz = -nmodf * kz0;
+  for (int p = 0; p < nmod2; ++p) {
+    real ty = -nmodf * ky0;
+    real cn00 = cn, sn00 = sn;
+    for (int q = 0; q < nmod2; ++q) {
+      real tx = -nmodf * kx0;
+      real cn0 = cn, sn0 = sn;
+      for (int r = 0; r < nmod2; ++r) {
+        int m = 3 * (r + nmod2 * q + nmod2 * nmod2 * p);
+        real ax = -c1[m] * sn + c2[m] * cn;
+        real ay = -c1[m + 1] * sn + c2[m + 1] * cn;
+        real az = -c1[m + 2] * sn + c2[m + 2] * cn;
+        gx += ty * az - tz * ay;
+        gy += -tx * az + tz * ax;
+        gz += tx * ay - ty * ax;
+        tx += kx0;
+        real cn_ = cn;
+        cn = cn_ * cnx - sn * snx;
+        sn = sn * cnx + cn_ * snx;
+      }
+      ty += ky0;
+      cn = cn0;
+      sn = sn0;
+      real cn_ = cn;
+      cn = cn_ * cny - sn * sny;
+      sn = sn * cny + cn_ * sny;
+    }
+    tz += kz0;
+    cn = cn00;
+    sn = sn00;
+    real cn_ = cn;
+    cn = cn_ * cnz - sn * snz;
+    sn = sn * cnz + cn_ * snz;
+  }
+  f[0] = (1. - dt_tau) * f[0] + f1 * gx;
+  f[1] = (1. - dt_tau) * f[1] + f1 * gy;
+  f[2] = (1. - dt_tau) * f[2] + f1 * gz;
+}
+
+/* integrator.pyx:176-194 update_physics -> turb_driv.pyx:34-107, on the
+ * predictor's update range (the reference passes lims before setting them;
+ * the predictor range is where apply_driv_force reads the force). */
+static void o_advance_driving(orc_sim *s, real dt) {
+  if (s->p.drive_f0 == 0.) return;
+  const int nmod2 = 2 * s->p.drive_nmod + 1;
+  const size_t nc = 3 * (size_t)nmod2 * nmod2 * nmod2;
+  real *c1 = (real *)malloc(nc * sizeof(real)), *c2 = (real *)malloc(nc * sizeof(real));
+  o_drive_modes(s, c1, c2);
+  real dt_tau = dt / s->p.drive_tau;
+  real f1 = sqrt(dt_tau) * s->p.drive_f0;
+  orc_coord *gc = &s->gc;
+  real kx0 = 2. * M_PI / (gc->lmax[0] - gc->lmin[0]);
+  real ky0 = 2. * M_PI / (gc->lmax[1] - gc->lmin[1]);
+  real kz0 = 2. * M_PI / (gc->lmax[2] - gc->lmin[2]);
+  int l[6];
+  integr_lims(s, 0, l);
+  for (int k = l[4]; k <= l[5]; ++k)
+    for (int j = l[2]; j <= l[3]; ++j)
+      for (int i = l[0]; i <= l[1]; ++i) {
+        size_t c = C3(s, k, j, i);
+        real f[3] = {s->fdriv[c], s->fdriv[s->ncell + c], s->fdriv[2 * s->ncell + c]};
+        o_drive_cell(f, c1, c2, gc->lv[0][i], gc->lv[1][j], gc->lv[2][k], kx0, ky0, kz0, dt_tau, f1,
+                     s->p.drive_nmod);
+        s->fdriv[c] = f[0];
+        s->fdriv[s->ncell + c] = f[1];
+        s->fdriv[2 * s->ncell + c] = f[2];
+      }
+  free(c1);
+  free(c2);
+}
+
+/* integrator.pyx:132-170 add_source_terms on the stage's update range:
+ * constant gravity (gravity.pyx:54-69; its u0 is not in scope there, the
+ * stage input w0 gives the density and momentum), then the driving force
+ * (turb_driv.pyx:109-124). */
+static void o_add_source_terms(orc_sim *s, real *u1, const real *w0, int order, real dt) {
+  const real *g = s->p.grav;
+  const int grav = g[0] != 0. || g[1] != 0. || g[2] != 0.;
+  const int drive = s->p.drive_f0 != 0.;
+  if (!grav && !drive) return;
+  int l[6];
+  integr_lims(s, order, l);
+  for (int k = l[4]; k <= l[5]; ++k)
+    for (int j = l[2]; j <= l[3]; ++j)
+      for (int i = l[0]; i <= l[1]; ++i) {
+        size_t c = C3(s, k, j, i);
+        const size_t sv = s->ncell;
+        real rho = w0[c], vx = w0[VX * sv + c], vy = w0[VY * sv + c], vz = w0[VZ * sv + c];
+        if (grav) {
+          for (int n = 0; n < 3; ++n) u1[(MX + n) * sv + c] += rho * g[n] * dt;
+          u1[EN * sv + c] += dt * ((rho * vx) * g[0] + (rho * vy) * g[1] + (rho * vz) * g[2]);
+        }
+        if (drive) {
+          const real *f = s->fdriv;
+          for (int n = 0; n < 3; ++n) u1[(MX + n) * sv + c] = u1[(MX + n) * sv + c] + dt * f[n * sv + c];
+          u1[EN * sv + c] = u1[EN * sv + c] + (dt * (f[c] * vx + f[sv + c] * vy + f[2 * sv + c] * vz));
+        }
+      }
+}
+
 void orc_vl2_step(orc_sim *s, real dtfull) {
   real *w = s->prim, *u = s->cons, *ws = s->prim, *us = s->cons_s;
   real *b = s->bfld, *bs = s->bfld_s;
   int lims[6];
+  /* vanleer.pyx:98 update_physics: the driving force at t_n+1/2 */
+  o_advance_driving(s, dtfull);
   /* predictor */
   int order = 0;
   real dt = 0.5 * dtfull;
@@ -1978,6 +2132,7 @@ void orc_vl2_step(orc_sim *s, real dtfull) {
 #else
   (void)bs;
 #endif
+  o_add_source_terms(s, us, w, order, dt);
   cons2prim_range(s, ws, us, lims);
   /* corrector */
   order = s->reconstr_order;
@@ -1987,6 +2142,7 @@ void orc_vl2_step(orc_sim *s, real dtfull) {
 #if ORC_MFIELD
   integrate_field(s, u, b, ws, b, order, dt);
 #endif
+  o_add_source_terms(s, u, ws, order, dt);
   cons2prim_range(s, s->prim, s->cons, lims);
   orc_diffuse(s, dt);
   orc_apply_bc(s, (1u << ORC_NVAR) - 1u);

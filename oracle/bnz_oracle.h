@@ -122,6 +122,12 @@ typedef struct {
   int outflow_face_aware; /* 1: outflow keeps the CT-updated outer face */
   int nthreads;         /* OpenMP threads (0: library default) */
   int rows_parallel;    /* 0: reference threading (prange over k / j only) */
+  /* source terms (src/srcterms): constant gravity and turbulence driving */
+  real grav[3];         /* gx, gy, gz (gravity.pyx:17-19) */
+  real drive_f0;        /* driving amplitude f0 (turb_driv.pyx:27), 0 = off */
+  real drive_tau;       /* correlation time tau */
+  int drive_nmod;       /* modes per axis nmod */
+  uint64_t drive_seed;  /* seed of the mode amplitudes (splitmix64) */
 } orc_params;
 
 typedef struct orc_sim orc_sim;

@@ -39,6 +39,8 @@ class OrcParams(C.Structure):
         ("fixdt", C.c_int), ("dt_fixed", C.c_double),
         ("outflow_face_aware", C.c_int),
         ("nthreads", C.c_int), ("rows_parallel", C.c_int),
+        ("grav", C.c_double * 3), ("drive_f0", C.c_double), ("drive_tau", C.c_double),
+        ("drive_nmod", C.c_int), ("drive_seed", C.c_uint64),
     ]
 
 
@@ -235,7 +237,7 @@ class OracleSim:
                  reconstr="linear", limiter="vl", charact_proj=0, kappa0=0.,
                  thcond_type="aniso", sat_hfe=0, cour_diff=0.5, fixdt=False, dt_fixed=0.,
                  outflow_face_aware=1, nthreads=0, rows_parallel=1, use_ref_kernels=False,
-                 hydro=False):
+                 hydro=False, grav=(0., 0., 0.), drive_f0=0., drive_tau=1., drive_nmod=1, drive_seed=0):
         self.hydro = hydro
         self.L = _lib(hydro)
         p = OrcParams()
@@ -252,6 +254,9 @@ class OracleSim:
         p.fixdt, p.dt_fixed = int(bool(fixdt)), dt_fixed
         p.outflow_face_aware = outflow_face_aware
         p.nthreads, p.rows_parallel = nthreads, rows_parallel
+        for a in range(3):
+            p.grav[a] = grav[a]
+        p.drive_f0, p.drive_tau, p.drive_nmod, p.drive_seed = drive_f0, drive_tau, drive_nmod, drive_seed
         self.params = p
         self.h = self.L.orc_create(C.byref(p))
         self.nmode = 6 if hydro else NMODE

@@ -17,6 +17,7 @@ def test_grid_and_integrator_from_config(tmp_path):
     assert g.prim.shape == (9, 1, 30, 30) and g.bfld.shape == (3, 1, 30, 30)
     assert i.rsolver == "hlld" and i.limiter == "mc" and abs(i.gam - 5. / 3) < 1e-15
     assert i.tmax == 0.02 and i.time == 0.0 and i.step == 0
+    assert i.grav == (0.0, 0.0, 0.0) and i.drive_f0 == 0.0 and i.drive_nmod == 1
 
 
 def test_io_header_and_schedule(tmp_path):
