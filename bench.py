@@ -41,7 +41,7 @@ CORR_BYTES_PER_ZONE = 288
 # DRAM bytes per active zone of one corrector launch (dram__bytes_read.sum +
 # dram__bytes_write.sum), from the ncu capture summarised in
 # profiles/k_corr2d_blast_batch.md (16-instance capture, scaled per zone).
-CORR_TRAFFIC_PER_ZONE = 267.7
+CORR_TRAFFIC_PER_ZONE = 269.1
 
 
 def parse():
@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
     ap.add_argument("--adjoint-only", action="store_true", help="print only the adjoint/forward measurement")
+    ap.add_argument("--configs", action="store_true",
+                    help="also time the 3D configurations (256^3 turbulence, 384^3 conduction; slow set-up)")
     return ap.parse_args()
 
 
@@ -413,6 +415,54 @@ def run_adjoint(warmup=1, reps=3):
                    "backward (incl. the loss); median of %d after %d warm-up" % (reps, warmup)}
 
 
+def run_configs(steps=3):
+    """The 3D configurations on the plain path, seeded synthetic initial states:
+    256^3 decaying turbulence (rms Mach 1, beta 1, VL2+PLM+HLLD+CT, CFL 0.3) and
+    384^3 field-aligned conduction (kappa_par 0.01, RKL2 super-time-stepping
+    interleaved with VL2+HLLD+CT).  Each: one warm-up step, then `steps` timed
+    steps with CUDA events; conduction steps count hyperbolic zone-updates and
+    RKL2 zone-stages (96 B each) separately."""
+    import torch
+    from bonzo_b200 import problems as P
+    from bonzo_b200._lib import Context
+    out = {}
+    stream = torch.cuda.Stream()
+    for name, n, kw, gen in (
+            ("turbulence_256^3", 256, dict(cour=0.3), lambda gc: P.turbulence3d(gc, seed=0)),
+            ("conduction_384^3", 384, dict(cour=0.4, kappa0=0.01, thcond_type="aniso"),
+             lambda gc: P.conduction3d(gc, seed=0))):
+        gc = P.make_grid(n, n, n, dims=3, bc=0)
+        prim, bfld = gen(gc)
+        c = Context(Nx=n, Ny=n, Nz=n, dims=3, bc=((0, 0), (0, 0), (0, 0)), gam=5. / 3, rsolver="hlld",
+                    limiter="vl", path="plain", **kw)
+        c.set_stream(stream.cuda_stream)
+        c.set_state(prim, bfld)
+        c.init()
+        del prim, bfld
+        c.advance(1e30, 1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        nsts = 0
+        e0.record(stream)
+        for _ in range(steps):
+            c.advance(1e30, 1)
+            nsts += c.last_nsts() if kw.get("kappa0", 0.0) > 0 else 0
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        zones = n ** 3
+        # algorithmic bytes: 192 per zone-update plus 96 per RKL2 zone-stage
+        byts = BYTES_PER_ZONE * zones + 96 * zones * nsts / steps
+        rec = {"ms_per_step": round(ms, 3), "mzone_updates_per_s": round(zones / (ms * 1e-3) / 1e6, 1),
+               "rkl2_stages_per_step": round(nsts / steps, 2),
+               "hbm_gbs_algorithmic": round(byts / (ms * 1e-3) / 1e9, 1)}
+        c.check()
+        out[name] = rec
+        c.close()
+        torch.cuda.empty_cache()
+    return out
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -452,6 +502,8 @@ def main():
     line = run_ours(args, rank, world, dist)
     if rank == 0 and not args.no_adjoint:
         line["adjoint"] = run_adjoint()
+    if rank == 0 and args.configs:
+        line["configs_3d"] = run_configs()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         batch = build_batch(args.instances, args.seed)
         cb = run_cpu_reference(batch, steps=2, warmup=1)

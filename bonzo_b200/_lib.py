@@ -25,7 +25,7 @@ PATH = {"fused": 0, "plain": 1}
 EXPORTS = [
     "bnz_create", "bnz_destroy", "bnz_last_error", "bnz_shape", "bnz_set_state", "bnz_init",
     "bnz_get_state", "bnz_apply_bc", "bnz_new_dt", "bnz_vl2_step", "bnz_diffuse", "bnz_advance",
-    "bnz_get_time", "bnz_set_time", "bnz_check", "bnz_sync", "bnz_advance_graph",
+    "bnz_get_time", "bnz_last_nsts", "bnz_set_time", "bnz_check", "bnz_sync", "bnz_advance_graph",
     "bnz_device_state", "bnz_stream", "bnz_set_stream", "bnz_launch_count",
     "bnz_batch_create", "bnz_batch_destroy", "bnz_batch_last_error", "bnz_batch_size",
     "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_advance_timed", "bnz_batch_set_stream", "bnz_batch_launch_count",
@@ -87,6 +87,7 @@ def load():
     L.bnz_advance.argtypes = [vp, C.c_double, C.c_int, _dp, C.POINTER(C.c_long)]
     L.bnz_get_time.argtypes = [vp, _dp, C.POINTER(C.c_long), _dp]
     L.bnz_set_time.argtypes = [vp, C.c_double, C.c_long]
+    L.bnz_last_nsts.argtypes = [vp, C.POINTER(C.c_int)]
     L.bnz_check.argtypes = [vp, C.POINTER(C.c_uint32)]
     L.bnz_sync.argtypes = [vp]
     L.bnz_advance_graph.argtypes = [vp, C.c_double, C.c_int]
@@ -254,6 +255,11 @@ class Context:
         s = C.c_long()
         self._ck(self.L.bnz_advance(self.h, tmax, max_steps, C.byref(t), C.byref(s)))
         return t.value, s.value
+
+    def last_nsts(self):
+        n = C.c_int()
+        self._ck(self.L.bnz_last_nsts(self.h, C.byref(n)))
+        return n.value
 
     def set_time(self, time, step):
         self._ck(self.L.bnz_set_time(self.h, float(time), int(step)))

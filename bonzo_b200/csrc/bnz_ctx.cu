@@ -802,6 +802,12 @@ int bnz_advance(bnz_ctx* c, double tmax, int max_steps, double* time_out, long* 
   return BNZ_OK;
 }
 
+int bnz_last_nsts(const bnz_ctx* c, int* nsts) {
+  if (!c || !nsts) return BNZ_ERR_ARG;
+  *nsts = c->last_nsts;
+  return BNZ_OK;
+}
+
 int bnz_get_time(bnz_ctx* c, double* t, long* s, double* last_dt) {
   if (!c) return BNZ_ERR_ARG;
   int rc = sync_time(c);

@@ -128,6 +128,8 @@ int bnz_diffuse(bnz_ctx* ctx, double dt, int* nsts_out);
  * on the device; the host reads back 8 bytes per step to stop the loop. */
 int bnz_advance(bnz_ctx* ctx, double tmax, int max_steps, double* time_out, long* step_out);
 int bnz_get_time(bnz_ctx* ctx, double* time_out, long* step_out, double* last_dt);
+/* RKL2 stages of the last conduction call (diffusion.pyx:217-224 get_nsts). */
+int bnz_last_nsts(const bnz_ctx* ctx, int* nsts);
 int bnz_set_time(bnz_ctx* ctx, double time, long step);
 /* Sticky device error word (bits: 1 rho<=0, 2 p<=0, 4 NaN, 8 unordered
  * Riemann fan, 16 timeout); cleared by the call. */
