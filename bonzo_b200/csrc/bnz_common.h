@@ -94,9 +94,12 @@ struct FusedTile {
 struct FusedVariant {
   int tx, ty, staged;
 };
-constexpr int FUSED_NVARIANT = 5;
+// 15 x 14 tiles give 256 x faces and 255 y faces per interior tile: each flux
+// phase of a 256-thread block is one full round (32 x 8 leaves 40% of the
+// threads idle in the second round of each phase).
+constexpr int FUSED_NVARIANT = 6;
 constexpr FusedVariant FUSED_VARIANTS[FUSED_NVARIANT] = {
-    {32, 8, 0}, {32, 8, 1}, {16, 16, 0}, {16, 16, 1}, {64, 4, 0}};
+    {32, 8, 0}, {32, 8, 1}, {16, 16, 0}, {16, 16, 1}, {15, 14, 0}, {15, 14, 1}};
 
 // dt modes of the fused step
 enum { FDT_CFL = 0, FDT_EXPLICIT = 1, FDT_FIXED = 2 };

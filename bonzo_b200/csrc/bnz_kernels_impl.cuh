@@ -341,7 +341,8 @@ void launch_pred_corr(const FusedLaunch& f, int parity) {
       case 1: launch_variant<32, 8, RS, 1>(f, parity); return;
       case 2: launch_variant<16, 16, RS, 0>(f, parity); return;
       case 3: launch_variant<16, 16, RS, 1>(f, parity); return;
-      case 4: launch_variant<64, 4, RS, 0>(f, parity); return;
+      case 4: launch_variant<15, 14, RS, 0>(f, parity); return;
+      case 5: launch_variant<15, 14, RS, 1>(f, parity); return;
       default: break;
     }
   }

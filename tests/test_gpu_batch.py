@@ -92,7 +92,7 @@ def test_batch_rejects_3d_and_conduction():
         Batch([dict(Nx=8, Ny=8, Nz=1, dims=2)], kappa0=0.1, **METHOD)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 def test_every_variant_bitwise_vs_oracle(variant):
     """Every autotuner candidate (tile shape, predictor staging) gives the same bits."""
     from bonzo_b200._lib import Batch
