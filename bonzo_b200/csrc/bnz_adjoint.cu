@@ -152,6 +152,7 @@ int reverse_step(bnz_ctx* c, double dt, int p, int q, double* gw, double* gb, do
   a.rsolver = c->md.rsolver;
   a.limiter = c->md.limiter;
   a.fold_in = fold_in ? 1 : 0;
+  a.clear_bsb = fold_in ? 1 : 0;  // the first reverse step of a pass
   a.stream = st;
   c->launches += c->L->adj_step(make_inst(c), a);
   CKC(cudaGetLastError());

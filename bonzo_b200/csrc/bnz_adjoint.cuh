@@ -110,6 +110,28 @@ __device__ __forceinline__ double bz_total(const Inst& I, const StageArgs& a, in
 
 // --- S1: per updated cell, ubar = VJP of cons2prim at the output; the
 // prim2cons of w^n that forms u^n gets ubar's hydro part --------------------
+__device__ __forceinline__ void cells_body(const Inst& I, const StageArgs& a, int i, int j, const double* g) {
+  const long long c = cidx(I, i, j);
+  double wo[NM], ub[NM];
+#pragma unroll
+  for (int v = 0; v < NM; ++v) {
+    wo[v] = a.Wout[v * I.sv + c];
+    ub[v] = 0.;
+  }
+  adj::vjp_cons2prim(wo, g, I.gam, ub);
+#pragma unroll
+  for (int v = 0; v < NM; ++v) a.Ub[v * I.sv + c] = ub[v];
+  // u^n = prim2cons(w^n); its B entries are replaced by the face averages
+  double wn[NM], wb[NM];
+  read_cell(I, a.Wn, i, j, a.order == 0, wn);
+  ub[BX] = ub[BY] = ub[BZ] = 0.;
+#pragma unroll
+  for (int v = 0; v < NM; ++v) wb[v] = 0.;
+  adj::vjp_prim2cons(wn, ub, I.gam, wb);
+#pragma unroll
+  for (int v = 0; v < NM; ++v) a.Vw[v * I.sv + c] += wb[v];
+}
+
 __global__ void k_cells(const Inst I, const StageArgs a) {
   const Box R = a.R;
   const int w = R.ib - R.ia + 1;
@@ -117,25 +139,10 @@ __global__ void k_cells(const Inst I, const StageArgs a) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int i = R.ia + (int)(t % w), j = R.ja + (int)(t / w);
     const long long c = cidx(I, i, j);
-    double wo[NM], g[NM], ub[NM];
+    double g[NM];
 #pragma unroll
-    for (int v = 0; v < NM; ++v) {
-      wo[v] = a.Wout[v * I.sv + c];
-      g[v] = a.Gw[v * I.sv + c];
-      ub[v] = 0.;
-    }
-    adj::vjp_cons2prim(wo, g, I.gam, ub);
-#pragma unroll
-    for (int v = 0; v < NM; ++v) a.Ub[v * I.sv + c] = ub[v];
-    // u^n = prim2cons(w^n); its B entries are replaced by the face averages
-    double wn[NM], wb[NM];
-    read_cell(I, a.Wn, i, j, a.order == 0, wn);
-    ub[BX] = ub[BY] = ub[BZ] = 0.;
-#pragma unroll
-    for (int v = 0; v < NM; ++v) wb[v] = 0.;
-    adj::vjp_prim2cons(wn, ub, I.gam, wb);
-#pragma unroll
-    for (int v = 0; v < NM; ++v) a.Vw[v * I.sv + c] += wb[v];
+    for (int v = 0; v < NM; ++v) g[v] = a.Gw[v * I.sv + c];
+    cells_body(I, a, i, j, g);
   }
 }
 
@@ -295,7 +302,10 @@ __global__ void __launch_bounds__(128, BNZ_ADJ_FACE_MINB) k_faces(const Inst I, 
 
 // --- S4: per cell read by the stage, the sum over the faces that read it,
 // plus the cell-centred EMF's cotangent ---------------------------------------
-__global__ void k_gather(const Inst I, const StageArgs a) {
+// With `next` (the corrector's gather, whose cells are exactly the
+// predictor's update range), the predictor's S1 runs on the gathered
+// cotangent at once instead of a separate launch reading it back.
+__global__ void k_gather(const Inst I, const StageArgs a, const StageArgs next, int fuse_next) {
   const Box R = a.R;
   const int h = a.order == 0 ? 1 : 2;
   const int gi0 = R.ia - h, gi1 = R.ib + h, gj0 = R.ja - h, gj1 = R.jb + h;
@@ -348,15 +358,18 @@ __global__ void k_gather(const Inst I, const StageArgs a) {
       }
     }
     const long long c = cidx(I, i, j);
+    // z face (cell-centred in 2D): bz = bz^n + ... on updated cells (reads Ub
+    // of this cell before the fused predictor S1 below overwrites it)
+    if (in(R, i, j)) a.Vb[2 * I.sv + c] += bz_total(I, a, i, j);
     if (a.order == 0) {
 #pragma unroll
       for (int v = 0; v < NM; ++v) a.Vw[v * I.sv + c] += acc[v];
+    } else if (fuse_next) {
+      cells_body(I, next, i, j, acc);
     } else {
 #pragma unroll
       for (int v = 0; v < NM; ++v) a.Wsrc_b[v * I.sv + c] = acc[v];
     }
-    // z face (cell-centred in 2D): bz = bz^n + ... on updated cells
-    if (in(R, i, j)) a.Vb[2 * I.sv + c] += bz_total(I, a, i, j);
   }
 }
 
@@ -382,31 +395,47 @@ __device__ __forceinline__ int fold_src(const Inst& I, int f, int a, double& sig
   return s;
 }
 
-// One thread per (field, line, remappable position): the ghosts on both sides
-// and the first active position (a zeroed reflecting face).  Sources are never
-// ghosts, so moving a ghost's value into its source with an atomic add is
-// exact whatever the order (several ghosts share a source under outflow).
-template <int AX>
-__global__ void k_fold(const Inst I, double* Vw, double* Vb) {
-  const int nline = AX == 0 ? I.ny : I.nx;
-  const int len = AX == 0 ? I.nx : I.ny;
-  const int a1 = I.ng, a2 = I.ng + I.N[AX] - 1;
-  const int nrem = a1 + 1 + (len - a2 - 1);  // positions 0..a1 and a2+1..len-1
-  const int total = 12 * nline * nrem;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-    const int r = t % nrem, fl = t / nrem;
-    const int f = fl / nline, line = fl % nline;
-    const int p = r <= a1 ? r : a2 + 1 + (r - a1 - 1);
+// One thread per remappable position of each field.  A ghost's value moves
+// into its source with an atomic add, which is exact whatever the order
+// (several ghosts share a source under outflow).
+// Both axes at once: every position whose x or y index can be remapped (the
+// ghost bands and the first active row / column) sends its value to the source
+// both axis maps give it, with the product of the signs; a zeroed face on
+// either axis drops it.  Sources are never remappable positions, so one pass
+// of atomic adds is exact.
+__global__ void k_fold2d(const Inst I, double* Vw, double* Vb) {
+  const int a1x = I.ng, a2x = I.ng + I.N[0] - 1, a1y = I.ng, a2y = I.ng + I.N[1] - 1;
+  const int rx = a1x + 1 + (I.nx - a2x - 1), ry = a1y + 1 + (I.ny - a2y - 1);
+  // band positions: rows j in the y band (all i), then rows outside it with i in the x band
+  const long long nband_y = (long long)ry * I.nx;
+  const long long nband_x = (long long)(I.ny - ry) * rx;
+  const long long per_field = nband_y + nband_x;
+  const long long total = 12 * per_field;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int f = (int)(t / per_field);
+    const long long u = t - (long long)f * per_field;
+    int i, j;
+    if (u < nband_y) {
+      const int r = (int)(u / I.nx);
+      i = (int)(u - (long long)r * I.nx);
+      j = r <= a1y ? r : a2y + 1 + (r - a1y - 1);
+    } else {
+      const long long v = u - nband_y;
+      const int r = (int)(v / rx), q = (int)(v - (long long)r * rx);
+      j = a1y + 1 + r;  // rows a1y+1 .. a2y
+      i = q <= a1x ? q : a2x + 1 + (q - a1x - 1);
+    }
+    double sx, sy;
+    bool zx, zy;
+    const int si = fold_src<0>(I, f, i, sx, zx);
+    const int sj = fold_src<1>(I, f, j, sy, zy);
+    if (si == i && sj == j && !zx && !zy) continue;
     double* V = f < NM ? Vw + (long long)f * I.sv : Vb + (long long)(f - NM) * I.sv;
-    const long long st = AX == 0 ? 1 : I.nx;
-    const long long base = AX == 0 ? (long long)line * I.nx : line;
-    double sign;
-    bool zero;
-    const int s = fold_src<AX>(I, f, p, sign, zero);
-    if (s == p && !zero) continue;
-    const double v = V[base + p * st];
-    V[base + p * st] = 0.;
-    if (!zero && v != 0.) atomicAdd(&V[base + s * st], sign * v);
+    const long long p = cidx(I, i, j);
+    const double val = V[p];
+    V[p] = 0.;
+    if (!zx && !zy && val != 0.) atomicAdd(&V[cidx(I, si, sj)], sx * sy * val);
   }
 }
 

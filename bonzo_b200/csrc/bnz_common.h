@@ -143,6 +143,7 @@ struct AdjStep {
   double dt;
   int rsolver, limiter;
   int fold_in;        // fold G1 first (it may carry ghost entries)
+  int clear_bsb;      // zero Bsb first (the first reverse step of a pass)
   cudaStream_t stream;
 };
 

@@ -377,8 +377,11 @@ int fused_cds(const FusedLaunch& f, int parity) {
 // --- discrete adjoint of one fused 2D step ------------------------------
 
 namespace {
+// One reverse stage: S1 cells (unless the previous stage's gather ran it),
+// S2 corners, S3 faces, S4 gather (optionally with the next stage's S1).
 template <int RS>
-void adj_stage(const FusedInst& I, const adjk::StageArgs& a, int lim, cudaStream_t st) {
+void adj_stage(const FusedInst& I, const adjk::StageArgs& a, int lim, cudaStream_t st, bool run_cells,
+               const adjk::StageArgs* next) {
   const int T = 128;
   const adjk::Box& R = a.R;
   const long long ncell = (long long)(R.ib - R.ia + 1) * (R.jb - R.ja + 1);
@@ -387,17 +390,17 @@ void adj_stage(const FusedInst& I, const adjk::StageArgs& a, int lim, cudaStream
   const long long nfy = (long long)(R.ib - R.ia + 3) * (R.jb - R.ja + 2);
   const int h = a.order == 0 ? 1 : 2;
   const long long ngat = (long long)(R.ib - R.ia + 1 + 2 * h) * (R.jb - R.ja + 1 + 2 * h);
-  adjk::k_cells<<<nblocks(ncell, T), T, 0, st>>>(I, a);
+  if (run_cells) adjk::k_cells<<<nblocks(ncell, T), T, 0, st>>>(I, a);
   adjk::k_corners<<<nblocks(ncorner, T), T, 0, st>>>(I, a);
   if (a.order == 0) adjk::k_faces<0, RS><<<nblocks(nfx + nfy, T), T, 0, st>>>(I, a, lim);
   else adjk::k_faces<1, RS><<<nblocks(nfx + nfy, T), T, 0, st>>>(I, a, lim);
-  adjk::k_gather<<<nblocks(ngat, T), T, 0, st>>>(I, a);
+  adjk::k_gather<<<nblocks(ngat, T), T, 0, st>>>(I, a, next ? *next : a, next ? 1 : 0);
 }
 
 void adj_fold(const FusedInst& I, double* Vw, double* Vb, cudaStream_t st) {
   const long long rx = I.nx - I.N[0] + 1, ry = I.ny - I.N[1] + 1;  // remappable positions per line
-  adjk::k_fold<0><<<nblocks(12LL * I.ny * rx, 128), 128, 0, st>>>(I, Vw, Vb);
-  adjk::k_fold<1><<<nblocks(12LL * I.nx * ry, 128), 128, 0, st>>>(I, Vw, Vb);
+  const long long n = 12LL * (ry * I.nx + (I.ny - ry) * rx);
+  adjk::k_fold2d<<<nblocks(n, 128), 128, 0, st>>>(I, Vw, Vb);
 }
 }  // namespace
 
@@ -405,10 +408,12 @@ int adj_step(const FusedInst& I, const AdjStep& s) {
   int launches = 0;
   cudaMemsetAsync(s.Vw, 0, 9 * (size_t)I.sv * sizeof(double), s.stream);
   cudaMemsetAsync(s.Vb, 0, 3 * (size_t)I.sv * sizeof(double), s.stream);
-  cudaMemsetAsync(s.Bsb, 0, 3 * (size_t)I.sv * sizeof(double), s.stream);
+  // Bsb: the corrector's faces set the same range every step and the rest stays
+  // zero, so the caller clears it once per reverse pass (clear_bsb on the first)
+  if (s.clear_bsb) cudaMemsetAsync(s.Bsb, 0, 3 * (size_t)I.sv * sizeof(double), s.stream);
   if (s.fold_in) {
     adj_fold(I, s.G1w, s.G1b, s.stream);
-    launches += 2;
+    launches += 1;
   }
   adjk::StageArgs a;
   // corrector: order 1 on the active cells
@@ -428,23 +433,29 @@ int adj_step(const FusedInst& I, const AdjStep& s) {
   a.Ub = s.Ub;
   a.Eb = s.Eb;
   a.Q = s.Q;
-  if (s.rsolver == dev::RS_HLLD) adj_stage<dev::RS_HLLD>(I, a, s.limiter, s.stream);
-  else adj_stage<dev::RS_HLL>(I, a, s.limiter, s.stream);
   // predictor: order 0 on cells 1..Ntot-2, half step
-  a.order = 0;
-  a.dt = 0.5 * s.dt;
-  a.R = {1, I.nx - 2, 1, I.ny - 2};
-  a.Wout = s.Ws;
-  a.Gw = s.Wsb;
-  a.Gb = s.Bsb;
-  a.Wsrc = s.Wn;
-  a.Bsrc = s.Bn;
-  a.Wsrc_b = s.Vw;
-  a.Bsrc_b = s.Vb;
-  if (s.rsolver == dev::RS_HLLD) adj_stage<dev::RS_HLLD>(I, a, s.limiter, s.stream);
-  else adj_stage<dev::RS_HLL>(I, a, s.limiter, s.stream);
+  adjk::StageArgs a0 = a;
+  a0.order = 0;
+  a0.dt = 0.5 * s.dt;
+  a0.R = {1, I.nx - 2, 1, I.ny - 2};
+  a0.Wout = s.Ws;
+  a0.Gw = s.Wsb;
+  a0.Gb = s.Bsb;
+  a0.Wsrc = s.Wn;
+  a0.Bsrc = s.Bn;
+  a0.Wsrc_b = s.Vw;
+  a0.Bsrc_b = s.Vb;
+  // the corrector's gather covers exactly the predictor's range: it runs the
+  // predictor's S1 on the spot
+  if (s.rsolver == dev::RS_HLLD) {
+    adj_stage<dev::RS_HLLD>(I, a, s.limiter, s.stream, true, &a0);
+    adj_stage<dev::RS_HLLD>(I, a0, s.limiter, s.stream, false, nullptr);
+  } else {
+    adj_stage<dev::RS_HLL>(I, a, s.limiter, s.stream, true, &a0);
+    adj_stage<dev::RS_HLL>(I, a0, s.limiter, s.stream, false, nullptr);
+  }
   adj_fold(I, s.Vw, s.Vb, s.stream);
-  return launches + 2 * 4 + 2;  // two stages of four kernels, the output fold
+  return launches + 4 + 3 + 1;  // corrector stage, predictor stage without S1, the output fold
 }
 
 }  // namespace BNZ_NS
