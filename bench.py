@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-instance comparison")
     ap.add_argument("--instances", type=int, default=64)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
     ap.add_argument("--adjoint-only", action="store_true", help="print only the adjoint/forward measurement")
@@ -298,12 +298,24 @@ def run_ours(args, rank, world, dist):
     h2d = sum(P.nbytes + B.nbytes for P, B in host)
     ke = max(1, args.e2e_steps)
 
-    def e2e_step():
-        for c, (P, B) in zip(ctxs, host):
-            c.set_state(P, B)
-        step()
-        for c, (P, B) in zip(ctxs, host):
-            c.get_state_into(P, None, B)
+    if args.path == "batch":
+        prims, bflds = [P for P, _ in host], [B for _, B in host]
+        e2e_how = ("bnz_batch_step_host: every instance's state copied in from pinned host buffers, one "
+                   "batch step, ghosts filled, copied back out; copies in, steps and copies out of 32 "
+                   "groups of instances overlap on three streams")
+
+        def e2e_step():
+            eng.step_host(prims, bflds, 1e30, 1)
+        e2e_step()  # untimed: creates the copy streams and events
+    else:
+        e2e_how = "bnz_set_state of every instance, one step each, bnz_get_state of every instance, pinned host buffers"
+
+        def e2e_step():
+            for c, (P, B) in zip(ctxs, host):
+                c.set_state(P, B)
+            step()
+            for c, (P, B) in zip(ctxs, host):
+                c.get_state_into(P, None, B)
 
     ems = _timed(stream, e2e_step, ke, dist)
     e2e = zones_all * ke / (ems * 1e-3) / 1e6
@@ -353,8 +365,7 @@ def run_ours(args, rank, world, dist):
                    "autotune": tune},
         "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(h2d),
-                "how": "bnz_set_state of every instance, one batch step, bnz_get_state of every "
-                       "instance, pinned host buffers"},
+                "how": e2e_how},
         "gpu_launches": int(launches),
         "roofline": roofline,
         "clocks": clk.record(),

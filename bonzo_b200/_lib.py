@@ -28,7 +28,7 @@ EXPORTS = [
     "bnz_get_time", "bnz_last_nsts", "bnz_set_time", "bnz_check", "bnz_sync", "bnz_advance_graph",
     "bnz_device_state", "bnz_stream", "bnz_set_stream", "bnz_launch_count",
     "bnz_batch_create", "bnz_batch_destroy", "bnz_batch_last_error", "bnz_batch_size",
-    "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_advance_timed", "bnz_batch_set_stream", "bnz_batch_launch_count",
+    "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_advance_timed", "bnz_batch_step_host", "bnz_batch_set_stream", "bnz_batch_launch_count",
     "bnz_batch_sync", "bnz_variant_count", "bnz_batch_set_variant", "bnz_batch_get_variant",
     "bnz_batch_time_variant", "bnz_batch_autotune", "bnz_vl2_step_noalloc", "bnz_noalloc_last_error",
     "bnz_noalloc_scratch_bytes", "bnz_set_state_device", "bnz_get_state_device", "bnz_rollout_forward",
@@ -103,6 +103,7 @@ def load():
     L.bnz_batch_instance.argtypes = [vp, C.c_int, C.POINTER(vp)]
     L.bnz_batch_advance.argtypes = [vp, C.c_double, C.c_int]
     L.bnz_batch_advance_timed.argtypes = [vp, C.c_double, C.c_int, _dp]
+    L.bnz_batch_step_host.argtypes = [vp, C.POINTER(_dp), C.POINTER(_dp), C.c_double, C.c_int, C.c_int]
     L.bnz_set_state_device.argtypes = [vp, vp, vp]
     L.bnz_get_state_device.argtypes = [vp, vp, vp]
     L.bnz_rollout_forward.argtypes = [vp, C.c_int, C.c_double, C.c_int]
@@ -383,6 +384,29 @@ class Batch:
         ms = (C.c_double * 3)()
         self._ck(self.L.bnz_batch_advance_timed(self.h, tmax, int(nsteps), ms))
         return {"dt": ms[0], "predictor": ms[1], "corrector": ms[2]}
+
+    def step_host(self, prims, bflds, tmax=1e30, nsteps=1, nchunks=0):
+        """Load every instance's state from the host arrays, advance nsteps
+        steps and write the result (ghosts filled) back into the same arrays.
+        Copies in, steps and copies out of groups of instances overlap
+        (bnz_batch_step_host); pinned arrays make the copies asynchronous."""
+        n = len(self.instances)
+        if len(prims) != n or len(bflds) != n:
+            raise ValueError("one prim and one bfld array per instance")
+        arrays = list(prims) + list(bflds)
+        cached = getattr(self, "_host_ptrs", None)
+        if cached is None or any(x is not y for x, y in zip(cached[0], arrays)):
+            pp, pb = (_dp * n)(), (_dp * n)()
+            for q, (c, P, B) in enumerate(zip(self.instances, prims, bflds)):
+                for a, nv in ((P, 9), (B, 3)):
+                    if (a.shape != (nv,) + c.shape or a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]
+                            or not a.flags["WRITEABLE"]):
+                        raise ValueError("state array of instance %d has the wrong shape or layout" % q)
+                pp[q] = P.ctypes.data_as(_dp)
+                pb[q] = B.ctypes.data_as(_dp)
+            # the same array objects (held here) reuse the pointer tables of the last call
+            cached = self._host_ptrs = (arrays, pp, pb)
+        self._ck(self.L.bnz_batch_step_host(self.h, cached[1], cached[2], float(tmax), int(nsteps), int(nchunks)))
 
     def set_stream(self, stream):
         self._ck(self.L.bnz_batch_set_stream(self.h, C.c_void_p(stream)))

@@ -105,8 +105,9 @@ constexpr FusedVariant FUSED_VARIANTS[FUSED_NVARIANT] = {
 enum { FDT_CFL = 0, FDT_EXPLICIT = 1, FDT_FIXED = 2 };
 
 struct FusedLaunch {
-  const FusedInst* insts;
-  int ninst;
+  const FusedInst* insts;   // indexed by the tiles' instance numbers
+  int ninst;                // the per-instance launches cover insts[inst0 .. inst0+ninst-1]
+  int inst0;
   const FusedTile* tilesA;  // predictor tiles (cells 1..Ntot-2 of each axis)
   int ntA;
   const FusedTile* tilesB;  // corrector tiles (active cells)

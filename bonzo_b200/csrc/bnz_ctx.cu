@@ -991,6 +991,11 @@ struct bnz_batch {
   int variant = 0;
   const Launchers* L = nullptr;
   std::string err;
+  // first predictor / corrector tile of every instance (n + 1 entries)
+  std::vector<int> offA, offB;
+  // host-state stepping: copy-in and copy-out streams and their events
+  cudaStream_t cin = nullptr, cout = nullptr;
+  std::vector<cudaEvent_t> hev;
 };
 
 namespace {
@@ -1032,10 +1037,14 @@ FusedLaunch batch_launch(const bnz_batch* b, int dt_mode) {
 int batch_build_tiles(bnz_batch* b) {
   const FusedVariant& v = FUSED_VARIANTS[b->variant];
   std::vector<FusedTile> tA, tB;
+  b->offA.assign(1, 0);
+  b->offB.assign(1, 0);
   for (int q = 0; q < (int)b->ctx.size(); ++q) {
     const bnz_ctx* c = b->ctx[q];
     make_tiles(q, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->ng, true, v.tx, v.ty, tA);
     make_tiles(q, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->ng, false, v.tx, v.ty, tB);
+    b->offA.push_back((int)tA.size());
+    b->offB.push_back((int)tB.size());
   }
   b->ntA = (int)tA.size();
   b->ntB = (int)tB.size();
@@ -1054,6 +1063,13 @@ int batch_build_tiles(bnz_batch* b) {
 __global__ void k_set_tmax(FusedInst* insts, int n, double tmax) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q < n) insts[q].ds->tmax = tmax;
+}
+
+// Clears the CFL slot `parity` of instances q0 .. q0+n-1 before k_cds_batch
+// folds the maximum of a freshly loaded state into it.
+__global__ void k_cds_clear(FusedInst* insts, int q0, int n, int parity) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) insts[q0 + q].ds->cds_bits[parity] = 0ULL;
 }
 
 }  // namespace
@@ -1097,6 +1113,11 @@ int bnz_batch_destroy(bnz_batch* b) {
   if (b->d_inst) cudaFree(b->d_inst);
   if (b->d_tiles) cudaFree(b->d_tiles);
   if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->cin) cudaStreamSynchronize(b->cin);
+  if (b->cout) cudaStreamSynchronize(b->cout);
+  for (cudaEvent_t e : b->hev) cudaEventDestroy(e);
+  if (b->cin) cudaStreamDestroy(b->cin);
+  if (b->cout) cudaStreamDestroy(b->cout);
   if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
   delete b;
   return BNZ_OK;
@@ -1246,6 +1267,98 @@ int bnz_batch_advance_timed(bnz_batch* b, double tmax, int nsteps, double* ms_ke
   if (e != cudaSuccess) return bfail(b, BNZ_ERR_CUDA, std::string("kernel timing: ") + cudaGetErrorString(e));
   for (int k = 0; k < 3; ++k) ms_kernels[k] = sum[k] / nsteps;
   batch_epilogue(b);
+  return BNZ_OK;
+}
+
+int bnz_batch_step_host(bnz_batch* b, double* const* prim, double* const* bfld, double tmax, int nsteps,
+                        int nchunks) {
+  if (!b || b->ctx.empty()) return BNZ_ERR_ARG;
+  const int n = (int)b->ctx.size();
+  if (!prim || !bfld) return bfail(b, BNZ_ERR_ARG, "null host state arrays");
+  for (int q = 0; q < n; ++q)
+    if (!prim[q] || !bfld[q]) return bfail(b, BNZ_ERR_ARG, "null host state of instance " + std::to_string(q));
+  if (nsteps < 1) return bfail(b, BNZ_ERR_ARG, "nsteps must be >= 1");
+  if (nchunks <= 0) nchunks = 32;
+  if (nchunks > n) nchunks = n;
+  int rc = batch_prologue(b, tmax);
+  if (rc) return rc;
+  if (!b->cin) {
+    CKB(cudaStreamCreateWithFlags(&b->cin, cudaStreamNonBlocking));
+    CKB(cudaStreamCreateWithFlags(&b->cout, cudaStreamNonBlocking));
+  }
+  while ((int)b->hev.size() < 2 * nchunks + 2) {
+    cudaEvent_t e = nullptr;
+    CKB(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->hev.push_back(e);
+  }
+  cudaEvent_t ev_entry = b->hev[0], ev_out = b->hev[1];
+  // chunks of consecutive instances holding about equal numbers of cells
+  std::vector<int> cut(1, 0);
+  {
+    double total = 0., acc = 0.;
+    for (bnz_ctx* c : b->ctx) total += (double)c->ncell;
+    for (int q = 0; q < n; ++q) {
+      acc += (double)b->ctx[q]->ncell;
+      const int left = n - (q + 1);
+      const int want = (int)cut.size();  // index of the chunk being closed
+      if (want < nchunks && acc >= total * want / nchunks && left >= nchunks - want) cut.push_back(q + 1);
+    }
+    if (cut.back() != n) cut.push_back(n);
+  }
+  const int nc = (int)cut.size() - 1;
+  // the copies in follow whatever the compute stream holds already
+  CKB(cudaEventRecord(ev_entry, b->stream));
+  CKB(cudaStreamWaitEvent(b->cin, ev_entry, 0));
+  for (int k = 0; k < nc; ++k) {
+    for (int q = cut[k]; q < cut[k + 1]; ++q) {
+      bnz_ctx* c = b->ctx[q];
+      CKB(cudaMemcpyAsync(c->prim, prim[q], 9 * c->ncell * sizeof(double), cudaMemcpyHostToDevice, b->cin));
+      CKB(cudaMemcpyAsync(c->bfld, bfld[q], 3 * c->ncell * sizeof(double), cudaMemcpyHostToDevice, b->cin));
+    }
+    CKB(cudaEventRecord(b->hev[2 + 2 * k], b->cin));
+  }
+  const int mode = b->md.fixdt ? FDT_FIXED : FDT_CFL;
+  const int p0 = b->parity, p1 = (p0 + nsteps) & 1;
+  for (int k = 0; k < nc; ++k) {
+    const int q0 = cut[k], q1 = cut[k + 1];
+    FusedLaunch f = batch_launch(b, mode);
+    f.inst0 = q0;
+    f.ninst = q1 - q0;
+    f.tilesA = b->d_tiles + b->offA[q0];
+    f.ntA = b->offA[q1] - b->offA[q0];
+    f.tilesB = b->d_tiles + b->ntA + b->offB[q0];
+    f.ntB = b->offB[q1] - b->offB[q0];
+    CKB(cudaStreamWaitEvent(b->stream, b->hev[2 + 2 * k], 0));
+    // the loaded state's CFL maximum, then the steps
+    k_cds_clear<<<(f.ninst + 127) / 128, 128, 0, b->stream>>>(b->d_inst, q0, f.ninst, p0);
+    b->launches += 1 + b->L->fused_cds(f, p0);
+    int p = p0;
+    for (int s = 0; s < nsteps; ++s) {
+      b->launches += b->L->fused_step(f, p);
+      b->launches += b->L->fused_time(f);
+      p ^= 1;
+    }
+    // ghosts of the result, as bnz_get_state returns them
+    for (int q = q0; q < q1; ++q) {
+      bnz_ctx* c = b->ctx[q];
+      set_parity(c, p1);
+      StepArgs a = step_args(c);
+      b->launches += c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
+    }
+    CKB(cudaEventRecord(b->hev[3 + 2 * k], b->stream));
+    CKB(cudaStreamWaitEvent(b->cout, b->hev[3 + 2 * k], 0));
+    for (int q = q0; q < q1; ++q) {
+      bnz_ctx* c = b->ctx[q];
+      CKB(cudaMemcpyAsync(prim[q], c->prim, 9 * c->ncell * sizeof(double), cudaMemcpyDeviceToHost, b->cout));
+      CKB(cudaMemcpyAsync(bfld[q], c->bfld, 3 * c->ncell * sizeof(double), cudaMemcpyDeviceToHost, b->cout));
+    }
+  }
+  CKB(cudaGetLastError());
+  CKB(cudaEventRecord(ev_out, b->cout));
+  CKB(cudaStreamWaitEvent(b->stream, ev_out, 0));
+  b->parity = p1;
+  batch_epilogue(b);  // cons is not derived here: ghosts stay marked stale
+  CKB(cudaStreamSynchronize(b->stream));
   return BNZ_OK;
 }
 

@@ -352,8 +352,8 @@ void launch_pred_corr(const FusedLaunch& f, int parity) {
 
 int fused_step(const FusedLaunch& f, int parity) {
   if (f.events) cudaEventRecord(f.events[0], f.stream);
-  fused::k_dt_batch<<<(f.ninst + 127) / 128, 128, 0, f.stream>>>(f.insts, f.ninst, parity, f.cour, f.dt_mode,
-                                                                  f.dt_fixed);
+  fused::k_dt_batch<<<(f.ninst + 127) / 128, 128, 0, f.stream>>>(f.insts + f.inst0, f.ninst, parity, f.cour,
+                                                                  f.dt_mode, f.dt_fixed);
   switch (f.rsolver) {
     case dev::RS_HLLD: launch_pred_corr<dev::RS_HLLD>(f, parity); break;
     case dev::RS_HLLT: launch_pred_corr<dev::RS_HLLT>(f, parity); break;
@@ -363,7 +363,7 @@ int fused_step(const FusedLaunch& f, int parity) {
 }
 
 int fused_time(const FusedLaunch& f) {
-  fused::k_time_batch<<<(f.ninst + 127) / 128, 128, 0, f.stream>>>(f.insts, f.ninst);
+  fused::k_time_batch<<<(f.ninst + 127) / 128, 128, 0, f.stream>>>(f.insts + f.inst0, f.ninst);
   return 1;
 }
 

@@ -177,6 +177,19 @@ int bnz_batch_advance(bnz_batch* batch, double tmax, int nsteps);
  * launch; ms_kernels[3] receives the mean duration in ms of the per-instance
  * dt launch, the predictor launch and the corrector launch.  For measurement. */
 int bnz_batch_advance_timed(bnz_batch* batch, double tmax, int nsteps, double* ms_kernels);
+/* Host-state stepping: loads every instance's state from host memory
+ * (prim[q]: 9 fields, bfld[q]: 3 face fields, each over the instance's full
+ * array with ghosts, as bnz_set_state takes them), advances nsteps steps with
+ * per-instance CFL dt clipped to tmax, and writes the result back in place
+ * with ghosts filled (as bnz_get_state(prim, NULL, bfld) returns it).  The
+ * instances are split into nchunks groups of about equal size (0: 32) and
+ * pipelined: the copy in of one group, the steps of the previous one and the
+ * copy out of the one before that run at the same time on three streams.
+ * Pinned host memory makes the copies asynchronous.  Returns when the copies
+ * out are complete.  No counterpart in the reference, whose state lives in
+ * host arrays between its steps (src/integration/vanleer.pyx:59-179). */
+int bnz_batch_step_host(bnz_batch* batch, double* const* prim, double* const* bfld, double tmax, int nsteps,
+                        int nchunks);
 int bnz_batch_set_stream(bnz_batch* batch, void* stream);
 int bnz_batch_launch_count(const bnz_batch* batch, long long* n);
 int bnz_batch_sync(bnz_batch* batch);

@@ -141,3 +141,55 @@ def test_autotune_restores_state(tmp_path, monkeypatch):
     # a second tuner call is served from the cache
     best2, _ = autotune.tune_batch(a, [n for n, *_ in inst], steps=2)
     assert best2 == best and a.variant == best
+
+
+@pytest.mark.parametrize("nchunks,nsteps", [(0, 1), (1, 1), (3, 2), (7, 1)])
+def test_batch_step_host_matches_device_stepping(nchunks, nsteps):
+    """bnz_batch_step_host (copy in, steps, ghost fill, copy out, pipelined over
+    groups of instances) gives bitwise what set_state + advance + get_state
+    give, for every boundary kind, over repeated calls."""
+    import torch
+    from bonzo_b200._lib import Batch
+    inst = _instances([16, 40, 24, 33, 64, 20, 8])
+    bcs = [((0, 0), (0, 0), (0, 0)), ((1, 1), (2, 2), (0, 0)), ((2, 2), (1, 1), (0, 0)),
+           ((1, 2), (0, 0), (0, 0)), ((2, 1), (2, 1), (0, 0)), ((1, 1), (1, 1), (0, 0)),
+           ((0, 0), (2, 2), (0, 0))]
+    grids = [dict(Nx=n, Ny=n, Nz=1, dims=2, bc=bc) for (n, *_), bc in zip(inst, bcs)]
+    a = Batch(grids, exact_fp=True, **METHOD)
+    b = Batch(grids, exact_fp=True, **METHOD)
+    host = []
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        for e in (a, b):
+            e[q].set_state(prim, bfld)
+            e[q].init()
+        P_ = torch.empty((9,) + b[q].shape, dtype=torch.float64, pin_memory=True).numpy()
+        B_ = torch.empty((3,) + b[q].shape, dtype=torch.float64, pin_memory=True).numpy()
+        b[q].get_state_into(P_, None, B_)
+        host.append((P_, B_))
+    for call in range(3):
+        a.advance(1e30, nsteps)
+        b.step_host([h[0] for h in host], [h[1] for h in host], 1e30, nsteps, nchunks)
+        for q in range(len(inst)):
+            pa, _, ba = a[q].get_state()
+            assert np.array_equal(pa, host[q][0]), (call, q)
+            assert np.array_equal(ba, host[q][1]), (call, q)
+            assert a[q].time() == b[q].time()
+            assert b[q].check() == 0
+    # the device copy stays consistent with the host one (cons derived on demand)
+    for q in range(len(inst)):
+        for x, y in zip(a[q].get_state(), b[q].get_state()):
+            assert np.array_equal(x, y), q
+
+
+def test_batch_step_host_rejects_bad_arrays():
+    from bonzo_b200._lib import Batch, BnzError
+    inst = _instances([16, 24])
+    grids = [dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((1, 1), (1, 1), (0, 0))) for n, *_ in inst]
+    b = Batch(grids, exact_fp=True, **METHOD)
+    good = [(np.zeros((9,) + c.shape), np.zeros((3,) + c.shape)) for c in b.instances]
+    with pytest.raises(ValueError):
+        b.step_host([good[0][0]], [good[0][1]])
+    with pytest.raises(ValueError):
+        b.step_host([good[1][0], good[1][0]], [g[1] for g in good])
+    with pytest.raises(BnzError):
+        b.step_host([g[0] for g in good], [g[1] for g in good], 1e30, 0)
