@@ -273,10 +273,11 @@ def run_ours(args, rank, world, dist):
         from bonzo_b200 import autotune
         best, ms = autotune.tune_batch(eng, [q["N"] for q, _, _, _ in batch], METHOD["rsolver"],
                                        METHOD["limiter"], steps=2, use_cache=False)
-        from bonzo_b200._lib import variants
+        from bonzo_b200._lib import variant_label, variants
         vs = variants()
-        tune = {"chosen": {"tile": "%dx%d" % vs[best][:2], "staged_predictor": bool(vs[best][2])},
-                "ms_per_step": {"%dx%d%s" % (vs[v][0], vs[v][1], "s" if vs[v][2] else ""): round(t, 4)
+        tune = {"chosen": {"tile": "%dx%d" % vs[best][:2], "staged_predictor": bool(vs[best][2]),
+                           "persistent_corrector": bool(vs[best][3])},
+                "ms_per_step": {variant_label(vs[v]): round(t, 4)
                                 for v, t in ms.items()}}
     for _ in range(args.warmup):
         step()

@@ -116,7 +116,7 @@ def load():
     L.bnz_batch_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.bnz_batch_sync.argtypes = [vp]
     ip = C.POINTER(C.c_int)
-    L.bnz_variant_count.argtypes = [ip, ip, ip, ip]
+    L.bnz_variant_count.argtypes = [ip, ip, ip, ip, ip]
     L.bnz_batch_set_variant.argtypes = [vp, C.c_int]
     L.bnz_batch_get_variant.argtypes = [vp, ip]
     L.bnz_batch_time_variant.argtypes = [vp, C.c_int, C.c_int, _dp]
@@ -449,10 +449,15 @@ class Batch:
 
 
 def variants():
-    """[(tx, ty, staged)] of the fused kernel variants."""
+    """[(tx, ty, staged, persistent)] of the fused kernel variants."""
     L = load()
     n = C.c_int()
-    L.bnz_variant_count(C.byref(n), None, None, None)
-    tx, ty, st = (C.c_int * n.value)(), (C.c_int * n.value)(), (C.c_int * n.value)()
-    L.bnz_variant_count(C.byref(n), tx, ty, st)
-    return [(tx[v], ty[v], st[v]) for v in range(n.value)]
+    L.bnz_variant_count(C.byref(n), None, None, None, None)
+    tx, ty, st, pe = [(C.c_int * n.value)() for _ in range(4)]
+    L.bnz_variant_count(C.byref(n), tx, ty, st, pe)
+    return [(tx[v], ty[v], st[v], pe[v]) for v in range(n.value)]
+
+
+def variant_label(v):
+    """'15x14s' style name of a variant tuple: s = staged predictor, p = persistent corrector."""
+    return "%dx%d%s%s" % (v[0], v[1], "s" if v[2] else "", "p" if v[3] else "")

@@ -85,6 +85,7 @@ struct FusedTile {
   int inst;
   int x0, y0;
   int wx, wy;
+  int tma;  // the instance has a tensor map of its ws (persistent corrector)
 };
 
 // Variants of the fused kernels the autotuner chooses from: tile shape
@@ -92,14 +93,18 @@ struct FusedTile {
 // shared memory.  Variant 0 is the default and exists for every Riemann
 // solver; the others are built for HLLD.
 struct FusedVariant {
-  int tx, ty, staged;
+  int tx, ty, staged, persistent;
 };
 // 15 x 14 tiles give 256 x faces and 255 y faces per interior tile: each flux
 // phase of a 256-thread block is one full round (32 x 8 leaves 40% of the
 // threads idle in the second round of each phase).
-constexpr int FUSED_NVARIANT = 6;
+// The persistent variants run the corrector as one resident grid fed by a tile
+// queue, with TMA double-buffering of its staged input (15 x 14 only: two
+// blocks of that kernel fit one SM's shared memory).
+constexpr int FUSED_NVARIANT = 8;
 constexpr FusedVariant FUSED_VARIANTS[FUSED_NVARIANT] = {
-    {32, 8, 0}, {32, 8, 1}, {16, 16, 0}, {16, 16, 1}, {15, 14, 0}, {15, 14, 1}};
+    {32, 8, 0, 0}, {32, 8, 1, 0}, {16, 16, 0, 0}, {16, 16, 1, 0},
+    {15, 14, 0, 0}, {15, 14, 1, 0}, {15, 14, 0, 1}, {15, 14, 1, 1}};
 
 // dt modes of the fused step
 enum { FDT_CFL = 0, FDT_EXPLICIT = 1, FDT_FIXED = 2 };
@@ -119,6 +124,10 @@ struct FusedLaunch {
   double dt_fixed;
   unsigned* err;
   cudaStream_t stream;
+  // persistent corrector: per-instance ws tensor maps (128 bytes each) and
+  // the work-queue counter; null where the variant is not persistent
+  const unsigned char* wsmaps;
+  unsigned* queue;
   // optional: events recorded before k_dt_batch, before the predictor, before
   // the corrector and after it (kernel timing; null in normal stepping)
   cudaEvent_t* events;

@@ -2,6 +2,7 @@
 //
 // One context = one grid (BnzGrid + BnzIntegr of the reference): coordinates,
 // device state, scratch and the CUDA stream its calls are ordered on.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -235,6 +236,7 @@ void make_tiles(int inst, int N0, int N1, int ng, bool pred, int tx, int ty, std
       ft.y0 = lo[1];
       ft.wx = hi[0] - lo[0] + 1;
       ft.wy = hi[1] - lo[1] + 1;
+      ft.tma = 0;
       out.push_back(ft);
     }
 }
@@ -996,6 +998,9 @@ struct bnz_batch {
   // host-state stepping: copy-in and copy-out streams and their events
   cudaStream_t cin = nullptr, cout = nullptr;
   std::vector<cudaEvent_t> hev;
+  // persistent corrector: tensor maps of every instance's ws, work-queue counter
+  unsigned char* d_maps = nullptr;
+  unsigned* d_queue = nullptr;
 };
 
 namespace {
@@ -1030,7 +1035,48 @@ FusedLaunch batch_launch(const bnz_batch* b, int dt_mode) {
   f.dt_fixed = b->md.dt_fixed;
   f.err = b->ctx.empty() ? nullptr : b->ctx[0]->d_err;
   f.stream = b->stream;
+  if (FUSED_VARIANTS[b->variant].persistent && b->d_maps) {
+    f.wsmaps = b->d_maps;
+    f.queue = b->d_queue;
+  }
   return f;
+}
+
+// cuTensorMapEncodeTiled from the driver, found once through the runtime.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// The persistent corrector's TMA box over ws: (x, y, field) = (bw, bh, 9)
+// doubles, bw even, from an even column.  A map needs 16-byte row and field
+// strides, so instances with odd Ntot_x get none (their tiles stage with
+// plain loads).  Returns whether instance q has a map.
+bool ws_map(const bnz_ctx* c, int bw, int bh, CUtensorMap* out) {
+  EncodeTiledFn enc = encode_tiled();
+  const int nx = c->Ntot[0], ny = c->Ntot[1];
+  if (!enc || (nx & 1) || ((uintptr_t)c->cons_s & 15)) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, 9};
+  const cuuint64_t strides[2] = {(cuuint64_t)nx * sizeof(double), (cuuint64_t)nx * ny * sizeof(double)};
+  const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 9};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return enc(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)c->cons_s, dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // Tile lists of every instance for the batch's variant (predictor list first).
@@ -1045,6 +1091,20 @@ int batch_build_tiles(bnz_batch* b) {
     make_tiles(q, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->ng, false, v.tx, v.ty, tB);
     b->offA.push_back((int)tA.size());
     b->offB.push_back((int)tB.size());
+  }
+  if (v.persistent) {
+    static_assert(sizeof(CUtensorMap) == 128, "tensor maps are 128 bytes");
+    // box of TmaBox<tx, ty> (bnz_fused.cuh): tx + 4 cells from an even column, ty + 4 rows
+    const int bw = (v.tx + 6) & ~1, bh = v.ty + 4;
+    std::vector<CUtensorMap> maps(b->ctx.size());
+    std::vector<int> ok(b->ctx.size(), 0);
+    memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
+    for (size_t q = 0; q < b->ctx.size(); ++q) ok[q] = ws_map(b->ctx[q], bw, bh, &maps[q]) ? 1 : 0;
+    for (FusedTile& t : tB) t.tma = ok[t.inst];
+    if (!b->d_maps) CKB(cudaMalloc((void**)&b->d_maps, maps.size() * sizeof(CUtensorMap)));
+    if (!b->d_queue) CKB(cudaMalloc((void**)&b->d_queue, sizeof(unsigned)));
+    CKB(cudaMemcpy(b->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+    CKB(cudaMemset(b->d_queue, 0, sizeof(unsigned)));
   }
   b->ntA = (int)tA.size();
   b->ntB = (int)tB.size();
@@ -1112,6 +1172,8 @@ int bnz_batch_destroy(bnz_batch* b) {
   for (bnz_ctx* c : b->ctx) bnz_destroy(c);
   if (b->d_inst) cudaFree(b->d_inst);
   if (b->d_tiles) cudaFree(b->d_tiles);
+  if (b->d_maps) cudaFree(b->d_maps);
+  if (b->d_queue) cudaFree(b->d_queue);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->cin) cudaStreamSynchronize(b->cin);
   if (b->cout) cudaStreamSynchronize(b->cout);
@@ -1376,12 +1438,13 @@ int bnz_batch_sync(bnz_batch* b) {
   return BNZ_OK;
 }
 
-int bnz_variant_count(int* n, int* tx, int* ty, int* staged) {
+int bnz_variant_count(int* n, int* tx, int* ty, int* staged, int* persistent) {
   if (n) *n = FUSED_NVARIANT;
   for (int v = 0; v < FUSED_NVARIANT; ++v) {
     if (tx) tx[v] = FUSED_VARIANTS[v].tx;
     if (ty) ty[v] = FUSED_VARIANTS[v].ty;
     if (staged) staged[v] = FUSED_VARIANTS[v].staged;
+    if (persistent) persistent[v] = FUSED_VARIANTS[v].persistent;
   }
   return BNZ_OK;
 }

@@ -693,39 +693,22 @@ __device__ __forceinline__ void copy_tile(const Inst& I, const Tile& T, int pari
   }
 }
 
+// Everything of the corrector after its input cells are staged: PLM fluxes,
+// EMFs, the cell update, the writes of w^(n+1) / b^(n+1) and the tile's CFL
+// maximum folded into the instance's slot.
+// sF: fluxes, EMFs and slopes, contiguous (x fluxes, y fluxes, E_c, E_e, slopes).
 template <int TXM, int TYM, int RS, int LIM>
-__global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
-                                                   int parity, int cp) {
-  constexpr int RING = 2;
-  extern __shared__ double smem[];
-  __shared__ double red[8];
-  __shared__ Inst sI;
-  const Tile T = tiles[blockIdx.x];
-  stage_inst(sI, insts, T.inst);
-  const Inst& I = sI;
-  const double dt = I.ds->dt;
-  if (!(dt > 0.)) {
-    // time has reached tmax: carry the state over unchanged
-    copy_tile(I, T, parity);
-    return;
-  }
+__device__ __forceinline__ void corr_tile(const Inst& I, const Tile& T, int parity, int cp, const SmemCells& W,
+                                          double* sF, double* red, double dt) {
+  using M = Smem<TXM, TYM, 2>;
+  double* sFX = sF;
+  double* sFY = sFX + NF * M::NFX;
+  double* sEC = sFY + NF * M::NFY;
+  double* sEE = sEC + M::NEC;
+  double* sD = sEE + M::NEE;
   Layout L;
   L.set(T.wx, T.wy);
-  double* sFX = smem;
-  double* sFY = sFX + NF * Smem<TXM, TYM, RING>::NFX;
-  double* sEC = sFY + NF * Smem<TXM, TYM, RING>::NFY;
-  double* sEE = sEC + Smem<TXM, TYM, RING>::NEC;
-  double* sW = sEE + Smem<TXM, TYM, RING>::NEE;
-  double* sD = sW + Smem<TXM, TYM, RING>::NSW;
-  Stage S;
-  S.x0 = T.x0 - 2;
-  S.y0 = T.y0 - 2;
-  S.w = T.wx + 4;
-  S.h = T.wy + 4;
-  stage_cells<false>(I, I.ws, S, sW);
-  __syncthreads();
   unsigned e = 0;
-  SmemCells W{sW, S, S.cells()};
   stage_fluxes_plm<LIM, RS>(I, T, L, W, I.bs, sFX, sFY, sEC, sD, cp, e);
   __syncthreads();
   stage_emf(L, sFX, sFY, sEC, sEE);
@@ -788,13 +771,214 @@ __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ inst
   if (e) atomicOr(I.err, e);
 }
 
+template <int TXM, int TYM, int RS, int LIM>
+__global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
+                                                   int parity, int cp) {
+  constexpr int RING = 2;
+  extern __shared__ double smem[];
+  __shared__ double red[8];
+  __shared__ Inst sI;
+  const Tile T = tiles[blockIdx.x];
+  stage_inst(sI, insts, T.inst);
+  const Inst& I = sI;
+  const double dt = I.ds->dt;
+  if (!(dt > 0.)) {
+    // time has reached tmax: carry the state over unchanged
+    copy_tile(I, T, parity);
+    return;
+  }
+  // staged cells first, then the fluxes, EMFs and slopes
+  double* sW = smem;
+  Stage S;
+  S.x0 = T.x0 - 2;
+  S.y0 = T.y0 - 2;
+  S.w = T.wx + 4;
+  S.h = T.wy + 4;
+  stage_cells<false>(I, I.ws, S, sW);
+  __syncthreads();
+  SmemCells W{sW, S, S.cells()};
+  corr_tile<TXM, TYM, RS, LIM>(I, T, parity, cp, W, smem + Smem<TXM, TYM, RING>::NSW, red, dt);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent corrector: a grid of (SMs x resident blocks) takes tiles from a
+// work queue (an atomic counter the dt kernel resets every step).  The staged
+// input (ws on the tile and two rings, 9 fields) of the NEXT tile is loaded by
+// TMA into the second of two shared-memory buffers while the current tile is
+// computed.  The TMA box starts at an even column (16-byte rule for FP64) and
+// is TmaBox::W cells wide; rows or columns past the array read as zeros and
+// are never used.  Instances whose rows are not a multiple of 16 bytes
+// (odd Ntot_x) have no tensor map: their tiles stage with plain loads.
+// ---------------------------------------------------------------------------
+
+template <int TXM, int TYM>
+struct TmaBox {
+  static constexpr int W = (TXM + 5 + 1) & ~1;  // TX+4 cells from an even column at or before x0-2
+  static constexpr int H = TYM + 4;
+  static constexpr int CELLS = W * H;
+  static constexpr unsigned BYTES = NM * CELLS * sizeof(double);
+  static constexpr int BUF = (NM * CELLS + 15) / 16 * 16;  // doubles per buffer, 128-byte multiple
+  static constexpr size_t smem_bytes = 128 +  // room to align the buffers
+      sizeof(double) * (2 * (size_t)BUF + (size_t)NF * (Smem<TXM, TYM, 2>::NFX + Smem<TXM, TYM, 2>::NFY) +
+                        Smem<TXM, TYM, 2>::NEC + Smem<TXM, TYM, 2>::NEE + Smem<TXM, TYM, 2>::NSD);
+};
+
+namespace tma {
+__device__ __forceinline__ unsigned saddr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void bar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_bar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(bar)) : "memory");
+}
+__device__ __forceinline__ void arrive_expect(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool try_wait(unsigned long long* bar, unsigned phase) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(saddr(bar)), "r"(phase)
+      : "memory");
+  return ok != 0u;
+}
+// bounded wait: false after about a second without the phase completing
+__device__ __forceinline__ bool wait(unsigned long long* bar, unsigned phase) {
+  const long long t0 = clock64();
+  while (!try_wait(bar, phase))
+    if (clock64() - t0 > (1LL << 31)) return false;
+  return true;
+}
+__device__ __forceinline__ void load_3d(void* dst, unsigned long long* bar, const void* map, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(saddr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(saddr(bar))
+      : "memory");
+}
+__device__ __forceinline__ void prefetch_map(const void* map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(map) : "memory");
+}
+}  // namespace tma
+
+// Issued by one thread for the tile that will use buffer dst / bar: its
+// staged input by TMA, or (no tensor map) a plain arrival, so that every use
+// of a buffer completes exactly one phase of its barrier.
+template <int TXM, int TYM>
+__device__ __forceinline__ void issue_ws(const Tile& T, const unsigned char* maps, double* dst,
+                                         unsigned long long* bar) {
+  if (T.tma) {
+    const void* map = maps + (size_t)T.inst * 128;
+    tma::fence_async_shared();
+    tma::arrive_expect(bar, TmaBox<TXM, TYM>::BYTES);
+    tma::load_3d(dst, bar, map, (T.x0 - 2) & ~1, T.y0 - 2, 0);
+  } else {
+    tma::arrive(bar);
+  }
+}
+
+// Iteration k of a block uses buffer k & 1; it is that buffer's (k >> 1)-th
+// use, so it waits for the phase of parity (k >> 1) & 1.
+template <int TXM, int TYM, int RS, int LIM>
+__global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
+                                                      int ntiles, int parity, int cp,
+                                                      const unsigned char* __restrict__ maps,
+                                                      unsigned* __restrict__ queue) {
+  using B = TmaBox<TXM, TYM>;
+  extern __shared__ __align__(128) double smem_raw[];
+  __shared__ double red[8];
+  __shared__ Inst sI;
+  __shared__ Tile sT;
+  __shared__ __align__(8) unsigned long long bar[2];
+  __shared__ int s_tile[2], s_fail;  // tile of iteration k in s_tile[k & 1]
+  // TMA destinations start on 128-byte boundaries (the launch adds 128 bytes)
+  double* smem = smem_raw + ((128u - (tma::saddr(smem_raw) & 127u)) & 127u) / sizeof(double);
+  // two staging buffers of B::BUF doubles, then the fluxes, EMFs and slopes
+  if (threadIdx.x == 0) {
+    tma::bar_init(&bar[0], 1);
+    tma::bar_init(&bar[1], 1);
+    tma::fence_bar_init();
+    s_fail = 0;
+    const int t0 = (int)atomicAdd(queue, 1u);
+    s_tile[0] = t0;
+    if (t0 < ntiles) {
+      const Tile T0 = tiles[t0];
+      if (T0.tma) tma::prefetch_map(maps + (size_t)T0.inst * 128);
+      issue_ws<TXM, TYM>(T0, maps, smem, &bar[0]);
+    }
+  }
+  __syncthreads();
+  for (int k = 0;; ++k) {
+    // written by thread 0 before the last barrier; the slot it writes next
+    // was last read before an earlier barrier
+    const int t = s_tile[k & 1];
+    if (t >= ntiles) break;
+    const int buf = k & 1;
+    if (threadIdx.x == 0) {
+      sT = tiles[t];
+      const int tn = (int)atomicAdd(queue, 1u);
+      s_tile[buf ^ 1] = tn;
+      // the other buffer is free: its tile finished before the last barrier
+      if (tn < ntiles) issue_ws<TXM, TYM>(tiles[tn], maps, smem + (buf ^ 1) * B::BUF, &bar[buf ^ 1]);
+    }
+    stage_inst(sI, insts, tiles[t].inst);  // ends with a barrier (sT, s_tile visible)
+    const Tile& T = sT;
+    const Inst& I = sI;
+    const unsigned ph = (unsigned)(k >> 1) & 1u;
+    // one thread waits (bounded) and tells the block; then every thread
+    // observes the completed phase itself
+    if (threadIdx.x == 0 && !tma::wait(&bar[buf], ph)) s_fail = 1;
+    __syncthreads();
+    if (s_fail) {
+      // flag it, give the next tile's load (if any) a bounded wait, and leave
+      if (threadIdx.x == 0) {
+        atomicOr(I.err, (unsigned)ERR_TIMEOUT);
+        if (s_tile[buf ^ 1] < ntiles) tma::wait(&bar[buf ^ 1], (unsigned)((k + 1) >> 1) & 1u);
+      }
+      return;
+    }
+    tma::wait(&bar[buf], ph);
+    const double dt = I.ds->dt;
+    double* sW = smem + buf * B::BUF;
+    Stage S;
+    if (T.tma) {
+      S.x0 = (T.x0 - 2) & ~1;
+      S.y0 = T.y0 - 2;
+      S.w = B::W;
+      S.h = B::H;
+    } else {
+      S.x0 = T.x0 - 2;
+      S.y0 = T.y0 - 2;
+      S.w = T.wx + 4;
+      S.h = T.wy + 4;
+      if (dt > 0.) stage_cells<false>(I, I.ws, S, sW);
+      __syncthreads();
+    }
+    if (dt > 0.) {
+      SmemCells W{sW, S, S.cells()};
+      corr_tile<TXM, TYM, RS, LIM>(I, T, parity, cp, W, smem + 2 * B::BUF, red, dt);
+    } else {
+      copy_tile(I, T, parity);  // time has reached tmax: carry the state over
+    }
+    __syncthreads();  // the tile's buffer, sT and sI are free again
+  }
+}
+
 // Per-instance dt for the step of parity p (new_dt.pyx:117, vanleer.pyx:95-96):
 // FDT_CFL  cour / max of slot p, clipped to tmax;
 // FDT_FIXED dt_fixed (the FIXDT build), clipped to tmax;
 // FDT_EXPLICIT keeps the dt the host wrote (bnz_vl2_step).
-// Clears the slot the corrector fills for the next step.
-__global__ void k_dt_batch(const Inst* __restrict__ insts, int n, int parity, double cour, int mode, double dt_fixed) {
+// Clears the slot the corrector fills for the next step (or carries the slot
+// over when the step does not advance), and the persistent corrector's
+// work-queue counter.
+__global__ void k_dt_batch(const Inst* __restrict__ insts, int n, int parity, double cour, int mode, double dt_fixed,
+                           unsigned* queue) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q == 0 && queue) *queue = 0u;  // the persistent corrector's tile counter
   if (q >= n) return;
   DtState* ds = insts[q].ds;
   if (mode != FDT_EXPLICIT) {
@@ -809,7 +993,9 @@ __global__ void k_dt_batch(const Inst* __restrict__ insts, int n, int parity, do
     if (ds->time >= ds->tmax) dt = 0.;
     ds->dt = dt;
   }
-  ds->cds_bits[parity ^ 1] = 0ULL;
+  // a step that does not advance (time at tmax) leaves the state, and so its
+  // CFL maximum, unchanged: the slot is carried over instead of refilled
+  ds->cds_bits[parity ^ 1] = ds->dt > 0. ? 0ULL : ds->cds_bits[parity];
 }
 
 __global__ void k_time_batch(const Inst* __restrict__ insts, int n) {

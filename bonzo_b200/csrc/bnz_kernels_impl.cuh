@@ -6,6 +6,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "bnz_common.h"
 #include "bnz_launch.h"
 
@@ -313,6 +315,37 @@ void launch_corr(const FusedLaunch& f, int parity) {
   fused::k_corr2d<TX, TY, RS, LIM><<<f.ntB, 256, smB, f.stream>>>(f.insts, f.tilesB, parity, f.charact_proj);
 }
 
+// Persistent corrector: (SMs x resident blocks) blocks, never more than tiles.
+template <int TX, int TY, int RS, int LIM>
+void launch_corr_pq(const FusedLaunch& f, int parity) {
+  constexpr size_t sm = fused::TmaBox<TX, TY>::smem_bytes;
+  static int per_sm = 0;
+  static int nsm[64] = {0};
+  if (!per_sm) {
+    cudaFuncSetAttribute(fused::k_corr2d_pq<TX, TY, RS, LIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused::k_corr2d_pq<TX, TY, RS, LIM>, 256, sm);
+    if (per_sm < 1) per_sm = 1;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (!nsm[dev]) cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::min(f.ntB, per_sm * std::max(1, nsm[dev]));
+  fused::k_corr2d_pq<TX, TY, RS, LIM><<<grid, 256, sm, f.stream>>>(f.insts, f.tilesB, f.ntB, parity,
+                                                                    f.charact_proj, f.wsmaps, f.queue);
+}
+
+template <int TX, int TY, int RS, int LIM>
+void launch_corr_any(const FusedLaunch& f, int parity) {
+  if constexpr (TX == 15 && TY == 14) {
+    if (f.wsmaps && f.queue) {
+      launch_corr_pq<TX, TY, RS, LIM>(f, parity);
+      return;
+    }
+  }
+  launch_corr<TX, TY, RS, LIM>(f, parity);
+}
+
 template <int TX, int TY, int RS, int STAGED>
 void launch_variant(const FusedLaunch& f, int parity) {
   constexpr int TXA = TX + 4, TYA = TY + 4;  // predictor tiles grow by the ghost rings
@@ -327,9 +360,9 @@ void launch_variant(const FusedLaunch& f, int parity) {
   fused::k_pred2d<TXA, TYA, RS, STAGED><<<f.ntA, 256, smA, f.stream>>>(f.insts, f.tilesA, parity, f.limiter);
   if (f.events) cudaEventRecord(f.events[2], f.stream);
   // the limiter is a compile-time choice of the corrector (reconstr_c.h:28-44)
-  if (f.limiter == dev::LIM_MC) launch_corr<TX, TY, RS, dev::LIM_MC>(f, parity);
-  else if (f.limiter == dev::LIM_MM) launch_corr<TX, TY, RS, dev::LIM_MM>(f, parity);
-  else launch_corr<TX, TY, RS, dev::LIM_VL>(f, parity);
+  if (f.limiter == dev::LIM_MC) launch_corr_any<TX, TY, RS, dev::LIM_MC>(f, parity);
+  else if (f.limiter == dev::LIM_MM) launch_corr_any<TX, TY, RS, dev::LIM_MM>(f, parity);
+  else launch_corr_any<TX, TY, RS, dev::LIM_VL>(f, parity);
   if (f.events) cudaEventRecord(f.events[3], f.stream);
 }
 
@@ -343,6 +376,8 @@ void launch_pred_corr(const FusedLaunch& f, int parity) {
       case 3: launch_variant<16, 16, RS, 1>(f, parity); return;
       case 4: launch_variant<15, 14, RS, 0>(f, parity); return;
       case 5: launch_variant<15, 14, RS, 1>(f, parity); return;
+      case 6: launch_variant<15, 14, RS, 0>(f, parity); return;  // persistent corrector when maps are given
+      case 7: launch_variant<15, 14, RS, 1>(f, parity); return;
       default: break;
     }
   }
@@ -353,7 +388,7 @@ void launch_pred_corr(const FusedLaunch& f, int parity) {
 int fused_step(const FusedLaunch& f, int parity) {
   if (f.events) cudaEventRecord(f.events[0], f.stream);
   fused::k_dt_batch<<<(f.ninst + 127) / 128, 128, 0, f.stream>>>(f.insts + f.inst0, f.ninst, parity, f.cour,
-                                                                  f.dt_mode, f.dt_fixed);
+                                                                  f.dt_mode, f.dt_fixed, f.queue);
   switch (f.rsolver) {
     case dev::RS_HLLD: launch_pred_corr<dev::RS_HLLD>(f, parity); break;
     case dev::RS_HLLT: launch_pred_corr<dev::RS_HLLT>(f, parity); break;

@@ -194,12 +194,13 @@ int bnz_batch_set_stream(bnz_batch* batch, void* stream);
 int bnz_batch_launch_count(const bnz_batch* batch, long long* n);
 int bnz_batch_sync(bnz_batch* batch);
 
-/* Kernel variants (tile shape tx x ty, predictor staging) and the autotuner.
+/* Kernel variants (tile shape tx x ty, predictor staging, persistent
+ * corrector fed by a tile queue with TMA-staged input) and the autotuner.
  * bnz_variant_count fills n and, if non-NULL, arrays of n entries.
  * bnz_batch_time_variant times `steps` steps of one variant on the live state
  * and restores the state afterwards; bnz_batch_autotune times every variant
  * and keeps the fastest (*best, and the per-variant ms, -1 where not built). */
-int bnz_variant_count(int* n, int* tx, int* ty, int* staged);
+int bnz_variant_count(int* n, int* tx, int* ty, int* staged, int* persistent);
 int bnz_batch_set_variant(bnz_batch* batch, int variant);
 int bnz_batch_get_variant(const bnz_batch* batch, int* variant);
 int bnz_batch_time_variant(bnz_batch* batch, int variant, int steps, double* ms);

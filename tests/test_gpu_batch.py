@@ -84,6 +84,31 @@ def test_batch_per_instance_tmax():
             assert np.array_equal(x, y)
 
 
+def test_batch_continues_after_tmax():
+    """Instances that stopped at tmax (extra steps did not advance them) go on
+    with the right CFL dt once tmax is raised."""
+    from bonzo_b200._lib import Batch
+    inst = _instances([24, 48])
+    grids = [dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((1, 1), (1, 1), (0, 0))) for n, *_ in inst]
+    b = Batch(grids, exact_fp=True, **METHOD)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        b[q].set_state(prim, bfld)
+        b[q].init()
+    b.advance(0.005, 40)   # both reach 0.005 well before 40 steps
+    b.advance(0.01, 40)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        o = oracle_sim(dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((1, 1), (1, 1), (0, 0))), **METHOD)
+        o.set_state(prim, bfld)
+        o.init()
+        o.advance(0.005)
+        o.advance(0.01)
+        t, s, _ = b[q].time()
+        assert t == 0.01 and s == o.nstep
+        for x, y in zip(o.get_state(), b[q].get_state()):
+            assert np.array_equal(x, y)
+        assert b[q].check() == 0
+
+
 def test_batch_rejects_3d_and_conduction():
     from bonzo_b200._lib import Batch, BnzError
     with pytest.raises(BnzError):
@@ -92,9 +117,11 @@ def test_batch_rejects_3d_and_conduction():
         Batch([dict(Nx=8, Ny=8, Nz=1, dims=2)], kappa0=0.1, **METHOD)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7])
 def test_every_variant_bitwise_vs_oracle(variant):
-    """Every autotuner candidate (tile shape, predictor staging) gives the same bits."""
+    """Every autotuner candidate (tile shape, predictor staging, persistent
+    corrector) gives the same bits.  Odd sizes have no tensor map: their tiles
+    take the persistent corrector's plain-load staging in the same launch."""
     from bonzo_b200._lib import Batch
     inst = _instances([16, 33, 64, 20, 97], seed=11)
     grids = [dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((1, 1), (1, 1), (0, 0))) for n, *_ in inst]
@@ -193,3 +220,45 @@ def test_batch_step_host_rejects_bad_arrays():
         b.step_host([good[1][0], good[1][0]], [g[1] for g in good])
     with pytest.raises(BnzError):
         b.step_host([g[0] for g in good], [g[1] for g in good], 1e30, 0)
+
+
+@pytest.mark.parametrize("variant", [6, 7])
+def test_persistent_corrector_tmax_bcs_and_host_stepping(variant):
+    """The persistent corrector (tile queue, TMA-staged input) with periodic,
+    outflow and reflecting instances, some stopping at tmax (their tiles are
+    carried over unchanged), stepped on the device and through the pipelined
+    host-state path: bitwise the default variant."""
+    import torch
+    from bonzo_b200._lib import Batch
+    inst = _instances([30, 40, 24, 33, 64, 20, 8, 46], seed=5)
+    bcs = [((0, 0), (0, 0), (0, 0)), ((1, 1), (2, 2), (0, 0)), ((2, 2), (1, 1), (0, 0)),
+           ((1, 2), (0, 0), (0, 0)), ((2, 1), (2, 1), (0, 0)), ((1, 1), (1, 1), (0, 0)),
+           ((0, 0), (2, 2), (0, 0)), ((2, 2), (2, 2), (0, 0))]
+    grids = [dict(Nx=n, Ny=n, Nz=1, dims=2, bc=bc) for (n, *_), bc in zip(inst, bcs)]
+    ref = Batch(grids, exact_fp=True, **METHOD)
+    per = Batch(grids, exact_fp=True, **METHOD)
+    per.set_variant(variant)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        for e in (ref, per):
+            e[q].set_state(prim, bfld)
+            e[q].init()
+    tmax = 0.004  # the small grids reach it within the steps below
+    ref.advance(tmax, 6)
+    per.advance(tmax, 6)
+    for q in range(len(inst)):
+        assert ref[q].time() == per[q].time()
+        for x, y in zip(ref[q].get_state(), per[q].get_state()):
+            assert np.array_equal(x, y), q
+        assert per[q].check() == 0
+    host = []
+    for c in per.instances:
+        P_ = torch.empty((9,) + c.shape, dtype=torch.float64, pin_memory=True).numpy()
+        B_ = torch.empty((3,) + c.shape, dtype=torch.float64, pin_memory=True).numpy()
+        c.get_state_into(P_, None, B_)
+        host.append((P_, B_))
+    ref.advance(1e30, 2)
+    per.step_host([h[0] for h in host], [h[1] for h in host], 1e30, 2, 3)
+    for q in range(len(inst)):
+        pa, _, ba = ref[q].get_state()
+        assert np.array_equal(pa, host[q][0]) and np.array_equal(ba, host[q][1]), q
+        assert per[q].check() == 0
