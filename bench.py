@@ -276,7 +276,7 @@ def run_ours(args, rank, world, dist):
         from bonzo_b200._lib import variant_label, variants
         vs = variants()
         tune = {"chosen": {"tile": "%dx%d" % vs[best][:2], "staged_predictor": bool(vs[best][2]),
-                           "persistent_corrector": bool(vs[best][3])},
+                           "persistent": ["none", "corrector", "predictor and corrector"][vs[best][3]]},
                 "ms_per_step": {variant_label(vs[v]): round(t, 4)
                                 for v, t in ms.items()}}
     for _ in range(args.warmup):

@@ -459,5 +459,6 @@ def variants():
 
 
 def variant_label(v):
-    """'15x14s' style name of a variant tuple: s = staged predictor, p = persistent corrector."""
-    return "%dx%d%s%s" % (v[0], v[1], "s" if v[2] else "", "p" if v[3] else "")
+    """'15x14s' style name of a variant tuple: s = staged predictor, p = persistent
+    corrector, pp = persistent predictor and corrector."""
+    return "%dx%d%s%s" % (v[0], v[1], "s" if v[2] else "", "p" * v[3])

@@ -98,13 +98,14 @@ struct FusedVariant {
 // 15 x 14 tiles give 256 x faces and 255 y faces per interior tile: each flux
 // phase of a 256-thread block is one full round (32 x 8 leaves 40% of the
 // threads idle in the second round of each phase).
-// The persistent variants run the corrector as one resident grid fed by a tile
-// queue, with TMA double-buffering of its staged input (15 x 14 only: two
-// blocks of that kernel fit one SM's shared memory).
-constexpr int FUSED_NVARIANT = 8;
+// The persistent variants run the corrector (persistent = 1) or both stages
+// (2) as one resident grid fed by a tile queue, with TMA double-buffering of
+// the staged input (15 x 14 only: two blocks of those kernels fit one SM's
+// shared memory).
+constexpr int FUSED_NVARIANT = 9;
 constexpr FusedVariant FUSED_VARIANTS[FUSED_NVARIANT] = {
-    {32, 8, 0, 0}, {32, 8, 1, 0}, {16, 16, 0, 0}, {16, 16, 1, 0},
-    {15, 14, 0, 0}, {15, 14, 1, 0}, {15, 14, 0, 1}, {15, 14, 1, 1}};
+    {32, 8, 0, 0}, {32, 8, 1, 0}, {16, 16, 0, 0}, {16, 16, 1, 0}, {15, 14, 0, 0},
+    {15, 14, 1, 0}, {15, 14, 0, 1}, {15, 14, 1, 1}, {15, 14, 0, 2}};
 
 // dt modes of the fused step
 enum { FDT_CFL = 0, FDT_EXPLICIT = 1, FDT_FIXED = 2 };
@@ -124,9 +125,11 @@ struct FusedLaunch {
   double dt_fixed;
   unsigned* err;
   cudaStream_t stream;
-  // persistent corrector: per-instance ws tensor maps (128 bytes each) and
-  // the work-queue counter; null where the variant is not persistent
+  // persistent kernels: per-instance tensor maps (128 bytes each) of ws
+  // (corrector) and of w[0], w[1] (predictor), and the two work-queue
+  // counters (corrector, predictor); null where the variant does not use them
   const unsigned char* wsmaps;
+  const unsigned char* wmaps;
   unsigned* queue;
   // optional: events recorded before k_dt_batch, before the predictor, before
   // the corrector and after it (kernel timing; null in normal stepping)

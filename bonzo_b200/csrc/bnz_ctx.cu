@@ -998,8 +998,10 @@ struct bnz_batch {
   // host-state stepping: copy-in and copy-out streams and their events
   cudaStream_t cin = nullptr, cout = nullptr;
   std::vector<cudaEvent_t> hev;
-  // persistent corrector: tensor maps of every instance's ws, work-queue counter
+  // persistent kernels: tensor maps of every instance's ws (corrector) and
+  // w[0], w[1] (predictor), work-queue counters (corrector, predictor)
   unsigned char* d_maps = nullptr;
+  unsigned char* d_wmaps = nullptr;
   unsigned* d_queue = nullptr;
 };
 
@@ -1038,6 +1040,7 @@ FusedLaunch batch_launch(const bnz_batch* b, int dt_mode) {
   if (FUSED_VARIANTS[b->variant].persistent && b->d_maps) {
     f.wsmaps = b->d_maps;
     f.queue = b->d_queue;
+    if (FUSED_VARIANTS[b->variant].persistent == 2) f.wmaps = b->d_wmaps;
   }
   return f;
 }
@@ -1062,19 +1065,19 @@ EncodeTiledFn encode_tiled() {
   return fn;
 }
 
-// The persistent corrector's TMA box over ws: (x, y, field) = (bw, bh, 9)
-// doubles, bw even, from an even column.  A map needs 16-byte row and field
-// strides, so instances with odd Ntot_x get none (their tiles stage with
-// plain loads).  Returns whether instance q has a map.
-bool ws_map(const bnz_ctx* c, int bw, int bh, CUtensorMap* out) {
+// A TMA box of (x, y, field) = (bw, bh, 9) doubles over one 9-field cell
+// array of the instance (ws or w[p]), bw even, used from even columns.  A map
+// needs 16-byte row and field strides, so instances with odd Ntot_x get none
+// (their tiles stage with plain loads).  Returns whether the map was made.
+bool cell_map(const bnz_ctx* c, const double* base, int bw, int bh, CUtensorMap* out) {
   EncodeTiledFn enc = encode_tiled();
   const int nx = c->Ntot[0], ny = c->Ntot[1];
-  if (!enc || (nx & 1) || ((uintptr_t)c->cons_s & 15)) return false;
+  if (!enc || (nx & 1) || ((uintptr_t)base & 15)) return false;
   const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, 9};
   const cuuint64_t strides[2] = {(cuuint64_t)nx * sizeof(double), (cuuint64_t)nx * ny * sizeof(double)};
   const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 9};
   const cuuint32_t es[3] = {1, 1, 1};
-  return enc(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)c->cons_s, dims, strides, box, es,
+  return enc(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)base, dims, strides, box, es,
              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -1099,12 +1102,33 @@ int batch_build_tiles(bnz_batch* b) {
     std::vector<CUtensorMap> maps(b->ctx.size());
     std::vector<int> ok(b->ctx.size(), 0);
     memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
-    for (size_t q = 0; q < b->ctx.size(); ++q) ok[q] = ws_map(b->ctx[q], bw, bh, &maps[q]) ? 1 : 0;
+    for (size_t q = 0; q < b->ctx.size(); ++q) ok[q] = cell_map(b->ctx[q], b->ctx[q]->cons_s, bw, bh, &maps[q]);
     for (FusedTile& t : tB) t.tma = ok[t.inst];
     if (!b->d_maps) CKB(cudaMalloc((void**)&b->d_maps, maps.size() * sizeof(CUtensorMap)));
-    if (!b->d_queue) CKB(cudaMalloc((void**)&b->d_queue, sizeof(unsigned)));
+    if (!b->d_queue) CKB(cudaMalloc((void**)&b->d_queue, 2 * sizeof(unsigned)));
     CKB(cudaMemcpy(b->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
-    CKB(cudaMemset(b->d_queue, 0, sizeof(unsigned)));
+    CKB(cudaMemset(b->d_queue, 0, 2 * sizeof(unsigned)));
+  }
+  if (v.persistent == 2) {
+    // predictor: box of TmaBoxP<tx, ty> over w[0] and w[1] (tx + 2 cells from
+    // an even column, ty + 2 rows); only full interior tiles use it
+    const int bw = (v.tx + 4) & ~1, bh = v.ty + 2;
+    std::vector<CUtensorMap> maps(2 * b->ctx.size());
+    std::vector<int> ok(b->ctx.size(), 0);
+    memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
+    for (size_t q = 0; q < b->ctx.size(); ++q) {
+      const bnz_ctx* c = b->ctx[q];
+      ok[q] = cell_map(c, c->wbuf[0], bw, bh, &maps[2 * q]) && cell_map(c, c->wbuf[1], bw, bh, &maps[2 * q + 1]);
+    }
+    for (FusedTile& t : tA) {
+      const bnz_ctx* c = b->ctx[t.inst];
+      const int ng = c->ng, n0 = c->i2 - c->i1 + 1, n1 = c->j2 - c->j1 + 1;
+      const bool interior = t.x0 - 1 >= ng && t.x0 + t.wx <= ng + n0 - 1 && t.y0 - 1 >= ng &&
+                            t.y0 + t.wy <= ng + n1 - 1;
+      t.tma = ok[t.inst] && interior && t.wx == v.tx && t.wy == v.ty;
+    }
+    if (!b->d_wmaps) CKB(cudaMalloc((void**)&b->d_wmaps, maps.size() * sizeof(CUtensorMap)));
+    CKB(cudaMemcpy(b->d_wmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
   }
   b->ntA = (int)tA.size();
   b->ntB = (int)tB.size();
@@ -1173,6 +1197,7 @@ int bnz_batch_destroy(bnz_batch* b) {
   if (b->d_inst) cudaFree(b->d_inst);
   if (b->d_tiles) cudaFree(b->d_tiles);
   if (b->d_maps) cudaFree(b->d_maps);
+  if (b->d_wmaps) cudaFree(b->d_wmaps);
   if (b->d_queue) cudaFree(b->d_queue);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->cin) cudaStreamSynchronize(b->cin);

@@ -596,45 +596,26 @@ __device__ __forceinline__ void stage_inst(Inst& sI, const Inst* __restrict__ in
   __syncthreads();
 }
 
-// Predictor.  STAGED = 1 copies w^n (tile + one ring, BC-mapped) into shared
-// memory first; STAGED = 0 reads it from global memory in the flux stage.
-template <int TXM, int TYM, int RS, int STAGED>
-__global__ void __launch_bounds__(256, 2) k_pred2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
-                                                   int parity, int lim) {
-  constexpr int RING = STAGED ? 1 : 0;
-  extern __shared__ double smem[];
-  __shared__ Inst sI;
-  const Tile T = tiles[blockIdx.x];
-  stage_inst(sI, insts, T.inst);
-  const Inst& I = sI;
-  const double dtf = I.ds->dt;
-  if (!(dtf > 0.)) return;
-  const double dt = 0.5 * dtf;
+// Everything of the predictor after its input is in place: fluxes (from the
+// staged cells W when SMEMW, else from global memory through the BC map),
+// EMFs, the half-step update, the writes of ws / bs.  sF: fluxes and EMFs,
+// contiguous (x fluxes, y fluxes, E_c, E_e).
+template <int TXM, int TYM, int RS, bool SMEMW>
+__device__ __forceinline__ void pred_tile(const Inst& I, const Tile& T, int parity, int lim, double* sF,
+                                          const SmemCells& Wsm, bool interior, double dt) {
+  using M = Smem<TXM, TYM, 0>;
+  double* sFX = sF;
+  double* sFY = sFX + NF * M::NFX;
+  double* sEC = sFY + NF * M::NFY;
+  double* sEE = sEC + M::NEC;
   Layout L;
   L.set(T.wx, T.wy);
-  double* sFX = smem;
-  double* sFY = sFX + NF * Smem<TXM, TYM, RING>::NFX;
-  double* sEC = sFY + NF * Smem<TXM, TYM, RING>::NFY;
-  double* sEE = sEC + Smem<TXM, TYM, RING>::NEC;
-  double* sW = sEE + Smem<TXM, TYM, RING>::NEE;
   const double* __restrict__ w = I.w[parity];
   const double* __restrict__ b = I.b[parity];
-  // a tile whose one-cell ring lies inside the active range needs no ghost mapping
-  const bool interior = T.x0 - 1 >= I.ng && T.x0 + T.wx <= I.ng + I.N[0] - 1 && T.y0 - 1 >= I.ng &&
-                        T.y0 + T.wy <= I.ng + I.N[1] - 1;
   const AxisMap mx = axis_map(I, 0), my = axis_map(I, 1);
-  Stage S;
-  S.x0 = T.x0 - 1;
-  S.y0 = T.y0 - 1;
-  S.w = T.wx + 2;
-  S.h = T.wy + 2;
   unsigned e = 0;
-  if constexpr (STAGED) {
-    if (interior) stage_cells<false>(I, w, S, sW);
-    else stage_cells<true>(I, w, S, sW);
-    __syncthreads();
-    SmemCells W{sW, S, S.cells()};
-    stage_fluxes<0, RS>(I, T, L, W, b, sFX, sFY, sEC, lim, interior, e);
+  if constexpr (SMEMW) {
+    stage_fluxes<0, RS>(I, T, L, Wsm, b, sFX, sFY, sEC, lim, interior, e);
   } else {
     GlobalCells W{&I, w, mx, my, interior};
     stage_fluxes<0, RS>(I, T, L, W, b, sFX, sFY, sEC, lim, interior, e);
@@ -649,10 +630,10 @@ __global__ void __launch_bounds__(256, 2) k_pred2d(const Inst* __restrict__ inst
     const int cj = dwx.div(t), ci = t - cj * T.wx;
     const int i = T.x0 + ci, j = T.y0 + cj;
     double wn[NM], un[NM];
-    if constexpr (STAGED) {
-      const int cs = S.at(0, i, j);
+    if constexpr (SMEMW) {
+      const int cs = Wsm.S.at(0, i, j);
 #pragma unroll
-      for (int n = 0; n < NM; ++n) wn[n] = sW[n * S.cells() + cs];
+      for (int n = 0; n < NM; ++n) wn[n] = Wsm.sW[n * Wsm.nc + cs];
     } else {
       load_prim_all(I, w, i, j, mx, my, interior, wn);
     }
@@ -674,6 +655,45 @@ __global__ void __launch_bounds__(256, 2) k_pred2d(const Inst* __restrict__ inst
     if (j == jlast) I.bs[I.sv + c + I.nx] = o.byt;
   }
   if (e) atomicOr(I.err, e);
+}
+
+// a tile whose one-cell ring lies inside the active range needs no ghost mapping
+__device__ __forceinline__ bool pred_interior(const Inst& I, const Tile& T) {
+  return T.x0 - 1 >= I.ng && T.x0 + T.wx <= I.ng + I.N[0] - 1 && T.y0 - 1 >= I.ng &&
+         T.y0 + T.wy <= I.ng + I.N[1] - 1;
+}
+
+// Predictor.  STAGED = 1 copies w^n (tile + one ring, BC-mapped) into shared
+// memory first; STAGED = 0 reads it from global memory in the flux stage.
+template <int TXM, int TYM, int RS, int STAGED>
+__global__ void __launch_bounds__(256, 2) k_pred2d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
+                                                   int parity, int lim) {
+  constexpr int RING = STAGED ? 1 : 0;
+  extern __shared__ double smem[];
+  __shared__ Inst sI;
+  const Tile T = tiles[blockIdx.x];
+  stage_inst(sI, insts, T.inst);
+  const Inst& I = sI;
+  const double dtf = I.ds->dt;
+  if (!(dtf > 0.)) return;
+  const bool interior = pred_interior(I, T);
+  // fluxes and EMFs first, then the staged cells
+  double* sW = smem + NF * (Smem<TXM, TYM, RING>::NFX + Smem<TXM, TYM, RING>::NFY) + Smem<TXM, TYM, RING>::NEC +
+               Smem<TXM, TYM, RING>::NEE;
+  Stage S;
+  S.x0 = T.x0 - 1;
+  S.y0 = T.y0 - 1;
+  S.w = T.wx + 2;
+  S.h = T.wy + 2;
+  SmemCells W{sW, S, S.cells()};
+  if constexpr (STAGED) {
+    if (interior) stage_cells<false>(I, I.w[parity], S, sW);
+    else stage_cells<true>(I, I.w[parity], S, sW);
+    __syncthreads();
+    pred_tile<TXM, TYM, RS, true>(I, T, parity, lim, smem, W, interior, 0.5 * dtf);
+  } else {
+    pred_tile<TXM, TYM, RS, false>(I, T, parity, lim, smem, W, interior, 0.5 * dtf);
+  }
 }
 
 __device__ __forceinline__ void copy_tile(const Inst& I, const Tile& T, int parity) {
@@ -968,6 +988,103 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
   }
 }
 
+// Persistent predictor: the same work queue and double buffering as the
+// persistent corrector.  Interior tiles (full TX x TY tiles whose one-cell ring
+// lies inside the active range, so no ghost is read) get w^n on the tile and
+// its ring by TMA; the other tiles read w^n from global memory through the BC
+// map as k_pred2d<.., 0> does.  The box starts at an even column and is
+// TmaBoxP::W cells wide.
+template <int TX, int TY>
+struct TmaBoxP {
+  static constexpr int W = (TX + 4) & ~1;  // TX+2 cells from an even column at or before x0-1
+  static constexpr int H = TY + 2;
+  static constexpr unsigned BYTES = NM * W * H * sizeof(double);
+  static constexpr int BUF = (NM * W * H + 15) / 16 * 16;
+  using M = Smem<TX + 4, TY + 4, 0>;
+  static constexpr size_t smem_bytes =
+      128 + sizeof(double) * (2 * (size_t)BUF + (size_t)NF * (M::NFX + M::NFY) + M::NEC + M::NEE);
+};
+
+template <int TX, int TY>
+__device__ __forceinline__ void issue_w(const Tile& T, const unsigned char* maps, int parity, double* dst,
+                                        unsigned long long* bar) {
+  if (T.tma) {
+    const void* map = maps + ((size_t)T.inst * 2 + parity) * 128;
+    tma::fence_async_shared();
+    tma::arrive_expect(bar, TmaBoxP<TX, TY>::BYTES);
+    tma::load_3d(dst, bar, map, (T.x0 - 1) & ~1, T.y0 - 1, 0);
+  } else {
+    tma::arrive(bar);
+  }
+}
+
+template <int TX, int TY, int RS>
+__global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
+                                                      int ntiles, int parity, int lim,
+                                                      const unsigned char* __restrict__ maps,
+                                                      unsigned* __restrict__ queue) {
+  using B = TmaBoxP<TX, TY>;
+  extern __shared__ __align__(128) double smem_raw[];
+  __shared__ Inst sI;
+  __shared__ Tile sT;
+  __shared__ __align__(8) unsigned long long bar[2];
+  __shared__ int s_tile[2], s_fail;  // tile of iteration k in s_tile[k & 1]
+  double* smem = smem_raw + ((128u - (tma::saddr(smem_raw) & 127u)) & 127u) / sizeof(double);
+  // two staging buffers of B::BUF doubles, then the fluxes and EMFs
+  if (threadIdx.x == 0) {
+    tma::bar_init(&bar[0], 1);
+    tma::bar_init(&bar[1], 1);
+    tma::fence_bar_init();
+    s_fail = 0;
+    const int t0 = (int)atomicAdd(queue, 1u);
+    s_tile[0] = t0;
+    if (t0 < ntiles) {
+      const Tile T0 = tiles[t0];
+      if (T0.tma) tma::prefetch_map(maps + ((size_t)T0.inst * 2 + parity) * 128);
+      issue_w<TX, TY>(T0, maps, parity, smem, &bar[0]);
+    }
+  }
+  __syncthreads();
+  for (int k = 0;; ++k) {
+    const int t = s_tile[k & 1];
+    if (t >= ntiles) break;
+    const int buf = k & 1;
+    if (threadIdx.x == 0) {
+      sT = tiles[t];
+      const int tn = (int)atomicAdd(queue, 1u);
+      s_tile[buf ^ 1] = tn;
+      if (tn < ntiles) issue_w<TX, TY>(tiles[tn], maps, parity, smem + (buf ^ 1) * B::BUF, &bar[buf ^ 1]);
+    }
+    stage_inst(sI, insts, tiles[t].inst);  // ends with a barrier (sT, s_tile visible)
+    const Tile& T = sT;
+    const Inst& I = sI;
+    const unsigned ph = (unsigned)(k >> 1) & 1u;
+    if (threadIdx.x == 0 && !tma::wait(&bar[buf], ph)) s_fail = 1;
+    __syncthreads();
+    if (s_fail) {
+      if (threadIdx.x == 0) {
+        atomicOr(I.err, (unsigned)ERR_TIMEOUT);
+        if (s_tile[buf ^ 1] < ntiles) tma::wait(&bar[buf ^ 1], (unsigned)((k + 1) >> 1) & 1u);
+      }
+      return;
+    }
+    tma::wait(&bar[buf], ph);
+    const double dtf = I.ds->dt;
+    if (dtf > 0.) {
+      Stage S;
+      S.x0 = (T.x0 - 1) & ~1;
+      S.y0 = T.y0 - 1;
+      S.w = B::W;
+      S.h = B::H;
+      SmemCells W{smem + buf * B::BUF, S, S.cells()};
+      if (T.tma) pred_tile<TX + 4, TY + 4, RS, true>(I, T, parity, lim, smem + 2 * B::BUF, W, true, 0.5 * dtf);
+      else pred_tile<TX + 4, TY + 4, RS, false>(I, T, parity, lim, smem + 2 * B::BUF, W, pred_interior(I, T),
+                                                0.5 * dtf);
+    }
+    __syncthreads();  // the tile's buffer, sT and sI are free again
+  }
+}
+
 // Per-instance dt for the step of parity p (new_dt.pyx:117, vanleer.pyx:95-96):
 // FDT_CFL  cour / max of slot p, clipped to tmax;
 // FDT_FIXED dt_fixed (the FIXDT build), clipped to tmax;
@@ -978,7 +1095,7 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
 __global__ void k_dt_batch(const Inst* __restrict__ insts, int n, int parity, double cour, int mode, double dt_fixed,
                            unsigned* queue) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q == 0 && queue) *queue = 0u;  // the persistent corrector's tile counter
+  if (q == 0 && queue) queue[0] = queue[1] = 0u;  // the persistent kernels' tile counters
   if (q >= n) return;
   DtState* ds = insts[q].ds;
   if (mode != FDT_EXPLICIT) {

@@ -315,24 +315,43 @@ void launch_corr(const FusedLaunch& f, int parity) {
   fused::k_corr2d<TX, TY, RS, LIM><<<f.ntB, 256, smB, f.stream>>>(f.insts, f.tilesB, parity, f.charact_proj);
 }
 
+// SM count of the current device (cached per device).
+inline int sm_count() {
+  static int nsm[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (!nsm[dev]) cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
+  return std::max(1, nsm[dev]);
+}
+
 // Persistent corrector: (SMs x resident blocks) blocks, never more than tiles.
 template <int TX, int TY, int RS, int LIM>
 void launch_corr_pq(const FusedLaunch& f, int parity) {
   constexpr size_t sm = fused::TmaBox<TX, TY>::smem_bytes;
   static int per_sm = 0;
-  static int nsm[64] = {0};
   if (!per_sm) {
     cudaFuncSetAttribute(fused::k_corr2d_pq<TX, TY, RS, LIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused::k_corr2d_pq<TX, TY, RS, LIM>, 256, sm);
     if (per_sm < 1) per_sm = 1;
   }
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64) dev = 0;
-  if (!nsm[dev]) cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
-  const int grid = std::min(f.ntB, per_sm * std::max(1, nsm[dev]));
+  const int grid = std::min(f.ntB, per_sm * sm_count());
   fused::k_corr2d_pq<TX, TY, RS, LIM><<<grid, 256, sm, f.stream>>>(f.insts, f.tilesB, f.ntB, parity,
                                                                     f.charact_proj, f.wsmaps, f.queue);
+}
+
+template <int TX, int TY, int RS>
+void launch_pred_pq(const FusedLaunch& f, int parity) {
+  constexpr size_t sm = fused::TmaBoxP<TX, TY>::smem_bytes;
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaFuncSetAttribute(fused::k_pred2d_pq<TX, TY, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused::k_pred2d_pq<TX, TY, RS>, 256, sm);
+    if (per_sm < 1) per_sm = 1;
+  }
+  const int grid = std::min(f.ntA, per_sm * sm_count());
+  fused::k_pred2d_pq<TX, TY, RS><<<grid, 256, sm, f.stream>>>(f.insts, f.tilesA, f.ntA, parity, f.limiter, f.wmaps,
+                                                              f.queue + 1);
 }
 
 template <int TX, int TY, int RS, int LIM>
@@ -357,7 +376,15 @@ void launch_variant(const FusedLaunch& f, int parity) {
     attrs = true;
   }
   if (f.events) cudaEventRecord(f.events[1], f.stream);
-  fused::k_pred2d<TXA, TYA, RS, STAGED><<<f.ntA, 256, smA, f.stream>>>(f.insts, f.tilesA, parity, f.limiter);
+  bool done = false;
+  if constexpr (TX == 15 && TY == 14 && STAGED == 0) {
+    if (f.wmaps && f.queue) {
+      launch_pred_pq<TX, TY, RS>(f, parity);
+      done = true;
+    }
+  }
+  if (!done)
+    fused::k_pred2d<TXA, TYA, RS, STAGED><<<f.ntA, 256, smA, f.stream>>>(f.insts, f.tilesA, parity, f.limiter);
   if (f.events) cudaEventRecord(f.events[2], f.stream);
   // the limiter is a compile-time choice of the corrector (reconstr_c.h:28-44)
   if (f.limiter == dev::LIM_MC) launch_corr_any<TX, TY, RS, dev::LIM_MC>(f, parity);
@@ -378,6 +405,7 @@ void launch_pred_corr(const FusedLaunch& f, int parity) {
       case 5: launch_variant<15, 14, RS, 1>(f, parity); return;
       case 6: launch_variant<15, 14, RS, 0>(f, parity); return;  // persistent corrector when maps are given
       case 7: launch_variant<15, 14, RS, 1>(f, parity); return;
+      case 8: launch_variant<15, 14, RS, 0>(f, parity); return;  // persistent predictor too
       default: break;
     }
   }
