@@ -39,9 +39,9 @@ BYTES_PER_ZONE = 192  # 9 conserved + 3 face-B doubles read once and written onc
 # 12 per zone it covers (active zones plus two ghost rings).
 CORR_BYTES_PER_ZONE = 288
 # DRAM bytes per active zone of one corrector launch (dram__bytes_read.sum +
-# dram__bytes_write.sum), from the ncu capture summarised in
-# profiles/k_corr2d_blast_batch.md (16-instance capture, scaled per zone).
-CORR_TRAFFIC_PER_ZONE = 269.1
+# dram__bytes_write.sum), from an ncu capture of the persistent corrector on
+# the first 16 instances of this batch (scaled per zone).
+CORR_TRAFFIC_PER_ZONE = 268.6
 
 
 def parse():
@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--path", default="batch", choices=["batch", "plain", "fused"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-instance comparison")
     ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--variant", type=int, default=None, help="fixed kernel variant instead of the autotuner's choice")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -269,12 +270,17 @@ def run_ours(args, rank, world, dist):
     eng, ctxs, step, count = make_engine(args.path, batch, stream)
     tune = None
     if args.path == "batch":
-        # autotuner: tile shape / staging on this workload (state restored after each trial)
-        from bonzo_b200 import autotune
-        best, ms = autotune.tune_batch(eng, [q["N"] for q, _, _, _ in batch], METHOD["rsolver"],
-                                       METHOD["limiter"], steps=2, use_cache=False)
         from bonzo_b200._lib import variant_label, variants
         vs = variants()
+        if args.variant is not None:
+            # a fixed variant (profiling runs: the autotuner's choice under a profiler is not the real one)
+            eng.set_variant(args.variant)
+            best, ms = args.variant, {}
+        else:
+            # autotuner: tile shape / staging on this workload (state restored after each trial)
+            from bonzo_b200 import autotune
+            best, ms = autotune.tune_batch(eng, [q["N"] for q, _, _, _ in batch], METHOD["rsolver"],
+                                           METHOD["limiter"], steps=2, use_cache=False)
         tune = {"chosen": {"tile": "%dx%d" % vs[best][:2], "staged_predictor": bool(vs[best][2]),
                            "persistent": ["none", "corrector", "predictor and corrector"][vs[best][3]]},
                 "ms_per_step": {variant_label(vs[v]): round(t, 4)
@@ -342,7 +348,9 @@ def run_ours(args, rank, world, dist):
         traffic = None if CORR_TRAFFIC_PER_ZONE is None else int(CORR_TRAFFIC_PER_ZONE * zones)
         roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_src,
-                    "kernel": "k_corr2d (corrector, one launch covers every instance)",
+                    "kernel": ("k_corr2d_pq (persistent corrector, one launch covers every instance)"
+                               if tune and vs[best][3] else
+                               "k_corr2d (corrector, one launch covers every instance)"),
                     "algorithmic_bytes_per_launch": CORR_BYTES_PER_ZONE * zones,
                     "ms_per_launch": round(kms["corrector"], 4),
                     "kernel_ms_per_launch": {k: round(v, 4) for k, v in kms.items()},
