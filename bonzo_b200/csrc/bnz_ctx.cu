@@ -241,6 +241,24 @@ void make_tiles(int inst, int N0, int N1, int ng, bool pred, int tx, int ty, std
     }
 }
 
+// Predictor tiles of the persistent predictor: the predictor range (cells 1 ..
+// Ntot-2 of each axis) in plain tx x ty steps from cell 1, so no tile is
+// larger than tx x ty.
+void make_tiles_uniform(int inst, int N0, int N1, int ng, int tx, int ty, std::vector<FusedTile>& out) {
+  const int hi0 = N0 + 2 * ng - 2, hi1 = N1 + 2 * ng - 2;
+  for (int y = 1; y <= hi1; y += ty)
+    for (int x = 1; x <= hi0; x += tx) {
+      FusedTile ft;
+      ft.inst = inst;
+      ft.x0 = x;
+      ft.y0 = y;
+      ft.wx = std::min(tx, hi0 - x + 1);
+      ft.wy = std::min(ty, hi1 - y + 1);
+      ft.tma = 0;
+      out.push_back(ft);
+    }
+}
+
 FusedInst make_inst(const bnz_ctx* c) {
   FusedInst I;
   memset(&I, 0, sizeof I);
@@ -1065,17 +1083,17 @@ EncodeTiledFn encode_tiled() {
   return fn;
 }
 
-// A TMA box of (x, y, field) = (bw, bh, 9) doubles over one 9-field cell
-// array of the instance (ws or w[p]), bw even, used from even columns.  A map
+// A TMA box of (x, y, field) = (bw, bh, nf) doubles over one nf-field array of
+// the instance (ws, w[p] or b[p]), bw even, used from even columns.  A map
 // needs 16-byte row and field strides, so instances with odd Ntot_x get none
 // (their tiles stage with plain loads).  Returns whether the map was made.
-bool cell_map(const bnz_ctx* c, const double* base, int bw, int bh, CUtensorMap* out) {
+bool cell_map(const bnz_ctx* c, const double* base, int nf, int bw, int bh, CUtensorMap* out) {
   EncodeTiledFn enc = encode_tiled();
   const int nx = c->Ntot[0], ny = c->Ntot[1];
   if (!enc || (nx & 1) || ((uintptr_t)base & 15)) return false;
-  const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, 9};
+  const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nf};
   const cuuint64_t strides[2] = {(cuuint64_t)nx * sizeof(double), (cuuint64_t)nx * ny * sizeof(double)};
-  const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 9};
+  const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, (cuuint32_t)nf};
   const cuuint32_t es[3] = {1, 1, 1};
   return enc(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)base, dims, strides, box, es,
              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -1090,7 +1108,8 @@ int batch_build_tiles(bnz_batch* b) {
   b->offB.assign(1, 0);
   for (int q = 0; q < (int)b->ctx.size(); ++q) {
     const bnz_ctx* c = b->ctx[q];
-    make_tiles(q, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->ng, true, v.tx, v.ty, tA);
+    if (v.persistent == 2) make_tiles_uniform(q, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->ng, v.tx, v.ty, tA);
+    else make_tiles(q, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->ng, true, v.tx, v.ty, tA);
     make_tiles(q, c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->ng, false, v.tx, v.ty, tB);
     b->offA.push_back((int)tA.size());
     b->offB.push_back((int)tB.size());
@@ -1102,7 +1121,7 @@ int batch_build_tiles(bnz_batch* b) {
     std::vector<CUtensorMap> maps(b->ctx.size());
     std::vector<int> ok(b->ctx.size(), 0);
     memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
-    for (size_t q = 0; q < b->ctx.size(); ++q) ok[q] = cell_map(b->ctx[q], b->ctx[q]->cons_s, bw, bh, &maps[q]);
+    for (size_t q = 0; q < b->ctx.size(); ++q) ok[q] = cell_map(b->ctx[q], b->ctx[q]->cons_s, 9, bw, bh, &maps[q]);
     for (FusedTile& t : tB) t.tma = ok[t.inst];
     if (!b->d_maps) CKB(cudaMalloc((void**)&b->d_maps, maps.size() * sizeof(CUtensorMap)));
     if (!b->d_queue) CKB(cudaMalloc((void**)&b->d_queue, 2 * sizeof(unsigned)));
@@ -1110,15 +1129,17 @@ int batch_build_tiles(bnz_batch* b) {
     CKB(cudaMemset(b->d_queue, 0, 2 * sizeof(unsigned)));
   }
   if (v.persistent == 2) {
-    // predictor: box of TmaBoxP<tx, ty> over w[0] and w[1] (tx + 2 cells from
-    // an even column, ty + 2 rows); only full interior tiles use it
+    // predictor: boxes of TmaBoxP<tx, ty> over w[0], w[1] (9 fields) and
+    // b[0], b[1] (3 faces): tx + 2 cells from an even column, ty + 2 rows;
+    // only full interior tiles use them
     const int bw = (v.tx + 4) & ~1, bh = v.ty + 2;
-    std::vector<CUtensorMap> maps(2 * b->ctx.size());
+    std::vector<CUtensorMap> maps(4 * b->ctx.size());
     std::vector<int> ok(b->ctx.size(), 0);
     memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
     for (size_t q = 0; q < b->ctx.size(); ++q) {
       const bnz_ctx* c = b->ctx[q];
-      ok[q] = cell_map(c, c->wbuf[0], bw, bh, &maps[2 * q]) && cell_map(c, c->wbuf[1], bw, bh, &maps[2 * q + 1]);
+      ok[q] = cell_map(c, c->wbuf[0], 9, bw, bh, &maps[4 * q]) && cell_map(c, c->wbuf[1], 9, bw, bh, &maps[4 * q + 1]) &&
+              cell_map(c, c->bbuf[0], 3, bw, bh, &maps[4 * q + 2]) && cell_map(c, c->bbuf[1], 3, bw, bh, &maps[4 * q + 3]);
     }
     for (FusedTile& t : tA) {
       const bnz_ctx* c = b->ctx[t.inst];

@@ -252,6 +252,11 @@ struct SmemCells {
   // value at (i, j) shifted by `o` cells along the axis with stride `st` (1: x, S.w: y)
   __device__ __forceinline__ const double* ptr(int n, int i, int j) const { return sW + n * nc + S.at(0, i, j); }
   __device__ __forceinline__ int stride(int ax) const { return ax == 0 ? 1 : S.w; }
+  __device__ __forceinline__ void load_all(int i, int j, double* out) const {
+    const int c = S.at(0, i, j);
+#pragma unroll
+    for (int n = 0; n < NM; ++n) out[n] = sW[n * nc + c];
+  }
 };
 
 struct GlobalCells {
@@ -266,19 +271,42 @@ struct GlobalCells {
     double v = w[n * I->sv + (long long)sj * I->nx + si];
     return ((fx && (n == VX || n == BX)) || (fy && (n == VY || n == BY))) ? -v : v;
   }
+  __device__ __forceinline__ void load_all(int i, int j, double* out) const {
+    load_prim_all(*I, w, i, j, mx, my, interior, out);
+  }
+};
+
+// Face readers of the predictor: global memory through the BC map, or the
+// faces a persistent predictor staged in shared memory (interior tiles).
+struct GlobalFaces {
+  const Inst* I;
+  const double* b;
+  AxisMap mx, my;
+  bool interior;
+  template <int COMP>
+  __device__ __forceinline__ double get(int i, int j) const {
+    return load_face<COMP>(*I, b, i, j, mx, my, interior);
+  }
+};
+
+struct SmemFaces {
+  const double* sB;
+  Stage S;
+  template <int COMP>
+  __device__ __forceinline__ double get(int i, int j) const {
+    return sB[COMP * S.cells() + S.at(0, i, j)];
+  }
 };
 
 // ---------------------------------------------------------------------------
-// Stage 1 of both kernels: interface fluxes and cell-centred EMF.
-// ORDER 0 (predictor): donor cell, normal B from b with the BC map.
-// ORDER 1 (corrector): PLM from staged ws, normal B from bs.
+// Stage 1 of the predictor: donor-cell interface fluxes and the cell-centred
+// EMF.  (The corrector's PLM flux stage is stage_fluxes_plm below.)
 // ---------------------------------------------------------------------------
 
-template <int ORDER, int RS, class Cells>
+template <int RS, class Cells, class Faces>
 __device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const Layout& L, const Cells& W,
-                                             const double* __restrict__ b, double* sFX, double* sFY, double* sEC,
-                                             int lim, bool interior, unsigned& err) {
-  const AxisMap mx = axis_map(I, 0), my = axis_map(I, 1);
+                                             const Faces& F, double* sFX, double* sFY, double* sEC,
+                                             unsigned& err) {
   const int total = L.nfx + L.nfy + L.nec;
   FastDiv dx1, dx2;
   dx1.set(L.wx + 1);
@@ -293,18 +321,10 @@ __device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const
 #pragma unroll
       for (int n = 0; n < NM; ++n) {
         if (n == BX) continue;
-        if constexpr (ORDER == 0) {
-          wL[n] = W.get(n, i - 1, j);
-          wR[n] = W.get(n, i, j);
-        } else {
-          const double* a = W.ptr(n, i, j);
-          double wm2 = a[-2], wm1 = a[-1], w0 = a[0], wp1 = a[1];
-          wL[n] = wm1 + plain::half_slope_rt(lim, wm2, wm1, w0);
-          wR[n] = w0 - plain::half_slope_rt(lim, wm1, w0, wp1);
-        }
+        wL[n] = W.get(n, i - 1, j);
+        wR[n] = W.get(n, i, j);
       }
-      if (ORDER == 0) wL[BX] = wR[BX] = load_face<0>(I, b, i, j, mx, my, interior);
-      else wL[BX] = wR[BX] = b[(long long)j * I.nx + i];
+      wL[BX] = wR[BX] = F.template get<0>(i, j);
       double f[NM];
       riemann<RS>(f, wL, wR, I.gam, err);
       const int qq = L.fx(fi, fj);
@@ -323,19 +343,10 @@ __device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const
       for (int n = 0; n < NM; ++n) {
         if (n == BX) continue;
         const int gv = plain::perm<1>(n);
-        if constexpr (ORDER == 0) {
-          wL[n] = W.get(gv, i, j - 1);
-          wR[n] = W.get(gv, i, j);
-        } else {
-          const double* a = W.ptr(gv, i, j);
-          const int sy = W.stride(1);
-          double wm2 = a[-2 * sy], wm1 = a[-sy], w0 = a[0], wp1 = a[sy];
-          wL[n] = wm1 + plain::half_slope_rt(lim, wm2, wm1, w0);
-          wR[n] = w0 - plain::half_slope_rt(lim, wm1, w0, wp1);
-        }
+        wL[n] = W.get(gv, i, j - 1);
+        wR[n] = W.get(gv, i, j);
       }
-      if (ORDER == 0) wL[BX] = wR[BX] = load_face<1>(I, b, i, j, mx, my, interior);
-      else wL[BX] = wR[BX] = b[I.sv + (long long)j * I.nx + i];
+      wL[BX] = wR[BX] = F.template get<1>(i, j);
       double f[NM];
       riemann<RS>(f, wL, wR, I.gam, err);
       // local -> global (godunov.pyx:297-324 for the y sweep)
@@ -596,13 +607,13 @@ __device__ __forceinline__ void stage_inst(Inst& sI, const Inst* __restrict__ in
   __syncthreads();
 }
 
-// Everything of the predictor after its input is in place: fluxes (from the
-// staged cells W when SMEMW, else from global memory through the BC map),
+// Everything of the predictor after its input is in place: fluxes from the
+// cells W and faces F (shared memory, or global memory through the BC map),
 // EMFs, the half-step update, the writes of ws / bs.  sF: fluxes and EMFs,
 // contiguous (x fluxes, y fluxes, E_c, E_e).
-template <int TXM, int TYM, int RS, bool SMEMW>
-__device__ __forceinline__ void pred_tile(const Inst& I, const Tile& T, int parity, int lim, double* sF,
-                                          const SmemCells& Wsm, bool interior, double dt) {
+template <int TXM, int TYM, int RS, class Cells, class Faces>
+__device__ __forceinline__ void pred_tile(const Inst& I, const Tile& T, double* sF, const Cells& W, const Faces& F,
+                                          double dt) {
   using M = Smem<TXM, TYM, 0>;
   double* sFX = sF;
   double* sFY = sFX + NF * M::NFX;
@@ -610,16 +621,8 @@ __device__ __forceinline__ void pred_tile(const Inst& I, const Tile& T, int pari
   double* sEE = sEC + M::NEC;
   Layout L;
   L.set(T.wx, T.wy);
-  const double* __restrict__ w = I.w[parity];
-  const double* __restrict__ b = I.b[parity];
-  const AxisMap mx = axis_map(I, 0), my = axis_map(I, 1);
   unsigned e = 0;
-  if constexpr (SMEMW) {
-    stage_fluxes<0, RS>(I, T, L, Wsm, b, sFX, sFY, sEC, lim, interior, e);
-  } else {
-    GlobalCells W{&I, w, mx, my, interior};
-    stage_fluxes<0, RS>(I, T, L, W, b, sFX, sFY, sEC, lim, interior, e);
-  }
+  stage_fluxes<RS>(I, T, L, W, F, sFX, sFY, sEC, e);
   __syncthreads();
   stage_emf(L, sFX, sFY, sEC, sEE);
   __syncthreads();
@@ -630,19 +633,13 @@ __device__ __forceinline__ void pred_tile(const Inst& I, const Tile& T, int pari
     const int cj = dwx.div(t), ci = t - cj * T.wx;
     const int i = T.x0 + ci, j = T.y0 + cj;
     double wn[NM], un[NM];
-    if constexpr (SMEMW) {
-      const int cs = Wsm.S.at(0, i, j);
-#pragma unroll
-      for (int n = 0; n < NM; ++n) wn[n] = Wsm.sW[n * Wsm.nc + cs];
-    } else {
-      load_prim_all(I, w, i, j, mx, my, interior, wn);
-    }
+    W.load_all(i, j, wn);
     prim2cons(un, wn, I.gam);
-    double bxl0 = load_face<0>(I, b, i, j, mx, my, interior);
-    double bxr0 = load_face<0>(I, b, i + 1, j, mx, my, interior);
-    double byb0 = load_face<1>(I, b, i, j, mx, my, interior);
-    double byt0 = load_face<1>(I, b, i, j + 1, mx, my, interior);
-    double bz0 = load_face<2>(I, b, i, j, mx, my, interior);
+    double bxl0 = F.template get<0>(i, j);
+    double bxr0 = F.template get<0>(i + 1, j);
+    double byb0 = F.template get<1>(i, j);
+    double byt0 = F.template get<1>(i, j + 1);
+    double bz0 = F.template get<2>(i, j);
     CellOut o;
     stage_cell(I, L, T, ci, cj, un, wn, bxl0, bxr0, byb0, byt0, bz0, sFX, sFY, sEE, dt, o);
     const long long c = (long long)j * I.nx + i;
@@ -685,15 +682,18 @@ __global__ void __launch_bounds__(256, 2) k_pred2d(const Inst* __restrict__ inst
   S.y0 = T.y0 - 1;
   S.w = T.wx + 2;
   S.h = T.wy + 2;
-  SmemCells W{sW, S, S.cells()};
+  const GlobalFaces F{&I, I.b[parity], axis_map(I, 0), axis_map(I, 1), interior};
   if constexpr (STAGED) {
     if (interior) stage_cells<false>(I, I.w[parity], S, sW);
     else stage_cells<true>(I, I.w[parity], S, sW);
     __syncthreads();
-    pred_tile<TXM, TYM, RS, true>(I, T, parity, lim, smem, W, interior, 0.5 * dtf);
+    const SmemCells W{sW, S, S.cells()};
+    pred_tile<TXM, TYM, RS>(I, T, smem, W, F, 0.5 * dtf);
   } else {
-    pred_tile<TXM, TYM, RS, false>(I, T, parity, lim, smem, W, interior, 0.5 * dtf);
+    const GlobalCells W{&I, I.w[parity], axis_map(I, 0), axis_map(I, 1), interior};
+    pred_tile<TXM, TYM, RS>(I, T, smem, W, F, 0.5 * dtf);
   }
+  (void)lim;
 }
 
 __device__ __forceinline__ void copy_tile(const Inst& I, const Tile& T, int parity) {
@@ -989,30 +989,38 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
 }
 
 // Persistent predictor: the same work queue and double buffering as the
-// persistent corrector.  Interior tiles (full TX x TY tiles whose one-cell ring
-// lies inside the active range, so no ghost is read) get w^n on the tile and
-// its ring by TMA; the other tiles read w^n from global memory through the BC
-// map as k_pred2d<.., 0> does.  The box starts at an even column and is
+// persistent corrector.  Its tiles cover the predictor range (cells 1 ..
+// Ntot-2) in plain tx x ty steps, so none is larger than tx x ty.  Interior
+// tiles (full tiles whose one-cell ring lies inside the active range, so no
+// ghost is read) get w^n (9 fields) and b^n (3 faces) on the tile and its ring
+// by two TMA loads into one buffer; the other tiles read them from global
+// memory through the BC map.  The boxes start at an even column and are
 // TmaBoxP::W cells wide.
 template <int TX, int TY>
 struct TmaBoxP {
   static constexpr int W = (TX + 4) & ~1;  // TX+2 cells from an even column at or before x0-1
   static constexpr int H = TY + 2;
-  static constexpr unsigned BYTES = NM * W * H * sizeof(double);
-  static constexpr int BUF = (NM * W * H + 15) / 16 * 16;
-  using M = Smem<TX + 4, TY + 4, 0>;
+  static constexpr int CELLS = W * H;
+  static constexpr unsigned WBYTES = NM * CELLS * sizeof(double);
+  static constexpr unsigned BYTES = (NM + 3) * CELLS * sizeof(double);
+  static constexpr int BUF = ((NM + 3) * CELLS + 15) / 16 * 16;
+  static_assert(WBYTES % 128 == 0, "the face box must start on a 128-byte boundary");
+  using M = Smem<TX, TY, 0>;
   static constexpr size_t smem_bytes =
       128 + sizeof(double) * (2 * (size_t)BUF + (size_t)NF * (M::NFX + M::NFY) + M::NEC + M::NEE);
 };
 
+// maps: 4 per instance, w[0], w[1], b[0], b[1]
 template <int TX, int TY>
-__device__ __forceinline__ void issue_w(const Tile& T, const unsigned char* maps, int parity, double* dst,
-                                        unsigned long long* bar) {
+__device__ __forceinline__ void issue_wb(const Tile& T, const unsigned char* maps, int parity, double* dst,
+                                         unsigned long long* bar) {
   if (T.tma) {
-    const void* map = maps + ((size_t)T.inst * 2 + parity) * 128;
+    const unsigned char* m = maps + (size_t)T.inst * 4 * 128;
+    const int x = (T.x0 - 1) & ~1, y = T.y0 - 1;
     tma::fence_async_shared();
     tma::arrive_expect(bar, TmaBoxP<TX, TY>::BYTES);
-    tma::load_3d(dst, bar, map, (T.x0 - 1) & ~1, T.y0 - 1, 0);
+    tma::load_3d(dst, bar, m + parity * 128, x, y, 0);
+    tma::load_3d(dst + NM * TmaBoxP<TX, TY>::CELLS, bar, m + (2 + parity) * 128, x, y, 0);
   } else {
     tma::arrive(bar);
   }
@@ -1020,8 +1028,7 @@ __device__ __forceinline__ void issue_w(const Tile& T, const unsigned char* maps
 
 template <int TX, int TY, int RS>
 __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
-                                                      int ntiles, int parity, int lim,
-                                                      const unsigned char* __restrict__ maps,
+                                                      int ntiles, int parity, const unsigned char* __restrict__ maps,
                                                       unsigned* __restrict__ queue) {
   using B = TmaBoxP<TX, TY>;
   extern __shared__ __align__(128) double smem_raw[];
@@ -1040,8 +1047,11 @@ __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ i
     s_tile[0] = t0;
     if (t0 < ntiles) {
       const Tile T0 = tiles[t0];
-      if (T0.tma) tma::prefetch_map(maps + ((size_t)T0.inst * 2 + parity) * 128);
-      issue_w<TX, TY>(T0, maps, parity, smem, &bar[0]);
+      if (T0.tma) {
+        tma::prefetch_map(maps + ((size_t)T0.inst * 4 + parity) * 128);
+        tma::prefetch_map(maps + ((size_t)T0.inst * 4 + 2 + parity) * 128);
+      }
+      issue_wb<TX, TY>(T0, maps, parity, smem, &bar[0]);
     }
   }
   __syncthreads();
@@ -1053,7 +1063,7 @@ __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ i
       sT = tiles[t];
       const int tn = (int)atomicAdd(queue, 1u);
       s_tile[buf ^ 1] = tn;
-      if (tn < ntiles) issue_w<TX, TY>(tiles[tn], maps, parity, smem + (buf ^ 1) * B::BUF, &bar[buf ^ 1]);
+      if (tn < ntiles) issue_wb<TX, TY>(tiles[tn], maps, parity, smem + (buf ^ 1) * B::BUF, &bar[buf ^ 1]);
     }
     stage_inst(sI, insts, tiles[t].inst);  // ends with a barrier (sT, s_tile visible)
     const Tile& T = sT;
@@ -1071,15 +1081,22 @@ __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ i
     tma::wait(&bar[buf], ph);
     const double dtf = I.ds->dt;
     if (dtf > 0.) {
-      Stage S;
-      S.x0 = (T.x0 - 1) & ~1;
-      S.y0 = T.y0 - 1;
-      S.w = B::W;
-      S.h = B::H;
-      SmemCells W{smem + buf * B::BUF, S, S.cells()};
-      if (T.tma) pred_tile<TX + 4, TY + 4, RS, true>(I, T, parity, lim, smem + 2 * B::BUF, W, true, 0.5 * dtf);
-      else pred_tile<TX + 4, TY + 4, RS, false>(I, T, parity, lim, smem + 2 * B::BUF, W, pred_interior(I, T),
-                                                0.5 * dtf);
+      if (T.tma) {
+        Stage S;
+        S.x0 = (T.x0 - 1) & ~1;
+        S.y0 = T.y0 - 1;
+        S.w = B::W;
+        S.h = B::H;
+        const double* sW = smem + buf * B::BUF;
+        const SmemCells W{sW, S, S.cells()};
+        const SmemFaces F{sW + NM * B::CELLS, S};
+        pred_tile<TX, TY, RS>(I, T, smem + 2 * B::BUF, W, F, 0.5 * dtf);
+      } else {
+        const bool interior = pred_interior(I, T);
+        const GlobalCells W{&I, I.w[parity], axis_map(I, 0), axis_map(I, 1), interior};
+        const GlobalFaces F{&I, I.b[parity], axis_map(I, 0), axis_map(I, 1), interior};
+        pred_tile<TX, TY, RS>(I, T, smem + 2 * B::BUF, W, F, 0.5 * dtf);
+      }
     }
     __syncthreads();  // the tile's buffer, sT and sI are free again
   }

@@ -350,7 +350,7 @@ void launch_pred_pq(const FusedLaunch& f, int parity) {
     if (per_sm < 1) per_sm = 1;
   }
   const int grid = std::min(f.ntA, per_sm * sm_count());
-  fused::k_pred2d_pq<TX, TY, RS><<<grid, 256, sm, f.stream>>>(f.insts, f.tilesA, f.ntA, parity, f.limiter, f.wmaps,
+  fused::k_pred2d_pq<TX, TY, RS><<<grid, 256, sm, f.stream>>>(f.insts, f.tilesA, f.ntA, parity, f.wmaps,
                                                               f.queue + 1);
 }
 
