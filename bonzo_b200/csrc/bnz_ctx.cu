@@ -1116,12 +1116,21 @@ int batch_build_tiles(bnz_batch* b) {
   }
   if (v.persistent) {
     static_assert(sizeof(CUtensorMap) == 128, "tensor maps are 128 bytes");
-    // box of TmaBox<tx, ty> (bnz_fused.cuh): tx + 4 cells from an even column, ty + 4 rows
+    // 5 maps per instance (TmaBox<tx, ty> in bnz_fused.cuh): ws with tx + 4
+    // cells from an even column and ty + 4 rows; w[0], w[1] (9 fields) and
+    // b[0], b[1] (3 faces) with tx + 1 positions from an even column and ty + 1 rows
     const int bw = (v.tx + 6) & ~1, bh = v.ty + 4;
-    std::vector<CUtensorMap> maps(b->ctx.size());
+    const int cw = (v.tx + 3) & ~1, ch = v.ty + 1;
+    std::vector<CUtensorMap> maps(5 * b->ctx.size());
     std::vector<int> ok(b->ctx.size(), 0);
     memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
-    for (size_t q = 0; q < b->ctx.size(); ++q) ok[q] = cell_map(b->ctx[q], b->ctx[q]->cons_s, 9, bw, bh, &maps[q]);
+    for (size_t q = 0; q < b->ctx.size(); ++q) {
+      const bnz_ctx* c = b->ctx[q];
+      CUtensorMap* m = &maps[5 * q];
+      ok[q] = cell_map(c, c->cons_s, 9, bw, bh, &m[0]) && cell_map(c, c->wbuf[0], 9, cw, ch, &m[1]) &&
+              cell_map(c, c->wbuf[1], 9, cw, ch, &m[2]) && cell_map(c, c->bbuf[0], 3, cw, ch, &m[3]) &&
+              cell_map(c, c->bbuf[1], 3, cw, ch, &m[4]);
+    }
     for (FusedTile& t : tB) t.tma = ok[t.inst];
     if (!b->d_maps) CKB(cudaMalloc((void**)&b->d_maps, maps.size() * sizeof(CUtensorMap)));
     if (!b->d_queue) CKB(cudaMalloc((void**)&b->d_queue, 2 * sizeof(unsigned)));

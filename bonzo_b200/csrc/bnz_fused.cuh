@@ -713,28 +713,89 @@ __device__ __forceinline__ void copy_tile(const Inst& I, const Tile& T, int pari
   }
 }
 
-// Everything of the corrector after its input cells are staged: PLM fluxes,
-// EMFs, the cell update, the writes of w^(n+1) / b^(n+1) and the tile's CFL
-// maximum folded into the instance's slot.
-// sF: fluxes, EMFs and slopes, contiguous (x fluxes, y fluxes, E_c, E_e, slopes).
+// Readers of the corrector's cell-update inputs: w^n and b^n of the cell
+// (ghost faces through the BC map) and the half-step state the source terms
+// use.  CorrInGlobal reads global memory; CorrInSmem reads w^n / b^n a
+// persistent corrector staged by TMA over the tile (edge cells still take
+// their faces through the map), and the source-term state from global ws.
+struct CorrInGlobal {
+  const Inst* I;
+  const double* w;
+  const double* b;
+  const SmemCells* W;
+  __device__ __forceinline__ void wn(int i, int j, double* out) const {
+    const long long c = (long long)j * I->nx + i;
+#pragma unroll
+    for (int n = 0; n < NM; ++n) out[n] = w[n * I->sv + c];
+  }
+  __device__ __forceinline__ double face(int comp, int i, int j, bool edge, const AxisMap& mx,
+                                         const AxisMap& my) const {
+    if (comp == 0) return load_face<0>(*I, b, i, j, mx, my, !edge);
+    if (comp == 1) return load_face<1>(*I, b, i, j, mx, my, !edge);
+    return b[2 * I->sv + (long long)j * I->nx + i];
+  }
+  __device__ __forceinline__ double half(int n, int i, int j) const {
+    return W ? W->get(n, i, j) : I->ws[n * I->sv + (long long)j * I->nx + i];
+  }
+};
+
+struct CorrInSmem {
+  const Inst* I;
+  const double* b;   // global b^n, for the mapped faces of edge cells
+  const double* sw;  // staged w^n (9 fields), layout S
+  const double* sb;  // staged b^n (3 faces), layout S
+  Stage S;
+  __device__ __forceinline__ void wn(int i, int j, double* out) const {
+    const int c = S.at(0, i, j);
+#pragma unroll
+    for (int n = 0; n < NM; ++n) out[n] = sw[n * S.cells() + c];
+  }
+  __device__ __forceinline__ double face(int comp, int i, int j, bool edge, const AxisMap& mx,
+                                         const AxisMap& my) const {
+    if (edge && comp == 0) return load_face<0>(*I, b, i, j, mx, my, false);
+    if (edge && comp == 1) return load_face<1>(*I, b, i, j, mx, my, false);
+    return sb[comp * S.cells() + S.at(0, i, j)];
+  }
+  __device__ __forceinline__ double half(int n, int i, int j) const {
+    return I->ws[n * I->sv + (long long)j * I->nx + i];
+  }
+};
+
+// The corrector's flux stages: PLM fluxes of every face of the tile and the
+// cell-centred EMFs, into sF (x fluxes, y fluxes, E_c, E_e, slopes).  Ends
+// with a barrier: the staged half-step cells are no longer needed after it.
 template <int TXM, int TYM, int RS, int LIM>
-__device__ __forceinline__ void corr_tile(const Inst& I, const Tile& T, int parity, int cp, const SmemCells& W,
-                                          double* sF, double* red, double dt) {
+__device__ __forceinline__ void corr_fluxes(const Inst& I, const Tile& T, int cp, const SmemCells& W, double* sF) {
+  using M = Smem<TXM, TYM, 2>;
+  double* sFX = sF;
+  double* sFY = sFX + NF * M::NFX;
+  double* sEC = sFY + NF * M::NFY;
+  double* sD = sEC + M::NEC + M::NEE;
+  Layout L;
+  L.set(T.wx, T.wy);
+  unsigned e = 0;
+  stage_fluxes_plm<LIM, RS>(I, T, L, W, I.bs, sFX, sFY, sEC, sD, cp, e);
+  if (e) atomicOr(I.err, e);
+  __syncthreads();
+}
+
+// Corner EMFs, then per cell the full-step update, the writes of w^(n+1) /
+// b^(n+1) and the tile's CFL maximum folded into the instance's slot.
+template <int TXM, int TYM, class In>
+__device__ __forceinline__ void corr_cells(const Inst& I, const Tile& T, int parity, const In& in, double* sF,
+                                           double* red, double dt, bool emf_done) {
   using M = Smem<TXM, TYM, 2>;
   double* sFX = sF;
   double* sFY = sFX + NF * M::NFX;
   double* sEC = sFY + NF * M::NFY;
   double* sEE = sEC + M::NEC;
-  double* sD = sEE + M::NEE;
   Layout L;
   L.set(T.wx, T.wy);
+  if (!emf_done) {
+    stage_emf(L, sFX, sFY, sEC, sEE);
+    __syncthreads();
+  }
   unsigned e = 0;
-  stage_fluxes_plm<LIM, RS>(I, T, L, W, I.bs, sFX, sFY, sEC, sD, cp, e);
-  __syncthreads();
-  stage_emf(L, sFX, sFY, sEC, sEE);
-  __syncthreads();
-  const double* __restrict__ w = I.w[parity];
-  const double* __restrict__ b = I.b[parity];
   double* __restrict__ w1 = I.w[parity ^ 1];
   double* __restrict__ b1 = I.b[parity ^ 1];
   const AxisMap mx = axis_map(I, 0), my = axis_map(I, 1);
@@ -747,18 +808,23 @@ __device__ __forceinline__ void corr_tile(const Inst& I, const Tile& T, int pari
     const int i = T.x0 + ci, j = T.y0 + cj;
     const long long c = (long long)j * I.nx + i;
     double wn[NM], un[NM];
-#pragma unroll
-    for (int n = 0; n < NM; ++n) wn[n] = w[n * I.sv + c];
+    in.wn(i, j, wn);
     prim2cons(un, wn, I.gam);
     // B^n on the cell's faces; the upper boundary face goes through the BC map
     const bool edge = (i == i2) || (j == j2) || (i == I.ng) || (j == I.ng);
-    double bxl0 = load_face<0>(I, b, i, j, mx, my, !edge);
-    double bxr0 = load_face<0>(I, b, i + 1, j, mx, my, !edge);
-    double byb0 = load_face<1>(I, b, i, j, mx, my, !edge);
-    double byt0 = load_face<1>(I, b, i, j + 1, mx, my, !edge);
-    double bz0 = b[2 * I.sv + c];
+    double bxl0 = in.face(0, i, j, edge, mx, my);
+    double bxr0 = in.face(0, i + 1, j, edge, mx, my);
+    double byb0 = in.face(1, i, j, edge, mx, my);
+    double byt0 = in.face(1, i, j + 1, edge, mx, my);
+    double bz0 = in.face(2, i, j, edge, mx, my);
     // the corrector's sources use the half-step state ws (vanleer.pyx:143)
-    const double w0[4] = {W.get(RHO, i, j), W.get(VX, i, j), W.get(VY, i, j), W.get(VZ, i, j)};
+    double w0[4] = {0., 0., 0., 0.};
+    if (I.src) {
+      w0[0] = in.half(RHO, i, j);
+      w0[1] = in.half(VX, i, j);
+      w0[2] = in.half(VY, i, j);
+      w0[3] = in.half(VZ, i, j);
+    }
     CellOut o;
     stage_cell(I, L, T, ci, cj, un, w0, bxl0, bxr0, byb0, byt0, bz0, sFX, sFY, sEE, dt, o);
     e |= plain::check_prim(o.w);
@@ -789,6 +855,15 @@ __device__ __forceinline__ void corr_tile(const Inst& I, const Tile& T, int pari
     if (m > 0.) atomicMax(&I.ds->cds_bits[parity ^ 1], (unsigned long long)__double_as_longlong(m));
   }
   if (e) atomicOr(I.err, e);
+}
+
+// The whole corrector on a tile whose half-step cells are staged in W.
+template <int TXM, int TYM, int RS, int LIM>
+__device__ __forceinline__ void corr_tile(const Inst& I, const Tile& T, int parity, int cp, const SmemCells& W,
+                                          double* sF, double* red, double dt) {
+  corr_fluxes<TXM, TYM, RS, LIM>(I, T, cp, W, sF);
+  const CorrInGlobal in{&I, I.w[parity], I.b[parity], &W};
+  corr_cells<TXM, TYM>(I, T, parity, in, sF, red, dt, false);
 }
 
 template <int TXM, int TYM, int RS, int LIM>
@@ -838,6 +913,14 @@ struct TmaBox {
   static constexpr int CELLS = W * H;
   static constexpr unsigned BYTES = NM * CELLS * sizeof(double);
   static constexpr int BUF = (NM * CELLS + 15) / 16 * 16;  // doubles per buffer, 128-byte multiple
+  // the cell update's w^n and b^n on the tile (faces up to x0+TX, y0+TY),
+  // loaded into the same buffer once the flux stages are done with it
+  static constexpr int CW = (TXM + 3) & ~1;  // TX+1 positions from an even column at or before x0
+  static constexpr int CH = TYM + 1;
+  static constexpr int CCELLS = CW * CH;
+  static constexpr int COFF = (NM * CCELLS + 15) / 16 * 16;  // b^n box, 128-byte aligned
+  static constexpr unsigned CBYTES = (NM + 3) * CCELLS * sizeof(double);
+  static_assert(COFF + 3 * CCELLS <= BUF, "the cell-update boxes must fit one staging buffer");
   static constexpr size_t smem_bytes = 128 +  // room to align the buffers
       sizeof(double) * (2 * (size_t)BUF + (size_t)NF * (Smem<TXM, TYM, 2>::NFX + Smem<TXM, TYM, 2>::NFY) +
                         Smem<TXM, TYM, 2>::NEC + Smem<TXM, TYM, 2>::NEE + Smem<TXM, TYM, 2>::NSD);
@@ -892,7 +975,7 @@ template <int TXM, int TYM>
 __device__ __forceinline__ void issue_ws(const Tile& T, const unsigned char* maps, double* dst,
                                          unsigned long long* bar) {
   if (T.tma) {
-    const void* map = maps + (size_t)T.inst * 128;
+    const void* map = maps + (size_t)T.inst * 5 * 128;
     tma::fence_async_shared();
     tma::arrive_expect(bar, TmaBox<TXM, TYM>::BYTES);
     tma::load_3d(dst, bar, map, (T.x0 - 2) & ~1, T.y0 - 2, 0);
@@ -901,14 +984,35 @@ __device__ __forceinline__ void issue_ws(const Tile& T, const unsigned char* map
   }
 }
 
-// Iteration k of a block uses buffer k & 1; it is that buffer's (k >> 1)-th
-// use, so it waits for the phase of parity (k >> 1) & 1.
+// Issued by one thread once the tile's flux stages are done with buffer dst:
+// w^n and b^n of the tile for the cell update (maps 1 + parity and 3 + parity
+// of the instance), or a plain arrival.
+template <int TXM, int TYM>
+__device__ __forceinline__ void issue_wn(const Tile& T, const unsigned char* maps, int parity, double* dst,
+                                         unsigned long long* bar) {
+  using B = TmaBox<TXM, TYM>;
+  if (T.tma) {
+    const unsigned char* m = maps + (size_t)T.inst * 5 * 128;
+    const int x = T.x0 & ~1, y = T.y0;
+    tma::fence_async_shared();
+    tma::arrive_expect(bar, B::CBYTES);
+    tma::load_3d(dst, bar, m + (1 + parity) * 128, x, y, 0);
+    tma::load_3d(dst + B::COFF, bar, m + (3 + parity) * 128, x, y, 0);
+  } else {
+    tma::arrive(bar);
+  }
+}
+
+// Iteration k of a block uses buffer k & 1.  Each use completes two phases
+// of that buffer's barrier: the staged half-step input (parity 0), then the
+// cell update's w^n / b^n (parity 1), loaded once the flux stages are done.
 template <int TXM, int TYM, int RS, int LIM>
 __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
                                                       int ntiles, int parity, int cp,
                                                       const unsigned char* __restrict__ maps,
                                                       unsigned* __restrict__ queue) {
   using B = TmaBox<TXM, TYM>;
+  using M = Smem<TXM, TYM, 2>;
   extern __shared__ __align__(128) double smem_raw[];
   __shared__ double red[8];
   __shared__ Inst sI;
@@ -927,7 +1031,7 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
     s_tile[0] = t0;
     if (t0 < ntiles) {
       const Tile T0 = tiles[t0];
-      if (T0.tma) tma::prefetch_map(maps + (size_t)T0.inst * 128);
+      if (T0.tma) tma::prefetch_map(maps + (size_t)T0.inst * 5 * 128);
       issue_ws<TXM, TYM>(T0, maps, smem, &bar[0]);
     }
   }
@@ -938,6 +1042,7 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
     const int t = s_tile[k & 1];
     if (t >= ntiles) break;
     const int buf = k & 1;
+    double* sW = smem + buf * B::BUF;
     if (threadIdx.x == 0) {
       sT = tiles[t];
       const int tn = (int)atomicAdd(queue, 1u);
@@ -948,41 +1053,71 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
     stage_inst(sI, insts, tiles[t].inst);  // ends with a barrier (sT, s_tile visible)
     const Tile& T = sT;
     const Inst& I = sI;
-    const unsigned ph = (unsigned)(k >> 1) & 1u;
-    // one thread waits (bounded) and tells the block; then every thread
-    // observes the completed phase itself
-    if (threadIdx.x == 0 && !tma::wait(&bar[buf], ph)) s_fail = 1;
-    __syncthreads();
-    if (s_fail) {
-      // flag it, give the next tile's load (if any) a bounded wait, and leave
-      if (threadIdx.x == 0) {
-        atomicOr(I.err, (unsigned)ERR_TIMEOUT);
-        if (s_tile[buf ^ 1] < ntiles) tma::wait(&bar[buf ^ 1], (unsigned)((k + 1) >> 1) & 1u);
+    for (int phase = 0; phase < 2; ++phase) {
+      if (phase == 1) {
+        // the flux stages are done with the buffer: the cell update's inputs
+        const double dt = I.ds->dt;
+        if (threadIdx.x == 0) {
+          if (T.tma && dt > 0.) issue_wn<TXM, TYM>(T, maps, parity, sW, &bar[buf]);
+          else tma::arrive(&bar[buf]);
+        }
+        if (dt > 0.) {
+          Layout L;
+          L.set(T.wx, T.wy);
+          double* sF = smem + 2 * B::BUF;
+          stage_emf(L, sF, sF + NF * M::NFX, sF + NF * (M::NFX + M::NFY), sF + NF * (M::NFX + M::NFY) + M::NEC);
+        }
       }
-      return;
-    }
-    tma::wait(&bar[buf], ph);
-    const double dt = I.ds->dt;
-    double* sW = smem + buf * B::BUF;
-    Stage S;
-    if (T.tma) {
-      S.x0 = (T.x0 - 2) & ~1;
-      S.y0 = T.y0 - 2;
-      S.w = B::W;
-      S.h = B::H;
-    } else {
-      S.x0 = T.x0 - 2;
-      S.y0 = T.y0 - 2;
-      S.w = T.wx + 4;
-      S.h = T.wy + 4;
-      if (dt > 0.) stage_cells<false>(I, I.ws, S, sW);
+      // one thread waits (bounded) and tells the block; then every thread
+      // observes the completed phase itself
+      if (threadIdx.x == 0 && !tma::wait(&bar[buf], (unsigned)phase)) s_fail = 1;
       __syncthreads();
-    }
-    if (dt > 0.) {
-      SmemCells W{sW, S, S.cells()};
-      corr_tile<TXM, TYM, RS, LIM>(I, T, parity, cp, W, smem + 2 * B::BUF, red, dt);
-    } else {
-      copy_tile(I, T, parity);  // time has reached tmax: carry the state over
+      if (s_fail) {
+        // flag it, give the next tile's load (if any) a bounded wait, and leave
+        if (threadIdx.x == 0) {
+          atomicOr(I.err, (unsigned)ERR_TIMEOUT);
+          if (s_tile[buf ^ 1] < ntiles) tma::wait(&bar[buf ^ 1], 0u);
+        }
+        return;
+      }
+      tma::wait(&bar[buf], (unsigned)phase);
+      const double dt = I.ds->dt;
+      if (phase == 0) {
+        if (!(dt > 0.)) {
+          copy_tile(I, T, parity);  // time has reached tmax: carry the state over
+          __syncthreads();
+          continue;
+        }
+        Stage S;
+        if (T.tma) {
+          S.x0 = (T.x0 - 2) & ~1;
+          S.y0 = T.y0 - 2;
+          S.w = B::W;
+          S.h = B::H;
+        } else {
+          S.x0 = T.x0 - 2;
+          S.y0 = T.y0 - 2;
+          S.w = T.wx + 4;
+          S.h = T.wy + 4;
+          stage_cells<false>(I, I.ws, S, sW);
+          __syncthreads();
+        }
+        const SmemCells W{sW, S, S.cells()};
+        corr_fluxes<TXM, TYM, RS, LIM>(I, T, cp, W, smem + 2 * B::BUF);  // ends with a barrier
+      } else if (dt > 0.) {
+        if (T.tma) {
+          Stage S;
+          S.x0 = T.x0 & ~1;
+          S.y0 = T.y0;
+          S.w = B::CW;
+          S.h = B::CH;
+          const CorrInSmem in{&I, I.b[parity], sW, sW + B::COFF, S};
+          corr_cells<TXM, TYM>(I, T, parity, in, smem + 2 * B::BUF, red, dt, true);
+        } else {
+          const CorrInGlobal in{&I, I.w[parity], I.b[parity], nullptr};
+          corr_cells<TXM, TYM>(I, T, parity, in, smem + 2 * B::BUF, red, dt, true);
+        }
+      }
     }
     __syncthreads();  // the tile's buffer, sT and sI are free again
   }

@@ -262,3 +262,34 @@ def test_persistent_corrector_tmax_bcs_and_host_stepping(variant):
         pa, _, ba = ref[q].get_state()
         assert np.array_equal(pa, host[q][0]) and np.array_equal(ba, host[q][1]), q
         assert per[q].check() == 0
+
+
+@pytest.mark.parametrize("variant", [6, 8])
+def test_persistent_kernels_with_gravity(variant):
+    """Source terms in the persistent kernels (the corrector's half-step state
+    for the sources comes from global memory there): bitwise the default
+    variant, and the default variant bitwise the oracle."""
+    from bonzo_b200._lib import Batch
+    inst = _instances([30, 33, 64, 46], seed=9)
+    grids = [dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((1, 1), (2, 2), (0, 0))) for n, *_ in inst]
+    meth = dict(METHOD, grav=(0.3, -1.0, 0.0))
+    ref = Batch(grids, exact_fp=True, **meth)
+    per = Batch(grids, exact_fp=True, **meth)
+    per.set_variant(variant)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        for e in (ref, per):
+            e[q].set_state(prim, bfld)
+            e[q].init()
+    ref.advance(1e30, 3)
+    per.advance(1e30, 3)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        for x, y in zip(ref[q].get_state(), per[q].get_state()):
+            assert np.array_equal(x, y), q
+        assert per[q].check() == 0
+    n, gc, prim, bfld = inst[0]
+    o = oracle_sim(grids[0], **meth)
+    o.set_state(prim, bfld)
+    o.init()
+    o.advance(1e30, max_steps=3)
+    for x, y in zip(o.get_state(), ref[0].get_state()):
+        assert np.array_equal(x, y)
