@@ -1116,20 +1116,23 @@ int batch_build_tiles(bnz_batch* b) {
   }
   if (v.persistent) {
     static_assert(sizeof(CUtensorMap) == 128, "tensor maps are 128 bytes");
-    // 5 maps per instance (TmaBox<tx, ty> in bnz_fused.cuh): ws with tx + 4
+    // 6 maps per instance (TmaBox<tx, ty> in bnz_fused.cuh): ws with tx + 4
     // cells from an even column and ty + 4 rows; w[0], w[1] (9 fields) and
-    // b[0], b[1] (3 faces) with tx + 1 positions from an even column and ty + 1 rows
+    // b[0], b[1] (3 faces) with tx + 1 positions from an even column and ty + 1
+    // rows; bs (its first 2 fields, an L2 prefetch box) with tx + 2 positions
+    // and ty + 2 rows
     const int bw = (v.tx + 6) & ~1, bh = v.ty + 4;
     const int cw = (v.tx + 3) & ~1, ch = v.ty + 1;
-    std::vector<CUtensorMap> maps(5 * b->ctx.size());
+    const int pw = (v.tx + 4) & ~1, ph = v.ty + 2;
+    std::vector<CUtensorMap> maps(6 * b->ctx.size());
     std::vector<int> ok(b->ctx.size(), 0);
     memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
     for (size_t q = 0; q < b->ctx.size(); ++q) {
       const bnz_ctx* c = b->ctx[q];
-      CUtensorMap* m = &maps[5 * q];
+      CUtensorMap* m = &maps[6 * q];
       ok[q] = cell_map(c, c->cons_s, 9, bw, bh, &m[0]) && cell_map(c, c->wbuf[0], 9, cw, ch, &m[1]) &&
               cell_map(c, c->wbuf[1], 9, cw, ch, &m[2]) && cell_map(c, c->bbuf[0], 3, cw, ch, &m[3]) &&
-              cell_map(c, c->bbuf[1], 3, cw, ch, &m[4]);
+              cell_map(c, c->bbuf[1], 3, cw, ch, &m[4]) && cell_map(c, c->bfld_s, 2, pw, ph, &m[5]);
     }
     for (FusedTile& t : tB) t.tma = ok[t.inst];
     if (!b->d_maps) CKB(cudaMalloc((void**)&b->d_maps, maps.size() * sizeof(CUtensorMap)));
@@ -1155,7 +1158,7 @@ int batch_build_tiles(bnz_batch* b) {
       const int ng = c->ng, n0 = c->i2 - c->i1 + 1, n1 = c->j2 - c->j1 + 1;
       const bool interior = t.x0 - 1 >= ng && t.x0 + t.wx <= ng + n0 - 1 && t.y0 - 1 >= ng &&
                             t.y0 + t.wy <= ng + n1 - 1;
-      t.tma = ok[t.inst] && interior && t.wx == v.tx && t.wy == v.ty;
+      t.tma = !ok[t.inst] ? 0 : (interior && t.wx == v.tx && t.wy == v.ty) ? 1 : 2;
     }
     if (!b->d_wmaps) CKB(cudaMalloc((void**)&b->d_wmaps, maps.size() * sizeof(CUtensorMap)));
     CKB(cudaMemcpy(b->d_wmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));

@@ -963,6 +963,11 @@ __device__ __forceinline__ void load_3d(void* dst, unsigned long long* bar, cons
       ::"r"(saddr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(saddr(bar))
       : "memory");
 }
+// the box of a tensor map at (x, y, z) into L2, no shared memory involved
+__device__ __forceinline__ void prefetch_l2_3d(const void* map, int x, int y, int z) {
+  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global [%0, {%1, %2, %3}];" ::"l"(map), "r"(x), "r"(y), "r"(z)
+               : "memory");
+}
 __device__ __forceinline__ void prefetch_map(const void* map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(map) : "memory");
 }
@@ -975,13 +980,25 @@ template <int TXM, int TYM>
 __device__ __forceinline__ void issue_ws(const Tile& T, const unsigned char* maps, double* dst,
                                          unsigned long long* bar) {
   if (T.tma) {
-    const void* map = maps + (size_t)T.inst * 5 * 128;
+    const void* map = maps + (size_t)T.inst * 6 * 128;
     tma::fence_async_shared();
     tma::arrive_expect(bar, TmaBox<TXM, TYM>::BYTES);
     tma::load_3d(dst, bar, map, (T.x0 - 2) & ~1, T.y0 - 2, 0);
   } else {
     tma::arrive(bar);
   }
+}
+
+// Issued with the staged input of the next tile: its flux stage's normal
+// faces of bs (map 5: bx, by over the faces the flux stage reads) and its
+// cell update's w^n / b^n, brought into L2 a tile ahead.
+template <int TXM, int TYM>
+__device__ __forceinline__ void prefetch_next(const Tile& T, const unsigned char* maps, int parity) {
+  if (!T.tma) return;
+  const unsigned char* m = maps + (size_t)T.inst * 6 * 128;
+  tma::prefetch_l2_3d(m + 5 * 128, (T.x0 - 1) & ~1, T.y0 - 1, 0);
+  tma::prefetch_l2_3d(m + (1 + parity) * 128, T.x0 & ~1, T.y0, 0);
+  tma::prefetch_l2_3d(m + (3 + parity) * 128, T.x0 & ~1, T.y0, 0);
 }
 
 // Issued by one thread once the tile's flux stages are done with buffer dst:
@@ -992,7 +1009,7 @@ __device__ __forceinline__ void issue_wn(const Tile& T, const unsigned char* map
                                          unsigned long long* bar) {
   using B = TmaBox<TXM, TYM>;
   if (T.tma) {
-    const unsigned char* m = maps + (size_t)T.inst * 5 * 128;
+    const unsigned char* m = maps + (size_t)T.inst * 6 * 128;
     const int x = T.x0 & ~1, y = T.y0;
     tma::fence_async_shared();
     tma::arrive_expect(bar, B::CBYTES);
@@ -1031,8 +1048,9 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
     s_tile[0] = t0;
     if (t0 < ntiles) {
       const Tile T0 = tiles[t0];
-      if (T0.tma) tma::prefetch_map(maps + (size_t)T0.inst * 5 * 128);
+      if (T0.tma) tma::prefetch_map(maps + (size_t)T0.inst * 6 * 128);
       issue_ws<TXM, TYM>(T0, maps, smem, &bar[0]);
+      prefetch_next<TXM, TYM>(T0, maps, parity);
     }
   }
   __syncthreads();
@@ -1048,7 +1066,11 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
       const int tn = (int)atomicAdd(queue, 1u);
       s_tile[buf ^ 1] = tn;
       // the other buffer is free: its tile finished before the last barrier
-      if (tn < ntiles) issue_ws<TXM, TYM>(tiles[tn], maps, smem + (buf ^ 1) * B::BUF, &bar[buf ^ 1]);
+      if (tn < ntiles) {
+        const Tile TN = tiles[tn];
+        issue_ws<TXM, TYM>(TN, maps, smem + (buf ^ 1) * B::BUF, &bar[buf ^ 1]);
+        prefetch_next<TXM, TYM>(TN, maps, parity);
+      }
     }
     stage_inst(sI, insts, tiles[t].inst);  // ends with a barrier (sT, s_tile visible)
     const Tile& T = sT;
@@ -1146,10 +1168,18 @@ struct TmaBoxP {
 };
 
 // maps: 4 per instance, w[0], w[1], b[0], b[1]
+// T.tma: 1 = staged by TMA; 2 = an edge tile of an instance with maps, whose
+// own box of w^n / b^n is brought into L2 (its reads go through the BC map);
+// 0 = neither.
 template <int TX, int TY>
 __device__ __forceinline__ void issue_wb(const Tile& T, const unsigned char* maps, int parity, double* dst,
                                          unsigned long long* bar) {
-  if (T.tma) {
+  if (T.tma == 2) {
+    const unsigned char* m = maps + (size_t)T.inst * 4 * 128;
+    tma::prefetch_l2_3d(m + parity * 128, (T.x0 - 1) & ~1, T.y0 - 1, 0);
+    tma::prefetch_l2_3d(m + (2 + parity) * 128, (T.x0 - 1) & ~1, T.y0 - 1, 0);
+  }
+  if (T.tma == 1) {
     const unsigned char* m = maps + (size_t)T.inst * 4 * 128;
     const int x = (T.x0 - 1) & ~1, y = T.y0 - 1;
     tma::fence_async_shared();
@@ -1182,7 +1212,7 @@ __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ i
     s_tile[0] = t0;
     if (t0 < ntiles) {
       const Tile T0 = tiles[t0];
-      if (T0.tma) {
+      if (T0.tma == 1) {
         tma::prefetch_map(maps + ((size_t)T0.inst * 4 + parity) * 128);
         tma::prefetch_map(maps + ((size_t)T0.inst * 4 + 2 + parity) * 128);
       }
@@ -1216,7 +1246,7 @@ __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ i
     tma::wait(&bar[buf], ph);
     const double dtf = I.ds->dt;
     if (dtf > 0.) {
-      if (T.tma) {
+      if (T.tma == 1) {
         Stage S;
         S.x0 = (T.x0 - 1) & ~1;
         S.y0 = T.y0 - 1;
