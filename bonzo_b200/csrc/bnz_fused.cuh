@@ -167,6 +167,7 @@ constexpr int NF = 8;  // stored flux values: 6 hydro + 2 field (for the EMFs)
 struct Layout {
   int wx, wy;
   int nfx, nfy, nec, nee;
+  int sfx, sfy;  // field strides of the x / y flux arrays (their allocated sizes)
   __device__ __forceinline__ void set(int wx_, int wy_) {
     wx = wx_;
     wy = wy_;
@@ -174,6 +175,16 @@ struct Layout {
     nfy = (wx + 2) * (wy + 1);
     nec = (wx + 2) * (wy + 2);
     nee = (wx + 1) * (wy + 1);
+    sfx = nfx;
+    sfy = nfy;
+  }
+  // the tile's arrays laid out for the largest tile TXM x TYM: compile-time
+  // field strides, whatever the tile's own size
+  template <int TXM, int TYM>
+  __device__ __forceinline__ void set_max(int wx_, int wy_) {
+    set(wx_, wy_);
+    sfx = (TXM + 1) * (TYM + 2);
+    sfy = (TXM + 2) * (TYM + 1);
   }
   // x faces i = x0..x0+wx, rows j = y0-1..y0+wy
   __device__ __forceinline__ int fx(int fi, int fj) const { return (fj + 1) * (wx + 1) + fi; }
@@ -239,6 +250,22 @@ __device__ __forceinline__ void stage_cells(const Inst& I, const double* __restr
       if (MAP && ((fx && (n == VX || n == BX)) || (fy && (n == VY || n == BY)))) v = -v;
       sW[n * S.cells() + t] = v;
     }
+  }
+}
+
+// The cells of region R (no ghost mapping) into shared memory laid out as S
+// (a larger region with fixed sizes): the plain-load counterpart of a TMA box.
+__device__ __forceinline__ void stage_cells_into(const Inst& I, const double* __restrict__ src, const Stage& R,
+                                                 const Stage& S, double* sW) {
+  FastDiv dw;
+  dw.set(R.w);
+  for (int t = threadIdx.x; t < R.cells(); t += blockDim.x) {
+    const int cj = dw.div(t), ci = t - cj * R.w;
+    const int i = R.x0 + ci, j = R.y0 + cj;
+    const long long c = (long long)j * I.nx + i;
+    const int d = S.at(0, i, j);
+#pragma unroll
+    for (int n = 0; n < NM; ++n) sW[n * S.cells() + d] = src[n * I.sv + c];
   }
 }
 
@@ -329,9 +356,9 @@ __device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const
       riemann<RS>(f, wL, wR, I.gam, err);
       const int qq = L.fx(fi, fj);
 #pragma unroll
-      for (int n = 0; n < 6; ++n) sFX[n * L.nfx + qq] = f[n];
-      sFX[6 * L.nfx + qq] = f[BY];  // fx[BY]
-      sFX[7 * L.nfx + qq] = f[BZ];  // fx[BZ]
+      for (int n = 0; n < 6; ++n) sFX[n * L.sfx + qq] = f[n];
+      sFX[6 * L.sfx + qq] = f[BY];  // fx[BY]
+      sFX[7 * L.sfx + qq] = f[BZ];  // fx[BZ]
     } else if (t < L.nfx + L.nfy) {
       // y face at row j (between cells j-1 and j), column i; sweep frame AX = 1
       const int u = t - L.nfx;
@@ -351,14 +378,14 @@ __device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const
       riemann<RS>(f, wL, wR, I.gam, err);
       // local -> global (godunov.pyx:297-324 for the y sweep)
       const int qq = L.fy(fi, fj);
-      sFY[0 * L.nfy + qq] = f[RHO];
-      sFY[1 * L.nfy + qq] = f[VZ];   // global MX
-      sFY[2 * L.nfy + qq] = f[VX];   // global MY
-      sFY[3 * L.nfy + qq] = f[VY];   // global MZ
-      sFY[4 * L.nfy + qq] = f[EN];
-      sFY[5 * L.nfy + qq] = f[PSC];
-      sFY[6 * L.nfy + qq] = f[BZ];   // fy[BX]
-      sFY[7 * L.nfy + qq] = f[BY];   // fy[BZ]
+      sFY[0 * L.sfy + qq] = f[RHO];
+      sFY[1 * L.sfy + qq] = f[VZ];   // global MX
+      sFY[2 * L.sfy + qq] = f[VX];   // global MY
+      sFY[3 * L.sfy + qq] = f[VY];   // global MZ
+      sFY[4 * L.sfy + qq] = f[EN];
+      sFY[5 * L.sfy + qq] = f[PSC];
+      sFY[6 * L.sfy + qq] = f[BZ];   // fy[BX]
+      sFY[7 * L.sfy + qq] = f[BY];   // fy[BZ]
     } else {
       // cell-centred E_z = -(vx by - vy bx) (ct.pyx:148)
       const int u = t - L.nfx - L.nfy;
@@ -377,8 +404,9 @@ __device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const
 // wL = w(i-1) + d(i-1), wR = w(i) - d(i) -- the same values reconstr_linear
 // forms per face (reconstr_c.c:54-91), with half the limiter evaluations.
 struct SlopeBuf {
-  double* d;  // 8 x (wx+2) x (wy+2)
+  double* d;  // 8 fields of s doubles, the cells (wx+2) x (wy+2) first in each
   int w, n;   // row width (wx+2), cells
+  int s;      // field stride
   int x0, y0; // array coordinates of the first cell (x0-1, y0-1)
   __device__ __forceinline__ int at(int i, int j) const { return (j - y0) * w + (i - x0); }
 };
@@ -408,19 +436,21 @@ __device__ __forceinline__ void stage_slopes(const Layout& L, const SmemCells& W
       half_slopes_char<LIM>(wm, wc, wp, gam, d);
 #pragma unroll
       for (int n = 0; n < NM; ++n)
-        if (n != BX) D.d[slot8(n) * D.n + t] = d[n];
+        if (n != BX) D.d[slot8(n) * D.s + t] = d[n];
     } else {
 #pragma unroll
       for (int n = 0; n < NM; ++n) {
         if (n == BX) continue;
         const double* a = W.ptr(plain::perm<AX>(n), i, j);
-        D.d[slot8(n) * D.n + t] = half_slope<LIM>(a[-st], a[0], a[st]);
+        D.d[slot8(n) * D.s + t] = half_slope<LIM>(a[-st], a[0], a[st]);
       }
     }
   }
 }
 
-template <int LIM, int RS>
+// SMAX: the slope buffer's field stride (its allocated cells per field), 0
+// for the tile's own cell count.
+template <int LIM, int RS, int SMAX = 0>
 __device__ __forceinline__ void stage_fluxes_plm(const Inst& I, const Tile& T, const Layout& L, const SmemCells& W,
                                                  const double* __restrict__ b, double* sFX, double* sFY, double* sEC,
                                                  double* sD, int cp, unsigned& err) {
@@ -428,6 +458,7 @@ __device__ __forceinline__ void stage_fluxes_plm(const Inst& I, const Tile& T, c
   D.d = sD;
   D.w = L.wx + 2;
   D.n = (L.wx + 2) * (L.wy + 2);
+  D.s = SMAX > 0 ? SMAX : D.n;
   D.x0 = T.x0 - 1;
   D.y0 = T.y0 - 1;
   // x direction: slopes, then x faces i = x0..x0+wx on rows y0-1..y0+wy
@@ -445,17 +476,17 @@ __device__ __forceinline__ void stage_fluxes_plm(const Inst& I, const Tile& T, c
 #pragma unroll
       for (int n = 0; n < NM; ++n) {
         if (n == BX) continue;
-        wL[n] = W.get(n, i - 1, j) + D.d[slot8(n) * D.n + cl];
-        wR[n] = W.get(n, i, j) - D.d[slot8(n) * D.n + cr];
+        wL[n] = W.get(n, i - 1, j) + D.d[slot8(n) * D.s + cl];
+        wR[n] = W.get(n, i, j) - D.d[slot8(n) * D.s + cr];
       }
       wL[BX] = wR[BX] = b[(long long)j * I.nx + i];
       double f[NM];
       riemann<RS>(f, wL, wR, I.gam, err);
       const int qq = L.fx(fi, fj);
 #pragma unroll
-      for (int n = 0; n < 6; ++n) sFX[n * L.nfx + qq] = f[n];
-      sFX[6 * L.nfx + qq] = f[BY];  // fx[BY]
-      sFX[7 * L.nfx + qq] = f[BZ];  // fx[BZ]
+      for (int n = 0; n < 6; ++n) sFX[n * L.sfx + qq] = f[n];
+      sFX[6 * L.sfx + qq] = f[BY];  // fx[BY]
+      sFX[7 * L.sfx + qq] = f[BZ];  // fx[BZ]
     }
   }
   __syncthreads();
@@ -477,21 +508,21 @@ __device__ __forceinline__ void stage_fluxes_plm(const Inst& I, const Tile& T, c
         for (int n = 0; n < NM; ++n) {
           if (n == BX) continue;
           const int gv = plain::perm<1>(n);
-          wL[n] = W.get(gv, i, j - 1) + D.d[slot8(n) * D.n + cl];
-          wR[n] = W.get(gv, i, j) - D.d[slot8(n) * D.n + cr];
+          wL[n] = W.get(gv, i, j - 1) + D.d[slot8(n) * D.s + cl];
+          wR[n] = W.get(gv, i, j) - D.d[slot8(n) * D.s + cr];
         }
         wL[BX] = wR[BX] = b[I.sv + (long long)j * I.nx + i];
         double f[NM];
         riemann<RS>(f, wL, wR, I.gam, err);
         const int qq = L.fy(fi, fj);
-        sFY[0 * L.nfy + qq] = f[RHO];
-        sFY[1 * L.nfy + qq] = f[VZ];   // global MX
-        sFY[2 * L.nfy + qq] = f[VX];   // global MY
-        sFY[3 * L.nfy + qq] = f[VY];   // global MZ
-        sFY[4 * L.nfy + qq] = f[EN];
-        sFY[5 * L.nfy + qq] = f[PSC];
-        sFY[6 * L.nfy + qq] = f[BZ];   // fy[BX]
-        sFY[7 * L.nfy + qq] = f[BY];   // fy[BZ]
+        sFY[0 * L.sfy + qq] = f[RHO];
+        sFY[1 * L.sfy + qq] = f[VZ];   // global MX
+        sFY[2 * L.sfy + qq] = f[VX];   // global MY
+        sFY[3 * L.sfy + qq] = f[VY];   // global MZ
+        sFY[4 * L.sfy + qq] = f[EN];
+        sFY[5 * L.sfy + qq] = f[PSC];
+        sFY[6 * L.sfy + qq] = f[BZ];   // fy[BX]
+        sFY[7 * L.sfy + qq] = f[BY];   // fy[BZ]
       } else {
         // cell-centred E_z = -(vx by - vy bx) (ct.pyx:148)
         const int u = t - L.nfy;
@@ -512,8 +543,8 @@ __device__ __forceinline__ void stage_emf(const Layout& L, const double* sFX, co
   dw.set(L.wx + 1);
   for (int t = threadIdx.x; t < L.nee; t += blockDim.x) {
     const int cj = dw.div(t), ci = t - cj * (L.wx + 1);
-    sEE[t] = (0.5 * (-sFX[6 * L.nfx + L.fx(ci, cj - 1)] - sFX[6 * L.nfx + L.fx(ci, cj)] +
-                     sFY[6 * L.nfy + L.fy(ci - 1, cj)] + sFY[6 * L.nfy + L.fy(ci, cj)]) -
+    sEE[t] = (0.5 * (-sFX[6 * L.sfx + L.fx(ci, cj - 1)] - sFX[6 * L.sfx + L.fx(ci, cj)] +
+                     sFY[6 * L.sfy + L.fy(ci - 1, cj)] + sFY[6 * L.sfy + L.fy(ci, cj)]) -
               0.25 * (sEC[L.ec(ci - 1, cj)] + sEC[L.ec(ci, cj)] + sEC[L.ec(ci - 1, cj - 1)] + sEC[L.ec(ci, cj - 1)]));
   }
 }
@@ -547,8 +578,8 @@ __device__ __forceinline__ void stage_cell(const Inst& I, const Layout& L, const
   const int qb = L.fy(ci, cj), qt = L.fy(ci, cj + 1);
 #pragma unroll
   for (int n = 0; n < 6; ++n) {
-    double v = un[n] - dtdv * (dax * sFX[n * L.nfx + qr] - dax * sFX[n * L.nfx + ql]);
-    v -= dtdv * (day * sFY[n * L.nfy + qt] - day * sFY[n * L.nfy + qb]);
+    double v = un[n] - dtdv * (dax * sFX[n * L.sfx + qr] - dax * sFX[n * L.sfx + ql]);
+    v -= dtdv * (day * sFY[n * L.sfy + qt] - day * sFY[n * L.sfy + qb]);
     u[n] = v;
   }
   // faces (2D: E_z at corners, E_y = fx[BZ] on x faces, E_x = -fy[BZ] on y faces)
@@ -573,8 +604,8 @@ __device__ __forceinline__ void stage_cell(const Inst& I, const Layout& L, const
 #else
   dtda = dt / (dx * dy);
 #endif
-  const double eyl = sFX[7 * L.nfx + ql], eyr = sFX[7 * L.nfx + qr];
-  const double exb = -sFY[7 * L.nfy + qb], ext = -sFY[7 * L.nfy + qt];
+  const double eyl = sFX[7 * L.sfx + ql], eyr = sFX[7 * L.sfx + qr];
+  const double exb = -sFY[7 * L.sfy + qb], ext = -sFY[7 * L.sfy + qt];
   double bz = bz0 - dtda * (dy * eyr - dy * eyl);
   bz += dtda * (dx * ext - dx * exb);
   o.bz = bz;
@@ -620,7 +651,7 @@ __device__ __forceinline__ void pred_tile(const Inst& I, const Tile& T, double* 
   double* sEC = sFY + NF * M::NFY;
   double* sEE = sEC + M::NEC;
   Layout L;
-  L.set(T.wx, T.wy);
+  L.set_max<TXM, TYM>(T.wx, T.wy);
   unsigned e = 0;
   stage_fluxes<RS>(I, T, L, W, F, sFX, sFY, sEC, e);
   __syncthreads();
@@ -772,9 +803,9 @@ __device__ __forceinline__ void corr_fluxes(const Inst& I, const Tile& T, int cp
   double* sEC = sFY + NF * M::NFY;
   double* sD = sEC + M::NEC + M::NEE;
   Layout L;
-  L.set(T.wx, T.wy);
+  L.set_max<TXM, TYM>(T.wx, T.wy);
   unsigned e = 0;
-  stage_fluxes_plm<LIM, RS>(I, T, L, W, I.bs, sFX, sFY, sEC, sD, cp, e);
+  stage_fluxes_plm<LIM, RS, (TXM + 2) * (TYM + 2)>(I, T, L, W, I.bs, sFX, sFY, sEC, sD, cp, e);
   if (e) atomicOr(I.err, e);
   __syncthreads();
 }
@@ -790,7 +821,7 @@ __device__ __forceinline__ void corr_cells(const Inst& I, const Tile& T, int par
   double* sEC = sFY + NF * M::NFY;
   double* sEE = sEC + M::NEC;
   Layout L;
-  L.set(T.wx, T.wy);
+  L.set_max<TXM, TYM>(T.wx, T.wy);
   if (!emf_done) {
     stage_emf(L, sFX, sFY, sEC, sEE);
     __syncthreads();
@@ -1085,7 +1116,7 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
         }
         if (dt > 0.) {
           Layout L;
-          L.set(T.wx, T.wy);
+          L.set_max<TXM, TYM>(T.wx, T.wy);
           double* sF = smem + 2 * B::BUF;
           stage_emf(L, sF, sF + NF * M::NFX, sF + NF * (M::NFX + M::NFY), sF + NF * (M::NFX + M::NFY) + M::NEC);
         }
@@ -1110,18 +1141,19 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
           __syncthreads();
           continue;
         }
+        // the TMA box's layout in both cases (compile-time sizes)
         Stage S;
-        if (T.tma) {
-          S.x0 = (T.x0 - 2) & ~1;
-          S.y0 = T.y0 - 2;
-          S.w = B::W;
-          S.h = B::H;
-        } else {
-          S.x0 = T.x0 - 2;
-          S.y0 = T.y0 - 2;
-          S.w = T.wx + 4;
-          S.h = T.wy + 4;
-          stage_cells<false>(I, I.ws, S, sW);
+        S.x0 = (T.x0 - 2) & ~1;
+        S.y0 = T.y0 - 2;
+        S.w = B::W;
+        S.h = B::H;
+        if (!T.tma) {
+          Stage R;
+          R.x0 = T.x0 - 2;
+          R.y0 = T.y0 - 2;
+          R.w = T.wx + 4;
+          R.h = T.wy + 4;
+          stage_cells_into(I, I.ws, R, S, sW);
           __syncthreads();
         }
         const SmemCells W{sW, S, S.cells()};
