@@ -1223,6 +1223,32 @@ __device__ __forceinline__ void issue_wb(const Tile& T, const unsigned char* map
   }
 }
 
+// The predictor's inputs of tile T (cells and faces on the tile and its ring,
+// ghost positions through the BC map) into the layout S of a TMA box: the
+// staging of tiles that have no TMA load.
+__device__ __forceinline__ void stage_pred_mapped(const Inst& I, const Tile& T, int parity, const Stage& S,
+                                                  double* sW, bool interior) {
+  const double* __restrict__ w = I.w[parity];
+  const double* __restrict__ b = I.b[parity];
+  const AxisMap mx = axis_map(I, 0), my = axis_map(I, 1);
+  const int rw = T.wx + 2, n = rw * (T.wy + 2);
+  FastDiv dw;
+  dw.set(rw);
+  double* sB = sW + NM * S.cells();
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    const int cj = dw.div(t), ci = t - cj * rw;
+    const int i = T.x0 - 1 + ci, j = T.y0 - 1 + cj;
+    const int d = S.at(0, i, j);
+    double v[NM];
+    load_prim_all(I, w, i, j, mx, my, interior, v);
+#pragma unroll
+    for (int q = 0; q < NM; ++q) sW[q * S.cells() + d] = v[q];
+    sB[d] = load_face<0>(I, b, i, j, mx, my, interior);
+    sB[S.cells() + d] = load_face<1>(I, b, i, j, mx, my, interior);
+    sB[2 * S.cells() + d] = load_face<2>(I, b, i, j, mx, my, interior);
+  }
+}
+
 template <int TX, int TY, int RS>
 __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
                                                       int ntiles, int parity, const unsigned char* __restrict__ maps,
@@ -1278,22 +1304,20 @@ __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ i
     tma::wait(&bar[buf], ph);
     const double dtf = I.ds->dt;
     if (dtf > 0.) {
-      if (T.tma == 1) {
-        Stage S;
-        S.x0 = (T.x0 - 1) & ~1;
-        S.y0 = T.y0 - 1;
-        S.w = B::W;
-        S.h = B::H;
-        const double* sW = smem + buf * B::BUF;
-        const SmemCells W{sW, S, S.cells()};
-        const SmemFaces F{sW + NM * B::CELLS, S};
-        pred_tile<TX, TY, RS>(I, T, smem + 2 * B::BUF, W, F, 0.5 * dtf);
-      } else {
-        const bool interior = pred_interior(I, T);
-        const GlobalCells W{&I, I.w[parity], axis_map(I, 0), axis_map(I, 1), interior};
-        const GlobalFaces F{&I, I.b[parity], axis_map(I, 0), axis_map(I, 1), interior};
-        pred_tile<TX, TY, RS>(I, T, smem + 2 * B::BUF, W, F, 0.5 * dtf);
+      // the TMA box's layout in both cases (compile-time sizes)
+      Stage S;
+      S.x0 = (T.x0 - 1) & ~1;
+      S.y0 = T.y0 - 1;
+      S.w = B::W;
+      S.h = B::H;
+      double* sW = smem + buf * B::BUF;
+      if (T.tma != 1) {
+        stage_pred_mapped(I, T, parity, S, sW, pred_interior(I, T));
+        __syncthreads();
       }
+      const SmemCells W{sW, S, S.cells()};
+      const SmemFaces F{sW + NM * B::CELLS, S};
+      pred_tile<TX, TY, RS>(I, T, smem + 2 * B::BUF, W, F, 0.5 * dtf);
     }
     __syncthreads();  // the tile's buffer, sT and sI are free again
   }
