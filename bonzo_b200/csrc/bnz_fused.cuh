@@ -1032,6 +1032,31 @@ __device__ __forceinline__ void prefetch_next(const Tile& T, const unsigned char
   tma::prefetch_l2_3d(m + (3 + parity) * 128, T.x0 & ~1, T.y0, 0);
 }
 
+// The cell update's w^n (cells of the tile) and b^n (faces up to x0+wx,
+// y0+wy) with plain loads into the layout S of the cell-update TMA boxes:
+// the staging of tiles that have no TMA load.  Faces on the domain boundary
+// are read through the BC map later, as with TMA.
+__device__ __forceinline__ void stage_corr_inputs(const Inst& I, const Tile& T, int parity, const Stage& S, int boff,
+                                                  double* sW) {
+  const double* __restrict__ w = I.w[parity];
+  const double* __restrict__ b = I.b[parity];
+  const int rw = T.wx + 1, n = rw * (T.wy + 1);
+  FastDiv dw;
+  dw.set(rw);
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    const int cj = dw.div(t), ci = t - cj * rw;
+    const int i = T.x0 + ci, j = T.y0 + cj;
+    const long long c = (long long)j * I.nx + i;
+    const int d = S.at(0, i, j);
+    if (ci < T.wx && cj < T.wy) {
+#pragma unroll
+      for (int q = 0; q < NM; ++q) sW[q * S.cells() + d] = w[q * I.sv + c];
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) sW[boff + q * S.cells() + d] = b[q * I.sv + c];
+  }
+}
+
 // Issued by one thread once the tile's flux stages are done with buffer dst:
 // w^n and b^n of the tile for the cell update (maps 1 + parity and 3 + parity
 // of the instance), or a plain arrival.
@@ -1159,18 +1184,18 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
         const SmemCells W{sW, S, S.cells()};
         corr_fluxes<TXM, TYM, RS, LIM>(I, T, cp, W, smem + 2 * B::BUF);  // ends with a barrier
       } else if (dt > 0.) {
-        if (T.tma) {
-          Stage S;
-          S.x0 = T.x0 & ~1;
-          S.y0 = T.y0;
-          S.w = B::CW;
-          S.h = B::CH;
-          const CorrInSmem in{&I, I.b[parity], sW, sW + B::COFF, S};
-          corr_cells<TXM, TYM>(I, T, parity, in, smem + 2 * B::BUF, red, dt, true);
-        } else {
-          const CorrInGlobal in{&I, I.w[parity], I.b[parity], nullptr};
-          corr_cells<TXM, TYM>(I, T, parity, in, smem + 2 * B::BUF, red, dt, true);
+        // the TMA boxes' layout in both cases (compile-time sizes)
+        Stage S;
+        S.x0 = T.x0 & ~1;
+        S.y0 = T.y0;
+        S.w = B::CW;
+        S.h = B::CH;
+        if (!T.tma) {
+          stage_corr_inputs(I, T, parity, S, B::COFF, sW);
+          __syncthreads();
         }
+        const CorrInSmem in{&I, I.b[parity], sW, sW + B::COFF, S};
+        corr_cells<TXM, TYM>(I, T, parity, in, smem + 2 * B::BUF, red, dt, true);
       }
     }
     __syncthreads();  // the tile's buffer, sT and sI are free again
