@@ -814,7 +814,7 @@ __device__ __forceinline__ void corr_fluxes(const Inst& I, const Tile& T, int cp
 // b^(n+1) and the tile's CFL maximum folded into the instance's slot.
 template <int TXM, int TYM, class In>
 __device__ __forceinline__ void corr_cells(const Inst& I, const Tile& T, int parity, const In& in, double* sF,
-                                           double* red, double dt, bool emf_done) {
+                                           double dt, bool emf_done) {
   using M = Smem<TXM, TYM, 2>;
   double* sFX = sF;
   double* sFY = sFX + NF * M::NFX;
@@ -876,25 +876,21 @@ __device__ __forceinline__ void corr_cells(const Inst& I, const Tile& T, int par
 #endif
     if (cds > cmax) cmax = cds;
   }
+  // each warp folds its maximum into the slot (positive doubles order as
+  // their bit patterns): no block-wide reduction, no barrier
   for (int o = 16; o > 0; o >>= 1) cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) red[wid] = cmax;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double m = 0.;
-    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) m = fmax(m, red[q]);
-    if (m > 0.) atomicMax(&I.ds->cds_bits[parity ^ 1], (unsigned long long)__double_as_longlong(m));
-  }
+  if ((threadIdx.x & 31) == 0 && cmax > 0.)
+    atomicMax(&I.ds->cds_bits[parity ^ 1], (unsigned long long)__double_as_longlong(cmax));
   if (e) atomicOr(I.err, e);
 }
 
 // The whole corrector on a tile whose half-step cells are staged in W.
 template <int TXM, int TYM, int RS, int LIM>
 __device__ __forceinline__ void corr_tile(const Inst& I, const Tile& T, int parity, int cp, const SmemCells& W,
-                                          double* sF, double* red, double dt) {
+                                          double* sF, double dt) {
   corr_fluxes<TXM, TYM, RS, LIM>(I, T, cp, W, sF);
   const CorrInGlobal in{&I, I.w[parity], I.b[parity], &W};
-  corr_cells<TXM, TYM>(I, T, parity, in, sF, red, dt, false);
+  corr_cells<TXM, TYM>(I, T, parity, in, sF, dt, false);
 }
 
 template <int TXM, int TYM, int RS, int LIM>
@@ -902,7 +898,6 @@ __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ inst
                                                    int parity, int cp) {
   constexpr int RING = 2;
   extern __shared__ double smem[];
-  __shared__ double red[8];
   __shared__ Inst sI;
   const Tile T = tiles[blockIdx.x];
   stage_inst(sI, insts, T.inst);
@@ -923,7 +918,7 @@ __global__ void __launch_bounds__(256, 2) k_corr2d(const Inst* __restrict__ inst
   stage_cells<false>(I, I.ws, S, sW);
   __syncthreads();
   SmemCells W{sW, S, S.cells()};
-  corr_tile<TXM, TYM, RS, LIM>(I, T, parity, cp, W, smem + Smem<TXM, TYM, RING>::NSW, red, dt);
+  corr_tile<TXM, TYM, RS, LIM>(I, T, parity, cp, W, smem + Smem<TXM, TYM, RING>::NSW, dt);
 }
 
 // ---------------------------------------------------------------------------
@@ -1087,7 +1082,6 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
   using B = TmaBox<TXM, TYM>;
   using M = Smem<TXM, TYM, 2>;
   extern __shared__ __align__(128) double smem_raw[];
-  __shared__ double red[8];
   __shared__ Inst sI;
   __shared__ Tile sT;
   __shared__ __align__(8) unsigned long long bar[2];
@@ -1127,8 +1121,11 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
         issue_ws<TXM, TYM>(TN, maps, smem + (buf ^ 1) * B::BUF, &bar[buf ^ 1]);
         prefetch_next<TXM, TYM>(TN, maps, parity);
       }
+      // this tile's staged input (bounded wait); the block learns the outcome
+      // at the barrier that ends the instance copy
+      if (!tma::wait(&bar[buf], 0u)) s_fail = 1;
     }
-    stage_inst(sI, insts, tiles[t].inst);  // ends with a barrier (sT, s_tile visible)
+    stage_inst(sI, insts, tiles[t].inst);  // ends with a barrier (sT, s_tile, s_fail visible)
     const Tile& T = sT;
     const Inst& I = sI;
     for (int phase = 0; phase < 2; ++phase) {
@@ -1147,9 +1144,11 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
         }
       }
       // one thread waits (bounded) and tells the block; then every thread
-      // observes the completed phase itself
-      if (threadIdx.x == 0 && !tma::wait(&bar[buf], (unsigned)phase)) s_fail = 1;
-      __syncthreads();
+      // observes the completed phase itself (phase 0: waited above)
+      if (phase == 1) {
+        if (threadIdx.x == 0 && !tma::wait(&bar[buf], 1u)) s_fail = 1;
+        __syncthreads();
+      }
       if (s_fail) {
         // flag it, give the next tile's load (if any) a bounded wait, and leave
         if (threadIdx.x == 0) {
@@ -1195,7 +1194,7 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
           __syncthreads();
         }
         const CorrInSmem in{&I, I.b[parity], sW, sW + B::COFF, S};
-        corr_cells<TXM, TYM>(I, T, parity, in, smem + 2 * B::BUF, red, dt, true);
+        corr_cells<TXM, TYM>(I, T, parity, in, smem + 2 * B::BUF, dt, true);
       }
     }
     __syncthreads();  // the tile's buffer, sT and sI are free again
@@ -1312,13 +1311,14 @@ __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ i
       const int tn = (int)atomicAdd(queue, 1u);
       s_tile[buf ^ 1] = tn;
       if (tn < ntiles) issue_wb<TX, TY>(tiles[tn], maps, parity, smem + (buf ^ 1) * B::BUF, &bar[buf ^ 1]);
+      // this tile's input (bounded wait); the block learns the outcome at the
+      // barrier that ends the instance copy
+      if (!tma::wait(&bar[buf], (unsigned)(k >> 1) & 1u)) s_fail = 1;
     }
-    stage_inst(sI, insts, tiles[t].inst);  // ends with a barrier (sT, s_tile visible)
+    stage_inst(sI, insts, tiles[t].inst);  // ends with a barrier (sT, s_tile, s_fail visible)
     const Tile& T = sT;
     const Inst& I = sI;
     const unsigned ph = (unsigned)(k >> 1) & 1u;
-    if (threadIdx.x == 0 && !tma::wait(&bar[buf], ph)) s_fail = 1;
-    __syncthreads();
     if (s_fail) {
       if (threadIdx.x == 0) {
         atomicOr(I.err, (unsigned)ERR_TIMEOUT);
