@@ -1021,6 +1021,20 @@ struct bnz_batch {
   unsigned char* d_maps = nullptr;
   unsigned char* d_wmaps = nullptr;
   unsigned* d_queue = nullptr;
+  // host-state stepping through a device staging buffer laid out like
+  // back-to-back host state (instance q: prim then bfld, at soff[q]), and the
+  // segment tables between it and the instances' buffers of either parity
+  double* d_stage = nullptr;
+  std::vector<size_t> soff;
+  struct SegCopy* d_segs[2] = {nullptr, nullptr};
+  bool stage_failed = false;
+};
+
+// One contiguous copy between the staging buffer (a) and an instance buffer (b).
+struct SegCopy {
+  double* a;
+  double* b;
+  long long n;
 };
 
 namespace {
@@ -1182,6 +1196,17 @@ __global__ void k_set_tmax(FusedInst* insts, int n, double tmax) {
   if (q < n) insts[q].ds->tmax = tmax;
 }
 
+// Copies of the segments segs[0 .. gridDim.y-1]: staging -> instance when
+// to_instance, else instance -> staging.
+__global__ void k_segcopy(const SegCopy* __restrict__ segs, int to_instance) {
+  const SegCopy sg = segs[blockIdx.y];
+  const double* __restrict__ src = to_instance ? sg.a : sg.b;
+  double* __restrict__ dst = to_instance ? sg.b : sg.a;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < sg.n;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
 // Clears the CFL slot `parity` of instances q0 .. q0+n-1 before k_cds_batch
 // folds the maximum of a freshly loaded state into it.
 __global__ void k_cds_clear(FusedInst* insts, int q0, int n, int parity) {
@@ -1231,6 +1256,9 @@ int bnz_batch_destroy(bnz_batch* b) {
   if (b->d_tiles) cudaFree(b->d_tiles);
   if (b->d_maps) cudaFree(b->d_maps);
   if (b->d_wmaps) cudaFree(b->d_wmaps);
+  if (b->d_stage) cudaFree(b->d_stage);
+  for (SegCopy* sg : b->d_segs)
+    if (sg) cudaFree(sg);
   if (b->d_queue) cudaFree(b->d_queue);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->cin) cudaStreamSynchronize(b->cin);
@@ -1390,6 +1418,78 @@ int bnz_batch_advance_timed(bnz_batch* b, double tmax, int nsteps, double* ms_ke
   return BNZ_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The staging buffer and segment tables, made on first use.  Without device
+// memory for them the host copies go to the instances' buffers one by one.
+bool stage_ready(bnz_batch* b) {
+  if (b->d_stage) return true;
+  if (b->stage_failed) return false;
+  const int n = (int)b->ctx.size();
+  b->soff.assign(n + 1, 0);
+  for (int q = 0; q < n; ++q) b->soff[q + 1] = b->soff[q] + 12 * b->ctx[q]->ncell;
+  if (cudaMalloc((void**)&b->d_stage, b->soff[n] * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    b->d_stage = nullptr;
+    b->stage_failed = true;
+    return false;
+  }
+  for (int p = 0; p < 2; ++p) {
+    std::vector<SegCopy> segs(2 * n);
+    for (int q = 0; q < n; ++q) {
+      const bnz_ctx* c = b->ctx[q];
+      segs[2 * q] = SegCopy{b->d_stage + b->soff[q], c->wbuf[p], 9 * (long long)c->ncell};
+      segs[2 * q + 1] = SegCopy{b->d_stage + b->soff[q] + 9 * c->ncell, c->bbuf[p], 3 * (long long)c->ncell};
+    }
+    if (cudaMalloc((void**)&b->d_segs[p], segs.size() * sizeof(SegCopy)) != cudaSuccess ||
+        cudaMemcpy(b->d_segs[p], segs.data(), segs.size() * sizeof(SegCopy), cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(b->d_stage);
+      b->d_stage = nullptr;
+      b->stage_failed = true;
+      return false;
+    }
+  }
+  return true;
+}
+
+// Host <-> staging copies of instances q0 .. q1-1: one copy per run of host
+// memory laid out like the staging buffer (prim[q], then bfld[q], then
+// prim[q+1], ...), two per instance otherwise.
+int stage_copies(bnz_batch* b, double* const* prim, double* const* bfld, int q0, int q1, bool in) {
+  cudaStream_t st = in ? b->cin : b->cout;
+  const cudaMemcpyKind kind = in ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+  auto copy = [&](double* host, size_t off, size_t count) {
+    double* dev = b->d_stage + off;
+    return in ? cudaMemcpyAsync(dev, host, count * sizeof(double), kind, st)
+              : cudaMemcpyAsync(host, dev, count * sizeof(double), kind, st);
+  };
+  int q = q0;
+  while (q < q1) {
+    const size_t nc = b->ctx[q]->ncell;
+    if (bfld[q] != prim[q] + 9 * nc) {
+      CKB(copy(prim[q], b->soff[q], 9 * nc));
+      CKB(copy(bfld[q], b->soff[q] + 9 * nc, 3 * nc));
+      ++q;
+      continue;
+    }
+    int e = q + 1;  // run of self-contiguous instances that follow one another
+    while (e < q1 && prim[e] == bfld[e - 1] + 3 * b->ctx[e - 1]->ncell &&
+           bfld[e] == prim[e] + 9 * b->ctx[e]->ncell)
+      ++e;
+    CKB(copy(prim[q], b->soff[q], b->soff[e] - b->soff[q]));
+    q = e;
+  }
+  return BNZ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int bnz_batch_step_host(bnz_batch* b, double* const* prim, double* const* bfld, double tmax, int nsteps,
                         int nchunks) {
   if (!b || b->ctx.empty()) return BNZ_ERR_ARG;
@@ -1426,14 +1526,20 @@ int bnz_batch_step_host(bnz_batch* b, double* const* prim, double* const* bfld, 
     if (cut.back() != n) cut.push_back(n);
   }
   const int nc = (int)cut.size() - 1;
+  const bool staged = stage_ready(b);
   // the copies in follow whatever the compute stream holds already
   CKB(cudaEventRecord(ev_entry, b->stream));
   CKB(cudaStreamWaitEvent(b->cin, ev_entry, 0));
   for (int k = 0; k < nc; ++k) {
-    for (int q = cut[k]; q < cut[k + 1]; ++q) {
-      bnz_ctx* c = b->ctx[q];
-      CKB(cudaMemcpyAsync(c->prim, prim[q], 9 * c->ncell * sizeof(double), cudaMemcpyHostToDevice, b->cin));
-      CKB(cudaMemcpyAsync(c->bfld, bfld[q], 3 * c->ncell * sizeof(double), cudaMemcpyHostToDevice, b->cin));
+    if (staged) {
+      rc = stage_copies(b, prim, bfld, cut[k], cut[k + 1], true);
+      if (rc) return rc;
+    } else {
+      for (int q = cut[k]; q < cut[k + 1]; ++q) {
+        bnz_ctx* c = b->ctx[q];
+        CKB(cudaMemcpyAsync(c->prim, prim[q], 9 * c->ncell * sizeof(double), cudaMemcpyHostToDevice, b->cin));
+        CKB(cudaMemcpyAsync(c->bfld, bfld[q], 3 * c->ncell * sizeof(double), cudaMemcpyHostToDevice, b->cin));
+      }
     }
     CKB(cudaEventRecord(b->hev[2 + 2 * k], b->cin));
   }
@@ -1449,6 +1555,11 @@ int bnz_batch_step_host(bnz_batch* b, double* const* prim, double* const* bfld, 
     f.tilesB = b->d_tiles + b->ntA + b->offB[q0];
     f.ntB = b->offB[q1] - b->offB[q0];
     CKB(cudaStreamWaitEvent(b->stream, b->hev[2 + 2 * k], 0));
+    if (staged) {
+      // staging buffer -> the instances' buffers of the current parity
+      k_segcopy<<<dim3(32, 2 * (q1 - q0)), 256, 0, b->stream>>>(b->d_segs[p0] + 2 * q0, 1);
+      b->launches += 1;
+    }
     // the loaded state's CFL maximum, then the steps
     k_cds_clear<<<(f.ninst + 127) / 128, 128, 0, b->stream>>>(b->d_inst, q0, f.ninst, p0);
     b->launches += 1 + b->L->fused_cds(f, p0);
@@ -1465,12 +1576,22 @@ int bnz_batch_step_host(bnz_batch* b, double* const* prim, double* const* bfld, 
       StepArgs a = step_args(c);
       b->launches += c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
     }
+    if (staged) {
+      // the results -> staging buffer (its part for this group was consumed above)
+      k_segcopy<<<dim3(32, 2 * (q1 - q0)), 256, 0, b->stream>>>(b->d_segs[p1] + 2 * q0, 0);
+      b->launches += 1;
+    }
     CKB(cudaEventRecord(b->hev[3 + 2 * k], b->stream));
     CKB(cudaStreamWaitEvent(b->cout, b->hev[3 + 2 * k], 0));
-    for (int q = q0; q < q1; ++q) {
-      bnz_ctx* c = b->ctx[q];
-      CKB(cudaMemcpyAsync(prim[q], c->prim, 9 * c->ncell * sizeof(double), cudaMemcpyDeviceToHost, b->cout));
-      CKB(cudaMemcpyAsync(bfld[q], c->bfld, 3 * c->ncell * sizeof(double), cudaMemcpyDeviceToHost, b->cout));
+    if (staged) {
+      rc = stage_copies(b, prim, bfld, q0, q1, false);
+      if (rc) return rc;
+    } else {
+      for (int q = q0; q < q1; ++q) {
+        bnz_ctx* c = b->ctx[q];
+        CKB(cudaMemcpyAsync(prim[q], c->prim, 9 * c->ncell * sizeof(double), cudaMemcpyDeviceToHost, b->cout));
+        CKB(cudaMemcpyAsync(bfld[q], c->bfld, 3 * c->ncell * sizeof(double), cudaMemcpyDeviceToHost, b->cout));
+      }
     }
   }
   CKB(cudaGetLastError());

@@ -208,6 +208,45 @@ def test_batch_step_host_matches_device_stepping(nchunks, nsteps):
             assert np.array_equal(x, y), q
 
 
+@pytest.mark.parametrize("layout", ["packed", "mixed"])
+def test_batch_step_host_packed_host_state(layout):
+    """Host state laid out back to back in one pinned allocation (prim[q],
+    bfld[q], prim[q+1], ...) is copied in runs; a layout that breaks the run
+    in places falls back to per-array copies there.  Bitwise the device path."""
+    import torch
+    from bonzo_b200._lib import Batch
+    inst = _instances([16, 40, 24, 33, 64, 20, 8])
+    grids = [dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((1, 1), (2, 2), (0, 0))) for n, *_ in inst]
+    a = Batch(grids, exact_fp=True, **METHOD)
+    b = Batch(grids, exact_fp=True, **METHOD)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        for e in (a, b):
+            e[q].set_state(prim, bfld)
+            e[q].init()
+    sizes = [12 * int(np.prod(c.shape)) for c in b.instances]
+    pool = torch.empty(sum(sizes) + 64, dtype=torch.float64, pin_memory=True).numpy()
+    host, off = [], 0
+    for q, c in enumerate(b.instances):
+        if layout == "mixed" and q in (2, 5):
+            off += 3  # a gap before this instance: the run breaks here
+        nc = int(np.prod(c.shape))
+        P_ = pool[off:off + 9 * nc].reshape((9,) + c.shape)
+        if layout == "mixed" and q == 4:
+            B_ = np.empty((3,) + c.shape)  # bfld elsewhere: two copies for this instance
+        else:
+            B_ = pool[off + 9 * nc:off + 12 * nc].reshape((3,) + c.shape)
+        off += 12 * nc
+        c.get_state_into(P_, None, B_)
+        host.append((P_, B_))
+    for call in range(2):
+        a.advance(1e30, 1)
+        b.step_host([h[0] for h in host], [h[1] for h in host], 1e30, 1, 3)
+        for q in range(len(inst)):
+            pa, _, ba = a[q].get_state()
+            assert np.array_equal(pa, host[q][0]) and np.array_equal(ba, host[q][1]), (call, q)
+            assert b[q].check() == 0
+
+
 def test_batch_step_host_rejects_bad_arrays():
     from bonzo_b200._lib import Batch, BnzError
     inst = _instances([16, 24])
