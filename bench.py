@@ -41,7 +41,7 @@ CORR_BYTES_PER_ZONE = 288
 # DRAM bytes per active zone of one corrector launch (dram__bytes_read.sum +
 # dram__bytes_write.sum), from an ncu capture of the persistent corrector on
 # the first 16 instances of this batch (scaled per zone).
-CORR_TRAFFIC_PER_ZONE = 268.6
+CORR_TRAFFIC_PER_ZONE = 269.9
 
 
 def parse():

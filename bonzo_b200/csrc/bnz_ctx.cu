@@ -1198,13 +1198,23 @@ __global__ void k_set_tmax(FusedInst* insts, int n, double tmax) {
 
 // Copies of the segments segs[0 .. gridDim.y-1]: staging -> instance when
 // to_instance, else instance -> staging.
+// 16-byte copies where both ends are 16-byte aligned (the staging offsets are
+// multiples of 12 doubles, the instance buffers are allocation starts).
 __global__ void k_segcopy(const SegCopy* __restrict__ segs, int to_instance) {
   const SegCopy sg = segs[blockIdx.y];
   const double* __restrict__ src = to_instance ? sg.a : sg.b;
   double* __restrict__ dst = to_instance ? sg.b : sg.a;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < sg.n;
-       i += (long long)gridDim.x * blockDim.x)
-    dst[i] = src[i];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long i0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if ((((uintptr_t)src | (uintptr_t)dst) & 15) == 0) {
+    const long long n2 = sg.n >> 1;
+    const double2* __restrict__ s2 = reinterpret_cast<const double2*>(src);
+    double2* __restrict__ d2 = reinterpret_cast<double2*>(dst);
+    for (long long i = i0; i < n2; i += stride) d2[i] = s2[i];
+    if ((sg.n & 1) && i0 == 0) dst[sg.n - 1] = src[sg.n - 1];
+  } else {
+    for (long long i = i0; i < sg.n; i += stride) dst[i] = src[i];
+  }
 }
 
 // Clears the CFL slot `parity` of instances q0 .. q0+n-1 before k_cds_batch
@@ -1557,7 +1567,7 @@ int bnz_batch_step_host(bnz_batch* b, double* const* prim, double* const* bfld, 
     CKB(cudaStreamWaitEvent(b->stream, b->hev[2 + 2 * k], 0));
     if (staged) {
       // staging buffer -> the instances' buffers of the current parity
-      k_segcopy<<<dim3(32, 2 * (q1 - q0)), 256, 0, b->stream>>>(b->d_segs[p0] + 2 * q0, 1);
+      k_segcopy<<<dim3(128, 2 * (q1 - q0)), 256, 0, b->stream>>>(b->d_segs[p0] + 2 * q0, 1);
       b->launches += 1;
     }
     // the loaded state's CFL maximum, then the steps
@@ -1578,7 +1588,7 @@ int bnz_batch_step_host(bnz_batch* b, double* const* prim, double* const* bfld, 
     }
     if (staged) {
       // the results -> staging buffer (its part for this group was consumed above)
-      k_segcopy<<<dim3(32, 2 * (q1 - q0)), 256, 0, b->stream>>>(b->d_segs[p1] + 2 * q0, 0);
+      k_segcopy<<<dim3(128, 2 * (q1 - q0)), 256, 0, b->stream>>>(b->d_segs[p1] + 2 * q0, 0);
       b->launches += 1;
     }
     CKB(cudaEventRecord(b->hev[3 + 2 * k], b->stream));
