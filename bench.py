@@ -42,6 +42,10 @@ CORR_BYTES_PER_ZONE = 288
 # dram__bytes_write.sum), from an ncu capture of the persistent corrector on
 # the first 16 instances of this batch (scaled per zone).
 CORR_TRAFFIC_PER_ZONE = 269.9
+# FP64 flops per zone-update of the persistent kernels (2 x DFMA + DADD + DMUL
+# thread instructions, those of the division and square-root sequences
+# included), from the same capture: predictor 1196 + corrector 1343.
+FLOPS_PER_ZONE = 2539
 
 
 def parse():
@@ -337,6 +341,15 @@ def run_ours(args, rank, world, dist):
 
     from bonzo_b200.peaks import hbm_peak
     peak, peak_src = hbm_peak()
+    # the step is FP64-issue bound: its FP64 rate against the measured FMA peak
+    from bonzo_b200._lib import fp64_fma_peak
+    fp64_peak = fp64_fma_peak()
+    fp64_achieved = FLOPS_PER_ZONE * zones / (ms_step * 1e-3) / 1e12
+    fp64 = {"achieved_tflops": round(fp64_achieved, 3), "peak_tflops": round(fp64_peak, 3),
+            "frac": round(fp64_achieved / fp64_peak, 4) if fp64_peak > 0 else None,
+            "flops_per_zone": FLOPS_PER_ZONE,
+            "peak_source": "measured in this run (bnz_fp64_fma_peak: independent FMA chains on every SM)",
+            "flops_source": "ncu FP64 instruction counts of the persistent kernels on the first 16 instances"}
     step_achieved = BYTES_PER_ZONE * zones / (ms_step * 1e-3) / 1e9
     step_roof = {"achieved": round(step_achieved, 1), "frac": round(step_achieved / peak, 4),
                  "bytes_per_zone": BYTES_PER_ZONE,
@@ -383,6 +396,7 @@ def run_ours(args, rank, world, dist):
                 "how": e2e_how},
         "gpu_launches": int(launches),
         "roofline": roofline,
+        "fp64": fp64,
         "clocks": clk.record(),
     }
     if plain_ms is not None:

@@ -28,7 +28,7 @@ EXPORTS = [
     "bnz_get_time", "bnz_last_nsts", "bnz_set_time", "bnz_check", "bnz_sync", "bnz_advance_graph",
     "bnz_device_state", "bnz_stream", "bnz_set_stream", "bnz_launch_count",
     "bnz_batch_create", "bnz_batch_destroy", "bnz_batch_last_error", "bnz_batch_size",
-    "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_advance_timed", "bnz_batch_step_host", "bnz_batch_set_stream", "bnz_batch_launch_count",
+    "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_advance_timed", "bnz_batch_step_host", "bnz_fp64_fma_peak", "bnz_batch_set_stream", "bnz_batch_launch_count",
     "bnz_batch_sync", "bnz_variant_count", "bnz_batch_set_variant", "bnz_batch_get_variant",
     "bnz_batch_time_variant", "bnz_batch_autotune", "bnz_vl2_step_noalloc", "bnz_noalloc_last_error",
     "bnz_noalloc_scratch_bytes", "bnz_set_state_device", "bnz_get_state_device", "bnz_rollout_forward",
@@ -103,6 +103,7 @@ def load():
     L.bnz_batch_instance.argtypes = [vp, C.c_int, C.POINTER(vp)]
     L.bnz_batch_advance.argtypes = [vp, C.c_double, C.c_int]
     L.bnz_batch_advance_timed.argtypes = [vp, C.c_double, C.c_int, _dp]
+    L.bnz_fp64_fma_peak.argtypes = [_dp]
     L.bnz_batch_step_host.argtypes = [vp, C.POINTER(_dp), C.POINTER(_dp), C.c_double, C.c_int, C.c_int]
     L.bnz_set_state_device.argtypes = [vp, vp, vp]
     L.bnz_get_state_device.argtypes = [vp, vp, vp]
@@ -446,6 +447,16 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def fp64_fma_peak():
+    """Measured FP64 FMA throughput of the current device, TFLOP/s."""
+    L = load()
+    t = C.c_double()
+    rc = L.bnz_fp64_fma_peak(C.byref(t))
+    if rc != BNZ_OK:
+        raise BnzError(rc, "bnz_fp64_fma_peak failed")
+    return t.value
 
 
 def variants():

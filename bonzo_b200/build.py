@@ -30,6 +30,7 @@ UNITS = [
     ("bnz_noalloc.cu", []),
     ("bnz_adjoint.cu", []),
     ("bnz_io.cu", []),
+    ("bnz_peak.cu", ["--fmad=true"]),
 ]
 
 

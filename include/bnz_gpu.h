@@ -271,6 +271,11 @@ const char* bnz_noalloc_last_error(void);
 /* Size in bytes of the fixed scratch array. */
 size_t bnz_noalloc_scratch_bytes(void);
 
+/* Measured FP64 FMA throughput of the current device in TFLOP/s (fma chains
+ * on every SM), the denominator of the kernels' FP64-pipe fraction.  No
+ * counterpart in the reference: a measurement helper. */
+int bnz_fp64_fma_peak(double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

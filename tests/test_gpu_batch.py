@@ -332,3 +332,10 @@ def test_persistent_kernels_with_gravity(variant):
     o.advance(1e30, max_steps=3)
     for x, y in zip(o.get_state(), ref[0].get_state()):
         assert np.array_equal(x, y)
+
+
+def test_fp64_fma_peak_measures():
+    """The FP64 FMA peak helper runs and gives a plausible B200 figure (tens of TFLOP/s)."""
+    from bonzo_b200._lib import fp64_fma_peak
+    t = fp64_fma_peak()
+    assert 5.0 < t < 200.0, t
