@@ -13,6 +13,10 @@
 //               fluxes from ws/bs, EMFs, the full-step update of u^n and B^n,
 //               cons2prim; writes the new prim and face field, and reduces the
 //               next step's CFL max into the instance's slot.
+// k_pred2d_pq / k_corr2d_pq are the same two stages as persistent kernels:
+// one resident grid per launch takes tiles from a work queue and loads the
+// next tile's inputs by TMA (cp.async.bulk.tensor, mbarrier-completed) into
+// the second of two shared-memory buffers while the current tile computes.
 // u^n is rebuilt as prim2cons(w^n), which is bitwise what the reference keeps
 // in its cons array between steps (vanleer.pyx:163).  Ghost values are never
 // stored: loads outside the active range go through the boundary-condition
@@ -95,27 +99,7 @@ __device__ __forceinline__ int map_face(int a, const AxisMap& m, bool& flip, boo
   return a;
 }
 
-// prim at cell (i, j) with ghost indices mapped; local sweep order along AX
-template <int AX>
-__device__ __forceinline__ void load_prim(const Inst& I, const double* __restrict__ w, int i, int j,
-                                          const AxisMap& mx, const AxisMap& my, bool interior, double* out) {
-  bool fx = false, fy = false;
-  int si = i, sj = j;
-  if (!interior) {
-    si = map_cell(i, mx, fx);
-    sj = map_cell(j, my, fy);
-  }
-  const long long c = (long long)sj * I.nx + si;
-#pragma unroll
-  for (int n = 0; n < NM; ++n) {
-    const int gv = plain::perm<AX>(n);
-    if (n == BX) continue;  // the normal component comes from the face array
-    double v = w[gv * I.sv + c];
-    if ((fx && (gv == VX || gv == BX)) || (fy && (gv == VY || gv == BY))) v = -v;
-    out[n] = v;
-  }
-}
-
+// prim at cell (i, j) with ghost indices mapped
 __device__ __forceinline__ void load_prim_all(const Inst& I, const double* __restrict__ w, int i, int j,
                                               const AxisMap& mx, const AxisMap& my, bool interior, double* out) {
   bool fx = false, fy = false;
