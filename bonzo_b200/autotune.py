@@ -62,9 +62,12 @@ def tune_batch(batch, sizes, rsolver="hlld", limiter="vl", steps=2, use_cache=Tr
             return hit["variant"], {int(k): v for k, v in hit["ms"].items()}
     vs = _lib.variants()
     timings = {}
-    n_try = len(vs) if rsolver == "hlld" else 1
-    for v in range(n_try):
-        timings[v] = batch.time_variant(v, steps)
+    for v in range(len(vs)):
+        try:
+            timings[v] = batch.time_variant(v, steps)
+        except _lib.BnzError as e:
+            if e.code != _lib.BNZ_ERR_UNSUPPORTED:  # not built for this Riemann solver
+                raise
     best = min(timings, key=timings.get)
     batch.set_variant(best)
     if use_cache:

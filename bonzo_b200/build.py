@@ -10,6 +10,7 @@ Translation units:
 linked with -shared into bonzo_b200/libbnzgpu.so.  nvcc cross-compiles, so
 this runs on machines without a GPU.
 """
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -44,17 +45,26 @@ def _newer(dst, srcs):
 def build(verbose=True, force=False, extra=()):
     os.makedirs(OUT, exist_ok=True)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "bnz_gpu.h")]
-    objs = []
+    objs, jobs = [], []
     for src, flags in UNITS:
         obj = os.path.join(OUT, src.replace(".cu", ".o"))
         objs.append(obj)
         if not force and _newer(obj, deps):
             continue
-        cmd = [NVCC] + ARCH + COMMON + list(flags) + list(extra) + ["-c", os.path.join(CSRC, src), "-o", obj]
+        jobs.append((src, [NVCC] + ARCH + COMMON + list(flags) + list(extra) +
+                     ["-c", os.path.join(CSRC, src), "-o", obj]))
+
+    def run(job):
+        src, cmd = job
         t0 = time.time()
         subprocess.run(cmd, check=True)
         if verbose:
             print("nvcc %s (%.1fs)" % (src, time.time() - t0))
+
+    # the units compile independently: one nvcc process per unit
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(run, j) for j in jobs]:
+            f.result()
     if force or not _newer(LIB, objs):
         subprocess.run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"], check=True)
         if verbose:

@@ -107,6 +107,10 @@ constexpr FusedVariant FUSED_VARIANTS[FUSED_NVARIANT] = {
     {32, 8, 0, 0}, {32, 8, 1, 0}, {16, 16, 0, 0}, {16, 16, 1, 0}, {15, 14, 0, 0},
     {15, 14, 1, 0}, {15, 14, 0, 1}, {15, 14, 1, 1}, {15, 14, 0, 2}};
 
+// Variants built for a Riemann solver: all for HLLD; the default and the
+// persistent 15 x 14 variant (8) for the others.
+inline bool fused_variant_built(int v, bool hlld) { return v == 0 || v == 8 || (hlld && v > 0 && v < FUSED_NVARIANT); }
+
 // dt modes of the fused step
 enum { FDT_CFL = 0, FDT_EXPLICIT = 1, FDT_FIXED = 2 };
 

@@ -1641,7 +1641,8 @@ int bnz_variant_count(int* n, int* tx, int* ty, int* staged, int* persistent) {
 int bnz_batch_set_variant(bnz_batch* b, int v) {
   if (!b) return BNZ_ERR_ARG;
   if (v < 0 || v >= FUSED_NVARIANT) return bfail(b, BNZ_ERR_ARG, "variant out of range");
-  if (v != 0 && b->md.rsolver != BNZ_RS_HLLD) return bfail(b, BNZ_ERR_UNSUPPORTED, "variants 1.. are built for hlld");
+  if (!fused_variant_built(v, b->md.rsolver == BNZ_RS_HLLD))
+    return bfail(b, BNZ_ERR_UNSUPPORTED, "variants 1-7 are built for hlld only");
   if (v == b->variant) return BNZ_OK;
   CKB(cudaStreamSynchronize(b->stream));
   b->variant = v;
@@ -1712,12 +1713,12 @@ int bnz_batch_time_variant(bnz_batch* b, int v, int steps, double* ms) {
 
 int bnz_batch_autotune(bnz_batch* b, int steps, int* best, double* ms_per_variant) {
   if (!b) return BNZ_ERR_ARG;
-  int nv = b->md.rsolver == BNZ_RS_HLLD ? FUSED_NVARIANT : 1;
+  const bool hlld = b->md.rsolver == BNZ_RS_HLLD;
   double best_ms = 1e300;
   int bv = 0;
   for (int v = 0; v < FUSED_NVARIANT; ++v) {
     double ms = -1.;
-    if (v < nv) {
+    if (fused_variant_built(v, hlld)) {
       int rc = bnz_batch_time_variant(b, v, steps, &ms);
       if (rc) return rc;
       if (ms < best_ms) {

@@ -395,7 +395,13 @@ void launch_variant(const FusedLaunch& f, int parity) {
 
 template <int RS>
 void launch_pred_corr(const FusedLaunch& f, int parity) {
-  // FUSED_VARIANTS in bnz_common.h; non-default variants are built for HLLD
+  // FUSED_VARIANTS in bnz_common.h; variants 1-7 are built for HLLD only
+  if constexpr (RS != dev::RS_HLLD) {
+    if (f.variant == 8) {
+      launch_variant<15, 14, RS, 0>(f, parity);  // persistent predictor and corrector
+      return;
+    }
+  }
   if constexpr (RS == dev::RS_HLLD) {
     switch (f.variant) {
       case 1: launch_variant<32, 8, RS, 1>(f, parity); return;
