@@ -336,6 +336,7 @@ void launch_corr_pq(const FusedLaunch& f, int parity) {
     if (per_sm < 1) per_sm = 1;
   }
   const int grid = std::min(f.ntB, per_sm * sm_count());
+  if (grid < 1) return;
   fused::k_corr2d_pq<TX, TY, RS, LIM><<<grid, 256, sm, f.stream>>>(f.insts, f.tilesB, f.ntB, parity,
                                                                     f.charact_proj, f.wsmaps, f.queue);
 }
@@ -350,6 +351,7 @@ void launch_pred_pq(const FusedLaunch& f, int parity) {
     if (per_sm < 1) per_sm = 1;
   }
   const int grid = std::min(f.ntA, per_sm * sm_count());
+  if (grid < 1) return;
   fused::k_pred2d_pq<TX, TY, RS><<<grid, 256, sm, f.stream>>>(f.insts, f.tilesA, f.ntA, parity, f.wmaps,
                                                               f.queue + 1);
 }
