@@ -399,15 +399,21 @@ __device__ __forceinline__ int slot8(int n) { return n < BX ? n : n - 1; }
 
 // cp (charact_proj): the nine local variables are limited in characteristic
 // variables of the cell (reconstr_c.c:54-91 with prim2char / char2prim).
+// sEC (x direction only, else null): the cell-centred E_z of the same cells,
+// -(vx by - vy bx) (ct.pyx:148); a cell's slot t is its E_c slot too.
 template <int AX, int LIM>
 __device__ __forceinline__ void stage_slopes(const Layout& L, const SmemCells& W, const SlopeBuf& D, int cp,
-                                             double gam) {
+                                             double gam, double* sEC) {
   FastDiv dw;
   dw.set(D.w);
   const int st = W.stride(AX);
   for (int t = threadIdx.x; t < D.n; t += blockDim.x) {
     const int cj = dw.div(t), ci = t - cj * D.w;
     const int i = D.x0 + ci, j = D.y0 + cj;
+    if (AX == 0 && sEC) {
+      const double vx = W.get(VX, i, j), vy = W.get(VY, i, j), bxc = W.get(BX, i, j), byc = W.get(BY, i, j);
+      sEC[t] = -(vx * byc - vy * bxc);
+    }
     if (cp) {
       double wm[NM], wc[NM], wp[NM], d[NM];
 #pragma unroll
@@ -445,8 +451,8 @@ __device__ __forceinline__ void stage_fluxes_plm(const Inst& I, const Tile& T, c
   D.s = SMAX > 0 ? SMAX : D.n;
   D.x0 = T.x0 - 1;
   D.y0 = T.y0 - 1;
-  // x direction: slopes, then x faces i = x0..x0+wx on rows y0-1..y0+wy
-  stage_slopes<0, LIM>(L, W, D, cp, I.gam);
+  // x direction: slopes (and E_c), then x faces i = x0..x0+wx on rows y0-1..y0+wy
+  stage_slopes<0, LIM>(L, W, D, cp, I.gam, sEC);
   __syncthreads();
   {
     FastDiv dx1;
@@ -474,48 +480,37 @@ __device__ __forceinline__ void stage_fluxes_plm(const Inst& I, const Tile& T, c
     }
   }
   __syncthreads();
-  // y direction: slopes, y faces j = y0..y0+wy on columns x0-1..x0+wx, and E_c
-  stage_slopes<1, LIM>(L, W, D, cp, I.gam);
+  // y direction: slopes, then y faces j = y0..y0+wy on columns x0-1..x0+wx
+  stage_slopes<1, LIM>(L, W, D, cp, I.gam, nullptr);
   __syncthreads();
   {
     FastDiv dx2;
     dx2.set(L.wx + 2);
-    const int total = L.nfy + L.nec;
-    for (int t = threadIdx.x; t < total; t += blockDim.x) {
-      if (t < L.nfy) {
-        const int q = dx2.div(t);
-        const int fi = t - q * (L.wx + 2) - 1, fj = q;
-        const int i = T.x0 + fi, j = T.y0 + fj;
-        const int cl = D.at(i, j - 1), cr = D.at(i, j);
-        double wL[NM], wR[NM];
+    for (int t = threadIdx.x; t < L.nfy; t += blockDim.x) {
+      const int q = dx2.div(t);
+      const int fi = t - q * (L.wx + 2) - 1, fj = q;
+      const int i = T.x0 + fi, j = T.y0 + fj;
+      const int cl = D.at(i, j - 1), cr = D.at(i, j);
+      double wL[NM], wR[NM];
 #pragma unroll
-        for (int n = 0; n < NM; ++n) {
-          if (n == BX) continue;
-          const int gv = plain::perm<1>(n);
-          wL[n] = W.get(gv, i, j - 1) + D.d[slot8(n) * D.s + cl];
-          wR[n] = W.get(gv, i, j) - D.d[slot8(n) * D.s + cr];
-        }
-        wL[BX] = wR[BX] = b[I.sv + (long long)j * I.nx + i];
-        double f[NM];
-        riemann<RS>(f, wL, wR, I.gam, err);
-        const int qq = L.fy(fi, fj);
-        sFY[0 * L.sfy + qq] = f[RHO];
-        sFY[1 * L.sfy + qq] = f[VZ];   // global MX
-        sFY[2 * L.sfy + qq] = f[VX];   // global MY
-        sFY[3 * L.sfy + qq] = f[VY];   // global MZ
-        sFY[4 * L.sfy + qq] = f[EN];
-        sFY[5 * L.sfy + qq] = f[PSC];
-        sFY[6 * L.sfy + qq] = f[BZ];   // fy[BX]
-        sFY[7 * L.sfy + qq] = f[BY];   // fy[BZ]
-      } else {
-        // cell-centred E_z = -(vx by - vy bx) (ct.pyx:148)
-        const int u = t - L.nfy;
-        const int q = dx2.div(u);
-        const int ci = u - q * (L.wx + 2) - 1, cj = q - 1;
-        const int i = T.x0 + ci, j = T.y0 + cj;
-        const double vx = W.get(VX, i, j), vy = W.get(VY, i, j), bxc = W.get(BX, i, j), byc = W.get(BY, i, j);
-        sEC[L.ec(ci, cj)] = -(vx * byc - vy * bxc);
+      for (int n = 0; n < NM; ++n) {
+        if (n == BX) continue;
+        const int gv = plain::perm<1>(n);
+        wL[n] = W.get(gv, i, j - 1) + D.d[slot8(n) * D.s + cl];
+        wR[n] = W.get(gv, i, j) - D.d[slot8(n) * D.s + cr];
       }
+      wL[BX] = wR[BX] = b[I.sv + (long long)j * I.nx + i];
+      double f[NM];
+      riemann<RS>(f, wL, wR, I.gam, err);
+      const int qq = L.fy(fi, fj);
+      sFY[0 * L.sfy + qq] = f[RHO];
+      sFY[1 * L.sfy + qq] = f[VZ];   // global MX
+      sFY[2 * L.sfy + qq] = f[VX];   // global MY
+      sFY[3 * L.sfy + qq] = f[VY];   // global MZ
+      sFY[4 * L.sfy + qq] = f[EN];
+      sFY[5 * L.sfy + qq] = f[PSC];
+      sFY[6 * L.sfy + qq] = f[BZ];   // fy[BX]
+      sFY[7 * L.sfy + qq] = f[BY];   // fy[BZ]
     }
   }
 }
