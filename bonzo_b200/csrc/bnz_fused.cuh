@@ -318,11 +318,21 @@ template <int RS, class Cells, class Faces>
 __device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const Layout& L, const Cells& W,
                                              const Faces& F, double* sFX, double* sFY, double* sEC,
                                              unsigned& err) {
-  const int total = L.nfx + L.nfy + L.nec;
+  // every face is one item; the first nec items also form one cell's E_c
+  // (nec <= nfx + nfy for any tile), so the loop is faces-only in length
+  const int total = L.nfx + L.nfy;
   FastDiv dx1, dx2;
   dx1.set(L.wx + 1);
   dx2.set(L.wx + 2);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    if (t < L.nec) {
+      // cell-centred E_z = -(vx by - vy bx) (ct.pyx:148) of cell slot t
+      const int q = dx2.div(t);
+      const int ci = t - q * (L.wx + 2) - 1, cj = q - 1;
+      const int i = T.x0 + ci, j = T.y0 + cj;
+      const double vx = W.get(VX, i, j), vy = W.get(VY, i, j), bxc = W.get(BX, i, j), byc = W.get(BY, i, j);
+      sEC[L.ec(ci, cj)] = -(vx * byc - vy * bxc);
+    }
     if (t < L.nfx) {
       // x face at column i (between cells i-1 and i), row j
       const int q = dx1.div(t);
@@ -343,7 +353,7 @@ __device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const
       for (int n = 0; n < 6; ++n) sFX[n * L.sfx + qq] = f[n];
       sFX[6 * L.sfx + qq] = f[BY];  // fx[BY]
       sFX[7 * L.sfx + qq] = f[BZ];  // fx[BZ]
-    } else if (t < L.nfx + L.nfy) {
+    } else {
       // y face at row j (between cells j-1 and j), column i; sweep frame AX = 1
       const int u = t - L.nfx;
       const int q = dx2.div(u);
@@ -370,14 +380,6 @@ __device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const
       sFY[5 * L.sfy + qq] = f[PSC];
       sFY[6 * L.sfy + qq] = f[BZ];   // fy[BX]
       sFY[7 * L.sfy + qq] = f[BY];   // fy[BZ]
-    } else {
-      // cell-centred E_z = -(vx by - vy bx) (ct.pyx:148)
-      const int u = t - L.nfx - L.nfy;
-      const int q = dx2.div(u);
-      const int ci = u - q * (L.wx + 2) - 1, cj = q - 1;
-      const int i = T.x0 + ci, j = T.y0 + cj;
-      const double vx = W.get(VX, i, j), vy = W.get(VY, i, j), bxc = W.get(BX, i, j), byc = W.get(BY, i, j);
-      sEC[L.ec(ci, cj)] = -(vx * byc - vy * bxc);
     }
   }
 }
