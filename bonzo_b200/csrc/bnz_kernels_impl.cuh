@@ -358,7 +358,7 @@ void launch_pred_pq(const FusedLaunch& f, int parity) {
 
 template <int TX, int TY, int RS, int LIM>
 void launch_corr_any(const FusedLaunch& f, int parity) {
-  if constexpr (TX == 15 && TY == 14) {
+  if constexpr ((TX == 15 && TY == 14) || (TX == 14 && TY == 14)) {
     if (f.wsmaps && f.queue) {
       launch_corr_pq<TX, TY, RS, LIM>(f, parity);
       return;
@@ -379,7 +379,7 @@ void launch_variant(const FusedLaunch& f, int parity) {
   }
   if (f.events) cudaEventRecord(f.events[1], f.stream);
   bool done = false;
-  if constexpr (TX == 15 && TY == 14 && STAGED == 0) {
+  if constexpr (((TX == 15 && TY == 14) || (TX == 14 && TY == 14)) && STAGED == 0) {
     if (f.wmaps && f.queue) {
       launch_pred_pq<TX, TY, RS>(f, parity);
       done = true;
@@ -403,6 +403,10 @@ void launch_pred_corr(const FusedLaunch& f, int parity) {
       launch_variant<15, 14, RS, 0>(f, parity);  // persistent predictor and corrector
       return;
     }
+    if (f.variant == 9) {
+      launch_variant<14, 14, RS, 0>(f, parity);
+      return;
+    }
   }
   if constexpr (RS == dev::RS_HLLD) {
     switch (f.variant) {
@@ -414,6 +418,7 @@ void launch_pred_corr(const FusedLaunch& f, int parity) {
       case 6: launch_variant<15, 14, RS, 0>(f, parity); return;  // persistent corrector when maps are given
       case 7: launch_variant<15, 14, RS, 1>(f, parity); return;
       case 8: launch_variant<15, 14, RS, 0>(f, parity); return;  // persistent predictor too
+      case 9: launch_variant<14, 14, RS, 0>(f, parity); return;
       default: break;
     }
   }

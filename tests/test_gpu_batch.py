@@ -117,7 +117,7 @@ def test_batch_rejects_3d_and_conduction():
         Batch([dict(Nx=8, Ny=8, Nz=1, dims=2)], kappa0=0.1, **METHOD)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9])
 def test_every_variant_bitwise_vs_oracle(variant):
     """Every autotuner candidate (tile shape, predictor staging, persistent
     corrector) gives the same bits.  Odd sizes have no tensor map: their tiles
@@ -261,7 +261,7 @@ def test_batch_step_host_rejects_bad_arrays():
         b.step_host([g[0] for g in good], [g[1] for g in good], 1e30, 0)
 
 
-@pytest.mark.parametrize("variant", [6, 7, 8])
+@pytest.mark.parametrize("variant", [6, 7, 8, 9])
 def test_persistent_corrector_tmax_bcs_and_host_stepping(variant):
     """The persistent corrector (tile queue, TMA-staged input) with periodic,
     outflow and reflecting instances, some stopping at tmax (their tiles are
@@ -303,7 +303,7 @@ def test_persistent_corrector_tmax_bcs_and_host_stepping(variant):
         assert per[q].check() == 0
 
 
-@pytest.mark.parametrize("variant", [6, 8])
+@pytest.mark.parametrize("variant", [6, 8, 9])
 def test_persistent_kernels_with_gravity(variant):
     """Source terms in the persistent kernels (the corrector's half-step state
     for the sources comes from global memory there): bitwise the default
