@@ -69,7 +69,11 @@ int check_adjoint_ctx(bnz_ctx* c) {
   if (!c->adj) c->adj = new bnz_adj();
   bnz_adj* A = c->adj;
   if (!A->rev) {
-    CKC(cudaStreamCreateWithFlags(&A->rev, cudaStreamNonBlocking));
+    // the reverse steps are the critical path: their stream outranks the
+    // context's stream, on which the previous segment is recomputed meanwhile
+    int least = 0, greatest = 0;
+    CKC(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    CKC(cudaStreamCreateWithPriority(&A->rev, cudaStreamNonBlocking, greatest));
     for (int p = 0; p < 2; ++p) {
       CKC(cudaEventCreateWithFlags(&A->ev_rec[p], cudaEventDisableTiming));
       CKC(cudaEventCreateWithFlags(&A->ev_rev[p], cudaEventDisableTiming));

@@ -296,12 +296,25 @@ BNZ_HD void vjp_hlld(const double* wL, const double* wR, double gam, const doubl
   const double num = sR * mxR - sL * mxL - (fmxR - fmxL);
   const double sM = num * deni;
   const double sLvxL = sL - vxL, sRvxR = sR - vxR;
+#if BNZ_FAST_MATH && defined(__CUDA_ARCH__)
+  // the fast forward's forms (bnz_device.cuh flux_hlld): one division for both
+  const double dLM = sL - sM, dRM = sR - sM;
+  const double inv2 = 1. / (dLM * dRM);
+  const double sLsMi = dRM * inv2, sRsMi = dLM * inv2;
+#else
   const double sLsMi = 1. / (sL - sM), sRsMi = 1. / (sR - sM);
+#endif
   const double xL = sLvxL * sLsMi, xR = sRvxR * sRsMi;
   const double rLs = rL * xL, rRs = rR * xR;
   const double pts = rL * sLvxL * (sM - vxL) + ptL;
   const double rvL = rL * sLvxL, rvR = rR * sRvxR;
+#if BNZ_FAST_MATH && defined(__CUDA_ARCH__)
+  const double DL = rvL * (sL - sM) - bx2, DR = rvR * (sR - sM) - bx2;
+  const double iD = 1. / (DL * DR);
+  const double wvbL = DR * iD, wvbR = DL * iD;
+#else
   const double wvbL = 1. / (rvL * (sL - sM) - bx2), wvbR = 1. / (rvR * (sR - sM) - bx2);
+#endif
   const double wvL = bx * (sM - vxL) * wvbL, wvR = bx * (sM - vxR) * wvbR;
   const double vyLs = wL[VY] - wL[BY] * wvL, vyRs = wR[VY] - wR[BY] * wvR;
   const double vzLs = wL[VZ] - wL[BZ] * wvL, vzRs = wR[VZ] - wR[BZ] * wvR;
@@ -311,8 +324,13 @@ BNZ_HD void vjp_hlld(const double* wL, const double* wR, double gam, const doubl
   const double bzLs = wL[BZ] * wbL, bzRs = wR[BZ] * wbR;
   const double vsbsL = sM * bx + vyLs * byLs + vzLs * bzLs;
   const double vsbsR = sM * bx + vyRs * byRs + vzRs * bzRs;
+#if BNZ_FAST_MATH && defined(__CUDA_ARCH__)
+  const double isrL = rsqrt(rLs), isrR = rsqrt(rRs);
+  const double srL = rLs * isrL, srR = rRs * isrR;
+#else
   const double srL = sqrt(rLs), srR = sqrt(rRs);
   const double isrL = 1. / srL, isrR = 1. / srR;
+#endif
   const double abx = fabs(bx);
   const double sLs = sM - abx * isrL, sRs = sM + abx * isrR;
   int r = 0;
