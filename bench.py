@@ -407,7 +407,7 @@ def run_ours(args, rank, world, dist):
     return line
 
 
-def run_adjoint(warmup=1, reps=3):
+def run_adjoint(warmup=1, reps=5):
     """adjoint/forward cost of a differentiable rollout: 256^2 periodic vortex
     with a seeded smooth perturbation (Fourier modes |k| <= 4, amplitude 1e-2 on
     v and Az), VL2 + PLM(mc) + HLLD + CT, 100 steps of fixed dt = 1e-4, loss =
