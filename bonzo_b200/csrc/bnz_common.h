@@ -89,9 +89,10 @@ struct FusedTile {
 };
 
 // Variants of the fused kernels the autotuner chooses from: tile shape
-// (cells along x, y) and whether the predictor stages its input cells in
-// shared memory.  Variant 0 is the default and exists for every Riemann
-// solver; the others are built for HLLD.
+// (cells along x, y), whether the predictor stages its input cells in shared
+// memory, and whether the stages run as persistent TMA-fed kernels.  A batch
+// starts on variant 8 (persistent, 15 x 14), a single grid on variant 0
+// (32 x 8: fewer tiles, one wave on a 256^2 grid).
 struct FusedVariant {
   int tx, ty, staged, persistent;
 };
@@ -114,6 +115,8 @@ constexpr FusedVariant FUSED_VARIANTS[FUSED_NVARIANT] = {
 inline bool fused_variant_built(int v, bool hlld) {
   return v == 0 || v == 8 || v == 9 || (hlld && v > 0 && v < FUSED_NVARIANT);
 }
+
+constexpr int BATCH_DEFAULT_VARIANT = 8;
 
 // dt modes of the fused step
 enum { FDT_CFL = 0, FDT_EXPLICIT = 1, FDT_FIXED = 2 };

@@ -1255,6 +1255,7 @@ int bnz_batch_create(const bnz_grid_desc* grids, int n, const bnz_method_desc* m
   b->L = b->ctx[0]->L;
   CKB(cudaMalloc((void**)&b->d_inst, insts.size() * sizeof(FusedInst)));
   CKB(cudaMemcpy(b->d_inst, insts.data(), insts.size() * sizeof(FusedInst), cudaMemcpyHostToDevice));
+  b->variant = BATCH_DEFAULT_VARIANT;
   return batch_build_tiles(b);
 }
 
