@@ -18,7 +18,6 @@ is reported.
 """
 import argparse
 import json
-import math
 import os
 import statistics
 import sys

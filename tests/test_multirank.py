@@ -4,7 +4,6 @@ unit reductions bench.py uses; no other collective is involved."""
 import os
 import socket
 
-import pytest
 
 
 def _free_port():

@@ -1,7 +1,6 @@
 """The torch transcription of the step (tests/torch_vl2.py), the checker of
 the adjoint, pinned against the oracle's step and self-checked: with branch
 decisions frozen, its central differences converge to its autograd gradient."""
-import math
 
 import numpy as np
 import pytest
