@@ -5,7 +5,6 @@ import os
 import socket
 
 
-
 def _free_port():
     s = socket.socket()
     s.bind(("127.0.0.1", 0))
