@@ -1052,9 +1052,14 @@ __device__ __forceinline__ void issue_wn(const Tile& T, const unsigned char* map
   }
 }
 
-// Iteration k of a block uses buffer k & 1.  Each use completes two phases
-// of that buffer's barrier: the staged half-step input (parity 0), then the
-// cell update's w^n / b^n (parity 1), loaded once the flux stages are done.
+// Iteration k of a block uses buffer, instance slot and tile slot k & 1.
+// Each buffer use completes two phases of that buffer's barrier: the staged
+// half-step input (parity 0), then the cell update's w^n / b^n (parity 1),
+// loaded once the flux stages are done.  The next tile's instance record is
+// copied at the end of the current tile, so the barrier that ends a tile also
+// publishes the next one: every thread then waits on the TMA barrier itself,
+// and a wait that ran out is acted on at the flux stage's closing barrier,
+// before the tile writes anything.
 template <int TXM, int TYM, int RS, int LIM>
 __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
                                                       int ntiles, int parity, int cp,
@@ -1063,8 +1068,8 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
   using B = TmaBox<TXM, TYM>;
   using M = Smem<TXM, TYM, 2>;
   extern __shared__ __align__(128) double smem_raw[];
-  __shared__ Inst sI;
-  __shared__ Tile sT;
+  __shared__ Inst sI[2];
+  __shared__ Tile sT[2];
   __shared__ __align__(8) unsigned long long bar[2];
   __shared__ int s_tile[2], s_fail;  // tile of iteration k in s_tile[k & 1]
   // TMA destinations start on 128-byte boundaries (the launch adds 128 bytes)
@@ -1079,12 +1084,14 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
     s_tile[0] = t0;
     if (t0 < ntiles) {
       const Tile T0 = tiles[t0];
+      sT[0] = T0;
       if (T0.tma) tma::prefetch_map(maps + (size_t)T0.inst * 6 * 128);
       issue_ws<TXM, TYM>(T0, maps, smem, &bar[0]);
       prefetch_next<TXM, TYM>(T0, maps, parity);
     }
   }
   __syncthreads();
+  if (s_tile[0] < ntiles) stage_inst(sI[0], insts, sT[0].inst);  // ends with a barrier
   for (int k = 0;; ++k) {
     // written by thread 0 before the last barrier; the slot it writes next
     // was last read before an earlier barrier
@@ -1093,7 +1100,6 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
     const int buf = k & 1;
     double* sW = smem + buf * B::BUF;
     if (threadIdx.x == 0) {
-      sT = tiles[t];
       const int tn = (int)atomicAdd(queue, 1u);
       s_tile[buf ^ 1] = tn;
       // the other buffer is free: its tile finished before the last barrier
@@ -1102,83 +1108,88 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
         issue_ws<TXM, TYM>(TN, maps, smem + (buf ^ 1) * B::BUF, &bar[buf ^ 1]);
         prefetch_next<TXM, TYM>(TN, maps, parity);
       }
-      // this tile's staged input (bounded wait); the block learns the outcome
-      // at the barrier that ends the instance copy
-      if (!tma::wait(&bar[buf], 0u)) s_fail = 1;
     }
-    stage_inst(sI, insts, tiles[t].inst);  // ends with a barrier (sT, s_tile, s_fail visible)
-    const Tile& T = sT;
-    const Inst& I = sI;
-    for (int phase = 0; phase < 2; ++phase) {
-      if (phase == 1) {
-        // the flux stages are done with the buffer: the cell update's inputs
-        const double dt = I.ds->dt;
-        if (threadIdx.x == 0) {
-          if (T.tma && dt > 0.) issue_wn<TXM, TYM>(T, maps, parity, sW, &bar[buf]);
-          else tma::arrive(&bar[buf]);
-        }
-        if (dt > 0.) {
-          Layout L;
-          L.set_max<TXM, TYM>(T.wx, T.wy);
-          double* sF = smem + 2 * B::BUF;
-          stage_emf(L, sF, sF + NF * M::NFX, sF + NF * (M::NFX + M::NFY), sF + NF * (M::NFX + M::NFY) + M::NEC);
-        }
-      }
-      // one thread waits (bounded) and tells the block; then every thread
-      // observes the completed phase itself (phase 0: waited above)
-      if (phase == 1) {
-        if (threadIdx.x == 0 && !tma::wait(&bar[buf], 1u)) s_fail = 1;
+    const Tile& T = sT[buf];
+    const Inst& I = sI[buf];
+    // this tile's staged input, each thread for itself (bounded)
+    if (!tma::wait(&bar[buf], 0u)) s_fail = 1;
+    const double dt = I.ds->dt;
+    bool alive = true;
+    if (!(dt > 0.)) {
+      copy_tile(I, T, parity);  // time has reached tmax: carry the state over (no staged data used)
+      // every thread has passed its parity-0 wait before phase 1 can complete
+      __syncthreads();
+    } else {
+      // the TMA box's layout in both cases (compile-time sizes)
+      Stage S;
+      S.x0 = (T.x0 - 2) & ~1;
+      S.y0 = T.y0 - 2;
+      S.w = B::W;
+      S.h = B::H;
+      if (!T.tma) {
+        Stage R;
+        R.x0 = T.x0 - 2;
+        R.y0 = T.y0 - 2;
+        R.w = T.wx + 4;
+        R.h = T.wy + 4;
+        stage_cells_into(I, I.ws, R, S, sW);
         __syncthreads();
       }
-      if (s_fail) {
-        // flag it, give the next tile's load (if any) a bounded wait, and leave
-        if (threadIdx.x == 0) {
-          atomicOr(I.err, (unsigned)ERR_TIMEOUT);
-          if (s_tile[buf ^ 1] < ntiles) tma::wait(&bar[buf ^ 1], 0u);
-        }
-        return;
-      }
-      tma::wait(&bar[buf], (unsigned)phase);
-      const double dt = I.ds->dt;
-      if (phase == 0) {
-        if (!(dt > 0.)) {
-          copy_tile(I, T, parity);  // time has reached tmax: carry the state over
-          __syncthreads();
-          continue;
-        }
-        // the TMA box's layout in both cases (compile-time sizes)
-        Stage S;
-        S.x0 = (T.x0 - 2) & ~1;
-        S.y0 = T.y0 - 2;
-        S.w = B::W;
-        S.h = B::H;
-        if (!T.tma) {
-          Stage R;
-          R.x0 = T.x0 - 2;
-          R.y0 = T.y0 - 2;
-          R.w = T.wx + 4;
-          R.h = T.wy + 4;
-          stage_cells_into(I, I.ws, R, S, sW);
-          __syncthreads();
-        }
-        const SmemCells W{sW, S, S.cells()};
-        corr_fluxes<TXM, TYM, RS, LIM>(I, T, cp, W, smem + 2 * B::BUF);  // ends with a barrier
-      } else if (dt > 0.) {
-        // the TMA boxes' layout in both cases (compile-time sizes)
-        Stage S;
-        S.x0 = T.x0 & ~1;
-        S.y0 = T.y0;
-        S.w = B::CW;
-        S.h = B::CH;
-        if (!T.tma) {
-          stage_corr_inputs(I, T, parity, S, B::COFF, sW);
-          __syncthreads();
-        }
-        const CorrInSmem in{&I, I.b[parity], sW, sW + B::COFF, S};
-        corr_cells<TXM, TYM>(I, T, parity, in, smem + 2 * B::BUF, dt, true);
-      }
+      const SmemCells W{sW, S, S.cells()};
+      corr_fluxes<TXM, TYM, RS, LIM>(I, T, cp, W, smem + 2 * B::BUF);  // ends with a barrier
+      alive = !s_fail;
     }
-    __syncthreads();  // the tile's buffer, sT and sI are free again
+    if (alive) {
+      // the flux stages are done with the buffer: the cell update's inputs
+      if (threadIdx.x == 0) {
+        if (T.tma && dt > 0.) issue_wn<TXM, TYM>(T, maps, parity, sW, &bar[buf]);
+        else tma::arrive(&bar[buf]);
+      }
+      if (dt > 0.) {
+        Layout L;
+        L.set_max<TXM, TYM>(T.wx, T.wy);
+        double* sF = smem + 2 * B::BUF;
+        stage_emf(L, sF, sF + NF * M::NFX, sF + NF * (M::NFX + M::NFY), sF + NF * (M::NFX + M::NFY) + M::NEC);
+      }
+      // one thread waits (bounded) and tells the block; then every thread
+      // observes the completed phase itself
+      if (threadIdx.x == 0 && !tma::wait(&bar[buf], 1u)) s_fail = 1;
+      __syncthreads();
+      alive = !s_fail;
+    }
+    if (!alive) {
+      // flag it, give the next tile's load (if any) a bounded wait, and leave
+      if (threadIdx.x == 0) {
+        atomicOr(I.err, (unsigned)ERR_TIMEOUT);
+        if (s_tile[buf ^ 1] < ntiles) tma::wait(&bar[buf ^ 1], 0u);
+      }
+      return;
+    }
+    tma::wait(&bar[buf], 1u);
+    if (dt > 0.) {
+      // the TMA boxes' layout in both cases (compile-time sizes)
+      Stage S;
+      S.x0 = T.x0 & ~1;
+      S.y0 = T.y0;
+      S.w = B::CW;
+      S.h = B::CH;
+      if (!T.tma) {
+        stage_corr_inputs(I, T, parity, S, B::COFF, sW);
+        __syncthreads();
+      }
+      const CorrInSmem in{&I, I.b[parity], sW, sW + B::COFF, S};
+      corr_cells<TXM, TYM>(I, T, parity, in, smem + 2 * B::BUF, dt, true);
+    }
+    // the next tile's records into the other slots (last used by the tile
+    // before this one), published by the barrier that ends this tile
+    const int tn = s_tile[buf ^ 1];
+    if (tn < ntiles) {
+      if (threadIdx.x == 0) sT[buf ^ 1] = tiles[tn];
+      const int* src = reinterpret_cast<const int*>(insts + tiles[tn].inst);
+      int* dst = reinterpret_cast<int*>(&sI[buf ^ 1]);
+      for (int q = threadIdx.x; q < (int)(sizeof(Inst) / sizeof(int)); q += blockDim.x) dst[q] = src[q];
+    }
+    __syncthreads();  // the tile's buffer and slots are free; the next tile's are set
   }
 }
 
