@@ -623,9 +623,11 @@ __device__ __forceinline__ void stage_inst(Inst& sI, const Inst* __restrict__ in
 // cells W and faces F (shared memory, or global memory through the BC map),
 // EMFs, the half-step update, the writes of ws / bs.  sF: fluxes and EMFs,
 // contiguous (x fluxes, y fluxes, E_c, E_e).
+// fail (optional): a flag the block checks at the flux stage's closing barrier;
+// when it is set the tile stops there, before writing anything (returns false).
 template <int TXM, int TYM, int RS, class Cells, class Faces>
-__device__ __forceinline__ void pred_tile(const Inst& I, const Tile& T, double* sF, const Cells& W, const Faces& F,
-                                          double dt) {
+__device__ __forceinline__ bool pred_tile(const Inst& I, const Tile& T, double* sF, const Cells& W, const Faces& F,
+                                          double dt, const volatile int* fail = nullptr) {
   using M = Smem<TXM, TYM, 0>;
   double* sFX = sF;
   double* sFY = sFX + NF * M::NFX;
@@ -636,6 +638,7 @@ __device__ __forceinline__ void pred_tile(const Inst& I, const Tile& T, double* 
   unsigned e = 0;
   stage_fluxes<RS>(I, T, L, W, F, sFX, sFY, sEC, e);
   __syncthreads();
+  if (fail && *fail) return false;
   stage_emf(L, sFX, sFY, sEC, sEE);
   __syncthreads();
   const int ilast = I.nx - 2, jlast = I.ny - 2;  // last predictor cell (vanleer lims)
@@ -664,6 +667,7 @@ __device__ __forceinline__ void pred_tile(const Inst& I, const Tile& T, double* 
     if (j == jlast) I.bs[I.sv + c + I.nx] = o.byt;
   }
   if (e) atomicOr(I.err, e);
+  return true;
 }
 
 // a tile whose one-cell ring lies inside the active range needs no ghost mapping
@@ -1265,16 +1269,22 @@ __device__ __forceinline__ void stage_pred_mapped(const Inst& I, const Tile& T, 
   }
 }
 
+// Iteration k uses buffer, instance slot and tile slot k & 1; each buffer use
+// completes one phase of its barrier.  As in the persistent corrector, the
+// next tile's records are copied at the end of the current tile and every
+// thread waits on the TMA barrier itself; a wait that ran out is acted on at
+// the flux stage's closing barrier (or at the top of the next tile).
 template <int TX, int TY, int RS>
 __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
                                                       int ntiles, int parity, const unsigned char* __restrict__ maps,
                                                       unsigned* __restrict__ queue) {
   using B = TmaBoxP<TX, TY>;
   extern __shared__ __align__(128) double smem_raw[];
-  __shared__ Inst sI;
-  __shared__ Tile sT;
+  __shared__ Inst sI[2];
+  __shared__ Tile sT[2];
   __shared__ __align__(8) unsigned long long bar[2];
-  __shared__ int s_tile[2], s_fail;  // tile of iteration k in s_tile[k & 1]
+  __shared__ int s_tile[2];  // tile of iteration k in s_tile[k & 1]
+  __shared__ volatile int s_fail;
   double* smem = smem_raw + ((128u - (tma::saddr(smem_raw) & 127u)) & 127u) / sizeof(double);
   // two staging buffers of B::BUF doubles, then the fluxes and EMFs
   if (threadIdx.x == 0) {
@@ -1286,6 +1296,7 @@ __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ i
     s_tile[0] = t0;
     if (t0 < ntiles) {
       const Tile T0 = tiles[t0];
+      sT[0] = T0;
       if (T0.tma == 1) {
         tma::prefetch_map(maps + ((size_t)T0.inst * 4 + parity) * 128);
         tma::prefetch_map(maps + ((size_t)T0.inst * 4 + 2 + parity) * 128);
@@ -1294,31 +1305,29 @@ __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ i
     }
   }
   __syncthreads();
+  if (s_tile[0] < ntiles) stage_inst(sI[0], insts, sT[0].inst);  // ends with a barrier
   for (int k = 0;; ++k) {
     const int t = s_tile[k & 1];
-    if (t >= ntiles) break;
     const int buf = k & 1;
-    if (threadIdx.x == 0) {
-      sT = tiles[t];
-      const int tn = (int)atomicAdd(queue, 1u);
-      s_tile[buf ^ 1] = tn;
-      if (tn < ntiles) issue_wb<TX, TY>(tiles[tn], maps, parity, smem + (buf ^ 1) * B::BUF, &bar[buf ^ 1]);
-      // this tile's input (bounded wait); the block learns the outcome at the
-      // barrier that ends the instance copy
-      if (!tma::wait(&bar[buf], (unsigned)(k >> 1) & 1u)) s_fail = 1;
-    }
-    stage_inst(sI, insts, tiles[t].inst);  // ends with a barrier (sT, s_tile, s_fail visible)
-    const Tile& T = sT;
-    const Inst& I = sI;
-    const unsigned ph = (unsigned)(k >> 1) & 1u;
+    const Inst& I = sI[buf];
     if (s_fail) {
+      // a load did not complete: flag it, give the load in flight (if any) a
+      // bounded wait, and leave
       if (threadIdx.x == 0) {
         atomicOr(I.err, (unsigned)ERR_TIMEOUT);
-        if (s_tile[buf ^ 1] < ntiles) tma::wait(&bar[buf ^ 1], (unsigned)((k + 1) >> 1) & 1u);
+        if (t < ntiles) tma::wait(&bar[buf], (unsigned)(k >> 1) & 1u);
       }
       return;
     }
-    tma::wait(&bar[buf], ph);
+    if (t >= ntiles) break;
+    if (threadIdx.x == 0) {
+      const int tn = (int)atomicAdd(queue, 1u);
+      s_tile[buf ^ 1] = tn;
+      if (tn < ntiles) issue_wb<TX, TY>(tiles[tn], maps, parity, smem + (buf ^ 1) * B::BUF, &bar[buf ^ 1]);
+    }
+    const Tile& T = sT[buf];
+    // this tile's input, each thread for itself (bounded)
+    if (!tma::wait(&bar[buf], (unsigned)(k >> 1) & 1u)) s_fail = 1;
     const double dtf = I.ds->dt;
     if (dtf > 0.) {
       // the TMA box's layout in both cases (compile-time sizes)
@@ -1334,9 +1343,24 @@ __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ i
       }
       const SmemCells W{sW, S, S.cells()};
       const SmemFaces F{sW + NM * B::CELLS, S};
-      pred_tile<TX, TY, RS>(I, T, smem + 2 * B::BUF, W, F, 0.5 * dtf);
+      if (!pred_tile<TX, TY, RS>(I, T, smem + 2 * B::BUF, W, F, 0.5 * dtf, &s_fail)) {
+        if (threadIdx.x == 0) {
+          atomicOr(I.err, (unsigned)ERR_TIMEOUT);
+          if (s_tile[buf ^ 1] < ntiles) tma::wait(&bar[buf ^ 1], (unsigned)((k + 1) >> 1) & 1u);
+        }
+        return;
+      }
     }
-    __syncthreads();  // the tile's buffer, sT and sI are free again
+    // the next tile's records into the other slots, published by the barrier
+    // that ends this tile
+    const int tn = s_tile[buf ^ 1];
+    if (tn < ntiles) {
+      if (threadIdx.x == 0) sT[buf ^ 1] = tiles[tn];
+      const int* src = reinterpret_cast<const int*>(insts + tiles[tn].inst);
+      int* dst = reinterpret_cast<int*>(&sI[buf ^ 1]);
+      for (int q = threadIdx.x; q < (int)(sizeof(Inst) / sizeof(int)); q += blockDim.x) dst[q] = src[q];
+    }
+    __syncthreads();  // the tile's buffer and slots are free; the next tile's are set
   }
 }
 
