@@ -333,45 +333,48 @@ __device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const
       const double vx = W.get(VX, i, j), vy = W.get(VY, i, j), bxc = W.get(BX, i, j), byc = W.get(BY, i, j);
       sEC[L.ec(ci, cj)] = -(vx * byc - vy * bxc);
     }
-    if (t < L.nfx) {
+    // one Riemann call site for both directions: the face's cells and normal
+    // field are gathered per direction, the flux stored per direction
+    const bool xf = t < L.nfx;
+    int i, j, di, dj, qq;
+    if (xf) {
       // x face at column i (between cells i-1 and i), row j
       const int q = dx1.div(t);
       const int fi = t - q * (L.wx + 1), fj = q - 1;
-      const int i = T.x0 + fi, j = T.y0 + fj;
-      double wL[NM], wR[NM];
-#pragma unroll
-      for (int n = 0; n < NM; ++n) {
-        if (n == BX) continue;
-        wL[n] = W.get(n, i - 1, j);
-        wR[n] = W.get(n, i, j);
-      }
-      wL[BX] = wR[BX] = F.template get<0>(i, j);
-      double f[NM];
-      riemann<RS>(f, wL, wR, I.gam, err);
-      const int qq = L.fx(fi, fj);
-#pragma unroll
-      for (int n = 0; n < 6; ++n) sFX[n * L.sfx + qq] = f[n];
-      sFX[6 * L.sfx + qq] = f[BY];  // fx[BY]
-      sFX[7 * L.sfx + qq] = f[BZ];  // fx[BZ]
+      i = T.x0 + fi;
+      j = T.y0 + fj;
+      di = 1;
+      dj = 0;
+      qq = L.fx(fi, fj);
     } else {
       // y face at row j (between cells j-1 and j), column i; sweep frame AX = 1
       const int u = t - L.nfx;
       const int q = dx2.div(u);
       const int fi = u - q * (L.wx + 2) - 1, fj = q;
-      const int i = T.x0 + fi, j = T.y0 + fj;
-      double wL[NM], wR[NM];
+      i = T.x0 + fi;
+      j = T.y0 + fj;
+      di = 0;
+      dj = 1;
+      qq = L.fy(fi, fj);
+    }
+    double wL[NM], wR[NM];
 #pragma unroll
-      for (int n = 0; n < NM; ++n) {
-        if (n == BX) continue;
-        const int gv = plain::perm<1>(n);
-        wL[n] = W.get(gv, i, j - 1);
-        wR[n] = W.get(gv, i, j);
-      }
-      wL[BX] = wR[BX] = F.template get<1>(i, j);
-      double f[NM];
-      riemann<RS>(f, wL, wR, I.gam, err);
+    for (int n = 0; n < NM; ++n) {
+      if (n == BX) continue;
+      const int gv = xf ? n : plain::perm<1>(n);
+      wL[n] = W.get(gv, i - di, j - dj);
+      wR[n] = W.get(gv, i, j);
+    }
+    wL[BX] = wR[BX] = xf ? F.template get<0>(i, j) : F.template get<1>(i, j);
+    double f[NM];
+    riemann<RS>(f, wL, wR, I.gam, err);
+    if (xf) {
+#pragma unroll
+      for (int n = 0; n < 6; ++n) sFX[n * L.sfx + qq] = f[n];
+      sFX[6 * L.sfx + qq] = f[BY];  // fx[BY]
+      sFX[7 * L.sfx + qq] = f[BZ];  // fx[BZ]
+    } else {
       // local -> global (godunov.pyx:297-324 for the y sweep)
-      const int qq = L.fy(fi, fj);
       sFY[0 * L.sfy + qq] = f[RHO];
       sFY[1 * L.sfy + qq] = f[VZ];   // global MX
       sFY[2 * L.sfy + qq] = f[VX];   // global MY
@@ -1350,6 +1353,10 @@ __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ i
         }
         return;
       }
+    } else {
+      // no work on this tile (time at tmax): thread 0's s_tile write above
+      // must still be visible before the next tile's records are read below
+      __syncthreads();
     }
     // the next tile's records into the other slots, published by the barrier
     // that ends this tile
