@@ -1,8 +1,9 @@
 """Build the reference's own C kernels into oracle/_ref/ (test infrastructure).
 
 Reads the C sources of the reference where they lie (REF_ROOT, default
-/root/reference), writes patched copies and the shared libraries ONLY under
-oracle/_ref/ (git-ignored; it travels to the GPU box with the prebuilt .so).
+/root/reference), compiles patched copies in a temporary directory outside
+the repository (deleted afterwards), and writes ONLY the shared libraries
+under oracle/_ref/ (git-ignored; they travel to the GPU box).
 
 The reference does not compile as shipped.  Four one-line compile fixes are
 applied to the copies (the reference's defect list D5-D8):
@@ -25,6 +26,7 @@ import re
 import shutil
 import subprocess
 import sys
+import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
@@ -72,32 +74,35 @@ def build(ref_root=None, quiet=False):
         if not quiet:
             print("build_ref: reference sources not found at %s; skipped" % ref_root)
         return False
-    src_out = os.path.join(OUT, "src")
-    if os.path.isdir(src_out):
-        shutil.rmtree(src_out)
-    for rel in FILES:
-        with open(os.path.join(ref_root, rel)) as f:
-            text = f.read()
-        dst = os.path.join(OUT, rel)
-        os.makedirs(os.path.dirname(dst), exist_ok=True)
-        with open(dst, "w") as f:
-            f.write(_patch(rel, text))
-    for mfield, name in ((1, "libbnzref.so"), (0, "libbnzref_hydro.so")):
-        objs = []
-        bdir = os.path.join(OUT, "obj_m%d" % mfield)
-        os.makedirs(bdir, exist_ok=True)
-        for rel in ("src/mhd/eos_c.c", "src/mhd/fluxes_c.c", "src/coordinates/reconstr_c.c"):
-            obj = os.path.join(bdir, os.path.basename(rel).replace(".c", ".o"))
-            cmd = ["gcc"] + CFLAGS + ["-DMFIELD=%d" % mfield,
-                                      "-I" + os.path.join(OUT, "src", "mhd"), "-c",
-                                      os.path.join(OUT, rel), "-o", obj]
-            subprocess.run(cmd, check=True)
-            objs.append(obj)
-        lib = os.path.join(OUT, name)
-        subprocess.run(["gcc", "-shared", "-Wl,--allow-multiple-definition", "-o", lib]
-                       + objs + ["-lm"], check=True)
-        if not quiet:
-            print("build_ref: built", lib)
+    os.makedirs(OUT, exist_ok=True)
+    with tempfile.TemporaryDirectory(prefix="bnzref_") as tmp:
+        for rel in FILES:
+            with open(os.path.join(ref_root, rel)) as f:
+                text = f.read()
+            dst = os.path.join(tmp, rel)
+            os.makedirs(os.path.dirname(dst), exist_ok=True)
+            with open(dst, "w") as f:
+                f.write(_patch(rel, text))
+        for mfield, name in ((1, "libbnzref.so"), (0, "libbnzref_hydro.so")):
+            objs = []
+            bdir = os.path.join(tmp, "obj_m%d" % mfield)
+            os.makedirs(bdir, exist_ok=True)
+            for rel in ("src/mhd/eos_c.c", "src/mhd/fluxes_c.c", "src/coordinates/reconstr_c.c"):
+                obj = os.path.join(bdir, os.path.basename(rel).replace(".c", ".o"))
+                cmd = ["gcc"] + CFLAGS + ["-DMFIELD=%d" % mfield,
+                                          "-I" + os.path.join(tmp, "src", "mhd"), "-c",
+                                          os.path.join(tmp, rel), "-o", obj]
+                subprocess.run(cmd, check=True)
+                objs.append(obj)
+            lib = os.path.join(OUT, name)
+            subprocess.run(["gcc", "-shared", "-Wl,--allow-multiple-definition", "-o", lib]
+                           + objs + ["-lm"], check=True)
+            if not quiet:
+                print("build_ref: built", lib)
+    # earlier builds kept their intermediates here: only the libraries stay
+    for d in ("src", "obj_m0", "obj_m1"):
+        if os.path.isdir(os.path.join(OUT, d)):
+            shutil.rmtree(os.path.join(OUT, d))
     return True
 
 
