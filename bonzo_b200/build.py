@@ -44,7 +44,9 @@ def _newer(dst, srcs):
 
 def build(verbose=True, force=False, extra=()):
     os.makedirs(OUT, exist_ok=True)
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "bnz_gpu.h")]
+    # sources, the C ABI header, and this recipe (a flag change rebuilds)
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "bnz_gpu.h"),
+                                                                 os.path.abspath(__file__)]
     objs, jobs = [], []
     for src, flags in UNITS:
         obj = os.path.join(OUT, src.replace(".cu", ".o"))
