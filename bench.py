@@ -40,7 +40,7 @@ CORR_BYTES_PER_ZONE = 288
 # DRAM bytes per active zone of one corrector launch (dram__bytes_read.sum +
 # dram__bytes_write.sum), from an ncu capture of the persistent corrector on
 # the first 16 instances of this batch (scaled per zone).
-CORR_TRAFFIC_PER_ZONE = 269.8
+CORR_TRAFFIC_PER_ZONE = 269.9
 # FP64 flops per zone-update of the persistent kernels (2 x DFMA + DADD + DMUL
 # thread instructions, those of the division and square-root sequences
 # included), from the same capture: predictor 1196 + corrector 1343.
