@@ -28,7 +28,7 @@ EXPORTS = [
     "bnz_get_time", "bnz_last_nsts", "bnz_set_time", "bnz_check", "bnz_sync", "bnz_advance_graph",
     "bnz_device_state", "bnz_stream", "bnz_set_stream", "bnz_launch_count",
     "bnz_batch_create", "bnz_batch_destroy", "bnz_batch_last_error", "bnz_batch_size",
-    "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_advance_timed", "bnz_batch_step_host", "bnz_fp64_fma_peak", "bnz_batch_set_stream", "bnz_batch_launch_count",
+    "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_advance_timed", "bnz_batch_step_host", "bnz_batch_test_withhold_loads", "bnz_fp64_fma_peak", "bnz_batch_set_stream", "bnz_batch_launch_count",
     "bnz_batch_sync", "bnz_variant_count", "bnz_batch_set_variant", "bnz_batch_get_variant",
     "bnz_batch_time_variant", "bnz_batch_autotune", "bnz_vl2_step_noalloc", "bnz_noalloc_last_error",
     "bnz_noalloc_scratch_bytes", "bnz_set_state_device", "bnz_get_state_device", "bnz_rollout_forward",
@@ -104,6 +104,7 @@ def load():
     L.bnz_batch_advance.argtypes = [vp, C.c_double, C.c_int]
     L.bnz_batch_advance_timed.argtypes = [vp, C.c_double, C.c_int, _dp]
     L.bnz_fp64_fma_peak.argtypes = [_dp]
+    L.bnz_batch_test_withhold_loads.argtypes = [vp, C.c_int]
     L.bnz_batch_step_host.argtypes = [vp, C.POINTER(_dp), C.POINTER(_dp), C.c_double, C.c_int, C.c_int]
     L.bnz_set_state_device.argtypes = [vp, vp, vp]
     L.bnz_get_state_device.argtypes = [vp, vp, vp]
@@ -411,6 +412,11 @@ class Batch:
 
     def set_stream(self, stream):
         self._ck(self.L.bnz_batch_set_stream(self.h, C.c_void_p(stream)))
+
+    def test_withhold_loads(self, on):
+        """Test switch: the persistent kernels' TMA loads are armed but not
+        issued, so their bounded waits run out (bnz_batch_test_withhold_loads)."""
+        self._ck(self.L.bnz_batch_test_withhold_loads(self.h, int(bool(on))))
 
     def launch_count(self):
         n = C.c_longlong()

@@ -142,6 +142,7 @@ struct FusedLaunch {
   const unsigned char* wsmaps;
   const unsigned char* wmaps;
   unsigned* queue;
+  int withhold;  // test switch: the persistent kernels' TMA loads are not issued
   // optional: events recorded before k_dt_batch, before the predictor, before
   // the corrector and after it (kernel timing; null in normal stepping)
   cudaEvent_t* events;

@@ -1024,6 +1024,7 @@ struct bnz_batch {
   // host-state stepping through a device staging buffer laid out like
   // back-to-back host state (instance q: prim then bfld, at soff[q]), and the
   // segment tables between it and the instances' buffers of either parity
+  int withhold = 0;  // test switch (bnz_batch_test_withhold_loads)
   double* d_stage = nullptr;
   std::vector<size_t> soff;
   struct SegCopy* d_segs[2] = {nullptr, nullptr};
@@ -1072,6 +1073,7 @@ FusedLaunch batch_launch(const bnz_batch* b, int dt_mode) {
   if (FUSED_VARIANTS[b->variant].persistent && b->d_maps) {
     f.wsmaps = b->d_maps;
     f.queue = b->d_queue;
+    f.withhold = b->withhold;
     if (FUSED_VARIANTS[b->variant].persistent == 2) f.wmaps = b->d_wmaps;
   }
   return f;
@@ -1611,6 +1613,17 @@ int bnz_batch_step_host(bnz_batch* b, double* const* prim, double* const* bfld, 
   b->parity = p1;
   batch_epilogue(b);  // cons is not derived here: ghosts stay marked stale
   CKB(cudaStreamSynchronize(b->stream));
+  return BNZ_OK;
+}
+
+int bnz_batch_test_withhold_loads(bnz_batch* b, int on) {
+  if (!b) return BNZ_ERR_ARG;
+  CKB(cudaStreamSynchronize(b->stream));
+  b->withhold = on ? 1 : 0;
+  if (b->graph) {  // a captured step holds the old value
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
   return BNZ_OK;
 }
 

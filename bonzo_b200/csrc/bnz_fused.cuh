@@ -992,12 +992,12 @@ __device__ __forceinline__ void prefetch_map(const void* map) {
 // of a buffer completes exactly one phase of its barrier.
 template <int TXM, int TYM>
 __device__ __forceinline__ void issue_ws(const Tile& T, const unsigned char* maps, double* dst,
-                                         unsigned long long* bar) {
+                                         unsigned long long* bar, int withhold) {
   if (T.tma) {
     const void* map = maps + (size_t)T.inst * 6 * 128;
     tma::fence_async_shared();
     tma::arrive_expect(bar, TmaBox<TXM, TYM>::BYTES);
-    tma::load_3d(dst, bar, map, (T.x0 - 2) & ~1, T.y0 - 2, 0);
+    if (!withhold) tma::load_3d(dst, bar, map, (T.x0 - 2) & ~1, T.y0 - 2, 0);
   } else {
     tma::arrive(bar);
   }
@@ -1045,15 +1045,17 @@ __device__ __forceinline__ void stage_corr_inputs(const Inst& I, const Tile& T, 
 // of the instance), or a plain arrival.
 template <int TXM, int TYM>
 __device__ __forceinline__ void issue_wn(const Tile& T, const unsigned char* maps, int parity, double* dst,
-                                         unsigned long long* bar) {
+                                         unsigned long long* bar, int withhold) {
   using B = TmaBox<TXM, TYM>;
   if (T.tma) {
     const unsigned char* m = maps + (size_t)T.inst * 6 * 128;
     const int x = T.x0 & ~1, y = T.y0;
     tma::fence_async_shared();
     tma::arrive_expect(bar, B::CBYTES);
-    tma::load_3d(dst, bar, m + (1 + parity) * 128, x, y, 0);
-    tma::load_3d(dst + B::COFF, bar, m + (3 + parity) * 128, x, y, 0);
+    if (!withhold) {
+      tma::load_3d(dst, bar, m + (1 + parity) * 128, x, y, 0);
+      tma::load_3d(dst + B::COFF, bar, m + (3 + parity) * 128, x, y, 0);
+    }
   } else {
     tma::arrive(bar);
   }
@@ -1067,11 +1069,13 @@ __device__ __forceinline__ void issue_wn(const Tile& T, const unsigned char* map
 // publishes the next one: every thread then waits on the TMA barrier itself,
 // and a wait that ran out is acted on at the flux stage's closing barrier,
 // before the tile writes anything.
+// withhold (a test switch, 0 in every normal call): the TMA loads are armed on
+// their barriers but not issued, so that the bounded waits run out.
 template <int TXM, int TYM, int RS, int LIM>
 __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
                                                       int ntiles, int parity, int cp,
                                                       const unsigned char* __restrict__ maps,
-                                                      unsigned* __restrict__ queue) {
+                                                      unsigned* __restrict__ queue, int withhold) {
   using B = TmaBox<TXM, TYM>;
   using M = Smem<TXM, TYM, 2>;
   extern __shared__ __align__(128) double smem_raw[];
@@ -1093,7 +1097,7 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
       const Tile T0 = tiles[t0];
       sT[0] = T0;
       if (T0.tma) tma::prefetch_map(maps + (size_t)T0.inst * 6 * 128);
-      issue_ws<TXM, TYM>(T0, maps, smem, &bar[0]);
+      issue_ws<TXM, TYM>(T0, maps, smem, &bar[0], withhold);
       prefetch_next<TXM, TYM>(T0, maps, parity);
     }
   }
@@ -1112,7 +1116,7 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
       // the other buffer is free: its tile finished before the last barrier
       if (tn < ntiles) {
         const Tile TN = tiles[tn];
-        issue_ws<TXM, TYM>(TN, maps, smem + (buf ^ 1) * B::BUF, &bar[buf ^ 1]);
+        issue_ws<TXM, TYM>(TN, maps, smem + (buf ^ 1) * B::BUF, &bar[buf ^ 1], withhold);
         prefetch_next<TXM, TYM>(TN, maps, parity);
       }
     }
@@ -1149,7 +1153,7 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
     if (alive) {
       // the flux stages are done with the buffer: the cell update's inputs
       if (threadIdx.x == 0) {
-        if (T.tma && dt > 0.) issue_wn<TXM, TYM>(T, maps, parity, sW, &bar[buf]);
+        if (T.tma && dt > 0.) issue_wn<TXM, TYM>(T, maps, parity, sW, &bar[buf], withhold);
         else tma::arrive(&bar[buf]);
       }
       if (dt > 0.) {
@@ -1228,7 +1232,7 @@ struct TmaBoxP {
 // 0 = neither.
 template <int TX, int TY>
 __device__ __forceinline__ void issue_wb(const Tile& T, const unsigned char* maps, int parity, double* dst,
-                                         unsigned long long* bar) {
+                                         unsigned long long* bar, int withhold) {
   if (T.tma == 2) {
     const unsigned char* m = maps + (size_t)T.inst * 4 * 128;
     tma::prefetch_l2_3d(m + parity * 128, (T.x0 - 1) & ~1, T.y0 - 1, 0);
@@ -1239,8 +1243,10 @@ __device__ __forceinline__ void issue_wb(const Tile& T, const unsigned char* map
     const int x = (T.x0 - 1) & ~1, y = T.y0 - 1;
     tma::fence_async_shared();
     tma::arrive_expect(bar, TmaBoxP<TX, TY>::BYTES);
-    tma::load_3d(dst, bar, m + parity * 128, x, y, 0);
-    tma::load_3d(dst + NM * TmaBoxP<TX, TY>::CELLS, bar, m + (2 + parity) * 128, x, y, 0);
+    if (!withhold) {
+      tma::load_3d(dst, bar, m + parity * 128, x, y, 0);
+      tma::load_3d(dst + NM * TmaBoxP<TX, TY>::CELLS, bar, m + (2 + parity) * 128, x, y, 0);
+    }
   } else {
     tma::arrive(bar);
   }
@@ -1280,7 +1286,7 @@ __device__ __forceinline__ void stage_pred_mapped(const Inst& I, const Tile& T, 
 template <int TX, int TY, int RS>
 __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
                                                       int ntiles, int parity, const unsigned char* __restrict__ maps,
-                                                      unsigned* __restrict__ queue) {
+                                                      unsigned* __restrict__ queue, int withhold) {
   using B = TmaBoxP<TX, TY>;
   extern __shared__ __align__(128) double smem_raw[];
   __shared__ Inst sI[2];
@@ -1304,7 +1310,7 @@ __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ i
         tma::prefetch_map(maps + ((size_t)T0.inst * 4 + parity) * 128);
         tma::prefetch_map(maps + ((size_t)T0.inst * 4 + 2 + parity) * 128);
       }
-      issue_wb<TX, TY>(T0, maps, parity, smem, &bar[0]);
+      issue_wb<TX, TY>(T0, maps, parity, smem, &bar[0], withhold);
     }
   }
   __syncthreads();
@@ -1326,7 +1332,7 @@ __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ i
     if (threadIdx.x == 0) {
       const int tn = (int)atomicAdd(queue, 1u);
       s_tile[buf ^ 1] = tn;
-      if (tn < ntiles) issue_wb<TX, TY>(tiles[tn], maps, parity, smem + (buf ^ 1) * B::BUF, &bar[buf ^ 1]);
+      if (tn < ntiles) issue_wb<TX, TY>(tiles[tn], maps, parity, smem + (buf ^ 1) * B::BUF, &bar[buf ^ 1], withhold);
     }
     const Tile& T = sT[buf];
     // this tile's input, each thread for itself (bounded)

@@ -338,7 +338,7 @@ void launch_corr_pq(const FusedLaunch& f, int parity) {
   const int grid = std::min(f.ntB, per_sm * sm_count());
   if (grid < 1) return;
   fused::k_corr2d_pq<TX, TY, RS, LIM><<<grid, 256, sm, f.stream>>>(f.insts, f.tilesB, f.ntB, parity,
-                                                                    f.charact_proj, f.wsmaps, f.queue);
+                                                                    f.charact_proj, f.wsmaps, f.queue, f.withhold);
 }
 
 template <int TX, int TY, int RS>
@@ -353,7 +353,7 @@ void launch_pred_pq(const FusedLaunch& f, int parity) {
   const int grid = std::min(f.ntA, per_sm * sm_count());
   if (grid < 1) return;
   fused::k_pred2d_pq<TX, TY, RS><<<grid, 256, sm, f.stream>>>(f.insts, f.tilesA, f.ntA, parity, f.wmaps,
-                                                              f.queue + 1);
+                                                              f.queue + 1, f.withhold);
 }
 
 template <int TX, int TY, int RS, int LIM>

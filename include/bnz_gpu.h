@@ -191,6 +191,14 @@ int bnz_batch_advance_timed(bnz_batch* batch, double tmax, int nsteps, double* m
 int bnz_batch_step_host(bnz_batch* batch, double* const* prim, double* const* bfld, double tmax, int nsteps,
                         int nchunks);
 int bnz_batch_set_stream(bnz_batch* batch, void* stream);
+/* Test switch, off unless a test turns it on; no counterpart in the
+ * reference.  With on != 0 the persistent kernels (variants 6-9) arm their
+ * TMA loads on the mbarriers but do not issue them, so every bounded wait for
+ * staged input runs out (about a second each): the kernels flag the
+ * instances' error words with the timeout bit (bnz_check then returns
+ * BNZ_ERR_TIMEOUT) and leave without writing the tiles.  It makes a device
+ * wait fail without a fault; the state it leaves is not a step's result. */
+int bnz_batch_test_withhold_loads(bnz_batch* batch, int on);
 int bnz_batch_launch_count(const bnz_batch* batch, long long* n);
 int bnz_batch_sync(bnz_batch* batch);
 

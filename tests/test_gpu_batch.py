@@ -397,3 +397,42 @@ def test_persistent_kernels_long_run_bitwise():
         for x, y in zip(runs[0][q].get_state(), runs[1][q].get_state()):
             assert np.array_equal(x, y), q
         assert runs[1][q].check() == 0
+
+
+def test_persistent_kernels_bounded_waits_run_out_and_recover():
+    """The persistent kernels' mbarrier waits are bounded.  With the TMA loads
+    armed but withheld (a test switch), a step reports BNZ_ERR_TIMEOUT within
+    seconds instead of hanging, and once the loads flow again the same batch
+    steps bitwise like the oracle."""
+    import time
+    from bonzo_b200._lib import BNZ_ERR_TIMEOUT, Batch, BnzError
+    inst = _instances([40, 64, 30], seed=13)  # even Ntot_x: every instance has tensor maps
+    grids = [dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((1, 1), (1, 1), (0, 0))) for n, *_ in inst]
+    b = Batch(grids, exact_fp=True, **METHOD)
+    b.set_variant(8)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        b[q].set_state(prim, bfld)
+        b[q].init()
+    b.test_withhold_loads(True)
+    t0 = time.time()
+    b.advance(1e30, 1)
+    b.sync()
+    assert time.time() - t0 < 60.0
+    for q in range(len(inst)):
+        with pytest.raises(BnzError) as e:
+            b[q].check()
+        assert e.value.code == BNZ_ERR_TIMEOUT
+    b.test_withhold_loads(False)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        b[q].set_state(prim, bfld)
+        b[q].init()
+    b.advance(1e30, 2)
+    for q, (n, gc, prim, bfld) in enumerate(inst):
+        o = oracle_sim(grids[q], **METHOD)
+        o.set_state(prim, bfld)
+        o.init()
+        o.advance(1e30, max_steps=2)
+        assert b[q].time()[1] == 2
+        for x, y in zip(o.get_state(), b[q].get_state()):
+            assert np.array_equal(x, y), q
+        assert b[q].check() == 0
