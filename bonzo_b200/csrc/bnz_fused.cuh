@@ -988,8 +988,8 @@ __device__ __forceinline__ void prefetch_map(const void* map) {
 }  // namespace tma
 
 // Issued by one thread for the tile that will use buffer dst / bar: its
-// staged input by TMA, or (no tensor map) a plain arrival, so that every use
-// of a buffer completes exactly one phase of its barrier.
+// staged input by TMA, or (no tensor map) a plain arrival, so that the
+// barrier's phase completes either way.
 template <int TXM, int TYM>
 __device__ __forceinline__ void issue_ws(const Tile& T, const unsigned char* maps, double* dst,
                                          unsigned long long* bar, int withhold) {
@@ -1209,9 +1209,9 @@ __global__ void __launch_bounds__(256, 2) k_corr2d_pq(const Inst* __restrict__ i
 // Ntot-2) in plain tx x ty steps, so none is larger than tx x ty.  Interior
 // tiles (full tiles whose one-cell ring lies inside the active range, so no
 // ghost is read) get w^n (9 fields) and b^n (3 faces) on the tile and its ring
-// by two TMA loads into one buffer; the other tiles read them from global
-// memory through the BC map.  The boxes start at an even column and are
-// TmaBoxP::W cells wide.
+// by two TMA loads into one buffer; the other tiles stage them with plain
+// loads through the BC map into the same layout.  The boxes start at an even
+// column and are TmaBoxP::W cells wide.
 template <int TX, int TY>
 struct TmaBoxP {
   static constexpr int W = (TX + 4) & ~1;  // TX+2 cells from an even column at or before x0-1
