@@ -78,3 +78,18 @@ def test_null_arguments():
     assert L.bnz_create(None, None, None) == _lib.BNZ_ERR_ARG
     assert L.bnz_vl2_step(None, 0.1) == _lib.BNZ_ERR_ARG
     assert L.bnz_destroy(None) == _lib.BNZ_OK
+
+
+def test_kernel_variants_and_their_labels():
+    """The autotuner's candidates (host-only query): tile shapes, predictor
+    staging, persistent kernels; every variant has its own label, so timings
+    keyed by label cannot overwrite each other."""
+    vs = _lib.variants()
+    assert len(vs) == 10
+    assert vs[0] == (32, 8, 0, 0)            # a single grid's default
+    assert vs[8] == (15, 14, 0, 2)           # a batch's default: persistent predictor and corrector
+    assert vs[9] == (14, 14, 0, 2)
+    assert [v[3] for v in vs].count(0) == 6 and [v[3] for v in vs].count(1) == 2
+    labels = [_lib.variant_label(v) for v in vs]
+    assert len(set(labels)) == len(labels)
+    assert labels[8] == "15x14pp" and labels[6] == "15x14p" and labels[1] == "32x8s"
