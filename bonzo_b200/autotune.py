@@ -1,7 +1,9 @@
-"""Autotuner for the fused 2D kernels: tile shape and predictor staging.
+"""Autotuner for the fused 2D kernels: tile shape, predictor staging and the
+persistent kernels.
 
 Every variant the library was built with (bonzo_b200._lib.variants(): tile
-tx x ty, shared-memory staging of the predictor's input or not) is timed on
+tx x ty, shared-memory staging of the predictor's input or not, persistent
+work-queue corrector and predictor or not) is timed on
 the batch's own state for a few steps (the state is restored after each
 trial) and the fastest is kept.  Choices are cached in a JSON file keyed by
 the workload shape, so later runs of a similar sweep skip the trials:
