@@ -13,6 +13,8 @@ from helpers import oracle_sim, setup_case
     ("blast", 20, dict()),
     ("blast_reflect", 16, dict(rsolver="hll")),
     ("mixed_bc", 16, dict(limiter="mm")),
+    ("blast", 16, dict(grav=(0.3, -1.2, 0.05))),
+    ("vortex", 16, dict(limiter="mc", rsolver="hll", grav=(-0.7, 0.4, 0.0))),
 ])
 def test_transcription_matches_oracle_step(case, n, kw):
     import torch
@@ -29,7 +31,7 @@ def test_transcription_matches_oracle_step(case, n, kw):
     P1, _, B1 = o.get_state()
     G = T.Grid(gc, face_aware=True)
     tp, tb = T.step(G, torch.from_numpy(P0[:, 0].copy()), torch.from_numpy(B0[:, 0].copy()), dt,
-                    rs=m["rsolver"], lim=m["limiter"])
+                    rs=m["rsolver"], lim=m["limiter"], grav=m.get("grav"))
     for a, b in ((tp.numpy(), P1[:, 0]), (tb.numpy(), B1[:, 0])):
         for v in range(a.shape[0]):
             s = max(np.abs(b[v]).max(), 1e-300)

@@ -288,11 +288,13 @@ def limit(lim, a, b):
 # one stage of the step and the whole step
 # ---------------------------------------------------------------------------
 
-def stage(G, Wf, Bf, Wn, Bn, dt, order, R, gam, rs, lim):
+def stage(G, Wf, Bf, Wn, Bn, dt, order, R, gam, rs, lim, grav=None):
     """Fluxes, EMFs and the update on cells R = (ia, ib, ja, jb).  Wf / Bf are
     the cell / face arrays the fluxes read, Wn / Bn the state whose u^n and
-    faces are updated (all as read).  Returns prim (9, R), bx faces (R rows,
-    ia..ib+1), by faces (ja..jb+1, R columns), bz (R)."""
+    faces are updated (all as read).  With `grav` (gx, gy, gz) the constant
+    gravity source of src/srcterms/gravity.pyx:54-69 is added after the update,
+    with the density and velocity of the stage input Wf.  Returns prim (9, R),
+    bx faces (R rows, ia..ib+1), by faces (ja..jb+1, R columns), bz (R)."""
     ia, ib, ja, jb = R
     solver = hlld if rs == "hlld" else hll
     # x faces i = ia..ib+1 on rows ja-1..jb+1
@@ -361,16 +363,25 @@ def stage(G, Wf, Bf, Wn, Bn, dt, order, R, gam, rs, lim):
     u[BY] = ((lvy - lfy[ja:jb + 1])[:, None] * byf[:-1, :] + (lfy[ja + 1:jb + 2] - lvy)[:, None] * byf[1:, :]) * \
         diy[:, None]
     u[BZ] = bz
+    if grav is not None:
+        rho, vx, vy, vz = (Wf[v][ja:jb + 1, ia:ib + 1] for v in (RHO, VX, VY, VZ))
+        u[VX] = u[VX] + rho * grav[0] * dt
+        u[VY] = u[VY] + rho * grav[1] * dt
+        u[VZ] = u[VZ] + rho * grav[2] * dt
+        u[PR] = u[PR] + dt * ((rho * vx) * grav[0] + (rho * vy) * grav[1] + (rho * vz) * grav[2])
     return torch.stack(cons2prim(u, gam)), bxf, byf, bz
 
 
-def step(G, prim, bfld, dt, gam=5.0 / 3.0, rs="hlld", lim="vl"):
+def step(G, prim, bfld, dt, gam=5.0 / 3.0, rs="hlld", lim="vl", grav=None):
     """One VL2 step: returns (prim, bfld) as the library's get_state gives them
-    (ghosts filled through the maps)."""
+    (ghosts filled through the maps).  `grav`: constant gravity (gx, gy, gz),
+    none when absent or all zero."""
+    if grav is not None and not any(g != 0.0 for g in grav):
+        grav = None
     wr = G.read_cells(prim)
     br = G.read_faces(bfld)
     ia, ib, ja, jb = G.R0
-    ws_, bxs, bys, bzs = stage(G, wr, br, wr, br, 0.5 * dt, 0, G.R0, gam, rs, lim)
+    ws_, bxs, bys, bzs = stage(G, wr, br, wr, br, 0.5 * dt, 0, G.R0, gam, rs, lim, grav)
     Ws = torch.zeros_like(prim)
     Ws[:, ja:jb + 1, ia:ib + 1] = ws_
     Bs = torch.zeros_like(bfld)
@@ -378,7 +389,7 @@ def step(G, prim, bfld, dt, gam=5.0 / 3.0, rs="hlld", lim="vl"):
     Bs[1, ja:jb + 2, ia:ib + 1] = bys
     Bs[2, ja:jb + 1, ia:ib + 1] = bzs
     ia, ib, ja, jb = G.R1
-    w1, bx1, by1, bz1 = stage(G, Ws, Bs, wr, br, dt, 1, G.R1, gam, rs, lim)
+    w1, bx1, by1, bz1 = stage(G, Ws, Bs, wr, br, dt, 1, G.R1, gam, rs, lim, grav)
     C = torch.zeros_like(prim)
     C[:, ja:jb + 1, ia:ib + 1] = w1
     Cb = torch.zeros_like(bfld)
