@@ -65,7 +65,9 @@ int check_adjoint_ctx(bnz_ctx* c) {
   if (c->md.rsolver != BNZ_RS_HLL && c->md.rsolver != BNZ_RS_HLLD)
     return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built for rsolver hll and hlld");
   if (c->md.charact_proj) return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built without charact_proj");
-  if (src_on(c->md)) return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built without source terms");
+  // constant gravity is differentiated; the driving force is a random field
+  // advanced every step, which the tape does not keep
+  if (drive_on(c->md)) return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built without turbulence driving");
   if (!c->adj) c->adj = new bnz_adj();
   bnz_adj* A = c->adj;
   if (!A->rev) {

@@ -108,8 +108,25 @@ __device__ __forceinline__ double bz_total(const Inst& I, const StageArgs& a, in
   return a.Gb[2 * I.sv + c] + a.Ub[BZ * I.sv + c];
 }
 
+// Constant gravity, added after a stage's update (bnz_source.cuh
+// srcterm::apply): u[M] += dt rho g, u[EN] += dt rho v.g, with rho and v of
+// the stage input.  Its VJP adds ubar's share onto that input's prim.
+__device__ __forceinline__ bool grav_on(const Inst& I) {
+  return I.grav[0] != 0. || I.grav[1] != 0. || I.grav[2] != 0.;
+}
+__device__ __forceinline__ void grav_vjp(const Inst& I, double dt, const double* ub, double rho, double vx, double vy,
+                                         double vz, double* wb) {
+  const double* g = I.grav;
+  const double e = dt * ub[EN];
+  wb[RHO] += dt * (g[0] * ub[MX] + g[1] * ub[MY] + g[2] * ub[MZ]) + e * (vx * g[0] + vy * g[1] + vz * g[2]);
+  wb[VX] += e * rho * g[0];
+  wb[VY] += e * rho * g[1];
+  wb[VZ] += e * rho * g[2];
+}
+
 // --- S1: per updated cell, ubar = VJP of cons2prim at the output; the
-// prim2cons of w^n that forms u^n gets ubar's hydro part --------------------
+// prim2cons of w^n that forms u^n gets ubar's hydro part; the predictor's
+// gravity term (stage input w^n) too --------------------------------------
 __device__ __forceinline__ void cells_body(const Inst& I, const StageArgs& a, int i, int j, const double* g) {
   const long long c = cidx(I, i, j);
   double wo[NM], ub[NM];
@@ -128,6 +145,7 @@ __device__ __forceinline__ void cells_body(const Inst& I, const StageArgs& a, in
 #pragma unroll
   for (int v = 0; v < NM; ++v) wb[v] = 0.;
   adj::vjp_prim2cons(wn, ub, I.gam, wb);
+  if (a.order == 0 && grav_on(I)) grav_vjp(I, a.dt, ub, wn[RHO], wn[VX], wn[VY], wn[VZ], wb);
 #pragma unroll
   for (int v = 0; v < NM; ++v) a.Vw[v * I.sv + c] += wb[v];
 }
@@ -358,6 +376,15 @@ __global__ void k_gather(const Inst I, const StageArgs a, const StageArgs next, 
       }
     }
     const long long c = cidx(I, i, j);
+    // the corrector's gravity term reads its stage input ws at updated cells
+    // (Ub of this cell is read before the fused predictor S1 below overwrites it)
+    if (a.order == 1 && in(R, i, j) && grav_on(I)) {
+      double ub[EN + 1];
+#pragma unroll
+      for (int v = 0; v <= EN; ++v) ub[v] = a.Ub[v * I.sv + c];
+      grav_vjp(I, a.dt, ub, a.Wsrc[RHO * I.sv + c], a.Wsrc[VX * I.sv + c], a.Wsrc[VY * I.sv + c],
+               a.Wsrc[VZ * I.sv + c], acc);
+    }
     // z face (cell-centred in 2D): bz = bz^n + ... on updated cells (reads Ub
     // of this cell before the fused predictor S1 below overwrites it)
     if (in(R, i, j)) a.Vb[2 * I.sv + c] += bz_total(I, a, i, j);

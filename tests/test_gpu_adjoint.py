@@ -50,6 +50,10 @@ def _rel(a, b):
     ("blast", 24, 1e-3, dict(limiter="mc")),
     ("blast_reflect", 20, 1e-3, dict(rsolver="hll")),
     ("mixed_bc", 20, 1e-3, dict(limiter="mm")),
+    # constant gravity (both stages' source terms), reflecting walls included
+    ("vortex", 24, 0.0, dict(limiter="mc", grav=(0.3, -0.8, 0.1))),
+    ("blast", 24, 1e-3, dict(grav=(0.5, -0.5, 0.2))),
+    ("blast_reflect", 20, 1e-3, dict(rsolver="hll", grav=(0.0, -1.0, 0.0))),
 ])
 def test_step_adjoint_matches_torch_autograd(case, n, noise, kw):
     import torch
@@ -58,7 +62,7 @@ def test_step_adjoint_matches_torch_autograd(case, n, noise, kw):
     G = T.Grid(gc, face_aware=True, device="cuda")
     p = P0.cuda().requires_grad_(True)
     b = B0.cuda().requires_grad_(True)
-    tp, tb = T.step(G, p, b, dt, rs=m["rsolver"], lim=m["limiter"])
+    tp, tb = T.step(G, p, b, dt, rs=m["rsolver"], lim=m["limiter"], grav=m.get("grav"))
     gen = torch.Generator(device="cpu").manual_seed(5)
     gp = torch.randn(tp.shape, generator=gen, dtype=torch.float64).cuda()
     gb = torch.randn(tb.shape, generator=gen, dtype=torch.float64).cuda()
@@ -87,12 +91,15 @@ def test_step_adjoint_matches_torch_autograd(case, n, noise, kw):
         assert _rel(ob[v, 0], ab[v]) < 1e-9, (v, _rel(ob[v, 0], ab[v]))
 
 
-@pytest.mark.parametrize("nsteps,every", [(7, 3), (6, 6), (5, 1)])
-def test_rollout_adjoint_matches_torch_autograd(nsteps, every):
+@pytest.mark.parametrize("nsteps,every,grav", [(7, 3, None), (6, 6, None), (5, 1, None), (6, 4, (0.2, -0.6, 0.0))])
+def test_rollout_adjoint_matches_torch_autograd(nsteps, every, grav):
     import torch
     import torch_vl2 as T
     from bonzo_b200.adjoint import rollout
-    gc, opts, m, P0, B0, dt = _state("vortex_pert", 32, limiter="mc")
+    kw = dict(limiter="mc")
+    if grav is not None:
+        kw["grav"] = grav
+    gc, opts, m, P0, B0, dt = _state("vortex_pert", 32, **kw)
     dt = 0.5 * dt
     G = T.Grid(gc, face_aware=True, device="cuda")
     gen = torch.Generator(device="cpu").manual_seed(9)
@@ -102,7 +109,7 @@ def test_rollout_adjoint_matches_torch_autograd(nsteps, every):
     b = B0.cuda().requires_grad_(True)
     x, y = p, b
     for _ in range(nsteps):
-        x, y = T.step(G, x, y, dt, rs="hlld", lim="mc")
+        x, y = T.step(G, x, y, dt, rs="hlld", lim="mc", grav=grav)
     loss_t = ((x[0] - target) ** 2).sum()
     ap, ab = torch.autograd.grad(loss_t, (p, b))
     # the adjoint through the autograd wrapper
@@ -224,3 +231,16 @@ def test_rollout_gradient_matches_central_differences_256():
     finally:
         T.BRANCHES.off()
     assert worst <= 1e-6, worst
+
+
+def test_adjoint_rejects_turbulence_driving():
+    """The driving force is a random field advanced every step that the tape
+    does not keep: the adjoint refuses it on the host, before any launch."""
+    from bonzo_b200 import _lib
+    gc, prim, bfld, opts = setup_case("vortex", n=16)
+    eng = device_ctx(opts, path="fused", rsolver="hlld", limiter="mc", drive_f0=0.5, drive_tau=1.0, drive_nmod=1)
+    eng.set_state(prim, bfld)
+    eng.init()
+    with pytest.raises(_lib.BnzError) as e:
+        eng.rollout_forward(3, 1e-4, 1)
+    assert e.value.code == _lib.BNZ_ERR_UNSUPPORTED and "driving" in str(e.value)
