@@ -1,7 +1,7 @@
 // bnz_adjoint_math.h -- pointwise vector-Jacobian products (reverse mode) of
 // the per-point math of the VL2 step: EOS conversions, the ideal-MHD flux,
-// the fast magnetosonic speed, the HLL and HLLD Riemann solvers and the PLM
-// slope limiters.  Hand-derived from the forward expressions in
+// the fast magnetosonic speed, the HLL, HLLT and HLLD Riemann solvers and
+// the PLM slope limiters.  Hand-derived from the forward expressions in
 // bnz_device.cuh (which restate src/mhd/eos_c.h, src/mhd/fluxes_c.c and
 // src/coordinates/reconstr_c.h); the reference has no adjoint.
 //
@@ -265,6 +265,231 @@ BNZ_HD void vjp_hll(const double* wL, const double* wR, double gam, const double
   aLb -= db;
   const double sLb = sL < 0. ? aLb : 0.;
   const double sRb = sR > 0. ? aRb : 0.;
+  vjp_flux(wL, fLb, gam, wLb);
+  vjp_flux(wR, fRb, gam, wRb);
+  vjp_prim2cons(wL, uLb, gam, wLb);
+  vjp_prim2cons(wR, uRb, gam, wRb);
+  vjp_wave_speeds(wL, wR, cfL, cfR, gam, sLb, sRb, wLb, wRb);
+}
+
+// HLLT flux (fluxes_c.c:447-607, as restated in bnz_device.cuh flux_hllt):
+// given fb, add wLb, wRb (the normal field's cotangent goes to the BX entries
+// of both sides; the caller sums them).  The star states' energy entries are
+// zero, as in the forward.  The fan region is the one the forward selects;
+// where it finds none (ERR_FAN) its flux is zero and so is the VJP.
+BNZ_HD void vjp_hllt(const double* wL, const double* wR, double gam, const double* fb, double* wLb, double* wRb) {
+  // ---- forward (values kept for the reverse sweep) ----
+  double uL[NM], uR[NM], fL[NM], fR[NM];
+  cons_of(wL, gam, uL);
+  cons_of(wR, gam, uR);
+  flux_of(wL, gam, fL);
+  flux_of(wR, gam, fR);
+  const double cfL = fms_val(wL, gam), cfR = fms_val(wR, gam);
+  const double cfm = cfL > cfR ? cfL : cfR;
+  const double sL = (wL[VX] < wR[VX] ? wL[VX] : wR[VX]) - cfm;
+  const double sR = (wL[VX] > wR[VX] ? wL[VX] : wR[VX]) + cfm;
+  const double bx = wL[BX], abx = fabs(bx);
+  const double Di = 1. / (sR - sL);
+  // HLL averages of rho, mx, the mass flux and the passive scalar
+  const double nr = sR * uR[RHO] - sL * uL[RHO] - (fR[RHO] - fL[RHO]);
+  const double nm = sR * uR[MX] - sL * uL[MX] - (fR[MX] - fL[MX]);
+  const double nf = sR * fL[RHO] - sL * fR[RHO] + sR * sL * (uR[RHO] - uL[RHO]);
+  const double np = sR * uR[PSC] - sL * uL[PSC] - (fR[PSC] - fL[PSC]);
+  const double rhos = nr * Di, mxs = nm * Di, frhos = nf * Di, pscs = np * Di;
+  const double us = frhos / rhos;
+  const double rhosi = 1. / rhos;
+  const double sqri = sqrt(rhosi);
+  const double sLs = us - abx * sqri, sRs = us + abx * sqri;
+  const double xL = 1. / ((sL - sLs) * (sL - sRs)), xR = 1. / ((sR - sLs) * (sR - sRs));
+  const double y1L = bx * xL * (us - wL[VX]), y1R = bx * xR * (us - wR[VX]);
+  const double AL = wL[RHO] * sq(sL - wL[VX]) - sq(bx), AR = wR[RHO] * sq(sR - wR[VX]) - sq(bx);
+  const double y2L = AL * rhosi * xL, y2R = AR * rhosi * xR;
+  double uLs[NM], uRs[NM], uCs[NM];
+  for (int n = 0; n < NM; ++n) uLs[n] = uRs[n] = uCs[n] = 0.;
+  uLs[RHO] = uRs[RHO] = uCs[RHO] = rhos;
+  uLs[MX] = uRs[MX] = uCs[MX] = mxs;
+  uLs[PSC] = uRs[PSC] = uCs[PSC] = pscs;
+  uLs[MY] = rhos * wL[VY] - y1L * wL[BY];
+  uRs[MY] = rhos * wR[VY] - y1R * wR[BY];
+  uLs[MZ] = rhos * wL[VZ] - y1L * wL[BZ];
+  uRs[MZ] = rhos * wR[VZ] - y1R * wR[BZ];
+  uLs[BY] = y2L * wL[BY];
+  uRs[BY] = y2R * wR[BY];
+  uLs[BZ] = y2L * wL[BZ];
+  uRs[BZ] = y2R * wR[BZ];
+  const double x = 0.5 * sgn(bx) / sqri, xr = x * rhosi;
+  uCs[MY] = 0.5 * (uLs[MY] + uRs[MY]) + x * (uRs[BY] - uLs[BY]);
+  uCs[MZ] = 0.5 * (uLs[MZ] + uRs[MZ]) + x * (uRs[BZ] - uLs[BZ]);
+  uCs[BY] = 0.5 * (uLs[BY] + uRs[BY]) + xr * (uRs[MY] - uLs[MY]);
+  uCs[BZ] = 0.5 * (uLs[BZ] + uRs[BZ]) + xr * (uRs[MZ] - uLs[MZ]);
+  int r = 0;
+  if (sL > 0.) r = 1;
+  if (sL <= 0. && 0. < sLs) r = 2;
+  if (sLs <= 0. && 0. < sRs) r = 3;
+  if (sRs <= 0. && 0. < sR) r = 4;
+  if (sR <= 0.) r = 5;
+  if (r == 0) return;
+  // ---- reverse ----
+  double fLb[NM], fRb[NM], uLb[NM], uRb[NM], uLsb[NM], uRsb[NM], uCsb[NM];
+  for (int n = 0; n < NM; ++n) fLb[n] = fRb[n] = uLb[n] = uRb[n] = uLsb[n] = uRsb[n] = uCsb[n] = 0.;
+  double sLb = 0., sRb = 0., sLsb = 0., sRsb = 0.;
+  for (int n = 0; n < NM; ++n) {
+    const double g = n == BX ? 0. : fb[n];
+    if (r == 1) {
+      fLb[n] += g;
+    } else if (r == 2 || r == 3) {  // fL + sL (uL* - uL) [+ sL* (uC* - uL*)]
+      fLb[n] += g;
+      sLb += g * (uLs[n] - uL[n]);
+      uLsb[n] += sL * g;
+      uLb[n] -= sL * g;
+      if (r == 3) {
+        sLsb += g * (uCs[n] - uLs[n]);
+        uCsb[n] += sLs * g;
+        uLsb[n] -= sLs * g;
+      }
+    } else if (r == 4) {  // fR + sR (uR* - uR)
+      fRb[n] += g;
+      sRb += g * (uRs[n] - uR[n]);
+      uRsb[n] += sR * g;
+      uRb[n] -= sR * g;
+    } else {
+      fRb[n] += g;
+    }
+  }
+  // central state
+  double rhosb = uCsb[RHO], mxsb = uCsb[MX], pscsb = uCsb[PSC], xb = 0., xrb = 0.;
+  {
+    const double c = uCsb[MY];
+    uLsb[MY] += 0.5 * c;
+    uRsb[MY] += 0.5 * c;
+    xb += c * (uRs[BY] - uLs[BY]);
+    uRsb[BY] += c * x;
+    uLsb[BY] -= c * x;
+  }
+  {
+    const double c = uCsb[MZ];
+    uLsb[MZ] += 0.5 * c;
+    uRsb[MZ] += 0.5 * c;
+    xb += c * (uRs[BZ] - uLs[BZ]);
+    uRsb[BZ] += c * x;
+    uLsb[BZ] -= c * x;
+  }
+  {
+    const double c = uCsb[BY];
+    uLsb[BY] += 0.5 * c;
+    uRsb[BY] += 0.5 * c;
+    xrb += c * (uRs[MY] - uLs[MY]);
+    uRsb[MY] += c * xr;
+    uLsb[MY] -= c * xr;
+  }
+  {
+    const double c = uCsb[BZ];
+    uLsb[BZ] += 0.5 * c;
+    uRsb[BZ] += 0.5 * c;
+    xrb += c * (uRs[MZ] - uLs[MZ]);
+    uRsb[MZ] += c * xr;
+    uLsb[MZ] -= c * xr;
+  }
+  xb += xrb * rhosi;
+  double rhosib = xrb * x;
+  double sqrib = -xb * x / sqri;  // x = 0.5 sgn(bx) / sqri
+  // outer star states
+  rhosb += uLsb[RHO] + uRsb[RHO];
+  mxsb += uLsb[MX] + uRsb[MX];
+  pscsb += uLsb[PSC] + uRsb[PSC];
+  rhosb += uLsb[MY] * wL[VY] + uLsb[MZ] * wL[VZ] + uRsb[MY] * wR[VY] + uRsb[MZ] * wR[VZ];
+  wLb[VY] += uLsb[MY] * rhos;
+  wLb[VZ] += uLsb[MZ] * rhos;
+  wRb[VY] += uRsb[MY] * rhos;
+  wRb[VZ] += uRsb[MZ] * rhos;
+  const double y1Lb = -(uLsb[MY] * wL[BY] + uLsb[MZ] * wL[BZ]);
+  const double y1Rb = -(uRsb[MY] * wR[BY] + uRsb[MZ] * wR[BZ]);
+  wLb[BY] += uLsb[BY] * y2L - uLsb[MY] * y1L;
+  wLb[BZ] += uLsb[BZ] * y2L - uLsb[MZ] * y1L;
+  wRb[BY] += uRsb[BY] * y2R - uRsb[MY] * y1R;
+  wRb[BZ] += uRsb[BZ] * y2R - uRsb[MZ] * y1R;
+  const double y2Lb = uLsb[BY] * wL[BY] + uLsb[BZ] * wL[BZ];
+  const double y2Rb = uRsb[BY] * wR[BY] + uRsb[BZ] * wR[BZ];
+  // y2 = (rho (s - vx)^2 - bx^2) / rho* x
+  double bxb = 0., xLb = 0., xRb = 0., usb = 0.;
+  {
+    const double Ab = y2Lb * rhosi * xL;
+    rhosib += y2Lb * AL * xL;
+    xLb += y2Lb * AL * rhosi;
+    wLb[RHO] += Ab * sq(sL - wL[VX]);
+    const double t = Ab * wL[RHO] * 2. * (sL - wL[VX]);
+    sLb += t;
+    wLb[VX] -= t;
+    bxb -= Ab * 2. * bx;
+  }
+  {
+    const double Ab = y2Rb * rhosi * xR;
+    rhosib += y2Rb * AR * xR;
+    xRb += y2Rb * AR * rhosi;
+    wRb[RHO] += Ab * sq(sR - wR[VX]);
+    const double t = Ab * wR[RHO] * 2. * (sR - wR[VX]);
+    sRb += t;
+    wRb[VX] -= t;
+    bxb -= Ab * 2. * bx;
+  }
+  // y1 = bx x (u* - vx)
+  bxb += y1Lb * xL * (us - wL[VX]) + y1Rb * xR * (us - wR[VX]);
+  xLb += y1Lb * bx * (us - wL[VX]);
+  xRb += y1Rb * bx * (us - wR[VX]);
+  usb += y1Lb * bx * xL + y1Rb * bx * xR;
+  wLb[VX] -= y1Lb * bx * xL;
+  wRb[VX] -= y1Rb * bx * xR;
+  // x = 1 / ((s - sL*) (s - sR*))
+  {
+    const double qb = -xLb * xL * xL;
+    sLb += qb * ((sL - sRs) + (sL - sLs));
+    sLsb -= qb * (sL - sRs);
+    sRsb -= qb * (sL - sLs);
+  }
+  {
+    const double qb = -xRb * xR * xR;
+    sRb += qb * ((sR - sRs) + (sR - sLs));
+    sLsb -= qb * (sR - sRs);
+    sRsb -= qb * (sR - sLs);
+  }
+  // sL* = u* - |bx| sqri, sR* = u* + |bx| sqri
+  usb += sLsb + sRsb;
+  sqrib += (sRsb - sLsb) * abx;
+  bxb += (sRsb - sLsb) * sqri * sgn(bx);
+  rhosib += sqrib * 0.5 / sqri;
+  rhosb -= rhosib * rhosi * rhosi;
+  // u* = frho* / rho*
+  const double frhosb = usb / rhos;
+  rhosb -= usb * us / rhos;
+  // the averages: numerator / (sR - sL)
+  const double Dib = rhosb * nr + mxsb * nm + frhosb * nf + pscsb * np;
+  {
+    const int ks[3] = {RHO, MX, PSC};
+    const double bs[3] = {rhosb * Di, mxsb * Di, pscsb * Di};
+    for (int q = 0; q < 3; ++q) {
+      const int k = ks[q];
+      const double b = bs[q];
+      sRb += b * uR[k];
+      uRb[k] += b * sR;
+      sLb -= b * uL[k];
+      uLb[k] -= b * sL;
+      fRb[k] -= b;
+      fLb[k] += b;
+    }
+  }
+  {
+    const double b = frhosb * Di;
+    sRb += b * (fL[RHO] + sL * (uR[RHO] - uL[RHO]));
+    sLb += b * (-fR[RHO] + sR * (uR[RHO] - uL[RHO]));
+    fLb[RHO] += b * sR;
+    fRb[RHO] -= b * sL;
+    uRb[RHO] += b * sR * sL;
+    uLb[RHO] -= b * sR * sL;
+  }
+  const double Db = -Dib * Di * Di;
+  sRb += Db;
+  sLb -= Db;
+  wLb[BX] += bxb;
   vjp_flux(wL, fLb, gam, wLb);
   vjp_flux(wR, fRb, gam, wRb);
   vjp_prim2cons(wL, uLb, gam, wLb);

@@ -11,7 +11,7 @@
 
 extern "C" {
 
-// forward Riemann flux (rs: 0 hll, 2 hlld) of one face; wL[BX] is the normal field
+// forward Riemann flux (rs: 0 hll, 2 hlld, 3 hllt) of one face; wL[BX] is the normal field
 void t_flux(int rs, const double* wL, const double* wR, double gam, double* f) {
   unsigned err = 0;
   double l[9], r[9];
@@ -21,6 +21,7 @@ void t_flux(int rs, const double* wL, const double* wR, double gam, double* f) {
   }
   r[dev::BX] = l[dev::BX];
   if (rs == 2) dev::flux_hlld(f, l, r, gam, err);
+  else if (rs == 3) dev::flux_hllt(f, l, r, gam, err);
   else dev::flux_hll(f, l, r, gam);
 }
 
@@ -34,6 +35,7 @@ void t_vjp_flux(int rs, const double* wL, const double* wR, double gam, const do
   }
   r[dev::BX] = l[dev::BX];
   if (rs == 2) adj::vjp_hlld(l, r, gam, fb, wLb, wRb);
+  else if (rs == 3) adj::vjp_hllt(l, r, gam, fb, wLb, wRb);
   else adj::vjp_hll(l, r, gam, fb, wLb, wRb);
 }
 
@@ -62,6 +64,34 @@ int t_hlld_region(const double* wL, const double* wR, double gam) {
   if (sM <= 0. && 0. < sRs) k = 4;
   if (sRs <= 0. && 0. < sR) k = 5;
   if (sR <= 0.) k = 6;
+  return k;
+}
+
+// HLLT wave-fan region (1..5, 0 where the forward flags ERR_FAN)
+int t_hllt_region(const double* wL, const double* wR, double gam) {
+  double l[9], r[9];
+  for (int n = 0; n < 9; ++n) {
+    l[n] = wL[n];
+    r[n] = wR[n];
+  }
+  r[dev::BX] = l[dev::BX];
+  double uL[9], uR[9], fL[9], fR[9];
+  dev::prim2cons(uL, l, gam);
+  dev::prim2cons(uR, r, gam);
+  dev::primcons2flux(fL, l, uL);
+  dev::primcons2flux(fR, r, uR);
+  double sL, sR;
+  dev::wave_speeds(l, r, gam, sL, sR);
+  const double rhos = (sR * uR[0] - sL * uL[0] - (fR[0] - fL[0])) / (sR - sL);
+  const double us = (sR * fL[0] - sL * fR[0] + sR * sL * (uR[0] - uL[0])) / (sR - sL) / rhos;
+  const double a = fabs(l[dev::BX]) * sqrt(1. / rhos);
+  const double sLs = us - a, sRs = us + a;
+  int k = 0;
+  if (sL > 0.) k = 1;
+  if (sL <= 0. && 0. < sLs) k = 2;
+  if (sLs <= 0. && 0. < sRs) k = 3;
+  if (sRs <= 0. && 0. < sR) k = 4;
+  if (sR <= 0.) k = 5;
   return k;
 }
 

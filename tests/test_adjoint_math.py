@@ -25,6 +25,7 @@ def lib():
     L.t_flux.argtypes = [C.c_int, dp, dp, C.c_double, dp]
     L.t_vjp_flux.argtypes = [C.c_int, dp, dp, C.c_double, dp, dp, dp]
     L.t_hlld_region.argtypes = [dp, dp, C.c_double]
+    L.t_hllt_region.argtypes = [dp, dp, C.c_double]
     L.t_cons2prim.argtypes = [dp, C.c_double, dp]
     L.t_prim2cons.argtypes = [dp, C.c_double, dp]
     L.t_vjp_cons2prim.argtypes = [dp, dp, C.c_double, dp]
@@ -83,7 +84,7 @@ def fd_flux(L, rs, wL, wR, fb, h):
     return np.array(g)
 
 
-@pytest.mark.parametrize("rs", [0, 2], ids=["hll", "hlld"])
+@pytest.mark.parametrize("rs", [0, 2, 3], ids=["hll", "hlld", "hllt"])
 def test_riemann_vjp_matches_finite_differences(lib, rs):
     rng = np.random.default_rng(7 + rs)
     ok = skipped = 0
@@ -106,10 +107,14 @@ def test_riemann_vjp_matches_finite_differences(lib, rs):
         ok += 1
         if rs == 2:
             regions.add(lib.t_hlld_region(wL, wR, GAM))
+        if rs == 3:
+            regions.add(lib.t_hllt_region(wL, wR, GAM))
     assert skipped <= 8, skipped
     assert ok >= 140
     if rs == 2:
         assert regions == {1, 2, 3, 4, 5, 6}, regions
+    if rs == 3:
+        assert regions == {1, 2, 3, 4, 5}, regions
 
 
 def test_eos_vjps_match_finite_differences(lib):

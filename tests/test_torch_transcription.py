@@ -15,6 +15,9 @@ from helpers import oracle_sim, setup_case
     ("mixed_bc", 16, dict(limiter="mm")),
     ("blast", 16, dict(grav=(0.3, -1.2, 0.05))),
     ("vortex", 16, dict(limiter="mc", rsolver="hll", grav=(-0.7, 0.4, 0.0))),
+    ("vortex", 20, dict(limiter="mc", rsolver="hllt")),
+    ("blast", 20, dict(rsolver="hllt")),
+    ("mixed_bc", 16, dict(limiter="mm", rsolver="hllt")),
 ])
 def test_transcription_matches_oracle_step(case, n, kw):
     import torch

@@ -6,9 +6,9 @@ oracle (forward) and with the hand-written adjoint (torch autograd).
 It restates, in vectorised torch, the same algorithm as oracle/bnz_oracle.c:
 the predictor of src/integration/vanleer.pyx:104-120 (donor cell, dt/2, cells
 1..Ntot-2), the corrector of vanleer.pyx:130-151 (PLM, dt, active cells), the
-Riemann solvers of src/mhd/fluxes_c.c:175-223 (HLL) and :616-834 (HLLD), the
-limiters of src/coordinates/reconstr_c.h:28-44 and the CT update of
-src/integration/ct.pyx:15-215.  Ghost values are read through the boundary
+Riemann solvers of src/mhd/fluxes_c.c:175-223 (HLL), :447-607 (HLLT) and
+:616-834 (HLLD), the limiters of src/coordinates/reconstr_c.h:28-44 and the
+CT update of src/integration/ct.pyx:15-215.  Ghost values are read through the boundary
 maps of src/bc/grid_bc_funcs.pyx (periodic, outflow with the face-aware
 option, reflect), as the fused path does.
 
@@ -268,6 +268,59 @@ def hlld(wL, wR, gam):
     return out
 
 
+def hllt(wL, wR, gam):
+    """The three-wave solver of fluxes_c.c:447-607 as the device restates it
+    (bnz_device.cuh flux_hllt): star-state energies zero, a zero flux where no
+    fan region matches."""
+    uL, uR = prim2cons(wL, gam), prim2cons(wR, gam)
+    fL, fR = flux(wL, uL), flux(wR, uR)
+    sL, sR = wave_speeds(wL, wR, gam)
+    bx = wL[BX]
+    sRsLi = 1.0 / (sR - sL)
+    rhos = (sR * uR[RHO] - sL * uL[RHO] - (fR[RHO] - fL[RHO])) * sRsLi
+    mxs = (sR * uR[1] - sL * uL[1] - (fR[1] - fL[1])) * sRsLi
+    frhos = (sR * fL[RHO] - sL * fR[RHO] + sR * sL * (uR[RHO] - uL[RHO])) * sRsLi
+    us = frhos / rhos
+    pscs = (sR * uR[PSC] - sL * uL[PSC] - (fR[PSC] - fL[PSC])) * sRsLi
+    rhosi = 1.0 / rhos
+    sqri = torch.sqrt(rhosi)
+    sgnb = branch_sign(bx)
+    absbx = sgnb * bx
+    sLs = us - absbx * sqri
+    sRs = us + absbx * sqri
+    zero = torch.zeros_like(rhos)
+    star = {}
+    for side, w, s in (("L", wL, sL), ("R", wR, sR)):
+        xs = 1.0 / ((s - sLs) * (s - sRs))
+        y1 = bx * xs * (us - w[VX])
+        y2 = (w[RHO] * (s - w[VX]) ** 2 - bx ** 2) * rhosi * xs
+        star[side] = [rhos, mxs, rhos * w[VY] - y1 * w[BY], rhos * w[VZ] - y1 * w[BZ], zero, pscs, zero,
+                      y2 * w[BY], y2 * w[BZ]]
+    uLs, uRs = star["L"], star["R"]
+    x = 0.5 * sgnb / sqri
+    uCs = [rhos, mxs,
+           0.5 * (uLs[VY] + uRs[VY]) + x * (uRs[BY] - uLs[BY]),
+           0.5 * (uLs[VZ] + uRs[VZ]) + x * (uRs[BZ] - uLs[BZ]),
+           zero, pscs, zero,
+           0.5 * (uLs[BY] + uRs[BY]) + x * rhosi * (uRs[VY] - uLs[VY]),
+           0.5 * (uLs[BZ] + uRs[BZ]) + x * rhosi * (uRs[VZ] - uLs[VZ])]
+    r1 = cond(sL > 0)
+    r2 = cond((sL <= 0) & (0 < sLs))
+    r3 = cond((sLs <= 0) & (0 < sRs))
+    r4 = cond((sRs <= 0) & (0 < sR))
+    r5 = cond(sR <= 0)
+    out = []
+    for n in range(9):
+        lstar = fL[n] + sL * (uLs[n] - uL[n])
+        v = torch.zeros_like(rhos)
+        for m, val in ((r1, fL[n]), (r2, lstar), (r3, lstar + sLs * (uCs[n] - uLs[n])),
+                       (r4, fR[n] + sR * (uRs[n] - uR[n])), (r5, fR[n])):
+            v = torch.where(m, val, v)
+        out.append(v)
+    out[BX] = torch.zeros_like(out[0])
+    return out
+
+
 def _mm(a, b):
     return torch.where(cond(a * b <= 0), torch.zeros_like(a),
                        torch.where(cond(a > 0), torch.where(cond(a < b), a, b), torch.where(cond(a > b), a, b)))
@@ -296,7 +349,7 @@ def stage(G, Wf, Bf, Wn, Bn, dt, order, R, gam, rs, lim, grav=None):
     with the density and velocity of the stage input Wf.  Returns prim (9, R),
     bx faces (R rows, ia..ib+1), by faces (ja..jb+1, R columns), bz (R)."""
     ia, ib, ja, jb = R
-    solver = hlld if rs == "hlld" else hll
+    solver = {"hlld": hlld, "hllt": hllt}.get(rs, hll)
     # x faces i = ia..ib+1 on rows ja-1..jb+1
     rows = slice(ja - 1, jb + 2)
     if order == 0:
