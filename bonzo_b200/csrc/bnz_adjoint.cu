@@ -62,8 +62,8 @@ int check_adjoint_ctx(bnz_ctx* c) {
   if (c->md.path != BNZ_PATH_FUSED)
     return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built for the fused 2D path (path = fused)");
   if (c->md.kappa0 > 0.) return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint covers the hyperbolic step only (kappa0 = 0)");
-  if (c->md.rsolver != BNZ_RS_HLL && c->md.rsolver != BNZ_RS_HLLD)
-    return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built for rsolver hll and hlld");
+  if (c->md.rsolver != BNZ_RS_HLL && c->md.rsolver != BNZ_RS_HLLD && c->md.rsolver != BNZ_RS_HLLT)
+    return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built for rsolver hll, hllt and hlld");
   if (c->md.charact_proj) return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built without charact_proj");
   // constant gravity is differentiated; the driving force is a random field
   // advanced every step, which the tape does not keep

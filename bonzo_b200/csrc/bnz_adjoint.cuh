@@ -274,6 +274,7 @@ __device__ __forceinline__ void face_vjp(const Inst& I, const StageArgs& a, int 
 #pragma unroll
     for (int v = 0; v < NM; ++v) wLb[v] = wRb[v] = 0.;
     if (RS == dev::RS_HLLD) adj::vjp_hlld(wL, wR, I.gam, fb, wLb, wRb);
+    else if (RS == dev::RS_HLLT) adj::vjp_hllt(wL, wR, I.gam, fb, wLb, wRb);
     else adj::vjp_hll(wL, wR, I.gam, fb, wLb, wRb);
     // per-cell contributions, global variable order
     double* Qa = a.Q + (long long)AX * 4 * NM * I.sv;

@@ -526,6 +526,9 @@ int adj_step(const FusedInst& I, const AdjStep& s) {
   if (s.rsolver == dev::RS_HLLD) {
     adj_stage<dev::RS_HLLD>(I, a, s.limiter, s.stream, true, &a0);
     adj_stage<dev::RS_HLLD>(I, a0, s.limiter, s.stream, false, nullptr);
+  } else if (s.rsolver == dev::RS_HLLT) {
+    adj_stage<dev::RS_HLLT>(I, a, s.limiter, s.stream, true, &a0);
+    adj_stage<dev::RS_HLLT>(I, a0, s.limiter, s.stream, false, nullptr);
   } else {
     adj_stage<dev::RS_HLL>(I, a, s.limiter, s.stream, true, &a0);
     adj_stage<dev::RS_HLL>(I, a0, s.limiter, s.stream, false, nullptr);
