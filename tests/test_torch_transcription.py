@@ -18,6 +18,9 @@ from helpers import oracle_sim, setup_case
     ("vortex", 20, dict(limiter="mc", rsolver="hllt")),
     ("blast", 20, dict(rsolver="hllt")),
     ("mixed_bc", 16, dict(limiter="mm", rsolver="hllt")),
+    ("vortex_pert", 20, dict(limiter="mc", charact_proj=1)),
+    ("blast", 20, dict(charact_proj=1)),
+    ("blast_reflect", 16, dict(limiter="mm", rsolver="hll", charact_proj=1)),
 ])
 def test_transcription_matches_oracle_step(case, n, kw):
     import torch
@@ -34,14 +37,15 @@ def test_transcription_matches_oracle_step(case, n, kw):
     P1, _, B1 = o.get_state()
     G = T.Grid(gc, face_aware=True)
     tp, tb = T.step(G, torch.from_numpy(P0[:, 0].copy()), torch.from_numpy(B0[:, 0].copy()), dt,
-                    rs=m["rsolver"], lim=m["limiter"], grav=m.get("grav"))
+                    rs=m["rsolver"], lim=m["limiter"], grav=m.get("grav"), charact=bool(m.get("charact_proj")))
     for a, b in ((tp.numpy(), P1[:, 0]), (tb.numpy(), B1[:, 0])):
         for v in range(a.shape[0]):
             s = max(np.abs(b[v]).max(), 1e-300)
             assert np.abs(a[v] - b[v]).max() <= 1e-13 * s
 
 
-def test_branch_frozen_differences_converge_to_autograd():
+@pytest.mark.parametrize("charact", [False, True], ids=["plm", "charact_proj"])
+def test_branch_frozen_differences_converge_to_autograd(charact):
     import torch
     import torch_vl2 as T
     from bonzo_b200 import problems as P
@@ -60,7 +64,7 @@ def test_branch_frozen_differences_converge_to_autograd():
     def L(p, b):
         x, y = p, b
         for _ in range(nsteps):
-            x, y = T.step(G, x, y, dt, rs="hlld", lim="mc")
+            x, y = T.step(G, x, y, dt, rs="hlld", lim="mc", charact=charact)
         return ((x[0] - tgt) ** 2).sum() + (x[1] ** 2).sum()
 
     p = p0.clone().requires_grad_(True)

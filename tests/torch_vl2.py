@@ -7,8 +7,10 @@ It restates, in vectorised torch, the same algorithm as oracle/bnz_oracle.c:
 the predictor of src/integration/vanleer.pyx:104-120 (donor cell, dt/2, cells
 1..Ntot-2), the corrector of vanleer.pyx:130-151 (PLM, dt, active cells), the
 Riemann solvers of src/mhd/fluxes_c.c:175-223 (HLL), :447-607 (HLLT) and
-:616-834 (HLLD), the limiters of src/coordinates/reconstr_c.h:28-44 and the
-CT update of src/integration/ct.pyx:15-215.  Ghost values are read through the boundary
+:616-834 (HLLD), the limiters of src/coordinates/reconstr_c.h:28-44 (with the
+characteristic projection of reconstr_c.c:54-91 and src/mhd/eos_c.h:100-333
+as an option), constant gravity (src/srcterms/gravity.pyx:54-69) and the CT
+update of src/integration/ct.pyx:15-215.  Ghost values are read through the boundary
 maps of src/bc/grid_bc_funcs.pyx (periodic, outflow with the face-aware
 option, reflect), as the fused path does.
 
@@ -321,6 +323,101 @@ def hllt(wL, wR, gam):
     return out
 
 
+def _abs(x):
+    return torch.where(cond(x >= 0), x, -x)
+
+
+def _char_basis(w, gam):
+    """The eigen-system coefficients that prim2char / char2prim of
+    src/mhd/eos_c.h:100-216, 245-333 (bnz_device.cuh) build from the cell
+    state w (local sweep frame)."""
+    rho, p, bx, by, bz = w[RHO], w[PR], w[BX], w[BY], w[BZ]
+    rhoi = 1.0 / rho
+    s = branch_sign(bx)
+    a2rho = gam * p
+    a = torch.sqrt(a2rho * rhoi)
+    bx2 = bx ** 2
+    bperp2 = by ** 2 + bz ** 2
+    x = a2rho + (bx2 + bperp2)
+    y = torch.sqrt(_abs(x * x - 4.0 * a2rho * bx2))
+    cf2rho = 0.5 * (x + y)
+    cs2rho = 0.5 * (x - y)
+    cf = torch.sqrt(rhoi * cf2rho)
+    cs = torch.sqrt(rhoi * _abs(cs2rho))
+    z = 1.0 / (cf2rho - cs2rho)
+    one, zero = torch.ones_like(rho), torch.zeros_like(rho)
+    c1, c2, c3 = cond(cf <= cs), cond(a <= cs), cond(cf <= a)
+    af = torch.where(c1, one, torch.where(c2, zero, torch.where(c3, one, torch.sqrt(z * _abs(a2rho - cs2rho)))))
+    as_ = torch.where(c1, zero, torch.where(c2, one, torch.where(c3, zero, torch.sqrt(z * _abs(cf2rho - a2rho)))))
+    nz = cond(bperp2 != 0)
+    bperpi = 1.0 / torch.sqrt(torch.where(nz, bperp2, one))
+    betay = torch.where(nz, bperpi * by, zero)
+    betaz = torch.where(nz, bperpi * bz, zero)
+    return dict(rho=rho, rhoi=rhoi, s=s, a2rho=a2rho, a=a, cf=cf, cs=cs, af=af, as_=as_, betay=betay, betaz=betaz)
+
+
+def prim2char(d, k):
+    """Differences d (9, local frame) into the characteristic basis; PSC and
+    BX pass through."""
+    rhoi, s, a, cf, cs = k["rhoi"], k["s"], k["a"], k["cf"], k["cs"]
+    by_, bz_ = k["betay"], k["betaz"]
+    nf = 0.5 / (k["a2rho"] * rhoi)
+    qf_ = nf * cf * k["af"] * s
+    qs_ = nf * cs * k["as_"] * s
+    af_ = nf * k["af"]
+    as__ = nf * k["as_"]
+    rhoisr = torch.sqrt(rhoi)
+    arhoisr = a * rhoisr
+    Af_ = af_ * arhoisr
+    As_ = as__ * arhoisr
+    x = s * rhoisr
+    v = by_ * d[VY] + bz_ * d[VZ]
+    b = by_ * d[BY] + bz_ * d[BZ]
+    out = list(d)
+    out[RHO] = af_ * (rhoi * d[PR] - cf * d[VX]) + qs_ * v + As_ * b
+    out[VX] = 0.5 * ((-bz_ * d[VY] + by_ * d[VZ]) + x * (-bz_ * d[BY] + by_ * d[BZ]))
+    out[VY] = as__ * (rhoi * d[PR] - cs * d[VX]) - qf_ * v - Af_ * b
+    out[VZ] = d[RHO] - 2.0 * nf * d[PR]
+    out[PR] = as__ * (rhoi * d[PR] + cs * d[VX]) + qf_ * v - Af_ * b
+    out[BY] = 0.5 * ((bz_ * d[VY] - by_ * d[VZ]) + x * (-bz_ * d[BY] + by_ * d[BZ]))
+    out[BZ] = af_ * (rhoi * d[PR] + cf * d[VX]) - qs_ * v + As_ * b
+    return out
+
+
+def char2prim(c, k):
+    """Characteristic amplitudes c (9) back to primitive differences."""
+    rho, s, a, cf, cs, af, as_ = k["rho"], k["s"], k["a"], k["cf"], k["cs"], k["af"], k["as_"]
+    by_, bz_ = k["betay"], k["betaz"]
+    qf = cf * af * s
+    qs = cs * as_ * s
+    rhosr = torch.sqrt(rho)
+    arhosr = a * rhosr
+    Af = af * arhosr
+    As = as_ * arhosr
+    fa = af * (c[RHO] + c[BZ]) + as_ * (c[VY] + c[PR])
+    t = qs * (c[RHO] - c[BZ]) - qf * (c[VY] - c[PR])
+    u = As * (c[RHO] + c[BZ]) - Af * (c[VY] + c[PR])
+    out = list(c)
+    out[RHO] = rho * fa + c[VZ]
+    out[VX] = cf * af * (c[BZ] - c[RHO]) + cs * as_ * (c[PR] - c[VY])
+    out[VY] = by_ * t - bz_ * (c[VX] - c[BY])
+    out[VZ] = bz_ * t + by_ * (c[VX] - c[BY])
+    out[PR] = k["a2rho"] * fa
+    out[BY] = by_ * u - bz_ * s * rhosr * (c[VX] + c[BY])
+    out[BZ] = bz_ * u + by_ * s * rhosr * (c[VX] + c[BY])
+    return out
+
+
+def half_slopes_char(wm, wc, wp, gam, lim):
+    """reconstr_c.c:54-91 with charact_proj: the one-sided differences of all
+    nine local variables projected on the cell's characteristic basis,
+    limited, halved and projected back."""
+    k = _char_basis(wc, gam)
+    dm = prim2char([wc[n] - wm[n] for n in range(9)], k)
+    dp = prim2char([wp[n] - wc[n] for n in range(9)], k)
+    return char2prim([0.5 * limit(lim, dm[n], dp[n]) for n in range(9)], k)
+
+
 def _mm(a, b):
     return torch.where(cond(a * b <= 0), torch.zeros_like(a),
                        torch.where(cond(a > 0), torch.where(cond(a < b), a, b), torch.where(cond(a > b), a, b)))
@@ -341,7 +438,19 @@ def limit(lim, a, b):
 # one stage of the step and the whole step
 # ---------------------------------------------------------------------------
 
-def stage(G, Wf, Bf, Wn, Bn, dt, order, R, gam, rs, lim, grav=None):
+def _plm_faces(c, gam, lim, charact):
+    """Face states from the four cells c[0..3] (local frame) around each face:
+    wL from the slope of c[1], wR from that of c[2]."""
+    if charact:
+        dL = half_slopes_char(c[0], c[1], c[2], gam, lim)
+        dR = half_slopes_char(c[1], c[2], c[3], gam, lim)
+        return [c[1][v] + dL[v] for v in range(9)], [c[2][v] - dR[v] for v in range(9)]
+    wL = [c[1][v] + 0.5 * limit(lim, c[1][v] - c[0][v], c[2][v] - c[1][v]) for v in range(9)]
+    wR = [c[2][v] - 0.5 * limit(lim, c[2][v] - c[1][v], c[3][v] - c[2][v]) for v in range(9)]
+    return wL, wR
+
+
+def stage(G, Wf, Bf, Wn, Bn, dt, order, R, gam, rs, lim, grav=None, charact=False):
     """Fluxes, EMFs and the update on cells R = (ia, ib, ja, jb).  Wf / Bf are
     the cell / face arrays the fluxes read, Wn / Bn the state whose u^n and
     faces are updated (all as read).  With `grav` (gx, gy, gz) the constant
@@ -357,8 +466,7 @@ def stage(G, Wf, Bf, Wn, Bn, dt, order, R, gam, rs, lim, grav=None):
         wR = [Wf[v][rows, ia:ib + 2] for v in range(9)]
     else:
         c = [[Wf[v][rows, ia - 2 + q:ib + q] for v in range(9)] for q in range(4)]
-        wL = [c[1][v] + 0.5 * limit(lim, c[1][v] - c[0][v], c[2][v] - c[1][v]) for v in range(9)]
-        wR = [c[2][v] - 0.5 * limit(lim, c[2][v] - c[1][v], c[3][v] - c[2][v]) for v in range(9)]
+        wL, wR = _plm_faces(c, gam, lim, charact)
     wL[BX] = wR[BX] = Bf[0][rows, ia:ib + 2]
     Fx = solver(wL, wR, gam)                      # (jb-ja+3, ib-ia+2), global order
     # y faces j = ja..jb+1 on columns ia-1..ib+1
@@ -368,8 +476,7 @@ def stage(G, Wf, Bf, Wn, Bn, dt, order, R, gam, rs, lim, grav=None):
         wR = [Wf[PERM_Y[n]][ja:jb + 2, cols] for n in range(9)]
     else:
         c = [[Wf[PERM_Y[n]][ja - 2 + q:jb + q, cols] for n in range(9)] for q in range(4)]
-        wL = [c[1][n] + 0.5 * limit(lim, c[1][n] - c[0][n], c[2][n] - c[1][n]) for n in range(9)]
-        wR = [c[2][n] - 0.5 * limit(lim, c[2][n] - c[1][n], c[3][n] - c[2][n]) for n in range(9)]
+        wL, wR = _plm_faces(c, gam, lim, charact)
     wL[BX] = wR[BX] = Bf[1][ja:jb + 2, cols]
     fy = solver(wL, wR, gam)
     Fy = [None] * 9
@@ -425,7 +532,7 @@ def stage(G, Wf, Bf, Wn, Bn, dt, order, R, gam, rs, lim, grav=None):
     return torch.stack(cons2prim(u, gam)), bxf, byf, bz
 
 
-def step(G, prim, bfld, dt, gam=5.0 / 3.0, rs="hlld", lim="vl", grav=None):
+def step(G, prim, bfld, dt, gam=5.0 / 3.0, rs="hlld", lim="vl", grav=None, charact=False):
     """One VL2 step: returns (prim, bfld) as the library's get_state gives them
     (ghosts filled through the maps).  `grav`: constant gravity (gx, gy, gz),
     none when absent or all zero."""
@@ -442,7 +549,7 @@ def step(G, prim, bfld, dt, gam=5.0 / 3.0, rs="hlld", lim="vl", grav=None):
     Bs[1, ja:jb + 2, ia:ib + 1] = bys
     Bs[2, ja:jb + 1, ia:ib + 1] = bzs
     ia, ib, ja, jb = G.R1
-    w1, bx1, by1, bz1 = stage(G, Ws, Bs, wr, br, dt, 1, G.R1, gam, rs, lim, grav)
+    w1, bx1, by1, bz1 = stage(G, Ws, Bs, wr, br, dt, 1, G.R1, gam, rs, lim, grav, charact)
     C = torch.zeros_like(prim)
     C[:, ja:jb + 1, ia:ib + 1] = w1
     Cb = torch.zeros_like(bfld)
