@@ -952,6 +952,216 @@ BNZ_HD void lim_grad_rt(int lim, double a, double b, double& da, double& db) {
   else lim_grad<0>(a, b, da, db);
 }
 
+BNZ_HD double lim_val_rt(int lim, double a, double b) {
+  const double ab = a * b;
+  if (lim == 0) return ab > 0. ? 2. * ab / (a + b) : 0.;
+  const double mm = ab <= 0. ? 0. : (a > 0. ? (a < b ? a : b) : (a > b ? a : b));
+  if (lim == 2) return mm;
+  const double p = 2. * mm, q = 0.5 * (a + b);
+  return p * q <= 0. ? 0. : (p > 0. ? (p < q ? p : q) : (p > q ? p : q));
+}
+
+// ---- characteristic projection of the PLM slopes (charact_proj) ----------
+// prim2char / char2prim of eos_c.h:100-333 as restated in bnz_device.cuh.
+// Both are linear in the differences they map, with coefficients built from
+// the cell state (rho, p and the three B components of the local frame).  The
+// VJP applies their transposes column by column and differentiates the
+// coefficients in forward mode: a Dual carries the derivative of every
+// coefficient along one direction of the cell state, through the same square
+// roots, divisions and case switches (taken on the values) as the forward.
+struct Dual {
+  double v, d;
+  BNZ_HD Dual(double x = 0., double y = 0.) : v(x), d(y) {}
+};
+BNZ_HD Dual operator+(Dual a, Dual b) { return Dual(a.v + b.v, a.d + b.d); }
+BNZ_HD Dual operator-(Dual a, Dual b) { return Dual(a.v - b.v, a.d - b.d); }
+BNZ_HD Dual operator-(Dual a) { return Dual(-a.v, -a.d); }
+BNZ_HD Dual operator*(Dual a, Dual b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
+BNZ_HD Dual operator/(Dual a, Dual b) {
+  const double q = a.v / b.v;
+  return Dual(q, (a.d - q * b.d) / b.v);
+}
+BNZ_HD double val(double x) { return x; }
+BNZ_HD double val(Dual x) { return x.v; }
+BNZ_HD double tsqrt(double x) { return sqrt(x); }
+BNZ_HD Dual tsqrt(Dual x) {
+  const double r = sqrt(x.v);
+  return Dual(r, r > 0. ? 0.5 * x.d / r : 0.);
+}
+BNZ_HD double tabs(double x) { return fabs(x); }
+BNZ_HD Dual tabs(Dual x) { return x.v >= 0. ? x : -x; }
+
+template <class T>
+struct CharK {
+  T rho, rhoi, a2rho, a, cf, cs, af, as, betay, betaz;
+  double s;
+};
+
+template <class T>
+BNZ_HD void char_basis(T rho, T p, T bx, T by, T bz, double gam, CharK<T>& k) {
+  k.rho = rho;
+  k.rhoi = T(1.) / rho;
+  k.s = sgn(val(bx));
+  k.a2rho = T(gam) * p;
+  k.a = tsqrt(k.a2rho * k.rhoi);
+  const T bx2 = bx * bx;
+  const T bperp2 = by * by + bz * bz;
+  const T x = k.a2rho + (bx2 + bperp2);
+  const T y = tsqrt(tabs(x * x - T(4.) * k.a2rho * bx2));
+  const T cf2 = T(0.5) * (x + y), cs2 = T(0.5) * (x - y);
+  k.cf = tsqrt(k.rhoi * cf2);
+  k.cs = tsqrt(k.rhoi * tabs(cs2));
+  if (val(k.cf) <= val(k.cs)) {
+    k.af = T(1.);
+    k.as = T(0.);
+  } else if (val(k.a) <= val(k.cs)) {
+    k.af = T(0.);
+    k.as = T(1.);
+  } else if (val(k.cf) <= val(k.a)) {
+    k.af = T(1.);
+    k.as = T(0.);
+  } else {
+    const T z = T(1.) / (cf2 - cs2);
+    k.af = tsqrt(z * tabs(k.a2rho - cs2));
+    k.as = tsqrt(z * tabs(cf2 - k.a2rho));
+  }
+  if (val(bperp2) != 0.) {
+    const T bperpi = T(1.) / tsqrt(bperp2);
+    k.betay = bperpi * by;
+    k.betaz = bperpi * bz;
+  } else {
+    k.betay = T(0.);
+    k.betaz = T(0.);
+  }
+}
+
+// out = prim2char(d); PSC and BX pass through
+template <class T>
+BNZ_HD void p2c_apply(const CharK<T>& k, const T* d, T* out) {
+  const T s = T(k.s);
+  const T nf = T(0.5) / (k.a2rho * k.rhoi);
+  const T qf_ = nf * k.cf * k.af * s, qs_ = nf * k.cs * k.as * s;
+  const T af_ = nf * k.af, as_ = nf * k.as;
+  const T rhoisr = tsqrt(k.rhoi);
+  const T arhoisr = k.a * rhoisr;
+  const T Af_ = af_ * arhoisr, As_ = as_ * arhoisr;
+  const T x = s * rhoisr;
+  const T v = k.betay * d[VY] + k.betaz * d[VZ];
+  const T b = k.betay * d[BY] + k.betaz * d[BZ];
+  const T tb = -(k.betaz * d[BY]) + k.betay * d[BZ];
+  out[RHO] = af_ * (k.rhoi * d[PR] - k.cf * d[VX]) + qs_ * v + As_ * b;
+  out[VX] = T(0.5) * ((-(k.betaz * d[VY]) + k.betay * d[VZ]) + x * tb);
+  out[VY] = as_ * (k.rhoi * d[PR] - k.cs * d[VX]) - qf_ * v - Af_ * b;
+  out[VZ] = d[RHO] - T(2.) * nf * d[PR];
+  out[PR] = as_ * (k.rhoi * d[PR] + k.cs * d[VX]) + qf_ * v - Af_ * b;
+  out[PSC] = d[PSC];
+  out[BX] = d[BX];
+  out[BY] = T(0.5) * ((k.betaz * d[VY] - k.betay * d[VZ]) + x * tb);
+  out[BZ] = af_ * (k.rhoi * d[PR] + k.cf * d[VX]) - qs_ * v + As_ * b;
+}
+
+// out = char2prim(c); PSC and BX pass through
+template <class T>
+BNZ_HD void c2p_apply(const CharK<T>& k, const T* c, T* out) {
+  const T s = T(k.s);
+  const T qf = k.cf * k.af * s, qs = k.cs * k.as * s;
+  const T rhosr = tsqrt(k.rho);
+  const T arhosr = k.a * rhosr;
+  const T Af = k.af * arhosr, As = k.as * arhosr;
+  const T fa = k.af * (c[RHO] + c[BZ]) + k.as * (c[VY] + c[PR]);
+  const T t = qs * (c[RHO] - c[BZ]) - qf * (c[VY] - c[PR]);
+  const T u = As * (c[RHO] + c[BZ]) - Af * (c[VY] + c[PR]);
+  const T srs = s * rhosr;
+  out[RHO] = k.rho * fa + c[VZ];
+  out[VX] = k.cf * k.af * (c[BZ] - c[RHO]) + k.cs * k.as * (c[PR] - c[VY]);
+  out[VY] = k.betay * t - k.betaz * (c[VX] - c[BY]);
+  out[VZ] = k.betaz * t + k.betay * (c[VX] - c[BY]);
+  out[PR] = k.a2rho * fa;
+  out[PSC] = c[PSC];
+  out[BX] = c[BX];
+  out[BY] = k.betay * u - k.betaz * srs * (c[VX] + c[BY]);
+  out[BZ] = k.betaz * u + k.betay * srs * (c[VX] + c[BY]);
+}
+
+// d = half_slopes_char(wm, wc, wp) (reconstr_c.c:54-91 with charact_proj):
+// the projected, limited and halved slope of the cell wc, local frame.
+BNZ_HD void slopes_char(int lim, const double* wm, const double* wc, const double* wp, double gam, double* d) {
+  CharK<double> k;
+  char_basis<double>(wc[RHO], wc[PR], wc[BX], wc[BY], wc[BZ], gam, k);
+  double dm0[NM], dp0[NM], dm[NM], dp[NM], c[NM];
+  for (int n = 0; n < NM; ++n) {
+    dm0[n] = wc[n] - wm[n];
+    dp0[n] = wp[n] - wc[n];
+  }
+  p2c_apply<double>(k, dm0, dm);
+  p2c_apply<double>(k, dp0, dp);
+  for (int n = 0; n < NM; ++n) c[n] = 0.5 * lim_val_rt(lim, dm[n], dp[n]);
+  c2p_apply<double>(k, c, d);
+}
+
+// VJP of slopes_char: given db (9), add the cotangents of wm, wc, wp.
+BNZ_HD void vjp_slopes_char(int lim, const double* wm, const double* wc, const double* wp, double gam,
+                            const double* db, double* wmb, double* wcb, double* wpb) {
+  CharK<double> k;
+  char_basis<double>(wc[RHO], wc[PR], wc[BX], wc[BY], wc[BZ], gam, k);
+  double dm0[NM], dp0[NM], dm[NM], dp[NM], c[NM];
+  for (int n = 0; n < NM; ++n) {
+    dm0[n] = wc[n] - wm[n];
+    dp0[n] = wp[n] - wc[n];
+  }
+  p2c_apply<double>(k, dm0, dm);
+  p2c_apply<double>(k, dp0, dp);
+  for (int n = 0; n < NM; ++n) c[n] = 0.5 * lim_val_rt(lim, dm[n], dp[n]);
+  // cb = Q^T db, then through the limiter, then dm0b = P^T dmb (columns of
+  // Q and P are their applications to unit vectors)
+  double e[NM], col[NM], cb[NM], dmb[NM], dpb[NM];
+  for (int q = 0; q < NM; ++q) {
+    for (int n = 0; n < NM; ++n) e[n] = n == q ? 1. : 0.;
+    c2p_apply<double>(k, e, col);
+    double acc = 0.;
+    for (int n = 0; n < NM; ++n) acc += db[n] * col[n];
+    cb[q] = acc;
+  }
+  for (int n = 0; n < NM; ++n) {
+    double la, lb;
+    lim_grad_rt(lim, dm[n], dp[n], la, lb);
+    dmb[n] = 0.5 * cb[n] * la;
+    dpb[n] = 0.5 * cb[n] * lb;
+  }
+  for (int q = 0; q < NM; ++q) {
+    for (int n = 0; n < NM; ++n) e[n] = n == q ? 1. : 0.;
+    p2c_apply<double>(k, e, col);
+    double am = 0., ap = 0.;
+    for (int n = 0; n < NM; ++n) {
+      am += dmb[n] * col[n];
+      ap += dpb[n] * col[n];
+    }
+    wmb[q] -= am;
+    wcb[q] += am - ap;
+    wpb[q] += ap;
+  }
+  // the coefficients' dependence on wc, one state direction at a time
+  const int ent[5] = {RHO, PR, BX, BY, BZ};
+  for (int q = 0; q < 5; ++q) {
+    Dual w5[5] = {Dual(wc[RHO]), Dual(wc[PR]), Dual(wc[BX]), Dual(wc[BY]), Dual(wc[BZ])};
+    w5[q].d = 1.;
+    CharK<Dual> kd;
+    char_basis<Dual>(w5[0], w5[1], w5[2], w5[3], w5[4], gam, kd);
+    Dual x[NM], y[NM];
+    double phi = 0.;
+    for (int n = 0; n < NM; ++n) x[n] = Dual(c[n]);
+    c2p_apply<Dual>(kd, x, y);
+    for (int n = 0; n < NM; ++n) phi += db[n] * y[n].d;
+    for (int n = 0; n < NM; ++n) x[n] = Dual(dm0[n]);
+    p2c_apply<Dual>(kd, x, y);
+    for (int n = 0; n < NM; ++n) phi += dmb[n] * y[n].d;
+    for (int n = 0; n < NM; ++n) x[n] = Dual(dp0[n]);
+    p2c_apply<Dual>(kd, x, y);
+    for (int n = 0; n < NM; ++n) phi += dpb[n] * y[n].d;
+    wcb[ent[q]] += phi;
+  }
+}
+
 // PLM face states of one variable at a face (reconstr_c.c:54-91):
 //   wL = wm1 + 0.5 lim(wm1 - wm2, w0 - wm1),  wR = w0 - 0.5 lim(w0 - wm1, wp1 - w0).
 // Given wLb, wRb, return the cotangents of (wm2, wm1, w0, wp1) in c[0..3].

@@ -127,4 +127,24 @@ void t_vjp_plm(int lim, const double* c4, double wLb, double wRb, double* cb) {
   adj::vjp_plm(lim, c4[0], c4[1], c4[2], c4[3], wLb, wRb, cb);
 }
 
+// characteristic-projected half slope of the cell wc (lim: 0 vl, 1 mc, 2 mm):
+// the device forward (which = 0) or the adjoint header's restatement (which = 1)
+void t_slopes_char(int which, int lim, const double* wm, const double* wc, const double* wp, double gam, double* d) {
+  if (which == 1) {
+    adj::slopes_char(lim, wm, wc, wp, gam, d);
+  } else if (lim == 1) {
+    dev::half_slopes_char<dev::LIM_MC>(wm, wc, wp, gam, d);
+  } else if (lim == 2) {
+    dev::half_slopes_char<dev::LIM_MM>(wm, wc, wp, gam, d);
+  } else {
+    dev::half_slopes_char<dev::LIM_VL>(wm, wc, wp, gam, d);
+  }
+}
+
+void t_vjp_slopes_char(int lim, const double* wm, const double* wc, const double* wp, double gam, const double* db,
+                       double* wmb, double* wcb, double* wpb) {
+  for (int n = 0; n < 9; ++n) wmb[n] = wcb[n] = wpb[n] = 0.;
+  adj::vjp_slopes_char(lim, wm, wc, wp, gam, db, wmb, wcb, wpb);
+}
+
 }  // extern "C"

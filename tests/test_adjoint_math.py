@@ -32,6 +32,8 @@ def lib():
     L.t_vjp_prim2cons.argtypes = [dp, dp, C.c_double, dp]
     L.t_plm.argtypes = [C.c_int, dp, dp]
     L.t_vjp_plm.argtypes = [C.c_int, dp, C.c_double, C.c_double, dp]
+    L.t_slopes_char.argtypes = [C.c_int, C.c_int, dp, dp, dp, C.c_double, dp]
+    L.t_vjp_slopes_char.argtypes = [C.c_int, dp, dp, dp, C.c_double, dp, dp, dp, dp]
     return L
 
 
@@ -183,3 +185,54 @@ def test_plm_vjp_matches_finite_differences(lib, lim):
         assert np.allclose(cb, g, rtol=1e-6, atol=1e-7), (lim, c4, cb, g)
         n += 1
     assert n > 250
+
+
+@pytest.mark.parametrize("lim", [0, 1, 2], ids=["vl", "mc", "mm"])
+def test_characteristic_slope_vjp_matches_finite_differences(lib, lim):
+    """The projected slope (prim2char, limiter, char2prim) of three cells: the
+    adjoint header's forward equals the device forward, and its VJP matches
+    central differences over all 27 inputs, the eigen-system coefficients'
+    dependence on the centre cell included."""
+    rng = np.random.default_rng(23 + lim)
+    ok = skipped = 0
+    for w in states(rng, 60):
+        wc = w[0].copy()
+        if wc[6] == 0.0:
+            continue  # sgn(bx) switches at bx = 0: a kink both FD steps straddle alike
+        wm = wc + 0.2 * rng.normal(size=9)
+        wp = wc + 0.2 * rng.normal(size=9)
+        for a in (wm, wp):
+            a[0] = abs(a[0]) + 0.1
+            a[4] = abs(a[4]) + 0.1
+        d0, d1 = np.zeros(9), np.zeros(9)
+        lib.t_slopes_char(0, lim, wm, wc, wp, GAM, d0)
+        lib.t_slopes_char(1, lim, wm, wc, wp, GAM, d1)
+        assert np.allclose(d0, d1, rtol=1e-12, atol=1e-13), (d0, d1)
+        db = rng.normal(size=9)
+        bm, bc, bp = np.zeros(9), np.zeros(9), np.zeros(9)
+        lib.t_vjp_slopes_char(lim, wm, wc, wp, GAM, db, bm, bc, bp)
+        v = np.concatenate([bm, bc, bp])
+
+        def fd(h):
+            g = np.zeros(27)
+            for t in range(27):
+                arrs = [wm.copy(), wc.copy(), wp.copy()]
+                base = arrs[t // 9][t % 9]
+                s_ = h * max(1.0, abs(base))
+                out = []
+                for sign in (1, -1):
+                    a = [x.copy() for x in arrs]
+                    a[t // 9][t % 9] = base + sign * s_
+                    d = np.zeros(9)
+                    lib.t_slopes_char(0, lim, a[0], a[1], a[2], GAM, d)
+                    out.append(db @ d)
+                g[t] = (out[0] - out[1]) / (2 * s_)
+            return g
+        g1, g2 = fd(1e-6), fd(1e-7)
+        scale = max(1.0, np.max(np.abs(g1)))
+        if np.max(np.abs(g1 - g2)) > 1e-5 * scale:
+            skipped += 1  # a limiter or eigen-system case switch within the stencil
+            continue
+        assert np.max(np.abs(v - g1)) <= 2e-6 * scale, (lim, v - g1)
+        ok += 1
+    assert ok >= 45, (ok, skipped)
