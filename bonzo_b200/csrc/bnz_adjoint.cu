@@ -64,7 +64,6 @@ int check_adjoint_ctx(bnz_ctx* c) {
   if (c->md.kappa0 > 0.) return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint covers the hyperbolic step only (kappa0 = 0)");
   if (c->md.rsolver != BNZ_RS_HLL && c->md.rsolver != BNZ_RS_HLLD && c->md.rsolver != BNZ_RS_HLLT)
     return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built for rsolver hll, hllt and hlld");
-  if (c->md.charact_proj) return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built without charact_proj");
   // constant gravity is differentiated; the driving force is a random field
   // advanced every step, which the tape does not keep
   if (drive_on(c->md)) return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built without turbulence driving");
@@ -157,6 +156,7 @@ int reverse_step(bnz_ctx* c, double dt, int p, int q, double* gw, double* gb, do
   a.dt = dt;
   a.rsolver = c->md.rsolver;
   a.limiter = c->md.limiter;
+  a.charact = c->md.charact_proj ? 1 : 0;
   a.fold_in = fold_in ? 1 : 0;
   a.clear_bsb = fold_in ? 1 : 0;  // the first reverse step of a pass
   a.stream = st;

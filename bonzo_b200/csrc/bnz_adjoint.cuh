@@ -33,6 +33,7 @@ struct Box {
 
 struct StageArgs {
   int order;
+  int charact;          // order 1 with charact_proj: projected slopes, the cells' normal B read too
   double dt;
   Box R;
   const double* Wout;   // the stage's output prim (9)
@@ -207,7 +208,7 @@ __device__ __forceinline__ void face_range(const Box& R, int& fi0, int& fj0, int
   n = (long long)w * (R.jb + 1 - fj0 + 1);
 }
 
-template <int AX, int ORDER, int RS>
+template <int AX, int ORDER, int RS, bool CHAR>
 __device__ __forceinline__ void face_vjp(const Inst& I, const StageArgs& a, int lim, long long t) {
   const Box R = a.R;
   int fi0, fj0, w;
@@ -257,6 +258,21 @@ __device__ __forceinline__ void face_vjp(const Inst& I, const StageArgs& a, int 
         wL[v] = cl_[gv];
         wR[v] = cr_[gv];
       }
+    } else if (CHAR) {
+      // projected slopes of the two cells (all nine local variables of the
+      // four-cell stencil), as the forward's half_slopes_char
+      double c4[4][NM], dL[NM], dR[NM];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int v = 0; v < NM; ++v) c4[q][v] = plm_cell<AX, ORDER>(I, a.Wsrc, i, j, q, plain::perm<AX>(v));
+      adj::slopes_char(lim, c4[0], c4[1], c4[2], I.gam, dL);
+      adj::slopes_char(lim, c4[1], c4[2], c4[3], I.gam, dR);
+#pragma unroll
+      for (int v = 0; v < NM; ++v) {
+        wL[v] = c4[1][v] + dL[v];
+        wR[v] = c4[2][v] - dR[v];
+      }
     } else {
 #pragma unroll
       for (int v = 0; v < NM; ++v) {
@@ -278,20 +294,52 @@ __device__ __forceinline__ void face_vjp(const Inst& I, const StageArgs& a, int 
     else adj::vjp_hll(wL, wR, I.gam, fb, wLb, wRb);
     // per-cell contributions, global variable order
     double* Qa = a.Q + (long long)AX * 4 * NM * I.sv;
+    if (ORDER == 1 && CHAR) {
+      // wL = c1 + d(c0, c1, c2), wR = c2 - d(c1, c2, c3); the face's normal
+      // field replaces both BX entries, the cells' own BX still shapes the
+      // eigen-system, so all nine entries of the four cells are written
+      double c4[4][NM], cb[4][NM], db[NM];
 #pragma unroll
-    for (int v = 0; v < NM; ++v) {
-      if (v == BX) continue;
-      const int gv = plain::perm<AX>(v);
-      if (ORDER == 0) {
-        Qa[(1 * NM + gv) * I.sv + f] = wLb[v];
-        Qa[(2 * NM + gv) * I.sv + f] = wRb[v];
-      } else {
-        double c4[4];
-        adj::vjp_plm(lim, plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 0, gv), plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 1, gv),
-                     plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 2, gv), plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 3, gv), wLb[v],
-                     wRb[v], c4);
+      for (int q = 0; q < 4; ++q)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) Qa[(q * NM + gv) * I.sv + f] = c4[q];
+        for (int v = 0; v < NM; ++v) {
+          c4[q][v] = plm_cell<AX, ORDER>(I, a.Wsrc, i, j, q, plain::perm<AX>(v));
+          cb[q][v] = 0.;
+        }
+#pragma unroll
+      for (int v = 0; v < NM; ++v) {
+        const double l = v == BX ? 0. : wLb[v];
+        cb[1][v] += l;
+        db[v] = l;
+      }
+      adj::vjp_slopes_char(lim, c4[0], c4[1], c4[2], I.gam, db, cb[0], cb[1], cb[2]);
+#pragma unroll
+      for (int v = 0; v < NM; ++v) {
+        const double r = v == BX ? 0. : wRb[v];
+        cb[2][v] += r;
+        db[v] = -r;
+      }
+      adj::vjp_slopes_char(lim, c4[1], c4[2], c4[3], I.gam, db, cb[1], cb[2], cb[3]);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int v = 0; v < NM; ++v) Qa[(q * NM + plain::perm<AX>(v)) * I.sv + f] = cb[q][v];
+    } else {
+#pragma unroll
+      for (int v = 0; v < NM; ++v) {
+        if (v == BX) continue;
+        const int gv = plain::perm<AX>(v);
+        if (ORDER == 0) {
+          Qa[(1 * NM + gv) * I.sv + f] = wLb[v];
+          Qa[(2 * NM + gv) * I.sv + f] = wRb[v];
+        } else {
+          double c4[4];
+          adj::vjp_plm(lim, plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 0, gv), plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 1, gv),
+                       plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 2, gv), plm_cell<AX, ORDER>(I, a.Wsrc, i, j, 3, gv), wLb[v],
+                       wRb[v], c4);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) Qa[(q * NM + gv) * I.sv + f] = c4[q];
+        }
       }
     }
     // the normal field of the face, and B^n's identity part of the update
@@ -306,7 +354,7 @@ __device__ __forceinline__ void face_vjp(const Inst& I, const StageArgs& a, int 
 
 // Both face directions in one launch (the x faces first), so the two halves
 // share the waves of one grid.
-template <int ORDER, int RS>
+template <int ORDER, int RS, bool CHAR>
 __global__ void __launch_bounds__(128, BNZ_ADJ_FACE_MINB) k_faces(const Inst I, const StageArgs a, int lim) {
   int fi0, fj0, w;
   long long nx, ny;
@@ -314,8 +362,8 @@ __global__ void __launch_bounds__(128, BNZ_ADJ_FACE_MINB) k_faces(const Inst I, 
   face_range<1>(a.R, fi0, fj0, w, ny);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nx + ny;
        t += (long long)gridDim.x * blockDim.x) {
-    if (t < nx) face_vjp<0, ORDER, RS>(I, a, lim, t);
-    else face_vjp<1, ORDER, RS>(I, a, lim, t - nx);
+    if (t < nx) face_vjp<0, ORDER, RS, CHAR>(I, a, lim, t);
+    else face_vjp<1, ORDER, RS, CHAR>(I, a, lim, t - nx);
   }
 }
 
@@ -347,7 +395,7 @@ __global__ void k_gather(const Inst I, const StageArgs a, const StageArgs next, 
         const long long fc = cidx(I, f, j);
 #pragma unroll
         for (int v = 0; v < NM; ++v)
-          if (v != BX) acc[v] += Qx[(s * NM + v) * I.sv + fc];
+          if (v != BX || a.charact) acc[v] += Qx[(s * NM + v) * I.sv + fc];
       }
     }
     // y faces (columns ia-1..ib+1, rows f in ja..jb+1)
@@ -360,7 +408,7 @@ __global__ void k_gather(const Inst I, const StageArgs a, const StageArgs next, 
         const long long fc = cidx(I, i, f);
 #pragma unroll
         for (int v = 0; v < NM; ++v)
-          if (v != BY) acc[v] += Qy[(s * NM + v) * I.sv + fc];
+          if (v != BY || a.charact) acc[v] += Qy[(s * NM + v) * I.sv + fc];
       }
     }
     // cell-centred E_z = -(vx by - vy bx) on cells ia-1..ib+1, ja-1..jb+1

@@ -167,6 +167,7 @@ struct AdjStep {
   double* Q;
   double dt;
   int rsolver, limiter;
+  int charact;        // the corrector's slopes are projected (charact_proj)
   int fold_in;        // fold G1 first (it may carry ghost entries)
   int clear_bsb;      // zero Bsb first (the first reverse step of a pass)
   cudaStream_t stream;

@@ -468,8 +468,9 @@ void adj_stage(const FusedInst& I, const adjk::StageArgs& a, int lim, cudaStream
   const long long ngat = (long long)(R.ib - R.ia + 1 + 2 * h) * (R.jb - R.ja + 1 + 2 * h);
   if (run_cells) adjk::k_cells<<<nblocks(ncell, T), T, 0, st>>>(I, a);
   adjk::k_corners<<<nblocks(ncorner, T), T, 0, st>>>(I, a);
-  if (a.order == 0) adjk::k_faces<0, RS><<<nblocks(nfx + nfy, T), T, 0, st>>>(I, a, lim);
-  else adjk::k_faces<1, RS><<<nblocks(nfx + nfy, T), T, 0, st>>>(I, a, lim);
+  if (a.order == 0) adjk::k_faces<0, RS, false><<<nblocks(nfx + nfy, T), T, 0, st>>>(I, a, lim);
+  else if (a.charact) adjk::k_faces<1, RS, true><<<nblocks(nfx + nfy, T), T, 0, st>>>(I, a, lim);
+  else adjk::k_faces<1, RS, false><<<nblocks(nfx + nfy, T), T, 0, st>>>(I, a, lim);
   adjk::k_gather<<<nblocks(ngat, T), T, 0, st>>>(I, a, next ? *next : a, next ? 1 : 0);
 }
 
@@ -494,6 +495,7 @@ int adj_step(const FusedInst& I, const AdjStep& s) {
   adjk::StageArgs a;
   // corrector: order 1 on the active cells
   a.order = 1;
+  a.charact = s.charact;
   a.dt = s.dt;
   a.R = {I.ng, I.ng + I.N[0] - 1, I.ng, I.ng + I.N[1] - 1};
   a.Wout = s.W1;
@@ -512,6 +514,7 @@ int adj_step(const FusedInst& I, const AdjStep& s) {
   // predictor: order 0 on cells 1..Ntot-2, half step
   adjk::StageArgs a0 = a;
   a0.order = 0;
+  a0.charact = 0;
   a0.dt = 0.5 * s.dt;
   a0.R = {1, I.nx - 2, 1, I.ny - 2};
   a0.Wout = s.Ws;

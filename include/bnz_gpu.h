@@ -230,9 +230,9 @@ int bnz_snapshot(bnz_ctx* ctx, double* prim, double* cons, double* bfld);
 int bnz_snapshot_wait(bnz_ctx* ctx);
 
 /* ------------------------------------------------------------------------
- * Discrete adjoint of the VL2 step (fused 2D path, PLM, rsolver hll, hllt or
- * hlld, constant gravity; no conduction, turbulence driving or charact_proj;
- * fixed dt).  No counterpart in the reference, which has no
+ * Discrete adjoint of the VL2 step (fused 2D path, PLM with or without
+ * charact_proj, rsolver hll, hllt or hlld, constant gravity; no conduction or
+ * turbulence driving; fixed dt).  No counterpart in the reference, which has no
  * adjoint; these serve the torch.autograd wrapper (bonzo_b200/adjoint.py).
  * All state and cotangent pointers are DEVICE pointers to full arrays with
  * ghosts, (9, Ntot) prim and (3, Ntot) face field, ordered on the context's

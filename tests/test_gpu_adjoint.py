@@ -63,6 +63,11 @@ def _rel(a, b):
     ("vortex", 24, 1e-3, dict(limiter="mc", rsolver="hllt")),
     ("blast", 24, 1e-3, dict(rsolver="hllt")),
     ("mixed_bc", 20, 1e-3, dict(limiter="mm", rsolver="hllt", grav=(0.2, -0.4, 0.0))),
+    # slopes projected on the characteristic basis (charact_proj)
+    ("vortex", 24, 0.0, dict(limiter="mc", charact_proj=1, exact_fp=1)),
+    ("vortex", 24, 1e-3, dict(limiter="mc", charact_proj=1)),
+    ("blast", 24, 1e-3, dict(charact_proj=1)),
+    ("blast_reflect", 20, 1e-3, dict(rsolver="hll", limiter="mm", charact_proj=1)),
 ])
 def test_step_adjoint_matches_torch_autograd(case, n, noise, kw):
     import torch
@@ -71,7 +76,8 @@ def test_step_adjoint_matches_torch_autograd(case, n, noise, kw):
     G = T.Grid(gc, face_aware=True, device="cuda")
     p = P0.cuda().requires_grad_(True)
     b = B0.cuda().requires_grad_(True)
-    tp, tb = T.step(G, p, b, dt, rs=m["rsolver"], lim=m["limiter"], grav=m.get("grav"))
+    tp, tb = T.step(G, p, b, dt, rs=m["rsolver"], lim=m["limiter"], grav=m.get("grav"),
+                    charact=bool(m.get("charact_proj")))
     gen = torch.Generator(device="cpu").manual_seed(5)
     gp = torch.randn(tp.shape, generator=gen, dtype=torch.float64).cuda()
     gb = torch.randn(tb.shape, generator=gen, dtype=torch.float64).cuda()
@@ -105,6 +111,7 @@ def test_step_adjoint_matches_torch_autograd(case, n, noise, kw):
     (6, 4, dict(grav=(0.2, -0.6, 0.0))),
     # HLLT on the exact build (the vortex's exact wave-speed ties, see above)
     (5, 2, dict(grav=(0.0, -0.5, 0.0), rsolver="hllt", exact_fp=1)),
+    (4, 2, dict(charact_proj=1, exact_fp=1)),
 ])
 def test_rollout_adjoint_matches_torch_autograd(nsteps, every, extra):
     import torch
@@ -123,7 +130,7 @@ def test_rollout_adjoint_matches_torch_autograd(nsteps, every, extra):
     b = B0.cuda().requires_grad_(True)
     x, y = p, b
     for _ in range(nsteps):
-        x, y = T.step(G, x, y, dt, rs=rs, lim="mc", grav=grav)
+        x, y = T.step(G, x, y, dt, rs=rs, lim="mc", grav=grav, charact=bool(kw.get("charact_proj")))
     loss_t = ((x[0] - target) ** 2).sum()
     ap, ab = torch.autograd.grad(loss_t, (p, b))
     # the adjoint through the autograd wrapper
