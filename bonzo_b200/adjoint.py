@@ -12,6 +12,11 @@ context's full shape (ghosts included).  The forward reads only the source
 entries of the input (active cells and the faces the CT update owns); the
 gradient is zero on the ghost entries.  dt is held fixed: the gradient does not
 differentiate a CFL time step.  Work is ordered on torch's current stream.
+
+The context must use the fused 2D path with rsolver hll, hllt or hlld; any
+limiter (with or without charact_proj), any boundary conditions and constant
+gravity are differentiated.  Conduction (kappa0 > 0) and turbulence driving
+are refused with BnzError (unsupported).
 """
 import torch
 
