@@ -161,14 +161,18 @@ def cpu_sample(batch, min_zones=1_200_000):
     return sample, z
 
 
-def run_cpu_reference(batch, steps, warmup):
+def run_cpu_reference(batch, steps, warmup, rows_parallel=1):
+    """One VL2 step of a bounded sample of the batch on the host cores.
+    rows_parallel=1: OpenMP over the rows of every sweep (the stronger, labelled
+    variant); rows_parallel=0: the reference's own structure, prange over k for
+    the x / y sweeps (godunov.pyx:20-209), one active thread in 2D."""
     from oracle import oracle as O
     use_ref = O.ref_lib() is not None
     sample, zones = cpu_sample(batch)
     sims = []
     for q, gc, prim, bfld in sample:
         s = O.OracleSim(Nx=q["N"], Ny=q["N"], Nz=1, use_ref_kernels=use_ref, nthreads=0,
-                        rows_parallel=1, **METHOD)
+                        rows_parallel=rows_parallel, **METHOD)
         s.set_state(prim, bfld)
         s.init()
         sims.append(s)
@@ -182,13 +186,14 @@ def run_cpu_reference(batch, steps, warmup):
             times.append(dt)
     per_step = statistics.median(times)
     value = zones / per_step / 1e6
-    desc = ("one VL2 step on the first %d instances of the batch (%d zones, N=%s); %s; "
-            "OpenMP rows-parallel over all host threads" %
+    desc = ("one VL2 step on the first %d instances of the batch (%d zones, N=%s); %s; %s" %
             (len(sample), zones, ",".join(str(x[0]["N"]) for x in sample),
              "reference C kernels (src/mhd/fluxes_c.c, src/coordinates/reconstr_c.c, "
              "src/mhd/eos_c.c) driven by the oracle's C restatement of the Cython sweeps"
-             if use_ref else "oracle C restatement"))
-    return dict(value=round(value, 3), unit=UNIT, cores=os.cpu_count(),
+             if use_ref else "oracle C restatement",
+             "OpenMP rows-parallel over all host threads" if rows_parallel else
+             "the reference's OpenMP structure (prange over k: one active thread in 2D)"))
+    return dict(value=round(value, 3), unit=UNIT, cores=os.cpu_count() if rows_parallel else 1,
                 kind="reference" if use_ref else "port", sample=desc,
                 per_step_s=round(per_step, 4))
 
@@ -197,15 +202,21 @@ def run_cpu_reference(batch, steps, warmup):
 # our arm
 # ---------------------------------------------------------------------------
 
-def _timed(stream, step_fn, steps, dist):
+def _timed(stream, step_fn, steps, dist, multi=None):
+    """ms of `steps` steps (max over ranks), CUDA events on the launching
+    stream.  multi(k), when given, runs k steps in one call (a batch replays
+    its captured two-step CUDA graph)."""
     import torch
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     ev0.record(stream)
-    for _ in range(steps):
-        step_fn()
+    if multi is not None:
+        multi(steps)
+    else:
+        for _ in range(steps):
+            step_fn()
     ev1.record(stream)
     torch.cuda.synchronize()
     if dist:
@@ -226,6 +237,7 @@ def make_engine(kind, batch, stream):
         eng.set_stream(stream.cuda_stream)
         ctxs = eng.instances
         step = lambda: eng.advance(1e30, 1)
+        multi = lambda k: eng.advance(1e30, k)
         count = eng.launch_count
     else:
         ctxs = []
@@ -239,11 +251,12 @@ def make_engine(kind, batch, stream):
             for c in ctxs:
                 c.advance_graph(1e30, 1)
 
+        multi = None
         count = lambda: sum(c.launch_count() for c in ctxs)
     for c, (q, gc, prim, bfld) in zip(ctxs, batch):
         c.set_state(prim, bfld)
         c.init()
-    return eng, ctxs, step, count
+    return eng, ctxs, step, multi, count
 
 
 def run_ours(args, rank, world, dist):
@@ -259,18 +272,18 @@ def run_ours(args, rank, world, dist):
     # the plain one-instance-per-launch path (the comparison the headline quotes)
     plain_ms = None
     if args.path == "batch" and not args.no_plain:
-        eng, ctxs, step, count = make_engine("plain", batch, stream)
+        eng, ctxs, step, multi, count = make_engine("plain", batch, stream)
         for _ in range(args.warmup):
             step()
         plain_steps = max(3, args.steps // 4)
         plain_ms = _timed(stream, step, plain_steps, dist) / plain_steps
         for c in ctxs:
             c.check()
-        del eng, ctxs, step, count
+        del eng, ctxs, step, multi, count
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
 
-    eng, ctxs, step, count = make_engine(args.path, batch, stream)
+    eng, ctxs, step, multi, count = make_engine(args.path, batch, stream)
     tune = None
     if args.path == "batch":
         from bonzo_b200._lib import variant_label, variants
@@ -290,10 +303,12 @@ def run_ours(args, rank, world, dist):
                                 for v, t in ms.items()}}
     for _ in range(args.warmup):
         step()
+    if multi is not None:
+        multi(2)  # untimed: captures the two-step graph at the current state parity
     torch.cuda.synchronize()
     launches0 = count()
     with ClockSampler(dev) as clk:
-        ms_max = _timed(stream, step, args.steps, dist)
+        ms_max = _timed(stream, step, args.steps, dist, multi)
     launches = count() - launches0
     ms_step = ms_max / args.steps
     value = zones_all * args.steps / (ms_max * 1e-3) / 1e6
@@ -362,14 +377,21 @@ def run_ours(args, rank, world, dist):
         kms = eng.advance_timed(1e30, args.steps)
         for c in ctxs:
             c.check()
-        achieved = CORR_BYTES_PER_ZONE * zones / (kms["corrector"] * 1e-3) / 1e9
+        # achieved in the zone-update unit: 192 B per active zone per launch
+        achieved = BYTES_PER_ZONE * zones / (kms["corrector"] * 1e-3) / 1e9
+        own = CORR_BYTES_PER_ZONE * zones / (kms["corrector"] * 1e-3) / 1e9
         traffic = None if CORR_TRAFFIC_PER_ZONE is None else int(CORR_TRAFFIC_PER_ZONE * zones)
         roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_src,
                     "kernel": ("k_corr2d_pq (persistent corrector, one launch covers every instance)"
                                if tune and vs[best][3] else
                                "k_corr2d (corrector, one launch covers every instance)"),
-                    "algorithmic_bytes_per_launch": CORR_BYTES_PER_ZONE * zones,
+                    "bytes_per_zone": BYTES_PER_ZONE,
+                    "algorithmic_bytes_per_launch": BYTES_PER_ZONE * zones,
+                    "corrector_own_bytes": {"bytes_per_zone": CORR_BYTES_PER_ZONE,
+                                            "achieved": round(own, 1), "frac": round(own / peak, 4),
+                                            "what": "w^n, b^n, w^(n+1/2), b^(n+1/2) read, w^(n+1), "
+                                                    "b^(n+1) written: the launch's own inputs and outputs"},
                     "ms_per_launch": round(kms["corrector"], 4),
                     "kernel_ms_per_launch": {k: round(v, 4) for k, v in kms.items()},
                     "step": step_roof}
@@ -523,6 +545,9 @@ def main():
                 "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
+        cs = run_cpu_reference(batch, steps=1, warmup=1, rows_parallel=0)
+        line["cpu_baseline_reference_structure"] = {k: cs[k] for k in ("value", "unit", "cores", "kind",
+                                                                          "sample")}
         print(json.dumps(line), flush=True)
         return 0
     if args.adjoint_only:
@@ -548,6 +573,9 @@ def main():
         batch = build_batch(args.instances, args.seed)
         cb = run_cpu_reference(batch, steps=2, warmup=1)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cs = run_cpu_reference(batch, steps=1, warmup=1, rows_parallel=0)
+        line["cpu_baseline_reference_structure"] = {k: cs[k] for k in ("value", "unit", "cores", "kind",
+                                                                          "sample")}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

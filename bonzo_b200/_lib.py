@@ -31,8 +31,8 @@ EXPORTS = [
     "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_advance_timed", "bnz_batch_step_host", "bnz_batch_test_withhold_loads", "bnz_fp64_fma_peak", "bnz_batch_set_stream", "bnz_batch_launch_count",
     "bnz_batch_sync", "bnz_variant_count", "bnz_batch_set_variant", "bnz_batch_get_variant",
     "bnz_batch_time_variant", "bnz_batch_autotune", "bnz_vl2_step_noalloc", "bnz_noalloc_last_error",
-    "bnz_noalloc_scratch_bytes", "bnz_set_state_device", "bnz_get_state_device", "bnz_rollout_forward",
-    "bnz_rollout_adjoint", "bnz_step_adjoint", "bnz_history", "bnz_snapshot", "bnz_snapshot_wait",
+    "bnz_noalloc_check", "bnz_noalloc_scratch_bytes", "bnz_set_state_device", "bnz_get_state_device", "bnz_rollout_forward",
+    "bnz_rollout_adjoint", "bnz_step_adjoint", "bnz_history", "bnz_div_b", "bnz_riemann", "bnz_snapshot", "bnz_snapshot_wait",
 ]
 
 
@@ -55,7 +55,7 @@ class MethodDesc(C.Structure):
                 ("cour_diff", C.c_double), ("fixdt", C.c_int), ("dt_fixed", C.c_double),
                 ("outflow_face_aware", C.c_int), ("exact_fp", C.c_int), ("path", C.c_int),
                 ("grav", C.c_double * 3), ("drive_f0", C.c_double), ("drive_tau", C.c_double),
-                ("drive_nmod", C.c_int), ("drive_seed", C.c_uint64)]
+                ("drive_nmod", C.c_int), ("drive_seed", C.c_uint64), ("hydro", C.c_int)]
 
 
 _dp = C.POINTER(C.c_double)
@@ -112,6 +112,8 @@ def load():
     L.bnz_rollout_adjoint.argtypes = [vp, vp, vp, vp, vp]
     L.bnz_step_adjoint.argtypes = [vp, C.c_double, vp, vp, vp, vp, vp, vp]
     L.bnz_history.argtypes = [vp, _dp]
+    L.bnz_div_b.argtypes = [vp, _dp]
+    L.bnz_riemann.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, C.c_int, C.c_double, C.c_int, vp, vp]
     L.bnz_snapshot.argtypes = [vp, _dp, _dp, _dp]
     L.bnz_snapshot_wait.argtypes = [vp]
     L.bnz_batch_set_stream.argtypes = [vp, vp]
@@ -147,7 +149,7 @@ def grid_desc(Nx, Ny=1, Nz=1, dims=2, lmin=(0., 0., 0.), lmax=(1., 1., 1.),
 def method_desc(gam=5. / 3, cour=0.4, rsolver="hlld", reconstr="linear", limiter="vl",
                 charact_proj=0, kappa0=0.0, thcond_type="aniso", sat_hfe=0, cour_diff=0.5,
                 fixdt=False, dt_fixed=0.0, outflow_face_aware=1, exact_fp=False, path="plain",
-                grav=(0.0, 0.0, 0.0), drive_f0=0.0, drive_tau=1.0, drive_nmod=1, drive_seed=0):
+                grav=(0.0, 0.0, 0.0), drive_f0=0.0, drive_tau=1.0, drive_nmod=1, drive_seed=0, hydro=False):
     m = MethodDesc()
     m.gam, m.cour = gam, cour
     m.rsolver = RS[rsolver] if isinstance(rsolver, str) else rsolver
@@ -161,6 +163,7 @@ def method_desc(gam=5. / 3, cour=0.4, rsolver="hlld", reconstr="linear", limiter
     for a in range(3):
         m.grav[a] = grav[a]
     m.drive_f0, m.drive_tau, m.drive_nmod, m.drive_seed = drive_f0, drive_tau, drive_nmod, drive_seed
+    m.hydro = int(bool(hydro))
     return m
 
 
@@ -295,6 +298,12 @@ class Context:
         out = np.zeros(16)
         self._ck(self.L.bnz_history(self.h, _p(out)))
         return out
+
+    def div_b(self):
+        """max |div B| * dx / max |B| over the active cells, reduced on the device."""
+        out = np.zeros(2)
+        self._ck(self.L.bnz_div_b(self.h, _p(out)))
+        return out[0] / out[1] if out[1] > 0 else out[0]
 
     def snapshot(self, prim=None, cons=None, bfld=None):
         """Queue a device->host copy of the state into the given float64 arrays
@@ -453,6 +462,26 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def riemann(rsolver, wl, wr, bx, gam, exact_fp=False):
+    """Device Riemann fluxes of face states given as torch CUDA float64 tensors
+    of shape (nvar, n) (bnz_riemann: the reference's C-level flux call, nvar 9
+    for MHD, 6 for the hydro build).  Returns the flux tensor."""
+    import torch
+    L = load()
+    nvar, n = wl.shape
+    wl, wr = wl.contiguous(), wr.contiguous()
+    bx = bx.contiguous() if bx is not None else None
+    flux = torch.empty_like(wl)
+    err = torch.zeros(1, dtype=torch.int32, device=wl.device)
+    rs = RS[rsolver] if isinstance(rsolver, str) else rsolver
+    rc = L.bnz_riemann(rs, nvar, wl.data_ptr(), wr.data_ptr(), bx.data_ptr() if bx is not None else None,
+                       flux.data_ptr(), n, float(gam), int(bool(exact_fp)), err.data_ptr(),
+                       torch.cuda.current_stream().cuda_stream)
+    if rc != BNZ_OK:
+        raise BnzError(rc, "bnz_riemann failed")
+    return flux
 
 
 def fp64_fma_peak():

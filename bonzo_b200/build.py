@@ -44,14 +44,15 @@ def _newer(dst, srcs):
 
 def build(verbose=True, force=False, extra=()):
     os.makedirs(OUT, exist_ok=True)
-    # sources, the C ABI header, and this recipe (a flag change rebuilds)
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "bnz_gpu.h"),
-                                                                 os.path.abspath(__file__)]
+    # a unit depends on its own source, every header (.h / .cuh), the C ABI
+    # header and this recipe (a flag change rebuilds)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    common = headers + [os.path.join(HERE, "..", "include", "bnz_gpu.h"), os.path.abspath(__file__)]
     objs, jobs = [], []
     for src, flags in UNITS:
         obj = os.path.join(OUT, src.replace(".cu", ".o"))
         objs.append(obj)
-        if not force and _newer(obj, deps):
+        if not force and _newer(obj, common + [os.path.join(CSRC, src)]):
             continue
         jobs.append((src, [NVCC] + ARCH + COMMON + list(flags) + list(extra) +
                      ["-c", os.path.join(CSRC, src), "-o", obj]))

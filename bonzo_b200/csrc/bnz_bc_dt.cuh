@@ -84,7 +84,8 @@ __global__ void k_bc_axis(GridDev g, int ax, double* prim, double* bfld, FieldLi
 // new_dt.pyx:55-99 + 117: per-cell (|v_d| + c_f)/dx_d, max over active cells.
 // Non-negative doubles order like their bit patterns, so the global max is an
 // integer atomicMax on the bits.
-__global__ void k_cds_max(GridDev g, const double* __restrict__ w, unsigned long long* slot) {
+// hydro: the hydro build's sound speed (no magnetic field).
+__global__ void k_cds_max(GridDev g, const double* __restrict__ w, unsigned long long* slot, int hydro) {
   double m = 0.;
   const int nxa = g.i2 - g.i1 + 1, nya = g.j2 - g.j1 + 1, nza = g.k2 - g.k1 + 1;
   const long long n = (long long)nxa * nya * nza;
@@ -96,7 +97,7 @@ __global__ void k_cds_max(GridDev g, const double* __restrict__ w, unsigned long
     double ww[NM];
 #pragma unroll
     for (int q = 0; q < NM; ++q) ww[q] = w[q * g.sv + c];
-    double vf = fms(ww, g.gam);
+    double vf = hydro ? fms_hydro(ww, g.gam) : fms(ww, g.gam);
     double cx = fabs(ww[VX]) + vf, cy = 0., cz = 0.;
     if (g.dims >= 2) cy = fabs(ww[VY]) + vf;
     if (g.dims >= 3) cz = fabs(ww[VZ]) + vf;

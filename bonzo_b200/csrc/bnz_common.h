@@ -43,6 +43,7 @@ struct StepArgs {
   double grav[3];
   const double* fdriv;
   int src;  // any source term on
+  int hydro;  // the reference's hydro build (MFIELD 0): no field, no CT
 };
 
 // Device time-step record used by graph-captured stepping.

@@ -111,6 +111,9 @@ StepArgs step_args(bnz_ctx* c) {
   for (int d = 0; d < 3; ++d) a.grav[d] = c->md.grav[d];
   a.fdriv = c->fdriv;
   a.src = src_on(c->md) ? 1 : 0;
+  a.hydro = c->md.hydro ? 1 : 0;
+  // the hydro build's HLL takes the hydro sound speed
+  if (a.hydro && a.rsolver == BNZ_RS_HLL) a.rsolver = 4;  // dev::RS_HLL_HYDRO
   return a;
 }
 
@@ -347,8 +350,17 @@ int validate(const bnz_grid_desc* g, const bnz_method_desc* m, std::string& why)
   }
   if (!(m->gam > 1.)) return why = "gam must exceed 1", 0;
   if (!(m->cour > 0.)) return why = "cour must be positive", 0;
-  if (m->rsolver != BNZ_RS_HLL && m->rsolver != BNZ_RS_HLLD && m->rsolver != BNZ_RS_HLLT)
-    return why = "rsolver must be hll, hlld or hllt for MHD (hllc is hydro-only in the reference)", 0;
+  if (m->hydro != 0 && m->hydro != 1) return why = "hydro must be 0 or 1", 0;
+  if (m->hydro) {
+    // the reference's hydro build (MFIELD 0, src/defs_c.h:72-96): hll or hllc
+    if (m->rsolver != BNZ_RS_HLL && m->rsolver != BNZ_RS_HLLC)
+      return why = "rsolver must be hll or hllc in hydro mode (hlld needs a magnetic field)", 0;
+    if (m->path != BNZ_PATH_PLAIN) return why = "hydro mode runs on the plain path", 0;
+    if (m->charact_proj) return why = "charact_proj is not available in hydro mode", 0;
+    if (m->kappa0 != 0.) return why = "field-aligned conduction needs a magnetic field (kappa0 = 0 in hydro mode)", 0;
+  } else if (m->rsolver != BNZ_RS_HLL && m->rsolver != BNZ_RS_HLLD && m->rsolver != BNZ_RS_HLLT) {
+    return why = "rsolver must be hll, hlld or hllt for MHD (hllc is hydro-only in the reference; set hydro = 1)", 0;
+  }
   if (m->reconstr != BNZ_RCN_CONST && m->reconstr != BNZ_RCN_LINEAR) return why = "reconstr must be const or linear", 0;
   if (m->limiter < 0 || m->limiter > 2) return why = "limiter must be vl, mc or mm", 0;
   if (m->charact_proj != 0 && m->charact_proj != 1) return why = "charact_proj must be 0 or 1", 0;
@@ -581,6 +593,11 @@ int bnz_set_state(bnz_ctx* c, const double* pc, int is_prim, const double* bfld)
   size_t n9 = 9 * c->ncell * sizeof(double), n3 = 3 * c->ncell * sizeof(double);
   CKC(cudaMemcpyAsync(is_prim ? c->prim : c->cons, pc, n9, cudaMemcpyHostToDevice, c->stream));
   if (bfld) CKC(cudaMemcpyAsync(c->bfld, bfld, n3, cudaMemcpyHostToDevice, c->stream));
+  if (c->md.hydro) {
+    // no magnetic field in the hydro build: the field entries are zero
+    CKC(cudaMemsetAsync((is_prim ? c->prim : c->cons) + 6 * c->ncell, 0, 3 * c->ncell * sizeof(double), c->stream));
+    CKC(cudaMemsetAsync(c->bfld, 0, n3, c->stream));
+  }
   // derive the other array on every cell, as init_sim does after set_problem
   StepArgs a = step_args(c);
   if (is_prim) c->launches += c->L->prim2cons_all(a);
@@ -950,6 +967,22 @@ int bnz_advance_graph(bnz_ctx* c, double tmax, int nsteps) {
   CKC(cudaGetLastError());
   c->time_on_device = true;
   return BNZ_OK;
+}
+
+int bnz_riemann(int rsolver, int nvar, const double* wl, const double* wr, const double* bx, double* flux, int n,
+                double gam, int exact_fp, unsigned* err_bits, void* stream) {
+  if (nvar != 6 && nvar != 9) return BNZ_ERR_ARG;
+  if (!wl || !wr || !flux || (nvar == 9 && !bx) || n < 0 || !(gam > 1.)) return BNZ_ERR_ARG;
+  if (rsolver < BNZ_RS_HLL || rsolver > BNZ_RS_HLLT) return BNZ_ERR_ARG;
+  // hllc exists in the hydro build only, hlld in the MHD builds only
+  if ((rsolver == BNZ_RS_HLLC && nvar != 6) || (rsolver == BNZ_RS_HLLD && nvar != 9)) return BNZ_ERR_UNSUPPORTED;
+  // the hydro build's hllt is not built (its field-free star states differ)
+  if (rsolver == BNZ_RS_HLLT && nvar != 9) return BNZ_ERR_UNSUPPORTED;
+  if (n == 0) return BNZ_OK;
+  const Launchers* L = exact_fp ? &exact::table : &fast::table;
+  const int rs = (rsolver == BNZ_RS_HLL && nvar == 6) ? 4 : rsolver;  // 4: dev::RS_HLL_HYDRO
+  L->riemann_rows(rs, wl, wr, bx, flux, n, nvar, gam, err_bits, (cudaStream_t)stream);
+  return cudaGetLastError() == cudaSuccess ? BNZ_OK : BNZ_ERR_CUDA;
 }
 
 int bnz_device_state(bnz_ctx* c, double** prim, double** cons, double** bfld) {

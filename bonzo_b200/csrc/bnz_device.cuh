@@ -21,6 +21,9 @@ constexpr int NM = 9;
 enum { RHO = 0, MX = 1, MY = 2, MZ = 3, EN = 4, PSC = 5, BX = 6, BY = 7, BZ = 8 };
 enum { VX = 1, VY = 2, VZ = 3, PR = 4 };
 enum { RS_HLL = 0, RS_HLLC = 1, RS_HLLD = 2, RS_HLLT = 3 };
+// HLL of the hydro build (MFIELD 0): the hydro sound speed in its wave
+// estimate.  Internal code, not an ABI value.
+enum { RS_HLL_HYDRO = 4 };
 enum { LIM_VL = 0, LIM_MC = 1, LIM_MM = 2 };
 // bits of the device error word
 enum { ERR_RHO = 1, ERR_PRES = 2, ERR_NAN = 4, ERR_FAN = 8, ERR_TIMEOUT = 16 };
@@ -142,6 +145,105 @@ __device__ __forceinline__ void flux_hll(double* flux, const double* wL, const d
 #pragma unroll
   for (int n = 0; n < NM; ++n) flux[n] = (aR * fL[n] - aL * fR[n] + aLaR * (uR[n] - uL[n])) * aRmaLi;
   flux[BX] = 0.;
+}
+
+// ---------------------------------------------------------------------------
+// Hydro build (MFIELD 0).  The magnetic entries of every state are zero, so
+// prim2cons, cons2prim and primcons2flux above give the hydro build's values
+// (their field terms add exact zeros); only the signal speeds differ.
+// ---------------------------------------------------------------------------
+
+// eos_c.h:468-530, hydro branch: the adiabatic sound speed.
+__device__ __forceinline__ double fms_hydro(const double* w, double gam) {
+  const double gamp = gam * w[PR];
+  return sqrt(gamp / w[RHO]);
+}
+
+// fluxes_c.c:25-42 with the hydro sound speed
+__device__ __forceinline__ void wave_speeds_hydro(const double* wL, const double* wR, double gam, double& sL,
+                                                  double& sR) {
+  const double cfL = fms_hydro(wL, gam), cfR = fms_hydro(wR, gam);
+  const double cf_max = fmax(cfL, cfR);
+  sL = fmin(wL[VX], wR[VX]) - cf_max;
+  sR = fmax(wL[VX], wR[VX]) + cf_max;
+}
+
+// fluxes_c.c:138-168: PVRS pressure-based wave speeds (Toro), used by HLLC.
+__device__ __forceinline__ void wave_speeds_pvrs(const double* wL, const double* wR, double gam, double& sL,
+                                                 double& sR) {
+  const double g1gh = 0.5 * (gam + 1.) / gam;
+  const double aL = fms_hydro(wL, gam), aR = fms_hydro(wR, gam);
+  const double ptL = wL[PR], ptR = wR[PR];
+  const double pvrs =
+      fmax(0., 0.5 * (ptL + ptR) - 0.125 * (wR[VX] - wL[VX]) * (wL[RHO] + wR[RHO]) * (aL + aR));
+  const double qL = pvrs < ptL ? 1. : sqrt(1. + g1gh * (pvrs / ptL - 1.));
+  const double qR = pvrs < ptR ? 1. : sqrt(1. + g1gh * (pvrs / ptR - 1.));
+  sL = wL[VX] - aL * qL;
+  sR = wR[VX] + aR * qR;
+}
+
+// fluxes_c.c:175-223 in the hydro build: six conserved entries, hydro speeds.
+__device__ __forceinline__ void flux_hll_hydro(double* flux, const double* wL, const double* wR, double gam) {
+  double uL[NM], uR[NM], fL[NM], fR[NM];
+  prim2cons(uL, wL, gam);
+  prim2cons(uR, wR, gam);
+  primcons2flux(fL, wL, uL);
+  primcons2flux(fR, wR, uR);
+  double sL, sR;
+  wave_speeds_hydro(wL, wR, gam, sL, sR);
+  const double aL = fmin(sL, 0.), aR = fmax(sR, 0.);
+  const double aLaR = aL * aR;
+  const double aRmaLi = 1. / (aR - aL);
+#pragma unroll
+  for (int n = 0; n < BX; ++n) flux[n] = (aR * fL[n] - aL * fR[n] + aLaR * (uR[n] - uL[n])) * aRmaLi;
+  flux[BX] = flux[BY] = flux[BZ] = 0.;
+}
+
+// fluxes_c.c:232-327 (Toro's HLLC; hydro builds only).  The contact speed sM
+// and star pressure come from both sides; the flux is z * F_side + sLR * p*
+// terms of the side the contact leaves the interface on, with the side's own
+// wave speed clipped at 0 -- the reference forms z_L F_L + z_R F_R with the
+// other side's weight exactly 0, so one side per lane gives the same values.
+__device__ __forceinline__ void flux_hllc(double* flux, const double* wL, const double* wR, double gam) {
+  double sL, sR;
+  wave_speeds_pvrs(wL, wR, gam, sL, sR);
+  const double gamm1i = 1. / (gam - 1.);
+  // the conserved rho and mx of both states (prim2cons, eos_c.h:60-95)
+  const double mxL = wL[RHO] * wL[VX], mxR = wR[RHO] * wR[VX];
+  double vLsL = wL[VX] - sL, vRsR = wR[VX] - sR;
+  const double xL = wL[RHO] * vLsL, xR = wR[RHO] * vRsR;
+  const double xRxLi = 1. / (xR - xL);
+  const double yL = wL[PR] + mxL * vLsL, yR = wR[PR] + mxR * vRsR;
+  const double sM = xRxLi * (yR - yL);
+  const double pts = xRxLi * (xR * yL - xL * yR);
+  sL = fmin(sL, 0.);
+  sR = fmax(sR, 0.);
+  const bool left = sM > 0.;
+  const double* w = left ? wL : wR;
+  const double s = left ? sL : sR;
+  const double v_s = w[VX] - s;
+  const double ssMi = 1. / (s - sM);
+  const double z = -sM * ssMi;
+  const double sLR = s * ssMi;
+  double u[NM];
+  u[RHO] = w[RHO];
+  u[MX] = w[RHO] * w[VX];
+  u[MY] = w[RHO] * w[VY];
+  u[MZ] = w[RHO] * w[VZ];
+  const double v2 = sqr(w[VX]) + sqr(w[VY]) + sqr(w[VZ]);
+  const double b2 = sqr(w[BX]) + sqr(w[BY]) + sqr(w[BZ]);
+  u[EN] = 0.5 * (w[RHO] * v2 + b2) + w[PR] * gamm1i;
+  u[PSC] = w[PSC];
+  double f[BX];
+#pragma unroll
+  for (int n = 0; n < BX; ++n) f[n] = u[n] * v_s;
+  f[MX] += w[PR];
+  f[EN] += w[PR] * w[VX];
+#pragma unroll
+  for (int n = 0; n < BX; ++n) flux[n] = z * f[n];
+  flux[MX] += sLR * pts;
+  flux[EN] += sLR * pts * sM;
+  flux[BX] = flux[BY] = flux[BZ] = 0.;
 }
 
 // fluxes_c.c:447-607 (Mignone 2012 isothermal-type three-wave solver).  The
@@ -482,6 +584,8 @@ __device__ __forceinline__ void riemann(double* flux, const double* wL, const do
                                         unsigned& err) {
   if constexpr (RS == RS_HLLD) flux_hlld(flux, wL, wR, gam, err);
   else if constexpr (RS == RS_HLLT) flux_hllt(flux, wL, wR, gam, err);
+  else if constexpr (RS == RS_HLLC) flux_hllc(flux, wL, wR, gam);
+  else if constexpr (RS == RS_HLL_HYDRO) flux_hll_hydro(flux, wL, wR, gam);
   else flux_hll(flux, wL, wR, gam);
 }
 

@@ -78,6 +78,40 @@ __global__ void k_hist_final(const double* __restrict__ part, int nblk, double* 
   }
 }
 
+// Face divergence of B over the active cells, the quantity constrained
+// transport keeps at round-off (ct.pyx:15-91 updates each face by the curl of
+// the edge EMFs, so sum over a cell's faces of A * dB cancels):
+// div = sum_d (b_d[upper face] - b_d[lower face]) / dlf_d.  out[0] receives
+// max |div| * dlf_x of the cell, out[1] max |B| of the cell-centred field, as
+// the bit patterns of non-negative doubles (which order like the values).
+__global__ void k_divb(GridDev g, const double* __restrict__ w, const double* __restrict__ b,
+                       unsigned long long* __restrict__ out) {
+  const int nx = g.i2 - g.i1 + 1, ny = g.j2 - g.j1 + 1, nz = g.k2 - g.k1 + 1;
+  const long long n = (long long)nx * ny * nz;
+  const long long sy = g.nx, sz = (long long)g.nx * g.ny;
+  double dmax = 0., bmax = 0.;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = g.i1 + (int)(t % nx);
+    const int j = g.j1 + (int)((t / nx) % ny);
+    const int k = g.k1 + (int)(t / ((long long)nx * ny));
+    const long long c = k * sz + j * sy + i;
+    double d = (b[c + 1] - b[c]) * g.dlf_inv[0][i];
+    if (g.dims >= 2) d += (b[g.sv + c + sy] - b[g.sv + c]) * g.dlf_inv[1][j];
+    if (g.dims >= 3) d += (b[2 * g.sv + c + sz] - b[2 * g.sv + c]) * g.dlf_inv[2][k];
+    dmax = fmax(dmax, fabs(d) * g.dlf[0][i]);
+    const double bx = w[6 * g.sv + c], by = w[7 * g.sv + c], bz = w[8 * g.sv + c];
+    bmax = fmax(bmax, sqrt(bx * bx + by * by + bz * bz));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&out[0], (unsigned long long)__double_as_longlong(dmax));
+    atomicMax(&out[1], (unsigned long long)__double_as_longlong(bmax));
+  }
+}
+
 }  // namespace
 
 struct bnz_io {
@@ -147,6 +181,25 @@ int bnz_history(bnz_ctx* c, double* out) {
   for (int q = 0; q < NHS; ++q) out[2 + q] = o->h_sums[q] / ncells;
   // output.pyx:136-138
   for (int q = 13; q < 16; ++q) out[q] = std::sqrt(std::fabs(out[q] - out[q - 3] * out[q - 3]));
+  return BNZ_OK;
+}
+
+int bnz_div_b(bnz_ctx* c, double* out) {
+  if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
+  if (!out) return fail(c, BNZ_ERR_ARG, "null output");
+  int rc = io_init(c);
+  if (rc) return rc;
+  bnz_io* o = c->io;
+  StepArgs a = step_args(c);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(o->part);
+  CKC(cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), c->stream));
+  k_divb<<<HIST_BLOCKS, HIST_T, 0, c->stream>>>(a.g, c->prim, c->bfld, d);
+  c->launches += 1;
+  CKC(cudaGetLastError());
+  CKC(cudaMemcpyAsync(o->h_sums, d, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CKC(cudaStreamSynchronize(c->stream));
+  out[0] = o->h_sums[0];
+  out[1] = o->h_sums[1];
   return BNZ_OK;
 }
 

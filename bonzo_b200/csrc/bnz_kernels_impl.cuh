@@ -66,6 +66,14 @@ int launch_flux_rs(const StepArgs& a, const double* w, const double* bf, const p
       plain::k_flux<AX, ORDER, dev::RS_HLLT><<<nb, T, 0, a.stream>>>(a.g, w, bf, a.flx[AX], b, a.limiter, a.charact_proj,
                                                                   a.err);
       break;
+    case dev::RS_HLLC:
+      plain::k_flux<AX, ORDER, dev::RS_HLLC><<<nb, T, 0, a.stream>>>(a.g, w, bf, a.flx[AX], b, a.limiter, a.charact_proj,
+                                                                  a.err);
+      break;
+    case dev::RS_HLL_HYDRO:
+      plain::k_flux<AX, ORDER, dev::RS_HLL_HYDRO><<<nb, T, 0, a.stream>>>(a.g, w, bf, a.flx[AX], b, a.limiter,
+                                                                       a.charact_proj, a.err);
+      break;
     default:
       plain::k_flux<AX, ORDER, dev::RS_HLL><<<nb, T, 0, a.stream>>>(a.g, w, bf, a.flx[AX], b, a.limiter, a.charact_proj,
                                                                   a.err);
@@ -167,12 +175,55 @@ int drive(const StepArgs& a, const DriveArgs& d, const double* dtp) {
   return 1;
 }
 
+namespace {
+// The reference's C-level Riemann call (fluxes_c.h:3-20: flux rows from wL / wR
+// rows and the face-normal field bx over i1..i2) on device rows: entry q of
+// row n at [n * count + q].  nvar = 9 (MHD: wL[BX] = wR[BX] = bx) or 6 (the
+// hydro build: the field entries are zero and not stored).
+template <int RS>
+__global__ void k_riemann_rows(const double* __restrict__ wl, const double* __restrict__ wr,
+                               const double* __restrict__ bx, double* __restrict__ flux, int count, int nvar,
+                               double gam, unsigned* err) {
+  unsigned e = 0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+    double wL[dev::NM], wR[dev::NM], f[dev::NM];
+#pragma unroll
+    for (int n = 0; n < dev::NM; ++n) {
+      wL[n] = n < nvar ? wl[(long long)n * count + q] : 0.;
+      wR[n] = n < nvar ? wr[(long long)n * count + q] : 0.;
+    }
+    if (nvar == dev::NM) wL[dev::BX] = wR[dev::BX] = bx[q];
+    dev::riemann<RS>(f, wL, wR, gam, e);
+#pragma unroll
+    for (int n = 0; n < dev::NM; ++n)
+      if (n < nvar) flux[(long long)n * count + q] = f[n];
+  }
+  if (e && err) atomicOr(err, e);
+}
+}  // namespace
+
+int riemann_rows(int rs, const double* wl, const double* wr, const double* bx, double* flux, int n, int nvar,
+                 double gam, unsigned* err, cudaStream_t s) {
+  const int T = 128, nb = nblocks(n, T);
+  switch (rs) {
+    case dev::RS_HLLD: k_riemann_rows<dev::RS_HLLD><<<nb, T, 0, s>>>(wl, wr, bx, flux, n, nvar, gam, err); break;
+    case dev::RS_HLLT: k_riemann_rows<dev::RS_HLLT><<<nb, T, 0, s>>>(wl, wr, bx, flux, n, nvar, gam, err); break;
+    case dev::RS_HLLC: k_riemann_rows<dev::RS_HLLC><<<nb, T, 0, s>>>(wl, wr, bx, flux, n, nvar, gam, err); break;
+    case dev::RS_HLL_HYDRO:
+      k_riemann_rows<dev::RS_HLL_HYDRO><<<nb, T, 0, s>>>(wl, wr, bx, flux, n, nvar, gam, err);
+      break;
+    default: k_riemann_rows<dev::RS_HLL><<<nb, T, 0, s>>>(wl, wr, bx, flux, n, nvar, gam, err); break;
+  }
+  return 1;
+}
+
 int plain_predictor_corrector(const StepArgs& a, const double* dtp) {
   const GridDev& g = a.g;
   int l[6];
   // predictor (vanleer.pyx:104-120): order 0, dt/2, Us from U, W, B
   int nl = integrate_hydro(a, a.cons_s, a.cons, a.prim, a.bfld, 0, dtp, 0.5);
-  nl += integrate_field(a, a.cons_s, a.bfld_s, a.prim, a.bfld, 0, dtp, 0.5);
+  // the hydro build has no field to transport (vanleer.pyx:110-112 under MFIELD)
+  if (!a.hydro) nl += integrate_field(a, a.cons_s, a.bfld_s, a.prim, a.bfld, 0, dtp, 0.5);
   if (a.src) nl += source(a, a.cons_s, a.prim, 0, dtp, 0.5);
   integr_lims(g, 0, l);
   {
@@ -182,7 +233,7 @@ int plain_predictor_corrector(const StepArgs& a, const double* dtp) {
   // corrector (vanleer.pyx:130-151): order reconstr_order, dt, U from Ws, Bs
   int order = a.reconstr_order;
   nl += integrate_hydro(a, a.cons, a.cons, a.prim, a.bfld_s, order, dtp, 1.0);
-  nl += integrate_field(a, a.cons, a.bfld, a.prim, a.bfld, order, dtp, 1.0);
+  if (!a.hydro) nl += integrate_field(a, a.cons, a.bfld, a.prim, a.bfld, order, dtp, 1.0);
   if (a.src) nl += source(a, a.cons, a.prim, order, dtp, 1.0);
   integr_lims(g, order, l);
   {
@@ -237,7 +288,7 @@ int new_dt(const StepArgs& a, const double* prim, DtState* ds, double cour, int 
   const GridDev& g = a.g;
   long long n = (long long)(g.i2 - g.i1 + 1) * (g.j2 - g.j1 + 1) * (g.k2 - g.k1 + 1);
   bcdt::k_dt_reset<<<1, 1, 0, a.stream>>>(ds);
-  bcdt::k_cds_max<<<nblocks(n, 256, 148 * 8), 256, 0, a.stream>>>(g, prim, &ds->cdsmax_bits);
+  bcdt::k_cds_max<<<nblocks(n, 256, 148 * 8), 256, 0, a.stream>>>(g, prim, &ds->cdsmax_bits, a.hydro);
   bcdt::k_dt_finalize<<<1, 1, 0, a.stream>>>(ds, cour, clip);
   return 3;
 }

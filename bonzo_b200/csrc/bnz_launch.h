@@ -22,6 +22,8 @@ struct Launchers {
   int (*adj_step)(const FusedInst& I, const AdjStep& s);
   int (*source)(const StepArgs&, double* u1, const double* w0, int order, const double* dtp, double fac);
   int (*drive)(const StepArgs&, const DriveArgs&, const double* dtp);
+  int (*riemann_rows)(int rs, const double* wl, const double* wr, const double* bx, double* flux, int n, int nvar,
+                      double gam, unsigned* err, cudaStream_t s);
 };
 
 #define BNZ_DECLARE_LAUNCHERS(NS)                                                                     \
@@ -43,6 +45,8 @@ struct Launchers {
   int adj_step(const FusedInst& I, const AdjStep& s);                                                \
   int source(const StepArgs&, double* u1, const double* w0, int order, const double* dtp, double fac);  \
   int drive(const StepArgs&, const DriveArgs&, const double* dtp);                                    \
+  int riemann_rows(int rs, const double* wl, const double* wr, const double* bx, double* flux, int n, int nvar, \
+                   double gam, unsigned* err, cudaStream_t s);                                          \
   extern const Launchers table;                                                                       \
   }
 
@@ -55,4 +59,4 @@ BNZ_DECLARE_LAUNCHERS(fast)
                                NS::prim2cons_all, NS::cons2prim_all, NS::interp_bc_active,           \
                                NS::new_dt, NS::set_dt, NS::time_advance, NS::diff_dt_max,            \
                                NS::diff_operator, NS::diff_stage_update, NS::adj_step, NS::source,    \
-                               NS::drive};
+                               NS::drive, NS::riemann_rows};

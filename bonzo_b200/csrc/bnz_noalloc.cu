@@ -10,9 +10,13 @@
 //
 // The step is the fused 2D predictor + corrector of the batch path run on one
 // grid; its scratch (predictor state, time record, error word, coordinates,
-// grid descriptor and tile list) is carved out of that array.  All calls share
-// the array: two calls whose work overlaps on the GPU (different streams, or
-// different host threads) race on it and corrupt each other's results.
+// grid descriptor and tile list) is carved out of that array.  A call queues
+// work and returns: a set-up kernel that takes its parameters by value writes
+// the descriptor, time record, tiles and coordinates into the array, so no
+// host buffer is copied and the host never waits.  All calls share the array:
+// two calls whose work overlaps on the GPU (different streams, or different
+// host threads) race on it and corrupt each other's results.  The error word
+// is sticky across calls until bnz_noalloc_check reads and clears it.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -65,81 +69,142 @@ int scratch_address(unsigned char** out) {
   return BNZ_OK;
 }
 
-// Face coordinates and spacings of one axis (coord.pyx:122-258,
-// cartesian.pyx:18-43); every array has Ntot+1 entries.
-void axis_coords(int n, int Ntot, int ind1, int ind2, const bnz_grid_desc* g, std::vector<double>& lf,
-                 std::vector<double>& lv, std::vector<double>& dlf, std::vector<double>& dlfi,
-                 std::vector<double>& dlvi) {
-  lf.assign(Ntot + 1, 0.);
-  if (Ntot == 1) {
-    lf[0] = g->lmin[n];
-    lf[1] = g->lmax[n];
-  } else {
-    int Nact = ind2 - ind1 + 1;
-    double dx = (g->lmax[n] - g->lmin[n]) / Nact;
-    double l1 = 0 * Nact * dx;
-    for (int i = 0; i < Ntot + 1; ++i) lf[i] = l1 + (i - ind1) * dx;
-    if (g->bc[n][0] == BNZ_BC_PERIODIC)
-      for (int i = ind1 - 1; i > -1; --i) {
-        int i_ = ind2 - i + (ind1 - 1);
-        double d = lf[i_ + 1] - lf[i_];
-        lf[i] = lf[i + 1] - d;
+// Everything a call needs in the scratch array besides the predictor state,
+// passed by value to one set-up kernel: no host buffer is read after the call
+// returns, so nothing is uploaded and nothing waits for the GPU.
+struct Setup {
+  FusedInst inst;      // its pointers already refer to the scratch array
+  FusedInst* d_inst;   // where the descriptor goes
+  DtState* d_ds;       // the time record: dt of this step, no tmax clip
+  double dt;
+  FusedTile* d_tiles;  // predictor tiles, then corrector tiles
+  int ntA, ntB;
+  int N[2], ng, tx, ty;
+  double* coord[3];    // 5 arrays of Ntot + 1 per axis: dlf, dlf_inv, lf, lv, dlv_inv
+  int Ntot[3], ind1[3], ind2[3];
+  double lmin[3], lmax[3];
+  int bc[3][2];
+};
+
+// Tile t of one list (variant 0 tiles; the predictor's cover cells
+// 1..Ntot-2, the corrector's the active cells), as make_tiles builds them.
+__device__ FusedTile tile_of(const Setup& p, int t, bool pred) {
+  const int T[2] = {p.tx, p.ty};
+  int nt[2];
+  for (int a = 0; a < 2; ++a) nt[a] = (p.N[a] + T[a] - 1) / T[a];
+  const int b[2] = {t % nt[0], t / nt[0]};
+  int lo[2], hi[2];
+  for (int a = 0; a < 2; ++a) {
+    lo[a] = p.ng + b[a] * T[a];
+    hi[a] = min(p.ng + (b[a] + 1) * T[a], p.ng + p.N[a]) - 1;
+    if (pred) {
+      if (b[a] == 0) lo[a] = 1;
+      if (b[a] == nt[a] - 1) hi[a] = p.N[a] + 2 * p.ng - 2;
+    }
+  }
+  FusedTile r;
+  r.inst = 0;
+  r.x0 = lo[0];
+  r.y0 = lo[1];
+  r.wx = hi[0] - lo[0] + 1;
+  r.wy = hi[1] - lo[1] + 1;
+  r.tma = 0;
+  return r;
+}
+
+// One block.  The coordinates follow coord.pyx:122-258 and cartesian.pyx:18-43
+// with the context's host arithmetic operation for operation (explicitly
+// rounded adds, multiplies and divisions, never contracted), so the step is
+// bitwise the context's.  The error word is left alone: it is sticky until
+// bnz_noalloc_check reads it.
+__global__ void k_noalloc_setup(Setup p) {
+  if (threadIdx.x == 0) {
+    *p.d_inst = p.inst;
+    DtState ds;
+    memset(&ds, 0, sizeof ds);
+    ds.dt = p.dt;
+    ds.tmax = 1e300;
+    *p.d_ds = ds;
+  }
+  for (int t = threadIdx.x; t < p.ntA + p.ntB; t += blockDim.x)
+    p.d_tiles[t] = t < p.ntA ? tile_of(p, t, true) : tile_of(p, t - p.ntA, false);
+  // face coordinates: the uniform formula, then the ghost spacings of
+  // periodic / reflecting boundaries (sequential: each face uses the next one)
+  for (int a = 0; a < 3; ++a) {
+    const int len = p.Ntot[a] + 1;
+    double* lf = p.coord[a] + 2 * (size_t)len;
+    if (p.Ntot[a] == 1) {
+      if (threadIdx.x == 0) {
+        lf[0] = p.lmin[a];
+        lf[1] = p.lmax[a];
       }
-    if (g->bc[n][1] == BNZ_BC_PERIODIC)
-      for (int i = ind2 + 1; i < Ntot; ++i) {
-        int i_ = ind1 + i - (ind2 + 1);
-        double d = lf[i_ + 1] - lf[i_];
-        lf[i + 1] = lf[i] + d;
+      continue;
+    }
+    const int nact = p.ind2[a] - p.ind1[a] + 1;
+    const double dx = __ddiv_rn(__dsub_rn(p.lmax[a], p.lmin[a]), (double)nact);
+    const double l1 = __dmul_rn(__dmul_rn(0., (double)nact), dx);
+    for (int i = threadIdx.x; i < len; i += blockDim.x) lf[i] = __dadd_rn(l1, __dmul_rn((double)(i - p.ind1[a]), dx));
+  }
+  __syncthreads();
+  if (threadIdx.x < 3 && p.Ntot[threadIdx.x] > 1) {
+    const int a = threadIdx.x, Ntot = p.Ntot[a], i1 = p.ind1[a], i2 = p.ind2[a];
+    double* lf = p.coord[a] + 2 * (size_t)(Ntot + 1);
+    if (p.bc[a][0] == BNZ_BC_PERIODIC)
+      for (int i = i1 - 1; i > -1; --i) {
+        const int j = i2 - i + (i1 - 1);
+        lf[i] = __dsub_rn(lf[i + 1], __dsub_rn(lf[j + 1], lf[j]));
       }
-    if (g->bc[n][0] == BNZ_BC_REFLECT)
-      for (int i = ind1 - 1; i > -1; --i) {
-        int i_ = ind1 - i + (ind1 - 1);
-        double d = lf[i_ + 1] - lf[i_];
-        lf[i] = lf[i + 1] - d;
+    if (p.bc[a][1] == BNZ_BC_PERIODIC)
+      for (int i = i2 + 1; i < Ntot; ++i) {
+        const int j = i1 + i - (i2 + 1);
+        lf[i + 1] = __dadd_rn(lf[i], __dsub_rn(lf[j + 1], lf[j]));
       }
-    if (g->bc[n][1] == BNZ_BC_REFLECT)
-      for (int i = ind2 + 1; i < Ntot; ++i) {
-        int i_ = ind2 - i + (ind2 + 1);
-        double d = lf[i_ + 1] - lf[i_];
-        lf[i + 1] = lf[i] + d;
+    if (p.bc[a][0] == BNZ_BC_REFLECT)
+      for (int i = i1 - 1; i > -1; --i) {
+        const int j = i1 - i + (i1 - 1);
+        lf[i] = __dsub_rn(lf[i + 1], __dsub_rn(lf[j + 1], lf[j]));
+      }
+    if (p.bc[a][1] == BNZ_BC_REFLECT)
+      for (int i = i2 + 1; i < Ntot; ++i) {
+        const int j = i2 - i + (i2 + 1);
+        lf[i + 1] = __dadd_rn(lf[i], __dsub_rn(lf[j + 1], lf[j]));
       }
   }
-  lv.assign(Ntot + 1, 0.);
-  dlf.assign(Ntot + 1, 0.);
-  dlfi.assign(Ntot + 1, 0.);
-  dlvi.assign(Ntot + 1, 0.);
-  for (int i = 0; i < Ntot; ++i) {
-    dlf[i] = lf[i + 1] - lf[i];
-    dlfi[i] = 1. / dlf[i];
-    lv[i] = 0.5 * (lf[i] + lf[i + 1]);
+  __syncthreads();
+  // spacings and centres (the last entry of each array stays 0, dlv_inv[0] too)
+  for (int a = 0; a < 3; ++a) {
+    const int Ntot = p.Ntot[a], len = Ntot + 1;
+    double* dlf = p.coord[a];
+    double* dlfi = dlf + len;
+    const double* lf = dlf + 2 * (size_t)len;
+    double* lv = dlf + 3 * (size_t)len;
+    for (int i = threadIdx.x; i < len; i += blockDim.x) {
+      if (i < Ntot) {
+        const double d = __dsub_rn(lf[i + 1], lf[i]);
+        dlf[i] = d;
+        dlfi[i] = __ddiv_rn(1., d);
+        lv[i] = __dmul_rn(0.5, __dadd_rn(lf[i], lf[i + 1]));
+      } else {
+        dlf[i] = dlfi[i] = lv[i] = 0.;
+      }
+    }
   }
-  for (int i = 1; i < Ntot; ++i) {
-    double dlv = lv[i] - lv[i - 1];
-    dlvi[i] = 1. / dlv;
+  __syncthreads();
+  for (int a = 0; a < 3; ++a) {
+    const int Ntot = p.Ntot[a], len = Ntot + 1;
+    const double* lv = p.coord[a] + 3 * (size_t)len;
+    double* dlvi = p.coord[a] + 4 * (size_t)len;
+    for (int i = threadIdx.x; i < len; i += blockDim.x)
+      dlvi[i] = (i >= 1 && i < Ntot) ? __ddiv_rn(1., __dsub_rn(lv[i], lv[i - 1])) : 0.;
   }
 }
 
-// Tile lists of the default fused variant (predictor tiles cover cells
-// 1..Ntot-2, corrector tiles the active cells).
-void tiles_of(int N0, int N1, int ng, bool pred, int tx, int ty, std::vector<FusedTile>& out) {
-  const int T[2] = {tx, ty};
-  const int N[2] = {N0, N1};
-  int nt[2];
-  for (int a = 0; a < 2; ++a) nt[a] = (N[a] + T[a] - 1) / T[a];
-  for (int by = 0; by < nt[1]; ++by)
-    for (int bx = 0; bx < nt[0]; ++bx) {
-      int lo[2], hi[2];
-      const int t[2] = {bx, by};
-      for (int a = 0; a < 2; ++a) {
-        lo[a] = ng + t[a] * T[a];
-        hi[a] = std::min(ng + (t[a] + 1) * T[a], ng + N[a]) - 1;
-        if (pred) {
-          if (t[a] == 0) lo[a] = 1;
-          if (t[a] == nt[a] - 1) hi[a] = N[a] + 2 * ng - 2;
-        }
-      }
-      out.push_back(FusedTile{0, lo[0], lo[1], hi[0] - lo[0] + 1, hi[1] - lo[1] + 1});
-    }
+// Tile counts of variant 0 (the predictor's list, then the corrector's).
+int tiles_count(int N, int t) { return (N + t - 1) / t; }
+
+bool overlap(const void* a, size_t na, const void* b, size_t nb) {
+  const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+  return x < y + nb && y < x + na;
 }
 
 }  // namespace
@@ -160,27 +225,25 @@ int bnz_vl2_step_noalloc(const bnz_grid_desc* g, const bnz_method_desc* m, const
   if (!(dt > 0.) || std::isinf(dt)) return fail(BNZ_ERR_ARG, "dt must be finite and > 0");
   const int ng = 3;
   if (g->Nx < ng || g->Ny < ng) return fail(BNZ_ERR_ARG, "each axis needs at least 3 active cells");
-  for (int a = 0; a < 2; ++a) {
-    if (!(g->lmax[a] > g->lmin[a])) return fail(BNZ_ERR_ARG, "lmax must exceed lmin");
+  for (int a = 0; a < 3; ++a) {
+    // the z extent is the depth of the single z cell (face areas and volumes)
+    if (!(g->lmax[a] > g->lmin[a])) return fail(BNZ_ERR_ARG, "lmax must exceed lmin on every axis (z: the cell depth)");
     for (int sd = 0; sd < 2; ++sd)
       if (g->bc[a][sd] < 0 || g->bc[a][sd] > 2) return fail(BNZ_ERR_ARG, "bc flag must be 0, 1 or 2");
-    if ((g->bc[a][0] == BNZ_BC_PERIODIC) != (g->bc[a][1] == BNZ_BC_PERIODIC))
+    if (a < 2 && (g->bc[a][0] == BNZ_BC_PERIODIC) != (g->bc[a][1] == BNZ_BC_PERIODIC))
       return fail(BNZ_ERR_ARG, "periodic boundaries must be set on both sides of an axis");
   }
   const int nx = g->Nx + 2 * ng, ny = g->Ny + 2 * ng;
   const size_t ncell = (size_t)nx * ny;
   const FusedVariant& v = FUSED_VARIANTS[0];
-  std::vector<FusedTile> tiles;
-  tiles_of(g->Nx, g->Ny, ng, true, v.tx, v.ty, tiles);
-  const int ntA = (int)tiles.size();
-  tiles_of(g->Nx, g->Ny, ng, false, v.tx, v.ty, tiles);
-  const int ntB = (int)tiles.size() - ntA;
+  const int ntA = tiles_count(g->Nx, v.tx) * tiles_count(g->Ny, v.ty);
+  const int ntB = ntA;
   // layout of the scratch array
   const size_t o_inst = 0;
   const size_t o_ds = align256(o_inst + sizeof(FusedInst));
   const size_t o_err = align256(o_ds + sizeof(DtState));
   const size_t o_tiles = align256(o_err + sizeof(unsigned));
-  const size_t o_coord = align256(o_tiles + tiles.size() * sizeof(FusedTile));
+  const size_t o_coord = align256(o_tiles + (size_t)(ntA + ntB) * sizeof(FusedTile));
   const size_t ncoord = 5 * (size_t)(nx + 1) + 5 * (size_t)(ny + 1) + 5 * 2;
   const size_t o_ws = align256(o_coord + ncoord * sizeof(double));
   const size_t o_bs = align256(o_ws + 9 * ncell * sizeof(double));
@@ -189,33 +252,41 @@ int bnz_vl2_step_noalloc(const bnz_grid_desc* g, const bnz_method_desc* m, const
     return fail(BNZ_ERR_ARG, "grid too large for the no-alloc step: it needs " + std::to_string(need) +
                                  " bytes of scratch and the fixed array holds " + std::to_string(kScratchBytes) +
                                  " ((Nx+6)*(Ny+6) must stay below about 40000 cells)");
+  // inputs are read while outputs are written: no output may share memory
+  // with an input or with the other output
+  const size_t pb = 9 * ncell * sizeof(double), bb = 3 * ncell * sizeof(double);
+  if (overlap(prim_in, pb, prim_out, pb) || overlap(prim_in, pb, bfld_out, bb) ||
+      overlap(bfld_in, bb, prim_out, pb) || overlap(bfld_in, bb, bfld_out, bb) || overlap(prim_out, pb, bfld_out, bb))
+    return fail(BNZ_ERR_ARG, "output buffers must not overlap the input buffers or each other");
   unsigned char* base = nullptr;
   int rc = scratch_address(&base);
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
 
-  // coordinates (x, y, and the single z cell), 5 arrays per axis
-  std::vector<double> host(ncoord, 0.);
-  const double* dcoord = reinterpret_cast<const double*>(base + o_coord);
+  Setup p;
+  memset(&p, 0, sizeof p);
+  // coordinates (x, y, and the single z cell), 5 arrays of Ntot + 1 per axis
+  double* dcoord = reinterpret_cast<double*>(base + o_coord);
   const double* ptr[3][5];
   {
     size_t off = 0;
     const int N[3] = {nx, ny, 1};
     const int i1[3] = {ng, ng, 0}, i2[3] = {ng + g->Nx - 1, ng + g->Ny - 1, 0};
     for (int a = 0; a < 3; ++a) {
-      std::vector<double> lf, lv, dlf, dlfi, dlvi;
-      axis_coords(a, N[a], i1[a], i2[a], g, lf, lv, dlf, dlfi, dlvi);
-      const std::vector<double>* arr[5] = {&dlf, &dlfi, &lf, &lv, &dlvi};
       const size_t len = (size_t)N[a] + 1;
-      for (int q = 0; q < 5; ++q) {
-        for (size_t k = 0; k < len; ++k) host[off + k] = (*arr[q])[k];
-        ptr[a][q] = dcoord + off;
-        off += len;
-      }
+      p.coord[a] = dcoord + off;
+      p.Ntot[a] = N[a];
+      p.ind1[a] = i1[a];
+      p.ind2[a] = i2[a];
+      p.lmin[a] = g->lmin[a];
+      p.lmax[a] = g->lmax[a];
+      p.bc[a][0] = g->bc[a][0];
+      p.bc[a][1] = g->bc[a][1];
+      for (int q = 0; q < 5; ++q) ptr[a][q] = dcoord + off + q * len;
+      off += 5 * len;
     }
   }
-  FusedInst I;
-  memset(&I, 0, sizeof I);
+  FusedInst& I = p.inst;
   I.nx = nx;
   I.ny = ny;
   I.N[0] = g->Nx;
@@ -243,31 +314,25 @@ int bnz_vl2_step_noalloc(const bnz_grid_desc* g, const bnz_method_desc* m, const
   I.err = reinterpret_cast<unsigned*>(base + o_err);
   for (int d = 0; d < 3; ++d) I.grav[d] = m->grav[d];
   I.src = (m->grav[0] != 0. || m->grav[1] != 0. || m->grav[2] != 0.) ? 1 : 0;
-  // the time record and the error word start from zero on every call: the
-  // array keeps whatever the previous call left in it
-  DtState ds;
-  memset(&ds, 0, sizeof ds);
-  ds.dt = dt;
-  ds.tmax = 1e300;
-  unsigned zero = 0;
-  cudaError_t e;
-  e = cudaMemcpyAsync(base + o_inst, &I, sizeof I, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(base + o_ds, &ds, sizeof ds, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(base + o_err, &zero, sizeof zero, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(base + o_tiles, tiles.data(), tiles.size() * sizeof(FusedTile), cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(base + o_coord, host.data(), ncoord * sizeof(double), cudaMemcpyHostToDevice, s);
-  // the host copies above must land before the host buffers go out of scope
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return fail(BNZ_ERR_CUDA, std::string("scratch upload: ") + cudaGetErrorString(e));
+  p.d_inst = reinterpret_cast<FusedInst*>(base + o_inst);
+  p.d_ds = I.ds;
+  p.dt = dt;
+  p.d_tiles = reinterpret_cast<FusedTile*>(base + o_tiles);
+  p.ntA = ntA;
+  p.ntB = ntB;
+  p.N[0] = g->Nx;
+  p.N[1] = g->Ny;
+  p.ng = ng;
+  p.tx = v.tx;
+  p.ty = v.ty;
+  k_noalloc_setup<<<1, 256, 0, s>>>(p);
 
   const Launchers* L = m->exact_fp ? &exact::table : &fast::table;
   FusedLaunch f;
   memset(&f, 0, sizeof f);
-  f.insts = reinterpret_cast<const FusedInst*>(base + o_inst);
+  f.insts = p.d_inst;
   f.ninst = 1;
-  f.tilesA = reinterpret_cast<const FusedTile*>(base + o_tiles);
+  f.tilesA = p.d_tiles;
   f.ntA = ntA;
   f.tilesB = f.tilesA + ntA;
   f.ntB = ntB;
@@ -309,8 +374,27 @@ int bnz_vl2_step_noalloc(const bnz_grid_desc* g, const bnz_method_desc* m, const
   a.face_aware = m->outflow_face_aware;
   a.stream = s;
   L->apply_bc(a, prim_out, bfld_out, 0xFFFu);
-  e = cudaGetLastError();
+  cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(BNZ_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+  return BNZ_OK;
+}
+
+int bnz_noalloc_check(void* stream, uint32_t* err_bits) {
+  unsigned char* base = nullptr;
+  int rc = scratch_address(&base);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  // the error word sits at the same place for every grid (after the
+  // descriptor and the time record)
+  unsigned* d_err = reinterpret_cast<unsigned*>(base + align256(align256(sizeof(FusedInst)) + sizeof(DtState)));
+  unsigned h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, d_err, sizeof h, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_err, 0, sizeof(unsigned), s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(BNZ_ERR_CUDA, std::string("error word: ") + cudaGetErrorString(e));
+  if (err_bits) *err_bits = h;
+  if (h & 16u) return fail(BNZ_ERR_TIMEOUT, "a bounded device wait ran out");
+  if (h) return fail(BNZ_ERR_STATE, "non-physical state on the device (error bits " + std::to_string(h) + ")");
   return BNZ_OK;
 }
 

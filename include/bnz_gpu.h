@@ -71,7 +71,11 @@ typedef struct {
  * constant acceleration (gravity.pyx:17-19); drive_f0 / drive_tau / drive_nmod
  * = the [physics] f0, tau, nmod of the solenoidal driving force
  * (turb_driv.pyx:27-29), whose random mode amplitudes come from a splitmix64
- * stream seeded with drive_seed.  Zero f0 and grav switch them off. */
+ * stream seeded with drive_seed.  Zero f0 and grav switch them off.
+ * hydro = 1 is the reference's hydro build (MFIELD 0, src/defs_c.h:72-96):
+ * the field entries of prim / cons and the face field are held at zero, no CT
+ * runs, signal speeds are the hydro sound speed, and rsolver is hll or hllc
+ * (fluxes_c.c:175-223, 232-327); plain path, no charact_proj, no conduction. */
 typedef struct {
   double gam, cour;
   int rsolver, reconstr, limiter, charact_proj;
@@ -87,6 +91,7 @@ typedef struct {
   double drive_f0, drive_tau;
   int drive_nmod;
   unsigned long long drive_seed;
+  int hydro;
 } bnz_method_desc;
 
 typedef struct bnz_ctx bnz_ctx;
@@ -226,6 +231,14 @@ int bnz_batch_autotune(bnz_batch* batch, int steps, int* best, double* ms_per_va
  * run.  The host buffers must stay valid (page-locked for a true overlap)
  * until bnz_snapshot_wait returns. */
 int bnz_history(bnz_ctx* ctx, double* out);
+/* Divergence check of the face field, reduced on the device (synchronises):
+ * out[0] = max over active cells of |div B| * dx, with div B the sum over
+ * the cell's faces of (b_upper - b_lower) / face spacing; out[1] = max |B| of
+ * the cell-centred field.  out[0] / out[1] is the relative divergence that
+ * constrained transport keeps at round-off (the face update of
+ * src/integration/ct.pyx:15-91).  The reference computes it only in
+ * commented-out checks (src/problem/weakshock.pyx:202-205). */
+int bnz_div_b(bnz_ctx* ctx, double* out);
 int bnz_snapshot(bnz_ctx* ctx, double* prim, double* cons, double* bfld);
 int bnz_snapshot_wait(bnz_ctx* ctx);
 
@@ -263,22 +276,44 @@ int bnz_step_adjoint(bnz_ctx* ctx, double dt, const double* prim, const double* 
  * programs whose device memory belongs to a framework allocator that reserved
  * it up front, or time loops that cannot take the device-wide synchronisation
  * of a cudaMalloc / cudaFree.  The caller passes device pointers to full
- * (ghosts included) prim / bfld arrays: the input state and the output state
- * (different buffers).  The step (predictor + corrector + ghost fill of the
- * outputs, no conduction) keeps its scratch in one fixed 4 MiB device array
- * that every GPU loading the library holds until exit, which bounds the grid
- * to 2D with (Nx+6)*(Ny+6) up to about 40000 cells (e.g. 192 x 192, PLM);
- * larger grids are rejected with BNZ_ERR_ARG.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress); make that first
- * call before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race and corrupt each other.  Work is queued on `stream`
- * (cudaStream_t as void*, NULL for the legacy stream).  The message of the
- * last failure on this host thread is bnz_noalloc_last_error(). */
+ * (ghosts included) prim / bfld arrays: the input state and the output state.
+ * The outputs must not overlap the inputs or each other (BNZ_ERR_ARG).  The
+ * step (predictor + corrector + ghost fill of the outputs, no conduction)
+ * keeps its scratch in one fixed 4 MiB device array that every GPU loading the
+ * library holds until exit, which bounds the grid to 2D with (Nx+6)*(Ny+6) up
+ * to about 40000 cells (e.g. 192 x 192, PLM); larger grids are rejected with
+ * BNZ_ERR_ARG.  lmax[2] - lmin[2] is the depth of the single z cell and must
+ * be positive.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * A call queues its kernels on `stream` (cudaStream_t as void*, NULL for the
+ * legacy stream) and returns without waiting for the GPU; the descriptor, tile
+ * list and coordinates are written into the array by a set-up kernel.  All
+ * calls share the array: calls that overlap on the GPU race and corrupt each
+ * other.  The message of the last failure on this host thread is
+ * bnz_noalloc_last_error(). */
 int bnz_vl2_step_noalloc(const bnz_grid_desc* grid, const bnz_method_desc* method, const double* prim_in,
                          const double* bfld_in, double* prim_out, double* bfld_out, double dt, void* stream);
 const char* bnz_noalloc_last_error(void);
+/* Error word of the no-alloc steps queued so far (bits as bnz_check: 1 rho<=0,
+ * 2 p<=0, 4 NaN, 8 unordered Riemann fan, 16 timeout): sticky across steps,
+ * read and cleared by this call, which waits for `stream`.  Returns BNZ_OK,
+ * BNZ_ERR_STATE or BNZ_ERR_TIMEOUT as bnz_check does.  No counterpart in the
+ * reference. */
+int bnz_noalloc_check(void* stream, uint32_t* err_bits);
 /* Size in bytes of the fixed scratch array. */
 size_t bnz_noalloc_scratch_bytes(void);
+
+/* The reference's C-level Riemann call (src/mhd/fluxes_c.h:3-20: hll_flux,
+ * hllc_flux, hllt_flux, hlld_flux(flux, wL, wR, bx, i1, i2, gam) over row
+ * pointers) on DEVICE rows: n interfaces, row q of wl / wr / flux at
+ * [q * n .. q * n + n), bx[n] the face-normal field.  nvar = 9 for MHD builds
+ * (wL[BX] = wR[BX] = bx) or 6 for the hydro build (rho, v, p, passive scalar;
+ * bx unused, hll takes the hydro sound speed, hllc available).  exact_fp
+ * selects the kernels built without multiply-add contraction.  Queued on
+ * `stream`; *err_bits (a device word, may be NULL) receives the fan-ordering
+ * flags OR-ed in. */
+int bnz_riemann(int rsolver, int nvar, const double* wl, const double* wr, const double* bx, double* flux, int n,
+                double gam, int exact_fp, unsigned* err_bits, void* stream);
 
 /* Measured FP64 FMA throughput of the current device in TFLOP/s (fma chains
  * on every SM), the denominator of the kernels' FP64-pipe fraction.  No

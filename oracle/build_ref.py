@@ -1,7 +1,9 @@
 """Build the reference's own C kernels into oracle/_ref/ (test infrastructure).
 
-Reads the C sources of the reference where they lie (REF_ROOT, default
-/root/reference), compiles patched copies in a temporary directory outside
+Reads the C sources of the reference where they lie: the directory given as
+the first argument, else $BNZ_REF_ROOT, else a checkout named `reference`
+beside this repository (../reference relative to the repository root).  It
+compiles patched copies in a temporary directory outside
 the repository (deleted afterwards), and writes ONLY the shared libraries
 under oracle/_ref/ (git-ignored; they travel to the GPU box).
 
@@ -68,8 +70,13 @@ def _patch(rel, text):
     return text
 
 
+# a reference checkout beside the repository, found relative to this file
+DEFAULT_REF_ROOT = os.path.normpath(os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "..",
+                                                 "reference"))
+
+
 def build(ref_root=None, quiet=False):
-    ref_root = ref_root or os.environ.get("BNZ_REF_ROOT", "/root/reference")
+    ref_root = ref_root or os.environ.get("BNZ_REF_ROOT") or DEFAULT_REF_ROOT
     if not os.path.isdir(os.path.join(ref_root, "src", "mhd")):
         if not quiet:
             print("build_ref: reference sources not found at %s; skipped" % ref_root)

@@ -46,6 +46,7 @@ def _try_create(**kw):
     m.charact_proj = kw.get("charact_proj", 0)
     m.kappa0, m.cour_diff = kw.get("kappa0", 0.), 0.5
     m.path = kw.get("path", 1)
+    m.hydro = kw.get("hydro", 0)
     L = _lib.load()
     h = C.c_void_p()
     rc = L.bnz_create(C.byref(g), C.byref(m), C.byref(h))
@@ -66,11 +67,29 @@ def _try_create(**kw):
     (dict(kappa0=-1.0), "kappa0"),
     (dict(Nx=2), "ng"),
     (dict(path=5), "path"),
+    (dict(hydro=1, rsolver=2), "hydro mode"),
+    (dict(hydro=1, rsolver=1, path=0), "plain path"),
+    (dict(hydro=1, rsolver=1, charact_proj=1), "charact_proj"),
+    (dict(hydro=1, rsolver=0, kappa0=0.1), "conduction"),
+    (dict(hydro=3, rsolver=1), "hydro"),
 ])
 def test_bad_config_rejected_on_host(kw, frag):
     rc, msg = _try_create(**kw)
     assert rc == _lib.BNZ_ERR_ARG
     assert frag in msg
+
+
+def test_riemann_entry_rejects_bad_arguments_on_host():
+    """bnz_riemann checks its arguments before any device call: hllc is the
+    hydro build's (nvar 6), hlld the MHD builds' (nvar 9)."""
+    L = _lib.load()
+    p = C.c_void_p(16)  # never dereferenced: every case fails its host checks
+    assert L.bnz_riemann(1, 9, p, p, p, p, 4, 5. / 3, 0, None, None) == _lib.BNZ_ERR_UNSUPPORTED
+    assert L.bnz_riemann(2, 6, p, p, p, p, 4, 5. / 3, 0, None, None) == _lib.BNZ_ERR_UNSUPPORTED
+    assert L.bnz_riemann(0, 7, p, p, p, p, 4, 5. / 3, 0, None, None) == _lib.BNZ_ERR_ARG
+    assert L.bnz_riemann(0, 9, p, p, None, p, 4, 5. / 3, 0, None, None) == _lib.BNZ_ERR_ARG
+    assert L.bnz_riemann(0, 9, p, p, p, p, -1, 5. / 3, 0, None, None) == _lib.BNZ_ERR_ARG
+    assert L.bnz_riemann(0, 9, p, p, p, p, 0, 5. / 3, 0, None, None) == _lib.BNZ_OK
 
 
 def test_null_arguments():
