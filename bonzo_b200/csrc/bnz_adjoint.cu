@@ -59,8 +59,8 @@ int ensure_buf(bnz_ctx* c, double** p, size_t* cap, size_t fields) {
 
 int check_adjoint_ctx(bnz_ctx* c) {
   if (!c || !c->prim) return fail(c, BNZ_ERR_ARG, "context not created");
-  if (c->md.path != BNZ_PATH_FUSED)
-    return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built for the fused 2D path (path = fused)");
+  if (c->md.path != BNZ_PATH_FUSED || c->gd.dims != 2)
+    return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built for the fused 2D path (path = fused, dims = 2)");
   if (c->md.kappa0 > 0.) return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint covers the hyperbolic step only (kappa0 = 0)");
   if (c->md.rsolver != BNZ_RS_HLL && c->md.rsolver != BNZ_RS_HLLD && c->md.rsolver != BNZ_RS_HLLT)
     return fail(c, BNZ_ERR_UNSUPPORTED, "the adjoint is built for rsolver hll, hllt and hlld");

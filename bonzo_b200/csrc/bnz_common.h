@@ -81,6 +81,60 @@ struct FusedInst {
   int src;
 };
 
+// Fused 3D path: one grid of a 3D batch (or a single 3D context).
+struct FusedInst3 {
+  int nx, ny, nz;      // Ntot per axis
+  int N[3];            // active cells
+  int ng;
+  long long sv;        // variable stride nx*ny*nz
+  double gam;
+  int bc[3][2];
+  int face_aware;
+  const double* dlf[3];
+  const double* dlf_inv[3];
+  const double* lf[3];
+  const double* lv[3];
+  double* w[2];        // prim, ping-pong by step parity
+  double* b[2];        // face field, ping-pong
+  double* ws;          // predictor prim
+  double* bs;          // predictor face field
+  DtState* ds;
+  unsigned* err;
+  double grav[3];
+  const double* fdriv;
+  int src;
+};
+
+// Chunk shape of the 3D kernels: at most F3_TX x F3_TY cells in x, y and about
+// F3_KZ planes; the corrector's TMA box of ws covers the chunk plus two cells
+// each side from an even column: F3_BW x F3_BH cells, one plane, 9 fields.
+constexpr int F3_TX = 16, F3_TY = 8, F3_KZ = 64;
+constexpr int F3_BW = (F3_TX + 6) & ~1, F3_BH = F3_TY + 4;
+
+// A column chunk of a 3D grid: cells [x0, x0+wx) x [y0, y0+wy) x [z0, z0+wz).
+struct FusedTile3 {
+  int inst;
+  int x0, y0, z0;
+  int wx, wy, wz;
+  int tma;  // the corrector stages ws by TMA (the instance has a tensor map)
+};
+
+struct Fused3Launch {
+  const FusedInst3* insts;
+  int ninst;
+  const FusedTile3* tilesA;  // predictor chunks (cells 1..Ntot-2 of each axis)
+  int ntA;
+  const FusedTile3* tilesB;  // corrector chunks (active cells)
+  int ntB;
+  int rsolver, limiter, charact_proj;
+  double cour;
+  int dt_mode;
+  double dt_fixed;
+  const unsigned char* wsmaps;  // per-instance 4D tensor maps of ws (128 bytes each), or null
+  cudaStream_t stream;
+  cudaEvent_t* events;  // optional: before dt, predictor, corrector and after (timing)
+};
+
 // A tile of cells [x0, x0+wx) x [y0, y0+wy) (array coordinates) of one instance.
 struct FusedTile {
   int inst;

@@ -201,6 +201,12 @@ void free_all(bnz_ctx* c) {
   if (c->d_tiles) cudaFree(c->d_tiles);
   c->d_inst = nullptr;
   c->d_tiles = nullptr;
+  if (c->d_inst3) cudaFree(c->d_inst3);
+  if (c->d_tiles3) cudaFree(c->d_tiles3);
+  if (c->d_map3) cudaFree(c->d_map3);
+  c->d_inst3 = nullptr;
+  c->d_tiles3 = nullptr;
+  c->d_map3 = nullptr;
   if (c->graph) cudaGraphExecDestroy(c->graph);
   if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
   c->d_err = nullptr;
@@ -209,9 +215,88 @@ void free_all(bnz_ctx* c) {
   c->stream = nullptr;
 }
 
-// The fused kernels cover 2D grids with PLM (the corrector is order 1).
+// The fused kernels cover 2D and 3D grids with PLM (the corrector is order 1).
 bool fused_available(const bnz_grid_desc* g, const bnz_method_desc* m) {
-  return g->dims == 2 && m->reconstr == BNZ_RCN_LINEAR;
+  return (g->dims == 2 || g->dims == 3) && m->reconstr == BNZ_RCN_LINEAR && !m->hydro;
+}
+
+void make_tiles3(int inst, const int* N, int ng, bool pred, int tx, int ty, int kz, std::vector<FusedTile3>& out) {
+  int lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = pred ? 1 : ng;
+    hi[a] = pred ? N[a] + 2 * ng - 2 : ng + N[a] - 1;
+  }
+  // about kz planes per chunk, the chunks of a column of equal depth
+  const int nz = hi[2] - lo[2] + 1, nch = (nz + kz - 1) / kz, cz = (nz + nch - 1) / nch;
+  for (int z = lo[2]; z <= hi[2]; z += cz)
+    for (int y = lo[1]; y <= hi[1]; y += ty)
+      for (int x = lo[0]; x <= hi[0]; x += tx) {
+        FusedTile3 t;
+        t.inst = inst;
+        t.x0 = x;
+        t.y0 = y;
+        t.z0 = z;
+        t.wx = std::min(tx, hi[0] - x + 1);
+        t.wy = std::min(ty, hi[1] - y + 1);
+        t.wz = std::min(cz, hi[2] - z + 1);
+        t.tma = 0;
+        out.push_back(t);
+      }
+}
+
+FusedInst3 make_inst3(const bnz_ctx* c) {
+  FusedInst3 I;
+  memset(&I, 0, sizeof I);
+  I.nx = c->Ntot[0];
+  I.ny = c->Ntot[1];
+  I.nz = c->Ntot[2];
+  I.N[0] = c->i2 - c->i1 + 1;
+  I.N[1] = c->j2 - c->j1 + 1;
+  I.N[2] = c->k2 - c->k1 + 1;
+  I.ng = c->ng;
+  I.sv = (long long)c->ncell;
+  I.gam = c->md.gam;
+  for (int a = 0; a < 3; ++a) {
+    I.bc[a][0] = c->gd.bc[a][0];
+    I.bc[a][1] = c->gd.bc[a][1];
+    I.dlf[a] = c->g.dlf[a];
+    I.dlf_inv[a] = c->g.dlf_inv[a];
+    I.lf[a] = c->g.lf[a];
+    I.lv[a] = c->g.lv[a];
+  }
+  I.face_aware = c->md.outflow_face_aware;
+  I.w[0] = c->wbuf[0];
+  I.w[1] = c->wbuf[1];
+  I.b[0] = c->bbuf[0];
+  I.b[1] = c->bbuf[1];
+  I.ws = c->cons_s;
+  I.bs = c->bfld_s;
+  I.ds = c->d_ds;
+  I.err = c->d_err;
+  for (int d = 0; d < 3; ++d) I.grav[d] = c->md.grav[d];
+  I.fdriv = c->fdriv;
+  I.src = src_on(c->md) ? 1 : 0;
+  return I;
+}
+
+Fused3Launch fused3_launch(const bnz_ctx* c, int dt_mode) {
+  Fused3Launch f;
+  memset(&f, 0, sizeof f);
+  f.insts = c->d_inst3;
+  f.ninst = 1;
+  f.tilesA = c->d_tiles3;
+  f.ntA = c->ntA3;
+  f.tilesB = c->d_tiles3 + c->ntA3;
+  f.ntB = c->ntB3;
+  f.rsolver = c->md.rsolver;
+  f.limiter = c->md.limiter;
+  f.charact_proj = c->md.charact_proj;
+  f.cour = c->md.cour;
+  f.dt_mode = dt_mode;
+  f.dt_fixed = c->md.dt_fixed;
+  f.wsmaps = c->d_map3;
+  f.stream = c->stream;
+  return f;
 }
 
 // Tiles of tx x ty cells over the active range; the predictor's edge tiles
@@ -318,6 +403,32 @@ FusedLaunch fused_launch(const bnz_ctx* c, int dt_mode) {
   f.err = c->d_err;
   f.stream = c->stream;
   return f;
+}
+
+// The 3D context's chunk lists, instance record and the tensor map of ws.
+cudaError_t build_ctx3(bnz_ctx* c) {
+  std::vector<FusedTile3> t;
+  const int N[3] = {c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->k2 - c->k1 + 1};
+  make_tiles3(0, N, c->ng, true, F3_TX, F3_TY, F3_KZ, t);
+  c->ntA3 = (int)t.size();
+  make_tiles3(0, N, c->ng, false, F3_TX, F3_TY, F3_KZ, t);
+  c->ntB3 = (int)t.size() - c->ntA3;
+  CUtensorMap m;
+  const bool ok = ws_map3(c, c->cons_s, &m);
+  for (size_t q = c->ntA3; q < t.size(); ++q) t[q].tma = ok ? 1 : 0;
+  cudaError_t e = cudaSuccess;
+  if (ok) {
+    e = cudaMalloc((void**)&c->d_map3, sizeof m);
+    if (e == cudaSuccess) e = cudaMemcpy(c->d_map3, &m, sizeof m, cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_tiles3, t.size() * sizeof(FusedTile3));
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_tiles3, t.data(), t.size() * sizeof(FusedTile3), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_inst3, sizeof(FusedInst3));
+  if (e == cudaSuccess) {
+    FusedInst3 I = make_inst3(c);
+    e = cudaMemcpy(c->d_inst3, &I, sizeof I, cudaMemcpyHostToDevice);
+  }
+  return e;
 }
 
 // (Re)build the single-grid tile lists for the context's variant.
@@ -535,7 +646,9 @@ int bnz_create(const bnz_grid_desc* gd, const bnz_method_desc* md, bnz_ctx** out
   }
   e = cudaMalloc((void**)&c->d_err, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_ds, sizeof(DtState));
-  if (e == cudaSuccess && md->path == BNZ_PATH_FUSED) {
+  if (e == cudaSuccess && md->path == BNZ_PATH_FUSED && dims == 3) {
+    e = build_ctx3(c);
+  } else if (e == cudaSuccess && md->path == BNZ_PATH_FUSED) {
     e = build_ctx_tiles(c);
     if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_inst, sizeof(FusedInst));
     if (e == cudaSuccess) {
@@ -736,7 +849,8 @@ int ensure_ghosts(bnz_ctx* c) {
 int refresh_cds(bnz_ctx* c) {
   if (c->md.path != BNZ_PATH_FUSED) return BNZ_OK;
   CKC(cudaMemsetAsync(&c->d_ds->cds_bits[c->parity], 0, sizeof(unsigned long long), c->stream));
-  c->launches += c->L->fused_cds(fused_launch(c, FDT_EXPLICIT), c->parity);
+  if (c->gd.dims == 3) c->launches += c->L->fused3_cds(fused3_launch(c, FDT_EXPLICIT), c->parity);
+  else c->launches += c->L->fused_cds(fused_launch(c, FDT_EXPLICIT), c->parity);
   CKC(cudaGetLastError());
   return BNZ_OK;
 }
@@ -761,7 +875,8 @@ int step_impl(bnz_ctx* c, double dt_host, int dt_mode) {
   if (c->md.path == BNZ_PATH_PLAIN) {
     c->launches += c->L->plain_predictor_corrector(a, dtp);
   } else {
-    c->launches += c->L->fused_step(fused_launch(c, dt_mode), c->parity);
+    if (c->gd.dims == 3) c->launches += c->L->fused3_step(fused3_launch(c, dt_mode), c->parity);
+    else c->launches += c->L->fused_step(fused_launch(c, dt_mode), c->parity);
     set_parity(c, c->parity ^ 1);
     c->ghosts_stale = true;
     a = step_args(c);
@@ -1149,6 +1264,26 @@ bool cell_map(const bnz_ctx* c, const double* base, int nf, int bw, int bh, CUte
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+}  // namespace
+
+namespace bnzi {
+bool ws_map3(const bnz_ctx* c, const double* base, void* map128) {
+  EncodeTiledFn enc = encode_tiled();
+  const int nx = c->Ntot[0], ny = c->Ntot[1], nz = c->Ntot[2];
+  if (!enc || (nx & 1) || ((uintptr_t)base & 15)) return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz, 9};
+  const cuuint64_t strides[3] = {(cuuint64_t)nx * sizeof(double), (cuuint64_t)nx * ny * sizeof(double),
+                                 (cuuint64_t)nx * ny * nz * sizeof(double)};
+  const cuuint32_t box[4] = {(cuuint32_t)F3_BW, (cuuint32_t)F3_BH, 1, 9};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  return enc(static_cast<CUtensorMap*>(map128), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void*)base, dims, strides, box,
+             es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+}  // namespace bnzi
+
+namespace {
+
 // Tile lists of every instance for the batch's variant (predictor list first).
 int batch_build_tiles(bnz_batch* b) {
   const FusedVariant& v = FUSED_VARIANTS[b->variant];
@@ -1271,6 +1406,8 @@ int bnz_batch_create(const bnz_grid_desc* grids, int n, const bnz_method_desc* m
   b->md.path = BNZ_PATH_FUSED;
   if (md->kappa0 > 0.) return bfail(b, BNZ_ERR_UNSUPPORTED, "batches advance the hyperbolic step only (kappa0 = 0)");
   if (drive_on(*md)) return bfail(b, BNZ_ERR_UNSUPPORTED, "batches do not drive turbulence (drive_f0 = 0)");
+  for (int q = 0; q < n; ++q)
+    if (grids[q].dims != 2) return bfail(b, BNZ_ERR_UNSUPPORTED, "batches take 2D grids");
   cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bfail(b, BNZ_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
   std::vector<FusedInst> insts;

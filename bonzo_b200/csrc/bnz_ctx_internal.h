@@ -41,6 +41,12 @@ struct bnz_ctx {
   FusedInst* d_inst = nullptr;
   FusedTile* d_tiles = nullptr;
   int ntA = 0, ntB = 0;
+  // fused 3D path: instance record, chunk lists (predictor then corrector),
+  // the 4D tensor map of ws (null when Ntot_x is odd)
+  FusedInst3* d_inst3 = nullptr;
+  FusedTile3* d_tiles3 = nullptr;
+  int ntA3 = 0, ntB3 = 0;
+  unsigned char* d_map3 = nullptr;
   int graph_parity = -1;
   int variant = 0;
   // conduction scratch
@@ -84,6 +90,15 @@ int fail(bnz_ctx* c, int code, const std::string& msg);
 StepArgs step_args(bnz_ctx* c);
 FusedInst make_inst(const bnz_ctx* c);
 FusedLaunch fused_launch(const bnz_ctx* c, int dt_mode);
+FusedInst3 make_inst3(const bnz_ctx* c);
+Fused3Launch fused3_launch(const bnz_ctx* c, int dt_mode);
+// chunk lists of a 3D grid: the predictor range (cells 1..Ntot-2) or the
+// active cells, in chunks of at most tx x ty cells and about kz planes
+void make_tiles3(int inst, const int* N, int ng, bool pred, int tx, int ty, int kz, std::vector<FusedTile3>& out);
+// the 4D tensor map (x, y, z, field) of a 9-field array of the context for
+// the 3D corrector's staging box; false when Ntot_x is odd or the driver
+// entry point is missing
+bool ws_map3(const bnz_ctx* c, const double* base, void* map128);
 bool fused_available(const bnz_grid_desc* g, const bnz_method_desc* m);
 void set_parity(bnz_ctx* c, int p);
 int ensure_ghosts(bnz_ctx* c);

@@ -1384,7 +1384,9 @@ __global__ void __launch_bounds__(256, 2) k_pred2d_pq(const Inst* __restrict__ i
 // Clears the slot the corrector fills for the next step (or carries the slot
 // over when the step does not advance), and the persistent corrector's
 // work-queue counter.
-__global__ void k_dt_batch(const Inst* __restrict__ insts, int n, int parity, double cour, int mode, double dt_fixed,
+// (IT: the instance record of the 2D or the 3D kernels; only its ds is read)
+template <class IT>
+__global__ void k_dt_batch(const IT* __restrict__ insts, int n, int parity, double cour, int mode, double dt_fixed,
                            unsigned* queue) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q == 0 && queue) queue[0] = queue[1] = 0u;  // the persistent kernels' tile counters
@@ -1407,7 +1409,8 @@ __global__ void k_dt_batch(const Inst* __restrict__ insts, int n, int parity, do
   ds->cds_bits[parity ^ 1] = ds->dt > 0. ? 0ULL : ds->cds_bits[parity];
 }
 
-__global__ void k_time_batch(const Inst* __restrict__ insts, int n) {
+template <class IT>
+__global__ void k_time_batch(const IT* __restrict__ insts, int n) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   DtState* ds = insts[q].ds;

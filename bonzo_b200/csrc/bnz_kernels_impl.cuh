@@ -19,6 +19,7 @@ namespace BNZ_NS {
 #include "bnz_diffusion.cuh"
 #include "bnz_source.cuh"
 #include "bnz_fused.cuh"
+#include "bnz_fused3d.cuh"
 #include "bnz_adjoint_math.h"
 #include "bnz_adjoint.cuh"
 
@@ -498,6 +499,58 @@ int fused_time(const FusedLaunch& f) {
 // fused step and after the state was replaced or diffused).
 int fused_cds(const FusedLaunch& f, int parity) {
   fused::k_cds_batch<<<f.ntB, 256, 0, f.stream>>>(f.insts, f.tilesB, parity);
+  return 1;
+}
+
+// --- fused 3D path (z-marching chunks, one launch per stage) -----------------
+
+namespace {
+
+template <int ORDER, int RS, int LIM>
+void launch_vl3d(const Fused3Launch& f, int parity, const FusedTile3* tiles, int nt) {
+  constexpr size_t sm = fused3::Lay<ORDER>::bytes;
+  static bool attrs = false;
+  if (!attrs) {
+    cudaFuncSetAttribute(fused3::k_vl3d<ORDER, RS, LIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    attrs = true;
+  }
+  if (nt < 1) return;
+  fused3::k_vl3d<ORDER, RS, LIM><<<nt, fused3::NT, sm, f.stream>>>(f.insts, tiles, parity, f.charact_proj,
+                                                                   ORDER ? f.wsmaps : nullptr);
+}
+
+template <int RS>
+void launch_pred_corr3(const Fused3Launch& f, int parity) {
+  if (f.events) cudaEventRecord(f.events[1], f.stream);
+  launch_vl3d<0, RS, dev::LIM_VL>(f, parity, f.tilesA, f.ntA);
+  if (f.events) cudaEventRecord(f.events[2], f.stream);
+  if (f.limiter == dev::LIM_MC) launch_vl3d<1, RS, dev::LIM_MC>(f, parity, f.tilesB, f.ntB);
+  else if (f.limiter == dev::LIM_MM) launch_vl3d<1, RS, dev::LIM_MM>(f, parity, f.tilesB, f.ntB);
+  else launch_vl3d<1, RS, dev::LIM_VL>(f, parity, f.tilesB, f.ntB);
+  if (f.events) cudaEventRecord(f.events[3], f.stream);
+}
+
+}  // namespace
+
+int fused3_step(const Fused3Launch& f, int parity) {
+  if (f.events) cudaEventRecord(f.events[0], f.stream);
+  fused::k_dt_batch<<<(f.ninst + 127) / 128, 128, 0, f.stream>>>(f.insts, f.ninst, parity, f.cour, f.dt_mode,
+                                                                  f.dt_fixed, (unsigned*)nullptr);
+  switch (f.rsolver) {
+    case dev::RS_HLLD: launch_pred_corr3<dev::RS_HLLD>(f, parity); break;
+    case dev::RS_HLLT: launch_pred_corr3<dev::RS_HLLT>(f, parity); break;
+    default: launch_pred_corr3<dev::RS_HLL>(f, parity); break;
+  }
+  return 3;
+}
+
+int fused3_time(const Fused3Launch& f) {
+  fused::k_time_batch<<<(f.ninst + 127) / 128, 128, 0, f.stream>>>(f.insts, f.ninst);
+  return 1;
+}
+
+int fused3_cds(const Fused3Launch& f, int parity) {
+  if (f.ntB > 0) fused3::k_cds3<<<f.ntB, 256, 0, f.stream>>>(f.insts, f.tilesB, parity);
   return 1;
 }
 

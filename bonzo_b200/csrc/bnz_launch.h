@@ -24,6 +24,9 @@ struct Launchers {
   int (*drive)(const StepArgs&, const DriveArgs&, const double* dtp);
   int (*riemann_rows)(int rs, const double* wl, const double* wr, const double* bx, double* flux, int n, int nvar,
                       double gam, unsigned* err, cudaStream_t s);
+  int (*fused3_step)(const Fused3Launch&, int parity);
+  int (*fused3_time)(const Fused3Launch&);
+  int (*fused3_cds)(const Fused3Launch&, int parity);
 };
 
 #define BNZ_DECLARE_LAUNCHERS(NS)                                                                     \
@@ -47,6 +50,9 @@ struct Launchers {
   int drive(const StepArgs&, const DriveArgs&, const double* dtp);                                    \
   int riemann_rows(int rs, const double* wl, const double* wr, const double* bx, double* flux, int n, int nvar, \
                    double gam, unsigned* err, cudaStream_t s);                                          \
+  int fused3_step(const Fused3Launch&, int parity);                                                  \
+  int fused3_time(const Fused3Launch&);                                                               \
+  int fused3_cds(const Fused3Launch&, int parity);                                                    \
   extern const Launchers table;                                                                       \
   }
 
@@ -59,4 +65,5 @@ BNZ_DECLARE_LAUNCHERS(fast)
                                NS::prim2cons_all, NS::cons2prim_all, NS::interp_bc_active,           \
                                NS::new_dt, NS::set_dt, NS::time_advance, NS::diff_dt_max,            \
                                NS::diff_operator, NS::diff_stage_update, NS::adj_step, NS::source,    \
-                               NS::drive, NS::riemann_rows};
+                               NS::drive, NS::riemann_rows, NS::fused3_step, NS::fused3_time,        \
+                               NS::fused3_cds};

@@ -124,10 +124,12 @@ def test_fast_persistent_batch_graph(sweep):
         assert b[q].div_b() <= DIVB_TOL
 
 
+@pytest.mark.parametrize("path", ["fused", "plain"])
 @pytest.mark.parametrize("case,bc", [("turb3d", 0), ("blast3d", 1)])
-def test_fast_3d_100_steps(case, bc):
+def test_fast_3d_100_steps(case, bc, path):
     """3D, 32^3: 100 steps of the fast build against the oracle, div B after
-    every step, and conservation on the periodic grid."""
+    every step, and conservation on the periodic grid; the fused z-marching
+    kernels and the plain path."""
     n = 32
     if case == "turb3d":
         # rms Mach 0.5: at Mach 1 this 32^3 box reaches p < 0 near step 20 in
@@ -141,7 +143,7 @@ def test_fast_3d_100_steps(case, bc):
         prim, bfld = P.blast(gc, b_mag=0.4, b_angle=0.6, center=(0.45, 0.55, 0.5), p_ratio=40.)
         opts = dict(Nx=n, Ny=n, Nz=n, dims=3, bc=((1, 1), (1, 1), (1, 1)), gam=5. / 3, cour=0.3)
     o = oracle_sim(opts, rsolver="hlld", limiter="vl")
-    d = device_ctx(opts, rsolver="hlld", limiter="vl")
+    d = device_ctx(opts, rsolver="hlld", limiter="vl", path=path)
     for s in (o, d):
         s.set_state(prim, bfld)
         s.init()
@@ -162,12 +164,13 @@ def test_fast_3d_100_steps(case, bc):
     assert d.check() == 0
 
 
-def test_fast_cond3d_20_steps():
+@pytest.mark.parametrize("path", ["fused", "plain"])
+def test_fast_cond3d_20_steps(path):
     """3D field-aligned conduction interleaved with the step (RKL2), 32^3,
     20 steps of the fast build against the oracle."""
     gc, prim, bfld, opts = setup_case("cond3d", n=32)
     o = oracle_sim(opts)
-    d = device_ctx(opts)
+    d = device_ctx(opts, path=path)
     for s in (o, d):
         s.set_state(prim, bfld)
         s.init()
