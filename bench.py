@@ -62,8 +62,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
     ap.add_argument("--adjoint-only", action="store_true", help="print only the adjoint/forward measurement")
-    ap.add_argument("--configs", action="store_true",
-                    help="also time the 3D configurations (256^3 turbulence, 384^3 conduction; slow set-up)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the 3D configurations (256^3 turbulence, 384^3 conduction; about a minute of set-up)")
     return ap.parse_args()
 
 
@@ -477,51 +477,76 @@ def run_adjoint(warmup=1, reps=5):
                    "backward (incl. the loss); median of %d after %d warm-up" % (reps, warmup)}
 
 
-def run_configs(steps=3):
-    """The 3D configurations on the plain path, seeded synthetic initial states:
-    256^3 decaying turbulence (rms Mach 1, beta 1, VL2+PLM+HLLD+CT, CFL 0.3) and
-    384^3 field-aligned conduction (kappa_par 0.01, RKL2 super-time-stepping
-    interleaved with VL2+HLLD+CT).  Each: one warm-up step, then `steps` timed
-    steps with CUDA events; conduction steps count hyperbolic zone-updates and
-    RKL2 zone-stages (96 B each) separately."""
+def _time_ctx(c, steps, graph, stream, clk=None):
+    """ms per step of `steps` steps of a context (CUDA events on its stream);
+    graph: replayed from the captured two-step graph, else bnz_advance (host
+    loop; needed with conduction, whose stage count is chosen on the host)."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    nsts = 0
+    e0.record(stream)
+    if graph:
+        c.advance_graph(1e30, steps)
+    else:
+        for _ in range(steps):
+            c.advance(1e30, 1)
+            nsts += c.last_nsts()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, nsts / steps
+
+
+def run_configs(fused_steps=6, plain_steps=2):
+    """The 3D configurations on seeded synthetic initial states, on the fused
+    z-marching path and on the plain one-launch-per-loop path:
+    256^3 decaying turbulence (rms Mach 1, beta 1, VL2+PLM(vl)+HLLD+CT, CFL 0.3)
+    and 384^3 field-aligned conduction (kappa_par 0.01, RKL2 super-time-stepping
+    interleaved with VL2+HLLD+CT).  Each path: two warm-up steps, then timed
+    steps with CUDA events on the context's stream and the SM clock sampled.
+    Throughput counts hyperbolic zone-updates; the HBM figure counts 192 B per
+    zone-update plus 96 B per RKL2 zone-stage."""
     import torch
     from bonzo_b200 import problems as P
     from bonzo_b200._lib import Context
+    from bonzo_b200.peaks import hbm_peak
+    peak, peak_src = hbm_peak()
     out = {}
     stream = torch.cuda.Stream()
-    for name, n, kw, gen in (
-            ("turbulence_256^3", 256, dict(cour=0.3), lambda gc: P.turbulence3d(gc, seed=0)),
+    dev = torch.cuda.current_device()
+    for name, n, kw, gen, graph in (
+            ("turbulence_256^3", 256, dict(cour=0.3), lambda gc: P.turbulence3d(gc, seed=0), True),
             ("conduction_384^3", 384, dict(cour=0.4, kappa0=0.01, thcond_type="aniso"),
-             lambda gc: P.conduction3d(gc, seed=0))):
+             lambda gc: P.conduction3d(gc, seed=0), False)):
         gc = P.make_grid(n, n, n, dims=3, bc=0)
         prim, bfld = gen(gc)
-        c = Context(Nx=n, Ny=n, Nz=n, dims=3, bc=((0, 0), (0, 0), (0, 0)), gam=5. / 3, rsolver="hlld",
-                    limiter="vl", path="plain", **kw)
-        c.set_stream(stream.cuda_stream)
-        c.set_state(prim, bfld)
-        c.init()
-        del prim, bfld
-        c.advance(1e30, 1)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        nsts = 0
-        e0.record(stream)
-        for _ in range(steps):
-            c.advance(1e30, 1)
-            nsts += c.last_nsts() if kw.get("kappa0", 0.0) > 0 else 0
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / steps
-        zones = n ** 3
-        # algorithmic bytes: 192 per zone-update plus 96 per RKL2 zone-stage
-        byts = BYTES_PER_ZONE * zones + 96 * zones * nsts / steps
-        rec = {"ms_per_step": round(ms, 3), "mzone_updates_per_s": round(zones / (ms * 1e-3) / 1e6, 1),
-               "rkl2_stages_per_step": round(nsts / steps, 2),
-               "hbm_gbs_algorithmic": round(byts / (ms * 1e-3) / 1e9, 1)}
-        c.check()
+        rec = {}
+        for path, steps in (("fused", fused_steps), ("plain", plain_steps)):
+            c = Context(Nx=n, Ny=n, Nz=n, dims=3, bc=((0, 0), (0, 0), (0, 0)), gam=5. / 3, rsolver="hlld",
+                        limiter="vl", path=path, **kw)
+            c.set_stream(stream.cuda_stream)
+            c.set_state(prim, bfld)
+            c.init()
+            _time_ctx(c, 2, graph, stream)
+            with ClockSampler(dev) as clk:
+                ms, nsts = _time_ctx(c, steps, graph, stream)
+            c.check()
+            zones = n ** 3
+            byts = BYTES_PER_ZONE * zones + 96 * zones * nsts
+            achieved = byts / (ms * 1e-3) / 1e9
+            rec[path] = {"ms_per_step": round(ms, 3), "mzone_updates_per_s": round(zones / (ms * 1e-3) / 1e6, 1),
+                         "rkl2_stages_per_step": round(nsts, 2), "steps_timed": steps,
+                         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                                      "frac": round(achieved / peak, 4), "peak_source": peak_src,
+                                      "bytes": "192 B per zone-update + 96 B per RKL2 zone-stage, whole step"},
+                         "clocks": clk.record()}
+            c.close()
+            torch.cuda.empty_cache()
+        rec["fused_vs_plain"] = round(rec["plain"]["ms_per_step"] / rec["fused"]["ms_per_step"], 3)
+        rec["workload"] = ("%d^3 periodic, seeded synthetic %s, VL2+PLM(vl)+HLLD+CT%s" %
+                           (n, name.split("_")[0], ", RKL2 conduction kappa_par 0.01" if kw.get("kappa0") else ""))
         out[name] = rec
-        c.close()
-        torch.cuda.empty_cache()
+        del prim, bfld
     return out
 
 
@@ -567,7 +592,7 @@ def main():
     line = run_ours(args, rank, world, dist)
     if rank == 0 and not args.no_adjoint:
         line["adjoint"] = run_adjoint()
-    if rank == 0 and args.configs:
+    if rank == 0 and world == 1 and not args.no_configs:
         line["configs_3d"] = run_configs()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         batch = build_batch(args.instances, args.seed)

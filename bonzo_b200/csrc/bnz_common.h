@@ -106,8 +106,11 @@ struct FusedInst3 {
 };
 
 // Chunk shape of the 3D kernels: at most F3_TX x F3_TY cells in x, y and about
-// F3_KZ planes; the corrector's TMA box of ws covers the chunk plus two cells
-// each side from an even column: F3_BW x F3_BH cells, one plane, 9 fields.
+// F3_KZ planes (16 x 8 on one 512-thread block per SM: the flux phase of a
+// plane is one round, and the halo recompute of x and y faces stays at one
+// Riemann solve per cell and direction plus a third); the corrector's TMA box
+// of ws covers the chunk plus two cells each side from an even column:
+// F3_BW x F3_BH cells, one plane, 9 fields.
 constexpr int F3_TX = 16, F3_TY = 8, F3_KZ = 64;
 constexpr int F3_BW = (F3_TX + 6) & ~1, F3_BH = F3_TY + 4;
 

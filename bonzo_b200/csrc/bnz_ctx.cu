@@ -1177,6 +1177,13 @@ struct bnz_batch {
   std::vector<size_t> soff;
   struct SegCopy* d_segs[2] = {nullptr, nullptr};
   bool stage_failed = false;
+  // 3D batches: instance records, chunk lists (predictor then corrector) and
+  // the instances' 4D tensor maps of ws (128 bytes each)
+  bool dims3 = false;
+  FusedInst3* d_inst3 = nullptr;
+  FusedTile3* d_tiles3 = nullptr;
+  int ntA3 = 0, ntB3 = 0;
+  unsigned char* d_maps3 = nullptr;
 };
 
 // One contiguous copy between the staging buffer (a) and an instance buffer (b).
@@ -1224,6 +1231,26 @@ FusedLaunch batch_launch(const bnz_batch* b, int dt_mode) {
     f.withhold = b->withhold;
     if (FUSED_VARIANTS[b->variant].persistent == 2) f.wmaps = b->d_wmaps;
   }
+  return f;
+}
+
+Fused3Launch batch_launch3(const bnz_batch* b, int dt_mode) {
+  Fused3Launch f;
+  memset(&f, 0, sizeof f);
+  f.insts = b->d_inst3;
+  f.ninst = (int)b->ctx.size();
+  f.tilesA = b->d_tiles3;
+  f.ntA = b->ntA3;
+  f.tilesB = b->d_tiles3 + b->ntA3;
+  f.ntB = b->ntB3;
+  f.rsolver = b->md.rsolver;
+  f.limiter = b->md.limiter;
+  f.charact_proj = b->md.charact_proj;
+  f.cour = b->md.cour;
+  f.dt_mode = dt_mode;
+  f.dt_fixed = b->md.dt_fixed;
+  f.wsmaps = b->d_maps3;
+  f.stream = b->stream;
   return f;
 }
 
@@ -1361,7 +1388,38 @@ int batch_build_tiles(bnz_batch* b) {
   return BNZ_OK;
 }
 
-__global__ void k_set_tmax(FusedInst* insts, int n, double tmax) {
+// Instance records, chunk lists and tensor maps of a 3D batch: every
+// instance's chunks in one predictor list and one corrector list.
+int batch_build3(bnz_batch* b) {
+  const int n = (int)b->ctx.size();
+  std::vector<FusedInst3> insts;
+  std::vector<FusedTile3> tA, tB;
+  std::vector<CUtensorMap> maps(n);
+  memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
+  for (int q = 0; q < n; ++q) {
+    const bnz_ctx* c = b->ctx[q];
+    insts.push_back(make_inst3(c));
+    const int N[3] = {c->i2 - c->i1 + 1, c->j2 - c->j1 + 1, c->k2 - c->k1 + 1};
+    make_tiles3(q, N, c->ng, true, F3_TX, F3_TY, F3_KZ, tA);
+    const size_t b0 = tB.size();
+    make_tiles3(q, N, c->ng, false, F3_TX, F3_TY, F3_KZ, tB);
+    const bool ok = ws_map3(c, c->cons_s, &maps[q]);
+    for (size_t t = b0; t < tB.size(); ++t) tB[t].tma = ok ? 1 : 0;
+  }
+  b->ntA3 = (int)tA.size();
+  b->ntB3 = (int)tB.size();
+  tA.insert(tA.end(), tB.begin(), tB.end());
+  CKB(cudaMalloc((void**)&b->d_inst3, insts.size() * sizeof(FusedInst3)));
+  CKB(cudaMemcpy(b->d_inst3, insts.data(), insts.size() * sizeof(FusedInst3), cudaMemcpyHostToDevice));
+  CKB(cudaMalloc((void**)&b->d_tiles3, tA.size() * sizeof(FusedTile3)));
+  CKB(cudaMemcpy(b->d_tiles3, tA.data(), tA.size() * sizeof(FusedTile3), cudaMemcpyHostToDevice));
+  CKB(cudaMalloc((void**)&b->d_maps3, maps.size() * sizeof(CUtensorMap)));
+  CKB(cudaMemcpy(b->d_maps3, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+  return BNZ_OK;
+}
+
+template <class IT>
+__global__ void k_set_tmax(IT* insts, int n, double tmax) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q < n) insts[q].ds->tmax = tmax;
 }
@@ -1404,10 +1462,13 @@ int bnz_batch_create(const bnz_grid_desc* grids, int n, const bnz_method_desc* m
   *out = b;
   b->md = *md;
   b->md.path = BNZ_PATH_FUSED;
-  if (md->kappa0 > 0.) return bfail(b, BNZ_ERR_UNSUPPORTED, "batches advance the hyperbolic step only (kappa0 = 0)");
-  if (drive_on(*md)) return bfail(b, BNZ_ERR_UNSUPPORTED, "batches do not drive turbulence (drive_f0 = 0)");
+  b->dims3 = grids[0].dims == 3;
   for (int q = 0; q < n; ++q)
-    if (grids[q].dims != 2) return bfail(b, BNZ_ERR_UNSUPPORTED, "batches take 2D grids");
+    if (grids[q].dims != grids[0].dims || (grids[q].dims != 2 && grids[q].dims != 3))
+      return bfail(b, BNZ_ERR_UNSUPPORTED, "a batch takes 2D grids or 3D grids, not a mix");
+  if (md->kappa0 > 0. && !b->dims3)
+    return bfail(b, BNZ_ERR_UNSUPPORTED, "2D batches advance the hyperbolic step only (kappa0 = 0)");
+  if (drive_on(*md)) return bfail(b, BNZ_ERR_UNSUPPORTED, "batches do not drive turbulence (drive_f0 = 0)");
   cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bfail(b, BNZ_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
   std::vector<FusedInst> insts;
@@ -1425,6 +1486,10 @@ int bnz_batch_create(const bnz_grid_desc* grids, int n, const bnz_method_desc* m
     insts.push_back(make_inst(c));
   }
   b->L = b->ctx[0]->L;
+  if (b->dims3) {
+    b->variant = 0;
+    return batch_build3(b);
+  }
   CKB(cudaMalloc((void**)&b->d_inst, insts.size() * sizeof(FusedInst)));
   CKB(cudaMemcpy(b->d_inst, insts.data(), insts.size() * sizeof(FusedInst), cudaMemcpyHostToDevice));
   b->variant = BATCH_DEFAULT_VARIANT;
@@ -1443,6 +1508,9 @@ int bnz_batch_destroy(bnz_batch* b) {
   for (SegCopy* sg : b->d_segs)
     if (sg) cudaFree(sg);
   if (b->d_queue) cudaFree(b->d_queue);
+  if (b->d_inst3) cudaFree(b->d_inst3);
+  if (b->d_tiles3) cudaFree(b->d_tiles3);
+  if (b->d_maps3) cudaFree(b->d_maps3);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->cin) cudaStreamSynchronize(b->cin);
   if (b->cout) cudaStreamSynchronize(b->cout);
@@ -1506,8 +1574,37 @@ int batch_prologue(bnz_batch* b, double tmax) {
     }
   }
   const int n = (int)b->ctx.size();
-  k_set_tmax<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_inst, n, tmax);
+  if (b->dims3) k_set_tmax<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_inst3, n, tmax);
+  else k_set_tmax<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_inst, n, tmax);
   b->launches += 1;
+  return BNZ_OK;
+}
+
+// One step of a 3D batch with conduction: the hyperbolic step of every
+// instance in one launch per stage, then each instance's RKL2 conduction over
+// its own dt (vanleer.pyx:147-151; the stage count is chosen on the host from
+// the instance's dt, read back after the step).
+int batch_step3_diffuse(bnz_batch* b) {
+  const int mode = b->md.fixdt ? FDT_FIXED : FDT_CFL;
+  const Fused3Launch f = batch_launch3(b, mode);
+  b->launches += b->L->fused3_step(f, b->parity);
+  const int n = (int)b->ctx.size();
+  std::vector<DtState> ds(n);
+  for (int q = 0; q < n; ++q)
+    CKB(cudaMemcpyAsync(&ds[q], b->ctx[q]->d_ds, sizeof(DtState), cudaMemcpyDeviceToHost, b->stream));
+  CKB(cudaStreamSynchronize(b->stream));
+  b->parity ^= 1;
+  for (int q = 0; q < n; ++q) {
+    bnz_ctx* c = b->ctx[q];
+    set_parity(c, b->parity);
+    c->ghosts_stale = true;
+    if (ds[q].dt > 0.) {
+      int rc = diffuse_impl(c, &c->d_ds->dt, ds[q].dt, nullptr);
+      if (!rc) rc = refresh_cds(c);
+      if (rc) return bfail(b, rc, c->err);
+    }
+  }
+  b->launches += b->L->fused3_time(f);
   return BNZ_OK;
 }
 
@@ -1530,7 +1627,23 @@ int bnz_batch_advance(bnz_batch* b, double tmax, int nsteps) {
   int rc = batch_prologue(b, tmax);
   if (rc) return rc;
   const int mode = b->md.fixdt ? FDT_FIXED : FDT_CFL;
+  if (b->dims3 && b->md.kappa0 > 0.) {
+    // conduction's stage count is chosen on the host: no graph
+    for (int s = 0; s < nsteps; ++s) {
+      rc = batch_step3_diffuse(b);
+      if (rc) return rc;
+    }
+    CKB(cudaGetLastError());
+    batch_epilogue(b);
+    return BNZ_OK;
+  }
   auto one_step = [&](int p) {
+    if (b->dims3) {
+      const Fused3Launch f = batch_launch3(b, mode);
+      b->launches += b->L->fused3_step(f, p);
+      b->launches += b->L->fused3_time(f);
+      return;
+    }
     FusedLaunch f = batch_launch(b, mode);
     b->launches += b->L->fused_step(f, p);
     b->launches += b->L->fused_time(f);
@@ -1578,11 +1691,22 @@ int bnz_batch_advance_timed(bnz_batch* b, double tmax, int nsteps, double* ms_ke
   // one event set per step, so every launch of the run is timed
   std::vector<cudaEvent_t> ev(4 * (size_t)nsteps, nullptr);
   for (auto& e : ev) CKB(cudaEventCreate(&e));
+  if (b->dims3 && b->md.kappa0 > 0.) {
+    for (auto& x : ev) cudaEventDestroy(x);
+    return bfail(b, BNZ_ERR_UNSUPPORTED, "per-launch timing covers batches without conduction");
+  }
   for (int s = 0; s < nsteps; ++s) {
-    FusedLaunch f = batch_launch(b, mode);
-    f.events = &ev[4 * (size_t)s];
-    b->launches += b->L->fused_step(f, b->parity);
-    b->launches += b->L->fused_time(f);
+    if (b->dims3) {
+      Fused3Launch f = batch_launch3(b, mode);
+      f.events = &ev[4 * (size_t)s];
+      b->launches += b->L->fused3_step(f, b->parity);
+      b->launches += b->L->fused3_time(f);
+    } else {
+      FusedLaunch f = batch_launch(b, mode);
+      f.events = &ev[4 * (size_t)s];
+      b->launches += b->L->fused_step(f, b->parity);
+      b->launches += b->L->fused_time(f);
+    }
     b->parity ^= 1;
   }
   CKB(cudaGetLastError());
@@ -1681,6 +1805,7 @@ int bnz_batch_step_host(bnz_batch* b, double* const* prim, double* const* bfld, 
   for (int q = 0; q < n; ++q)
     if (!prim[q] || !bfld[q]) return bfail(b, BNZ_ERR_ARG, "null host state of instance " + std::to_string(q));
   if (nsteps < 1) return bfail(b, BNZ_ERR_ARG, "nsteps must be >= 1");
+  if (b->dims3) return bfail(b, BNZ_ERR_UNSUPPORTED, "host-state stepping covers 2D batches");
   if (nchunks <= 0) nchunks = 32;
   if (nchunks > n) nchunks = n;
   int rc = batch_prologue(b, tmax);
@@ -1824,6 +1949,7 @@ int bnz_variant_count(int* n, int* tx, int* ty, int* staged, int* persistent) {
 
 int bnz_batch_set_variant(bnz_batch* b, int v) {
   if (!b) return BNZ_ERR_ARG;
+  if (b->dims3) return v == 0 ? BNZ_OK : bfail(b, BNZ_ERR_UNSUPPORTED, "3D batches have one kernel shape");
   if (v < 0 || v >= FUSED_NVARIANT) return bfail(b, BNZ_ERR_ARG, "variant out of range");
   if (!fused_variant_built(v, b->md.rsolver == BNZ_RS_HLLD))
     return bfail(b, BNZ_ERR_UNSUPPORTED, "variants 1-7 are built for hlld only");
@@ -1843,6 +1969,7 @@ int bnz_batch_get_variant(const bnz_batch* b, int* v) {
 // state, then put the state, the time records and the variant back.
 int bnz_batch_time_variant(bnz_batch* b, int v, int steps, double* ms) {
   if (!b || steps < 1) return BNZ_ERR_ARG;
+  if (b->dims3) return bfail(b, BNZ_ERR_UNSUPPORTED, "3D batches have one kernel shape");
   const int v0 = b->variant, p0 = b->parity;
   int rc = bnz_batch_set_variant(b, v);
   if (rc) return rc;
@@ -1897,6 +2024,7 @@ int bnz_batch_time_variant(bnz_batch* b, int v, int steps, double* ms) {
 
 int bnz_batch_autotune(bnz_batch* b, int steps, int* best, double* ms_per_variant) {
   if (!b) return BNZ_ERR_ARG;
+  if (b->dims3) return bfail(b, BNZ_ERR_UNSUPPORTED, "3D batches have one kernel shape");
   const bool hlld = b->md.rsolver == BNZ_RS_HLLD;
   double best_ms = 1e300;
   int bv = 0;

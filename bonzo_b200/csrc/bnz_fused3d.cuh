@@ -59,7 +59,7 @@ constexpr unsigned BOX_BYTES = NM * BC * sizeof(double);
 
 template <int ORDER>
 struct Lay {
-  static constexpr int NWB = ORDER ? 4 : 3;  // ring depth
+  static constexpr int NWB = 4;  // ring depth
   static constexpr int WB = ORDER ? WB1 : WB0;
   static constexpr int oW = 0;
   static constexpr int oSX = oW + NWB * WB;               // corrector: x slopes of the plane
@@ -75,7 +75,7 @@ struct Lay {
   static constexpr int total = oEY + 2 * NEY;
   static constexpr size_t bytes = 128 + sizeof(double) * (size_t)total;
 };
-static_assert(Lay<1>::bytes <= 227 * 1024, "corrector shared memory");
+static_assert(Lay<1>::bytes <= 227 * 1024 && Lay<0>::bytes <= 227 * 1024, "one block per SM");
 static_assert(WB1 * sizeof(double) % 128 == 0 && BOX_BYTES <= WB1 * sizeof(double), "TMA buffers");
 
 // Index maps of a chunk (array coordinates; max-size strides).
@@ -270,11 +270,358 @@ struct Smem3 {
   __device__ __forceinline__ double* dz(int q) const { return DZ + (q & 1) * 8 * RC; }
 };
 
+// Everything one chunk's phases read and write.
+template <int ORDER>
+struct March {
+  const Inst* I;
+  Geo G;
+  Smem3<ORDER> S;
+  int parity, cp, pbase;
+  double dt;
+  AxisMap mx, my, mz;
+  int i2, j2, k2, ilast, jlast, klast;
+  long long sy, sz;
+  __device__ __forceinline__ double* buf(int p) const { return S.W + ((p - pbase) & 3) * Lay<ORDER>::WB; }
+  // the z faces and z slopes of the ring region skip its four corners (no
+  // edge EMF or cell update reads them)
+  __device__ __forceinline__ bool corner(int ci, int cj) const {
+    return (ci == 0 || ci == G.wx + 1) && (cj == 0 || cj == G.wy + 1);
+  }
+};
+
+// Pre-flux items of plane q (ORDER 1: x slopes with E_c, y slopes, z slopes;
+// ORDER 0: E_c only); u < npre(M).
+template <int ORDER>
+__device__ __forceinline__ int npre(const March<ORDER>& M) {
+  const int nc = (M.G.wx + 2) * (M.G.wy + 2);
+  return ORDER ? 3 * nc : nc;
+}
+
+template <int ORDER, int LIM>
+__device__ __forceinline__ void pre_item(const March<ORDER>& M, int q, int u) {
+  const Geo& G = M.G;
+  const int rw = G.wx + 2, nc = rw * (G.wy + 2);
+  const int dir = ORDER ? (u >= 2 * nc ? 2 : (u >= nc ? 1 : 0)) : 0;
+  const int v = u - dir * nc;
+  const int cj = v / rw, ci = v - cj * rw;
+  const int i = G.x0 - 1 + ci, j = G.y0 - 1 + cj;
+  const Plane<ORDER> Wq{M.buf(q)};
+  if (dir == 0) {
+    // cell-centred E (ct.pyx:128-148) of plane q
+    const int r = G.ri(i, j);
+    double* EC = M.S.ec(q);
+    const double vx = Wq(G, VX, i, j), vy = Wq(G, VY, i, j), vz = Wq(G, VZ, i, j);
+    const double bx = Wq(G, BX, i, j), by = Wq(G, BY, i, j), bz = Wq(G, BZ, i, j);
+    EC[r] = -(vy * bz - vz * by);
+    EC[RC + r] = (vx * bz - vz * bx);
+    EC[2 * RC + r] = -(vx * by - vy * bx);
+  }
+  if constexpr (ORDER == 1) {
+    const Plane<1> Wm{M.buf(q - 1)}, Wc{M.buf(q)}, Wp{M.buf(q + 1)};
+    if (dir == 0) slope_cell<0, LIM>(G, Wm, Wc, Wp, i, j, M.cp, M.I->gam, M.S.SX);
+    else if (dir == 1) slope_cell<1, LIM>(G, Wm, Wc, Wp, i, j, M.cp, M.I->gam, M.S.SY);
+    else if (!M.corner(ci, cj)) slope_cell<2, LIM>(G, Wm, Wc, Wp, i, j, M.cp, M.I->gam, M.S.dz(q));
+  }
+}
+
+// Flux item t of plane q: x faces, y faces, then (unless first) the z faces
+// of level q, one Riemann call site for the three directions.
+template <int ORDER, int RS>
+__device__ __forceinline__ void flux_item(const March<ORDER>& M, int q, int t, int nfx, int nfy, unsigned& e) {
+  const Geo& G = M.G;
+  const Inst& I = *M.I;
+  const int rw = G.wx + 2;
+  const int dir = t >= nfx + nfy ? 2 : (t >= nfx ? 1 : 0);
+  int i, j;
+  if (dir == 0) {
+    const int fj = t / (G.wx + 1), fi = t - fj * (G.wx + 1);
+    i = G.x0 + fi;
+    j = G.y0 - 1 + fj;
+  } else if (dir == 1) {
+    const int u = t - nfx;
+    const int fj = u / rw, fi = u - fj * rw;
+    i = G.x0 - 1 + fi;
+    j = G.y0 + fj;
+  } else {
+    const int u = t - nfx - nfy;
+    const int cj = u / rw, ci = u - cj * rw;
+    if (M.corner(ci, cj)) return;
+    i = G.x0 - 1 + ci;
+    j = G.y0 - 1 + cj;
+  }
+  const Plane<ORDER> Wq{M.buf(q)};
+  double wL[NM], wR[NM];
+  double bn;
+  if (dir == 0) {
+#pragma unroll
+    for (int n = 0; n < NM; ++n) {
+      if (n == BX) continue;
+      if (ORDER == 1) {
+        wL[n] = Wq(G, n, i - 1, j) + M.S.SX[fused::slot8(n) * RC + G.ri(i - 1, j)];
+        wR[n] = Wq(G, n, i, j) - M.S.SX[fused::slot8(n) * RC + G.ri(i, j)];
+      } else {
+        wL[n] = Wq(G, n, i - 1, j);
+        wR[n] = Wq(G, n, i, j);
+      }
+    }
+    bn = ORDER ? I.bs[q * M.sz + j * M.sy + i] : Wq(G, NM, i, j);
+  } else if (dir == 1) {
+#pragma unroll
+    for (int n = 0; n < NM; ++n) {
+      if (n == BX) continue;
+      const int gv = plain::perm<1>(n);
+      if (ORDER == 1) {
+        wL[n] = Wq(G, gv, i, j - 1) + M.S.SY[fused::slot8(n) * RC + G.ri(i, j - 1)];
+        wR[n] = Wq(G, gv, i, j) - M.S.SY[fused::slot8(n) * RC + G.ri(i, j)];
+      } else {
+        wL[n] = Wq(G, gv, i, j - 1);
+        wR[n] = Wq(G, gv, i, j);
+      }
+    }
+    bn = ORDER ? I.bs[I.sv + q * M.sz + j * M.sy + i] : Wq(G, NM + 1, i, j);
+  } else {
+    const Plane<ORDER> Wm{M.buf(q - 1)};
+    const double* DZm = M.S.dz(q - 1);
+    const double* DZc = M.S.dz(q);
+#pragma unroll
+    for (int n = 0; n < NM; ++n) {
+      if (n == BX) continue;
+      const int gv = plain::perm<2>(n);
+      if (ORDER == 1) {
+        wL[n] = Wm(G, gv, i, j) + DZm[fused::slot8(n) * RC + G.ri(i, j)];
+        wR[n] = Wq(G, gv, i, j) - DZc[fused::slot8(n) * RC + G.ri(i, j)];
+      } else {
+        wL[n] = Wm(G, gv, i, j);
+        wR[n] = Wq(G, gv, i, j);
+      }
+    }
+    bn = ORDER ? I.bs[2 * I.sv + q * M.sz + j * M.sy + i] : Wq(G, NM + 2, i, j);
+  }
+  wL[BX] = wR[BX] = bn;
+  double f[NM];
+  riemann<RS>(f, wL, wR, I.gam, e);
+  // local sweep frame -> global variables (godunov.pyx:297-324)
+  if (dir == 0) {
+    double* FX = M.S.fx(q);
+    const int o = G.fxi(i, j);
+#pragma unroll
+    for (int n = 0; n < 6; ++n) FX[n * NFX + o] = f[n];
+    FX[6 * NFX + o] = f[BY];  // fx[BY]
+    FX[7 * NFX + o] = f[BZ];  // fx[BZ]
+  } else if (dir == 1) {
+    double* FY = M.S.fy(q);
+    const int o = G.fyi(i, j);
+    FY[0 * NFY + o] = f[RHO];
+    FY[1 * NFY + o] = f[VZ];  // global MX
+    FY[2 * NFY + o] = f[VX];  // global MY
+    FY[3 * NFY + o] = f[VY];  // global MZ
+    FY[4 * NFY + o] = f[EN];
+    FY[5 * NFY + o] = f[PSC];
+    FY[6 * NFY + o] = f[BZ];  // fy[BX]
+    FY[7 * NFY + o] = f[BY];  // fy[BZ]
+  } else {
+    double* FZ = M.S.fz(q);
+    const int o = G.ri(i, j);
+    FZ[0 * RC + o] = f[RHO];
+    FZ[1 * RC + o] = f[VY];  // global MX
+    FZ[2 * RC + o] = f[VZ];  // global MY
+    FZ[3 * RC + o] = f[VX];  // global MZ
+    FZ[4 * RC + o] = f[EN];
+    FZ[5 * RC + o] = f[PSC];
+    FZ[6 * RC + o] = f[BY];  // fz[BX]
+    FZ[7 * RC + o] = f[BZ];  // fz[BY]
+  }
+}
+
+// Edge item t (ct.pyx:153-215, interp_ee1): Ez corners of plane q, then
+// (unless first) Ex and Ey edges of level q.
+template <int ORDER>
+__device__ __forceinline__ void edge_item(const March<ORDER>& M, int q, int t, int nez, int nex) {
+  const Geo& G = M.G;
+  const double *FXc = M.S.fx(q), *FYc = M.S.fy(q), *FZc = M.S.fz(q), *ECc = M.S.ec(q);
+  if (t < nez) {
+    const int cj = t / (G.wx + 1), ci = t - cj * (G.wx + 1);
+    const int i = G.x0 + ci, j = G.y0 + cj;
+    M.S.ez(q)[G.ezi(i, j)] =
+        (0.5 * (-FXc[6 * NFX + G.fxi(i, j - 1)] - FXc[6 * NFX + G.fxi(i, j)] + FYc[6 * NFY + G.fyi(i - 1, j)] +
+                FYc[6 * NFY + G.fyi(i, j)]) -
+         0.25 * (ECc[2 * RC + G.ri(i - 1, j)] + ECc[2 * RC + G.ri(i, j)] + ECc[2 * RC + G.ri(i - 1, j - 1)] +
+                 ECc[2 * RC + G.ri(i, j - 1)]));
+    return;
+  }
+  const double *FXm = M.S.fx(q - 1), *FYm = M.S.fy(q - 1), *ECm = M.S.ec(q - 1);
+  if (t < nez + nex) {
+    const int u = t - nez;
+    const int cj = u / G.wx, ci = u - cj * G.wx;
+    const int i = G.x0 + ci, j = G.y0 + cj;
+    M.S.ex(q)[G.exi(i, j)] =
+        (0.5 * (-FYm[7 * NFY + G.fyi(i, j)] - FYc[7 * NFY + G.fyi(i, j)] + FZc[7 * RC + G.ri(i, j - 1)] +
+                FZc[7 * RC + G.ri(i, j)]) -
+         0.25 * (ECc[G.ri(i, j - 1)] + ECc[G.ri(i, j)] + ECm[G.ri(i, j - 1)] + ECm[G.ri(i, j)]));
+  } else {
+    const int u = t - nez - nex;
+    const int cj = u / (G.wx + 1), ci = u - cj * (G.wx + 1);
+    const int i = G.x0 + ci, j = G.y0 + cj;
+    M.S.ey(q)[G.eyi(i, j)] =
+        (0.5 * (-FZc[6 * RC + G.ri(i - 1, j)] - FZc[6 * RC + G.ri(i, j)] + FXm[7 * NFX + G.fxi(i, j)] +
+                FXc[7 * NFX + G.fxi(i, j)]) -
+         0.25 * (ECc[RC + G.ri(i - 1, j)] + ECc[RC + G.ri(i, j)] + ECm[RC + G.ri(i - 1, j)] + ECm[RC + G.ri(i, j)]));
+  }
+}
+
+// Update item t of plane k (godunov.pyx:215-252, ct.pyx:15-123, cons2prim):
+// the plane's fluxes, the z fluxes of levels k and k+1, Ez of plane k and
+// Ex, Ey of levels k and k+1 are complete.  Returns the new state's CFL
+// value (corrector) or 0.
+template <int ORDER>
+__device__ __forceinline__ double update_item(const March<ORDER>& M, int k, int t, unsigned& e) {
+  const Geo& G = M.G;
+  const Inst& I = *M.I;
+  const int cj = t / G.wx, ci = t - cj * G.wx;
+  const int i = G.x0 + ci, j = G.y0 + cj;
+  const long long c = k * M.sz + j * M.sy + i;
+  const double *FXp = M.S.fx(k), *FYp = M.S.fy(k), *FZp = M.S.fz(k), *FZq = M.S.fz(k + 1);
+  const double *EZp = M.S.ez(k), *EXp = M.S.ex(k), *EXq = M.S.ex(k + 1), *EYp = M.S.ey(k), *EYq = M.S.ey(k + 1);
+  double w0[NM], un[NM];
+  double bxl0, bxr0, byb0, byt0, bzb0, bzt0;
+  if constexpr (ORDER == 0) {
+    // the stage input, staged through the index maps
+    const Plane<0> Wk{M.buf(k)}, Wt{M.buf(k + 1)};
+#pragma unroll
+    for (int n = 0; n < NM; ++n) w0[n] = Wk(G, n, i, j);
+    bxl0 = Wk(G, NM, i, j);
+    bxr0 = Wk(G, NM, i + 1, j);
+    byb0 = Wk(G, NM + 1, i, j);
+    byt0 = Wk(G, NM + 1, i, j + 1);
+    bzb0 = Wk(G, NM + 2, i, j);
+    bzt0 = Wt(G, NM + 2, i, j);
+  } else {
+    // w^n and b^n from global memory; faces on the domain boundary through the maps
+    const double* __restrict__ wn = I.w[M.parity];
+    const double* __restrict__ bnf = I.b[M.parity];
+#pragma unroll
+    for (int n = 0; n < NM; ++n) w0[n] = wn[n * I.sv + c];
+    const bool edge = i == I.ng || i == M.i2 || j == I.ng || j == M.j2 || k == I.ng || k == M.k2;
+    if (edge) {
+      bxl0 = face_mapped<0>(I, bnf, i, j, k, M.mx, M.my, M.mz);
+      bxr0 = face_mapped<0>(I, bnf, i + 1, j, k, M.mx, M.my, M.mz);
+      byb0 = face_mapped<1>(I, bnf, i, j, k, M.mx, M.my, M.mz);
+      byt0 = face_mapped<1>(I, bnf, i, j + 1, k, M.mx, M.my, M.mz);
+      bzb0 = face_mapped<2>(I, bnf, i, j, k, M.mx, M.my, M.mz);
+      bzt0 = face_mapped<2>(I, bnf, i, j, k + 1, M.mx, M.my, M.mz);
+    } else {
+      bxl0 = bnf[c];
+      bxr0 = bnf[c + 1];
+      byb0 = bnf[I.sv + c];
+      byt0 = bnf[I.sv + c + M.sy];
+      bzb0 = bnf[2 * I.sv + c];
+      bzt0 = bnf[2 * I.sv + c + M.sz];
+    }
+  }
+  prim2cons(un, w0, I.gam);
+  const double dt = M.dt;
+  const double dx = I.dlf[0][i], dy = I.dlf[1][j], dz = I.dlf[2][k];
+#if BNZ_FAST_MATH
+  const double idx = I.dlf_inv[0][i], idy = I.dlf_inv[1][j], idz = I.dlf_inv[2][k];
+  const double dtdv = dt * idx * idy * idz;
+#else
+  const double vol = dx * dy * dz;
+  const double dtdv = dt / vol;
+#endif
+  const double dax = dy * dz, day = dx * dz, daz = dx * dy;
+  double u[NM];
+  const int ql = G.fxi(i, j), qr = G.fxi(i + 1, j), qb = G.fyi(i, j), qt = G.fyi(i, j + 1), qz = G.ri(i, j);
+#pragma unroll
+  for (int n = 0; n < 6; ++n) {
+    double v = un[n] - dtdv * (dax * FXp[n * NFX + qr] - dax * FXp[n * NFX + ql]);
+    v -= dtdv * (day * FYp[n * NFY + qt] - day * FYp[n * NFY + qb]);
+    v -= dtdv * (daz * FZq[n * RC + qz] - daz * FZp[n * RC + qz]);
+    u[n] = v;
+  }
+  // faces (ct.pyx:15-91): Bx from Ez of the plane and Ey of its two levels,
+  // By from Ez and Ex, Bz (levels k and k+1) from Ey and Ex of its level
+#if BNZ_FAST_MATH
+  double dtda = dt * idy * idz;
+#else
+  double dtda = dt / (dy * dz);
+#endif
+  double vxl = bxl0;
+  vxl -= dtda * (dz * EZp[G.ezi(i, j + 1)] - dz * EZp[G.ezi(i, j)]);
+  vxl += dtda * (dy * EYq[G.eyi(i, j)] - dy * EYp[G.eyi(i, j)]);
+  double vxr = bxr0;
+  vxr -= dtda * (dz * EZp[G.ezi(i + 1, j + 1)] - dz * EZp[G.ezi(i + 1, j)]);
+  vxr += dtda * (dy * EYq[G.eyi(i + 1, j)] - dy * EYp[G.eyi(i + 1, j)]);
+#if BNZ_FAST_MATH
+  dtda = dt * idx * idz;
+#else
+  dtda = dt / (dx * dz);
+#endif
+  double vyb = byb0 + dtda * (dz * EZp[G.ezi(i + 1, j)] - dz * EZp[G.ezi(i, j)]);
+  vyb -= dtda * (dx * EXq[G.exi(i, j)] - dx * EXp[G.exi(i, j)]);
+  double vyt = byt0 + dtda * (dz * EZp[G.ezi(i + 1, j + 1)] - dz * EZp[G.ezi(i, j + 1)]);
+  vyt -= dtda * (dx * EXq[G.exi(i, j + 1)] - dx * EXp[G.exi(i, j + 1)]);
+#if BNZ_FAST_MATH
+  dtda = dt * idx * idy;
+#else
+  dtda = dt / (dx * dy);
+#endif
+  double vzb = bzb0 - dtda * (dy * EYp[G.eyi(i + 1, j)] - dy * EYp[G.eyi(i, j)]);
+  vzb += dtda * (dx * EXp[G.exi(i, j + 1)] - dx * EXp[G.exi(i, j)]);
+  double vzt = bzt0 - dtda * (dy * EYq[G.eyi(i + 1, j)] - dy * EYq[G.eyi(i, j)]);
+  vzt += dtda * (dx * EXq[G.exi(i, j + 1)] - dx * EXq[G.exi(i, j)]);
+  // face-to-cell field (ct.pyx:96-123)
+  u[BX] = ((I.lv[0][i] - I.lf[0][i]) * vxl + (I.lf[0][i + 1] - I.lv[0][i]) * vxr) * I.dlf_inv[0][i];
+  u[BY] = ((I.lv[1][j] - I.lf[1][j]) * vyb + (I.lf[1][j + 1] - I.lv[1][j]) * vyt) * I.dlf_inv[1][j];
+  u[BZ] = ((I.lv[2][k] - I.lf[2][k]) * vzb + (I.lf[2][k + 1] - I.lv[2][k]) * vzt) * I.dlf_inv[2][k];
+  if (I.src) {
+    // integrator.pyx:132-170 add_source_terms, with the stage input's rho and
+    // v: w^n in the predictor, ws in the corrector
+    double fs[3];
+    if (I.fdriv) {
+      fs[0] = I.fdriv[c];
+      fs[1] = I.fdriv[I.sv + c];
+      fs[2] = I.fdriv[2 * I.sv + c];
+    }
+    const double srho = ORDER ? I.ws[c] : w0[RHO];
+    const double svx = ORDER ? I.ws[VX * I.sv + c] : w0[VX];
+    const double svy = ORDER ? I.ws[VY * I.sv + c] : w0[VY];
+    const double svz = ORDER ? I.ws[VZ * I.sv + c] : w0[VZ];
+    const bool grav = I.grav[0] != 0. || I.grav[1] != 0. || I.grav[2] != 0.;
+    srcterm::apply(u, srho, svx, svy, svz, I.grav, grav, I.fdriv ? fs : nullptr, dt);
+  }
+  double wo[NM];
+  cons2prim(wo, u, I.gam);
+  if (ORDER == 1) e |= plain::check_prim(wo);
+  double* __restrict__ wout = ORDER ? I.w[M.parity ^ 1] : I.ws;
+  double* __restrict__ bout = ORDER ? I.b[M.parity ^ 1] : I.bs;
+#pragma unroll
+  for (int n = 0; n < NM; ++n) wout[n * I.sv + c] = wo[n];
+  bout[c] = vxl;
+  bout[I.sv + c] = vyb;
+  bout[2 * I.sv + c] = vzb;
+  if (i == M.ilast) bout[c + 1] = vxr;
+  if (j == M.jlast) bout[I.sv + c + M.sy] = vyt;
+  if (k == M.klast) bout[2 * I.sv + c + M.sz] = vzt;
+  if (ORDER == 0) return 0.;
+  // the next step's CFL (new_dt.pyx:55-99) on the new state
+  const double vf = fms(wo, I.gam);
+  const double cx = fabs(wo[VX]) + vf, cy = fabs(wo[VY]) + vf, cz = fabs(wo[VZ]) + vf;
+#if BNZ_FAST_MATH
+  return fmax(fmax(cx * idx, cy * idy), cz * idz);
+#else
+  return fmax(fmax(cx / dx, cy / dy), cz / dz);
+#endif
+}
+
 // The march of one chunk.  ORDER 0: predictor, ORDER 1: corrector.
+// Per plane q: the flux items of plane q (and the z faces of level q), then
+// the edge items, then -- in one phase -- the update of plane q-1 together
+// with the pre-flux items of plane q+1 (slopes, E_c), which touch disjoint
+// slots: three barriers per plane, and the update's threads share the phase
+// with the next plane's work.
 template <int ORDER, int RS, int LIM>
 __global__ void __launch_bounds__(NT, 1) k_vl3d(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
                                                 int parity, int cp, const unsigned char* __restrict__ maps) {
-  using L = Lay<ORDER>;
   extern __shared__ __align__(128) double smem_raw[];
   __shared__ Inst sI;
   __shared__ __align__(8) unsigned long long bar[4];
@@ -314,49 +661,65 @@ __global__ void __launch_bounds__(NT, 1) k_vl3d(const Inst* __restrict__ insts, 
     }
     return;
   }
-  const double dt = ORDER == 0 ? 0.5 * dtf : dtf;
-  Smem3<ORDER> S;
-  S.set(sm);
-  Geo G;
-  G.x0 = T.x0;
-  G.y0 = T.y0;
-  G.wx = T.wx;
-  G.wy = T.wy;
-  G.xs = (T.x0 - 2) & ~1;
-  G.ys = T.y0 - 2;
-  const int zlo = T.z0 - 1, zhi = T.z0 + T.wz;  // iterations q = zlo .. zhi update planes z0 .. z0+wz-1
-  const int pbase = ORDER ? T.z0 - 2 : T.z0 - 1;  // first staged plane
-  const int plast = ORDER ? zhi + 1 : zhi;        // last staged plane
+  March<ORDER> M;
+  M.I = &I;
+  M.S.set(sm);
+  M.G.x0 = T.x0;
+  M.G.y0 = T.y0;
+  M.G.wx = T.wx;
+  M.G.wy = T.wy;
+  M.G.xs = (T.x0 - 2) & ~1;
+  M.G.ys = T.y0 - 2;
+  M.parity = parity;
+  M.cp = cp;
+  M.dt = ORDER == 0 ? 0.5 * dtf : dtf;
+  M.mx = axis_map3(I, 0);
+  M.my = axis_map3(I, 1);
+  M.mz = axis_map3(I, 2);
+  M.i2 = I.ng + I.N[0] - 1;
+  M.j2 = I.ng + I.N[1] - 1;
+  M.k2 = I.ng + I.N[2] - 1;
+  M.ilast = ORDER ? M.i2 : I.nx - 2;
+  M.jlast = ORDER ? M.j2 : I.ny - 2;
+  M.klast = ORDER ? M.k2 : I.nz - 2;
+  M.sy = sy;
+  M.sz = sz;
+  const Geo& G = M.G;
+  const int zlo = T.z0 - 1, zhi = T.z0 + T.wz;  // planes q = zlo .. zhi; updates of z0 .. z0+wz-1
+  M.pbase = ORDER ? T.z0 - 2 : T.z0 - 1;        // first staged plane
+  const int pbase = M.pbase;
+  const int plast = ORDER ? zhi + 1 : zhi;      // last staged plane
   const bool tma_on = ORDER == 1 && T.tma && maps;
   const void* map = tma_on ? (const void*)(maps + (size_t)T.inst * 128) : nullptr;
-  auto buf = [&](int p) -> double* { return S.W + ((p - pbase) % L::NWB) * L::WB; };
-  // issue the staging of plane p (one thread for TMA, all threads otherwise)
+  // stage plane p into its ring buffer (one thread issues the TMA box; all
+  // threads issue cp.async and commit one group, an empty one past plast)
   auto issue = [&](int p) {
     if (p > plast) {
-      if (!tma_on) cp_async_commit();  // keep one group per iteration
+      if (!tma_on) cp_async_commit();
       return;
     }
     if (ORDER == 0) {
-      stage_pred_plane(I, G, p, I.w[parity], I.b[parity], buf(p));
+      stage_pred_plane(I, G, p, I.w[parity], I.b[parity], M.buf(p));
       cp_async_commit();
     } else if (tma_on) {
       if (threadIdx.x == 0) {
         unsigned long long* b = &bar[(p - pbase) & 3];
         fused::tma::fence_async_shared();
         fused::tma::arrive_expect(b, BOX_BYTES);
-        load_4d(buf(p), b, map, G.xs, G.ys, p, 0);
+        load_4d(M.buf(p), b, map, G.xs, G.ys, p, 0);
       }
     } else {
-      stage_ws_plane(I, G, p, buf(p));
+      stage_ws_plane(I, G, p, M.buf(p));
       cp_async_commit();
     }
   };
-  // wait for plane p: TMA -- every thread observes the buffer's phase
-  // (bounded; a wait that runs out flags the block); cp.async -- the groups up
-  // to the one before the newest are complete, then a barrier
+  // every thread observes plane p's TMA phase (bounded); cp.async: all but the
+  // newest group are complete
   auto ready = [&](int p) {
     if (tma_on) {
       if (!fused::tma::wait(&bar[(p - pbase) & 3], (unsigned)((p - pbase) >> 2) & 1u)) s_fail = 1;
+    } else {
+      cp_async_wait1();
     }
   };
   if (tma_on && threadIdx.x == 0) {
@@ -365,377 +728,84 @@ __global__ void __launch_bounds__(NT, 1) k_vl3d(const Inst* __restrict__ insts, 
     fused::tma::prefetch_map(map);
   }
   __syncthreads();
-  // prologue: the planes the first iteration reads
+  // prologue: the planes of the first pre-flux phase, and one ahead
+  int issued, waited;
   if (ORDER == 1) {
-    issue(pbase);
-    issue(pbase + 1);
-    issue(pbase + 2);
-    if (!tma_on) cp_async_wait1();  // planes pbase, pbase+1 complete; pbase+2 may be in flight
-    ready(pbase);
-    ready(pbase + 1);
+    issue(pbase);      // zlo - 1
+    issue(pbase + 1);  // zlo
+    issue(pbase + 2);  // zlo + 1
+    issue(pbase + 3);  // zlo + 2
+    if (tma_on) {
+      ready(pbase);
+      ready(pbase + 1);
+      ready(pbase + 2);
+    } else {
+      cp_async_wait1();
+    }
+    issued = pbase + 3;
+    waited = pbase + 2;
   } else {
-    issue(pbase);
+    issue(pbase);      // zlo
+    issue(pbase + 1);  // zlo + 1
+    cp_async_wait1();
+    issued = pbase + 1;
+    waited = pbase;
   }
-  int waited = ORDER ? pbase + 1 : pbase - 1;  // newest plane every thread has waited for
-  int issued = ORDER ? pbase + 2 : pbase;      // newest plane issued
+  __syncthreads();
+  for (int u = threadIdx.x; u < npre(M); u += NT) pre_item<ORDER, LIM>(M, zlo, u);
+  __syncthreads();
   unsigned e = 0;
-  const AxisMap mx = axis_map3(I, 0), my = axis_map3(I, 1), mz = axis_map3(I, 2);
-  const int i2 = I.ng + I.N[0] - 1, j2 = I.ng + I.N[1] - 1, k2 = I.ng + I.N[2] - 1;
-  const int ilast = ORDER ? i2 : I.nx - 2, jlast = ORDER ? j2 : I.ny - 2, klast = ORDER ? k2 : I.nz - 2;
   double cmax = 0.;
+  const int nfx = (G.wx + 1) * (G.wy + 2), nfy = (G.wx + 2) * (G.wy + 1), nc = (G.wx + 2) * (G.wy + 2);
+  const int nez = (G.wx + 1) * (G.wy + 1), nexy = G.wx * (G.wy + 1) + (G.wx + 1) * G.wy;
+  const int ncell = G.wx * G.wy;
   for (int q = zlo; q <= zhi; ++q) {
     const bool first = q == zlo;
-    // --- staging: the plane this iteration needs last, and the next one ---
-    if (ORDER == 1) {
-      issue(q + 2);  // into the buffer of plane q-2 (done with since the last barrier)
+    if (ORDER == 0) {
+      issue(q + 2);  // into the buffer of plane q-2 (last read before the previous barrier)
       issued = q + 2;
-      if (!tma_on) cp_async_wait1();
-      ready(q + 1);
-      waited = q + 1;
-    } else {
-      issue(q + 1);
-      issued = q + 1;
-      cp_async_wait1();
-      waited = q;
+    }
+    // --- fluxes of plane q and the z faces of level q ---
+    {
+      const int nf = nfx + nfy + (first ? 0 : nc);
+      for (int t = threadIdx.x; t < nf; t += NT) flux_item<ORDER, RS>(M, q, t, nfx, nfy, e);
+    }
+    __syncthreads();
+    if (ORDER == 1) {
+      issue(q + 3);  // into the buffer of plane q-1: its last reader was the z-face phase above
+      issued = q + 3;
+    }
+    // --- edge EMFs: Ez of plane q, Ex / Ey of level q ---
+    {
+      const int ne = nez + (first ? 0 : nexy);
+      for (int t = threadIdx.x; t < ne; t += NT) edge_item(M, q, t, nez, G.wx * (G.wy + 1));
+    }
+    // the plane the next pre-flux phase reads last
+    const int need = ORDER ? q + 2 : q + 1;
+    if (need <= plast) {
+      ready(need);
+      waited = need;
     }
     __syncthreads();
     if (s_fail) break;
-    const Plane<ORDER> Wq{buf(q)};
-    const Plane<ORDER> Wm{ORDER || !first ? buf(q - 1) : buf(q)};
-    // --- P1 (corrector): half slopes of plane q (x, y), z slopes of plane q, E_c ---
-    const int rw = G.wx + 2, nc = rw * (G.wy + 2);
-    if (ORDER == 1) {
-      const Plane<1> W1q{buf(q)}, W1m{buf(q - 1)}, W1p{buf(q + 1)};
-      FastDiv dr;
-      dr.set(rw);
-      double* EC = S.ec(q);
-      for (int t = threadIdx.x; t < 3 * nc; t += NT) {
-        const int dir = t >= 2 * nc ? 2 : (t >= nc ? 1 : 0);
-        const int u = t - dir * nc;
-        const int cj = dr.div(u), ci = u - cj * rw;
-        const int i = G.x0 - 1 + ci, j = G.y0 - 1 + cj;
-        if (dir == 0) {
-          const int r = G.ri(i, j);
-          const double vx = W1q(G, VX, i, j), vy = W1q(G, VY, i, j), vz = W1q(G, VZ, i, j);
-          const double bx = W1q(G, BX, i, j), by = W1q(G, BY, i, j), bz = W1q(G, BZ, i, j);
-          EC[r] = -(vy * bz - vz * by);
-          EC[RC + r] = (vx * bz - vz * bx);
-          EC[2 * RC + r] = -(vx * by - vy * bx);
-          slope_cell<0, LIM>(G, W1m, W1q, W1p, i, j, cp, I.gam, S.SX);
-        } else if (dir == 1) {
-          slope_cell<1, LIM>(G, W1m, W1q, W1p, i, j, cp, I.gam, S.SY);
-        } else {
-          slope_cell<2, LIM>(G, W1m, W1q, W1p, i, j, cp, I.gam, S.dz(q));
-        }
-      }
-      __syncthreads();
-    }
-    // --- P2: Riemann fluxes of the x and y faces of plane q and the z faces of level q ---
+    // --- the update of plane q-1 and the pre-flux items of plane q+1 ---
     {
-      const int nfx = (G.wx + 1) * (G.wy + 2), nfy = rw * (G.wy + 1), nfz = first ? 0 : nc;
-      FastDiv d1, d2;
-      d1.set(G.wx + 1);
-      d2.set(rw);
-      double* FX = S.fx(q);
-      double* FY = S.fy(q);
-      double* FZ = S.fz(q);
-      double* EC = S.ec(q);
-      const double* DZm = S.dz(q - 1);
-      const double* DZc = S.dz(q);
-      for (int t = threadIdx.x; t < nfx + nfy + nfz; t += NT) {
-        const int dir = t >= nfx + nfy ? 2 : (t >= nfx ? 1 : 0);
-        int i, j;
-        if (dir == 0) {
-          const int fj = d1.div(t), fi = t - fj * (G.wx + 1);
-          i = G.x0 + fi;
-          j = G.y0 - 1 + fj;
-        } else if (dir == 1) {
-          const int u = t - nfx;
-          const int fj = d2.div(u), fi = u - fj * rw;
-          i = G.x0 - 1 + fi;
-          j = G.y0 + fj;
+      const int nu = (!first && q - 1 >= T.z0) ? ncell : 0;
+      const int np = q + 1 <= zhi ? npre(M) : 0;
+      for (int t = threadIdx.x; t < np + nu; t += NT) {
+        if (t < np) {
+          pre_item<ORDER, LIM>(M, q + 1, t);
         } else {
-          const int u = t - nfx - nfy;
-          const int cj = d2.div(u), ci = u - cj * rw;
-          i = G.x0 - 1 + ci;
-          j = G.y0 - 1 + cj;
-        }
-        if (ORDER == 0 && t < nc) {
-          // predictor: E_c of cell slot t (ct.pyx:128-148) with the face items
-          const int cj = d2.div(t), ci = t - cj * rw;
-          const int ii = G.x0 - 1 + ci, jj = G.y0 - 1 + cj;
-          const int r = G.ri(ii, jj);
-          const double vx = Wq(G, VX, ii, jj), vy = Wq(G, VY, ii, jj), vz = Wq(G, VZ, ii, jj);
-          const double bx = Wq(G, BX, ii, jj), by = Wq(G, BY, ii, jj), bz = Wq(G, BZ, ii, jj);
-          EC[r] = -(vy * bz - vz * by);
-          EC[RC + r] = (vx * bz - vz * bx);
-          EC[2 * RC + r] = -(vx * by - vy * bx);
-        }
-        // one Riemann call site: the face's states and normal field per direction
-        double wL[NM], wR[NM];
-        double bn;
-        if (dir == 0) {
-#pragma unroll
-          for (int n = 0; n < NM; ++n) {
-            if (n == BX) continue;
-            if (ORDER == 1) {
-              wL[n] = Wq(G, n, i - 1, j) + S.SX[fused::slot8(n) * RC + G.ri(i - 1, j)];
-              wR[n] = Wq(G, n, i, j) - S.SX[fused::slot8(n) * RC + G.ri(i, j)];
-            } else {
-              wL[n] = Wq(G, n, i - 1, j);
-              wR[n] = Wq(G, n, i, j);
-            }
-          }
-          bn = ORDER ? I.bs[q * sz + j * sy + i] : Wq(G, NM, i, j);
-        } else if (dir == 1) {
-#pragma unroll
-          for (int n = 0; n < NM; ++n) {
-            if (n == BX) continue;
-            const int gv = plain::perm<1>(n);
-            if (ORDER == 1) {
-              wL[n] = Wq(G, gv, i, j - 1) + S.SY[fused::slot8(n) * RC + G.ri(i, j - 1)];
-              wR[n] = Wq(G, gv, i, j) - S.SY[fused::slot8(n) * RC + G.ri(i, j)];
-            } else {
-              wL[n] = Wq(G, gv, i, j - 1);
-              wR[n] = Wq(G, gv, i, j);
-            }
-          }
-          bn = ORDER ? I.bs[I.sv + q * sz + j * sy + i] : Wq(G, NM + 1, i, j);
-        } else {
-#pragma unroll
-          for (int n = 0; n < NM; ++n) {
-            if (n == BX) continue;
-            const int gv = plain::perm<2>(n);
-            if (ORDER == 1) {
-              wL[n] = Wm(G, gv, i, j) + DZm[fused::slot8(n) * RC + G.ri(i, j)];
-              wR[n] = Wq(G, gv, i, j) - DZc[fused::slot8(n) * RC + G.ri(i, j)];
-            } else {
-              wL[n] = Wm(G, gv, i, j);
-              wR[n] = Wq(G, gv, i, j);
-            }
-          }
-          bn = ORDER ? I.bs[2 * I.sv + q * sz + j * sy + i] : Wq(G, NM + 2, i, j);
-        }
-        wL[BX] = wR[BX] = bn;
-        double f[NM];
-        riemann<RS>(f, wL, wR, I.gam, e);
-        // local sweep frame -> global variables (godunov.pyx:297-324)
-        if (dir == 0) {
-          const int o = G.fxi(i, j);
-#pragma unroll
-          for (int n = 0; n < 6; ++n) FX[n * NFX + o] = f[n];
-          FX[6 * NFX + o] = f[BY];  // fx[BY]
-          FX[7 * NFX + o] = f[BZ];  // fx[BZ]
-        } else if (dir == 1) {
-          const int o = G.fyi(i, j);
-          FY[0 * NFY + o] = f[RHO];
-          FY[1 * NFY + o] = f[VZ];  // global MX
-          FY[2 * NFY + o] = f[VX];  // global MY
-          FY[3 * NFY + o] = f[VY];  // global MZ
-          FY[4 * NFY + o] = f[EN];
-          FY[5 * NFY + o] = f[PSC];
-          FY[6 * NFY + o] = f[BZ];  // fy[BX]
-          FY[7 * NFY + o] = f[BY];  // fy[BZ]
-        } else {
-          const int o = G.ri(i, j);
-          FZ[0 * RC + o] = f[RHO];
-          FZ[1 * RC + o] = f[VY];  // global MX
-          FZ[2 * RC + o] = f[VZ];  // global MY
-          FZ[3 * RC + o] = f[VX];  // global MZ
-          FZ[4 * RC + o] = f[EN];
-          FZ[5 * RC + o] = f[PSC];
-          FZ[6 * RC + o] = f[BY];  // fz[BX]
-          FZ[7 * RC + o] = f[BZ];  // fz[BY]
+          const double c = update_item<ORDER>(M, q - 1, t - np, e);
+          if (c > cmax) cmax = c;
         }
       }
     }
-    __syncthreads();
-    // --- P3: edge EMFs (ct.pyx:153-215, interp_ee1): Ez of plane q, Ex and Ey of level q ---
-    {
-      const int nez = (G.wx + 1) * (G.wy + 1), nex = first ? 0 : G.wx * (G.wy + 1),
-                ney = first ? 0 : (G.wx + 1) * G.wy;
-      FastDiv d1, d0;
-      d1.set(G.wx + 1);
-      d0.set(G.wx);
-      const double *FXc = S.fx(q), *FYc = S.fy(q), *FZc = S.fz(q), *ECc = S.ec(q);
-      const double *FXm = S.fx(q - 1), *FYm = S.fy(q - 1), *ECm = S.ec(q - 1);
-      for (int t = threadIdx.x; t < nez + nex + ney; t += NT) {
-        if (t < nez) {
-          const int cj = d1.div(t), ci = t - cj * (G.wx + 1);
-          const int i = G.x0 + ci, j = G.y0 + cj;
-          S.ez(q)[G.ezi(i, j)] =
-              (0.5 * (-FXc[6 * NFX + G.fxi(i, j - 1)] - FXc[6 * NFX + G.fxi(i, j)] + FYc[6 * NFY + G.fyi(i - 1, j)] +
-                      FYc[6 * NFY + G.fyi(i, j)]) -
-               0.25 * (ECc[2 * RC + G.ri(i - 1, j)] + ECc[2 * RC + G.ri(i, j)] + ECc[2 * RC + G.ri(i - 1, j - 1)] +
-                       ECc[2 * RC + G.ri(i, j - 1)]));
-        } else if (t < nez + nex) {
-          const int u = t - nez;
-          const int cj = d0.div(u), ci = u - cj * G.wx;
-          const int i = G.x0 + ci, j = G.y0 + cj;
-          S.ex(q)[G.exi(i, j)] =
-              (0.5 * (-FYm[7 * NFY + G.fyi(i, j)] - FYc[7 * NFY + G.fyi(i, j)] + FZc[7 * RC + G.ri(i, j - 1)] +
-                      FZc[7 * RC + G.ri(i, j)]) -
-               0.25 * (ECc[G.ri(i, j - 1)] + ECc[G.ri(i, j)] + ECm[G.ri(i, j - 1)] + ECm[G.ri(i, j)]));
-        } else {
-          const int u = t - nez - nex;
-          const int cj = d1.div(u), ci = u - cj * (G.wx + 1);
-          const int i = G.x0 + ci, j = G.y0 + cj;
-          S.ey(q)[G.eyi(i, j)] =
-              (0.5 * (-FZc[6 * RC + G.ri(i - 1, j)] - FZc[6 * RC + G.ri(i, j)] + FXm[7 * NFX + G.fxi(i, j)] +
-                      FXc[7 * NFX + G.fxi(i, j)]) -
-               0.25 * (ECc[RC + G.ri(i - 1, j)] + ECc[RC + G.ri(i, j)] + ECm[RC + G.ri(i - 1, j)] +
-                       ECm[RC + G.ri(i, j)]));
-        }
-      }
-    }
-    __syncthreads();
-    // --- P4: update plane k = q-1 (godunov.pyx:215-252, ct.pyx:15-123, cons2prim) ---
-    if (!first && q - 1 >= T.z0) {
-      const int k = q - 1;
-      const double *FXp = S.fx(k), *FYp = S.fy(k), *FZp = S.fz(k), *FZq = S.fz(q);
-      const double *EZp = S.ez(k), *EXp = S.ex(k), *EXq = S.ex(q), *EYp = S.ey(k), *EYq = S.ey(q);
-      const Plane<ORDER> Wk{buf(k)};
-      double* __restrict__ wout = ORDER ? I.w[parity ^ 1] : I.ws;
-      double* __restrict__ bout = ORDER ? I.b[parity ^ 1] : I.bs;
-      const double* __restrict__ wn = I.w[parity];
-      const double* __restrict__ bnf = I.b[parity];
-      FastDiv d0;
-      d0.set(G.wx);
-      for (int t = threadIdx.x; t < G.wx * G.wy; t += NT) {
-        const int cj = d0.div(t), ci = t - cj * G.wx;
-        const int i = G.x0 + ci, j = G.y0 + cj;
-        const long long c = k * sz + j * sy + i;
-        // stage input: w^n (u^n = prim2cons(w^n)) and b^n on the cell's faces
-        double w0[NM], un[NM];
-        double bxl0, bxr0, byb0, byt0, bzb0, bzt0;
-        if (ORDER == 0) {
-#pragma unroll
-          for (int n = 0; n < NM; ++n) w0[n] = Wk(G, n, i, j);
-          bxl0 = Wk(G, NM, i, j);
-          bxr0 = Wk(G, NM, i + 1, j);
-          byb0 = Wk(G, NM + 1, i, j);
-          byt0 = Wk(G, NM + 1, i, j + 1);
-          bzb0 = Wk(G, NM + 2, i, j);
-          bzt0 = Wq(G, NM + 2, i, j);
-        } else {
-#pragma unroll
-          for (int n = 0; n < NM; ++n) w0[n] = wn[n * I.sv + c];
-          const bool edge = i == I.ng || i == i2 || j == I.ng || j == j2 || k == I.ng || k == k2;
-          if (edge) {
-            bxl0 = face_mapped<0>(I, bnf, i, j, k, mx, my, mz);
-            bxr0 = face_mapped<0>(I, bnf, i + 1, j, k, mx, my, mz);
-            byb0 = face_mapped<1>(I, bnf, i, j, k, mx, my, mz);
-            byt0 = face_mapped<1>(I, bnf, i, j + 1, k, mx, my, mz);
-            bzb0 = face_mapped<2>(I, bnf, i, j, k, mx, my, mz);
-            bzt0 = face_mapped<2>(I, bnf, i, j, k + 1, mx, my, mz);
-          } else {
-            bxl0 = bnf[c];
-            bxr0 = bnf[c + 1];
-            byb0 = bnf[I.sv + c];
-            byt0 = bnf[I.sv + c + sy];
-            bzb0 = bnf[2 * I.sv + c];
-            bzt0 = bnf[2 * I.sv + c + sz];
-          }
-        }
-        prim2cons(un, w0, I.gam);
-        const double dx = I.dlf[0][i], dy = I.dlf[1][j], dz = I.dlf[2][k];
-#if BNZ_FAST_MATH
-        const double idx = I.dlf_inv[0][i], idy = I.dlf_inv[1][j], idz = I.dlf_inv[2][k];
-        const double dtdv = dt * idx * idy * idz;
-#else
-        const double vol = dx * dy * dz;
-        const double dtdv = dt / vol;
-#endif
-        const double dax = dy * dz, day = dx * dz, daz = dx * dy;
-        double u[NM];
-        const int ql = G.fxi(i, j), qr = G.fxi(i + 1, j), qb = G.fyi(i, j), qt = G.fyi(i, j + 1), qz = G.ri(i, j);
-#pragma unroll
-        for (int n = 0; n < 6; ++n) {
-          double v = un[n] - dtdv * (dax * FXp[n * NFX + qr] - dax * FXp[n * NFX + ql]);
-          v -= dtdv * (day * FYp[n * NFY + qt] - day * FYp[n * NFY + qb]);
-          v -= dtdv * (daz * FZq[n * RC + qz] - daz * FZp[n * RC + qz]);
-          u[n] = v;
-        }
-        // faces (ct.pyx:15-91): Bx needs Ez of plane k and Ey of levels k, k+1;
-        // By Ez and Ex; Bz (levels k and k+1) Ey and Ex of its level
-#if BNZ_FAST_MATH
-        double dtda = dt * idy * idz;
-#else
-        double dtda = dt / (dy * dz);
-#endif
-        double vxl = bxl0;
-        vxl -= dtda * (dz * EZp[G.ezi(i, j + 1)] - dz * EZp[G.ezi(i, j)]);
-        vxl += dtda * (dy * EYq[G.eyi(i, j)] - dy * EYp[G.eyi(i, j)]);
-        double vxr = bxr0;
-        vxr -= dtda * (dz * EZp[G.ezi(i + 1, j + 1)] - dz * EZp[G.ezi(i + 1, j)]);
-        vxr += dtda * (dy * EYq[G.eyi(i + 1, j)] - dy * EYp[G.eyi(i + 1, j)]);
-#if BNZ_FAST_MATH
-        dtda = dt * idx * idz;
-#else
-        dtda = dt / (dx * dz);
-#endif
-        double vyb = byb0 + dtda * (dz * EZp[G.ezi(i + 1, j)] - dz * EZp[G.ezi(i, j)]);
-        vyb -= dtda * (dx * EXq[G.exi(i, j)] - dx * EXp[G.exi(i, j)]);
-        double vyt = byt0 + dtda * (dz * EZp[G.ezi(i + 1, j + 1)] - dz * EZp[G.ezi(i, j + 1)]);
-        vyt -= dtda * (dx * EXq[G.exi(i, j + 1)] - dx * EXp[G.exi(i, j + 1)]);
-#if BNZ_FAST_MATH
-        dtda = dt * idx * idy;
-#else
-        dtda = dt / (dx * dy);
-#endif
-        double vzb = bzb0 - dtda * (dy * EYp[G.eyi(i + 1, j)] - dy * EYp[G.eyi(i, j)]);
-        vzb += dtda * (dx * EXp[G.exi(i, j + 1)] - dx * EXp[G.exi(i, j)]);
-        double vzt = bzt0 - dtda * (dy * EYq[G.eyi(i + 1, j)] - dy * EYq[G.eyi(i, j)]);
-        vzt += dtda * (dx * EXq[G.exi(i, j + 1)] - dx * EXq[G.exi(i, j)]);
-        // face-to-cell field (ct.pyx:96-123)
-        u[BX] = ((I.lv[0][i] - I.lf[0][i]) * vxl + (I.lf[0][i + 1] - I.lv[0][i]) * vxr) * I.dlf_inv[0][i];
-        u[BY] = ((I.lv[1][j] - I.lf[1][j]) * vyb + (I.lf[1][j + 1] - I.lv[1][j]) * vyt) * I.dlf_inv[1][j];
-        u[BZ] = ((I.lv[2][k] - I.lf[2][k]) * vzb + (I.lf[2][k + 1] - I.lv[2][k]) * vzt) * I.dlf_inv[2][k];
-        if (I.src) {
-          // integrator.pyx:132-170 add_source_terms, with the stage input's
-          // rho and v: w^n in the predictor, ws in the corrector
-          double fs[3];
-          if (I.fdriv) {
-            fs[0] = I.fdriv[c];
-            fs[1] = I.fdriv[I.sv + c];
-            fs[2] = I.fdriv[2 * I.sv + c];
-          }
-          const double srho = ORDER ? Wk(G, RHO, i, j) : w0[RHO];
-          const double svx = ORDER ? Wk(G, VX, i, j) : w0[VX];
-          const double svy = ORDER ? Wk(G, VY, i, j) : w0[VY];
-          const double svz = ORDER ? Wk(G, VZ, i, j) : w0[VZ];
-          const bool grav = I.grav[0] != 0. || I.grav[1] != 0. || I.grav[2] != 0.;
-          srcterm::apply(u, srho, svx, svy, svz, I.grav, grav, I.fdriv ? fs : nullptr, dt);
-        }
-        double wo[NM];
-        cons2prim(wo, u, I.gam);
-        if (ORDER == 1) e |= plain::check_prim(wo);
-#pragma unroll
-        for (int n = 0; n < NM; ++n) wout[n * I.sv + c] = wo[n];
-        bout[c] = vxl;
-        bout[I.sv + c] = vyb;
-        bout[2 * I.sv + c] = vzb;
-        if (i == ilast) bout[c + 1] = vxr;
-        if (j == jlast) bout[I.sv + c + sy] = vyt;
-        if (k == klast) bout[2 * I.sv + c + sz] = vzt;
-        if (ORDER == 1) {
-          // next step's CFL (new_dt.pyx:55-99) on the new state
-          const double vf = fms(wo, I.gam);
-          const double cx = fabs(wo[VX]) + vf, cy = fabs(wo[VY]) + vf, cz = fabs(wo[VZ]) + vf;
-#if BNZ_FAST_MATH
-          const double cds = fmax(fmax(cx * idx, cy * idy), cz * idz);
-#else
-          const double cds = fmax(fmax(cx / dx, cy / dy), cz / dz);
-#endif
-          if (cds > cmax) cmax = cds;
-        }
-      }
-    }
-    __syncthreads();  // the iteration's buffers and slots are free
+    __syncthreads();  // the plane's slots and buffers are free
   }
   if (s_fail) {
-    // a staged plane did not arrive: flag it, give the loads still in flight
-    // a bounded wait, and leave without writing the rest of the chunk
+    // a staged plane did not arrive: flag it, give the loads still in flight a
+    // bounded wait, and leave without writing the rest of the chunk
     if (threadIdx.x == 0) {
       atomicOr(I.err, (unsigned)ERR_TIMEOUT);
       for (int p = waited + 1; p <= issued && p <= plast; ++p)

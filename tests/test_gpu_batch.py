@@ -109,12 +109,105 @@ def test_batch_continues_after_tmax():
         assert b[q].check() == 0
 
 
-def test_batch_rejects_3d_and_conduction():
+def test_batch_rejects_mixed_dims_and_2d_conduction():
     from bonzo_b200._lib import Batch, BnzError
     with pytest.raises(BnzError):
-        Batch([dict(Nx=8, Ny=8, Nz=8, dims=3)], **METHOD)
+        Batch([dict(Nx=8, Ny=8, Nz=8, dims=3), dict(Nx=8, Ny=8, Nz=1, dims=2)], **METHOD)
     with pytest.raises(BnzError):
         Batch([dict(Nx=8, Ny=8, Nz=1, dims=2)], kappa0=0.1, **METHOD)
+
+
+def _instances3(shapes, seed=7):
+    rng = np.random.default_rng(seed)
+    out = []
+    for q, n in enumerate(shapes):
+        bc = q % 2  # periodic and outflow instances side by side
+        gc = P.make_grid(*n, dims=3, bc=bc)
+        if bc == 0:
+            prim, bfld = P.turbulence3d(gc, seed=seed + q, kmax=min(6, min(n) // 3), mach=0.5)
+        else:
+            prim, bfld = P.blast(gc, b_mag=rng.uniform(0.2, 0.6), b_angle=rng.uniform(0, 6.28),
+                                 center=(rng.uniform(0.3, 0.7), rng.uniform(0.3, 0.7), rng.uniform(0.3, 0.7)),
+                                 radius=0.2, p_ratio=rng.uniform(10, 100))
+        grid = dict(Nx=n[0], Ny=n[1], Nz=n[2], dims=3, bc=((bc, bc),) * 3)
+        out.append((grid, gc, prim, bfld))
+    return out
+
+
+@pytest.mark.parametrize("steps", [1, 4])
+def test_batch3d_bitwise_vs_oracle(steps):
+    """Uneven 3D grids (one odd Ntot_x, staged without TMA) advanced together by
+    the fused 3D kernels, each with its own CFL dt, against each grid alone in
+    the oracle."""
+    from bonzo_b200._lib import Batch
+    inst = _instances3([(16, 16, 16), (24, 20, 18), (21, 15, 13), (32, 24, 20)])
+    meth = dict(METHOD, cour=0.3)
+    b = Batch([g for g, *_ in inst], exact_fp=True, **meth)
+    for q, (grid, gc, prim, bfld) in enumerate(inst):
+        b[q].set_state(prim, bfld)
+        b[q].init()
+    b.advance(1e30, steps)
+    for q, (grid, gc, prim, bfld) in enumerate(inst):
+        o = oracle_sim(grid, **meth)
+        o.set_state(prim, bfld)
+        o.init()
+        o.advance(1e30, max_steps=steps)
+        t, s, _ = b[q].time()
+        assert s == steps and t == o.time, (q, t, o.time)
+        for x, y in zip(o.get_state(), b[q].get_state()):
+            assert np.array_equal(x, y), q
+        assert b[q].check() == 0
+
+
+def test_batch3d_conduction_bitwise_vs_oracle():
+    """A 3D batch with field-aligned conduction: one launch per hyperbolic stage
+    for all instances, then each instance's RKL2 stages over its own dt."""
+    from bonzo_b200._lib import Batch
+    shapes = [(16, 16, 16), (20, 18, 16)]
+    inst = []
+    for q, n in enumerate(shapes):
+        gc = P.make_grid(*n, dims=3, bc=0)
+        prim, bfld = P.conduction3d(gc, seed=q, kmax=4)
+        inst.append((dict(Nx=n[0], Ny=n[1], Nz=n[2], dims=3, bc=((0, 0),) * 3), gc, prim, bfld))
+    meth = dict(METHOD, kappa0=0.01)
+    b = Batch([g for g, *_ in inst], exact_fp=True, **meth)
+    for q, (grid, gc, prim, bfld) in enumerate(inst):
+        b[q].set_state(prim, bfld)
+        b[q].init()
+    b.advance(1e30, 3)
+    for q, (grid, gc, prim, bfld) in enumerate(inst):
+        o = oracle_sim(grid, **meth)
+        o.set_state(prim, bfld)
+        o.init()
+        o.advance(1e30, max_steps=3)
+        assert b[q].time()[1] == 3 and b[q].time()[0] == o.time
+        for x, y in zip(o.get_state(), b[q].get_state()):
+            assert np.array_equal(x, y), q
+
+
+def test_batch3d_timed_and_tmax():
+    """Per-launch timing of a 3D batch, and instances stopping at tmax."""
+    from bonzo_b200._lib import Batch
+    inst = _instances3([(16, 16, 16), (24, 24, 24)])
+    meth = dict(METHOD, cour=0.3)
+    b = Batch([g for g, *_ in inst], exact_fp=True, **meth)
+    for q, (grid, gc, prim, bfld) in enumerate(inst):
+        b[q].set_state(prim, bfld)
+        b[q].init()
+    ms = b.advance_timed(1e30, 2)
+    assert ms["predictor"] > 0 and ms["corrector"] > 0
+    tmax = b[0].time()[0] + 0.004
+    b.advance(tmax, 40)
+    for q, (grid, gc, prim, bfld) in enumerate(inst):
+        o = oracle_sim(grid, **meth)
+        o.set_state(prim, bfld)
+        o.init()
+        o.advance(1e30, max_steps=2)
+        o.advance(tmax)
+        t, s, _ = b[q].time()
+        assert t == tmax and s == o.nstep
+        for x, y in zip(o.get_state(), b[q].get_state()):
+            assert np.array_equal(x, y), q
 
 
 @pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9])
