@@ -547,7 +547,77 @@ def run_configs(fused_steps=6, plain_steps=2):
                            (n, name.split("_")[0], ", RKL2 conduction kappa_par 0.01" if kw.get("kappa0") else ""))
         out[name] = rec
         del prim, bfld
+    out["conduction_batch_4x192^3"] = run_batch3d(stream, dev, peak, peak_src, fused_steps)
     return out
+
+
+def run_batch3d(stream, dev, peak, peak_src, steps, n=192, count=4):
+    """The conduction configuration's batch: 4 instances of 192^3 (seeds 0..3)
+    advanced together -- one launch per hyperbolic stage for all instances, then
+    each instance's RKL2 stages over its own dt -- beside the same instances as
+    separate fused contexts stepped one after another."""
+    import torch
+    from bonzo_b200 import problems as P
+    from bonzo_b200._lib import Batch, Context
+    ics = []
+    for q in range(count):
+        gc = P.make_grid(n, n, n, dims=3, bc=0)
+        ics.append(P.conduction3d(gc, seed=q))
+    meth = dict(gam=5. / 3, cour=0.4, rsolver="hlld", limiter="vl", kappa0=0.01, thcond_type="aniso")
+    grid = dict(Nx=n, Ny=n, Nz=n, dims=3, bc=((0, 0), (0, 0), (0, 0)))
+    rec = {"workload": "%d instances of %d^3 periodic field-aligned conduction (seeds 0..%d), VL2+PLM(vl)+HLLD+CT "
+                       "with RKL2, per-instance CFL dt" % (count, n, count - 1)}
+    zones = count * n ** 3
+    b = Batch([grid] * count, **meth)
+    b.set_stream(stream.cuda_stream)
+    for q, (prim, bfld) in enumerate(ics):
+        b[q].set_state(prim, bfld)
+        b[q].init()
+    b.advance(1e30, 2)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        e0.record(stream)
+        b.advance(1e30, steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    nsts = sum(b[q].last_nsts() for q in range(count))
+    for q in range(count):
+        b[q].check()
+    byts = BYTES_PER_ZONE * zones + 96 * n ** 3 * nsts
+    ach = byts / (ms * 1e-3) / 1e9
+    rec["batch"] = {"ms_per_step": round(ms, 3), "mzone_updates_per_s": round(zones / (ms * 1e-3) / 1e6, 1),
+                    "rkl2_stages_per_step_all_instances": nsts, "steps_timed": steps,
+                    "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                                 "frac": round(ach / peak, 4), "peak_source": peak_src},
+                    "clocks": clk.record()}
+    b.close()
+    torch.cuda.empty_cache()
+    ctxs = []
+    for prim, bfld in ics:
+        c = Context(path="fused", **grid, **meth)
+        c.set_stream(stream.cuda_stream)
+        c.set_state(prim, bfld)
+        c.init()
+        c.advance(1e30, 2)
+        ctxs.append(c)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        for c in ctxs:
+            c.advance(1e30, 1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_sep = e0.elapsed_time(e1) / steps
+    rec["separate_contexts"] = {"ms_per_step": round(ms_sep, 3),
+                                "mzone_updates_per_s": round(zones / (ms_sep * 1e-3) / 1e6, 1)}
+    rec["batch_vs_separate"] = round(ms_sep / ms, 3)
+    for c in ctxs:
+        c.check()
+        c.close()
+    torch.cuda.empty_cache()
+    return rec
 
 
 def main():

@@ -825,8 +825,7 @@ int diffuse_impl(bnz_ctx* c, const double* dtp, double dt_hyp, int* nsts_out) {
   c->last_nsts = s;
   if (nsts_out) *nsts_out = s;
   for (int n = 1; n <= s; ++n) {
-    c->launches += c->L->diff_operator(a, c->da);
-    c->launches += c->L->diff_stage_update(a, c->da, n == 1, &cf[(size_t)n * 4], dtp);
+    c->launches += c->L->diff_stage(a, c->da, n == 1, &cf[(size_t)n * 4], dtp);
     if (n % c->ng == 0 && n != s) c->L->apply_bc(a, c->prim, c->bfld, 1u << 4);
   }
   CKC(cudaGetLastError());

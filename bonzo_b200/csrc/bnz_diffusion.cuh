@@ -38,148 +38,204 @@ __device__ __forceinline__ double saturate(double f, double h, double Tl, double
   return f * qsat / (fabs(f) + qsat + SMALL_NUM);
 }
 
-// thcond_elec.pyx:154-303: face flux along AX on faces [lo, hi] of that axis,
-// cells 1..Ntot-2 on the other active axes.
+// thcond_elec.pyx:154-303: the conductive flux through the AX face of cell
+// (i, j, k) (the face between cells c - s and c), from T = p / rho.
 template <int AX>
-__global__ void k_flux(GridDev g, const double* __restrict__ w, const double* __restrict__ bf,
-                       const double* __restrict__ T, double* __restrict__ F, DiffArgs da, int3 lo, int3 hi) {
-  const int nxr = hi.x - lo.x + 1, nyr = hi.y - lo.y + 1, nzr = hi.z - lo.z + 1;
-  const long long n = (long long)nxr * nyr * nzr;
+__device__ __forceinline__ double face_flux(const GridDev& g, const double* __restrict__ w,
+                                            const double* __restrict__ bf, const double* __restrict__ T,
+                                            const DiffArgs& da, int i, int j, int k) {
   const long long sy = g.nx, sz = (long long)g.nx * g.ny, sv = g.sv;
   const double k0 = da.kappa0;
   const double kappah = (2. * k0 * k0 / (k0 + k0 + SMALL_NUM));
   const double* dvi0 = g.dlv_inv[0];
   const double* dvi1 = g.dlv_inv[1];
   const double* dvi2 = g.dlv_inv[2];
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    int i = lo.x + (int)(t % nxr);
-    long long r = t / nxr;
-    int j = lo.y + (int)(r % nyr), k = lo.z + (int)(r / nyr);
-    const long long c = c3(g, i, j, k);
-    const long long s = AX == 0 ? 1 : AX == 1 ? sy : sz;
-    double dTdx = 0., dTdy = 0., dTdz = 0., h = 0., f;
-    // neighbours: cell c (right of the face) and c - s (left)
-    if (AX == 0) dTdx = dvi0[i] * (T[c] - T[c - 1]);
-    if (AX == 1) dTdy = dvi1[j] * (T[c] - T[c - sy]);
-    if (AX == 2) dTdz = dvi2[k] * (T[c] - T[c - sz]);
-    if (da.aniso) {
-      double bxh, byh, bzh;
-      if (AX == 0) {
-        bxh = bf[c];
-        byh = 0.5 * (w[BY * sv + c - 1] + w[BY * sv + c]);
-        bzh = 0.5 * (w[BZ * sv + c - 1] + w[BZ * sv + c]);
-      } else if (AX == 1) {
-        byh = bf[sv + c];
-        bxh = 0.5 * (w[BX * sv + c - sy] + w[BX * sv + c]);
-        bzh = 0.5 * (w[BZ * sv + c - sy] + w[BZ * sv + c]);
-      } else {
-        bzh = bf[2 * sv + c];
-        bxh = 0.5 * (w[BX * sv + c - sz] + w[BX * sv + c]);
-        byh = 0.5 * (w[BY * sv + c - sz] + w[BY * sv + c]);
-      }
-      double bhi = 1. / sqrt(bxh * bxh + byh * byh + bzh * bzh + SMALL_NUM);
-      double bxh1 = bxh * bhi, byh1 = byh * bhi, bzh1 = bzh * bhi;
-      if (AX == 0) {
-        h = fabs(bxh1);
-        if (g.dims >= 2)  // tr_grad_lim_yx (syxv = 1 on Cartesian grids)
-          dTdy = dlim(dlim((T[c - 1] - T[c - 1 - sy]) * dvi1[j], (T[c - 1 + sy] - T[c - 1]) * dvi1[j + 1]) * 1.,
-                      dlim((T[c] - T[c - sy]) * dvi1[j], (T[c + sy] - T[c]) * dvi1[j + 1]) * 1.);
-        if (g.dims >= 3)  // tr_grad_lim_zx
-          dTdz = dlim(dlim((T[c - 1] - T[c - 1 - sz]) * dvi2[k], (T[c - 1 + sz] - T[c - 1]) * dvi2[k + 1]) * 1. * 1.,
-                      dlim((T[c] - T[c - sz]) * dvi2[k], (T[c + sz] - T[c]) * dvi2[k + 1]) * 1. * 1.);
-        f = -kappah * bxh1 * (bxh1 * dTdx + byh1 * dTdy + bzh1 * dTdz);
-      } else if (AX == 1) {
-        h = fabs(byh1);
-        // tr_grad_lim_xy
-        dTdx = dlim(dlim((T[c - sy] - T[c - sy - 1]) * dvi0[i], (T[c - sy + 1] - T[c - sy]) * dvi0[i + 1]),
-                    dlim((T[c] - T[c - 1]) * dvi0[i], (T[c + 1] - T[c]) * dvi0[i + 1]));
-        if (g.dims >= 3)  // tr_grad_lim_zy
-          dTdz = dlim(dlim((T[c - sy] - T[c - sy - sz]) * dvi2[k], (T[c - sy + sz] - T[c - sy]) * dvi2[k + 1]) * 1. * 1.,
-                      dlim((T[c] - T[c - sz]) * dvi2[k], (T[c + sz] - T[c]) * dvi2[k + 1]) * 1. * 1.);
-        f = -kappah * byh1 * (bxh1 * dTdx + byh1 * dTdy + bzh1 * dTdz);
-      } else {
-        h = fabs(bzh1);
-        // tr_grad_lim_xz, tr_grad_lim_yz
-        dTdx = dlim(dlim((T[c - sz] - T[c - sz - 1]) * dvi0[i], (T[c - sz + 1] - T[c - sz]) * dvi0[i + 1]),
-                    dlim((T[c] - T[c - 1]) * dvi0[i], (T[c + 1] - T[c]) * dvi0[i + 1]));
-        dTdy = dlim(dlim((T[c - sz] - T[c - sz - sy]) * dvi1[j], (T[c - sz + sy] - T[c - sz]) * dvi1[j + 1]) * 1.,
-                    dlim((T[c] - T[c - sy]) * dvi1[j], (T[c + sy] - T[c]) * dvi1[j + 1]) * 1.);
-        f = -kappah * bzh1 * (bxh1 * dTdx + byh1 * dTdy + bzh1 * dTdz);
-      }
+  const long long c = c3(g, i, j, k);
+  const long long s = AX == 0 ? 1 : AX == 1 ? sy : sz;
+  double dTdx = 0., dTdy = 0., dTdz = 0., h = 0., f;
+  // neighbours: cell c (right of the face) and c - s (left)
+  if (AX == 0) dTdx = dvi0[i] * (T[c] - T[c - 1]);
+  if (AX == 1) dTdy = dvi1[j] * (T[c] - T[c - sy]);
+  if (AX == 2) dTdz = dvi2[k] * (T[c] - T[c - sz]);
+  if (da.aniso) {
+    double bxh, byh, bzh;
+    if (AX == 0) {
+      bxh = bf[c];
+      byh = 0.5 * (w[BY * sv + c - 1] + w[BY * sv + c]);
+      bzh = 0.5 * (w[BZ * sv + c - 1] + w[BZ * sv + c]);
+    } else if (AX == 1) {
+      byh = bf[sv + c];
+      bxh = 0.5 * (w[BX * sv + c - sy] + w[BX * sv + c]);
+      bzh = 0.5 * (w[BZ * sv + c - sy] + w[BZ * sv + c]);
     } else {
-      if (AX == 0) {
-        if (g.dims >= 2)  // tr_grad_yx
-          dTdy = 0.25 * (((T[c - 1] - T[c - 1 - sy]) * dvi1[j] + (T[c - 1 + sy] - T[c - 1]) * dvi1[j + 1]) * 1. +
-                         ((T[c] - T[c - sy]) * dvi1[j] + (T[c + sy] - T[c]) * dvi1[j + 1]) * 1.);
-        if (g.dims >= 3)  // tr_grad_zx
-          dTdz = 0.25 * (((T[c - sy] - T[c - sy - sz]) * dvi2[k] + (T[c - sy + sz] - T[c - sy]) * dvi2[k + 1]) * 1. * 1. +
-                         ((T[c] - T[c - sz]) * dvi2[k] + (T[c + sz] - T[c]) * dvi2[k + 1]) * 1. * 1.);
-        double dTds = sqrt(dTdx * dTdx + dTdy * dTdy + dTdz * dTdz + SMALL_NUM);
-        h = fabs(dTdx / dTds);
-        f = -kappah * dTdx;
-      } else if (AX == 1) {
-        dTdx = 0.25 * (((T[c - sy] - T[c - sy - 1]) * dvi0[i] + (T[c - sy + 1] - T[c - sy]) * dvi0[i + 1]) +
-                       ((T[c] - T[c - 1]) * dvi0[i] + (T[c + 1] - T[c]) * dvi0[i + 1]));
-        if (g.dims >= 3)  // tr_grad_zy
-          dTdz = 0.25 * (((T[c - sy] - T[c - sy - sz]) * dvi2[k] + (T[c - sy + sz] - T[c - sy]) * dvi2[k + 1]) * 1. * 1. +
-                         ((T[c] - T[c - sz]) * dvi2[k] + (T[c + sz] - T[c]) * dvi2[k + 1]) * 1. * 1.);
-        double dTds = sqrt(dTdx * dTdx + dTdy * dTdy + dTdz * dTdz + SMALL_NUM);
-        h = fabs(dTdy / dTds);
-        f = -kappah * dTdy;
-      } else {
-        dTdx = 0.25 * (((T[c - sz] - T[c - sz - 1]) * dvi0[i] + (T[c - sz + 1] - T[c - sz]) * dvi0[i + 1]) +
-                       ((T[c] - T[c - 1]) * dvi0[i] + (T[c + 1] - T[c]) * dvi0[i + 1]));
-        dTdy = 0.25 * (((T[c - sz] - T[c - sz - sy]) * dvi1[j] + (T[c - sz + sy] - T[c - sz]) * dvi1[j + 1]) * 1. +
-                       ((T[c] - T[c - sy]) * dvi1[j] + (T[c + sy] - T[c]) * dvi1[j + 1]) * 1.);
-        double dTds = sqrt(dTdx * dTdx + dTdy * dTdy + dTdz * dTdz + SMALL_NUM);
-        h = fabs(dTdz / dTds);
-        f = -kappah * dTdz;
-      }
+      bzh = bf[2 * sv + c];
+      bxh = 0.5 * (w[BX * sv + c - sz] + w[BX * sv + c]);
+      byh = 0.5 * (w[BY * sv + c - sz] + w[BY * sv + c]);
     }
-    if (da.sat) f = saturate(f, h, T[c - s], T[c], w[RHO * sv + c - s], w[RHO * sv + c]);
-    F[c] = f;
+#if BNZ_FAST_MATH
+    // one reciprocal square root in place of a square root and a division
+    double bhi = rsqrt(bxh * bxh + byh * byh + bzh * bzh + SMALL_NUM);
+#else
+    double bhi = 1. / sqrt(bxh * bxh + byh * byh + bzh * bzh + SMALL_NUM);
+#endif
+    double bxh1 = bxh * bhi, byh1 = byh * bhi, bzh1 = bzh * bhi;
+    if (AX == 0) {
+      h = fabs(bxh1);
+      if (g.dims >= 2)  // tr_grad_lim_yx (syxv = 1 on Cartesian grids)
+        dTdy = dlim(dlim((T[c - 1] - T[c - 1 - sy]) * dvi1[j], (T[c - 1 + sy] - T[c - 1]) * dvi1[j + 1]) * 1.,
+                    dlim((T[c] - T[c - sy]) * dvi1[j], (T[c + sy] - T[c]) * dvi1[j + 1]) * 1.);
+      if (g.dims >= 3)  // tr_grad_lim_zx
+        dTdz = dlim(dlim((T[c - 1] - T[c - 1 - sz]) * dvi2[k], (T[c - 1 + sz] - T[c - 1]) * dvi2[k + 1]) * 1. * 1.,
+                    dlim((T[c] - T[c - sz]) * dvi2[k], (T[c + sz] - T[c]) * dvi2[k + 1]) * 1. * 1.);
+      f = -kappah * bxh1 * (bxh1 * dTdx + byh1 * dTdy + bzh1 * dTdz);
+    } else if (AX == 1) {
+      h = fabs(byh1);
+      // tr_grad_lim_xy
+      dTdx = dlim(dlim((T[c - sy] - T[c - sy - 1]) * dvi0[i], (T[c - sy + 1] - T[c - sy]) * dvi0[i + 1]),
+                  dlim((T[c] - T[c - 1]) * dvi0[i], (T[c + 1] - T[c]) * dvi0[i + 1]));
+      if (g.dims >= 3)  // tr_grad_lim_zy
+        dTdz = dlim(dlim((T[c - sy] - T[c - sy - sz]) * dvi2[k], (T[c - sy + sz] - T[c - sy]) * dvi2[k + 1]) * 1. * 1.,
+                    dlim((T[c] - T[c - sz]) * dvi2[k], (T[c + sz] - T[c]) * dvi2[k + 1]) * 1. * 1.);
+      f = -kappah * byh1 * (bxh1 * dTdx + byh1 * dTdy + bzh1 * dTdz);
+    } else {
+      h = fabs(bzh1);
+      // tr_grad_lim_xz, tr_grad_lim_yz
+      dTdx = dlim(dlim((T[c - sz] - T[c - sz - 1]) * dvi0[i], (T[c - sz + 1] - T[c - sz]) * dvi0[i + 1]),
+                  dlim((T[c] - T[c - 1]) * dvi0[i], (T[c + 1] - T[c]) * dvi0[i + 1]));
+      dTdy = dlim(dlim((T[c - sz] - T[c - sz - sy]) * dvi1[j], (T[c - sz + sy] - T[c - sz]) * dvi1[j + 1]) * 1.,
+                  dlim((T[c] - T[c - sy]) * dvi1[j], (T[c + sy] - T[c]) * dvi1[j + 1]) * 1.);
+      f = -kappah * bzh1 * (bxh1 * dTdx + byh1 * dTdy + bzh1 * dTdz);
+    }
+  } else {
+    if (AX == 0) {
+      if (g.dims >= 2)  // tr_grad_yx
+        dTdy = 0.25 * (((T[c - 1] - T[c - 1 - sy]) * dvi1[j] + (T[c - 1 + sy] - T[c - 1]) * dvi1[j + 1]) * 1. +
+                       ((T[c] - T[c - sy]) * dvi1[j] + (T[c + sy] - T[c]) * dvi1[j + 1]) * 1.);
+      if (g.dims >= 3)  // tr_grad_zx
+        dTdz = 0.25 * (((T[c - sy] - T[c - sy - sz]) * dvi2[k] + (T[c - sy + sz] - T[c - sy]) * dvi2[k + 1]) * 1. * 1. +
+                       ((T[c] - T[c - sz]) * dvi2[k] + (T[c + sz] - T[c]) * dvi2[k + 1]) * 1. * 1.);
+      double dTds = sqrt(dTdx * dTdx + dTdy * dTdy + dTdz * dTdz + SMALL_NUM);
+      h = fabs(dTdx / dTds);
+      f = -kappah * dTdx;
+    } else if (AX == 1) {
+      dTdx = 0.25 * (((T[c - sy] - T[c - sy - 1]) * dvi0[i] + (T[c - sy + 1] - T[c - sy]) * dvi0[i + 1]) +
+                     ((T[c] - T[c - 1]) * dvi0[i] + (T[c + 1] - T[c]) * dvi0[i + 1]));
+      if (g.dims >= 3)  // tr_grad_zy
+        dTdz = 0.25 * (((T[c - sy] - T[c - sy - sz]) * dvi2[k] + (T[c - sy + sz] - T[c - sy]) * dvi2[k + 1]) * 1. * 1. +
+                       ((T[c] - T[c - sz]) * dvi2[k] + (T[c + sz] - T[c]) * dvi2[k + 1]) * 1. * 1.);
+      double dTds = sqrt(dTdx * dTdx + dTdy * dTdy + dTdz * dTdz + SMALL_NUM);
+      h = fabs(dTdy / dTds);
+      f = -kappah * dTdy;
+    } else {
+      dTdx = 0.25 * (((T[c - sz] - T[c - sz - 1]) * dvi0[i] + (T[c - sz + 1] - T[c - sz]) * dvi0[i + 1]) +
+                     ((T[c] - T[c - 1]) * dvi0[i] + (T[c + 1] - T[c]) * dvi0[i + 1]));
+      dTdy = 0.25 * (((T[c - sz] - T[c - sz - sy]) * dvi1[j] + (T[c - sz + sy] - T[c - sz]) * dvi1[j + 1]) * 1. +
+                     ((T[c] - T[c - sy]) * dvi1[j] + (T[c + sy] - T[c]) * dvi1[j + 1]) * 1.);
+      double dTds = sqrt(dTdx * dTdx + dTdy * dTdy + dTdz * dTdz + SMALL_NUM);
+      h = fabs(dTdz / dTds);
+      f = -kappah * dTdz;
+    }
   }
+  if (da.sat) f = saturate(f, h, T[c - s], T[c], w[RHO * sv + c - s], w[RHO * sv + c]);
+  return f;
 }
 
-// thcond_elec.pyx:332-338
-__global__ void k_dtemp(GridDev g, const double* __restrict__ fx, const double* __restrict__ fy,
-                        const double* __restrict__ fz, double* __restrict__ dT, int3 lo, int3 hi) {
-  const int nxr = hi.x - lo.x + 1, nyr = hi.y - lo.y + 1, nzr = hi.z - lo.z + 1;
-  const long long n = (long long)nxr * nyr * nzr;
-  const long long sy = g.nx, sz = (long long)g.nx * g.ny;
-  const double gamm1 = g.gam - 1.;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    int i = lo.x + (int)(t % nxr);
-    long long r = t / nxr;
-    int j = lo.y + (int)(r % nyr), k = lo.z + (int)(r / nyr);
-    const long long c = c3(g, i, j, k);
-    double v = -(fx[c + 1] - fx[c]) * gamm1 * g.dlf_inv[0][i];
-    if (g.dims >= 2) v -= (fy[c + sy] - fy[c]) * gamm1 * g.dlf_inv[1][j];
-    if (g.dims >= 3) v -= (fz[c + sz] - fz[c]) * gamm1 * g.dlf_inv[2][k];
-    dT[c] = v;
-  }
-}
-
-// thcond_elec.pyx:75-94: (stage 1) save p0 and M(p0); RKL2 update of p.
-__global__ void k_sts_update(GridDev g, double* __restrict__ w, DiffArgs da, int3 lo, int3 hi, int first,
-                             double mu, double nu, double mut, double gamt, const double* dtp) {
+// One whole RKL2 stage per cell (thcond_elec.pyx:75-94 with the operator of
+// :118-338): the cell's six face fluxes from T (each interior face is formed
+// by both of its cells with the same expression, so both see one value), the
+// divergence M(p) = -(gamma-1) div q (thcond_elec.pyx:332-338) and the stage
+// update p = mu p + nu p_(j-2) + (1 - mu - nu) p0 + dt (mut M(p) + gamt M(p0)).
+// Only the cell's own p is read and written; the neighbours enter through T,
+// which k_temp formed before the launch, so the face fluxes never see a
+// pressure of this stage.  Stage 1 saves p0 and M(p0).  Per zone-stage this
+// moves p, p_(j-2), p0, M(p0), the cell field and the face field, and T.
+__global__ void k_stage(GridDev g, double* __restrict__ w, const double* __restrict__ bf,
+                        const double* __restrict__ T, DiffArgs da, int3 lo, int3 hi, int first, double mu, double nu,
+                        double mut, double gamt, const double* dtp) {
   const double dt = *dtp;
+  const double gamm1 = g.gam - 1.;
   const int nxr = hi.x - lo.x + 1, nyr = hi.y - lo.y + 1, nzr = hi.z - lo.z + 1;
   const long long n = (long long)nxr * nyr * nzr;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    int i = lo.x + (int)(t % nxr);
-    long long r = t / nxr;
-    int j = lo.y + (int)(r % nyr), k = lo.z + (int)(r / nyr);
+    const int i = lo.x + (int)(t % nxr);
+    const long long r = t / nxr;
+    const int j = lo.y + (int)(r % nyr), k = lo.z + (int)(r / nyr);
     const long long c = c3(g, i, j, k);
+    double v = -(face_flux<0>(g, w, bf, T, da, i + 1, j, k) - face_flux<0>(g, w, bf, T, da, i, j, k)) * gamm1 *
+               g.dlf_inv[0][i];
+    if (g.dims >= 2)
+      v -= (face_flux<1>(g, w, bf, T, da, i, j + 1, k) - face_flux<1>(g, w, bf, T, da, i, j, k)) * gamm1 *
+           g.dlf_inv[1][j];
+    if (g.dims >= 3)
+      v -= (face_flux<2>(g, w, bf, T, da, i, j, k + 1) - face_flux<2>(g, w, bf, T, da, i, j, k)) * gamm1 *
+           g.dlf_inv[2][k];
     double* pp = w + PR * g.sv + c;
     if (first) {
       da.pres0[c] = *pp;
-      da.dtemp0[c] = da.dtemp[c];
+      da.dtemp0[c] = v;
     }
-    double a = *pp;
-    *pp = (mu * a + nu * da.presm1[c] + (1. - mu - nu) * da.pres0[c] + dt * (mut * da.dtemp[c] + gamt * da.dtemp0[c]));
+    const double a = *pp;
+    *pp = (mu * a + nu * da.presm1[c] + (1. - mu - nu) * da.pres0[c] + dt * (mut * v + gamt * da.dtemp0[c]));
     da.presm1[c] = a;
   }
+}
+
+// The same stage on a tile of TXC x TYC x TZC cells per block: the tile's
+// face fluxes (each face once, the tile's far faces included) go to shared
+// memory, then every cell forms M(p) from its six faces and updates.  Face
+// values, divergence and update are the expressions of k_stage, so the two
+// kernels give the same bits; the tile forms 1 + 1/T of a flux per face
+// direction and cell instead of two.
+template <int TXC, int TYC, int TZC>
+__global__ void __launch_bounds__(TXC * TYC * TZC) k_stage_tile(GridDev g, double* __restrict__ w,
+                                                                 const double* __restrict__ bf,
+                                                                 const double* __restrict__ T, DiffArgs da, int3 lo,
+                                                                 int3 hi, int first, double mu, double nu, double mut,
+                                                                 double gamt, const double* dtp) {
+  constexpr int NX = (TXC + 1) * TYC * TZC, NY = TXC * (TYC + 1) * TZC, NZ = TXC * TYC * (TZC + 1);
+  __shared__ double sfx[NX], sfy[NY], sfz[NZ];
+  const int nbx = (hi.x - lo.x + TXC) / TXC, nby = (hi.y - lo.y + TYC) / TYC;
+  const int bx = blockIdx.x % nbx, by = (blockIdx.x / nbx) % nby, bz = blockIdx.x / (nbx * nby);
+  const int x0 = lo.x + bx * TXC, y0 = lo.y + by * TYC, z0 = lo.z + bz * TZC;
+  const int wx = min(TXC, hi.x - x0 + 1), wy = min(TYC, hi.y - y0 + 1), wz = min(TZC, hi.z - z0 + 1);
+  const int nfx = (wx + 1) * wy * wz, nfy = g.dims >= 2 ? wx * (wy + 1) * wz : 0,
+            nfz = g.dims >= 3 ? wx * wy * (wz + 1) : 0;
+  for (int t = threadIdx.x; t < nfx + nfy + nfz; t += blockDim.x) {
+    if (t < nfx) {
+      const int fi = t % (wx + 1), r = t / (wx + 1), fj = r % wy, fk = r / wy;
+      sfx[(fk * TYC + fj) * (TXC + 1) + fi] = face_flux<0>(g, w, bf, T, da, x0 + fi, y0 + fj, z0 + fk);
+    } else if (t < nfx + nfy) {
+      const int u = t - nfx;
+      const int fi = u % wx, r = u / wx, fj = r % (wy + 1), fk = r / (wy + 1);
+      sfy[(fk * (TYC + 1) + fj) * TXC + fi] = face_flux<1>(g, w, bf, T, da, x0 + fi, y0 + fj, z0 + fk);
+    } else {
+      const int u = t - nfx - nfy;
+      const int fi = u % wx, r = u / wx, fj = r % wy, fk = r / wy;
+      sfz[(fk * TYC + fj) * TXC + fi] = face_flux<2>(g, w, bf, T, da, x0 + fi, y0 + fj, z0 + fk);
+    }
+  }
+  __syncthreads();
+  const int ci = threadIdx.x % TXC, cj = (threadIdx.x / TXC) % TYC, ck = threadIdx.x / (TXC * TYC);
+  if (ci >= wx || cj >= wy || ck >= wz) return;
+  const int i = x0 + ci, j = y0 + cj, k = z0 + ck;
+  const double dt = *dtp;
+  const double gamm1 = g.gam - 1.;
+  const long long c = c3(g, i, j, k);
+  double v = -(sfx[(ck * TYC + cj) * (TXC + 1) + ci + 1] - sfx[(ck * TYC + cj) * (TXC + 1) + ci]) * gamm1 *
+             g.dlf_inv[0][i];
+  if (g.dims >= 2)
+    v -= (sfy[(ck * (TYC + 1) + cj + 1) * TXC + ci] - sfy[(ck * (TYC + 1) + cj) * TXC + ci]) * gamm1 *
+         g.dlf_inv[1][j];
+  if (g.dims >= 3)
+    v -= (sfz[((ck + 1) * TYC + cj) * TXC + ci] - sfz[(ck * TYC + cj) * TXC + ci]) * gamm1 * g.dlf_inv[2][k];
+  double* pp = w + PR * g.sv + c;
+  if (first) {
+    da.pres0[c] = *pp;
+    da.dtemp0[c] = v;
+  }
+  const double a = *pp;
+  *pp = (mu * a + nu * da.presm1[c] + (1. - mu - nu) * da.pres0[c] + dt * (mut * v + gamt * da.dtemp0[c]));
+  da.presm1[c] = a;
 }
 
 // thcond_elec.pyx:355-466: max over active cells of kappa0 (gamma-1)/rho sum 1/dx^2

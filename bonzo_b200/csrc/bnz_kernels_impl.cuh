@@ -312,44 +312,27 @@ int diff_dt_max(const StepArgs& a, const DiffArgs& d, unsigned long long* slot) 
   return 1;
 }
 
-// thcond_elec.pyx:118-338 (apply_diff_oper)
-int diff_operator(const StepArgs& a, const DiffArgs& d) {
+// One RKL2 stage (thcond_elec.pyx:75-94 with the operator of :118-338):
+// T = p / rho on every cell, then the fused flux / divergence / update pass on
+// cells 1..Ntot-2 of every active axis.
+int diff_stage(const StepArgs& a, const DiffArgs& d, int first, const double* coef, const double* dtp) {
   const GridDev& g = a.g;
   diff::k_temp<<<nblocks(g.sv, 256), 256, 0, a.stream>>>(g, a.prim, d.temp);
   int il = 1, iu = g.nx - 2;
   int jl = g.dims >= 2 ? 1 : 0, ju = g.dims >= 2 ? g.ny - 2 : 0;
   int kl = g.dims >= 3 ? 1 : 0, ku = g.dims >= 3 ? g.nz - 2 : 0;
-  {
-    int3 lo = make_int3(il, jl, kl), hi = make_int3(iu + 1, ju, ku);
-    long long n = (long long)(hi.x - lo.x + 1) * (hi.y - lo.y + 1) * (hi.z - lo.z + 1);
-    diff::k_flux<0><<<nblocks(n, 256), 256, 0, a.stream>>>(g, a.prim, a.bfld, d.temp, d.fx, d, lo, hi);
-  }
-  if (g.dims >= 2) {
-    int3 lo = make_int3(il, jl, kl), hi = make_int3(iu, ju + 1, ku);
-    long long n = (long long)(hi.x - lo.x + 1) * (hi.y - lo.y + 1) * (hi.z - lo.z + 1);
-    diff::k_flux<1><<<nblocks(n, 256), 256, 0, a.stream>>>(g, a.prim, a.bfld, d.temp, d.fy, d, lo, hi);
-  }
-  if (g.dims >= 3) {
-    int3 lo = make_int3(il, jl, kl), hi = make_int3(iu, ju, ku + 1);
-    long long n = (long long)(hi.x - lo.x + 1) * (hi.y - lo.y + 1) * (hi.z - lo.z + 1);
-    diff::k_flux<2><<<nblocks(n, 256), 256, 0, a.stream>>>(g, a.prim, a.bfld, d.temp, d.fz, d, lo, hi);
-  }
   int3 lo = make_int3(il, jl, kl), hi = make_int3(iu, ju, ku);
   long long n = (long long)(hi.x - lo.x + 1) * (hi.y - lo.y + 1) * (hi.z - lo.z + 1);
-  diff::k_dtemp<<<nblocks(n, 256), 256, 0, a.stream>>>(g, d.fx, d.fy, d.fz, d.dtemp, lo, hi);
-  return 2 + g.dims;
-}
-
-int diff_stage_update(const StepArgs& a, const DiffArgs& d, int first, const double* coef, const double* dtp) {
-  const GridDev& g = a.g;
-  int il = 1, iu = g.nx - 2;
-  int jl = g.dims >= 2 ? 1 : 0, ju = g.dims >= 2 ? g.ny - 2 : 0;
-  int kl = g.dims >= 3 ? 1 : 0, ku = g.dims >= 3 ? g.nz - 2 : 0;
-  int3 lo = make_int3(il, jl, kl), hi = make_int3(iu, ju, ku);
-  long long n = (long long)(hi.x - lo.x + 1) * (hi.y - lo.y + 1) * (hi.z - lo.z + 1);
-  diff::k_sts_update<<<nblocks(n, 256), 256, 0, a.stream>>>(g, a.prim, d, lo, hi, first, coef[0], coef[1], coef[2],
-                                                              coef[3], dtp);
-  return 1;
+  if (g.dims == 3) {
+    // tiles of 8 x 8 x 8 cells: every face flux formed once per tile
+    const int nb = ((hi.x - lo.x + 8) / 8) * ((hi.y - lo.y + 8) / 8) * ((hi.z - lo.z + 8) / 8);
+    diff::k_stage_tile<8, 8, 8><<<nb, 512, 0, a.stream>>>(g, a.prim, a.bfld, d.temp, d, lo, hi, first, coef[0],
+                                                          coef[1], coef[2], coef[3], dtp);
+  } else {
+    diff::k_stage<<<nblocks(n, 256), 256, 0, a.stream>>>(g, a.prim, a.bfld, d.temp, d, lo, hi, first, coef[0],
+                                                          coef[1], coef[2], coef[3], dtp);
+  }
+  return 2;
 }
 
 // --- fused 2D path (one launch per stage for the whole batch) --------------

@@ -17,8 +17,7 @@ struct Launchers {
   int (*set_dt)(cudaStream_t, DtState*, double);
   int (*time_advance)(cudaStream_t, DtState*);
   int (*diff_dt_max)(const StepArgs&, const DiffArgs&, unsigned long long* slot);
-  int (*diff_operator)(const StepArgs&, const DiffArgs&);
-  int (*diff_stage_update)(const StepArgs&, const DiffArgs&, int first, const double* coef, const double* dtp);
+  int (*diff_stage)(const StepArgs&, const DiffArgs&, int first, const double* coef, const double* dtp);
   int (*adj_step)(const FusedInst& I, const AdjStep& s);
   int (*source)(const StepArgs&, double* u1, const double* w0, int order, const double* dtp, double fac);
   int (*drive)(const StepArgs&, const DriveArgs&, const double* dtp);
@@ -43,8 +42,7 @@ struct Launchers {
   int set_dt(cudaStream_t, DtState*, double);                                                        \
   int time_advance(cudaStream_t, DtState*);                                                          \
   int diff_dt_max(const StepArgs&, const DiffArgs&, unsigned long long* slot);                      \
-  int diff_operator(const StepArgs&, const DiffArgs&);                                               \
-  int diff_stage_update(const StepArgs&, const DiffArgs&, int first, const double* coef, const double* dtp); \
+  int diff_stage(const StepArgs&, const DiffArgs&, int first, const double* coef, const double* dtp);  \
   int adj_step(const FusedInst& I, const AdjStep& s);                                                \
   int source(const StepArgs&, double* u1, const double* w0, int order, const double* dtp, double fac);  \
   int drive(const StepArgs&, const DriveArgs&, const double* dtp);                                    \
@@ -64,6 +62,6 @@ BNZ_DECLARE_LAUNCHERS(fast)
                                NS::fused_cds, NS::apply_bc,                                           \
                                NS::prim2cons_all, NS::cons2prim_all, NS::interp_bc_active,           \
                                NS::new_dt, NS::set_dt, NS::time_advance, NS::diff_dt_max,            \
-                               NS::diff_operator, NS::diff_stage_update, NS::adj_step, NS::source,    \
+                               NS::diff_stage, NS::adj_step, NS::source,    \
                                NS::drive, NS::riemann_rows, NS::fused3_step, NS::fused3_time,        \
                                NS::fused3_cds};
