@@ -254,6 +254,109 @@ def test_rollout_gradient_matches_central_differences_256():
     assert worst <= 1e-6, worst
 
 
+def _c3_setup(n, seed=3):
+    """The adjoint configuration's state at n^2: the periodic vortex plus a
+    seeded smooth perturbation (Fourier modes |k| <= 4, amplitude 1e-2) on v
+    and Az, a seeded smooth density target, the corner potential recovered
+    from the faces."""
+    import torch
+    from bonzo_b200 import problems as P
+    gc = P.make_grid(n, n, 1, dims=2, bc=0)
+    prim0, bfld0 = P.otvortex(gc, pert_amp=1e-2, seed=seed)
+    i1, i2, j1, j2 = gc.i1, gc.i2, gc.j1, gc.j2
+    v0 = torch.from_numpy(prim0[1:3, 0, j1:j2 + 1, i1:i2 + 1].copy()).cuda()
+    dx, dy = gc.dlf[0][i1], gc.dlf[1][j1]
+    sb = math.sqrt(4 * math.pi)
+    bx = bfld0[0, 0, j1:j2 + 1, i1:i2 + 2]
+    by = bfld0[1, 0, j1:j2 + 2, i1:i2 + 1]
+    az = np.zeros((n + 1, n + 1))
+    az[0, 1:] = -np.cumsum(by[0, :]) * dx * sb
+    az[1:, :] = az[0:1, :] + np.cumsum(bx, axis=0) * dy * sb
+    x = gc.lv[0][i1:i2 + 1]
+    y = gc.lv[1][j1:j2 + 1]
+    X, Y = np.meshgrid(x, y)
+    target = torch.from_numpy((5. / 3) ** 2 * (1 + 0.05 * np.sin(2 * math.pi * X) * np.cos(4 * math.pi * Y))).cuda()
+    return gc, v0, torch.from_numpy(az).cuda(), target
+
+
+def test_rollout_adjoint_64_matches_torch_autograd():
+    """The adjoint configuration at 64 x 64 as it is worded: 100 steps of
+    dt = 1e-4 (VL2 + PLM(mc) + HLLD + CT), checkpoint every 10 steps, loss =
+    squared misfit of the final density; the gradient with respect to the
+    initial velocity and Az from the device adjoint against torch autograd
+    through the FP64 torch transcription of the step."""
+    import torch
+    import torch_vl2 as T
+    from bonzo_b200.adjoint import rollout
+    n, nsteps, dt = 64, 100, 1e-4
+    gc, v0, az0, target = _c3_setup(n)
+    i1, i2, j1, j2 = gc.i1, gc.i2, gc.j1, gc.j2
+    opts = dict(Nx=n, Ny=n, Nz=1, dims=2, bc=((0, 0), (0, 0), (0, 0)), gam=5. / 3, cour=0.4,
+                rsolver="hlld", limiter="mc", path="fused")
+    eng = device_ctx(opts)
+    v = v0.clone().requires_grad_(True)
+    a = az0.clone().requires_grad_(True)
+    p, b = _vortex_ic(gc, v, a)
+    xp, _ = rollout(p, b, eng, nsteps, dt, checkpoint_every=10)
+    L = ((xp[0, 0, j1:j2 + 1, i1:i2 + 1] - target) ** 2).sum()
+    L.backward()
+    G = T.Grid(gc, face_aware=True, device="cuda")
+    vt = v0.clone().requires_grad_(True)
+    at = az0.clone().requires_grad_(True)
+    pt, bt = _vortex_ic(gc, vt, at)
+    xx, yy = pt[:, 0], bt[:, 0]
+    for _ in range(nsteps):
+        xx, yy = T.step(G, xx, yy, dt, rs="hlld", lim="mc")
+    Lt = ((xx[0, j1:j2 + 1, i1:i2 + 1] - target) ** 2).sum()
+    Lt.backward()
+    assert abs(float(L.detach()) - float(Lt.detach())) <= 1e-12 * abs(float(Lt.detach()))
+    assert _rel(v.grad, vt.grad) < 1e-9, _rel(v.grad, vt.grad)
+    assert _rel(a.grad, at.grad) < 1e-9, _rel(a.grad, at.grad)
+
+
+@pytest.mark.parametrize("nsteps", [1, 3])
+def test_adjoint_dot_product(nsteps):
+    """<J v, w> = <v, J^T w> for the map of nsteps steps at a perturbed vortex
+    state: J v by forward-mode differentiation of the torch transcription
+    (torch.func.jvp), J^T w by the device's hand-written reverse pass -- two
+    independent derivative implementations."""
+    import torch
+    import torch_vl2 as T
+    gc, opts, m, P0, B0, dt = _state("vortex_pert", 48, limiter="mc")
+    G = T.Grid(gc, face_aware=True, device="cuda")
+    gen = torch.Generator(device="cpu").manual_seed(11)
+    a = (slice(None),) + tuple(gc.active[1:])
+    vp = torch.zeros(P0.shape, dtype=torch.float64)
+    vb = torch.zeros(B0.shape, dtype=torch.float64)
+    vp[a] = torch.randn(vp[a].shape, generator=gen, dtype=torch.float64)
+    vb[a] = torch.randn(vb[a].shape, generator=gen, dtype=torch.float64)
+    vp, vb = vp.cuda(), vb.cuda()
+
+    def f(p, b):
+        for _ in range(nsteps):
+            p, b = T.step(G, p, b, dt, rs="hlld", lim="mc")
+        return p, b
+
+    out, (jp, jb) = torch.func.jvp(f, (P0.cuda(), B0.cuda()), (vp, vb))
+    wp = torch.randn(out[0].shape, generator=gen, dtype=torch.float64).cuda()
+    wb = torch.randn(out[1].shape, generator=gen, dtype=torch.float64).cuda()
+    lhs = float((jp * wp).sum() + (jb * wb).sum())
+    # J^T w on the device: the rollout adjoint (tape of every step)
+    eng = device_ctx(opts, path="fused", **m)
+    eng.set_stream(torch.cuda.current_stream().cuda_stream)
+    shp = (1,) + tuple(P0.shape[1:])
+    P = P0.reshape((9,) + shp).cuda().contiguous()
+    B = B0.reshape((3,) + shp).cuda().contiguous()
+    eng.set_state_device(P.data_ptr(), B.data_ptr())
+    eng.rollout_forward(nsteps, dt, 1)
+    gp4, gb4 = wp.reshape(P.shape).contiguous(), wb.reshape(B.shape).contiguous()
+    op, ob = torch.empty_like(P), torch.empty_like(B)
+    eng.rollout_adjoint(gp4.data_ptr(), gb4.data_ptr(), op.data_ptr(), ob.data_ptr())
+    torch.cuda.synchronize()
+    rhs = float((vp * op[:, 0]).sum() + (vb * ob[:, 0]).sum())
+    assert abs(lhs - rhs) <= 1e-10 * abs(lhs), (lhs, rhs)
+
+
 def test_adjoint_rejects_turbulence_driving():
     """The driving force is a random field advanced every step that the tape
     does not keep: the adjoint refuses it on the host, before any launch."""
