@@ -64,6 +64,11 @@ def parse():
     ap.add_argument("--adjoint-only", action="store_true", help="print only the adjoint/forward measurement")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the 3D configurations (256^3 turbulence, 384^3 conduction; about a minute of set-up)")
+    ap.add_argument("--configs-only", action="store_true",
+                    help="print only the 3D configurations (no 2D batch, adjoint or CPU baseline)")
+    ap.add_argument("--n3d", type=int, default=0,
+                    help="side of the 3D configurations' grids instead of 256 / 384 (batch: half of it); small "
+                         "cases for profiling")
     return ap.parse_args()
 
 
@@ -497,7 +502,7 @@ def _time_ctx(c, steps, graph, stream, clk=None):
     return e0.elapsed_time(e1) / steps, nsts / steps
 
 
-def run_configs(fused_steps=6, plain_steps=2):
+def run_configs(fused_steps=6, plain_steps=2, n3d=0):
     """The 3D configurations on seeded synthetic initial states, on the fused
     z-marching path and on the plain one-launch-per-loop path:
     256^3 decaying turbulence (rms Mach 1, beta 1, VL2+PLM(vl)+HLLD+CT, CFL 0.3)
@@ -514,9 +519,10 @@ def run_configs(fused_steps=6, plain_steps=2):
     out = {}
     stream = torch.cuda.Stream()
     dev = torch.cuda.current_device()
+    nt, nc = (n3d, n3d) if n3d else (256, 384)
     for name, n, kw, gen, graph in (
-            ("turbulence_256^3", 256, dict(cour=0.3), lambda gc: P.turbulence3d(gc, seed=0), True),
-            ("conduction_384^3", 384, dict(cour=0.4, kappa0=0.01, thcond_type="aniso"),
+            ("turbulence_%d^3" % nt, nt, dict(cour=0.3), lambda gc: P.turbulence3d(gc, seed=0), True),
+            ("conduction_%d^3" % nc, nc, dict(cour=0.4, kappa0=0.01, thcond_type="aniso"),
              lambda gc: P.conduction3d(gc, seed=0), False)):
         gc = P.make_grid(n, n, n, dims=3, bc=0)
         prim, bfld = gen(gc)
@@ -547,7 +553,8 @@ def run_configs(fused_steps=6, plain_steps=2):
                            (n, name.split("_")[0], ", RKL2 conduction kappa_par 0.01" if kw.get("kappa0") else ""))
         out[name] = rec
         del prim, bfld
-    out["conduction_batch_4x192^3"] = run_batch3d(stream, dev, peak, peak_src, fused_steps)
+    nb = n3d // 2 if n3d else 192
+    out["conduction_batch_4x%d^3" % nb] = run_batch3d(stream, dev, peak, peak_src, fused_steps, n=nb)
     return out
 
 
@@ -645,6 +652,12 @@ def main():
                                                                           "sample")}
         print(json.dumps(line), flush=True)
         return 0
+    if args.configs_only:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "configs_3d": run_configs(n3d=args.n3d)}), flush=True)
+        return 0
     if args.adjoint_only:
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
@@ -663,7 +676,7 @@ def main():
     if rank == 0 and not args.no_adjoint:
         line["adjoint"] = run_adjoint()
     if rank == 0 and world == 1 and not args.no_configs:
-        line["configs_3d"] = run_configs()
+        line["configs_3d"] = run_configs(n3d=args.n3d)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         batch = build_batch(args.instances, args.seed)
         cb = run_cpu_reference(batch, steps=2, warmup=1)
