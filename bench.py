@@ -504,7 +504,8 @@ def _time_ctx(c, steps, graph, stream, clk=None):
 
 def run_configs(fused_steps=6, plain_steps=2, n3d=0):
     """The 3D configurations on seeded synthetic initial states, on the fused
-    z-marching path and on the plain one-launch-per-loop path:
+    z-marching path, the split path (fluxes once per face, fused update) and
+    the plain one-launch-per-loop path:
     256^3 decaying turbulence (rms Mach 1, beta 1, VL2+PLM(vl)+HLLD+CT, CFL 0.3)
     and 384^3 field-aligned conduction (kappa_par 0.01, RKL2 super-time-stepping
     interleaved with VL2+HLLD+CT).  Each path: two warm-up steps, then timed
@@ -527,7 +528,7 @@ def run_configs(fused_steps=6, plain_steps=2, n3d=0):
         gc = P.make_grid(n, n, n, dims=3, bc=0)
         prim, bfld = gen(gc)
         rec = {}
-        for path, steps in (("fused", fused_steps), ("plain", plain_steps)):
+        for path, steps in (("fused", fused_steps), ("split", fused_steps), ("plain", plain_steps)):
             c = Context(Nx=n, Ny=n, Nz=n, dims=3, bc=((0, 0), (0, 0), (0, 0)), gam=5. / 3, rsolver="hlld",
                         limiter="vl", path=path, **kw)
             c.set_stream(stream.cuda_stream)
@@ -549,6 +550,7 @@ def run_configs(fused_steps=6, plain_steps=2, n3d=0):
             c.close()
             torch.cuda.empty_cache()
         rec["fused_vs_plain"] = round(rec["plain"]["ms_per_step"] / rec["fused"]["ms_per_step"], 3)
+        rec["split_vs_plain"] = round(rec["plain"]["ms_per_step"] / rec["split"]["ms_per_step"], 3)
         rec["workload"] = ("%d^3 periodic, seeded synthetic %s, VL2+PLM(vl)+HLLD+CT%s" %
                            (n, name.split("_")[0], ", RKL2 conduction kappa_par 0.01" if kw.get("kappa0") else ""))
         out[name] = rec

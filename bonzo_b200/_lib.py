@@ -19,7 +19,7 @@ RS = {"hll": 0, "hllc": 1, "hlld": 2, "hllt": 3}
 RCN = {"const": 0, "linear": 1}
 LIM = {"vl": 0, "mc": 1, "mm": 2}
 TC = {"iso": 0, "aniso": 1}
-PATH = {"fused": 0, "plain": 1}
+PATH = {"fused": 0, "plain": 1, "split": 2}
 
 # every entry point include/bnz_gpu.h declares (checked by the CPU tests)
 EXPORTS = [

@@ -481,7 +481,8 @@ int validate(const bnz_grid_desc* g, const bnz_method_desc* m, std::string& why)
   }
   if (m->kappa0 < 0.) return why = "kappa0 must be >= 0", 0;
   if (m->kappa0 > 0. && !(m->cour_diff > 0.)) return why = "cour_diff must be positive", 0;
-  if (m->path != BNZ_PATH_FUSED && m->path != BNZ_PATH_PLAIN) return why = "path must be fused or plain", 0;
+  if (m->path != BNZ_PATH_FUSED && m->path != BNZ_PATH_PLAIN && m->path != BNZ_PATH_SPLIT)
+    return why = "path must be fused, plain or split", 0;
   if (m->path == BNZ_PATH_FUSED && !fused_available(g, m)) return why = "fused path not available for this grid", 0;
   int ng = m->reconstr == BNZ_RCN_CONST ? 2 : 3;
   int N[3] = {g->Nx, g->Ny, g->Nz};
@@ -601,7 +602,8 @@ int bnz_create(const bnz_grid_desc* gd, const bnz_method_desc* md, bnz_ctx** out
   ALLOC(c->prim, n9);
   ALLOC(c->cons, n9);
   ALLOC(c->bfld, n3);
-  if (md->path == BNZ_PATH_PLAIN) {
+  if (md->path != BNZ_PATH_FUSED) {
+    // plain and split paths; the split path keeps the step's b^n in ec
     ALLOC(c->cons_s, n9);
     ALLOC(c->bfld_s, n3);
     for (int d = 0; d < dims; ++d) ALLOC(c->flx[d], n9);
@@ -873,6 +875,8 @@ int step_impl(bnz_ctx* c, double dt_host, int dt_mode) {
   const double* dtp = &c->d_ds->dt;
   if (c->md.path == BNZ_PATH_PLAIN) {
     c->launches += c->L->plain_predictor_corrector(a, dtp);
+  } else if (c->md.path == BNZ_PATH_SPLIT) {
+    c->launches += c->L->split_predictor_corrector(a, dtp);
   } else {
     if (c->gd.dims == 3) c->launches += c->L->fused3_step(fused3_launch(c, dt_mode), c->parity);
     else c->launches += c->L->fused_step(fused_launch(c, dt_mode), c->parity);
@@ -889,7 +893,7 @@ int step_impl(bnz_ctx* c, double dt_host, int dt_mode) {
       if (rc) return rc;
     }
   }
-  if (c->md.path == BNZ_PATH_PLAIN) {
+  if (c->md.path != BNZ_PATH_FUSED) {
     c->launches += c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
     c->launches += c->L->prim2cons_all(a);
   }

@@ -1,0 +1,300 @@
+// bnz_split.cuh -- the split path: one launch per face direction, each face's
+// flux formed once, then one fused update per stage.
+//
+// Where the plain path (bnz_plain.cuh) follows the reference loop by loop, the
+// split path keeps its decomposition (fluxes and edge EMFs through HBM) and
+// removes its costs:
+//   * k_flux_tile: a block stages a pencil tile of cells (NB lines of NA faces
+//     along the sweep axis, with the two-cell halo) in shared memory and forms
+//     every cell's PLM half slopes once (reconstr_c.c:54-91), where
+//     plain::k_flux forms both one-sided slopes of every face itself;
+//   * k_ee forms the cell-centred EMF (ct.pyx:128-148) of the cells it needs
+//     on the fly instead of reading a separate array;
+//   * k_update: per cell, the conservative update (godunov.pyx:215-252), the
+//     face update (ct.pyx:15-91), face-to-cell B (ct.pyx:96-123), the source
+//     terms (integrator.pyx:132-170) and cons2prim (eos.pyx:13-44) in one
+//     pass, where the plain path runs up to eight launches.
+// A face is formed by exactly one block and no kernel waits on a barrier
+// between Riemann solves (what bounds the z-marching chunk kernels).  Every
+// expression is the plain path's, so the exact build is bitwise equal to it
+// and to the oracle.  Included inside the per-floating-point-mode namespace,
+// after bnz_plain.cuh and bnz_source.cuh.
+#pragma once
+
+namespace split {
+
+using namespace dev;
+
+// slope slot of variable n (the normal field has none)
+__device__ __forceinline__ constexpr int slot8(int n) { return n < BX ? n : n - 1; }
+
+// Pencil tiles of the flux kernel of axis AX: NA faces along AX on each of NB
+// lines along the transverse axis TAX (y for the x sweep, x for the y and z
+// sweeps, so that a warp's loads and stores run along x); OAX is the axis the
+// block index walks one line at a time.  (NA + 1) NB = 256 threads: one slope
+// cell per thread.  Shared arrays are laid out with x fastest, which keeps a
+// warp's accesses on distinct banks.
+template <int AX>
+struct FT {
+  static constexpr int NA = AX == 0 ? 31 : 15;
+  static constexpr int NB = AX == 0 ? 8 : 16;
+  static constexpr int TAX = AX == 0 ? 1 : 0;
+  static constexpr int OAX = AX == 2 ? 1 : 2;
+  static constexpr int NS = NA + 3;             // staged cells along AX
+  static constexpr int NT = (NA + 1) * NB;
+  static constexpr int DA = AX == 0 ? 1 : NB;   // stride along AX (staged cells and slopes)
+  static constexpr int WN = NB * NS;            // stride between staged fields
+  __device__ static constexpr int ws(int n, int sa, int lb) {  // staged cell sa of line lb
+    return AX == 0 ? (n * NB + lb) * NS + sa : (n * NS + sa) * NB + lb;
+  }
+  __device__ static constexpr int ds(int s, int la, int lb) {  // slope of cell la of line lb
+    return AX == 0 ? (s * NB + lb) * (NA + 1) + la : (s * (NA + 1) + la) * NB + lb;
+  }
+  static_assert(NT == 256, "one slope cell per thread");
+};
+
+__device__ __forceinline__ int ax_of(int3 v, int a) { return a == 0 ? v.x : a == 1 ? v.y : v.z; }
+
+// Fluxes of the AX faces of `box` (face index along AX = the cell on its
+// right), in the global variable order as plain::k_flux stores them (the
+// normal field entry, which nothing reads, is not stored).  ORDER 0: donor
+// cell (reconstr_c.c:8-22); ORDER 1: PLM with limiter lim (reconstr_c.c:29-91),
+// in characteristic variables when cp.  Normal field from the face array.
+template <int AX, int ORDER, int RS>
+__global__ void __launch_bounds__(256, 2) k_flux_tile(GridDev g, const double* __restrict__ w,
+                                                      const double* __restrict__ bf, double* __restrict__ F,
+                                                      plain::Box box, int lim, int cp, unsigned* err) {
+  using T = FT<AX>;
+  constexpr int NA = T::NA, NB = T::NB, NS = T::NS, DA = T::DA, WN = T::WN;
+  __shared__ double sW[NM * WN];
+  __shared__ double sD[ORDER ? 8 * NB * (NA + 1) : 1];
+  const int lo_a = ax_of(box.lo, AX), hi_a = ax_of(box.hi, AX);
+  const int lo_b = ax_of(box.lo, T::TAX), hi_b = ax_of(box.hi, T::TAX);
+  const int na = (hi_a - lo_a + NA) / NA, nb = (hi_b - lo_b + NB) / NB;
+  const int ta = blockIdx.x % na, tb = (blockIdx.x / na) % nb, to = blockIdx.x / (na * nb);
+  const int a0 = lo_a + ta * NA, b0 = lo_b + tb * NB, o = ax_of(box.lo, T::OAX) + to;
+  const long long st[3] = {1, (long long)g.nx, (long long)g.nx * g.ny};
+  const int N[3] = {g.nx, g.ny, g.nz};
+  const long long sa = st[AX], sb = st[T::TAX], so = st[T::OAX];
+  // stage cells a0-2 .. a0+NA of the NB lines, in the sweep frame's variable
+  // order; cells outside the array are neither loaded nor used
+  for (int t = threadIdx.x; t < NS * NB; t += T::NT) {
+    const int ia = AX == 0 ? t % NS : t / NB;
+    const int ib = AX == 0 ? t / NS : t % NB;
+    const int a = a0 - 2 + ia, b = b0 + ib;
+    if (a < 0 || a >= N[AX] || b > hi_b) continue;
+    const long long c = a * sa + b * sb + o * so;
+#pragma unroll
+    for (int n = 0; n < NM; ++n) sW[T::ws(n, ia, ib)] = w[plain::perm<AX>(n) * g.sv + c];
+  }
+  __syncthreads();
+  const int la = AX == 0 ? threadIdx.x % (NA + 1) : threadIdx.x / NB;
+  const int lb = AX == 0 ? threadIdx.x / (NA + 1) : threadIdx.x % NB;
+  if (ORDER == 1) {
+    // the half slope of cell a0-1+la (staged index la+1), once per cell
+    const int a = a0 - 1 + la;
+    if (a >= 1 && a + 1 < N[AX] && a <= hi_a && b0 + lb <= hi_b) {
+      const double* p = sW + T::ws(0, la + 1, lb);
+      if (cp) {
+        double wm[NM], wc[NM], wp[NM], d[NM];
+#pragma unroll
+        for (int n = 0; n < NM; ++n) {
+          wm[n] = p[n * WN - DA];
+          wc[n] = p[n * WN];
+          wp[n] = p[n * WN + DA];
+        }
+        plain::half_slopes_char_rt(lim, wm, wc, wp, g.gam, d);
+#pragma unroll
+        for (int n = 0; n < NM; ++n)
+          if (n != BX) sD[T::ds(slot8(n), la, lb)] = d[n];
+      } else {
+#pragma unroll
+        for (int n = 0; n < NM; ++n) {
+          if (n == BX) continue;
+          sD[T::ds(slot8(n), la, lb)] = plain::half_slope_rt(lim, p[n * WN - DA], p[n * WN], p[n * WN + DA]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // the face a0+la between cells a0+la-1 and a0+la (threads la == NA have none)
+  const int f = a0 + la, b = b0 + lb;
+  if (la >= NA || f > hi_a || b > hi_b) return;
+  const long long c = f * sa + b * sb + o * so;
+  const double* p = sW + T::ws(0, la + 2, lb);  // staged cell f
+  double wL[NM], wR[NM];
+#pragma unroll
+  for (int n = 0; n < NM; ++n) {
+    if (n == BX) continue;
+    if (ORDER == 0) {
+      wL[n] = p[n * WN - DA];
+      wR[n] = p[n * WN];
+    } else {
+      wL[n] = p[n * WN - DA] + sD[T::ds(slot8(n), la, lb)];
+      wR[n] = p[n * WN] - sD[T::ds(slot8(n), la + 1, lb)];
+    }
+  }
+  const double bx = bf[AX * g.sv + c];
+  wL[BX] = bx;
+  wR[BX] = bx;
+  unsigned e = 0;
+  double fl[NM];
+  riemann<RS>(fl, wL, wR, g.gam, e);
+#pragma unroll
+  for (int n = 0; n < NM; ++n)
+    if (n != BX) F[plain::perm<AX>(n) * g.sv + c] = fl[n];
+  if (e) atomicOr(err, e);
+}
+
+// ct.pyx:128-148: component COMP of the cell-centred EMF -(v x B) of cell c
+template <int COMP>
+__device__ __forceinline__ double ec_at(const double* __restrict__ w, long long sv, long long c) {
+  const double* q = w + c;
+  if (COMP == 0) return -(q[VY * sv] * q[BZ * sv] - q[VZ * sv] * q[BY * sv]);
+  if (COMP == 1) return (q[VX * sv] * q[BZ * sv] - q[VZ * sv] * q[BX * sv]);
+  return -(q[VX * sv] * q[BY * sv] - q[VY * sv] * q[BX * sv]);
+}
+
+// ct.pyx:153-215 (interp_ee1): plain::k_ee with the cell EMFs formed from w
+__global__ void k_ee(GridDev g, const double* __restrict__ w, const double* __restrict__ fx,
+                     const double* __restrict__ fy, const double* __restrict__ fz, double* __restrict__ ee,
+                     plain::Box box) {
+  const long long sv = g.sv, sy = g.nx, sz = (long long)g.nx * g.ny;
+  BOX_LOOP(box, i, j, k) {
+    const long long c = plain::cidx(g, i, j, k);
+    if (g.dims == 3) {
+      ee[c] = (0.5 * (-fy[BZ * sv + c - sz] - fy[BZ * sv + c] + fz[BY * sv + c - sy] + fz[BY * sv + c]) -
+               0.25 * (ec_at<0>(w, sv, c - sy) + ec_at<0>(w, sv, c) + ec_at<0>(w, sv, c - sz - sy) +
+                       ec_at<0>(w, sv, c - sz)));
+      ee[sv + c] = (0.5 * (-fz[BX * sv + c - 1] - fz[BX * sv + c] + fx[BZ * sv + c - sz] + fx[BZ * sv + c]) -
+                    0.25 * (ec_at<1>(w, sv, c - 1) + ec_at<1>(w, sv, c) + ec_at<1>(w, sv, c - sz - 1) +
+                            ec_at<1>(w, sv, c - sz)));
+      ee[2 * sv + c] = (0.5 * (-fx[BY * sv + c - sy] - fx[BY * sv + c] + fy[BX * sv + c - 1] + fy[BX * sv + c]) -
+                        0.25 * (ec_at<2>(w, sv, c - 1) + ec_at<2>(w, sv, c) + ec_at<2>(w, sv, c - sy - 1) +
+                                ec_at<2>(w, sv, c - sy)));
+    } else if (g.dims == 2) {
+      ee[c] = -fy[BZ * sv + c];
+      ee[sv + c] = fx[BZ * sv + c];
+      ee[2 * sv + c] = (0.5 * (-fx[BY * sv + c - sy] - fx[BY * sv + c] + fy[BX * sv + c - 1] + fy[BX * sv + c]) -
+                        0.25 * (ec_at<2>(w, sv, c - 1) + ec_at<2>(w, sv, c) + ec_at<2>(w, sv, c - sy - 1) +
+                                ec_at<2>(w, sv, c - sy)));
+    } else {
+      ee[c] = -ec_at<0>(w, sv, c);
+      ee[sv + c] = fx[BZ * sv + c];
+      ee[2 * sv + c] = -fx[BY * sv + c];
+    }
+  }
+}
+
+// One stage's update of the cells of `box` (the stage's update range): the
+// plain path's k_advance_hydro, k_advance_b (the cell's lower faces, and its
+// upper ones on the range's last cells), k_interp_bc, k_source and
+// k_cons2prim, with the same expressions.  u1 may be u0 and w1 may be w0: a
+// thread reads and writes only its own cell of them.  b0 must not be b1 (a
+// cell reads its upper faces' old values, which the neighbour updates); bsave,
+// when not null, receives the b0 faces the update reads (the step's b^n, for
+// the corrector).
+__global__ void __launch_bounds__(256) k_update(GridDev g, double* u1, const double* u0, double* w1,
+                                                const double* w0, double* __restrict__ b1,
+                                                const double* __restrict__ b0, double* __restrict__ bsave,
+                                                const double* __restrict__ fx, const double* __restrict__ fy,
+                                                const double* __restrict__ fz, const double* __restrict__ ee,
+                                                plain::Box box, const double* dtp, double fac, int src,
+                                                double gx, double gy, double gz, const double* __restrict__ fdriv,
+                                                unsigned* err) {
+  const double dt = fac * *dtp;
+  const long long sv = g.sv, sy = g.nx, sz = (long long)g.nx * g.ny;
+  const double gv[3] = {gx, gy, gz};
+  const bool grav = gx != 0. || gy != 0. || gz != 0.;
+  unsigned e = 0;
+  BOX_LOOP(box, i, j, k) {
+    const long long c = plain::cidx(g, i, j, k);
+    // godunov.pyx:215-252
+    const double vol = g.dlf[0][i] * g.dlf[1][j] * g.dlf[2][k];
+    const double dtdv = dt / vol;
+    const double dax = g.dlf[1][j] * g.dlf[2][k];
+    const double day = g.dlf[0][i] * g.dlf[2][k];
+    const double daz = g.dlf[0][i] * g.dlf[1][j];
+    double u[NM];
+#pragma unroll
+    for (int n = 0; n < BX; ++n) {
+      const long long q = n * sv + c;
+      double v = u0[q] - dtdv * (dax * fx[q + 1] - dax * fx[q]);
+      if (g.dims >= 2) v -= dtdv * (day * fy[q + sy] - day * fy[q]);
+      if (g.dims >= 3) v -= dtdv * (daz * fz[q + sz] - daz * fz[q]);
+      u[n] = v;
+    }
+    // ct.pyx:15-91 on the cell's faces; a face's expressions depend only on
+    // its transverse indices, so the upper face is the lower one shifted
+    const double dsx = g.dlf[0][i], dsy = g.dlf[1][j], dsz = g.dlf[2][k];
+    auto bxf = [&](long long q) {
+      const double dtda = dt / (dsy * dsz);
+      double v = b0[q];
+      if (g.dims >= 2) v -= dtda * (dsz * ee[2 * sv + q + sy] - dsz * ee[2 * sv + q]);
+      if (g.dims >= 3) v += dtda * (dsy * ee[sv + q + sz] - dsy * ee[sv + q]);
+      return v;
+    };
+    auto byf = [&](long long q) {
+      const double dtda = dt / (dsx * dsz);
+      double v = b0[sv + q] + dtda * (dsz * ee[2 * sv + q + 1] - dsz * ee[2 * sv + q]);
+      if (g.dims >= 3) v -= dtda * (dsx * ee[q + sz] - dsx * ee[q]);
+      return v;
+    };
+    auto bzf = [&](long long q) {
+      const double dtda = dt / (dsx * dsy);
+      double v = b0[2 * sv + q] - dtda * (dsy * ee[sv + q + 1] - dsy * ee[sv + q]);
+      if (g.dims >= 2) v += dtda * (dsx * ee[q + sy] - dsx * ee[q]);
+      return v;
+    };
+    const double bxl = bxf(c), byl = byf(c), bzl = bzf(c), bxr = bxf(c + 1);
+    const double byr = g.dims >= 2 ? byf(c + sy) : 0.;
+    const double bzr = g.dims >= 3 ? bzf(c + sz) : 0.;
+    b1[c] = bxl;
+    b1[sv + c] = byl;
+    b1[2 * sv + c] = bzl;
+    const bool ux = i == box.hi.x, uy = g.dims >= 2 && j == box.hi.y, uz = g.dims >= 3 && k == box.hi.z;
+    if (ux) b1[c + 1] = bxr;
+    if (uy) b1[sv + c + sy] = byr;
+    if (uz) b1[2 * sv + c + sz] = bzr;
+    if (bsave) {
+      bsave[c] = b0[c];
+      bsave[sv + c] = b0[sv + c];
+      bsave[2 * sv + c] = b0[2 * sv + c];
+      if (ux) bsave[c + 1] = b0[c + 1];
+      if (uy) bsave[sv + c + sy] = b0[sv + c + sy];
+      if (uz) bsave[2 * sv + c + sz] = b0[2 * sv + c + sz];
+    }
+    // ct.pyx:96-123
+    u[BX] = ((g.lv[0][i] - g.lf[0][i]) * bxl + (g.lf[0][i + 1] - g.lv[0][i]) * bxr) * g.dlf_inv[0][i];
+    if (g.dims >= 2)
+      u[BY] = ((g.lv[1][j] - g.lf[1][j]) * byl + (g.lf[1][j + 1] - g.lv[1][j]) * byr) * g.dlf_inv[1][j];
+    else
+      u[BY] = byl;
+    if (g.dims >= 3)
+      u[BZ] = ((g.lv[2][k] - g.lf[2][k]) * bzl + (g.lf[2][k + 1] - g.lv[2][k]) * bzr) * g.dlf_inv[2][k];
+    else
+      u[BZ] = bzl;
+    if (src) {
+      // integrator.pyx:132-170 with the stage input w0 (read before w1 is written)
+      double f[3];
+      if (fdriv) {
+        f[0] = fdriv[c];
+        f[1] = fdriv[sv + c];
+        f[2] = fdriv[2 * sv + c];
+      }
+      srcterm::apply(u, w0[c], w0[VX * sv + c], w0[VY * sv + c], w0[VZ * sv + c], gv, grav, fdriv ? f : nullptr,
+                     dt);
+    }
+#pragma unroll
+    for (int n = 0; n < NM; ++n) u1[n * sv + c] = u[n];
+    // eos.pyx:13-44
+    double ww[NM];
+    cons2prim(ww, u, g.gam);
+    e |= plain::check_prim(ww);
+#pragma unroll
+    for (int n = 0; n < NM; ++n) w1[n * sv + c] = ww[n];
+  }
+  if (e) atomicOr(err, e);
+}
+
+}  // namespace split

@@ -46,8 +46,11 @@ enum { BNZ_RCN_CONST = 0, BNZ_RCN_LINEAR = 1 };
 enum { BNZ_LIM_VL = 0, BNZ_LIM_MC = 1, BNZ_LIM_MM = 2 };
 enum { BNZ_BC_PERIODIC = 0, BNZ_BC_OUTFLOW = 1, BNZ_BC_REFLECT = 2 };
 enum { BNZ_TC_ISO = 0, BNZ_TC_ANISO = 1 };
-/* kernel path: fused tile kernels (default) or one kernel per reference loop */
-enum { BNZ_PATH_FUSED = 0, BNZ_PATH_PLAIN = 1 };
+/* kernel path: fused tile kernels (default), one kernel per reference loop
+ * (plain), or the plain path's decomposition with each face's flux formed once
+ * from per-cell slopes and one fused update per stage (split; not in hydro
+ * mode).  All three give the same bits in the exact build. */
+enum { BNZ_PATH_FUSED = 0, BNZ_PATH_PLAIN = 1, BNZ_PATH_SPLIT = 2 };
 
 /* Grid: the [computation] Nx..Nz / xmin..zmax keys and the [physics]
  * bc_x1..bc_z2 flags (src/coordinates/grid.pyx:107-232,
@@ -65,7 +68,7 @@ typedef struct {
  * limiter is the added `limiter: vl|mc|mm` key (the reference hard-wires vl).
  * outflow_face_aware keeps the CT-updated outer face under outflow BCs.
  * exact_fp selects kernels built without multiply-add contraction, which
- * reproduce the CPU reference bit for bit; path selects fused or plain kernels.
+ * reproduce the CPU reference bit for bit; path selects fused, plain or split kernels.
  * Source terms (src/srcterms, applied in both stages by
  * integrator.pyx:132-170 add_source_terms): grav = the [physics] gx, gy, gz
  * constant acceleration (gravity.pyx:17-19); drive_f0 / drive_tau / drive_nmod
