@@ -718,6 +718,7 @@ int bnz_set_state(bnz_ctx* c, const double* pc, int is_prim, const double* bfld)
   if (is_prim) c->launches += c->L->prim2cons_all(a);
   else c->launches += c->L->cons2prim_all(a);
   c->ghosts_stale = false;
+  c->cons_stale = false;
   int rc = refresh_cds(c);
   if (rc) return rc;
   CKC(cudaGetLastError());
@@ -736,6 +737,7 @@ int bnz_init(bnz_ctx* c) {
   memset(&ds, 0, sizeof ds);
   CKC(cudaMemcpyAsync(c->d_ds, &ds, sizeof ds, cudaMemcpyHostToDevice, c->stream));
   c->ghosts_stale = false;
+  c->cons_stale = false;
   int rc = refresh_cds(c);
   if (rc) return rc;
   CKC(cudaGetLastError());
@@ -834,15 +836,17 @@ int diffuse_impl(bnz_ctx* c, const double* dtp, double dt_hyp, int* nsts_out) {
   return BNZ_OK;
 }
 
-// Fill ghosts and cons of the fused path's current state (what the
-// reference's end-of-step BC + prim2cons leave behind, vanleer.pyx:162-163).
+// Fill ghosts and cons of the fused path's current state, or cons of the split
+// path's (what the reference's end-of-step BC + prim2cons leave behind,
+// vanleer.pyx:162-163).
 int ensure_ghosts(bnz_ctx* c) {
-  if (!c->ghosts_stale) return BNZ_OK;
+  if (!c->ghosts_stale && !c->cons_stale) return BNZ_OK;
   StepArgs a = step_args(c);
-  c->launches += c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
+  if (c->ghosts_stale) c->launches += c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
   c->launches += c->L->prim2cons_all(a);
   CKC(cudaGetLastError());
   c->ghosts_stale = false;
+  c->cons_stale = false;
   return BNZ_OK;
 }
 
@@ -893,10 +897,11 @@ int step_impl(bnz_ctx* c, double dt_host, int dt_mode) {
       if (rc) return rc;
     }
   }
-  if (c->md.path != BNZ_PATH_FUSED) {
-    c->launches += c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
-    c->launches += c->L->prim2cons_all(a);
-  }
+  if (c->md.path != BNZ_PATH_FUSED) c->launches += c->L->apply_bc(a, c->prim, c->bfld, 0xFFFu);
+  // vanleer.pyx:162-163; the split path reads no conserved state, so it forms
+  // cons when it is asked for
+  if (c->md.path == BNZ_PATH_PLAIN) c->launches += c->L->prim2cons_all(a);
+  if (c->md.path == BNZ_PATH_SPLIT) c->cons_stale = true;
   CKC(cudaGetLastError());
   return BNZ_OK;
 }
@@ -915,6 +920,7 @@ int bnz_diffuse(bnz_ctx* c, double dt, int* nsts_out) {
     c->ghosts_stale = true;  // cons no longer matches prim
     rc = refresh_cds(c);
   }
+  if (c->md.path == BNZ_PATH_SPLIT) c->cons_stale = true;
   return rc;
 }
 
@@ -1077,6 +1083,7 @@ int bnz_advance_graph(bnz_ctx* c, double tmax, int nsteps) {
       c->launches += c->graph_launches;
     }
     if (c->md.path == BNZ_PATH_FUSED) c->ghosts_stale = true;
+    if (c->md.path == BNZ_PATH_SPLIT) c->cons_stale = true;
   }
   for (int r = 0; r < rest; ++r) {
     int rc = one_step();

@@ -38,6 +38,7 @@ struct bnz_ctx {
   double* bbuf[2] = {nullptr, nullptr};
   int parity = 0;
   bool ghosts_stale = false;  // fused path: ghosts / cons not refreshed since the last step
+  bool cons_stale = false;    // split path: cons not formed from prim since the last step
   FusedInst* d_inst = nullptr;
   FusedTile* d_tiles = nullptr;
   int ntA = 0, ntB = 0;

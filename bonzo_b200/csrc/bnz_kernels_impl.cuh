@@ -246,39 +246,56 @@ int plain_predictor_corrector(const StepArgs& a, const double* dtp) {
 }
 
 namespace {
+// Blocks of 32 x 8 cells of the box, split::UPD_KZ z indices each.
+inline dim3 cell_grid(const plain::Box& b) {
+  const int kz = split::UPD_KZ;
+  return dim3((b.hi.x - b.lo.x + 32) / 32, (b.hi.y - b.lo.y + 8) / 8, (b.hi.z - b.lo.z + kz) / kz);
+}
+
+// The prim arrays a split stage reads: w on [vlo, vhi], wfb elsewhere.
+struct SplitSrc {
+  const double* w;
+  const double* wfb;
+  int3 vlo, vhi;
+};
+
 template <int AX, int ORDER>
-int split_flux(const StepArgs& a, const double* w, const double* bf, const plain::Box& b) {
+int split_flux(const StepArgs& a, const SplitSrc& s, const double* bf, const plain::Box& b) {
   using T = split::FT<AX>;
   const int lo[3] = {b.lo.x, b.lo.y, b.lo.z}, hi[3] = {b.hi.x, b.hi.y, b.hi.z};
   const long long na = (hi[AX] - lo[AX] + T::NA) / T::NA, nb = (hi[T::TAX] - lo[T::TAX] + T::NB) / T::NB;
-  const long long nblk = na * nb * (hi[T::OAX] - lo[T::OAX] + 1);
+  const unsigned nblk = (unsigned)(na * nb * (hi[T::OAX] - lo[T::OAX] + 1));
   switch (a.rsolver) {
     case dev::RS_HLLD:
-      split::k_flux_tile<AX, ORDER, dev::RS_HLLD><<<(unsigned)nblk, T::NT, 0, a.stream>>>(
-          a.g, w, bf, a.flx[AX], b, a.limiter, a.charact_proj, a.err);
+      split::k_flux_tile<AX, ORDER, dev::RS_HLLD><<<nblk, T::NT, 0, a.stream>>>(
+          a.g, s.w, s.wfb, s.vlo, s.vhi, bf, a.flx[AX], b, a.limiter, a.charact_proj, a.err);
       break;
     case dev::RS_HLLT:
-      split::k_flux_tile<AX, ORDER, dev::RS_HLLT><<<(unsigned)nblk, T::NT, 0, a.stream>>>(
-          a.g, w, bf, a.flx[AX], b, a.limiter, a.charact_proj, a.err);
+      split::k_flux_tile<AX, ORDER, dev::RS_HLLT><<<nblk, T::NT, 0, a.stream>>>(
+          a.g, s.w, s.wfb, s.vlo, s.vhi, bf, a.flx[AX], b, a.limiter, a.charact_proj, a.err);
       break;
     default:
-      split::k_flux_tile<AX, ORDER, dev::RS_HLL><<<(unsigned)nblk, T::NT, 0, a.stream>>>(
-          a.g, w, bf, a.flx[AX], b, a.limiter, a.charact_proj, a.err);
+      split::k_flux_tile<AX, ORDER, dev::RS_HLL><<<nblk, T::NT, 0, a.stream>>>(
+          a.g, s.w, s.wfb, s.vlo, s.vhi, bf, a.flx[AX], b, a.limiter, a.charact_proj, a.err);
       break;
   }
   return 1;
 }
 
+// Donor-cell fluxes from one prim array go through plain::k_flux: with no
+// slopes to share, staging the cells in shared memory only adds a barrier
+// (the split tile kernel measured about 9 % slower there).
 template <int AX>
-int split_flux(const StepArgs& a, int order, const double* w, const double* bf, const plain::Box& b) {
-  return order == 0 ? split_flux<AX, 0>(a, w, bf, b) : split_flux<AX, 1>(a, w, bf, b);
+int split_flux(const StepArgs& a, int order, const SplitSrc& s, const double* bf, const plain::Box& b) {
+  if (order == 0 && s.w == s.wfb) return launch_flux<AX>(a, 0, s.w, bf, b);
+  return order == 0 ? split_flux<AX, 0>(a, s, bf, b) : split_flux<AX, 1>(a, s, bf, b);
 }
 
 // One VL2 stage on the split path (vanleer.pyx:104-120 or 130-151): the face
 // fluxes over the boxes of integrate_hydro, the edge EMFs over the box of
-// integrate_field, then the fused update of the stage's range.  The prim
-// state a.prim is the stage input and receives the stage output.
-int split_stage(const StepArgs& a, double* u1, const double* u0, double* b1, const double* b0, double* bsave,
+// integrate_field, then the fused update of the stage's range from U^n =
+// prim2cons(a.prim) into w1.
+int split_stage(const StepArgs& a, const SplitSrc& s, double* w1, double* b1, const double* b0, double* bsave,
                 const double* bf, int order, const double* dtp, double fac) {
   const GridDev& g = a.g;
   int l[6];
@@ -286,29 +303,44 @@ int split_stage(const StepArgs& a, double* u1, const double* u0, double* b1, con
   const int il = l[0], iu = l[1], jl = l[2], ju = l[3], kl = l[4], ku = l[5];
   const int jb = g.dims >= 2 ? jl - 1 : 0, je = g.dims >= 2 ? ju + 1 : 0;
   const int kb = g.dims >= 3 ? kl - 1 : 0, ke = g.dims >= 3 ? ku + 1 : 0;
-  int nl = split_flux<0>(a, order, a.prim, bf, mkbox(il, iu + 1, jb, je, kb, ke));
-  if (g.dims >= 2) nl += split_flux<1>(a, order, a.prim, bf, mkbox(il - 1, iu + 1, jl, ju + 1, kb, ke));
-  if (g.dims >= 3) nl += split_flux<2>(a, order, a.prim, bf, mkbox(il - 1, iu + 1, jl - 1, ju + 1, kl, ku + 1));
+  int nl = split_flux<0>(a, order, s, bf, mkbox(il, iu + 1, jb, je, kb, ke));
+  if (g.dims >= 2) nl += split_flux<1>(a, order, s, bf, mkbox(il - 1, iu + 1, jl, ju + 1, kb, ke));
+  if (g.dims >= 3) nl += split_flux<2>(a, order, s, bf, mkbox(il - 1, iu + 1, jl - 1, ju + 1, kl, ku + 1));
   {
     plain::Box b = mkbox(il, iu + 1, jl, g.dims >= 2 ? ju + 1 : 0, kl, g.dims >= 3 ? ku + 1 : 0);
-    split::k_ee<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(g, a.prim, a.flx[0], a.flx[1], a.flx[2], a.ee, b);
+    split::k_ee<<<cell_grid(b), dim3(32, 8), 0, a.stream>>>(g, s.w, s.wfb, s.vlo, s.vhi, a.flx[0], a.flx[1],
+                                                             a.flx[2], a.ee, b);
   }
   plain::Box b = mkbox(il, iu, jl, ju, kl, ku);
-  split::k_update<<<nblocks(boxn(b), 256), 256, 0, a.stream>>>(
-      g, u1, u0, a.prim, a.prim, b1, b0, bsave, a.flx[0], a.flx[1], a.flx[2], a.ee, b, dtp, fac, a.src, a.grav[0],
+  split::k_update<<<cell_grid(b), dim3(32, 8), 0, a.stream>>>(
+      g, w1, a.prim, s.w, b1, b0, bsave, a.flx[0], a.flx[1], a.flx[2], a.ee, b, dtp, fac, a.src, a.grav[0],
       a.grav[1], a.grav[2], a.fdriv, a.err);
   return nl + 2;
 }
 }  // namespace
 
-// vanleer.pyx:101-151 on the split path.  The predictor saves the faces of
-// b^n it reads into the spare face array a.ec (the split path forms the cell
-// EMFs on the fly), so that the corrector can update a.bfld in place of a
-// neighbour's reads: it reads b^n from the copy.
+// vanleer.pyx:101-151 on the split path.  The predictor writes W^(n+1/2) to
+// a.cons_s (cells 1..Ntot-2 of each active axis), so that a.prim keeps W^n for
+// the corrector's U^n; the corrector reads W^(n+1/2) there and W^n on the
+// outer cells, as the plain path's in-place prim holds them.  The predictor
+// also saves the faces of b^n it reads into the spare face array a.ec (the
+// split path forms the cell EMFs on the fly), so that the corrector can
+// update a.bfld in place of a neighbour's reads: it reads b^n from the copy.
+// The conserved state is not written: the context forms it from prim after
+// the boundary fill, when it is asked for.
 int split_predictor_corrector(const StepArgs& a, const double* dtp) {
   if (a.hydro) return 0;
-  int nl = split_stage(a, a.cons_s, a.cons, a.bfld_s, a.bfld, a.ec, a.bfld, 0, dtp, 0.5);
-  nl += split_stage(a, a.cons, a.cons, a.bfld, a.ec, nullptr, a.bfld_s, a.reconstr_order, dtp, 1.0);
+  const GridDev& g = a.g;
+  const int N[3] = {g.nx, g.ny, g.nz};
+  int lo[3], hi[3];
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = d < g.dims ? 1 : 0;
+    hi[d] = d < g.dims ? N[d] - 2 : 0;
+  }
+  const SplitSrc pred = {a.prim, a.prim, make_int3(0, 0, 0), make_int3(g.nx - 1, g.ny - 1, g.nz - 1)};
+  const SplitSrc corr = {a.cons_s, a.prim, make_int3(lo[0], lo[1], lo[2]), make_int3(hi[0], hi[1], hi[2])};
+  int nl = split_stage(a, pred, a.cons_s, a.bfld_s, a.bfld, a.ec, a.bfld, 0, dtp, 0.5);
+  nl += split_stage(a, corr, a.prim, a.bfld, a.ec, nullptr, a.bfld_s, a.reconstr_order, dtp, 1.0);
   return nl;
 }
 

@@ -10,10 +10,12 @@
 //     plain::k_flux forms both one-sided slopes of every face itself;
 //   * k_ee forms the cell-centred EMF (ct.pyx:128-148) of the cells it needs
 //     on the fly instead of reading a separate array;
-//   * k_update: per cell, the conservative update (godunov.pyx:215-252), the
-//     face update (ct.pyx:15-91), face-to-cell B (ct.pyx:96-123), the source
-//     terms (integrator.pyx:132-170) and cons2prim (eos.pyx:13-44) in one
-//     pass, where the plain path runs up to eight launches.
+//   * k_update: per cell, prim2cons of the step's input, the conservative
+//     update (godunov.pyx:215-252), the face update (ct.pyx:15-91),
+//     face-to-cell B (ct.pyx:96-123), the source terms
+//     (integrator.pyx:132-170) and cons2prim (eos.pyx:13-44) in one pass,
+//     where the plain path runs up to eight launches and keeps a conserved
+//     state in HBM between them.
 // A face is formed by exactly one block and no kernel waits on a barrier
 // between Riemann solves (what bounds the z-marching chunk kernels).  Every
 // expression is the plain path's, so the exact build is bitwise equal to it
@@ -60,8 +62,12 @@ __device__ __forceinline__ int ax_of(int3 v, int a) { return a == 0 ? v.x : a ==
 // normal field entry, which nothing reads, is not stored).  ORDER 0: donor
 // cell (reconstr_c.c:8-22); ORDER 1: PLM with limiter lim (reconstr_c.c:29-91),
 // in characteristic variables when cp.  Normal field from the face array.
+// Cells outside [vlo, vhi] are read from wfb instead of w (the corrector reads
+// the predictor's output, which covers cells 1..Ntot-2 of each active axis,
+// and the step's input prim elsewhere).
 template <int AX, int ORDER, int RS>
 __global__ void __launch_bounds__(256, 2) k_flux_tile(GridDev g, const double* __restrict__ w,
+                                                      const double* __restrict__ wfb, int3 vlo, int3 vhi,
                                                       const double* __restrict__ bf, double* __restrict__ F,
                                                       plain::Box box, int lim, int cp, unsigned* err) {
   using T = FT<AX>;
@@ -84,8 +90,11 @@ __global__ void __launch_bounds__(256, 2) k_flux_tile(GridDev g, const double* _
     const int a = a0 - 2 + ia, b = b0 + ib;
     if (a < 0 || a >= N[AX] || b > hi_b) continue;
     const long long c = a * sa + b * sb + o * so;
+    const bool in = a >= ax_of(vlo, AX) && a <= ax_of(vhi, AX) && b >= ax_of(vlo, T::TAX) &&
+                    b <= ax_of(vhi, T::TAX) && o >= ax_of(vlo, T::OAX) && o <= ax_of(vhi, T::OAX);
+    const double* src = in ? w : wfb;
 #pragma unroll
-    for (int n = 0; n < NM; ++n) sW[T::ws(n, ia, ib)] = w[plain::perm<AX>(n) * g.sv + c];
+    for (int n = 0; n < NM; ++n) sW[T::ws(n, ia, ib)] = src[plain::perm<AX>(n) * g.sv + c];
   }
   __syncthreads();
   const int la = AX == 0 ? threadIdx.x % (NA + 1) : threadIdx.x / NB;
@@ -146,6 +155,15 @@ __global__ void __launch_bounds__(256, 2) k_flux_tile(GridDev g, const double* _
   if (e) atomicOr(err, e);
 }
 
+// k_ee and k_update: a thread walks UPD_KZ cells up z (blocks of 32 x 8
+// columns) and asks L2 for the inputs of the cell two planes ahead while it
+// computes, since a cell's loads outnumber what its registers hold in flight.
+// (Staging each tile's inputs in shared memory by asynchronous copies first
+// measured slower: 2.3 and 0.66 ms per 256^3 launch against 1.8 and 0.47.)
+constexpr int UPD_KZ = 8;
+
+__device__ __forceinline__ void prefetch_l2(const double* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // ct.pyx:128-148: component COMP of the cell-centred EMF -(v x B) of cell c
 template <int COMP>
 __device__ __forceinline__ double ec_at(const double* __restrict__ w, long long sv, long long c) {
@@ -155,31 +173,58 @@ __device__ __forceinline__ double ec_at(const double* __restrict__ w, long long 
   return -(q[VX * sv] * q[BY * sv] - q[VY * sv] * q[BX * sv]);
 }
 
-// ct.pyx:153-215 (interp_ee1): plain::k_ee with the cell EMFs formed from w
-__global__ void k_ee(GridDev g, const double* __restrict__ w, const double* __restrict__ fx,
-                     const double* __restrict__ fy, const double* __restrict__ fz, double* __restrict__ ee,
-                     plain::Box box) {
+// ct.pyx:153-215 (interp_ee1): plain::k_ee with the cell EMFs formed from the
+// stage input prim: w on [vlo, vhi], wfb elsewhere (as in k_flux_tile)
+__global__ void k_ee(GridDev g, const double* __restrict__ w_in, const double* __restrict__ wfb, int3 vlo,
+                     int3 vhi, const double* __restrict__ fx, const double* __restrict__ fy,
+                     const double* __restrict__ fz, double* __restrict__ ee, plain::Box box) {
   const long long sv = g.sv, sy = g.nx, sz = (long long)g.nx * g.ny;
-  BOX_LOOP(box, i, j, k) {
+  const int i = box.lo.x + (int)(blockIdx.x * 32 + threadIdx.x);
+  const int j = box.lo.y + (int)(blockIdx.y * 8 + threadIdx.y);
+  if (i > box.hi.x || j > box.hi.y) return;
+  const int kb = box.lo.z + (int)blockIdx.z * UPD_KZ, ke = min(kb + UPD_KZ - 1, box.hi.z);
+  for (int k = kb; k <= ke; ++k) {
     const long long c = plain::cidx(g, i, j, k);
+    if (k + 2 <= ke) {
+      const long long p = c + 2 * sz;
+#pragma unroll
+      for (int n = VX; n <= BZ; ++n) {
+        if (n == PR || n == PSC) continue;
+        prefetch_l2(w_in + n * sv + p);
+        prefetch_l2(w_in + n * sv + p - sy);
+      }
+      prefetch_l2(fx + BY * sv + p);
+      prefetch_l2(fx + BY * sv + p - sy);
+      prefetch_l2(fx + BZ * sv + p);
+      prefetch_l2(fy + BX * sv + p);
+      prefetch_l2(fy + BZ * sv + p);
+      prefetch_l2(fz + BX * sv + p);
+      prefetch_l2(fz + BY * sv + p);
+      prefetch_l2(fz + BY * sv + p - sy);
+    }
+    // the source array of the cell (i - di, j - dj, k - dk)
+    auto W = [&](int di, int dj, int dk) {
+      const int x = i - di, y = j - dj, z = k - dk;
+      return x >= vlo.x && x <= vhi.x && y >= vlo.y && y <= vhi.y && z >= vlo.z && z <= vhi.z ? w_in : wfb;
+    };
     if (g.dims == 3) {
       ee[c] = (0.5 * (-fy[BZ * sv + c - sz] - fy[BZ * sv + c] + fz[BY * sv + c - sy] + fz[BY * sv + c]) -
-               0.25 * (ec_at<0>(w, sv, c - sy) + ec_at<0>(w, sv, c) + ec_at<0>(w, sv, c - sz - sy) +
-                       ec_at<0>(w, sv, c - sz)));
+               0.25 * (ec_at<0>(W(0, 1, 0), sv, c - sy) + ec_at<0>(W(0, 0, 0), sv, c) +
+                       ec_at<0>(W(0, 1, 1), sv, c - sz - sy) + ec_at<0>(W(0, 0, 1), sv, c - sz)));
       ee[sv + c] = (0.5 * (-fz[BX * sv + c - 1] - fz[BX * sv + c] + fx[BZ * sv + c - sz] + fx[BZ * sv + c]) -
-                    0.25 * (ec_at<1>(w, sv, c - 1) + ec_at<1>(w, sv, c) + ec_at<1>(w, sv, c - sz - 1) +
-                            ec_at<1>(w, sv, c - sz)));
+                    0.25 * (ec_at<1>(W(1, 0, 0), sv, c - 1) + ec_at<1>(W(0, 0, 0), sv, c) +
+                            ec_at<1>(W(1, 0, 1), sv, c - sz - 1) + ec_at<1>(W(0, 0, 1), sv, c - sz)));
       ee[2 * sv + c] = (0.5 * (-fx[BY * sv + c - sy] - fx[BY * sv + c] + fy[BX * sv + c - 1] + fy[BX * sv + c]) -
-                        0.25 * (ec_at<2>(w, sv, c - 1) + ec_at<2>(w, sv, c) + ec_at<2>(w, sv, c - sy - 1) +
-                                ec_at<2>(w, sv, c - sy)));
+                        0.25 * (ec_at<2>(W(1, 0, 0), sv, c - 1) + ec_at<2>(W(0, 0, 0), sv, c) +
+                                ec_at<2>(W(1, 1, 0), sv, c - sy - 1) + ec_at<2>(W(0, 1, 0), sv, c - sy)));
     } else if (g.dims == 2) {
       ee[c] = -fy[BZ * sv + c];
       ee[sv + c] = fx[BZ * sv + c];
       ee[2 * sv + c] = (0.5 * (-fx[BY * sv + c - sy] - fx[BY * sv + c] + fy[BX * sv + c - 1] + fy[BX * sv + c]) -
-                        0.25 * (ec_at<2>(w, sv, c - 1) + ec_at<2>(w, sv, c) + ec_at<2>(w, sv, c - sy - 1) +
-                                ec_at<2>(w, sv, c - sy)));
+                        0.25 * (ec_at<2>(W(1, 0, 0), sv, c - 1) + ec_at<2>(W(0, 0, 0), sv, c) +
+                                ec_at<2>(W(1, 1, 0), sv, c - sy - 1) + ec_at<2>(W(0, 1, 0), sv, c - sy)));
     } else {
-      ee[c] = -ec_at<0>(w, sv, c);
+      ee[c] = -ec_at<0>(W(0, 0, 0), sv, c);
       ee[sv + c] = fx[BZ * sv + c];
       ee[2 * sv + c] = -fx[BY * sv + c];
     }
@@ -189,13 +234,17 @@ __global__ void k_ee(GridDev g, const double* __restrict__ w, const double* __re
 // One stage's update of the cells of `box` (the stage's update range): the
 // plain path's k_advance_hydro, k_advance_b (the cell's lower faces, and its
 // upper ones on the range's last cells), k_interp_bc, k_source and
-// k_cons2prim, with the same expressions.  u1 may be u0 and w1 may be w0: a
-// thread reads and writes only its own cell of them.  b0 must not be b1 (a
-// cell reads its upper faces' old values, which the neighbour updates); bsave,
-// when not null, receives the b0 faces the update reads (the step's b^n, for
-// the corrector).
-__global__ void __launch_bounds__(256) k_update(GridDev g, double* u1, const double* u0, double* w1,
-                                                const double* w0, double* __restrict__ b1,
+// k_cons2prim, with the same expressions.  The stage starts from U^n =
+// prim2cons(wn) (what the plain path's cons array holds: eos.pyx:48-78 after
+// the last step's boundary fill) and writes only the stage's prim w1 and
+// faces b1; the conserved state of the step's end is formed from prim after
+// the boundary fill, as the plain path does.  w0 is the stage input prim (the
+// source terms).  w1 may be wn: a thread reads and writes only its own cell of
+// them.  b0 must not be b1 (a cell reads its upper faces' old values, which
+// the neighbour updates); bsave, when not null, receives the b0 faces the
+// update reads (the step's b^n, for the corrector).
+__global__ void __launch_bounds__(256, 3) k_update(GridDev g, double* w1, const double* wn,
+                                                const double* __restrict__ w0, double* __restrict__ b1,
                                                 const double* __restrict__ b0, double* __restrict__ bsave,
                                                 const double* __restrict__ fx, const double* __restrict__ fy,
                                                 const double* __restrict__ fz, const double* __restrict__ ee,
@@ -207,8 +256,34 @@ __global__ void __launch_bounds__(256) k_update(GridDev g, double* u1, const dou
   const double gv[3] = {gx, gy, gz};
   const bool grav = gx != 0. || gy != 0. || gz != 0.;
   unsigned e = 0;
-  BOX_LOOP(box, i, j, k) {
+  const int i = box.lo.x + (int)(blockIdx.x * 32 + threadIdx.x);
+  const int j = box.lo.y + (int)(blockIdx.y * 8 + threadIdx.y);
+  if (i > box.hi.x || j > box.hi.y) return;
+  const int kb = box.lo.z + (int)blockIdx.z * UPD_KZ, ke = min(kb + UPD_KZ - 1, box.hi.z);
+  for (int k = kb; k <= ke; ++k) {
     const long long c = plain::cidx(g, i, j, k);
+    if (k + 2 <= ke) {
+      const long long p = c + 2 * sz;
+#pragma unroll
+      for (int n = 0; n < NM; ++n) prefetch_l2(wn + n * sv + p);
+#pragma unroll
+      for (int n = 0; n < BX; ++n) {
+        prefetch_l2(fx + n * sv + p);
+        prefetch_l2(fy + n * sv + p);
+        prefetch_l2(fy + n * sv + p + sy);
+        prefetch_l2(fz + n * sv + p + sz);
+      }
+#pragma unroll
+      for (int n = 0; n < 3; ++n) {
+        prefetch_l2(b0 + n * sv + p);
+        prefetch_l2(ee + n * sv + p);
+        prefetch_l2(ee + n * sv + p + sy);
+      }
+      if (src) {
+#pragma unroll
+        for (int n = 0; n <= VZ; ++n) prefetch_l2(w0 + n * sv + p);
+      }
+    }
     // godunov.pyx:215-252
     const double vol = g.dlf[0][i] * g.dlf[1][j] * g.dlf[2][k];
     const double dtdv = dt / vol;
@@ -216,10 +291,16 @@ __global__ void __launch_bounds__(256) k_update(GridDev g, double* u1, const dou
     const double day = g.dlf[0][i] * g.dlf[2][k];
     const double daz = g.dlf[0][i] * g.dlf[1][j];
     double u[NM];
+    {
+      double wc[NM];
+#pragma unroll
+      for (int n = 0; n < NM; ++n) wc[n] = wn[n * sv + c];
+      prim2cons(u, wc, g.gam);
+    }
 #pragma unroll
     for (int n = 0; n < BX; ++n) {
       const long long q = n * sv + c;
-      double v = u0[q] - dtdv * (dax * fx[q + 1] - dax * fx[q]);
+      double v = u[n] - dtdv * (dax * fx[q + 1] - dax * fx[q]);
       if (g.dims >= 2) v -= dtdv * (day * fy[q + sy] - day * fy[q]);
       if (g.dims >= 3) v -= dtdv * (daz * fz[q + sz] - daz * fz[q]);
       u[n] = v;
@@ -275,7 +356,7 @@ __global__ void __launch_bounds__(256) k_update(GridDev g, double* u1, const dou
     else
       u[BZ] = bzl;
     if (src) {
-      // integrator.pyx:132-170 with the stage input w0 (read before w1 is written)
+      // integrator.pyx:132-170 with the stage input w0
       double f[3];
       if (fdriv) {
         f[0] = fdriv[c];
@@ -285,8 +366,6 @@ __global__ void __launch_bounds__(256) k_update(GridDev g, double* u1, const dou
       srcterm::apply(u, w0[c], w0[VX * sv + c], w0[VY * sv + c], w0[VZ * sv + c], gv, grav, fdriv ? f : nullptr,
                      dt);
     }
-#pragma unroll
-    for (int n = 0; n < NM; ++n) u1[n * sv + c] = u[n];
     // eos.pyx:13-44
     double ww[NM];
     cons2prim(ww, u, g.gam);

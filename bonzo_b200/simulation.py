@@ -271,7 +271,9 @@ class Simulation:
         self.io = BnzIO(usr_dir)
         gc = self.grid.coord
         if path == "fused" and not (gc.dims == 2 and self.integr.reconstr == "linear"):
-            path = "plain"  # the fused kernels cover 2D PLM grids
+            # the fused tile kernels are the fastest on 2D PLM grids, the split
+            # path (fluxes once per face, one update per stage) elsewhere
+            path = "split"
         self.ctx = Context(Nx=gc.Nact[0], Ny=gc.Nact[1], Nz=gc.Nact[2], dims=gc.dims, lmin=gc.lmin,
                            lmax=gc.lmax, bc=self.grid.bc, path=path, exact_fp=int(exact_fp),
                            **self.integr.method())
