@@ -28,7 +28,7 @@ EXPORTS = [
     "bnz_get_time", "bnz_last_nsts", "bnz_set_time", "bnz_check", "bnz_sync", "bnz_advance_graph",
     "bnz_device_state", "bnz_stream", "bnz_set_stream", "bnz_launch_count",
     "bnz_batch_create", "bnz_batch_destroy", "bnz_batch_last_error", "bnz_batch_size",
-    "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_advance_timed", "bnz_batch_step_host", "bnz_batch_test_withhold_loads", "bnz_fp64_fma_peak", "bnz_batch_set_stream", "bnz_batch_launch_count",
+    "bnz_batch_instance", "bnz_batch_advance", "bnz_batch_advance_timed", "bnz_batch_step_host", "bnz_batch_test_withhold_loads", "bnz_fp64_fma_peak", "bnz_fast_rcp", "bnz_batch_set_stream", "bnz_batch_launch_count",
     "bnz_batch_sync", "bnz_variant_count", "bnz_batch_set_variant", "bnz_batch_get_variant",
     "bnz_batch_time_variant", "bnz_batch_autotune", "bnz_vl2_step_noalloc", "bnz_noalloc_last_error",
     "bnz_noalloc_check", "bnz_noalloc_scratch_bytes", "bnz_set_state_device", "bnz_get_state_device", "bnz_rollout_forward",
@@ -104,6 +104,7 @@ def load():
     L.bnz_batch_advance.argtypes = [vp, C.c_double, C.c_int]
     L.bnz_batch_advance_timed.argtypes = [vp, C.c_double, C.c_int, _dp]
     L.bnz_fp64_fma_peak.argtypes = [_dp]
+    L.bnz_fast_rcp.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     L.bnz_batch_test_withhold_loads.argtypes = [vp, C.c_int]
     L.bnz_batch_step_host.argtypes = [vp, C.POINTER(_dp), C.POINTER(_dp), C.c_double, C.c_int, C.c_int]
     L.bnz_set_state_device.argtypes = [vp, vp, vp]
@@ -492,6 +493,18 @@ def fp64_fma_peak():
     if rc != BNZ_OK:
         raise BnzError(rc, "bnz_fp64_fma_peak failed")
     return t.value
+
+
+def fast_rcp(x):
+    """1 / x (a CUDA float64 tensor) by the fast build's Newton-refined reciprocal."""
+    import torch
+    L = load()
+    x = x.contiguous()
+    y = torch.empty_like(x)
+    rc = L.bnz_fast_rcp(x.data_ptr(), y.data_ptr(), x.numel(), torch.cuda.current_stream().cuda_stream)
+    if rc != BNZ_OK:
+        raise BnzError(rc, "bnz_fast_rcp failed")
+    return y
 
 
 def variants():

@@ -2,8 +2,10 @@
 // denominator of the kernels' FP64-pipe fraction (the HBM roofline's
 // denominator is a measured copy bandwidth).  Eight independent FMA chains per
 // thread keep the pipe busy; the result is written so nothing is elided.
+// Also the check entry of the fast build's reciprocal (bnz_fastmath.cuh).
 #include <cuda_runtime.h>
 
+#include "bnz_fastmath.cuh"
 #include "bnz_gpu.h"
 
 namespace {
@@ -25,7 +27,19 @@ __global__ void k_fp64_fma(double* __restrict__ out, double a, double b) {
   out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+__global__ void k_nr_rcp(const double* __restrict__ x, double* __restrict__ y, int n) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) y[q] = bnz_nr_rcp(x[q]);
+}
+
 }  // namespace
+
+extern "C" int bnz_fast_rcp(const double* x, double* y, int n, void* stream) {
+  if (n < 0 || (n > 0 && (!x || !y))) return BNZ_ERR_ARG;
+  if (n == 0) return BNZ_OK;
+  const int threads = 256, blocks = (n + threads - 1) / threads < 4096 ? (n + threads - 1) / threads : 4096;
+  k_nr_rcp<<<blocks, threads, 0, (cudaStream_t)stream>>>(x, y, n);
+  return cudaGetLastError() == cudaSuccess ? BNZ_OK : BNZ_ERR_CUDA;
+}
 
 extern "C" int bnz_fp64_fma_peak(double* tflops) {
   if (!tflops) return BNZ_ERR_ARG;

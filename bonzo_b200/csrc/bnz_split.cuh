@@ -243,7 +243,7 @@ __global__ void k_ee(GridDev g, const double* __restrict__ w_in, const double* _
 // them.  b0 must not be b1 (a cell reads its upper faces' old values, which
 // the neighbour updates); bsave, when not null, receives the b0 faces the
 // update reads (the step's b^n, for the corrector).
-__global__ void __launch_bounds__(256, 3) k_update(GridDev g, double* w1, const double* wn,
+__global__ void __launch_bounds__(256, 2) k_update(GridDev g, double* w1, const double* wn,
                                                 const double* __restrict__ w0, double* __restrict__ b1,
                                                 const double* __restrict__ b0, double* __restrict__ bsave,
                                                 const double* __restrict__ fx, const double* __restrict__ fy,
@@ -260,8 +260,20 @@ __global__ void __launch_bounds__(256, 3) k_update(GridDev g, double* w1, const 
   const int j = box.lo.y + (int)(blockIdx.y * 8 + threadIdx.y);
   if (i > box.hi.x || j > box.hi.y) return;
   const int kb = box.lo.z + (int)blockIdx.z * UPD_KZ, ke = min(kb + UPD_KZ - 1, box.hi.z);
+  const bool d2 = g.dims >= 2, d3 = g.dims >= 3;
+  // the column's coordinates (loaded once: the stores below may alias them
+  // for all the compiler knows)
+  const double dsx = g.dlf[0][i], dsy = g.dlf[1][j];
+  const double lvx = g.lv[0][i], lfx0 = g.lf[0][i], lfx1 = g.lf[0][i + 1], dix = g.dlf_inv[0][i];
+  const double lvy = d2 ? g.lv[1][j] : 0., lfy0 = d2 ? g.lf[1][j] : 0., lfy1 = d2 ? g.lf[1][j + 1] : 0.;
+  const double diy = d2 ? g.dlf_inv[1][j] : 0.;
+  // carried up z: the cell's lower z-face values (fluxes, b0, the new face),
+  // and the edge EMFs of its lower level
+  double fzl[BX], bz0l = 0., bzl = 0.;
+  double eyl[2], exl[2];  // ee_y at (i, i+1), ee_x at (j, j+1) on level k
   for (int k = kb; k <= ke; ++k) {
     const long long c = plain::cidx(g, i, j, k);
+    const bool first = k == kb;
     if (k + 2 <= ke) {
       const long long p = c + 2 * sz;
 #pragma unroll
@@ -271,7 +283,7 @@ __global__ void __launch_bounds__(256, 3) k_update(GridDev g, double* w1, const 
         prefetch_l2(fx + n * sv + p);
         prefetch_l2(fy + n * sv + p);
         prefetch_l2(fy + n * sv + p + sy);
-        prefetch_l2(fz + n * sv + p + sz);
+        prefetch_l2(fz + n * sv + p);
       }
 #pragma unroll
       for (int n = 0; n < 3; ++n) {
@@ -284,12 +296,24 @@ __global__ void __launch_bounds__(256, 3) k_update(GridDev g, double* w1, const 
         for (int n = 0; n <= VZ; ++n) prefetch_l2(w0 + n * sv + p);
       }
     }
+    if (first) {
+      if (d3) {
+#pragma unroll
+        for (int n = 0; n < BX; ++n) fzl[n] = fz[n * sv + c];
+      }
+      bz0l = b0[2 * sv + c];
+      eyl[0] = ee[sv + c];
+      eyl[1] = ee[sv + c + 1];
+      exl[0] = d2 ? ee[c] : 0.;
+      exl[1] = d2 ? ee[c + sy] : 0.;
+    }
     // godunov.pyx:215-252
-    const double vol = g.dlf[0][i] * g.dlf[1][j] * g.dlf[2][k];
+    const double dsz = g.dlf[2][k];
+    const double vol = dsx * dsy * dsz;
     const double dtdv = dt / vol;
-    const double dax = g.dlf[1][j] * g.dlf[2][k];
-    const double day = g.dlf[0][i] * g.dlf[2][k];
-    const double daz = g.dlf[0][i] * g.dlf[1][j];
+    const double dax = dsy * dsz;
+    const double day = dsx * dsz;
+    const double daz = dsx * dsy;
     double u[NM];
     {
       double wc[NM];
@@ -297,61 +321,81 @@ __global__ void __launch_bounds__(256, 3) k_update(GridDev g, double* w1, const 
       for (int n = 0; n < NM; ++n) wc[n] = wn[n * sv + c];
       prim2cons(u, wc, g.gam);
     }
+    double fzu[BX];
 #pragma unroll
     for (int n = 0; n < BX; ++n) {
       const long long q = n * sv + c;
       double v = u[n] - dtdv * (dax * fx[q + 1] - dax * fx[q]);
-      if (g.dims >= 2) v -= dtdv * (day * fy[q + sy] - day * fy[q]);
-      if (g.dims >= 3) v -= dtdv * (daz * fz[q + sz] - daz * fz[q]);
+      if (d2) v -= dtdv * (day * fy[q + sy] - day * fy[q]);
+      if (d3) {
+        fzu[n] = fz[q + sz];
+        v -= dtdv * (daz * fzu[n] - daz * fzl[n]);
+      }
       u[n] = v;
     }
     // ct.pyx:15-91 on the cell's faces; a face's expressions depend only on
     // its transverse indices, so the upper face is the lower one shifted
-    const double dsx = g.dlf[0][i], dsy = g.dlf[1][j], dsz = g.dlf[2][k];
-    auto bxf = [&](long long q) {
+    // (the new lower z face is the cell below's upper one)
+    double ez[2][2];  // ee_z at (i + dx, j + dy) on level k
+    ez[0][0] = ee[2 * sv + c];
+    ez[1][0] = ee[2 * sv + c + 1];
+    ez[0][1] = d2 ? ee[2 * sv + c + sy] : 0.;
+    ez[1][1] = d2 ? ee[2 * sv + c + sy + 1] : 0.;
+    double eyu[2] = {0., 0.}, exu[2] = {0., 0.};  // level k + 1
+    if (d3) {
+      eyu[0] = ee[sv + c + sz];
+      eyu[1] = ee[sv + c + sz + 1];
+      exu[0] = ee[c + sz];
+      exu[1] = ee[c + sz + sy];
+    }
+    const double bx0[2] = {b0[c], b0[c + 1]};
+    const double by0[2] = {b0[sv + c], d2 ? b0[sv + c + sy] : 0.};
+    const double bz0u = d3 ? b0[2 * sv + c + sz] : 0.;
+    auto bxf = [&](int dx) {
       const double dtda = dt / (dsy * dsz);
-      double v = b0[q];
-      if (g.dims >= 2) v -= dtda * (dsz * ee[2 * sv + q + sy] - dsz * ee[2 * sv + q]);
-      if (g.dims >= 3) v += dtda * (dsy * ee[sv + q + sz] - dsy * ee[sv + q]);
+      double v = bx0[dx];
+      if (d2) v -= dtda * (dsz * ez[dx][1] - dsz * ez[dx][0]);
+      if (d3) v += dtda * (dsy * eyu[dx] - dsy * eyl[dx]);
       return v;
     };
-    auto byf = [&](long long q) {
+    auto byf = [&](int dy) {
       const double dtda = dt / (dsx * dsz);
-      double v = b0[sv + q] + dtda * (dsz * ee[2 * sv + q + 1] - dsz * ee[2 * sv + q]);
-      if (g.dims >= 3) v -= dtda * (dsx * ee[q + sz] - dsx * ee[q]);
+      double v = by0[dy] + dtda * (dsz * ez[1][dy] - dsz * ez[0][dy]);
+      if (d3) v -= dtda * (dsx * exu[dy] - dsx * exl[dy]);
       return v;
     };
-    auto bzf = [&](long long q) {
+    auto bzf = [&](double bz, const double* ey, const double* ex) {
       const double dtda = dt / (dsx * dsy);
-      double v = b0[2 * sv + q] - dtda * (dsy * ee[sv + q + 1] - dsy * ee[sv + q]);
-      if (g.dims >= 2) v += dtda * (dsx * ee[q + sy] - dsx * ee[q]);
+      double v = bz - dtda * (dsy * ey[1] - dsy * ey[0]);
+      if (d2) v += dtda * (dsx * ex[1] - dsx * ex[0]);
       return v;
     };
-    const double bxl = bxf(c), byl = byf(c), bzl = bzf(c), bxr = bxf(c + 1);
-    const double byr = g.dims >= 2 ? byf(c + sy) : 0.;
-    const double bzr = g.dims >= 3 ? bzf(c + sz) : 0.;
+    if (first) bzl = bzf(bz0l, eyl, exl);
+    const double bxl = bxf(0), byl = byf(0), bxr = bxf(1);
+    const double byr = d2 ? byf(1) : 0.;
+    const double bzr = d3 ? bzf(bz0u, eyu, exu) : 0.;
     b1[c] = bxl;
     b1[sv + c] = byl;
     b1[2 * sv + c] = bzl;
-    const bool ux = i == box.hi.x, uy = g.dims >= 2 && j == box.hi.y, uz = g.dims >= 3 && k == box.hi.z;
+    const bool ux = i == box.hi.x, uy = d2 && j == box.hi.y, uz = d3 && k == box.hi.z;
     if (ux) b1[c + 1] = bxr;
     if (uy) b1[sv + c + sy] = byr;
     if (uz) b1[2 * sv + c + sz] = bzr;
     if (bsave) {
-      bsave[c] = b0[c];
-      bsave[sv + c] = b0[sv + c];
-      bsave[2 * sv + c] = b0[2 * sv + c];
-      if (ux) bsave[c + 1] = b0[c + 1];
-      if (uy) bsave[sv + c + sy] = b0[sv + c + sy];
-      if (uz) bsave[2 * sv + c + sz] = b0[2 * sv + c + sz];
+      bsave[c] = bx0[0];
+      bsave[sv + c] = by0[0];
+      bsave[2 * sv + c] = bz0l;
+      if (ux) bsave[c + 1] = bx0[1];
+      if (uy) bsave[sv + c + sy] = by0[1];
+      if (uz) bsave[2 * sv + c + sz] = bz0u;
     }
     // ct.pyx:96-123
-    u[BX] = ((g.lv[0][i] - g.lf[0][i]) * bxl + (g.lf[0][i + 1] - g.lv[0][i]) * bxr) * g.dlf_inv[0][i];
-    if (g.dims >= 2)
-      u[BY] = ((g.lv[1][j] - g.lf[1][j]) * byl + (g.lf[1][j + 1] - g.lv[1][j]) * byr) * g.dlf_inv[1][j];
+    u[BX] = ((lvx - lfx0) * bxl + (lfx1 - lvx) * bxr) * dix;
+    if (d2)
+      u[BY] = ((lvy - lfy0) * byl + (lfy1 - lvy) * byr) * diy;
     else
       u[BY] = byl;
-    if (g.dims >= 3)
+    if (d3)
       u[BZ] = ((g.lv[2][k] - g.lf[2][k]) * bzl + (g.lf[2][k + 1] - g.lv[2][k]) * bzr) * g.dlf_inv[2][k];
     else
       u[BZ] = bzl;
@@ -372,6 +416,17 @@ __global__ void __launch_bounds__(256, 3) k_update(GridDev g, double* w1, const 
     e |= plain::check_prim(ww);
 #pragma unroll
     for (int n = 0; n < NM; ++n) w1[n * sv + c] = ww[n];
+    // the upper face values become the next cell's lower ones
+    if (d3) {
+#pragma unroll
+      for (int n = 0; n < BX; ++n) fzl[n] = fzu[n];
+    }
+    bz0l = bz0u;
+    bzl = bzr;
+    eyl[0] = eyu[0];
+    eyl[1] = eyu[1];
+    exl[0] = exu[0];
+    exl[1] = exu[1];
   }
   if (e) atomicOr(err, e);
 }

@@ -323,6 +323,13 @@ int bnz_riemann(int rsolver, int nvar, const double* wl, const double* wr, const
  * counterpart in the reference: a measurement helper. */
 int bnz_fp64_fma_peak(double* tflops);
 
+/* y[q] = 1 / x[q] (device arrays of n doubles, queued on `stream`) by the
+ * reciprocal the fast build uses in place of a division (the van Leer
+ * limiter's): an approximate hardware reciprocal refined by two Newton-Raphson
+ * steps.  For normal x it is within 2 ulp of the IEEE quotient; the tests
+ * check that bound.  No counterpart in the reference: a check helper. */
+int bnz_fast_rcp(const double* x, double* y, int n, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
