@@ -69,6 +69,10 @@ def parse():
     ap.add_argument("--n3d", type=int, default=0,
                     help="side of the 3D configurations' grids instead of 256 / 384 (batch: half of it); small "
                          "cases for profiling")
+    ap.add_argument("--config-names", default="turbulence,conduction,batch",
+                    help="which 3D configurations to run (profiling one of them)")
+    ap.add_argument("--config-paths", default="fused,split,plain",
+                    help="which kernel paths the single-grid 3D configurations run on")
     return ap.parse_args()
 
 
@@ -502,7 +506,8 @@ def _time_ctx(c, steps, graph, stream, clk=None):
     return e0.elapsed_time(e1) / steps, nsts / steps
 
 
-def run_configs(fused_steps=6, plain_steps=2, n3d=0):
+def run_configs(fused_steps=6, plain_steps=2, n3d=0, names=("turbulence", "conduction", "batch"),
+                paths=("fused", "split", "plain")):
     """The 3D configurations on seeded synthetic initial states, on the fused
     z-marching path, the split path (fluxes once per face, fused update) and
     the plain one-launch-per-loop path:
@@ -525,10 +530,14 @@ def run_configs(fused_steps=6, plain_steps=2, n3d=0):
             ("turbulence_%d^3" % nt, nt, dict(cour=0.3), lambda gc: P.turbulence3d(gc, seed=0), True),
             ("conduction_%d^3" % nc, nc, dict(cour=0.4, kappa0=0.01, thcond_type="aniso"),
              lambda gc: P.conduction3d(gc, seed=0), False)):
+        if name.split("_")[0] not in names:
+            continue
         gc = P.make_grid(n, n, n, dims=3, bc=0)
         prim, bfld = gen(gc)
         rec = {}
         for path, steps in (("fused", fused_steps), ("split", fused_steps), ("plain", plain_steps)):
+            if path not in paths:
+                continue
             c = Context(Nx=n, Ny=n, Nz=n, dims=3, bc=((0, 0), (0, 0), (0, 0)), gam=5. / 3, rsolver="hlld",
                         limiter="vl", path=path, **kw)
             c.set_stream(stream.cuda_stream)
@@ -549,14 +558,16 @@ def run_configs(fused_steps=6, plain_steps=2, n3d=0):
                          "clocks": clk.record()}
             c.close()
             torch.cuda.empty_cache()
-        rec["fused_vs_plain"] = round(rec["plain"]["ms_per_step"] / rec["fused"]["ms_per_step"], 3)
-        rec["split_vs_plain"] = round(rec["plain"]["ms_per_step"] / rec["split"]["ms_per_step"], 3)
+        for p in ("fused", "split"):
+            if p in rec and "plain" in rec:
+                rec[p + "_vs_plain"] = round(rec["plain"]["ms_per_step"] / rec[p]["ms_per_step"], 3)
         rec["workload"] = ("%d^3 periodic, seeded synthetic %s, VL2+PLM(vl)+HLLD+CT%s" %
                            (n, name.split("_")[0], ", RKL2 conduction kappa_par 0.01" if kw.get("kappa0") else ""))
         out[name] = rec
         del prim, bfld
     nb = n3d // 2 if n3d else 192
-    out["conduction_batch_4x%d^3" % nb] = run_batch3d(stream, dev, peak, peak_src, fused_steps, n=nb)
+    if "batch" in names:
+        out["conduction_batch_4x%d^3" % nb] = run_batch3d(stream, dev, peak, peak_src, fused_steps, n=nb)
     return out
 
 
@@ -658,7 +669,9 @@ def main():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         if rank == 0:
-            print(json.dumps({"metric": METRIC, "configs_3d": run_configs(n3d=args.n3d)}), flush=True)
+            print(json.dumps({"metric": METRIC, "configs_3d": run_configs(n3d=args.n3d, names=args.config_names.split(","),
+                                                                         paths=args.config_paths.split(","))}),
+                  flush=True)
         return 0
     if args.adjoint_only:
         import torch
@@ -678,7 +691,8 @@ def main():
     if rank == 0 and not args.no_adjoint:
         line["adjoint"] = run_adjoint()
     if rank == 0 and world == 1 and not args.no_configs:
-        line["configs_3d"] = run_configs(n3d=args.n3d)
+        line["configs_3d"] = run_configs(n3d=args.n3d, names=args.config_names.split(","),
+                                         paths=args.config_paths.split(","))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         batch = build_batch(args.instances, args.seed)
         cb = run_cpu_reference(batch, steps=2, warmup=1)

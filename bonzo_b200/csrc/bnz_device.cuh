@@ -598,12 +598,7 @@ __device__ __forceinline__ double mm_lim(double a, double b) {
 __device__ __forceinline__ double mc_lim(double a, double b) { return mm_lim(2. * mm_lim(a, b), 0.5 * (a + b)); }
 __device__ __forceinline__ double vl_lim(double a, double b) {
   double ab = a * b;
-#if BNZ_FAST_MATH
-  // ab > 0: a and b have one sign and |a + b| >= 2 sqrt(ab), a normal number
-  return (ab > 0.) ? (2. * ab) * bnz_nr_rcp(a + b) : 0.;
-#else
   return (ab > 0.) ? (2. * ab / (a + b)) : 0.;
-#endif
 }
 template <int LIM>
 __device__ __forceinline__ double limit(double a, double b) {

@@ -57,6 +57,20 @@ struct FT {
 
 __device__ __forceinline__ int ax_of(int3 v, int a) { return a == 0 ? v.x : a == 1 ? v.y : v.z; }
 
+// reconstr_c.c:54-91 half slope; in the fast build the van Leer limiter's
+// quotient 2ab/(a+b) is 2ab times the Newton-refined reciprocal of a + b
+// (bnz_fastmath.cuh: within 2 ulp; ab > 0 makes a and b one-signed, so
+// |a + b| >= 2 sqrt(ab) is a normal number)
+__device__ __forceinline__ double half_slope_split(int lim, double wm, double wc, double wp) {
+#if BNZ_FAST_MATH
+  if (lim == LIM_VL) {
+    const double a = wc - wm, b = wp - wc, ab = a * b;
+    return 0.5 * ((ab > 0.) ? (2. * ab) * bnz_nr_rcp(a + b) : 0.);
+  }
+#endif
+  return plain::half_slope_rt(lim, wm, wc, wp);
+}
+
 // Fluxes of the AX faces of `box` (face index along AX = the cell on its
 // right), in the global variable order as plain::k_flux stores them (the
 // normal field entry, which nothing reads, is not stored).  ORDER 0: donor
@@ -120,7 +134,7 @@ __global__ void __launch_bounds__(256, 2) k_flux_tile(GridDev g, const double* _
 #pragma unroll
         for (int n = 0; n < NM; ++n) {
           if (n == BX) continue;
-          sD[T::ds(slot8(n), la, lb)] = plain::half_slope_rt(lim, p[n * WN - DA], p[n * WN], p[n * WN + DA]);
+          sD[T::ds(slot8(n), la, lb)] = half_slope_split(lim, p[n * WN - DA], p[n * WN], p[n * WN + DA]);
         }
       }
     }
