@@ -575,7 +575,8 @@ def run_batch3d(stream, dev, peak, peak_src, steps, n=192, count=4):
     """The conduction configuration's batch: 4 instances of 192^3 (seeds 0..3)
     advanced together -- one launch per hyperbolic stage for all instances, then
     each instance's RKL2 stages over its own dt -- beside the same instances as
-    separate fused contexts stepped one after another."""
+    separate fused contexts and as separate split-path contexts stepped one
+    after another."""
     import torch
     from bonzo_b200 import problems as P
     from bonzo_b200._lib import Batch, Context
@@ -614,29 +615,31 @@ def run_batch3d(stream, dev, peak, peak_src, steps, n=192, count=4):
                     "clocks": clk.record()}
     b.close()
     torch.cuda.empty_cache()
-    ctxs = []
-    for prim, bfld in ics:
-        c = Context(path="fused", **grid, **meth)
-        c.set_stream(stream.cuda_stream)
-        c.set_state(prim, bfld)
-        c.init()
-        c.advance(1e30, 2)
-        ctxs.append(c)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(steps):
+    for path, key in (("fused", "separate_contexts"), ("split", "separate_split_contexts")):
+        ctxs = []
+        for prim, bfld in ics:
+            c = Context(path=path, **grid, **meth)
+            c.set_stream(stream.cuda_stream)
+            c.set_state(prim, bfld)
+            c.init()
+            c.advance(1e30, 2)
+            ctxs.append(c)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            for c in ctxs:
+                c.advance(1e30, 1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_sep = e0.elapsed_time(e1) / steps
+        rec[key] = {"ms_per_step": round(ms_sep, 3), "mzone_updates_per_s": round(zones / (ms_sep * 1e-3) / 1e6, 1)}
         for c in ctxs:
-            c.advance(1e30, 1)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms_sep = e0.elapsed_time(e1) / steps
-    rec["separate_contexts"] = {"ms_per_step": round(ms_sep, 3),
-                                "mzone_updates_per_s": round(zones / (ms_sep * 1e-3) / 1e6, 1)}
-    rec["batch_vs_separate"] = round(ms_sep / ms, 3)
-    for c in ctxs:
-        c.check()
-        c.close()
-    torch.cuda.empty_cache()
+            c.check()
+            c.close()
+        del ctxs
+        torch.cuda.empty_cache()
+    rec["batch_vs_separate"] = round(rec["separate_contexts"]["ms_per_step"] / ms, 3)
+    rec["split_contexts_vs_batch"] = round(ms / rec["separate_split_contexts"]["ms_per_step"], 3)
     return rec
 
 

@@ -124,12 +124,12 @@ def test_fast_persistent_batch_graph(sweep):
         assert b[q].div_b() <= DIVB_TOL
 
 
-@pytest.mark.parametrize("path", ["fused", "plain"])
+@pytest.mark.parametrize("path", ["fused", "split", "plain"])
 @pytest.mark.parametrize("case,bc", [("turb3d", 0), ("blast3d", 1)])
 def test_fast_3d_100_steps(case, bc, path):
     """3D, 32^3: 100 steps of the fast build against the oracle, div B after
     every step, and conservation on the periodic grid; the fused z-marching
-    kernels and the plain path."""
+    kernels, the split path and the plain path."""
     n = 32
     if case == "turb3d":
         # rms Mach 0.5: at Mach 1 this 32^3 box reaches p < 0 near step 20 in
@@ -164,7 +164,7 @@ def test_fast_3d_100_steps(case, bc, path):
     assert d.check() == 0
 
 
-@pytest.mark.parametrize("path", ["fused", "plain"])
+@pytest.mark.parametrize("path", ["fused", "split", "plain"])
 def test_fast_cond3d_20_steps(path):
     """3D field-aligned conduction interleaved with the step (RKL2), 32^3,
     20 steps of the fast build against the oracle."""
