@@ -576,7 +576,8 @@ def run_batch3d(stream, dev, peak, peak_src, steps, n=192, count=4):
     advanced together -- one launch per hyperbolic stage for all instances, then
     each instance's RKL2 stages over its own dt -- beside the same instances as
     separate fused contexts and as separate split-path contexts stepped one
-    after another."""
+    after another; and the same batch on the split path (each instance's
+    launches in turn)."""
     import torch
     from bonzo_b200 import problems as P
     from bonzo_b200._lib import Batch, Context
@@ -589,32 +590,35 @@ def run_batch3d(stream, dev, peak, peak_src, steps, n=192, count=4):
     rec = {"workload": "%d instances of %d^3 periodic field-aligned conduction (seeds 0..%d), VL2+PLM(vl)+HLLD+CT "
                        "with RKL2, per-instance CFL dt" % (count, n, count - 1)}
     zones = count * n ** 3
-    b = Batch([grid] * count, **meth)
-    b.set_stream(stream.cuda_stream)
-    for q, (prim, bfld) in enumerate(ics):
-        b[q].set_state(prim, bfld)
-        b[q].init()
-    b.advance(1e30, 2)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    with ClockSampler(dev) as clk:
-        e0.record(stream)
-        b.advance(1e30, steps)
-        e1.record(stream)
+    for path, key in (("fused", "batch"), ("split", "split_batch")):
+        b = Batch([grid] * count, path=path, **meth)
+        b.set_stream(stream.cuda_stream)
+        for q, (prim, bfld) in enumerate(ics):
+            b[q].set_state(prim, bfld)
+            b[q].init()
+        b.advance(1e30, 2)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    nsts = sum(b[q].last_nsts() for q in range(count))
-    for q in range(count):
-        b[q].check()
-    byts = BYTES_PER_ZONE * zones + 96 * n ** 3 * nsts
-    ach = byts / (ms * 1e-3) / 1e9
-    rec["batch"] = {"ms_per_step": round(ms, 3), "mzone_updates_per_s": round(zones / (ms * 1e-3) / 1e6, 1),
+        with ClockSampler(dev) as clk:
+            e0.record(stream)
+            b.advance(1e30, steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        nsts = sum(b[q].last_nsts() for q in range(count))
+        for q in range(count):
+            b[q].check()
+        byts = BYTES_PER_ZONE * zones + 96 * n ** 3 * nsts
+        ach = byts / (ms * 1e-3) / 1e9
+        rec[key] = {"ms_per_step": round(ms, 3), "mzone_updates_per_s": round(zones / (ms * 1e-3) / 1e6, 1),
                     "rkl2_stages_per_step_all_instances": nsts, "steps_timed": steps,
                     "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                                  "frac": round(ach / peak, 4), "peak_source": peak_src},
                     "clocks": clk.record()}
-    b.close()
-    torch.cuda.empty_cache()
+        b.close()
+        del b
+        torch.cuda.empty_cache()
+    ms = rec["batch"]["ms_per_step"]
     for path, key in (("fused", "separate_contexts"), ("split", "separate_split_contexts")):
         ctxs = []
         for prim, bfld in ics:
@@ -640,6 +644,7 @@ def run_batch3d(stream, dev, peak, peak_src, steps, n=192, count=4):
         torch.cuda.empty_cache()
     rec["batch_vs_separate"] = round(rec["separate_contexts"]["ms_per_step"] / ms, 3)
     rec["split_contexts_vs_batch"] = round(ms / rec["separate_split_contexts"]["ms_per_step"], 3)
+    rec["split_batch_vs_batch"] = round(ms / rec["split_batch"]["ms_per_step"], 3)
     return rec
 
 

@@ -353,8 +353,10 @@ class Context:
 
 
 class Batch:
-    """Many independent 2D grids of uneven size with one method, advanced by
-    one launch per stage (bnz_batch_* in include/bnz_gpu.h)."""
+    """Many independent grids of uneven size with one method (bnz_batch_* in
+    include/bnz_gpu.h): 2D grids by one launch per stage over every instance,
+    3D grids likewise on the fused chunk kernels, or with path="split" on the
+    split path one instance after another."""
 
     def __init__(self, grids, **method):
         self.L = load()

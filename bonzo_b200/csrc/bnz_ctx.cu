@@ -1190,6 +1190,7 @@ struct bnz_batch {
   // 3D batches: instance records, chunk lists (predictor then corrector) and
   // the instances' 4D tensor maps of ws (128 bytes each)
   bool dims3 = false;
+  bool split = false;  // 3D batch on the split path: each instance's step in turn
   FusedInst3* d_inst3 = nullptr;
   FusedTile3* d_tiles3 = nullptr;
   int ntA3 = 0, ntB3 = 0;
@@ -1471,11 +1472,17 @@ int bnz_batch_create(const bnz_grid_desc* grids, int n, const bnz_method_desc* m
   bnz_batch* b = new bnz_batch();
   *out = b;
   b->md = *md;
-  b->md.path = BNZ_PATH_FUSED;
   b->dims3 = grids[0].dims == 3;
   for (int q = 0; q < n; ++q)
     if (grids[q].dims != grids[0].dims || (grids[q].dims != 2 && grids[q].dims != 3))
       return bfail(b, BNZ_ERR_UNSUPPORTED, "a batch takes 2D grids or 3D grids, not a mix");
+  // 3D batches run the fused chunk kernels over every instance in one launch
+  // per stage, or (path = split) the split path's launches instance by
+  // instance; 2D batches run the fused tile kernels
+  b->split = md->path == BNZ_PATH_SPLIT;
+  if (b->split && !b->dims3)
+    return bfail(b, BNZ_ERR_UNSUPPORTED, "the split path batches 3D grids (2D batches run the fused tile kernels)");
+  b->md.path = b->split ? BNZ_PATH_SPLIT : BNZ_PATH_FUSED;
   if (md->kappa0 > 0. && !b->dims3)
     return bfail(b, BNZ_ERR_UNSUPPORTED, "2D batches advance the hyperbolic step only (kappa0 = 0)");
   if (drive_on(*md)) return bfail(b, BNZ_ERR_UNSUPPORTED, "batches do not drive turbulence (drive_f0 = 0)");
@@ -1493,9 +1500,10 @@ int bnz_batch_create(const bnz_grid_desc* grids, int n, const bnz_method_desc* m
     b->ctx.push_back(c);
     rc = bnz_set_stream(c, (void*)b->stream);
     if (rc) return bfail(b, rc, c->err);
-    insts.push_back(make_inst(c));
+    if (!b->split) insts.push_back(make_inst(c));
   }
   b->L = b->ctx[0]->L;
+  if (b->split) return BNZ_OK;
   if (b->dims3) {
     b->variant = 0;
     return batch_build3(b);
@@ -1584,6 +1592,13 @@ int batch_prologue(bnz_batch* b, double tmax) {
     }
   }
   const int n = (int)b->ctx.size();
+  if (b->split) {
+    for (bnz_ctx* c : b->ctx) {
+      c->h_stage[2] = tmax;
+      CKB(cudaMemcpyAsync(&c->d_ds->tmax, &c->h_stage[2], sizeof(double), cudaMemcpyHostToDevice, b->stream));
+    }
+    return BNZ_OK;
+  }
   if (b->dims3) k_set_tmax<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_inst3, n, tmax);
   else k_set_tmax<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_inst, n, tmax);
   b->launches += 1;
@@ -1620,10 +1635,44 @@ int batch_step3_diffuse(bnz_batch* b) {
 
 void batch_epilogue(bnz_batch* b) {
   for (bnz_ctx* c : b->ctx) {
-    set_parity(c, b->parity);
-    c->ghosts_stale = true;
+    if (b->split) {
+      c->cons_stale = true;
+    } else {
+      set_parity(c, b->parity);
+      c->ghosts_stale = true;
+    }
     c->time_on_device = true;
   }
+}
+
+// One step of every instance of a split batch, in turn: the device CFL dt
+// clipped to the instance's tmax, the split step and its boundary fill, the
+// time record.  With conduction the stage count of each instance's RKL2 comes
+// from its dt on the host (one read-back of every instance's dt per step); an
+// instance at its tmax is not stepped.  An instance whose dt is zero on the
+// graph path passes through the step unchanged (the update kernels return
+// when dt is zero).
+int batch_step_split(bnz_batch* b, bool host_dt) {
+  const int n = (int)b->ctx.size();
+  for (bnz_ctx* c : b->ctx) {
+    StepArgs a = step_args(c);
+    if (!c->md.fixdt) c->launches += c->L->new_dt(a, c->prim, c->d_ds, c->md.cour, 1);
+    else c->launches += c->L->set_dt(c->stream, c->d_ds, c->md.dt_fixed);
+  }
+  std::vector<DtState> ds(host_dt ? n : 0);
+  if (host_dt) {
+    for (int q = 0; q < n; ++q)
+      CKB(cudaMemcpyAsync(&ds[q], b->ctx[q]->d_ds, sizeof(DtState), cudaMemcpyDeviceToHost, b->stream));
+    CKB(cudaStreamSynchronize(b->stream));
+  }
+  for (int q = 0; q < n; ++q) {
+    bnz_ctx* c = b->ctx[q];
+    if (host_dt && !(ds[q].dt > 0.)) continue;
+    int rc = step_impl(c, host_dt ? ds[q].dt : 0.);
+    if (rc) return bfail(b, rc, c->err);
+    c->launches += c->L->time_advance(c->stream, c->d_ds);
+  }
+  return BNZ_OK;
 }
 
 }  // namespace
@@ -1637,6 +1686,33 @@ int bnz_batch_advance(bnz_batch* b, double tmax, int nsteps) {
   int rc = batch_prologue(b, tmax);
   if (rc) return rc;
   const int mode = b->md.fixdt ? FDT_FIXED : FDT_CFL;
+  if (b->split) {
+    const bool host_dt = b->md.kappa0 > 0.;
+    if (host_dt) {
+      // conduction's stage count is chosen on the host: no graph
+      for (int s = 0; s < nsteps && rc == BNZ_OK; ++s) rc = batch_step_split(b, true);
+    } else {
+      if (!b->graph) {
+        CKB(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        rc = batch_step_split(b, false);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        if (rc) {
+          if (g) cudaGraphDestroy(g);
+          return rc;
+        }
+        if (e != cudaSuccess) return bfail(b, BNZ_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return bfail(b, BNZ_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+      }
+      for (int s = 0; s < nsteps; ++s) CKB(cudaGraphLaunch(b->graph, b->stream));
+    }
+    if (rc) return rc;
+    CKB(cudaGetLastError());
+    batch_epilogue(b);
+    return BNZ_OK;
+  }
   if (b->dims3 && b->md.kappa0 > 0.) {
     // conduction's stage count is chosen on the host: no graph
     for (int s = 0; s < nsteps; ++s) {
@@ -1701,9 +1777,9 @@ int bnz_batch_advance_timed(bnz_batch* b, double tmax, int nsteps, double* ms_ke
   // one event set per step, so every launch of the run is timed
   std::vector<cudaEvent_t> ev(4 * (size_t)nsteps, nullptr);
   for (auto& e : ev) CKB(cudaEventCreate(&e));
-  if (b->dims3 && b->md.kappa0 > 0.) {
+  if ((b->dims3 && b->md.kappa0 > 0.) || b->split) {
     for (auto& x : ev) cudaEventDestroy(x);
-    return bfail(b, BNZ_ERR_UNSUPPORTED, "per-launch timing covers batches without conduction");
+    return bfail(b, BNZ_ERR_UNSUPPORTED, "per-launch timing covers fused batches without conduction");
   }
   for (int s = 0; s < nsteps; ++s) {
     if (b->dims3) {

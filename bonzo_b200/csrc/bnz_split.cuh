@@ -266,6 +266,9 @@ __global__ void __launch_bounds__(256, 2) k_update(GridDev g, double* w1, const 
                                                 double gx, double gy, double gz, const double* __restrict__ fdriv,
                                                 unsigned* err) {
   const double dt = fac * *dtp;
+  // a step of zero length (an instance at its tmax) leaves the state as it
+  // is, as the reference's loop does by not stepping
+  if (dt == 0.) return;
   const long long sv = g.sv, sy = g.nx, sz = (long long)g.nx * g.ny;
   const double gv[3] = {gx, gy, gz};
   const bool grav = gx != 0. || gy != 0. || gz != 0.;

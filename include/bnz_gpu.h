@@ -169,7 +169,11 @@ int bnz_launch_count(const bnz_ctx* ctx, long long* n);
  * launch over a tile list that spans every instance, each instance keeps its
  * own CFL time step, and steps are replayed from a CUDA graph.  No reference
  * counterpart: the reference runs one grid per process (vanleer.advance).
- * 2D grids, PLM, kappa0 = 0.
+ * All 2D (the fused tile kernels; kappa0 = 0) or all 3D grids: the fused
+ * chunk kernels over every instance in one launch per stage, or with
+ * method->path = BNZ_PATH_SPLIT the split path's launches for each instance
+ * in turn (faster per step on large grids); with kappa0 > 0 each instance's
+ * RKL2 stages follow its own hyperbolic step over its own dt.
  * ------------------------------------------------------------------------ */
 typedef struct bnz_batch bnz_batch;
 int bnz_batch_create(const bnz_grid_desc* grids, int n, const bnz_method_desc* method, bnz_batch** out);

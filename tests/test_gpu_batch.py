@@ -115,6 +115,9 @@ def test_batch_rejects_mixed_dims_and_2d_conduction():
         Batch([dict(Nx=8, Ny=8, Nz=8, dims=3), dict(Nx=8, Ny=8, Nz=1, dims=2)], **METHOD)
     with pytest.raises(BnzError):
         Batch([dict(Nx=8, Ny=8, Nz=1, dims=2)], kappa0=0.1, **METHOD)
+    with pytest.raises(BnzError) as e:
+        Batch([dict(Nx=8, Ny=8, Nz=1, dims=2)], path="split", **METHOD)
+    assert "3D" in str(e.value)
 
 
 def _instances3(shapes, seed=7):
@@ -134,15 +137,16 @@ def _instances3(shapes, seed=7):
     return out
 
 
+@pytest.mark.parametrize("path", ["fused", "split"])
 @pytest.mark.parametrize("steps", [1, 4])
-def test_batch3d_bitwise_vs_oracle(steps):
+def test_batch3d_bitwise_vs_oracle(steps, path):
     """Uneven 3D grids (one odd Ntot_x, staged without TMA) advanced together by
-    the fused 3D kernels, each with its own CFL dt, against each grid alone in
-    the oracle."""
+    the fused 3D kernels, or instance by instance on the split path, each with
+    its own CFL dt, against each grid alone in the oracle."""
     from bonzo_b200._lib import Batch
     inst = _instances3([(16, 16, 16), (24, 20, 18), (21, 15, 13), (32, 24, 20)])
     meth = dict(METHOD, cour=0.3)
-    b = Batch([g for g, *_ in inst], exact_fp=True, **meth)
+    b = Batch([g for g, *_ in inst], exact_fp=True, path=path, **meth)
     for q, (grid, gc, prim, bfld) in enumerate(inst):
         b[q].set_state(prim, bfld)
         b[q].init()
@@ -159,9 +163,11 @@ def test_batch3d_bitwise_vs_oracle(steps):
         assert b[q].check() == 0
 
 
-def test_batch3d_conduction_bitwise_vs_oracle():
-    """A 3D batch with field-aligned conduction: one launch per hyperbolic stage
-    for all instances, then each instance's RKL2 stages over its own dt."""
+@pytest.mark.parametrize("path", ["fused", "split"])
+def test_batch3d_conduction_bitwise_vs_oracle(path):
+    """A 3D batch with field-aligned conduction: the hyperbolic step of every
+    instance (one launch per stage for all of them on the fused kernels), then
+    each instance's RKL2 stages over its own dt."""
     from bonzo_b200._lib import Batch
     shapes = [(16, 16, 16), (20, 18, 16)]
     inst = []
@@ -170,7 +176,7 @@ def test_batch3d_conduction_bitwise_vs_oracle():
         prim, bfld = P.conduction3d(gc, seed=q, kmax=4)
         inst.append((dict(Nx=n[0], Ny=n[1], Nz=n[2], dims=3, bc=((0, 0),) * 3), gc, prim, bfld))
     meth = dict(METHOD, kappa0=0.01)
-    b = Batch([g for g, *_ in inst], exact_fp=True, **meth)
+    b = Batch([g for g, *_ in inst], exact_fp=True, path=path, **meth)
     for q, (grid, gc, prim, bfld) in enumerate(inst):
         b[q].set_state(prim, bfld)
         b[q].init()
@@ -208,6 +214,36 @@ def test_batch3d_timed_and_tmax():
         assert t == tmax and s == o.nstep
         for x, y in zip(o.get_state(), b[q].get_state()):
             assert np.array_equal(x, y), q
+
+
+def test_batch3d_split_tmax_and_graph():
+    """A split-path 3D batch: instances stop at tmax (further steps leave them
+    as they are), graph replays continue where the last call stopped, and
+    per-launch timing is refused."""
+    from bonzo_b200._lib import Batch, BnzError
+    inst = _instances3([(16, 16, 16), (24, 20, 22)])
+    meth = dict(METHOD, cour=0.3)
+    b = Batch([g for g, *_ in inst], exact_fp=True, path="split", **meth)
+    for q, (grid, gc, prim, bfld) in enumerate(inst):
+        b[q].set_state(prim, bfld)
+        b[q].init()
+    with pytest.raises(BnzError):
+        b.advance_timed(1e30, 1)
+    b.advance(1e30, 2)
+    tmax = b[0].time()[0] + 0.004
+    b.advance(tmax, 40)
+    b.advance(tmax, 3)
+    for q, (grid, gc, prim, bfld) in enumerate(inst):
+        o = oracle_sim(grid, **meth)
+        o.set_state(prim, bfld)
+        o.init()
+        o.advance(1e30, max_steps=2)
+        o.advance(tmax)
+        t, s, _ = b[q].time()
+        assert t == tmax and s == o.nstep
+        for x, y in zip(o.get_state(), b[q].get_state()):
+            assert np.array_equal(x, y), q
+        assert b[q].check() == 0
 
 
 @pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9])
