@@ -180,12 +180,89 @@ __global__ void k_stage(GridDev g, double* __restrict__ w, const double* __restr
   }
 }
 
+// thcond_elec.pyx:154-303, the field-aligned (anisotropic) face flux of
+// face_flux<AX> with T and the limited transverse gradients read from a
+// block's shared-memory tables: T over the tile and one cell around it
+// (tT[(c * RY + b) * RX + a] is cell (x0 - 1 + a, y0 - 1 + b, z0 - 1 + c)),
+// and for each direction d the inner limited gradient of every cell that a
+// face's transverse gradient takes (util_diffusion.pyx:16-20), formed once
+// per cell instead of once per face that uses it.  Same expressions, same
+// bits as face_flux<AX>.
+template <int TXC, int TYC, int TZC>
+struct StageTab {
+  static constexpr int RX = TXC + 2, RY = TYC + 2, RZ = TZC + 2;
+  double T[RZ * RY * RX];
+  double gx[RZ * RY * TXC];  // cells a = 1..TXC (the tile's x range), all b, c
+  double gy[RZ * TYC * RX];  // cells b = 1..TYC, all a, c
+  double gz[TZC * RY * RX];  // cells c = 1..TZC, all a, b
+  __device__ int t(int a, int b, int c) const { return (c * RY + b) * RX + a; }
+  __device__ int ix(int a, int b, int c) const { return (c * RY + b) * TXC + a - 1; }
+  __device__ int iy(int a, int b, int c) const { return (c * TYC + b - 1) * RX + a; }
+  __device__ int iz(int a, int b, int c) const { return ((c - 1) * RY + b) * RX + a; }
+};
+
+// the AX face whose right cell is (x0 - 1 + a, y0 - 1 + b, z0 - 1 + c) = (i, j, k)
+template <int AX, int TXC, int TYC, int TZC>
+__device__ __forceinline__ double face_flux_tab(const GridDev& g, const double* __restrict__ w,
+                                                const double* __restrict__ bf, const StageTab<TXC, TYC, TZC>& S,
+                                                const DiffArgs& da, int i, int j, int k, int a, int b, int cz) {
+  const long long sy = g.nx, sz = (long long)g.nx * g.ny, sv = g.sv;
+  const double k0 = da.kappa0;
+  const double kappah = (2. * k0 * k0 / (k0 + k0 + SMALL_NUM));
+  const long long c = c3(g, i, j, k);
+  // the left cell's table coordinates
+  const int al = AX == 0 ? a - 1 : a, bl = AX == 1 ? b - 1 : b, cl = AX == 2 ? cz - 1 : cz;
+  double dTdx = 0., dTdy = 0., dTdz = 0., h, f;
+  if (AX == 0) dTdx = g.dlv_inv[0][i] * (S.T[S.t(a, b, cz)] - S.T[S.t(al, bl, cl)]);
+  if (AX == 1) dTdy = g.dlv_inv[1][j] * (S.T[S.t(a, b, cz)] - S.T[S.t(al, bl, cl)]);
+  if (AX == 2) dTdz = g.dlv_inv[2][k] * (S.T[S.t(a, b, cz)] - S.T[S.t(al, bl, cl)]);
+  double bxh, byh, bzh;
+  if (AX == 0) {
+    bxh = bf[c];
+    byh = 0.5 * (w[BY * sv + c - 1] + w[BY * sv + c]);
+    bzh = 0.5 * (w[BZ * sv + c - 1] + w[BZ * sv + c]);
+  } else if (AX == 1) {
+    byh = bf[sv + c];
+    bxh = 0.5 * (w[BX * sv + c - sy] + w[BX * sv + c]);
+    bzh = 0.5 * (w[BZ * sv + c - sy] + w[BZ * sv + c]);
+  } else {
+    bzh = bf[2 * sv + c];
+    bxh = 0.5 * (w[BX * sv + c - sz] + w[BX * sv + c]);
+    byh = 0.5 * (w[BY * sv + c - sz] + w[BY * sv + c]);
+  }
+#if BNZ_FAST_MATH
+  double bhi = rsqrt(bxh * bxh + byh * byh + bzh * bzh + SMALL_NUM);
+#else
+  double bhi = 1. / sqrt(bxh * bxh + byh * byh + bzh * bzh + SMALL_NUM);
+#endif
+  double bxh1 = bxh * bhi, byh1 = byh * bhi, bzh1 = bzh * bhi;
+  if (AX == 0) {
+    h = fabs(bxh1);
+    if (g.dims >= 2) dTdy = dlim(S.gy[S.iy(al, bl, cl)] * 1., S.gy[S.iy(a, b, cz)] * 1.);
+    if (g.dims >= 3) dTdz = dlim(S.gz[S.iz(al, bl, cl)] * 1. * 1., S.gz[S.iz(a, b, cz)] * 1. * 1.);
+    f = -kappah * bxh1 * (bxh1 * dTdx + byh1 * dTdy + bzh1 * dTdz);
+  } else if (AX == 1) {
+    h = fabs(byh1);
+    dTdx = dlim(S.gx[S.ix(al, bl, cl)], S.gx[S.ix(a, b, cz)]);
+    if (g.dims >= 3) dTdz = dlim(S.gz[S.iz(al, bl, cl)] * 1. * 1., S.gz[S.iz(a, b, cz)] * 1. * 1.);
+    f = -kappah * byh1 * (bxh1 * dTdx + byh1 * dTdy + bzh1 * dTdz);
+  } else {
+    h = fabs(bzh1);
+    dTdx = dlim(S.gx[S.ix(al, bl, cl)], S.gx[S.ix(a, b, cz)]);
+    dTdy = dlim(S.gy[S.iy(al, bl, cl)] * 1., S.gy[S.iy(a, b, cz)] * 1.);
+    f = -kappah * bzh1 * (bxh1 * dTdx + byh1 * dTdy + bzh1 * dTdz);
+  }
+  if (da.sat) f = saturate(f, h, S.T[S.t(al, bl, cl)], S.T[S.t(a, b, cz)], w[RHO * sv + c - (AX == 0 ? 1 : AX == 1 ? sy : sz)], w[RHO * sv + c]);
+  return f;
+}
+
 // The same stage on a tile of TXC x TYC x TZC cells per block: the tile's
 // face fluxes (each face once, the tile's far faces included) go to shared
 // memory, then every cell forms M(p) from its six faces and updates.  Face
 // values, divergence and update are the expressions of k_stage, so the two
 // kernels give the same bits; the tile forms 1 + 1/T of a flux per face
-// direction and cell instead of two.
+// direction and cell instead of two.  With the field-aligned flux the block
+// first stages T and each cell's limited transverse gradients (StageTab).
 template <int TXC, int TYC, int TZC>
 __global__ void __launch_bounds__(TXC * TYC * TZC) k_stage_tile(GridDev g, double* __restrict__ w,
                                                                  const double* __restrict__ bf,
@@ -193,25 +270,72 @@ __global__ void __launch_bounds__(TXC * TYC * TZC) k_stage_tile(GridDev g, doubl
                                                                  int3 hi, int first, double mu, double nu, double mut,
                                                                  double gamt, const double* dtp) {
   constexpr int NX = (TXC + 1) * TYC * TZC, NY = TXC * (TYC + 1) * TZC, NZ = TXC * TYC * (TZC + 1);
+  using Tab = StageTab<TXC, TYC, TZC>;
   __shared__ double sfx[NX], sfy[NY], sfz[NZ];
+  __shared__ Tab S;
   const int nbx = (hi.x - lo.x + TXC) / TXC, nby = (hi.y - lo.y + TYC) / TYC;
   const int bx = blockIdx.x % nbx, by = (blockIdx.x / nbx) % nby, bz = blockIdx.x / (nbx * nby);
   const int x0 = lo.x + bx * TXC, y0 = lo.y + by * TYC, z0 = lo.z + bz * TZC;
   const int wx = min(TXC, hi.x - x0 + 1), wy = min(TYC, hi.y - y0 + 1), wz = min(TZC, hi.z - z0 + 1);
   const int nfx = (wx + 1) * wy * wz, nfy = g.dims >= 2 ? wx * (wy + 1) * wz : 0,
             nfz = g.dims >= 3 ? wx * wy * (wz + 1) : 0;
+  if (da.aniso) {
+    // T on the tile and one cell around it (the grid's cells only)
+    for (int t = threadIdx.x; t < Tab::RX * Tab::RY * Tab::RZ; t += blockDim.x) {
+      const int a = t % Tab::RX, r = t / Tab::RX, b = r % Tab::RY, cz = r / Tab::RY;
+      const int x = x0 - 1 + a, y = y0 - 1 + b, z = z0 - 1 + cz;
+      if (x < g.nx && y < g.ny && z < g.nz) S.T[t] = T[c3(g, x, y, z)];
+    }
+    __syncthreads();
+    // each cell's inner limited gradient in each direction, where a face's
+    // transverse gradient takes it: x gradients of the tile's x range, and so
+    // on (the cell's own dvi, as face_flux<AX> forms them)
+    constexpr int NGX = Tab::RZ * Tab::RY * TXC, NGY = Tab::RZ * TYC * Tab::RX, NGZ = TZC * Tab::RY * Tab::RX;
+    for (int t = threadIdx.x; t < NGX + NGY + NGZ; t += blockDim.x) {
+      if (t < NGX) {
+        const int a = 1 + t % TXC, r = t / TXC, b = r % Tab::RY, cz = r / Tab::RY;
+        const int x = x0 - 1 + a, y = y0 - 1 + b, z = z0 - 1 + cz;
+        if (a > wx || y >= g.ny || z >= g.nz) continue;
+        S.gx[t] = dlim((S.T[S.t(a, b, cz)] - S.T[S.t(a - 1, b, cz)]) * g.dlv_inv[0][x],
+                       (S.T[S.t(a + 1, b, cz)] - S.T[S.t(a, b, cz)]) * g.dlv_inv[0][x + 1]);
+      } else if (t < NGX + NGY) {
+        if (g.dims < 2) continue;
+        const int u = t - NGX;
+        const int a = u % Tab::RX, r = u / Tab::RX, b = 1 + r % TYC, cz = r / TYC;
+        const int x = x0 - 1 + a, y = y0 - 1 + b, z = z0 - 1 + cz;
+        if (b > wy || x >= g.nx || z >= g.nz) continue;
+        S.gy[u] = dlim((S.T[S.t(a, b, cz)] - S.T[S.t(a, b - 1, cz)]) * g.dlv_inv[1][y],
+                       (S.T[S.t(a, b + 1, cz)] - S.T[S.t(a, b, cz)]) * g.dlv_inv[1][y + 1]);
+      } else {
+        if (g.dims < 3) continue;
+        const int u = t - NGX - NGY;
+        const int a = u % Tab::RX, r = u / Tab::RX, b = r % Tab::RY, cz = 1 + r / Tab::RY;
+        const int x = x0 - 1 + a, y = y0 - 1 + b, z = z0 - 1 + cz;
+        if (cz > wz || x >= g.nx || y >= g.ny) continue;
+        S.gz[u] = dlim((S.T[S.t(a, b, cz)] - S.T[S.t(a, b, cz - 1)]) * g.dlv_inv[2][z],
+                       (S.T[S.t(a, b, cz + 1)] - S.T[S.t(a, b, cz)]) * g.dlv_inv[2][z + 1]);
+      }
+    }
+    __syncthreads();
+  }
   for (int t = threadIdx.x; t < nfx + nfy + nfz; t += blockDim.x) {
     if (t < nfx) {
       const int fi = t % (wx + 1), r = t / (wx + 1), fj = r % wy, fk = r / wy;
-      sfx[(fk * TYC + fj) * (TXC + 1) + fi] = face_flux<0>(g, w, bf, T, da, x0 + fi, y0 + fj, z0 + fk);
+      sfx[(fk * TYC + fj) * (TXC + 1) + fi] =
+          da.aniso ? face_flux_tab<0>(g, w, bf, S, da, x0 + fi, y0 + fj, z0 + fk, fi + 1, fj + 1, fk + 1)
+                   : face_flux<0>(g, w, bf, T, da, x0 + fi, y0 + fj, z0 + fk);
     } else if (t < nfx + nfy) {
       const int u = t - nfx;
       const int fi = u % wx, r = u / wx, fj = r % (wy + 1), fk = r / (wy + 1);
-      sfy[(fk * (TYC + 1) + fj) * TXC + fi] = face_flux<1>(g, w, bf, T, da, x0 + fi, y0 + fj, z0 + fk);
+      sfy[(fk * (TYC + 1) + fj) * TXC + fi] =
+          da.aniso ? face_flux_tab<1>(g, w, bf, S, da, x0 + fi, y0 + fj, z0 + fk, fi + 1, fj + 1, fk + 1)
+                   : face_flux<1>(g, w, bf, T, da, x0 + fi, y0 + fj, z0 + fk);
     } else {
       const int u = t - nfx - nfy;
       const int fi = u % wx, r = u / wx, fj = r % wy, fk = r / wy;
-      sfz[(fk * TYC + fj) * TXC + fi] = face_flux<2>(g, w, bf, T, da, x0 + fi, y0 + fj, z0 + fk);
+      sfz[(fk * TYC + fj) * TXC + fi] =
+          da.aniso ? face_flux_tab<2>(g, w, bf, S, da, x0 + fi, y0 + fj, z0 + fk, fi + 1, fj + 1, fk + 1)
+                   : face_flux<2>(g, w, bf, T, da, x0 + fi, y0 + fj, z0 + fk);
     }
   }
   __syncthreads();
