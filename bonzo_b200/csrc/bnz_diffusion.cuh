@@ -277,8 +277,6 @@ __global__ void __launch_bounds__(TXC * TYC * TZC) k_stage_tile(GridDev g, doubl
   const int bx = blockIdx.x % nbx, by = (blockIdx.x / nbx) % nby, bz = blockIdx.x / (nbx * nby);
   const int x0 = lo.x + bx * TXC, y0 = lo.y + by * TYC, z0 = lo.z + bz * TZC;
   const int wx = min(TXC, hi.x - x0 + 1), wy = min(TYC, hi.y - y0 + 1), wz = min(TZC, hi.z - z0 + 1);
-  const int nfx = (wx + 1) * wy * wz, nfy = g.dims >= 2 ? wx * (wy + 1) * wz : 0,
-            nfz = g.dims >= 3 ? wx * wy * (wz + 1) : 0;
   if (da.aniso) {
     // T on the tile and one cell around it (the grid's cells only)
     for (int t = threadIdx.x; t < Tab::RX * Tab::RY * Tab::RZ; t += blockDim.x) {
@@ -318,24 +316,28 @@ __global__ void __launch_bounds__(TXC * TYC * TZC) k_stage_tile(GridDev g, doubl
     }
     __syncthreads();
   }
-  for (int t = threadIdx.x; t < nfx + nfy + nfz; t += blockDim.x) {
-    if (t < nfx) {
-      const int fi = t % (wx + 1), r = t / (wx + 1), fj = r % wy, fk = r / wy;
-      sfx[(fk * TYC + fj) * (TXC + 1) + fi] =
-          da.aniso ? face_flux_tab<0>(g, w, bf, S, da, x0 + fi, y0 + fj, z0 + fk, fi + 1, fj + 1, fk + 1)
-                   : face_flux<0>(g, w, bf, T, da, x0 + fi, y0 + fj, z0 + fk);
-    } else if (t < nfx + nfy) {
-      const int u = t - nfx;
-      const int fi = u % wx, r = u / wx, fj = r % (wy + 1), fk = r / (wy + 1);
-      sfy[(fk * (TYC + 1) + fj) * TXC + fi] =
-          da.aniso ? face_flux_tab<1>(g, w, bf, S, da, x0 + fi, y0 + fj, z0 + fk, fi + 1, fj + 1, fk + 1)
-                   : face_flux<1>(g, w, bf, T, da, x0 + fi, y0 + fj, z0 + fk);
+  // the faces of the full tile shape (compile-time index arithmetic); faces
+  // past a partial tile's extent are skipped
+  for (int t = threadIdx.x; t < NX + NY + NZ; t += blockDim.x) {
+    if (t < NX) {
+      const int fi = t % (TXC + 1), r = t / (TXC + 1), fj = r % TYC, fk = r / TYC;
+      if (fi > wx || fj >= wy || fk >= wz) continue;
+      sfx[t] = da.aniso ? face_flux_tab<0>(g, w, bf, S, da, x0 + fi, y0 + fj, z0 + fk, fi + 1, fj + 1, fk + 1)
+                        : face_flux<0>(g, w, bf, T, da, x0 + fi, y0 + fj, z0 + fk);
+    } else if (t < NX + NY) {
+      if (g.dims < 2) continue;
+      const int u = t - NX;
+      const int fi = u % TXC, r = u / TXC, fj = r % (TYC + 1), fk = r / (TYC + 1);
+      if (fi >= wx || fj > wy || fk >= wz) continue;
+      sfy[u] = da.aniso ? face_flux_tab<1>(g, w, bf, S, da, x0 + fi, y0 + fj, z0 + fk, fi + 1, fj + 1, fk + 1)
+                        : face_flux<1>(g, w, bf, T, da, x0 + fi, y0 + fj, z0 + fk);
     } else {
-      const int u = t - nfx - nfy;
-      const int fi = u % wx, r = u / wx, fj = r % wy, fk = r / wy;
-      sfz[(fk * TYC + fj) * TXC + fi] =
-          da.aniso ? face_flux_tab<2>(g, w, bf, S, da, x0 + fi, y0 + fj, z0 + fk, fi + 1, fj + 1, fk + 1)
-                   : face_flux<2>(g, w, bf, T, da, x0 + fi, y0 + fj, z0 + fk);
+      if (g.dims < 3) continue;
+      const int u = t - NX - NY;
+      const int fi = u % TXC, r = u / TXC, fj = r % TYC, fk = r / TYC;
+      if (fi >= wx || fj >= wy || fk > wz) continue;
+      sfz[u] = da.aniso ? face_flux_tab<2>(g, w, bf, S, da, x0 + fi, y0 + fj, z0 + fk, fi + 1, fj + 1, fk + 1)
+                        : face_flux<2>(g, w, bf, T, da, x0 + fi, y0 + fj, z0 + fk);
     }
   }
   __syncthreads();
