@@ -36,23 +36,27 @@ __device__ __forceinline__ void half_slopes_char_rt(int lim, const double* wm, c
   else half_slopes_char<LIM_VL>(wm, wc, wp, gam, d);
 }
 
+// Index boxes walk their cells with 32-bit unsigned arithmetic: a grid that
+// fits in device memory (at 66 doubles a cell or more for the paths that use
+// boxes, 180 GB hold about 340 M cells) has fewer than 2^31 cells, and 64-bit
+// division by a runtime divisor costs several times the 32-bit one.
 struct Box {
   int3 lo, hi;
-  __device__ __forceinline__ long long size() const {
-    return (long long)(hi.x - lo.x + 1) * (hi.y - lo.y + 1) * (hi.z - lo.z + 1);
+  __device__ __forceinline__ unsigned size() const {
+    return (unsigned)(hi.x - lo.x + 1) * (unsigned)(hi.y - lo.y + 1) * (unsigned)(hi.z - lo.z + 1);
   }
-  __device__ __forceinline__ void at(long long t, int& i, int& j, int& k) const {
-    int nxr = hi.x - lo.x + 1, nyr = hi.y - lo.y + 1;
-    i = lo.x + (int)(t % nxr);
-    long long r = t / nxr;
-    j = lo.y + (int)(r % nyr);
-    k = lo.z + (int)(r / nyr);
+  __device__ __forceinline__ void at(unsigned t, int& i, int& j, int& k) const {
+    const unsigned nxr = hi.x - lo.x + 1, nyr = hi.y - lo.y + 1;
+    const unsigned r = t / nxr, q = r / nyr;
+    i = lo.x + (int)(t - r * nxr);
+    j = lo.y + (int)(r - q * nyr);
+    k = lo.z + (int)q;
   }
 };
 
-#define BOX_LOOP(box, i, j, k)                                                                  \
-  for (long long _t = blockIdx.x * (long long)blockDim.x + threadIdx.x, _n = (box).size(); _t < _n; \
-       _t += (long long)gridDim.x * blockDim.x)                                                 \
+#define BOX_LOOP(box, i, j, k)                                                                   \
+  for (unsigned _t = blockIdx.x * blockDim.x + threadIdx.x, _n = (box).size(); _t < _n;          \
+       _t += gridDim.x * blockDim.x)                                                             \
     if (int i, j, k; (box).at(_t, i, j, k), true)
 
 // godunov.pyx:84-207: Godunov flux on the AX faces of `box` (face index along
