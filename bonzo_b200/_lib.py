@@ -172,7 +172,12 @@ _GRID_KEYS = ("Nx", "Ny", "Nz", "dims", "lmin", "lmax", "bc")
 
 
 class Context:
-    """One grid on the device (owns a bnz_ctx, or views an instance of a Batch)."""
+    """One grid on the device (owns a bnz_ctx, or views an instance of a Batch).
+
+    path: "fused" (the tile kernels: fastest for 2D PLM grids), "split" (per-axis
+    flux kernels and one fused update per stage: fastest for 1D and 3D grids) or
+    "plain" (one kernel per loop of the reference; the hydro build runs here).
+    The three give the same bits with exact_fp=True."""
 
     def __init__(self, Nx=None, Ny=1, Nz=1, dims=2, lmin=(0., 0., 0.), lmax=(1., 1., 1.),
                  bc=((0, 0), (0, 0), (0, 0)), _handle=None, _owner=None, **method):
