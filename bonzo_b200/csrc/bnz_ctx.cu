@@ -1693,8 +1693,15 @@ int bnz_batch_advance(bnz_batch* b, double tmax, int nsteps) {
       for (int s = 0; s < nsteps && rc == BNZ_OK; ++s) rc = batch_step_split(b, true);
     } else {
       if (!b->graph) {
+        long long before = 0;
+        for (const bnz_ctx* c : b->ctx) before += c->launches;
         CKB(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         rc = batch_step_split(b, false);
+        // the captured launches run at each replay, not at capture
+        long long after = 0;
+        for (const bnz_ctx* c : b->ctx) after += c->launches;
+        b->graph_launches = after - before;
+        b->launches -= b->graph_launches;
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(b->stream, &g);
         if (rc) {
@@ -1706,7 +1713,10 @@ int bnz_batch_advance(bnz_batch* b, double tmax, int nsteps) {
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return bfail(b, BNZ_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
       }
-      for (int s = 0; s < nsteps; ++s) CKB(cudaGraphLaunch(b->graph, b->stream));
+      for (int s = 0; s < nsteps; ++s) {
+        CKB(cudaGraphLaunch(b->graph, b->stream));
+        b->launches += b->graph_launches;
+      }
     }
     if (rc) return rc;
     CKB(cudaGetLastError());

@@ -230,6 +230,12 @@ def test_batch3d_split_tmax_and_graph():
     with pytest.raises(BnzError):
         b.advance_timed(1e30, 1)
     b.advance(1e30, 2)
+    # every replayed step counts its launches (dt, the split step and the
+    # boundary fill of each instance, the time record)
+    n0 = b.launch_count()
+    b.advance(1e30, 1)
+    per_step = b.launch_count() - n0
+    assert per_step >= 2 * (3 + 10 + 3 + 1)
     tmax = b[0].time()[0] + 0.004
     b.advance(tmax, 40)
     b.advance(tmax, 3)
@@ -237,7 +243,7 @@ def test_batch3d_split_tmax_and_graph():
         o = oracle_sim(grid, **meth)
         o.set_state(prim, bfld)
         o.init()
-        o.advance(1e30, max_steps=2)
+        o.advance(1e30, max_steps=3)
         o.advance(tmax)
         t, s, _ = b[q].time()
         assert t == tmax and s == o.nstep
