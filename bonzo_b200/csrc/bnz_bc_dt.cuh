@@ -129,6 +129,10 @@ __global__ void k_dt_finalize(DtState* ds, double cour, int clip) {
 
 __global__ void k_dt_set(DtState* ds, double dt) { ds->dt = dt; }
 
+// the fixed time step (vanleer.pyx:87-99 with fixdt), zero once the record's
+// time has reached tmax: the loop takes no further step
+__global__ void k_dt_fixed(DtState* ds, double dt) { ds->dt = ds->time >= ds->tmax ? 0. : dt; }
+
 // vanleer.pyx:166-167
 __global__ void k_time_advance(DtState* ds) {
   if (ds->dt > 0.) {

@@ -1043,7 +1043,7 @@ int bnz_advance_graph(bnz_ctx* c, double tmax, int nsteps) {
     } else {
       StepArgs a = step_args(c);
       if (!c->md.fixdt) c->launches += c->L->new_dt(a, c->prim, c->d_ds, c->md.cour, 1);
-      else c->launches += c->L->set_dt(c->stream, c->d_ds, c->md.dt_fixed);
+      else c->launches += c->L->fixed_dt(c->stream, c->d_ds, c->md.dt_fixed);
       rc = step_impl(c, 0.);
     }
     if (rc) return rc;
@@ -1657,7 +1657,7 @@ int batch_step_split(bnz_batch* b, bool host_dt) {
   for (bnz_ctx* c : b->ctx) {
     StepArgs a = step_args(c);
     if (!c->md.fixdt) c->launches += c->L->new_dt(a, c->prim, c->d_ds, c->md.cour, 1);
-    else c->launches += c->L->set_dt(c->stream, c->d_ds, c->md.dt_fixed);
+    else c->launches += c->L->fixed_dt(c->stream, c->d_ds, c->md.dt_fixed);
   }
   std::vector<DtState> ds(host_dt ? n : 0);
   if (host_dt) {

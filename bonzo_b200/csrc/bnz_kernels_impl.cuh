@@ -398,6 +398,11 @@ int set_dt(cudaStream_t s, DtState* ds, double dt) {
   bcdt::k_dt_set<<<1, 1, 0, s>>>(ds, dt);
   return 1;
 }
+
+int fixed_dt(cudaStream_t s, DtState* ds, double dt) {
+  bcdt::k_dt_fixed<<<1, 1, 0, s>>>(ds, dt);
+  return 1;
+}
 int time_advance(cudaStream_t s, DtState* ds) {
   bcdt::k_time_advance<<<1, 1, 0, s>>>(ds);
   return 1;

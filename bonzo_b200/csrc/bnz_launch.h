@@ -27,6 +27,7 @@ struct Launchers {
   int (*fused3_time)(const Fused3Launch&);
   int (*fused3_cds)(const Fused3Launch&, int parity);
   int (*split_predictor_corrector)(const StepArgs&, const double* dtp);
+  int (*fixed_dt)(cudaStream_t, DtState*, double);
 };
 
 #define BNZ_DECLARE_LAUNCHERS(NS)                                                                     \
@@ -53,6 +54,7 @@ struct Launchers {
   int fused3_time(const Fused3Launch&);                                                               \
   int fused3_cds(const Fused3Launch&, int parity);                                                    \
   int split_predictor_corrector(const StepArgs&, const double* dtp);                                \
+  int fixed_dt(cudaStream_t, DtState*, double);                                                      \
   extern const Launchers table;                                                                       \
   }
 
@@ -66,4 +68,4 @@ BNZ_DECLARE_LAUNCHERS(fast)
                                NS::new_dt, NS::set_dt, NS::time_advance, NS::diff_dt_max,            \
                                NS::diff_stage, NS::adj_step, NS::source,    \
                                NS::drive, NS::riemann_rows, NS::fused3_step, NS::fused3_time,        \
-                               NS::fused3_cds, NS::split_predictor_corrector};
+                               NS::fused3_cds, NS::split_predictor_corrector, NS::fixed_dt};

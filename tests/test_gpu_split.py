@@ -191,3 +191,32 @@ def test_split_nonphysical_state_is_reported():
         d.check()
     assert e.value.code == BNZ_ERR_STATE
     assert d.check() == 0
+
+
+@pytest.mark.parametrize("path", ["split", "plain", "fused"])
+@pytest.mark.parametrize("case,n", [("vortex", 32), ("turb3d", 12)])
+def test_fixed_dt_advance_matches_oracle(path, case, n):
+    """fixdt (vanleer.pyx:87-99): every step takes dt_fixed, with no clip to
+    tmax; the loop stops once the time has reached tmax.  The host loop on
+    every path, and graph stepping past tmax on the split and fused paths
+    (further steps take dt = 0 and leave the state as it is)."""
+    gc, prim, bfld, opts = setup_case(case, n=n)
+    kw = dict(fixdt=True, dt_fixed=1.25e-3)
+    tmax = 0.0106  # not a multiple of dt_fixed: the last step overshoots
+    o = oracle_sim(opts, **kw)
+    o.set_state(prim, bfld)
+    o.init()
+    o.advance(tmax)
+    runs = [("host", None)] + ([("graph", 14)] if path != "plain" else [])
+    for how, nsteps in runs:
+        d = device_ctx(opts, exact_fp=True, path=path, **kw)
+        d.set_state(prim, bfld)
+        d.init()
+        if how == "host":
+            d.advance(tmax)
+        else:
+            d.advance_graph(tmax, nsteps)
+        t, s, _ = d.time()
+        assert t == o.time and s == o.nstep, (how, t, o.time, s, o.nstep)
+        for a, b in zip(o.get_state(), d.get_state()):
+            assert np.array_equal(a, b), how
