@@ -33,7 +33,9 @@ CASES = [("vortex", 32, {}), ("vortex", 32, dict(rsolver="hll")), ("vortex", 32,
          ("vortex_pert", 32, dict(limiter="mc")), ("vortex_pert", 32, dict(limiter="mm")),
          ("vortex", 32, dict(reconstr="const")), ("blast", 33, {}), ("blast", 32, dict(outflow_face_aware=0)),
          ("blast_reflect", 29, {}), ("mixed_bc", 32, {}),
-         ("turb3d", 12, {}), ("cond2d", 32, {}), ("cond3d", 12, dict(sat_hfe=1)), ("wave1d", 64, {}),
+         ("turb3d", 12, {}), ("cond2d", 32, {}), ("cond3d", 12, dict(sat_hfe=1)),
+         ("cond3d", 12, dict(thcond_type="iso")), ("cond3d", 14, dict(thcond_type="iso", sat_hfe=1)),
+         ("wave1d", 64, {}),
          ("wave1d", 70, dict(reconstr="const")),
          ("vortex_pert", 32, dict(limiter="mc", charact_proj=1)), ("blast", 32, dict(charact_proj=1)),
          ("turb3d", 12, dict(charact_proj=1)), ("blast", 32, dict(grav=(0.3, -0.8, 0.0))),
