@@ -7,7 +7,7 @@ import os
 import numpy as np
 import pytest
 
-from sim_cases import write_cfg
+from sim_cases import write_cfg, write_cfg3d
 
 pytestmark = pytest.mark.gpu
 
@@ -93,3 +93,29 @@ def test_snapshot_equals_state(tmp_path):
     s.ctx.snapshot_wait()
     P2, U2, B2 = s.ctx.get_state()
     assert np.array_equal(P, P2) and np.array_equal(U, U2) and np.array_equal(B, B2)
+
+
+@pytest.mark.parametrize("kappa0", [0.0, 0.01])
+def test_simulation_3d_runs_on_split_path(tmp_path, kappa0):
+    """A 3D run from config.cfg goes through the split path and matches the
+    oracle (the facade's fast build: 1e-11 relative), conduction included."""
+    from bonzo_b200 import problems
+    from bonzo_b200._lib import PATH
+    from bonzo_b200.simulation import Simulation
+    from oracle.oracle import OracleSim
+    d = str(tmp_path)
+    write_cfg3d(d, n=16, tmax=0.01, kappa0=kappa0)
+    sim = Simulation(d)
+    assert sim.ctx.method_desc.path == PATH["split"]
+    prim, bfld = problems.turbulence3d(sim.grid.coord, seed=3, mach=0.5, kmax=4)
+    o = OracleSim(Nx=16, Ny=16, Nz=16, dims=3, bc=sim.grid.bc, gam=5. / 3, cour=0.3, rsolver="hlld", limiter="vl",
+                  kappa0=kappa0)
+    o.set_state(prim, bfld)
+    o.init()
+    sim.advance()
+    o.advance(0.01)
+    P, U, B = o.get_state()
+    assert sim.integr.step == o.nstep and abs(sim.integr.time - 0.01) < 1e-15
+    for a, b in ((sim.prim, P), (sim.cons, U), (sim.bfld, B)):
+        for v in range(a.shape[0]):
+            assert np.abs(a[v] - b[v]).max() <= 1e-11 * max(np.abs(b[v]).max(), 1e-300)
