@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(256, 2) k_flux_tile(GridDev g, const double* _
 // computes, since a cell's loads outnumber what its registers hold in flight.
 // (Staging each tile's inputs in shared memory by asynchronous copies first
 // measured slower: 2.3 and 0.66 ms per 256^3 launch against 1.8 and 0.47.)
-constexpr int UPD_KZ = 8;
+constexpr int UPD_KZ = 16;
 
 __device__ __forceinline__ void prefetch_l2(const double* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
