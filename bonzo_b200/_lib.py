@@ -176,7 +176,8 @@ class Context:
 
     path: "fused" (the tile kernels: fastest for 2D PLM grids), "split" (per-axis
     flux kernels and one fused update per stage: fastest for 1D and 3D grids) or
-    "plain" (one kernel per loop of the reference; the hydro build runs here).
+    "plain" (one kernel per loop of the reference).  The hydro build runs on
+    "plain" and "split".
     The three give the same bits with exact_fp=True."""
 
     def __init__(self, Nx=None, Ny=1, Nz=1, dims=2, lmin=(0., 0., 0.), lmax=(1., 1., 1.),

@@ -466,7 +466,7 @@ int validate(const bnz_grid_desc* g, const bnz_method_desc* m, std::string& why)
     // the reference's hydro build (MFIELD 0, src/defs_c.h:72-96): hll or hllc
     if (m->rsolver != BNZ_RS_HLL && m->rsolver != BNZ_RS_HLLC)
       return why = "rsolver must be hll or hllc in hydro mode (hlld needs a magnetic field)", 0;
-    if (m->path != BNZ_PATH_PLAIN) return why = "hydro mode runs on the plain path", 0;
+    if (m->path == BNZ_PATH_FUSED) return why = "hydro mode runs on the plain path or the split path", 0;
     if (m->charact_proj) return why = "charact_proj is not available in hydro mode", 0;
     if (m->kappa0 != 0.) return why = "field-aligned conduction needs a magnetic field (kappa0 = 0 in hydro mode)", 0;
   } else if (m->rsolver != BNZ_RS_HLL && m->rsolver != BNZ_RS_HLLD && m->rsolver != BNZ_RS_HLLT) {

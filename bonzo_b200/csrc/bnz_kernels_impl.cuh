@@ -274,6 +274,14 @@ int split_flux(const StepArgs& a, const SplitSrc& s, const double* bf, const pla
       split::k_flux_tile<AX, ORDER, dev::RS_HLLT><<<nblk, T::NT, 0, a.stream>>>(
           a.g, s.w, s.wfb, s.vlo, s.vhi, bf, a.flx[AX], b, a.limiter, a.charact_proj, a.err);
       break;
+    case dev::RS_HLLC:
+      split::k_flux_tile<AX, ORDER, dev::RS_HLLC><<<nblk, T::NT, 0, a.stream>>>(
+          a.g, s.w, s.wfb, s.vlo, s.vhi, bf, a.flx[AX], b, a.limiter, a.charact_proj, a.err);
+      break;
+    case dev::RS_HLL_HYDRO:
+      split::k_flux_tile<AX, ORDER, dev::RS_HLL_HYDRO><<<nblk, T::NT, 0, a.stream>>>(
+          a.g, s.w, s.wfb, s.vlo, s.vhi, bf, a.flx[AX], b, a.limiter, a.charact_proj, a.err);
+      break;
     default:
       split::k_flux_tile<AX, ORDER, dev::RS_HLL><<<nblk, T::NT, 0, a.stream>>>(
           a.g, s.w, s.wfb, s.vlo, s.vhi, bf, a.flx[AX], b, a.limiter, a.charact_proj, a.err);
@@ -327,9 +335,10 @@ int split_stage(const StepArgs& a, const SplitSrc& s, double* w1, double* b1, co
 // split path forms the cell EMFs on the fly), so that the corrector can
 // update a.bfld in place of a neighbour's reads: it reads b^n from the copy.
 // The conserved state is not written: the context forms it from prim after
-// the boundary fill, when it is asked for.
+// the boundary fill, when it is asked for.  In the hydro build (field entries
+// and face field held at zero, the hydro solvers' field fluxes zero) the same
+// launches run and the field stays zero.
 int split_predictor_corrector(const StepArgs& a, const double* dtp) {
-  if (a.hydro) return 0;
   const GridDev& g = a.g;
   const int N[3] = {g.nx, g.ny, g.nz};
   int lo[3], hi[3];

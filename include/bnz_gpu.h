@@ -48,8 +48,8 @@ enum { BNZ_BC_PERIODIC = 0, BNZ_BC_OUTFLOW = 1, BNZ_BC_REFLECT = 2 };
 enum { BNZ_TC_ISO = 0, BNZ_TC_ANISO = 1 };
 /* kernel path: fused tile kernels (default), one kernel per reference loop
  * (plain), or the plain path's decomposition with each face's flux formed once
- * from per-cell slopes and one fused update per stage (split; not in hydro
- * mode).  All three give the same bits in the exact build. */
+ * from per-cell slopes and one fused update per stage (split).  All three
+ * give the same bits in the exact build; hydro mode runs on plain or split. */
 enum { BNZ_PATH_FUSED = 0, BNZ_PATH_PLAIN = 1, BNZ_PATH_SPLIT = 2 };
 
 /* Grid: the [computation] Nx..Nz / xmin..zmax keys and the [physics]
@@ -78,7 +78,8 @@ typedef struct {
  * hydro = 1 is the reference's hydro build (MFIELD 0, src/defs_c.h:72-96):
  * the field entries of prim / cons and the face field are held at zero, no CT
  * runs, signal speeds are the hydro sound speed, and rsolver is hll or hllc
- * (fluxes_c.c:175-223, 232-327); plain path, no charact_proj, no conduction. */
+ * (fluxes_c.c:175-223, 232-327); plain or split path, no charact_proj, no
+ * conduction. */
 typedef struct {
   double gam, cour;
   int rsolver, reconstr, limiter, charact_proj;

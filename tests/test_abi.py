@@ -69,7 +69,6 @@ def _try_create(**kw):
     (dict(path=5), "path"),
     (dict(hydro=1, rsolver=2), "hydro mode"),
     (dict(hydro=1, rsolver=1, path=0), "plain path"),
-    (dict(hydro=1, rsolver=1, path=2), "plain path"),
     (dict(hydro=1, rsolver=1, charact_proj=1), "charact_proj"),
     (dict(hydro=1, rsolver=0, kappa0=0.1), "conduction"),
     (dict(hydro=3, rsolver=1), "hydro"),

@@ -2,7 +2,8 @@
 
 The reference compiles HLLC only without a magnetic field (fluxes_c.c:230-327
 under #if !MFIELD).  The device's hydro mode holds the field at zero, skips
-constrained transport and uses the hydro sound speed; its kernels must equal
+constrained transport on the plain path (the split path runs it on zero
+fields) and uses the hydro sound speed; its kernels must equal
 the reference's hydro-build kernels (tests/golden/kernels_hydro.npz, made by
 the reference's own compiled code) bit for bit in the exact build, and its
 steps the oracle's hydro build.  The device Riemann entry point (the
@@ -61,13 +62,14 @@ def _hydro_case(n, dims=2, bc=1, seed=0):
     return gc, prim, bfld, opts
 
 
+@pytest.mark.parametrize("path", ["plain", "split"])
 @pytest.mark.parametrize("rs,limiter,dims,bc", [("hllc", "vl", 2, 1), ("hllc", "mc", 2, 0), ("hll", "vl", 2, 1),
                                                  ("hllc", "mm", 3, 0), ("hll", "mc", 3, 1), ("hllc", "vl", 2, 2)])
-def test_hydro_step_bitwise_vs_oracle(rs, limiter, dims, bc):
+def test_hydro_step_bitwise_vs_oracle(rs, limiter, dims, bc, path):
     n = 40 if dims == 2 else 14
     gc, prim, bfld, opts = _hydro_case(n, dims, bc)
     o = oracle_sim(opts, rsolver=rs, limiter=limiter, hydro=True)
-    d = device_ctx(opts, rsolver=rs, limiter=limiter, hydro=True, exact_fp=True, path="plain")
+    d = device_ctx(opts, rsolver=rs, limiter=limiter, hydro=True, exact_fp=True, path=path)
     o.set_state(prim[:6], bfld)
     d.set_state(prim, bfld)
     o.init()
@@ -85,10 +87,11 @@ def test_hydro_step_bitwise_vs_oracle(rs, limiter, dims, bc):
     assert d.check() == 0
 
 
-def test_hydro_fast_100_steps_vs_oracle():
+@pytest.mark.parametrize("path", ["plain", "split"])
+def test_hydro_fast_100_steps_vs_oracle(path):
     gc, prim, bfld, opts = _hydro_case(96, 2, 1, seed=3)
     o = oracle_sim(opts, rsolver="hllc", hydro=True)
-    d = device_ctx(opts, rsolver="hllc", hydro=True, path="plain")
+    d = device_ctx(opts, rsolver="hllc", hydro=True, path=path)
     o.set_state(prim[:6], bfld)
     d.set_state(prim, bfld)
     o.init()
