@@ -61,14 +61,26 @@ __device__ __forceinline__ int ax_of(int3 v, int a) { return a == 0 ? v.x : a ==
 // quotient 2ab/(a+b) is 2ab times the Newton-refined reciprocal of a + b
 // (bnz_fastmath.cuh: within 2 ulp; ab > 0 makes a and b one-signed, so
 // |a + b| >= 2 sqrt(ab) is a normal number)
-__device__ __forceinline__ double half_slope_split(int lim, double wm, double wc, double wp) {
+template <int LIM>
+__device__ __forceinline__ double half_slope_split(double wm, double wc, double wp) {
 #if BNZ_FAST_MATH
-  if (lim == LIM_VL) {
+  if (LIM == LIM_VL) {
     const double a = wc - wm, b = wp - wc, ab = a * b;
     return 0.5 * ((ab > 0.) ? (2. * ab) * bnz_nr_rcp(a + b) : 0.);
   }
 #endif
-  return plain::half_slope_rt(lim, wm, wc, wp);
+  return half_slope<LIM>(wm, wc, wp);
+}
+
+// the eight half slopes (all but the normal field) of the staged cell at p
+// into the slope table, one limiter for the whole loop
+template <int LIM, class T>
+__device__ __forceinline__ void cell_slopes(const double* p, double* sD, int la, int lb) {
+#pragma unroll
+  for (int n = 0; n < NM; ++n) {
+    if (n == BX) continue;
+    sD[T::ds(slot8(n), la, lb)] = half_slope_split<LIM>(p[n * T::WN - T::DA], p[n * T::WN], p[n * T::WN + T::DA]);
+  }
 }
 
 // Fluxes of the AX faces of `box` (face index along AX = the cell on its
@@ -130,12 +142,12 @@ __global__ void __launch_bounds__(256, 2) k_flux_tile(GridDev g, const double* _
 #pragma unroll
         for (int n = 0; n < NM; ++n)
           if (n != BX) sD[T::ds(slot8(n), la, lb)] = d[n];
+      } else if (lim == LIM_MC) {
+        cell_slopes<LIM_MC, T>(p, sD, la, lb);
+      } else if (lim == LIM_MM) {
+        cell_slopes<LIM_MM, T>(p, sD, la, lb);
       } else {
-#pragma unroll
-        for (int n = 0; n < NM; ++n) {
-          if (n == BX) continue;
-          sD[T::ds(slot8(n), la, lb)] = half_slope_split(lim, p[n * WN - DA], p[n * WN], p[n * WN + DA]);
-        }
+        cell_slopes<LIM_VL, T>(p, sD, la, lb);
       }
     }
     __syncthreads();
