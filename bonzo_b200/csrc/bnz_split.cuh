@@ -7,7 +7,8 @@
 //   * k_flux_tile: a block stages a pencil tile of cells (NB lines of NA faces
 //     along the sweep axis, with the two-cell halo) in shared memory and forms
 //     every cell's PLM half slopes once (reconstr_c.c:54-91), where
-//     plain::k_flux forms both one-sided slopes of every face itself;
+//     plain::k_flux forms both one-sided slopes of every face itself (the
+//     donor-cell predictor, with no slopes to share, keeps plain::k_flux);
 //   * k_ee forms the cell-centred EMF (ct.pyx:128-148) of the cells it needs
 //     on the fly instead of reading a separate array;
 //   * k_update: per cell, prim2cons of the step's input, the conservative
@@ -19,8 +20,10 @@
 // A face is formed by exactly one block and no kernel waits on a barrier
 // between Riemann solves (what bounds the z-marching chunk kernels).  Every
 // expression is the plain path's, so the exact build is bitwise equal to it
-// and to the oracle.  Included inside the per-floating-point-mode namespace,
-// after bnz_plain.cuh and bnz_source.cuh.
+// and to the oracle (the fast build's van Leer limiter differs: see
+// half_slope_split).  The hydro build runs the same launches on zero fields.
+// Included inside the per-floating-point-mode namespace, after bnz_plain.cuh
+// and bnz_source.cuh.
 #pragma once
 
 namespace split {
