@@ -44,6 +44,9 @@ struct StepArgs {
   const double* fdriv;
   int src;  // any source term on
   int hydro;  // the reference's hydro build (MFIELD 0): no field, no CT
+  // split path, 3D grids with even Ntot_x: the tensor maps of the update
+  // kernel's TMA boxes (split::TM_COUNT maps of 128 bytes), or null
+  const unsigned char* smaps;
 };
 
 // Device time-step record used by graph-captured stepping.

@@ -112,6 +112,7 @@ StepArgs step_args(bnz_ctx* c) {
   a.fdriv = c->fdriv;
   a.src = src_on(c->md) ? 1 : 0;
   a.hydro = c->md.hydro ? 1 : 0;
+  a.smaps = c->d_smaps;
   // the hydro build's HLL takes the hydro sound speed
   if (a.hydro && a.rsolver == BNZ_RS_HLL) a.rsolver = 4;  // dev::RS_HLL_HYDRO
   return a;
@@ -204,9 +205,11 @@ void free_all(bnz_ctx* c) {
   if (c->d_inst3) cudaFree(c->d_inst3);
   if (c->d_tiles3) cudaFree(c->d_tiles3);
   if (c->d_map3) cudaFree(c->d_map3);
+  if (c->d_smaps) cudaFree(c->d_smaps);
   c->d_inst3 = nullptr;
   c->d_tiles3 = nullptr;
   c->d_map3 = nullptr;
+  c->d_smaps = nullptr;
   if (c->graph) cudaGraphExecDestroy(c->graph);
   if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
   c->d_err = nullptr;
@@ -648,7 +651,9 @@ int bnz_create(const bnz_grid_desc* gd, const bnz_method_desc* md, bnz_ctx** out
   }
   e = cudaMalloc((void**)&c->d_err, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_ds, sizeof(DtState));
-  if (e == cudaSuccess && md->path == BNZ_PATH_FUSED && dims == 3) {
+  if (e == cudaSuccess && md->path == BNZ_PATH_SPLIT && dims == 3) {
+    e = build_split_maps(c);
+  } else if (e == cudaSuccess && md->path == BNZ_PATH_FUSED && dims == 3) {
     e = build_ctx3(c);
   } else if (e == cudaSuccess && md->path == BNZ_PATH_FUSED) {
     e = build_ctx_tiles(c);
@@ -1305,6 +1310,38 @@ bool cell_map(const bnz_ctx* c, const double* base, int nf, int bw, int bh, CUte
 }  // namespace
 
 namespace bnzi {
+// A 4D map (x, y, z, field) over an nft-field array of a 3D context, with
+// boxes of 34 x 9 cells (split::TW x TH), bz planes and bf fields: the split
+// update kernel's TMA boxes.  Needs even Ntot_x (16-byte strides).
+bool split_map(const bnz_ctx* c, const double* base, int nft, int bz, int bf, void* map128) {
+  EncodeTiledFn enc = encode_tiled();
+  const int nx = c->Ntot[0], ny = c->Ntot[1], nz = c->Ntot[2];
+  if (!enc || (nx & 1) || ((uintptr_t)base & 15)) return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)nft};
+  const cuuint64_t strides[3] = {(cuuint64_t)nx * sizeof(double), (cuuint64_t)nx * ny * sizeof(double),
+                                 (cuuint64_t)nx * ny * nz * sizeof(double)};
+  const cuuint32_t box[4] = {34, 9, (cuuint32_t)bz, (cuuint32_t)bf};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  return enc(static_cast<CUtensorMap*>(map128), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void*)base, dims, strides, box,
+             es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The split update kernel's maps (prim, the three flux arrays, bfld, the b^n
+// copy in ec, ee; the order of split::TM_*) into device memory, when every
+// map can be made.
+cudaError_t build_split_maps(bnz_ctx* c) {
+  CUtensorMap m[7];
+  const bool ok = split_map(c, c->prim, 9, 1, 9, &m[0]) && split_map(c, c->flx[0], 9, 1, 6, &m[1]) &&
+                  split_map(c, c->flx[1], 9, 1, 6, &m[2]) && split_map(c, c->flx[2], 9, 2, 6, &m[3]) &&
+                  split_map(c, c->bfld, 3, 2, 3, &m[4]) && split_map(c, c->ec, 3, 2, 3, &m[5]) &&
+                  split_map(c, c->ee, 3, 2, 3, &m[6]);
+  if (!ok) return cudaSuccess;  // the kernel without TMA runs
+  cudaError_t e = cudaMalloc((void**)&c->d_smaps, sizeof m);
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_smaps, m, sizeof m, cudaMemcpyHostToDevice);
+  return e;
+}
+
 bool ws_map3(const bnz_ctx* c, const double* base, void* map128) {
   EncodeTiledFn enc = encode_tiled();
   const int nx = c->Ntot[0], ny = c->Ntot[1], nz = c->Ntot[2];

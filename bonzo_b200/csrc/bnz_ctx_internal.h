@@ -48,6 +48,7 @@ struct bnz_ctx {
   FusedTile3* d_tiles3 = nullptr;
   int ntA3 = 0, ntB3 = 0;
   unsigned char* d_map3 = nullptr;
+  unsigned char* d_smaps = nullptr;  // split path, 3D: the update kernel's tensor maps
   int graph_parity = -1;
   int variant = 0;
   // conduction scratch
@@ -100,6 +101,7 @@ void make_tiles3(int inst, const int* N, int ng, bool pred, int tx, int ty, int 
 // the 3D corrector's staging box; false when Ntot_x is odd or the driver
 // entry point is missing
 bool ws_map3(const bnz_ctx* c, const double* base, void* map128);
+cudaError_t build_split_maps(bnz_ctx* c);
 bool fused_available(const bnz_grid_desc* g, const bnz_method_desc* m);
 void set_parity(bnz_ctx* c, int p);
 int ensure_ghosts(bnz_ctx* c);

@@ -21,6 +21,7 @@ namespace BNZ_NS {
 #include "bnz_split.cuh"
 #include "bnz_fused.cuh"
 #include "bnz_fused3d.cuh"
+#include "bnz_split_tma.cuh"
 #include "bnz_adjoint_math.h"
 #include "bnz_adjoint.cuh"
 
@@ -320,6 +321,24 @@ int split_stage(const StepArgs& a, const SplitSrc& s, double* w1, double* b1, co
                                                              a.flx[2], a.ee, b);
   }
   plain::Box b = mkbox(il, iu, jl, ju, kl, ku);
+  if (g.dims == 3 && a.smaps) {
+    // the TMA-fed form (3D, even Ntot_x): blocks of 32 x 8 columns from an
+    // even first column, split::UPD_KZ planes each
+    constexpr size_t sm = sizeof(split::TmaSmem);
+    static bool attr = false;  // once per floating-point build
+    if (!attr) {
+      cudaFuncSetAttribute(split::k_update_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      attr = true;
+    }
+    const int x0base = b.lo.x & ~1;
+    const dim3 grid((b.hi.x - x0base + 32) / 32, (b.hi.y - b.lo.y + 8) / 8,
+                    (b.hi.z - b.lo.z + split::UPD_KZ) / split::UPD_KZ);
+    const int b0map = b0 == a.bfld ? split::TM_BFLD : split::TM_BSAVE;
+    split::k_update_tma<<<grid, dim3(32, 8), sm, a.stream>>>(g, w1, s.w, b1, bsave, a.smaps, b0map, b, x0base, dtp,
+                                                             fac, a.src, a.grav[0], a.grav[1], a.grav[2], a.fdriv,
+                                                             a.err);
+    return nl + 2;
+  }
   split::k_update<<<cell_grid(b), dim3(32, 8), 0, a.stream>>>(
       g, w1, a.prim, s.w, b1, b0, bsave, a.flx[0], a.flx[1], a.flx[2], a.ee, b, dtp, fac, a.src, a.grav[0],
       a.grav[1], a.grav[2], a.fdriv, a.err);

@@ -111,7 +111,8 @@ def test_split_golden_steps_bitwise(case):
 @pytest.mark.parametrize("case,n", [("vortex_pert", 32), ("turb3d", 12)])
 def test_split_driving_equals_plain(case, n):
     """With the driving force (device sin/cos) and gravity on, the split and
-    plain paths of the same build agree bit for bit."""
+    plain paths agree bit for bit in the exact build (and to the parity
+    tolerance in the fast one)."""
     gc, prim, bfld, opts = setup_case(case, n=n)
     kw = dict(grav=(0.0, -0.4, 0.1), drive_f0=0.8, drive_tau=0.05, drive_nmod=1, drive_seed=11)
     for exact in (True, False):
@@ -122,7 +123,11 @@ def test_split_driving_equals_plain(case, n):
             s.init()
         for _ in range(4):
             dt = a.new_dt()
-            assert b.new_dt() == dt
+            if exact:
+                assert b.new_dt() == dt
+            else:
+                # the fast build contracts the paths' expressions differently
+                assert abs(b.new_dt() - dt) <= 1e-13 * dt
             a.step(dt)
             b.step(dt)
         Pa, Ua, Ba = a.get_state()
