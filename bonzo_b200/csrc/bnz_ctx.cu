@@ -1311,31 +1311,34 @@ bool cell_map(const bnz_ctx* c, const double* base, int nf, int bw, int bh, CUte
 
 namespace bnzi {
 // A 4D map (x, y, z, field) over an nft-field array of a 3D context, with
-// boxes of 34 x 9 cells (split::TW x TH), bz planes and bf fields: the split
-// update kernel's TMA boxes.  Needs even Ntot_x (16-byte strides).
-bool split_map(const bnz_ctx* c, const double* base, int nft, int bz, int bf, void* map128) {
+// boxes of bx x by x bz cells and bf fields: the split kernels' TMA boxes.
+// Needs even Ntot_x (16-byte strides).
+bool split_map(const bnz_ctx* c, const double* base, int nft, int bx, int by, int bz, int bf, void* map128) {
   EncodeTiledFn enc = encode_tiled();
   const int nx = c->Ntot[0], ny = c->Ntot[1], nz = c->Ntot[2];
   if (!enc || (nx & 1) || ((uintptr_t)base & 15)) return false;
   const cuuint64_t dims[4] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)nft};
   const cuuint64_t strides[3] = {(cuuint64_t)nx * sizeof(double), (cuuint64_t)nx * ny * sizeof(double),
                                  (cuuint64_t)nx * ny * nz * sizeof(double)};
-  const cuuint32_t box[4] = {34, 9, (cuuint32_t)bz, (cuuint32_t)bf};
+  const cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz, (cuuint32_t)bf};
   const cuuint32_t es[4] = {1, 1, 1, 1};
   return enc(static_cast<CUtensorMap*>(map128), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void*)base, dims, strides, box,
              es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// The split update kernel's maps (prim, the three flux arrays, bfld, the b^n
-// copy in ec, ee; the order of split::TM_*) into device memory, when every
-// map can be made.
+// The split kernels' maps into device memory, when every map can be made, in
+// the order of split::TM_*: for the update (boxes of 34 x 9 cells, 1 or 2
+// planes) prim, the three flux arrays, bfld, the b^n copy in ec, ee; for the
+// corrector's PLM flux tiles, the predictor's prim in cons_s in the boxes of
+// the x (34 x 8 x 1), y (16 x 18 x 1) and z (16 x 1 x 18) sweeps.
 cudaError_t build_split_maps(bnz_ctx* c) {
-  CUtensorMap m[7];
-  const bool ok = split_map(c, c->prim, 9, 1, 9, &m[0]) && split_map(c, c->flx[0], 9, 1, 6, &m[1]) &&
-                  split_map(c, c->flx[1], 9, 1, 6, &m[2]) && split_map(c, c->flx[2], 9, 2, 6, &m[3]) &&
-                  split_map(c, c->bfld, 3, 2, 3, &m[4]) && split_map(c, c->ec, 3, 2, 3, &m[5]) &&
-                  split_map(c, c->ee, 3, 2, 3, &m[6]);
+  CUtensorMap m[10];
+  const bool ok = split_map(c, c->prim, 9, 34, 9, 1, 9, &m[0]) && split_map(c, c->flx[0], 9, 34, 9, 1, 6, &m[1]) &&
+                  split_map(c, c->flx[1], 9, 34, 9, 1, 6, &m[2]) && split_map(c, c->flx[2], 9, 34, 9, 2, 6, &m[3]) &&
+                  split_map(c, c->bfld, 3, 34, 9, 2, 3, &m[4]) && split_map(c, c->ec, 3, 34, 9, 2, 3, &m[5]) &&
+                  split_map(c, c->ee, 3, 34, 9, 2, 3, &m[6]) && split_map(c, c->cons_s, 9, 34, 8, 1, 9, &m[7]) &&
+                  split_map(c, c->cons_s, 9, 16, 18, 1, 9, &m[8]) && split_map(c, c->cons_s, 9, 16, 1, 18, 9, &m[9]);
   if (!ok) return cudaSuccess;  // the kernel without TMA runs
   cudaError_t e = cudaMalloc((void**)&c->d_smaps, sizeof m);
   if (e == cudaSuccess) e = cudaMemcpy(c->d_smaps, m, sizeof m, cudaMemcpyHostToDevice);

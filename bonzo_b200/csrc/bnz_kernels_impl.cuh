@@ -246,6 +246,16 @@ int plain_predictor_corrector(const StepArgs& a, const double* dtp) {
   return nl + 2;
 }
 
+// SM count of the current device (cached per device).
+inline int sm_count() {
+  static int nsm[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (!nsm[dev]) cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
+  return std::max(1, nsm[dev]);
+}
+
 namespace {
 // Blocks of 32 x 8 cells of the box, split::UPD_KZ z indices each.
 inline dim3 cell_grid(const plain::Box& b) {
@@ -260,9 +270,44 @@ struct SplitSrc {
   int3 vlo, vhi;
 };
 
+// The corrector's PLM fluxes of a 3D grid with tensor maps: a persistent
+// kernel of two blocks per SM (at most one per tile), each tile one TMA box of
+// the predictor's prim (x sweep: first face column even).
+template <int AX, int RS>
+void launch_flux_tma(const StepArgs& a, const SplitSrc& s, const double* bf, const plain::Box& b, unsigned nblk) {
+  constexpr size_t sm = sizeof(split::FluxSmem<AX>);
+  static bool attr = false;  // once per kernel
+  if (!attr) {
+    cudaFuncSetAttribute(split::k_flux_tile_tma<AX, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    attr = true;
+  }
+  split::k_flux_tile_tma<AX, RS><<<nblk, 256, sm, a.stream>>>(a.g, a.smaps, s.wfb, s.vlo, s.vhi, bf, a.flx[AX], b,
+                                                              a.limiter, a.charact_proj, a.err);
+}
+
+template <int AX>
+int split_flux_tma(const StepArgs& a, const SplitSrc& s, const double* bf, const plain::Box& b) {
+  using T = split::FTT<AX>;
+  const int lo[3] = {b.lo.x, b.lo.y, b.lo.z}, hi[3] = {b.hi.x, b.hi.y, b.hi.z};
+  const int lb0 = AX == 0 ? lo[T::TAX] : (lo[T::TAX] & ~1);
+  const long long na = (hi[AX] - lo[AX] + T::NA) / T::NA, nb = (hi[T::TAX] - lb0 + T::NB) / T::NB;
+  const long long ntile = na * nb * (hi[T::OAX] - lo[T::OAX] + 1);
+  const unsigned nblk = (unsigned)std::min<long long>(ntile, 2LL * sm_count());
+  switch (a.rsolver) {
+    case dev::RS_HLLD: launch_flux_tma<AX, dev::RS_HLLD>(a, s, bf, b, nblk); break;
+    case dev::RS_HLLT: launch_flux_tma<AX, dev::RS_HLLT>(a, s, bf, b, nblk); break;
+    case dev::RS_HLLC: launch_flux_tma<AX, dev::RS_HLLC>(a, s, bf, b, nblk); break;
+    case dev::RS_HLL_HYDRO: launch_flux_tma<AX, dev::RS_HLL_HYDRO>(a, s, bf, b, nblk); break;
+    default: launch_flux_tma<AX, dev::RS_HLL>(a, s, bf, b, nblk); break;
+  }
+  return 1;
+}
+
 template <int AX, int ORDER>
 int split_flux(const StepArgs& a, const SplitSrc& s, const double* bf, const plain::Box& b) {
   using T = split::FT<AX>;
+  if (ORDER == 1 && a.g.dims == 3 && a.smaps && s.w == a.cons_s && (AX != 0 || (b.lo.x & 1) == 0))
+    return split_flux_tma<AX>(a, s, bf, b);
   const int lo[3] = {b.lo.x, b.lo.y, b.lo.z}, hi[3] = {b.hi.x, b.hi.y, b.hi.z};
   const long long na = (hi[AX] - lo[AX] + T::NA) / T::NA, nb = (hi[T::TAX] - lo[T::TAX] + T::NB) / T::NB;
   const unsigned nblk = (unsigned)(na * nb * (hi[T::OAX] - lo[T::OAX] + 1));
@@ -481,16 +526,6 @@ void launch_corr(const FusedLaunch& f, int parity) {
     attrs = true;
   }
   fused::k_corr2d<TX, TY, RS, LIM><<<f.ntB, 256, smB, f.stream>>>(f.insts, f.tilesB, parity, f.charact_proj);
-}
-
-// SM count of the current device (cached per device).
-inline int sm_count() {
-  static int nsm[64] = {0};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64) dev = 0;
-  if (!nsm[dev]) cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
-  return std::max(1, nsm[dev]);
 }
 
 // Persistent corrector: (SMs x resident blocks) blocks, never more than tiles.
