@@ -62,10 +62,14 @@ __global__ void k_bc_axis(GridDev g, int ax, double* prim, double* bfld, FieldLi
   const bool face_normal = (f >= NM) && (f - NM == ax);
   const bool normal_cell = (f == VX + ax) || (f == BX + ax);
   const long long st[3] = {1, g.nx, (long long)g.nx * g.ny};
+  // along x the ghost layers of a row are neighbours in memory: the layer is
+  // the fastest index there, so that a warp reads and writes a few rows'
+  // ends instead of one double per row
+  const long long nl = 2LL * ng;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < per_field;
        t += (long long)gridDim.x * blockDim.x) {
-    long long rest = t % nother;
-    int layer = (int)(t / nother);
+    long long rest = ax == 0 ? t / nl : t % nother;
+    int layer = (int)(ax == 0 ? t % nl : t / nother);
     int side = layer / ng, gl = layer % ng;
     int c1 = (int)(rest % N[o1]), c2 = (int)(rest / N[o1]);
     int d = side == 0 ? a1 - ng + gl : a2 + 1 + gl;
