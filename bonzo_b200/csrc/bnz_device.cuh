@@ -96,10 +96,21 @@ __device__ __forceinline__ double fms(const double* w, double gam) {
   return sqrt(0.5 / w[RHO] * (c1 + c2));
 }
 
+// 1/x: an IEEE division, or with NR in the fast build the Newton-refined
+// reciprocal of bnz_fastmath.cuh (within 2 ulp, for normal finite x)
+template <bool NR>
+__device__ __forceinline__ double rcp_nr(double x) {
+#if BNZ_FAST_MATH
+  if constexpr (NR) return bnz_nr_rcp(x);
+#endif
+  return 1. / x;
+}
+
 #if BNZ_FAST_MATH
 // fms of both face states with one division for the two 0.5 / rho
+template <bool NR = false>
 __device__ __forceinline__ void fms2(const double* wL, const double* wR, double gam, double& cfL, double& cfR) {
-  const double h = 0.5 / (wL[RHO] * wR[RHO]);
+  const double h = NR ? 0.5 * rcp_nr<NR>(wL[RHO] * wR[RHO]) : 0.5 / (wL[RHO] * wR[RHO]);
   double q[2];
 #pragma unroll
   for (int s = 0; s < 2; ++s) {
@@ -117,11 +128,12 @@ __device__ __forceinline__ void fms2(const double* wL, const double* wR, double 
 #endif
 
 // fluxes_c.c:25-42
+template <bool NR = false>
 __device__ __forceinline__ void wave_speeds(const double* wL, const double* wR, double gam,
                                             double& sL, double& sR) {
 #if BNZ_FAST_MATH
   double cfL, cfR;
-  fms2(wL, wR, gam, cfL, cfR);
+  fms2<NR>(wL, wR, gam, cfL, cfR);
 #else
   double cfL = fms(wL, gam);
   double cfR = fms(wR, gam);
@@ -334,7 +346,9 @@ __device__ __forceinline__ void flux_hllt(double* flux, const double* wL, const 
 // formulas.  The scalar star quantities (sM, p*, tangential star velocities
 // and fields) are formed for both sides, the side is chosen per lane, and the
 // 9-vectors are evaluated once -- about half the live registers of forming
-// both sides, with no warp divergence.
+// both sides, with no warp divergence.  NR (fast build only): the five
+// reciprocals by bnz_nr_rcp instead of IEEE divisions.
+template <bool NR = false>
 __device__ __forceinline__ void flux_hlld(double* flux, const double* wL, const double* wR, double gam,
                                           unsigned& err) {
   const double bx = wL[BX];
@@ -348,9 +362,9 @@ __device__ __forceinline__ void flux_hlld(double* flux, const double* wL, const 
   const double fmxL = mxL * wL[VX] + ptL - bx2;                   // f[MX]
   const double fmxR = mxR * wR[VX] + ptR - bx2;
   double sL, sR;
-  wave_speeds(wL, wR, gam, sL, sR);
+  wave_speeds<NR>(wL, wR, gam, sL, sR);
 
-  double deni = 1. / (sR * wR[RHO] - sL * wL[RHO] - (mxR - mxL));
+  double deni = rcp_nr<NR>(sR * wR[RHO] - sL * wL[RHO] - (mxR - mxL));
   double sM = (sR * mxR - sL * mxL - (fmxR - fmxL)) * deni;
 
   double sLvxL = sL - wL[VX];
@@ -358,7 +372,7 @@ __device__ __forceinline__ void flux_hlld(double* flux, const double* wL, const 
 #if BNZ_FAST_MATH
   // one division for both reciprocals (sL < sM < sR)
   const double dLM = sL - sM, dRM = sR - sM;
-  const double inv2 = 1. / (dLM * dRM);
+  const double inv2 = rcp_nr<NR>(dLM * dRM);
   double sLsMi = dRM * inv2;
   double sRsMi = dLM * inv2;
 #else
@@ -374,7 +388,7 @@ __device__ __forceinline__ void flux_hlld(double* flux, const double* wL, const 
   double rhosRvxR = wR[RHO] * sRvxR;
 #if BNZ_FAST_MATH
   const double DL = rhosLvxL * (sL - sM) - bx2, DR = rhosRvxR * (sR - sM) - bx2;
-  const double iD = 1. / (DL * DR);
+  const double iD = rcp_nr<NR>(DL * DR);
   double wvbL = DR * iD;
   double wvbR = DL * iD;
 #else
@@ -417,7 +431,7 @@ __device__ __forceinline__ void flux_hlld(double* flux, const double* wL, const 
   if (r == 0) err |= ERR_FAN;
 
   // double-star tangential state (needs both sides)
-  double rhoLRi = 1. / (sqrt_rhoLs + sqrt_rhoRs);
+  double rhoLRi = rcp_nr<NR>(sqrt_rhoLs + sqrt_rhoRs);
   double sgnb = sgnd(bx);
   double vyss = (sqrt_rhoLs * vyLs + sqrt_rhoRs * vyRs + (byRs - byLs) * sgnb) * rhoLRi;
   double vzss = (sqrt_rhoLs * vzLs + sqrt_rhoRs * vzRs + (bzRs - bzLs) * sgnb) * rhoLRi;
@@ -581,10 +595,11 @@ __device__ __forceinline__ void char2prim(double* vc, const double* w, double ga
   vc[BZ] = betaz * (As * (vc_rho + vc_bz) - Af * (vc_vy + vc_p)) + betay * s * rhosr * (vc_vx + vc_by);
 }
 
-template <int RS>
+// NR: the fast build's HLLD takes its reciprocals by bnz_nr_rcp
+template <int RS, bool NR = false>
 __device__ __forceinline__ void riemann(double* flux, const double* wL, const double* wR, double gam,
                                         unsigned& err) {
-  if constexpr (RS == RS_HLLD) flux_hlld(flux, wL, wR, gam, err);
+  if constexpr (RS == RS_HLLD) flux_hlld<NR>(flux, wL, wR, gam, err);
   else if constexpr (RS == RS_HLLT) flux_hllt(flux, wL, wR, gam, err);
   else if constexpr (RS == RS_HLLC) flux_hllc(flux, wL, wR, gam);
   else if constexpr (RS == RS_HLL_HYDRO) flux_hll_hydro(flux, wL, wR, gam);

@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(128) k_flux(GridDev g, const double* __restric
     wL[BX] = bx;
     wR[BX] = bx;
     double f[NM];
-    riemann<RS>(f, wL, wR, g.gam, e);
+    riemann<RS, true>(f, wL, wR, g.gam, e);
 #pragma unroll
     for (int n = 0; n < NM; ++n) F[perm<AX>(n) * g.sv + c] = f[n];
   }

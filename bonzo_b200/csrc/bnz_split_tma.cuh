@@ -406,7 +406,7 @@ __global__ void __launch_bounds__(256, 2) k_flux_tile_tma(GridDev g, const unsig
       wL[BX] = bx;
       wR[BX] = bx;
       double fl[NM];
-      riemann<RS>(fl, wL, wR, g.gam, e);
+      riemann<RS, true>(fl, wL, wR, g.gam, e);
 #pragma unroll
       for (int n = 0; n < NM; ++n)
         if (n != BX) F[plain::perm<AX>(n) * g.sv + c] = fl[n];
