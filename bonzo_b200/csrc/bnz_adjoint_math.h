@@ -32,6 +32,17 @@ constexpr int NM = 9;
 BNZ_HD double sq(double x) { return x * x; }
 BNZ_HD double sgn(double a) { return (double)((0.0 < a) - (a < 0.0)); }
 
+// a / b: in the fast build's device code a times the Newton-refined
+// reciprocal the forward HLLD uses (bnz_fastmath.cuh), elsewhere the IEEE
+// quotient
+BNZ_HD double quo(double a, double b) {
+#if BNZ_FAST_MATH && defined(__CUDA_ARCH__)
+  return a * bnz_nr_rcp(b);
+#else
+  return a / b;
+#endif
+}
+
 // w = cons2prim(u): given wbar, add ubar.  Expressed through w (the forward's
 // output), which holds rho, v and B.
 BNZ_HD void vjp_cons2prim(const double* w, const double* wb, double gam, double* ub) {
@@ -184,7 +195,7 @@ BNZ_HD double fms_val(const double* w, double gam) {
   const double gamp = gam * w[PR];
   const double c1 = gamp + b2;
   const double c2 = sqrt(fabs(c1 * c1 - 4. * gamp * bx2));
-  return sqrt(0.5 / w[RHO] * (c1 + c2));
+  return sqrt(quo(0.5, w[RHO]) * (c1 + c2));
 }
 
 // VJP of cf = fms(w) given its value cf (> 0)
@@ -196,14 +207,14 @@ BNZ_HD void vjp_fms(const double* w, double cf, double cfb, double gam, double* 
   const double c1 = gamp + b2;
   const double disc = c1 * c1 - 4. * gamp * bx2;
   const double c2 = sqrt(fabs(disc));
-  const double rhoi = 1. / w[RHO];
-  const double qb = cfb * 0.5 / cf;  // q = 0.5 / rho (c1 + c2)
+  const double rhoi = quo(1., w[RHO]);
+  const double qb = quo(cfb * 0.5, cf);  // q = 0.5 / rho (c1 + c2)
   wb[RHO] += -qb * 0.5 * rhoi * rhoi * (c1 + c2);
   double c1b = qb * 0.5 * rhoi;
   const double c2b = c1b;
   double gampb = 0., bx2b = 0., b2b = 0.;
   if (c2 > 0.) {
-    const double discb = c2b * 0.5 / c2 * sgn(disc);
+    const double discb = quo(c2b * 0.5, c2) * sgn(disc);
     c1b += 2. * c1 * discb;
     gampb -= 4. * bx2 * discb;
     bx2b -= 4. * gamp * discb;
@@ -517,14 +528,14 @@ BNZ_HD void vjp_hlld(const double* wL, const double* wR, double gam, const doubl
   const double sL = (vxL < vxR ? vxL : vxR) - cfm;
   const double sR = (vxL > vxR ? vxL : vxR) + cfm;
   const double den = sR * rR - sL * rL - (mxR - mxL);
-  const double deni = 1. / den;
+  const double deni = quo(1., den);
   const double num = sR * mxR - sL * mxL - (fmxR - fmxL);
   const double sM = num * deni;
   const double sLvxL = sL - vxL, sRvxR = sR - vxR;
 #if BNZ_FAST_MATH && defined(__CUDA_ARCH__)
   // the fast forward's forms (bnz_device.cuh flux_hlld): one division for both
   const double dLM = sL - sM, dRM = sR - sM;
-  const double inv2 = 1. / (dLM * dRM);
+  const double inv2 = quo(1., dLM * dRM);
   const double sLsMi = dRM * inv2, sRsMi = dLM * inv2;
 #else
   const double sLsMi = 1. / (sL - sM), sRsMi = 1. / (sR - sM);
@@ -535,7 +546,7 @@ BNZ_HD void vjp_hlld(const double* wL, const double* wR, double gam, const doubl
   const double rvL = rL * sLvxL, rvR = rR * sRvxR;
 #if BNZ_FAST_MATH && defined(__CUDA_ARCH__)
   const double DL = rvL * (sL - sM) - bx2, DR = rvR * (sR - sM) - bx2;
-  const double iD = 1. / (DL * DR);
+  const double iD = quo(1., DL * DR);
   const double wvbL = DR * iD, wvbR = DL * iD;
 #else
   const double wvbL = 1. / (rvL * (sL - sM) - bx2), wvbR = 1. / (rvR * (sR - sM) - bx2);
@@ -567,7 +578,7 @@ BNZ_HD void vjp_hlld(const double* wL, const double* wR, double gam, const doubl
   if (sR <= 0.) r = 6;
   if (r == 0) return;
   const double dsum = srL + srR;
-  const double rhoLRi = 1. / dsum;
+  const double rhoLRi = quo(1., dsum);
   const double sgnb = sgn(bx);
   const double Nvy = srL * vyLs + srR * vyRs + (byRs - byLs) * sgnb;
   const double Nvz = srL * vzLs + srR * vzRs + (bzRs - bzLs) * sgnb;

@@ -367,7 +367,7 @@ __device__ __forceinline__ void stage_fluxes(const Inst& I, const Tile& T, const
     }
     wL[BX] = wR[BX] = xf ? F.template get<0>(i, j) : F.template get<1>(i, j);
     double f[NM];
-    riemann<RS>(f, wL, wR, I.gam, err);
+    riemann<RS, true>(f, wL, wR, I.gam, err);
     if (xf) {
 #pragma unroll
       for (int n = 0; n < 6; ++n) sFX[n * L.sfx + qq] = f[n];
@@ -476,7 +476,7 @@ __device__ __forceinline__ void stage_fluxes_plm(const Inst& I, const Tile& T, c
       }
       wL[BX] = wR[BX] = b[(long long)j * I.nx + i];
       double f[NM];
-      riemann<RS>(f, wL, wR, I.gam, err);
+      riemann<RS, true>(f, wL, wR, I.gam, err);
       const int qq = L.fx(fi, fj);
 #pragma unroll
       for (int n = 0; n < 6; ++n) sFX[n * L.sfx + qq] = f[n];
@@ -506,7 +506,7 @@ __device__ __forceinline__ void stage_fluxes_plm(const Inst& I, const Tile& T, c
       }
       wL[BX] = wR[BX] = b[I.sv + (long long)j * I.nx + i];
       double f[NM];
-      riemann<RS>(f, wL, wR, I.gam, err);
+      riemann<RS, true>(f, wL, wR, I.gam, err);
       const int qq = L.fy(fi, fj);
       sFY[0 * L.sfy + qq] = f[RHO];
       sFY[1 * L.sfy + qq] = f[VZ];   // global MX

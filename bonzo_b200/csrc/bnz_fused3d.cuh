@@ -399,7 +399,7 @@ __device__ __forceinline__ void flux_item(const March<ORDER>& M, int q, int t, i
   }
   wL[BX] = wR[BX] = bn;
   double f[NM];
-  riemann<RS>(f, wL, wR, I.gam, e);
+  riemann<RS, true>(f, wL, wR, I.gam, e);
   // local sweep frame -> global variables (godunov.pyx:297-324)
   if (dir == 0) {
     double* FX = M.S.fx(q);
